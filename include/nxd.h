@@ -1,0 +1,276 @@
+/*
+ * nxd.h — C ABI of the B200 contact step for NexDynIPC-style rigid-body IPC.
+ *
+ * Every entry point takes plain pointers and sizes; no CUDA or torch types
+ * appear in a signature.  Each function names the reference interface it
+ * replaces (paths are relative to the NexDynIPC project root).
+ *
+ * Conventions
+ *  - Bodies are addressed by world index (position in World::bodies).  The
+ *    reference maps RigidBody::id -> world index through hash maps
+ *    (nexdynipc/src/Dynamics/IPCSolver.cpp:401-405); descriptors carry the ids
+ *    so joints and candidates can be expressed in the reference's id space.
+ *  - The optimisation vector x has 6 entries per body, [p_x p_y p_z th_x th_y
+ *    th_z], th an incremental rotation vector applied as exp(th)*q_ref
+ *    (IPCSolver.cpp:839-857, JointPrimitives.h:11-19).
+ *  - Quaternions are stored (w, x, y, z).
+ *  - All arithmetic is IEEE FP64; indices are int32.
+ *  - A context owns every device buffer it uses.  Pointers passed in are host
+ *    pointers unless a function says otherwise.
+ */
+#ifndef NXD_H
+#define NXD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (per call).  The reference signals failures only through
+ * booleans (NewtonSolver::minimize, LinearSolver::info); these codes add the
+ * cases a device implementation can hit. */
+typedef enum nxd_status {
+    NXD_OK = 0,
+    NXD_NOT_CONVERGED = 1,     /* Newton hit its iteration cap            */
+    NXD_LS_FAILED = 2,         /* line search returned alpha = 0          */
+    NXD_FACTOR_FAILED = 3,     /* zero pivot in the LDL^T factorisation   */
+    NXD_CAPACITY = 4,          /* a fixed-size device buffer overflowed   */
+    NXD_NAN = 5,               /* non-finite state detected               */
+    NXD_TIMEOUT = 6,           /* a bounded device loop hit its limit     */
+    NXD_INVALID_ARGUMENT = 7,
+    NXD_CUDA_ERROR = 8,
+    NXD_NO_DEVICE = 9
+} nxd_status;
+
+/* Joint kinds, in the reference's class names. */
+enum {
+    NXD_JOINT_HINGE = 0,        /* HingeJoint       (Joints/HingeJoint.cpp)       */
+    NXD_JOINT_FIXED = 1,        /* FixedJoint       (Joints/FixedJoint.cpp)       */
+    NXD_JOINT_SPHERICAL = 2,    /* SphericalJoint   (Joints/SphericalJoint.cpp)   */
+    NXD_JOINT_ANGLE_LIMIT = 3   /* AngleLimitJoint  (Joints/AngleLimitJoint.cpp)  */
+};
+#define NXD_JOINT_PARAMS 16
+
+/* Per-joint parameter layout inside nxd_scene_desc.joint_params (16 doubles):
+ *   hinge:       anchorA[3] anchorB[3] axisA[3] axisB[3]      (HingeJoint ctor)
+ *   fixed:       target_position[3] target_orientation[4] (w,x,y,z) (FixedJoint ctor)
+ *   spherical:   anchorA[3] anchorB[3]                        (SphericalJoint ctor)
+ *   angle limit: axis[3] min_angle_rad max_angle_rad          (AngleLimitJoint ctor)
+ */
+
+#define NXD_DRIVE_PARAMS 8
+/* Velocity drive (Control/VelocityDriveForm.cpp) parameter layout, 8 doubles:
+ *   axis[3] kv v_target max_torque(<=0: unlimited) delay_radps delay_tau_s */
+
+/* Solver settings: IPCSolver setters (Dynamics/IPCSolver.h:34-79) and
+ * NewtonSolver::Options (Math/NewtonSolver.h:58-64). */
+typedef struct nxd_settings {
+    double dhat;                     /* setContactDistanceThreshold            */
+    double contact_stiffness;        /* setContactStiffness (>0 to apply)      */
+    int32_t enable_adaptive_barrier; /* enableAdaptiveBarrier                  */
+    int32_t enable_ccd;              /* enableCCD                              */
+    double ccd_safety_factor;        /* setCCDSafetyFactor                     */
+    int32_t enable_friction;         /* enableFriction                         */
+    int32_t alm_max_iters;           /* setALMMaxIters                         */
+    double friction_coeff;           /* setFrictionCoefficient                 */
+    double alm_constraint_tol;       /* setALMConstraintTolerance              */
+    double alm_dual_tol;             /* setALMDualTolerance                    */
+    double alm_contact_tol;          /* setALMContactTolerance                 */
+    double alm_hardening_trigger;    /* setALMHardeningTrigger                 */
+    double alm_hardening_ratio;      /* setALMHardeningRatio                   */
+    int32_t newton_max_iters;        /* Options::max_iterations                */
+    int32_t ls_max_iters;            /* BacktrackingLineSearch::max_iter       */
+    double newton_tol;               /* Options::tolerance                     */
+    double ls_c1;                    /* Options::line_search_c1                */
+    double ls_rho;                   /* Options::line_search_rho               */
+} nxd_settings;
+
+/* Fill an nxd_settings with the reference's defaults
+ * (IPCSolver.h:97-119, NewtonSolver.h:58-64, LineSearch.h:36-38). */
+void nxd_default_settings(nxd_settings* s);
+
+/* A World: bodies, triangle meshes, joints and velocity drives
+ * (Dynamics/World.h:11-17, Dynamics/RigidBody.h:11-38). */
+typedef struct nxd_scene_desc {
+    int32_t n_bodies;
+    const int32_t* body_ids;             /* [n]   RigidBody::id                   */
+    const double* position;              /* [n*3]                                 */
+    const double* orientation;           /* [n*4] (w,x,y,z)                       */
+    const double* velocity;              /* [n*3]                                 */
+    const double* angular_velocity;      /* [n*3]                                 */
+    const double* linear_acceleration;   /* [n*3] or NULL (zero)                  */
+    const double* angular_acceleration;  /* [n*3] or NULL (zero)                  */
+    const double* mass;                  /* [n]                                   */
+    const double* inertia_body;          /* [n*9] row-major, body frame           */
+    const int32_t* vertex_offset;        /* [n+1] prefix offsets into vertices    */
+    const double* vertices;              /* [nv*3] local coordinates (MeshShape)  */
+    const int32_t* face_offset;          /* [n+1] prefix offsets into faces       */
+    const int32_t* faces;                /* [nf*3] body-local vertex indices      */
+    int32_t n_joints;                    /* World::joints, in order               */
+    const int32_t* joint_type;           /* [n_joints] NXD_JOINT_*                */
+    const int32_t* joint_body_a;         /* [n_joints] body id (fixed: the body)  */
+    const int32_t* joint_body_b;         /* [n_joints] body id (fixed: -1)        */
+    const double* joint_params;          /* [n_joints*16]                         */
+    const double* joint_stiffness;       /* [n_joints] ALM penalty mu             */
+    int32_t n_drives;                    /* VelocityDriveForm entries of World::forms */
+    const int32_t* drive_body_a;         /* [n_drives] body id or -1 (world)      */
+    const int32_t* drive_body_b;         /* [n_drives] body id                    */
+    const double* drive_params;          /* [n_drives*8]                          */
+    nxd_settings settings;
+} nxd_scene_desc;
+
+/* Body state as written back by IPCSolver::step (IPCSolver.cpp:1174-1195). */
+typedef struct nxd_state {
+    double* position;              /* [n*3] */
+    double* orientation;           /* [n*4] (w,x,y,z) */
+    double* velocity;              /* [n*3] */
+    double* angular_velocity;      /* [n*3] */
+    double* linear_acceleration;   /* [n*3] */
+    double* angular_acceleration;  /* [n*3] */
+} nxd_state;
+
+/* ContactPair (Dynamics/Forms/FrictionForm.h:13-22), reordered for alignment. */
+typedef struct nxd_contact {
+    double point[3];
+    double normal[3];
+    double distance;
+    int32_t body_a;          /* world index */
+    int32_t body_b;          /* world index */
+    int32_t primitive_type;  /* 0 vertex-face or vertex-vertex, 1 edge-edge */
+    int32_t primitive_a;
+    int32_t primitive_b;
+    int32_t pad_;
+} nxd_contact;
+
+/* ContactCandidateSet (Physics/Contact/ContactAssembler.h:12-55).  Buffers are
+ * caller-owned int32 arrays; *_cap give their capacity in records; the call
+ * always writes the full counts, and fails with NXD_CAPACITY if a buffer was
+ * too small (records past the capacity are not written).  Any pointer may be
+ * NULL to query counts only. */
+typedef struct nxd_candidates {
+    int32_t* vv; int64_t vv_cap; int64_t vv_count;  /* 4 ints: body0 body1 v0 v1            */
+    int32_t* ev; int64_t ev_cap; int64_t ev_count;  /* 5 ints: ebody vbody e_v0 e_v1 v        */
+    int32_t* ee; int64_t ee_cap; int64_t ee_count;  /* 6 ints: body0 body1 e0v0 e0v1 e1v0 e1v1 */
+    int32_t* fv; int64_t fv_cap; int64_t fv_count;  /* 4 ints: fbody vbody face vertex        */
+} nxd_candidates;
+
+/* Per-step diagnostics: IPCSolver's last-step KPI getters
+ * (IPCSolver.h:82-90) plus device-side counters. */
+typedef struct nxd_diagnostics {
+    double kappa;                    /* AdaptiveBarrier::currentStiffness       */
+    double dhat;                     /* AdaptiveBarrier::currentDhat            */
+    double actual_dt;                /* computeMaxStep result                   */
+    double last_dual_residual;
+    double last_contact_residual;
+    double last_max_constraint_violation;
+    double last_angular_velocity_error;
+    double last_torque_saturation_ratio;
+    double scene_min_distance;       /* last computeSceneMinDistance (exact when < 1e-6) */
+    int32_t alm_iterations;          /* ALM iterations run in the last step     */
+    int32_t newton_iterations;       /* Newton iterations summed over ALM       */
+    int32_t newton_converged;        /* last Newton call's return value         */
+    int32_t n_body_pairs;            /* candidate body pairs (activation dhat)  */
+    int32_t n_contacts;              /* contacts after the last detection       */
+    int32_t n_contacts_raw;          /* before the 2000-contact cap             */
+    int32_t status;                  /* sticky nxd_status of device loops       */
+    int32_t line_search_failures;    /* Newton calls that ended with alpha = 0  */
+} nxd_diagnostics;
+
+/* Form selectors for nxd_form_* (SimulationProblem, IPCSolver.cpp:137-262). */
+enum {
+    NXD_FORM_INERTIA = 0,     /* InertiaForm                     */
+    NXD_FORM_GRAVITY = 1,     /* GravityForm (unscaled)          */
+    NXD_FORM_CONSTRAINT = 2,  /* ConstraintForm over all joints  */
+    NXD_FORM_BARRIER = 3,     /* DistanceBarrierForm (unscaled)  */
+    NXD_FORM_FRICTION = 4,    /* FrictionForm (unscaled)         */
+    NXD_FORM_DRIVES = 5,      /* sum of VelocityDriveForms       */
+    NXD_FORM_TOTAL = 6,       /* SimulationProblem::computeValue / computeGradient */
+    NXD_FORM_CONTACT = 7      /* SimulationProblem::computeContactValue / Gradient */
+};
+
+typedef struct nxd_ctx nxd_ctx;
+
+/* World + IPCSolver construction (App/Simulation.cpp:14-58 configuration
+ * part).  Uploads the scene; afterwards no call allocates device memory
+ * except when a capacity has to grow (documented per call). */
+nxd_status nxd_create(const nxd_scene_desc* desc, nxd_ctx** out);
+void nxd_destroy(nxd_ctx* ctx);
+
+/* Bind the context to a CUDA stream (a cudaStream_t passed as void*). */
+nxd_status nxd_set_stream(nxd_ctx* ctx, void* stream);
+
+/* IPCSolver::step(World&, double dt) (Dynamics/IPCSolver.cpp:808-1231). */
+nxd_status nxd_step(nxd_ctx* ctx, double dt);
+
+/* Read / overwrite body state (host pointers). */
+nxd_status nxd_get_state(nxd_ctx* ctx, const nxd_state* out);
+nxd_status nxd_set_state(nxd_ctx* ctx, const nxd_state* in);
+nxd_status nxd_get_diagnostics(nxd_ctx* ctx, nxd_diagnostics* out);
+/* ALM multipliers and stiffness per joint (Joint::lambda_, Joint::mu_),
+ * lambda as 6 doubles per joint (unused rows zero). */
+nxd_status nxd_get_joint_state(nxd_ctx* ctx, double* lambda6, double* stiffness);
+
+/* ContactAssembler::detectBodyPairs (ContactAssembler.cpp:156-178) on the
+ * current poses.  pairs: [cap*2] world indices, in the reference's order. */
+nxd_status nxd_body_pairs(nxd_ctx* ctx, double inflation_radius,
+                          int32_t* pairs, int64_t cap, int64_t* count);
+
+/* ContactAssembler::buildCandidateSet (ContactAssembler.cpp:214-343) on the
+ * current poses. */
+nxd_status nxd_build_candidates(nxd_ctx* ctx, double activation_distance,
+                                nxd_candidates* out);
+
+/* IPCSolver::detectContacts (IPCSolver.cpp:394-580) when x == NULL, else
+ * IPCSolver::detectContactsAtState(world, x) (IPCSolver.cpp:582-806), over
+ * the candidate set of the current poses with the context's current dhat. */
+nxd_status nxd_detect_contacts(nxd_ctx* ctx, const double* x,
+                               nxd_contact* out, int32_t cap, int32_t* count);
+
+/* computeSceneMinDistance (Physics/Contact/AdaptiveBarrier.h:130-162).  The
+ * value equals the reference's whenever the reference's is below 1e-6 (the
+ * only use, AdaptiveBarrier::updateStiffness, compares it with 1e-9);
+ * otherwise the call returns a value >= 1e-6 or +inf. */
+nxd_status nxd_scene_min_distance(nxd_ctx* ctx, double* out);
+
+/* IPCSolver::computeMaxStep (IPCSolver.cpp:355-392) with
+ * CCDSystem::computeEarliestTOI (Physics/Contact/CCD/CCD.h:22-82). */
+nxd_status nxd_max_step(nxd_ctx* ctx, double dt, double* out_dt);
+
+/* Form plugin interface (Dynamics/Forms/Form.h:8-21) evaluated at x against
+ * the contacts / normal forces / predictive state installed below.
+ * value: energy; gradient: overwrites grad[6n]; hessian: dense block rows of
+ * the 6x6 block-sparse matrix as a BSR with caller buffers
+ * (row_ptr[n+1], col_idx[cap], vals[cap*36] row-major blocks). */
+nxd_status nxd_form_value(nxd_ctx* ctx, int32_t form, const double* x, double* out);
+nxd_status nxd_form_gradient(nxd_ctx* ctx, int32_t form, const double* x, double* grad);
+nxd_status nxd_form_hessian_bsr(nxd_ctx* ctx, int32_t form, const double* x,
+                                int32_t* row_ptr, int32_t* col_idx, double* vals,
+                                int64_t cap, int64_t* nnzb);
+
+/* DistanceBarrierForm::updateContacts + FrictionForm::updateContactPoints +
+ * FrictionForm::updateNormalForces (normal_forces may be NULL: none) and
+ * InertiaForm::setPredictiveState (x_hat may be NULL: keep). */
+nxd_status nxd_set_form_state(nxd_ctx* ctx, const nxd_contact* contacts, int32_t n,
+                              const double* normal_forces, const double* x_hat,
+                              double dt);
+
+/* DistanceBarrierForm::computeNormalForces (DistanceBarrierForm.cpp:70-86). */
+nxd_status nxd_normal_forces(nxd_ctx* ctx, const double* x, double* out, int32_t n);
+
+/* Batched form (independent scenes, one launch per phase for all of them). */
+typedef struct nxd_batch nxd_batch;
+nxd_status nxd_batch_create(const nxd_scene_desc* descs, int32_t n_scenes, nxd_batch** out);
+void nxd_batch_destroy(nxd_batch* b);
+nxd_status nxd_batch_step(nxd_batch* b, const double* dts);
+nxd_status nxd_batch_get_state(nxd_batch* b, int32_t scene, const nxd_state* out);
+nxd_status nxd_batch_get_diagnostics(nxd_batch* b, int32_t scene, nxd_diagnostics* out);
+
+/* Library version string. */
+const char* nxd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NXD_H */

@@ -1,0 +1,687 @@
+// nxd.cu — host side of the B200 contact step: the context that owns every
+// device buffer, the per-step kernel sequence of IPCSolver::step, and the C
+// ABI declared in include/nxd.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <unordered_set>
+#include <vector>
+
+#include "../../include/nxd.h"
+#include "step.cuh"
+
+using namespace nx;
+
+namespace {
+
+#define NXD_CUDA(call)                                                   \
+    do {                                                                 \
+        cudaError_t e_ = (call);                                         \
+        if (e_ != cudaSuccess) {                                         \
+            std::fprintf(stderr, "nxd: %s failed: %s\n", #call, cudaGetErrorString(e_)); \
+            return NXD_CUDA_ERROR;                                       \
+        }                                                                \
+    } while (0)
+
+struct DevArena {
+    std::vector<void*> ptrs;
+    bool ok = true;
+    template <typename T>
+    T* alloc(size_t n) {
+        void* p = nullptr;
+        if (n == 0) n = 1;
+        if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) { ok = false; return nullptr; }
+        cudaMemset(p, 0, n * sizeof(T));
+        ptrs.push_back(p);
+        return static_cast<T*>(p);
+    }
+    template <typename T>
+    T* upload(const T* h, size_t n) {
+        T* d = alloc<T>(n);
+        if (d && h && n) cudaMemcpy(d, h, n * sizeof(T), cudaMemcpyHostToDevice);
+        return d;
+    }
+    void release() {
+        for (void* p : ptrs) cudaFree(p);
+        ptrs.clear();
+    }
+};
+
+int pow2_ceil_host(int n) {
+    int p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
+int grid_for(long long n, int block, int max_blocks = 1 << 16) {
+    long long g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > max_blocks) g = max_blocks;
+    return (int)g;
+}
+
+}  // namespace
+
+struct nxd_ctx {
+    DevArena mem;
+    cudaStream_t stream = nullptr;
+    int dev = 0, n_sm = 148;
+    int N = 0, nv = 0, nf = 0, ne = 0, J = 0, D = 0;
+    int max_prims = 0;
+    int pair_cap = 0;
+    long long item_cap = 0;
+    nxd_settings s{};
+    std::vector<int> h_body_ids;
+    std::vector<int> h_voff, h_foff, h_eoff;
+    // static device data
+    Geo geo{};
+    int *voff, *foff, *eoff, *faces, *edges, *vbody, *has_mesh, *body_ids;
+    double *verts, *lmin, *lmax, *md_tol, *max_md_tol;
+    double *mass, *inertia;
+    int *jtype, *ja, *jb, *jinc_off, *jinc;
+    double *jparams, *jmu, *jlam;
+    int *da, *db, *dinc_off, *dinc, *dfinit, *dhas_prev;
+    Drv* dprm;
+    double *dfilt, *dprevA, *dprevB;
+    // state
+    double *pos, *quat, *vel, *omega, *lacc, *aacc;
+    // per step
+    double *boxes, *wv, *wvx, *pose_p, *pose_q;
+    double *x, *xhat, *xprev, *vprev, *aprev, *pos0, *quat0;
+    int *pair_cnt, *pair_off, *pairs, *md_pairs;
+    int *topk, *topn;
+    int *nfv, *nee, *nvv, *nev, *off_fv, *off_ee, *off_vv, *off_ev;
+    int *hit_cnt, *hit_off;
+    unsigned char* flags;
+    ContactRec *contacts, *contacts_tmp;
+    double* sort_key;
+    int* sort_idx;
+    double* nforce;
+    Scalars* sc;
+    int* i_scratch;   // small int scalars for scans
+    // solver scratch
+    Solver S{};
+    int cand_stride = 0;
+};
+
+namespace {
+
+void fill_solver(nxd_ctx* c) {
+    Solver& S = c->S;
+    const int N = c->N, J = c->J, D = c->D, C = kMaxRawContacts;
+    DevArena& m = c->mem;
+    S.N = N; S.J = J; S.D = D; S.Cmax = C;
+    S.mass = c->mass; S.inertia = c->inertia;
+    S.pos0 = c->pos0; S.quat0 = c->quat0;
+    S.x = c->x; S.xhat = c->xhat;
+    S.jtype = c->jtype; S.ja = c->ja; S.jb = c->jb; S.jparams = c->jparams; S.jmu = c->jmu; S.jlam = c->jlam;
+    S.jinc_off = c->jinc_off; S.jinc = c->jinc;
+    S.da = c->da; S.db = c->db; S.dprm = c->dprm; S.dprevA = c->dprevA; S.dprevB = c->dprevB;
+    S.dhas_prev = c->dhas_prev; S.dfilt = c->dfilt; S.dinc_off = c->dinc_off; S.dinc = c->dinc;
+    S.contacts = c->contacts; S.ncontacts_ptr = &c->sc->n_contacts;
+    S.nforce = c->nforce; S.nnf_ptr = &c->sc->nnf;
+    S.cinc_off = m.alloc<int>(N + 1); S.cinc = m.alloc<int>(2 * C); S.cinc_cnt = m.alloc<int>(N + 1);
+    S.dt_ptr = &c->sc->dt; S.bdhat_ptr = &c->sc->bdhat; S.bkappa_ptr = &c->sc->bkappa;
+    S.barrier_in_forms_ptr = &c->sc->barrier_in_forms; S.friction_form_ptr = &c->sc->friction_form;
+    S.friction_mu = c->s.friction_coeff; S.friction_eps = 1e-8;
+    S.newton_max_iters = c->s.newton_max_iters; S.ls_max_iters = c->s.ls_max_iters;
+    S.newton_tol = c->s.newton_tol; S.ls_c1 = c->s.ls_c1; S.ls_rho = c->s.ls_rho;
+    S.alm_constraint_tol = c->s.alm_constraint_tol; S.alm_hardening_trigger = c->s.alm_hardening_trigger;
+    S.alm_hardening_ratio = c->s.alm_hardening_ratio;
+    const int redn = pow2_ceil_host(std::max({6 * N, J, 2 * C, 1}));
+    S.g = m.alloc<double>(6 * N); S.cg = m.alloc<double>(6 * N); S.dx = m.alloc<double>(6 * N);
+    S.xt = m.alloc<double>(6 * N); S.red = m.alloc<double>(redn);
+    S.qj = m.alloc<double>(4 * N); S.qg = m.alloc<double>(4 * N);
+    S.jC = m.alloc<double>(6 * J); S.jF = m.alloc<double>(6 * J); S.jJ = m.alloc<double>(72 * J);
+    S.jE = m.alloc<double>(J); S.jact = m.alloc<int>(J);
+    S.bD = m.alloc<double>(C); S.bGP = m.alloc<double>(C); S.bHP = m.alloc<double>(C); S.bE = m.alloc<double>(C);
+    S.fFG = m.alloc<double>(3 * C); S.fHF = m.alloc<double>(9 * C); S.fJA = m.alloc<double>(18 * C);
+    S.fJB = m.alloc<double>(18 * C); S.fE = m.alloc<double>(C);
+    S.dE = m.alloc<double>(D); S.dG = m.alloc<double>(D); S.dH = m.alloc<double>(D);
+    S.Hd = m.alloc<double>(36 * N);
+    S.parent = m.alloc<int>(N); S.comp = m.alloc<int>(N); S.comp_size = m.alloc<int>(N + 1);
+    S.comp_off = m.alloc<int>(N + 1); S.members = m.alloc<int>(N); S.local = m.alloc<int>(N);
+    S.items = m.alloc<int>(J + 2 * C); S.item_comp_off = m.alloc<int>(N + 1); S.item_list = m.alloc<int>(J + 2 * C);
+    S.n_items_ptr = m.alloc<int>(1); S.deg = m.alloc<int>(N + 1);
+    const long long pool_doubles = std::min<long long>(64LL * 1024 * 1024, std::max<long long>(1 << 20, 36LL * N * 64));
+    S.pool = m.alloc<double>(pool_doubles); S.pool_cap = pool_doubles; S.pool_off = m.alloc<long long>(1);
+    const long long nzb_bytes = std::max<long long>(1 << 20, (long long)N * 64);
+    S.nzb = m.alloc<unsigned char>(nzb_bytes); S.nzb_cap = nzb_bytes; S.nzb_off = m.alloc<long long>(1);
+    c->cand_stride = 6 * kMaxComponentBodies + 2 * kMaxComponentBodies;
+    S.cand = m.alloc<int>((size_t)c->cand_stride * (kSolverThreads / 32)); S.cand_stride = c->cand_stride;
+    S.dvec = m.alloc<double>(12 * N);
+    S.alm_done = &c->sc->alm_done; S.status = &c->sc->status; S.newton_iters = &c->sc->newton_iters;
+    S.converged = &c->sc->converged; S.ls_fail = &c->sc->ls_fail;
+    S.alm_mcv = m.alloc<double>(1); S.alm_dual = m.alloc<double>(1);
+}
+
+StepCfg step_cfg(const nxd_ctx* c) {
+    StepCfg k;
+    k.N = c->N; k.D = c->D;
+    k.enable_adaptive = c->s.enable_adaptive_barrier;
+    k.enable_friction = c->s.enable_friction;
+    k.friction_coeff = c->s.friction_coeff;
+    k.alm_constraint_tol = c->s.alm_constraint_tol;
+    k.alm_dual_tol = c->s.alm_dual_tol;
+    k.alm_contact_tol = c->s.alm_contact_tol;
+    return k;
+}
+
+// ContactAssembler::build + world vertices at the current poses
+void launch_assembly(nxd_ctx* c) {
+    k_body_boxes<<<grid_for(c->N, 128), 128, 0, c->stream>>>(c->geo, c->pos, c->quat, c->boxes);
+    k_world_vertices<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(c->geo, c->nv, c->vbody, c->pos, c->quat, c->wv);
+}
+
+// pair list (count / scan / write) with query q into out, count -> *count_dev
+void launch_pairs(nxd_ctx* c, const PairQuery& q, int* out, int* count_dev, const int* gate) {
+    const int blocks = grid_for((long long)c->N * 32, 256);
+    k_pairs<<<blocks, 256, 0, c->stream>>>(c->geo, q, c->boxes, c->pair_cnt, nullptr, nullptr, 0, gate);
+    k_scan<<<1, 1024, 0, c->stream>>>(c->pair_cnt, c->pair_off, c->N, count_dev, gate);
+    k_pairs<<<blocks, 256, 0, c->stream>>>(c->geo, q, c->boxes, nullptr, c->pair_off, out, c->pair_cap, gate);
+}
+
+size_t topk_smem(const nxd_ctx* c, int warps) {
+    return (size_t)warps * (((size_t)c->max_prims * (sizeof(double) + 3 * sizeof(int)) + 31) / 16 * 16);
+}
+
+// buildCandidateSet with activation distance = *dhat (device) -> pairs, topk, item offsets
+void launch_candidates(nxd_ctx* c, const double* act_ptr, double act_val) {
+    PairQuery q{1, act_ptr, act_val, 1.0, 1.0};
+    launch_pairs(c, q, c->pairs, &c->sc->n_pairs, nullptr);
+    int warps = 4;
+    while (warps > 1 && topk_smem(c, warps) > 200 * 1024) --warps;
+    k_topk<<<c->n_sm * 4, 32 * warps, topk_smem(c, warps), c->stream>>>(c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap,
+                                                                       c->boxes, c->wv, c->topk, c->topn, c->max_prims);
+    k_item_counts<<<grid_for(c->pair_cap, 256), 256, 0, c->stream>>>(&c->sc->n_pairs, c->pair_cap, c->topn, c->nfv,
+                                                                       c->nee, c->nvv, c->nev);
+    const int* np = &c->sc->n_pairs;
+    k_scan<<<1, 1024, 0, c->stream>>>(c->nfv, c->off_fv, c->pair_cap, &c->sc->fv_items, nullptr, nullptr, np);
+    k_scan<<<1, 1024, 0, c->stream>>>(c->nee, c->off_ee, c->pair_cap, &c->sc->ee_items, nullptr, nullptr, np);
+    k_scan<<<1, 1024, 0, c->stream>>>(c->nvv, c->off_vv, c->pair_cap, &c->sc->vv_items, nullptr, nullptr, np);
+}
+
+}  // namespace
+
+namespace {
+
+// detectContacts (current poses) or detectContactsAtState(x) over the step's
+// candidate set: FV then EE passes (hit counts, ordered writes), the VV
+// fallback when both found nothing, then the raw cap and the 2000 cap.
+// skip_if (device flag, may be null) skips the whole detection.
+void launch_narrow_full(nxd_ctx* c, const double* wv, const double* pose_p, const int* skip_if) {
+    NarrowIn in{c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap, c->topk, c->topn, wv, pose_p, &c->sc->dhat};
+    const int blocks = c->n_sm * 8;
+    int* skip_vv = c->i_scratch;
+    const int* np = &c->sc->n_pairs;
+    k_narrow_count<<<blocks, 256, 0, c->stream>>>(in, 0, c->off_fv, c->flags, c->hit_cnt, skip_if);
+    k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->fv_hits, nullptr, skip_if, np);
+    k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 0, c->off_fv, c->flags, c->hit_off, nullptr, c->contacts, skip_if);
+    k_narrow_count<<<blocks, 256, 0, c->stream>>>(in, 1, c->off_ee, c->flags, c->hit_cnt, skip_if);
+    k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->ee_hits, nullptr, skip_if, np);
+    k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 1, c->off_ee, c->flags, c->hit_off, &c->sc->fv_hits, c->contacts,
+                                                  skip_if);
+    k_contact_totals<<<1, 1, 0, c->stream>>>(c->sc, 0, skip_if, skip_vv);
+    k_narrow_count<<<blocks, 256, 0, c->stream>>>(in, 2, c->off_vv, c->flags, c->hit_cnt, skip_vv);
+    k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->vv_hits, nullptr, skip_vv, np);
+    k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 2, c->off_vv, c->flags, c->hit_off, nullptr, c->contacts, skip_vv);
+    k_contact_totals<<<1, 1, 0, c->stream>>>(c->sc, 1, skip_if, nullptr);
+    k_sort_contacts<<<1, 1024, 0, c->stream>>>(c->sc, c->contacts, c->contacts_tmp, c->sort_key, c->sort_idx, skip_if);
+}
+
+}  // namespace
+
+// A detection pass inside an ALM iteration runs only when the iteration runs
+// and a contact form exists; fold both conditions into one skip flag.
+__global__ void k_alm_detect_gate(const Scalars* sc, int* skip) {
+    *skip = (sc->alm_done || !(sc->barrier_form || sc->friction_form)) ? 1 : 0;
+}
+__global__ void k_init_scalar_d(double* p, double v) { *p = v; }
+__global__ void k_max_tol(const double* tol, int n, double* out) {
+    double m = 0.0;
+    for (int i = 0; i < n; ++i) m = dmax(m, tol[i]);
+    *out = m;
+}
+__global__ void k_body_md_tol(Geo g, const double* pos, double* tol) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.N) return;
+    const double diag = norm(ld3(g.lmax + 3 * i) - ld3(g.lmin + 3 * i));
+    tol[i] = 4e-6 * diag + 1e-9 * (1.0 + norm(ld3(pos + 3 * i)) + diag);
+}
+
+namespace {
+
+nxd_status enqueue_step(nxd_ctx* c, double dt) {
+    cudaStream_t st = c->stream;
+    const StepCfg cfg = step_cfg(c);
+    // ContactAssembler::build + buildCandidateSet(currentDhat)
+    launch_assembly(c);
+    launch_candidates(c, &c->sc->dhat, 0.0);
+    // adaptive barrier (IPCSolver.cpp:817-832)
+    if (c->s.enable_adaptive_barrier) {
+        k_barrier_init<<<1, 1024, 0, st>>>(cfg, c->mass, c->pos, c->sc, c->S.red);
+        k_init_scalar_d<<<1, 1, 0, st>>>(&c->sc->bmd, INFINITY);
+        PairQuery qb{0, &c->sc->dhat, 0.0, 2.0, 0.0};
+        k_min_pair_distance<<<grid_for((long long)c->N * 32, 256), 256, 0, st>>>(c->geo, qb, c->boxes, &c->sc->bmd);
+        k_body_md_tol<<<grid_for(c->N, 128), 128, 0, st>>>(c->geo, c->pos, c->md_tol);
+        k_max_tol<<<1, 1, 0, st>>>(c->md_tol, c->N, c->max_md_tol);
+        k_md_gate<<<1, 1, 0, st>>>(c->sc, c->max_md_tol);
+        PairQuery qm{2, &c->sc->md_radius, 0.0, 1.0, 0.0};
+        launch_pairs(c, qm, c->md_pairs, &c->sc->n_md_pairs, &c->sc->md_gate);
+        k_min_distance<<<c->n_sm * 4, 256, 0, st>>>(c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
+                                                    &c->sc->md, &c->sc->md_gate);
+        k_kappa_update<<<1, 1, 0, st>>>(c->sc);
+    }
+    // computeMaxStep: the FV root box fails the reference's domain predicate
+    // before any bisection, so the earliest TOI is 1 and the step is dt.
+    // integrator init, contact forms, drives
+    k_step_setup<<<grid_for(std::max(c->N, c->D), 128), 128, 0, st>>>(
+        cfg, dt, c->pos, c->quat, c->vel, c->omega, c->lacc, c->aacc, c->x, c->xhat, c->xprev, c->vprev, c->aprev, c->pos0,
+        c->quat0, c->sc, c->dprm, c->dfilt, c->dfinit, c->dhas_prev);
+    // detectContacts at the step-start poses (when a contact form is needed)
+    const bool needs = c->s.enable_adaptive_barrier || (c->s.enable_friction && c->s.friction_coeff > 0.0);
+    if (needs) launch_narrow_full(c, c->wv, c->pos, nullptr);
+    else k_contact_totals<<<1, 1, 0, st>>>(c->sc, 2, nullptr, nullptr);
+    int* skip_detect = c->i_scratch + 1;
+    for (int alm = 0; alm < c->s.alm_max_iters; ++alm) {
+        k_newton<<<1, kSolverThreads, 0, st>>>(c->S);
+        k_alm_detect_gate<<<1, 1, 0, st>>>(c->sc, skip_detect);
+        k_pose_at_x<<<grid_for(c->N, 128), 128, 0, st>>>(c->N, c->x, c->quat, c->pose_p, c->pose_q);
+        k_world_vertices<<<grid_for(c->nv, 256), 256, 0, st>>>(c->geo, c->nv, c->vbody, c->pose_p, c->pose_q, c->wvx);
+        launch_narrow_full(c, c->wvx, c->pose_p, skip_detect);
+        k_alm_post<<<1, kSolverThreads, 0, st>>>(c->S, c->sc, cfg, c->nforce);
+    }
+    k_update_state<<<grid_for(c->N, 128), 128, 0, st>>>(cfg, c->x, c->xprev, c->vprev, c->pos, c->quat, c->vel, c->omega,
+                                                        c->lacc, c->aacc, c->sc, c->da, c->db, c->dprm, c->dfilt);
+    if (c->D > 0) k_drive_kpi<<<1, 1, 0, st>>>(cfg, c->omega, c->sc, c->da, c->db, c->dprm, c->dfilt);
+    NXD_CUDA(cudaGetLastError());
+    return NXD_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+void nxd_default_settings(nxd_settings* s) {
+    std::memset(s, 0, sizeof(*s));
+    s->dhat = 1e-3;
+    s->contact_stiffness = -1.0;
+    s->enable_adaptive_barrier = 1;
+    s->enable_ccd = 1;
+    s->ccd_safety_factor = 0.8;
+    s->enable_friction = 0;
+    s->alm_max_iters = 10;
+    s->friction_coeff = 0.0;
+    s->alm_constraint_tol = 1e-4;
+    s->alm_dual_tol = 1e-3;
+    s->alm_contact_tol = 1e-3;
+    s->alm_hardening_trigger = 2.0;
+    s->alm_hardening_ratio = 2.0;
+    s->newton_max_iters = 20;
+    s->ls_max_iters = 20;
+    s->newton_tol = 1e-6;
+    s->ls_c1 = 1e-4;
+    s->ls_rho = 0.5;
+}
+
+const char* nxd_version(void) { return "nxd-b200 0.1 (sm_100a, FP64)"; }
+
+nxd_status nxd_create(const nxd_scene_desc* d, nxd_ctx** out) {
+    if (!d || !out || d->n_bodies <= 0 || !d->position || !d->orientation || !d->mass || !d->inertia_body ||
+        !d->vertex_offset || !d->face_offset)
+        return NXD_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return NXD_NO_DEVICE;
+    nxd_ctx* c = new (std::nothrow) nxd_ctx();
+    if (!c) return NXD_INVALID_ARGUMENT;
+    cudaGetDevice(&c->dev);
+    cudaDeviceGetAttribute(&c->n_sm, cudaDevAttrMultiProcessorCount, c->dev);
+    c->s = d->settings;
+    const int N = d->n_bodies;
+    c->N = N;
+    c->J = d->n_joints;
+    c->D = d->n_drives;
+    c->h_voff.assign(d->vertex_offset, d->vertex_offset + N + 1);
+    c->h_foff.assign(d->face_offset, d->face_offset + N + 1);
+    c->nv = c->h_voff[N];
+    c->nf = c->h_foff[N];
+    c->h_body_ids.resize(N);
+    for (int i = 0; i < N; ++i) c->h_body_ids[i] = d->body_ids ? d->body_ids[i] : i;
+    auto idx_of = [&](int id) -> int {
+        for (int i = 0; i < N; ++i) if (c->h_body_ids[i] == id) return i;
+        return -1;
+    };
+    // static mesh topology: unique edges in first-seen order
+    // (build_unique_edges, ContactAssembler.cpp:90-120), local AABBs
+    // (MeshShape ctor, MeshShape.cpp:6-11), vertex -> body map
+    std::vector<int> edges, eoff(N + 1, 0), vbody(c->nv), has_mesh(N, 0);
+    std::vector<double> lmin(3 * N, 0.0), lmax(3 * N, 0.0);
+    for (int i = 0; i < N; ++i) {
+        const int v0 = c->h_voff[i], v1 = c->h_voff[i + 1], f0 = c->h_foff[i], f1 = c->h_foff[i + 1];
+        for (int v = v0; v < v1; ++v) vbody[v] = i;
+        eoff[i] = (int)(edges.size() / 2);
+        if (v1 > v0 && f1 > f0) {
+            has_mesh[i] = 1;
+            for (int k = 0; k < 3; ++k) { lmin[3 * i + k] = d->vertices[3 * v0 + k]; lmax[3 * i + k] = d->vertices[3 * v0 + k]; }
+            for (int v = v0; v < v1; ++v)
+                for (int k = 0; k < 3; ++k) {
+                    lmin[3 * i + k] = std::min(lmin[3 * i + k], d->vertices[3 * v + k]);
+                    lmax[3 * i + k] = std::max(lmax[3 * i + k], d->vertices[3 * v + k]);
+                }
+            std::unordered_set<unsigned long long> seen;
+            for (int f = f0; f < f1; ++f) {
+                const int* F = d->faces + 3 * f;
+                const int pr[3][2] = {{F[0], F[1]}, {F[1], F[2]}, {F[2], F[0]}};
+                for (auto& e : pr) {
+                    const int lo = std::min(e[0], e[1]), hi = std::max(e[0], e[1]);
+                    const unsigned long long key = ((unsigned long long)(unsigned)lo << 32) | (unsigned)hi;
+                    if (seen.insert(key).second) { edges.push_back(lo); edges.push_back(hi); }
+                }
+            }
+        }
+        const int nvb = v1 - v0, nfb = f1 - f0, neb = (int)(edges.size() / 2) - eoff[i];
+        c->max_prims = std::max({c->max_prims, nvb, nfb, neb});
+    }
+    eoff[N] = (int)(edges.size() / 2);
+    c->ne = eoff[N];
+    c->h_eoff = eoff;
+    // joints: world indices, angle-limit axis normalised (AngleLimitJoint ctor)
+    std::vector<int> jtype(c->J), ja(c->J), jb(c->J);
+    std::vector<double> jparams((size_t)16 * c->J), jmu(c->J), jlam((size_t)6 * c->J, 0.0);
+    std::vector<std::vector<int>> jinc_l(N), dinc_l(N);
+    for (int j = 0; j < c->J; ++j) {
+        jtype[j] = d->joint_type[j];
+        ja[j] = idx_of(d->joint_body_a[j]);
+        jb[j] = jtype[j] == NXD_JOINT_FIXED ? -1 : idx_of(d->joint_body_b[j]);
+        if (ja[j] < 0 || (jtype[j] != NXD_JOINT_FIXED && jb[j] < 0) || jtype[j] < 0 || jtype[j] > 3) {
+            c->mem.release(); delete c; return NXD_INVALID_ARGUMENT;
+        }
+        for (int k = 0; k < 16; ++k) jparams[16 * j + k] = d->joint_params[16 * j + k];
+        if (jtype[j] == NXD_JOINT_ANGLE_LIMIT) {
+            V3 a = normalized(v3(jparams[16 * j], jparams[16 * j + 1], jparams[16 * j + 2]));
+            jparams[16 * j] = a.x; jparams[16 * j + 1] = a.y; jparams[16 * j + 2] = a.z;
+        }
+        jmu[j] = d->joint_stiffness[j];
+        jinc_l[ja[j]].push_back(2 * j);
+        if (jb[j] >= 0) jinc_l[jb[j]].push_back(2 * j + 1);
+    }
+    std::vector<int> da(c->D), db(c->D);
+    std::vector<Drv> dprm(c->D);
+    std::vector<double> dfilt(c->D);
+    for (int k = 0; k < c->D; ++k) {
+        da[k] = d->drive_body_a[k] >= 0 ? idx_of(d->drive_body_a[k]) : -1;
+        db[k] = idx_of(d->drive_body_b[k]);
+        if (db[k] < 0) { c->mem.release(); delete c; return NXD_INVALID_ARGUMENT; }
+        const double* p = d->drive_params + 8 * k;
+        const V3 ax = normalized(v3(p[0], p[1], p[2]));
+        dprm[k] = Drv{ax.x, ax.y, ax.z, p[3], p[4], p[5] <= 0.0 ? INFINITY : p[5], std::max(0.0, p[6]), std::max(0.0, p[7])};
+        dfilt[k] = p[4];
+        if (da[k] >= 0) dinc_l[da[k]].push_back(2 * k);
+        dinc_l[db[k]].push_back(2 * k + 1);
+    }
+    auto csr = [&](const std::vector<std::vector<int>>& L, std::vector<int>& off, std::vector<int>& val) {
+        off.assign(N + 1, 0);
+        for (int i = 0; i < N; ++i) { off[i + 1] = off[i] + (int)L[i].size(); for (int v : L[i]) val.push_back(v); }
+    };
+    std::vector<int> jinc_off, jinc, dinc_off, dinc;
+    csr(jinc_l, jinc_off, jinc);
+    csr(dinc_l, dinc_off, dinc);
+
+    DevArena& m = c->mem;
+    c->voff = m.upload(c->h_voff.data(), N + 1);
+    c->foff = m.upload(c->h_foff.data(), N + 1);
+    c->eoff = m.upload(eoff.data(), N + 1);
+    c->verts = m.upload(d->vertices, (size_t)3 * c->nv);
+    c->faces = m.upload(d->faces, (size_t)3 * c->nf);
+    c->edges = m.upload(edges.data(), edges.size());
+    c->vbody = m.upload(vbody.data(), vbody.size());
+    c->has_mesh = m.upload(has_mesh.data(), N);
+    c->body_ids = m.upload(c->h_body_ids.data(), N);
+    c->lmin = m.upload(lmin.data(), 3 * N);
+    c->lmax = m.upload(lmax.data(), 3 * N);
+    c->md_tol = m.alloc<double>(N);
+    c->max_md_tol = m.alloc<double>(1);
+    c->mass = m.upload(d->mass, N);
+    c->inertia = m.upload(d->inertia_body, (size_t)9 * N);
+    c->jtype = m.upload(jtype.data(), c->J); c->ja = m.upload(ja.data(), c->J); c->jb = m.upload(jb.data(), c->J);
+    c->jparams = m.upload(jparams.data(), jparams.size()); c->jmu = m.upload(jmu.data(), c->J);
+    c->jlam = m.upload(jlam.data(), jlam.size());
+    c->jinc_off = m.upload(jinc_off.data(), N + 1); c->jinc = m.upload(jinc.data(), jinc.size());
+    c->da = m.upload(da.data(), c->D); c->db = m.upload(db.data(), c->D); c->dprm = m.upload(dprm.data(), c->D);
+    c->dfilt = m.upload(dfilt.data(), c->D); c->dfinit = m.alloc<int>(c->D); c->dhas_prev = m.alloc<int>(c->D);
+    c->dprevA = m.alloc<double>(3 * c->D); c->dprevB = m.alloc<double>(3 * c->D);
+    c->dinc_off = m.upload(dinc_off.data(), N + 1); c->dinc = m.upload(dinc.data(), dinc.size());
+    std::vector<double> zeros(3 * N, 0.0);
+    c->pos = m.upload(d->position, 3 * N);
+    c->quat = m.upload(d->orientation, 4 * N);
+    c->vel = m.upload(d->velocity ? d->velocity : zeros.data(), 3 * N);
+    c->omega = m.upload(d->angular_velocity ? d->angular_velocity : zeros.data(), 3 * N);
+    c->lacc = m.upload(d->linear_acceleration ? d->linear_acceleration : zeros.data(), 3 * N);
+    c->aacc = m.upload(d->angular_acceleration ? d->angular_acceleration : zeros.data(), 3 * N);
+    c->geo = Geo{N, c->voff, c->foff, c->eoff, c->verts, c->faces, c->edges, c->lmin, c->lmax, c->has_mesh, c->md_tol};
+    c->boxes = m.alloc<double>(6 * N);
+    c->wv = m.alloc<double>(3 * (size_t)c->nv); c->wvx = m.alloc<double>(3 * (size_t)c->nv);
+    c->pose_p = m.alloc<double>(3 * N); c->pose_q = m.alloc<double>(4 * N);
+    c->x = m.alloc<double>(6 * N); c->xhat = m.alloc<double>(6 * N); c->xprev = m.alloc<double>(6 * N);
+    c->vprev = m.alloc<double>(6 * N); c->aprev = m.alloc<double>(6 * N);
+    c->pos0 = m.alloc<double>(3 * N); c->quat0 = m.alloc<double>(4 * N);
+    c->pair_cap = std::max(4096, 16 * N);
+    c->pair_cnt = m.alloc<int>(N); c->pair_off = m.alloc<int>(N);
+    c->pairs = m.alloc<int>(2 * (size_t)c->pair_cap); c->md_pairs = m.alloc<int>(2 * (size_t)c->pair_cap);
+    c->topk = m.alloc<int>((size_t)c->pair_cap * 6 * kTopK); c->topn = m.alloc<int>((size_t)c->pair_cap * 6);
+    c->nfv = m.alloc<int>(c->pair_cap); c->nee = m.alloc<int>(c->pair_cap); c->nvv = m.alloc<int>(c->pair_cap);
+    c->nev = m.alloc<int>(c->pair_cap);
+    c->off_fv = m.alloc<int>(c->pair_cap); c->off_ee = m.alloc<int>(c->pair_cap); c->off_vv = m.alloc<int>(c->pair_cap);
+    c->off_ev = m.alloc<int>(c->pair_cap);
+    c->hit_cnt = m.alloc<int>(c->pair_cap); c->hit_off = m.alloc<int>(c->pair_cap);
+    c->item_cap = (long long)c->pair_cap * 2 * kTopK * kTopK;
+    c->flags = m.alloc<unsigned char>((size_t)c->item_cap);
+    c->contacts = m.alloc<ContactRec>(kMaxRawContacts);
+    c->contacts_tmp = m.alloc<ContactRec>(kMaxContacts);
+    c->sort_key = m.alloc<double>(65536); c->sort_idx = m.alloc<int>(65536);
+    c->nforce = m.alloc<double>(kMaxRawContacts);
+    c->sc = m.alloc<Scalars>(1);
+    c->i_scratch = m.alloc<int>(16);
+    Scalars hs{};
+    hs.dhat = std::max(1e-9, c->s.dhat);
+    hs.kappa = c->s.contact_stiffness > 0.0 ? c->s.contact_stiffness : 0.0;
+    hs.bmd = INFINITY;
+    hs.md = INFINITY;
+    cudaMemcpy(c->sc, &hs, sizeof(hs), cudaMemcpyHostToDevice);
+    fill_solver(c);
+    // top-k kernel needs opt-in shared memory above 48 KB
+    cudaFuncSetAttribute(k_topk, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    if (!m.ok || cudaDeviceSynchronize() != cudaSuccess) {
+        m.release();
+        delete c;
+        return NXD_CUDA_ERROR;
+    }
+    *out = c;
+    return NXD_OK;
+}
+
+void nxd_destroy(nxd_ctx* c) {
+    if (!c) return;
+    cudaDeviceSynchronize();
+    c->mem.release();
+    delete c;
+}
+
+nxd_status nxd_set_stream(nxd_ctx* c, void* stream) {
+    if (!c) return NXD_INVALID_ARGUMENT;
+    c->stream = static_cast<cudaStream_t>(stream);
+    return NXD_OK;
+}
+
+nxd_status nxd_step(nxd_ctx* c, double dt) {
+    if (!c || !(dt > 0.0)) return NXD_INVALID_ARGUMENT;
+    return enqueue_step(c, dt);
+}
+
+nxd_status nxd_get_state(nxd_ctx* c, const nxd_state* o) {
+    if (!c || !o) return NXD_INVALID_ARGUMENT;
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    const size_t n3 = 3 * (size_t)c->N * sizeof(double), n4 = 4 * (size_t)c->N * sizeof(double);
+    if (o->position) NXD_CUDA(cudaMemcpy(o->position, c->pos, n3, cudaMemcpyDeviceToHost));
+    if (o->orientation) NXD_CUDA(cudaMemcpy(o->orientation, c->quat, n4, cudaMemcpyDeviceToHost));
+    if (o->velocity) NXD_CUDA(cudaMemcpy(o->velocity, c->vel, n3, cudaMemcpyDeviceToHost));
+    if (o->angular_velocity) NXD_CUDA(cudaMemcpy(o->angular_velocity, c->omega, n3, cudaMemcpyDeviceToHost));
+    if (o->linear_acceleration) NXD_CUDA(cudaMemcpy(o->linear_acceleration, c->lacc, n3, cudaMemcpyDeviceToHost));
+    if (o->angular_acceleration) NXD_CUDA(cudaMemcpy(o->angular_acceleration, c->aacc, n3, cudaMemcpyDeviceToHost));
+    return NXD_OK;
+}
+
+nxd_status nxd_set_state(nxd_ctx* c, const nxd_state* o) {
+    if (!c || !o) return NXD_INVALID_ARGUMENT;
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    const size_t n3 = 3 * (size_t)c->N * sizeof(double), n4 = 4 * (size_t)c->N * sizeof(double);
+    if (o->position) NXD_CUDA(cudaMemcpy(c->pos, o->position, n3, cudaMemcpyHostToDevice));
+    if (o->orientation) NXD_CUDA(cudaMemcpy(c->quat, o->orientation, n4, cudaMemcpyHostToDevice));
+    if (o->velocity) NXD_CUDA(cudaMemcpy(c->vel, o->velocity, n3, cudaMemcpyHostToDevice));
+    if (o->angular_velocity) NXD_CUDA(cudaMemcpy(c->omega, o->angular_velocity, n3, cudaMemcpyHostToDevice));
+    if (o->linear_acceleration) NXD_CUDA(cudaMemcpy(c->lacc, o->linear_acceleration, n3, cudaMemcpyHostToDevice));
+    if (o->angular_acceleration) NXD_CUDA(cudaMemcpy(c->aacc, o->angular_acceleration, n3, cudaMemcpyHostToDevice));
+    return NXD_OK;
+}
+
+nxd_status nxd_get_diagnostics(nxd_ctx* c, nxd_diagnostics* o) {
+    if (!c || !o) return NXD_INVALID_ARGUMENT;
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    Scalars h;
+    NXD_CUDA(cudaMemcpy(&h, c->sc, sizeof(h), cudaMemcpyDeviceToHost));
+    std::memset(o, 0, sizeof(*o));
+    o->kappa = h.kappa; o->dhat = h.dhat; o->actual_dt = h.dt;
+    o->last_dual_residual = h.alm_dual; o->last_contact_residual = h.alm_cres;
+    o->last_max_constraint_violation = h.alm_mcv;
+    o->last_angular_velocity_error = h.last_vw; o->last_torque_saturation_ratio = h.last_tsat;
+    o->scene_min_distance = h.md;
+    o->alm_iterations = h.alm_iters; o->newton_iterations = h.newton_iters; o->newton_converged = h.converged;
+    o->n_body_pairs = h.n_pairs; o->n_contacts = h.n_contacts; o->n_contacts_raw = h.n_contacts_raw;
+    o->status = h.status | ((h.n_pairs > c->pair_cap || h.n_md_pairs > c->pair_cap) ? NXD_CAPACITY : 0);
+    o->line_search_failures = h.ls_fail;
+    return NXD_OK;
+}
+
+nxd_status nxd_get_joint_state(nxd_ctx* c, double* lambda6, double* stiffness) {
+    if (!c) return NXD_INVALID_ARGUMENT;
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    if (lambda6 && c->J) NXD_CUDA(cudaMemcpy(lambda6, c->jlam, 6 * (size_t)c->J * sizeof(double), cudaMemcpyDeviceToHost));
+    if (stiffness && c->J) NXD_CUDA(cudaMemcpy(stiffness, c->jmu, (size_t)c->J * sizeof(double), cudaMemcpyDeviceToHost));
+    return NXD_OK;
+}
+
+nxd_status nxd_body_pairs(nxd_ctx* c, double r, int32_t* pairs, int64_t cap, int64_t* count) {
+    if (!c || !count) return NXD_INVALID_ARGUMENT;
+    launch_assembly(c);
+    PairQuery q{0, nullptr, r, 1.0, 0.0};
+    launch_pairs(c, q, c->md_pairs, &c->sc->n_md_pairs, nullptr);
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    int n = 0;
+    NXD_CUDA(cudaMemcpy(&n, &c->sc->n_md_pairs, sizeof(int), cudaMemcpyDeviceToHost));
+    *count = n;
+    if (n > c->pair_cap) return NXD_CAPACITY;
+    if (pairs && cap > 0)
+        NXD_CUDA(cudaMemcpy(pairs, c->md_pairs, 2 * sizeof(int) * (size_t)std::min<int64_t>(n, cap), cudaMemcpyDeviceToHost));
+    return n > cap && pairs ? NXD_CAPACITY : NXD_OK;
+}
+
+nxd_status nxd_build_candidates(nxd_ctx* c, double act, nxd_candidates* o) {
+    if (!c || !o) return NXD_INVALID_ARGUMENT;
+    launch_assembly(c);
+    launch_candidates(c, nullptr, act);
+    k_item_counts<<<grid_for(c->pair_cap, 256), 256, 0, c->stream>>>(&c->sc->n_pairs, c->pair_cap, c->topn, c->nfv, c->nee,
+                                                                       c->nvv, c->nev);
+    int* tot = c->i_scratch + 4;
+    k_scan<<<1, 1024, 0, c->stream>>>(c->nev, c->off_ev, c->pair_cap, tot, nullptr, nullptr, &c->sc->n_pairs);
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    Scalars h;
+    int nev_total = 0;
+    NXD_CUDA(cudaMemcpy(&h, c->sc, sizeof(h), cudaMemcpyDeviceToHost));
+    NXD_CUDA(cudaMemcpy(&nev_total, tot, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h.n_pairs > c->pair_cap) return NXD_CAPACITY;
+    o->vv_count = h.vv_items; o->ev_count = nev_total; o->ee_count = h.ee_items; o->fv_count = h.fv_items;
+    nxd_status st = NXD_OK;
+    auto need = [&](int32_t* buf, int64_t cap, int64_t cnt) { if (buf && cnt > cap) st = NXD_CAPACITY; };
+    need(o->vv, o->vv_cap, o->vv_count); need(o->ev, o->ev_cap, o->ev_count);
+    need(o->ee, o->ee_cap, o->ee_count); need(o->fv, o->fv_cap, o->fv_count);
+    if (!o->vv && !o->ev && !o->ee && !o->fv) return st;
+    DevArena tmp;
+    CandOut co{};
+    co.vv = tmp.alloc<int>(4 * (size_t)std::max<int64_t>(1, o->vv_count)); co.vv_cap = o->vv_count;
+    co.ev = tmp.alloc<int>(5 * (size_t)std::max<int64_t>(1, o->ev_count)); co.ev_cap = o->ev_count;
+    co.ee = tmp.alloc<int>(6 * (size_t)std::max<int64_t>(1, o->ee_count)); co.ee_cap = o->ee_count;
+    co.fv = tmp.alloc<int>(4 * (size_t)std::max<int64_t>(1, o->fv_count)); co.fv_cap = o->fv_count;
+    if (!tmp.ok) { tmp.release(); return NXD_CUDA_ERROR; }
+    k_materialize<<<c->n_sm * 4, 256, 0, c->stream>>>(c->geo, c->body_ids, c->pairs, &c->sc->n_pairs, c->pair_cap, c->topk,
+                                                     c->topn, c->off_vv, c->off_ev, c->off_ee, c->off_fv, co);
+    cudaStreamSynchronize(c->stream);
+    auto back = [&](int32_t* buf, int64_t cap, const int* dev, int64_t cnt, int w) {
+        if (buf && cnt > 0) cudaMemcpy(buf, dev, sizeof(int) * w * (size_t)std::min(cap, cnt), cudaMemcpyDeviceToHost);
+    };
+    back(o->vv, o->vv_cap, co.vv, o->vv_count, 4);
+    back(o->ev, o->ev_cap, co.ev, o->ev_count, 5);
+    back(o->ee, o->ee_cap, co.ee, o->ee_count, 6);
+    back(o->fv, o->fv_cap, co.fv, o->fv_count, 4);
+    tmp.release();
+    return st;
+}
+
+nxd_status nxd_detect_contacts(nxd_ctx* c, const double* x, nxd_contact* out, int32_t cap, int32_t* count) {
+    if (!c) return NXD_INVALID_ARGUMENT;
+    launch_assembly(c);
+    launch_candidates(c, &c->sc->dhat, 0.0);
+    if (x) {
+        NXD_CUDA(cudaMemcpyAsync(c->S.xt, x, 6 * (size_t)c->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        k_pose_at_x<<<grid_for(c->N, 128), 128, 0, c->stream>>>(c->N, c->S.xt, c->quat, c->pose_p, c->pose_q);
+        k_world_vertices<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(c->geo, c->nv, c->vbody, c->pose_p, c->pose_q, c->wvx);
+        launch_narrow_full(c, c->wvx, c->pose_p, nullptr);
+    } else {
+        launch_narrow_full(c, c->wv, c->pos, nullptr);
+    }
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    Scalars h;
+    NXD_CUDA(cudaMemcpy(&h, c->sc, sizeof(h), cudaMemcpyDeviceToHost));
+    if (count) *count = h.n_contacts;
+    if (out && cap > 0)
+        NXD_CUDA(cudaMemcpy(out, c->contacts, sizeof(nxd_contact) * (size_t)std::min(cap, h.n_contacts), cudaMemcpyDeviceToHost));
+    return h.n_contacts > cap && out ? NXD_CAPACITY : NXD_OK;
+}
+
+nxd_status nxd_scene_min_distance(nxd_ctx* c, double* out) {
+    if (!c || !out) return NXD_INVALID_ARGUMENT;
+    launch_assembly(c);
+    cudaStream_t st = c->stream;
+    k_body_md_tol<<<grid_for(c->N, 128), 128, 0, st>>>(c->geo, c->pos, c->md_tol);
+    k_max_tol<<<1, 1, 0, st>>>(c->md_tol, c->N, c->max_md_tol);
+    // force the gate open: bmd = 0
+    k_init_scalar_d<<<1, 1, 0, st>>>(&c->sc->bmd, 0.0);
+    k_md_gate<<<1, 1, 0, st>>>(c->sc, c->max_md_tol);
+    PairQuery qm{2, &c->sc->md_radius, 0.0, 1.0, 0.0};
+    launch_pairs(c, qm, c->md_pairs, &c->sc->n_md_pairs, &c->sc->md_gate);
+    k_min_distance<<<c->n_sm * 4, 256, 0, st>>>(c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
+                                                &c->sc->md, &c->sc->md_gate);
+    NXD_CUDA(cudaStreamSynchronize(st));
+    Scalars h;
+    NXD_CUDA(cudaMemcpy(&h, c->sc, sizeof(h), cudaMemcpyDeviceToHost));
+    *out = h.md;
+    return h.n_md_pairs > c->pair_cap ? NXD_CAPACITY : NXD_OK;
+}
+
+nxd_status nxd_max_step(nxd_ctx* c, double dt, double* out_dt) {
+    // IPCSolver::computeMaxStep (IPCSolver.cpp:355-392).  Every early exit
+    // returns dt; otherwise CCDSystem::computeEarliestTOI (CCD.h:22-82) runs the
+    // face-vertex root finder, whose first box ([0,1],[0,1],[0,1]) fails the
+    // domain predicate w = 1-u-v in [0,1] (TimeOfImpact.cpp:130-139) before any
+    // bisection, so no impact is ever reported and the bound is dt.
+    if (!c || !out_dt) return NXD_INVALID_ARGUMENT;
+    *out_dt = dt;
+    return NXD_OK;
+}
+
+}  // extern "C"

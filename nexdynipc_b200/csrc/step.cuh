@@ -1,0 +1,301 @@
+// step.cuh — per-step bookkeeping kernels of IPCSolver::step
+// (src/Dynamics/IPCSolver.cpp:808-1231) around the geometry and Newton
+// kernels: adaptive-barrier initialisation and stiffness update, integrator
+// set-up, contact-form installation, the ALM convergence test, the 2000
+// contact cap and the state write-back.
+#pragma once
+
+#include "solver.cuh"
+
+namespace nx {
+
+// Device-resident scalars of one context.
+struct Scalars {
+    double dhat;            // AdaptiveBarrier::currentDhat
+    double kappa;           // AdaptiveBarrier::currentStiffness
+    double dt;              // step dt (computeMaxStep result)
+    double bdhat, bkappa;   // DistanceBarrierForm parameters
+    double bmd;             // estimateBroadPhaseMinDistance(2 dhat)
+    double md;              // computeSceneMinDistance (pruned)
+    double md_radius;       // half the widest pruning band
+    double alm_mcv, alm_dual, alm_cres;
+    double last_vw, last_tsat;
+    int barrier_initialized;
+    int md_gate;
+    int alm_done;
+    int barrier_form, barrier_in_forms, friction_form;
+    int n_pairs, n_md_pairs;
+    int fv_items, ee_items, vv_items;
+    int fv_hits, ee_hits, vv_hits;
+    int zero_hits;          // 1 when FV+EE produced nothing (VV fallback runs)
+    int n_contacts, n_contacts_raw;
+    int nnf;
+    int status;
+    int newton_iters, converged, ls_fail, alm_iters;
+    int n_pairs_overflow;
+};
+
+struct StepCfg {
+    int N, D;
+    int enable_adaptive, enable_friction;
+    double friction_coeff;
+    double alm_constraint_tol, alm_dual_tol, alm_contact_tol;
+};
+
+// IPCSolver::initializeAdaptiveBarrier (IPCSolver.cpp:327-353) +
+// AdaptiveBarrier::initialize (AdaptiveBarrier.h:27-31); runs once per context.
+__global__ void k_barrier_init(StepCfg cfg, const double* mass, const double* pos, Scalars* sc, double* red) {
+    __shared__ double bb[6];
+    if (!cfg.enable_adaptive || sc->barrier_initialized || cfg.N == 0) return;
+    for (int i = threadIdx.x; i < cfg.N; i += blockDim.x) red[i] = mass[i];
+    const double tm = block_tree_sum(red, cfg.N);
+    if (threadIdx.x == 0) {
+        V3 mn = v3(INFINITY, INFINITY, INFINITY), mx = v3(-INFINITY, -INFINITY, -INFINITY);
+        for (int i = 0; i < cfg.N; ++i) { mn = cwmin(mn, ld3(pos + 3 * i)); mx = cwmax(mx, ld3(pos + 3 * i)); }
+        st3(bb, mn); st3(bb + 3, mx);
+        const double am = tm / (double)cfg.N;
+        double diag = norm(mx - mn);
+        if (diag < 1e-6) diag = 1.0;
+        sc->kappa = 1e11 * am / (diag * diag);
+        sc->dhat = 1e-3;
+        sc->barrier_initialized = 1;
+    }
+}
+
+__global__ void k_md_gate(Scalars* sc, const double* max_md_tol) {
+    sc->md_gate = (sc->bmd < sc->dhat * 2.0) ? 1 : 0;
+    sc->md = INFINITY;
+    sc->md_radius = 0.5 * (kPruneBand + *max_md_tol) + 1e-12;
+}
+
+// AdaptiveBarrier::updateStiffness (AdaptiveBarrier.h:33-37)
+__global__ void k_kappa_update(Scalars* sc) {
+    if (!sc->md_gate) return;
+    const double md = sc->md;
+    if (md < INFINITY && md < 1e-9 && sc->kappa < 1e20) sc->kappa = dmin(sc->kappa * 2.0, 1e20);
+}
+
+// Integrator init / x_tilde (IPCSolver.cpp:839-861, ImplicitEulerIntegrator.cpp:5-11),
+// contact-form flags (IPCSolver.cpp:873-921) and drive set-up (IPCSolver.cpp:923-958).
+__global__ void k_step_setup(StepCfg cfg, double dt, const double* pos, const double* quat, const double* vel,
+                             const double* omega, const double* lacc, const double* aacc, double* x, double* xhat,
+                             double* xprev, double* vprev, double* aprev, double* pos0, double* quat0, Scalars* sc,
+                             const Drv* dprm, double* dfilt, int* dfinit, int* dhas_prev) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < cfg.N) {
+        for (int k = 0; k < 3; ++k) {
+            const double p = pos[3 * i + k];
+            xprev[6 * i + k] = p; xprev[6 * i + 3 + k] = 0.0;
+            vprev[6 * i + k] = vel[3 * i + k]; vprev[6 * i + 3 + k] = omega[3 * i + k];
+            aprev[6 * i + k] = lacc[3 * i + k]; aprev[6 * i + 3 + k] = aacc[3 * i + k];
+            pos0[3 * i + k] = p;
+        }
+        for (int k = 0; k < 4; ++k) quat0[4 * i + k] = quat[4 * i + k];
+        for (int k = 0; k < 6; ++k) {
+            const double xh = xprev[6 * i + k] + dt * vprev[6 * i + k];
+            xhat[6 * i + k] = xh;
+            x[6 * i + k] = xh;
+        }
+    }
+    if (i < cfg.D) {
+        const Drv& p = dprm[i];
+        if (p.tau <= 0.0) { dfilt[i] = p.vt; dfinit[i] = 0; }
+        else if (!dfinit[i]) { dfilt[i] = p.vt; dfinit[i] = 1; }
+        else if (dt > 0.0) { const double al = dt / (p.tau + dt); dfilt[i] += al * (p.vt - dfilt[i]); }
+        dhas_prev[i] = 0;
+    }
+    if (i == 0) {
+        sc->dt = dt;
+        const bool needs = cfg.enable_adaptive || (cfg.enable_friction && cfg.friction_coeff > 0.0);
+        sc->barrier_form = needs ? 1 : 0;
+        sc->barrier_in_forms = (cfg.enable_adaptive && needs) ? 1 : 0;
+        sc->friction_form = (cfg.enable_friction && cfg.friction_coeff > 0.0) ? 1 : 0;
+        sc->bdhat = dmax(1e-9, sc->dhat);
+        sc->bkappa = dmax(0.0, sc->kappa);
+        sc->nnf = 0;
+        sc->alm_done = 0;
+        sc->newton_iters = 0;
+        sc->ls_fail = 0;
+        sc->alm_iters = 0;
+        sc->converged = 0;
+        sc->alm_mcv = 0.0; sc->alm_dual = 0.0; sc->alm_cres = 0.0;
+    }
+}
+
+// Contact totals after FV + EE (+VV) passes; gates the VV fallback.
+// stage 2 clears the counts (no detection this step).
+__global__ void k_contact_totals(Scalars* sc, int stage, const int* skip_if, int* skip_vv) {
+    if (skip_if && *skip_if != 0) { if (skip_vv) *skip_vv = 1; return; }
+    if (stage == 2) { sc->n_contacts = 0; sc->n_contacts_raw = 0; return; }
+    if (stage == 0) {
+        sc->zero_hits = (sc->fv_hits + sc->ee_hits) == 0 ? 1 : 0;
+        if (skip_vv) *skip_vv = sc->zero_hits ? 0 : 1;
+        if (!sc->zero_hits) sc->vv_hits = 0;
+    } else {
+        const int total = sc->fv_hits + sc->ee_hits + (sc->zero_hits ? sc->vv_hits : 0);
+        const int raw = total < kMaxRawContacts ? total : kMaxRawContacts;
+        sc->n_contacts_raw = raw;
+        sc->n_contacts = raw > kMaxContacts ? kMaxContacts : raw;
+    }
+}
+
+// std::sort by distance + truncation to 2000 (IPCSolver.cpp:571-577): a
+// bitonic sort on (distance, original position); equal distances keep their
+// detection order.  One CTA; runs only when more than 2000 contacts exist.
+__global__ void k_sort_contacts(Scalars* sc, ContactRec* c, ContactRec* tmp, double* key, int* idx, const int* skip_if) {
+    if (skip_if && *skip_if != 0) return;
+    const int raw = sc->n_contacts_raw;
+    if (raw <= kMaxContacts) return;
+    const int P = pow2_ceil(raw);
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        key[i] = i < raw ? c[i].distance : INFINITY;
+        idx[i] = i;
+    }
+    __syncthreads();
+    for (int k = 2; k <= P; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const bool up = (i & k) == 0;
+                    const double ki = key[i], kl = key[l];
+                    const int ii = idx[i], il = idx[l];
+                    const bool gt = (ki > kl) || (ki == kl && ii > il);
+                    if (gt == up) { key[i] = kl; key[l] = ki; idx[i] = il; idx[l] = ii; }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = threadIdx.x; i < kMaxContacts; i += blockDim.x) tmp[i] = c[idx[i]];
+    __syncthreads();
+    for (int i = threadIdx.x; i < kMaxContacts; i += blockDim.x) c[i] = tmp[i];
+}
+
+// After the Newton solve and the detection at x_new (IPCSolver.cpp:1112-1165):
+// normal forces, contact residual, ALM convergence.
+__global__ void __launch_bounds__(kSolverThreads) k_alm_post(Solver S, Scalars* sc, StepCfg cfg, double* nforce_out) {
+    __shared__ double sh_red[32];
+    if (sc->alm_done) return;
+    const int C = sc->n_contacts;
+    const bool bform = sc->barrier_form != 0, fform = sc->friction_form != 0;
+    if (bform || fform) {
+        eval_poses(S, S.x);
+        __syncthreads();
+        for (int c = threadIdx.x; c < C; c += blockDim.x) barrier_eval(S, c, S.x);
+        __syncthreads();
+        if (cfg.enable_friction && fform) {
+            // DistanceBarrierForm::computeNormalForces (DistanceBarrierForm.cpp:70-86)
+            for (int c = threadIdx.x; c < C; c += blockDim.x) {
+                double nf = 0.0;
+                if (bform) {
+                    const double d = S.bD[c];
+                    if (d < sc->bdhat && d > 0.0) nf = fabs(barrier_gradient(d, sc->bdhat, sc->bkappa));
+                }
+                nforce_out[c] = nf;
+            }
+            if (threadIdx.x == 0) sc->nnf = C;
+        }
+        __syncthreads();
+        if (cfg.enable_friction && fform)
+            for (int c = threadIdx.x; c < C; c += blockDim.x) friction_eval(S, c, S.x, true);
+        // contact incidence for the gather
+        for (int i = threadIdx.x; i <= S.N; i += blockDim.x) S.cinc_cnt[i] = 0;
+        __syncthreads();
+        for (int e = threadIdx.x; e < 2 * C; e += blockDim.x) {
+            const ContactRec& cr = S.contacts[e >> 1];
+            atomicAdd(&S.cinc_cnt[(e & 1) ? cr.body_b : cr.body_a], 1);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int acc = 0;
+            for (int i = 0; i < S.N; ++i) { S.cinc_off[i] = acc; acc += S.cinc_cnt[i]; }
+            S.cinc_off[S.N] = acc;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i <= S.N; i += blockDim.x) S.cinc_cnt[i] = S.cinc_off[i];
+        __syncthreads();
+        warp_stable_place(2 * C, [&](int e) { const ContactRec& cr = S.contacts[e >> 1]; return (e & 1) ? cr.body_b : cr.body_a; },
+                          S.cinc_cnt, S.cinc);
+        __syncthreads();
+        double m = 0.0;
+        const double dh = sc->bdhat;
+        const int nnf = sc->nnf;
+        for (int i = threadIdx.x; i < S.N; i += blockDim.x) {
+            double cb[6] = {0, 0, 0, 0, 0, 0}, cf[6] = {0, 0, 0, 0, 0, 0};
+            for (int q = S.cinc_off[i]; q < S.cinc_off[i + 1]; ++q) {
+                const int c = S.cinc[q] >> 1, side = S.cinc[q] & 1;
+                if (bform && S.bD[c] < dh) {
+                    const double gpv = S.bGP[c];
+                    const V3 n = ld3(S.contacts[c].normal);
+                    const V3 contrib = side == 0 ? (-gpv) * n : gpv * n;
+                    cb[0] += contrib.x; cb[1] += contrib.y; cb[2] += contrib.z;
+                }
+                if (cfg.enable_friction && fform && c < nnf && S.nforce[c] > 0) {
+                    const double* Jx = (side == 0 ? S.fJA : S.fJB) + 18 * c;
+                    const V3 fg = ld3(S.fFG + 3 * c);
+                    for (int k = 0; k < 6; ++k) cf[k] += Jx[k] * fg.x + Jx[6 + k] * fg.y + Jx[12 + k] * fg.z;
+                }
+            }
+            for (int k = 0; k < 6; ++k) {
+                double v = 0.0;
+                if (bform) v += cb[k];
+                if (cfg.enable_friction && fform) v += cf[k];
+                m = dmax(m, fabs(v));
+            }
+        }
+        m = block_max(m, sh_red);
+        if (threadIdx.x == 0) sc->alm_cres = isfinite(m) ? m : 1e12;
+    } else if (threadIdx.x == 0) {
+        sc->alm_cres = 0.0;
+    }
+    if (threadIdx.x == 0) {
+        sc->alm_mcv = *S.alm_mcv;
+        sc->alm_dual = *S.alm_dual;
+        sc->alm_iters += 1;
+        if (*S.converged && sc->alm_mcv <= cfg.alm_constraint_tol && sc->alm_dual <= cfg.alm_dual_tol &&
+            sc->alm_cres <= cfg.alm_contact_tol)
+            sc->alm_done = 1;
+    }
+}
+
+// ImplicitEuler::update_quantities + write-back (IPCSolver.cpp:1168-1195)
+// and the velocity-drive KPIs (IPCSolver.cpp:1197-1215).
+__global__ void k_update_state(StepCfg cfg, const double* x, const double* xprev, const double* vprev, double* pos,
+                               double* quat, double* vel, double* omega, double* lacc, double* aacc, Scalars* sc,
+                               const int* da, const int* db, const Drv* dprm, const double* dfilt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double dt = sc->dt;
+    if (i < cfg.N) {
+        double vn[6], an[6];
+        for (int k = 0; k < 6; ++k) vn[k] = (x[6 * i + k] - xprev[6 * i + k]) / dt;
+        for (int k = 0; k < 6; ++k) an[k] = (vn[k] - vprev[6 * i + k]) / dt;
+        for (int k = 0; k < 3; ++k) {
+            lacc[3 * i + k] = an[k]; aacc[3 * i + k] = an[3 + k];
+            vel[3 * i + k] = vn[k]; omega[3 * i + k] = vn[3 + k];
+            pos[3 * i + k] = x[6 * i + k];
+        }
+        stq(quat + 4 * i, rot_gt(ldq(quat + 4 * i), ld3(x + 6 * i + 3)));
+    }
+}
+
+__global__ void k_drive_kpi(StepCfg cfg, const double* omega, Scalars* sc, const int* da, const int* db, const Drv* dprm,
+                            const double* dfilt) {
+    double max_vw = 0.0;
+    int sat = 0;
+    for (int d = 0; d < cfg.D; ++d) {
+        const Drv& p = dprm[d];
+        const V3 oA = da[d] >= 0 ? ld3(omega + 3 * da[d]) : v3(0, 0, 0);
+        const V3 oB = ld3(omega + 3 * db[d]);
+        const double ve = drive_target(p, dfilt[d]) - dot(oB - oA, v3(p.ax, p.ay, p.az));
+        max_vw = dmax(max_vw, fabs(ve));
+        if (isfinite(p.maxT)) {
+            const double tq = drive_sat(p, drive_dead(p, ve));
+            if (fabs(tq) >= 0.98 * p.maxT) ++sat;
+        }
+    }
+    sc->last_vw = max_vw;
+    sc->last_tsat = cfg.D > 0 ? (double)sat / cfg.D : 0.0;
+}
+
+}  // namespace nx

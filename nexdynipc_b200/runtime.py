@@ -1,0 +1,201 @@
+"""Python binding of libnxd_b200.so (the C ABI in include/nxd.h).
+
+`Context` owns one device-resident scene and drives the B200 contact step.
+`IPCSolver` / `World` mirror the reference's class names and setters
+(nexdynipc/NexDynIPC/Dynamics/IPCSolver.h:21-91) for callers that think in
+those terms.  There is no CPU path here: loading fails loudly when the CUDA
+library is absent, and every call goes through the shared library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnxd_b200.so")
+_lib = None
+
+
+class NxdError(RuntimeError):
+    def __init__(self, fn: str, status: int):
+        super().__init__(f"{fn} failed: {abi.STATUS_NAMES.get(status, status)}")
+        self.status = status
+
+
+def lib():
+    """Load libnxd_b200.so (build it with nexdynipc_b200/build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python nexdynipc_b200/build.py` (no CPU fallback exists)")
+    L = C.CDLL(LIB_PATH)
+    vp, dp, ip, i64p = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_int64)
+    L.nxd_version.restype = C.c_char_p
+    L.nxd_default_settings.argtypes = [C.POINTER(abi.NxdSettings)]
+    L.nxd_create.argtypes = [C.POINTER(abi.NxdSceneDesc), C.POINTER(vp)]
+    L.nxd_destroy.argtypes = [vp]
+    L.nxd_set_stream.argtypes = [vp, vp]
+    L.nxd_step.argtypes = [vp, C.c_double]
+    L.nxd_get_state.argtypes = [vp, C.POINTER(abi.NxdState)]
+    L.nxd_set_state.argtypes = [vp, C.POINTER(abi.NxdState)]
+    L.nxd_get_diagnostics.argtypes = [vp, C.POINTER(abi.NxdDiagnostics)]
+    L.nxd_get_joint_state.argtypes = [vp, dp, dp]
+    L.nxd_body_pairs.argtypes = [vp, C.c_double, ip, C.c_int64, i64p]
+    L.nxd_build_candidates.argtypes = [vp, C.c_double, C.POINTER(abi.NxdCandidates)]
+    L.nxd_detect_contacts.argtypes = [vp, dp, C.c_void_p, C.c_int32, ip]
+    L.nxd_scene_min_distance.argtypes = [vp, dp]
+    L.nxd_max_step.argtypes = [vp, C.c_double, dp]
+    for name in ("nxd_create", "nxd_set_stream", "nxd_step", "nxd_get_state", "nxd_set_state", "nxd_get_diagnostics",
+                 "nxd_get_joint_state", "nxd_body_pairs", "nxd_build_candidates", "nxd_detect_contacts",
+                 "nxd_scene_min_distance", "nxd_max_step"):
+        getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def _check(fn: str, st: int):
+    if st != 0:
+        raise NxdError(fn, st)
+
+
+class Context:
+    """One scene resident on the GPU (World + IPCSolver of the reference)."""
+
+    def __init__(self, scene):
+        self.scene = scene
+        self._desc = scene.desc()
+        h = C.c_void_p()
+        _check("nxd_create", lib().nxd_create(C.byref(self._desc), C.byref(h)))
+        self.h = h
+        self.n = scene.n_bodies
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().nxd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, dt=None, n: int = 1):
+        dt = float(self.scene.dt if dt is None else dt)
+        for _ in range(n):
+            _check("nxd_step", lib().nxd_step(self.h, dt))
+
+    def state(self) -> dict:
+        sb = abi.StateBuffers(self.n)
+        v = sb.view()
+        _check("nxd_get_state", lib().nxd_get_state(self.h, C.byref(v)))
+        return sb.as_dict()
+
+    def set_state(self, st: dict):
+        sb = abi.StateBuffers(self.n).load(st)
+        v = sb.view()
+        _check("nxd_set_state", lib().nxd_set_state(self.h, C.byref(v)))
+
+    def diagnostics(self) -> dict:
+        d = abi.NxdDiagnostics()
+        _check("nxd_get_diagnostics", lib().nxd_get_diagnostics(self.h, C.byref(d)))
+        return d.as_dict()
+
+    def joint_state(self):
+        nj = len(self.scene.joint_type)
+        lam = np.zeros((max(nj, 1), 6))
+        mu = np.zeros(max(nj, 1))
+        _check("nxd_get_joint_state", lib().nxd_get_joint_state(self.h, abi.dptr(lam), abi.dptr(mu)))
+        return lam[:nj], mu[:nj]
+
+    def body_pairs(self, r: float) -> np.ndarray:
+        cnt = C.c_int64(0)
+        _check("nxd_body_pairs", lib().nxd_body_pairs(self.h, r, None, 0, C.byref(cnt)))
+        out = np.zeros((max(cnt.value, 1), 2), dtype=np.int32)
+        _check("nxd_body_pairs", lib().nxd_body_pairs(self.h, r, abi.iptr(out), cnt.value, C.byref(cnt)))
+        return out[:cnt.value]
+
+    def candidates(self, act: float) -> dict:
+        c = abi.NxdCandidates()
+        _check("nxd_build_candidates", lib().nxd_build_candidates(self.h, act, C.byref(c)))
+        counts = {"vv": c.vv_count, "ev": c.ev_count, "ee": c.ee_count, "fv": c.fv_count}
+        widths = {"vv": 4, "ev": 5, "ee": 6, "fv": 4}
+        bufs = {k: np.zeros((max(counts[k], 1), widths[k]), np.int32) for k in counts}
+        for k, b in bufs.items():
+            setattr(c, k, abi.iptr(b))
+            setattr(c, k + "_cap", counts[k])
+        _check("nxd_build_candidates", lib().nxd_build_candidates(self.h, act, C.byref(c)))
+        return {k: bufs[k][:counts[k]] for k in bufs}
+
+    def detect_contacts(self, x=None) -> np.ndarray:
+        cap = 40000
+        out = np.zeros(cap, dtype=abi.CONTACT_DTYPE)
+        cnt = C.c_int32(0)
+        xp = abi.dptr(np.ascontiguousarray(x, dtype=np.float64)) if x is not None else None
+        _check("nxd_detect_contacts", lib().nxd_detect_contacts(self.h, xp, out.ctypes.data_as(C.c_void_p), cap,
+                                                                C.byref(cnt)))
+        return out[:cnt.value].copy()
+
+    def scene_min_distance(self) -> float:
+        v = C.c_double(0)
+        _check("nxd_scene_min_distance", lib().nxd_scene_min_distance(self.h, C.byref(v)))
+        return v.value
+
+    def max_step(self, dt: float) -> float:
+        v = C.c_double(0)
+        _check("nxd_max_step", lib().nxd_max_step(self.h, dt, C.byref(v)))
+        return v.value
+
+
+class World:
+    """World of the reference (Dynamics/World.h:11-17): a generated scene."""
+
+    def __init__(self, scene):
+        self.scene = scene
+
+
+class IPCSolver:
+    """IPCSolver facade (Dynamics/IPCSolver.h:21-91): settings are applied to
+    the scene's nxd_settings before the device context is created on the
+    first step(world, dt)."""
+
+    def __init__(self):
+        self._overrides = {}
+        self.ctx = None
+
+    def enableCCD(self, on: bool): self._overrides["enable_ccd"] = int(on)
+    def setCCDSafetyFactor(self, f: float): self._overrides["ccd_safety_factor"] = float(f)
+    def enableAdaptiveBarrier(self, on: bool): self._overrides["enable_adaptive_barrier"] = int(on)
+    def enableFriction(self, on: bool): self._overrides["enable_friction"] = int(on)
+    def setFrictionCoefficient(self, mu: float): self._overrides["friction_coeff"] = float(mu)
+    def setContactDistanceThreshold(self, dhat: float): self._overrides["dhat"] = max(1e-9, float(dhat))
+    def setContactStiffness(self, k: float):
+        if k > 0.0:
+            self._overrides["contact_stiffness"] = float(k)
+    def setALMMaxIters(self, n: int): self._overrides["alm_max_iters"] = max(1, int(n))
+    def setALMConstraintTolerance(self, t: float): self._overrides["alm_constraint_tol"] = max(1e-12, float(t))
+    def setALMDualTolerance(self, t: float): self._overrides["alm_dual_tol"] = max(1e-12, float(t))
+    def setALMContactTolerance(self, t: float): self._overrides["alm_contact_tol"] = max(1e-12, float(t))
+    def setALMHardeningTrigger(self, t: float): self._overrides["alm_hardening_trigger"] = max(1.0, float(t))
+    def setALMHardeningRatio(self, r: float): self._overrides["alm_hardening_ratio"] = max(1.0, float(r))
+
+    def step(self, world: World, dt: float):
+        if self.ctx is None:
+            for k, v in self._overrides.items():
+                setattr(world.scene.settings, k, v)
+            self.ctx = Context(world.scene)
+        self.ctx.step(dt)
+
+    def diagnostics(self) -> dict:
+        return self.ctx.diagnostics()
+
+    def lastDualResidual(self): return self.diagnostics()["last_dual_residual"]
+    def lastContactResidual(self): return self.diagnostics()["last_contact_residual"]
+    def lastMaxConstraintViolation(self): return self.diagnostics()["last_max_constraint_violation"]
+    def lastAngularVelocityError(self): return self.diagnostics()["last_angular_velocity_error"]
+    def lastTorqueSaturationRatio(self): return self.diagnostics()["last_torque_saturation_ratio"]

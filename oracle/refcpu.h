@@ -1,0 +1,89 @@
+/*
+ * refcpu.h — CPU oracle for the NexDynIPC contact step (test infrastructure).
+ *
+ * This library is the parity checker, not the product: only tests/, the
+ * smoke check in __graft_entry__.py and bench.py's CPU-baseline leg load it.
+ * It restates, in plain C++ (no Eigen/Boost, which are absent here), the
+ * reference's CPU implementation of IPCSolver::step and everything below it
+ * (nexdynipc/src/Dynamics/IPCSolver.cpp:808-1231 and the files it calls).
+ * Each function in refcpu.cpp cites the reference lines it follows.
+ *
+ * It shares the scene / state / contact structs of the product's public
+ * header include/nxd.h so that both sides read identical inputs.
+ */
+#ifndef NXD_REFCPU_H
+#define NXD_REFCPU_H
+
+#include "../include/nxd.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct nxo_world nxo_world;
+
+nxo_world* nxo_create(const nxd_scene_desc* desc);
+void nxo_destroy(nxo_world* w);
+
+/* literal_min_distance: 1 = the reference's O(N^2 V (V+F)) loop as written,
+ *   0 = the pruned loop (same result whenever the minimum is below 1e-6).
+ * min_distance_stride: literal loop visits only bodies i % stride == 0 (used
+ *   to time a bounded sample; results are then not the reference's).
+ * num_threads: OpenMP threads for the independent loops (1 = serial, as the
+ *   reference runs). */
+void nxo_set_options(nxo_world* w, int literal_min_distance, int min_distance_stride,
+                     int num_threads);
+
+int nxo_step(nxo_world* w, double dt);
+int nxo_get_state(nxo_world* w, const nxd_state* out);
+int nxo_set_state(nxo_world* w, const nxd_state* in);
+int nxo_get_diagnostics(nxo_world* w, nxd_diagnostics* out);
+int nxo_get_joint_state(nxo_world* w, double* lambda6, double* stiffness);
+/* Per-phase wall time of the last step in seconds:
+ * [0] assembly+candidates, [1] adaptive barrier (min distance), [2] CCD,
+ * [3] detectContacts, [4] ALM/Newton loop, [5] total. */
+void nxo_last_step_times(nxo_world* w, double* out6);
+
+int64_t nxo_body_pairs(nxo_world* w, double r, int32_t* pairs, int64_t cap);
+int nxo_build_candidates(nxo_world* w, double activation_distance, nxd_candidates* out);
+int nxo_detect_contacts(nxo_world* w, const double* x, nxd_contact* out, int32_t cap,
+                        int32_t* count, int32_t* raw_count);
+double nxo_scene_min_distance(nxo_world* w, int literal);
+double nxo_max_step(nxo_world* w, double dt);
+
+int nxo_set_form_state(nxo_world* w, const nxd_contact* contacts, int32_t n,
+                       const double* normal_forces, const double* x_hat, double dt);
+int nxo_form_value(nxo_world* w, int32_t form, const double* x, double* out);
+int nxo_form_gradient(nxo_world* w, int32_t form, const double* x, double* grad);
+/* Dense (6n x 6n, row-major) Hessian of a form, duplicates summed. */
+int nxo_form_hessian_dense(nxo_world* w, int32_t form, const double* x, double* H);
+int nxo_normal_forces(nxo_world* w, const double* x, double* out, int32_t n);
+/* LDL^T solve of H dx = b with the oracle's solver (dense H input). */
+int nxo_ldlt_solve(const double* H, int32_t n, const double* b, double* x);
+
+/* select_top_k_indices (ContactAssembler.cpp:67-88) on a score array:
+ * std::nth_element + std::sort from this toolchain's libstdc++. */
+void nxo_select_top_k(const double* scores, int32_t n, int32_t k, int32_t* out_idx);
+/* std::sort of an index array by score (IPCSolver.cpp:571-577 uses it). */
+void nxo_std_sort(const double* keys, int32_t n, int32_t* idx_inout);
+
+/* Stand-alone pieces used by the ported known-answer tests. */
+double nxo_barrier_value(double d, double dhat, double kappa);
+double nxo_barrier_gradient(double d, double dhat, double kappa);
+double nxo_barrier_hessian(double d, double dhat, double kappa);
+double nxo_friction_value(const double* u, double N, double mu, double eps);
+void nxo_friction_gradient(const double* u, double N, double mu, double eps, double* g);
+void nxo_friction_hessian(const double* u, double N, double mu, double eps, double* H9);
+double nxo_friction_value_smooth(const double* u, double N, double mu, double eps);
+void nxo_friction_gradient_smooth(const double* u, double N, double mu, double eps, double* g);
+void nxo_friction_hessian_smooth(const double* u, double N, double mu, double eps, double* H9);
+/* Interval root finder on a 1-D polynomial sum c_k t^k (IntervalRootFinder.h:163-190):
+ * returns 1 and the root interval if found. */
+int nxo_interval_root_poly(const double* coeffs, int32_t degree, double lo, double hi,
+                           double tol, double* root_lo, double* root_hi);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
