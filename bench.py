@@ -1,0 +1,305 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 contact step (IPCSolver::step of NexDynIPC).
+
+Workload: the 1024-body hopper scene (1024 convex hulls of 64 seeded sphere
+points scaled to 0.05 m in a 1x1x4 m open hopper, plus 32 hinge chains of 8
+links with angle limits; 1313 bodies; dt 5e-3, dhat 5e-4, mu 0.3, 2 ALM
+iterations), generated from a seed (no dataset).  A step is one
+IPCSolver::step.  Prints one JSON line.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun each rank steps its own replica of the scene on its GPU (the
+single-scene step does not shard: replicas only); the value is the steps of
+all ranks divided by the slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "steps/s @1024 bodies (1e-6 traj err), GPU plain vs batched; fwd+adj/fwd time"
+UNIT = "steps/s"
+WORKLOAD = ("hopper_chains: 1024 convex hulls (64 seeded sphere points, 124 tris, scaled 0.05 m) in a 1x1x4 m "
+            "open hopper + 32 hinge chains x 8 links with +-60 deg angle limits; 1313 bodies, 130442 tris; "
+            "dt=5e-3, dhat=5e-4, mu=0.3, 2 ALM iterations; FP64")
+FAMILIES = ["assembly", "broad_phase", "topk", "narrow_phase", "min_distance", "newton", "alm_post", "scan", "other"]
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                vals = [v.strip() for v in out.stdout.strip().split(",")]
+                if len(vals) >= 7:
+                    self.samples.append(vals)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_narrow_bytes(ctx_diag_items):
+    """Compulsory bytes of one narrow-phase pass: per face-vertex candidate
+    16 B of ids + 4 x 24 B of vertex coordinates, per edge-edge candidate
+    24 B + 4 x 24 B, plus the 1 B hit flag written and read back; 88 B per
+    contact written."""
+    fv, ee, contacts = ctx_diag_items
+    return fv * (16 + 96 + 2) + ee * (24 + 96 + 2) + contacts * 88
+
+
+def cpu_baseline_sample(scene_fn, threads: int, stride: int):
+    """One oracle step on the same scene with the reference's literal
+    computeSceneMinDistance restricted to bodies i % stride == 0; its time is
+    scaled by stride.  Returns estimated seconds per step."""
+    from oracle.refcpu import OracleWorld
+    sc = scene_fn()
+    ow = OracleWorld(sc, literal_min_distance=True, threads=threads, md_stride=stride)
+    t0 = time.perf_counter()
+    ow.step()
+    wall = time.perf_counter() - t0
+    t = ow.step_times()
+    est = t[5] + t[1] * (stride - 1)
+    ow.close()
+    return est, wall
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    from nexdynipc_b200 import scenes
+    threads = os.cpu_count() or 1
+    stride = 64
+    ests, walls = [], []
+    for i in range(args.warmup + args.steps):
+        est, wall = cpu_baseline_sample(scenes.hopper_chains, threads, stride)
+        if i >= args.warmup:
+            ests.append(est)
+            walls.append(wall)
+    value = len(ests) / sum(ests)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(ests) / len(ests),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": (f"each step: first step of the scene through the CPU oracle (the reference "
+                                    f"cannot be built here: Eigen/Boost absent) with {threads} OpenMP threads, "
+                                    f"literal O(N^2 V F) computeSceneMinDistance over bodies i % {stride} == 0 "
+                                    f"scaled x{stride}; measured wall {np.mean(walls):.1f} s per sample")},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from nexdynipc_b200 import abi, runtime, scenes
+
+    sc = scenes.hopper_chains()
+    ctx = runtime.Context(sc)
+    lib = runtime.lib()
+    stream = torch.cuda.Stream()
+    lib.nxd_set_stream(ctx.h, C.c_void_p(stream.cuda_stream))
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")   # > 126 MB L2
+    dt = sc.dt
+
+    def step():
+        st = lib.nxd_step(ctx.h, dt)
+        if st != 0:
+            raise runtime.NxdError("nxd_step", st)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    init_state = ctx.state()
+
+    # --- device-timed steps (inputs resident in HBM), L2 flushed between steps
+    prof_ms = np.zeros(9)
+    prof_n = np.zeros(9, dtype=np.int64)
+    lib.nxd_profile(ctx.h, 1, None, None)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.fill_(k & 0xFF)
+                starts[k].record(stream)
+                step()
+                ends[k].record(stream)
+        torch.cuda.synchronize()
+    lib.nxd_profile(ctx.h, 0, abi.dptr(prof_ms), prof_n.ctypes.data_as(C.POINTER(C.c_int64)))
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    diag = ctx.diagnostics()
+    if ws > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = ws * args.steps / (total_ms / 1e3)
+
+    # --- narrow-phase item counts of the current candidate set (roofline units)
+    cand_counts = ctx.candidate_counts(sc.settings.dhat) if hasattr(ctx, "candidate_counts") else None
+
+    # --- end to end through the C ABI with pinned host buffers
+    n = sc.n_bodies
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in init_state.items()}
+    out_pinned = {k: torch.empty_like(v).pin_memory() for k, v in pinned.items()}
+    dp = C.POINTER(C.c_double)
+
+    def view(d):
+        return abi.NxdState(*[C.cast(C.c_void_p(d[k].data_ptr()), dp) for k in
+                              ("position", "orientation", "velocity", "angular_velocity", "linear_acceleration",
+                               "angular_acceleration")])
+
+    vin, vout = view(pinned), view(out_pinned)
+    h2d = sum(v.numel() * 8 for v in pinned.values())
+    d2h = sum(v.numel() * 8 for v in out_pinned.values())
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        lib.nxd_set_state(ctx.h, C.byref(vin))
+        step()
+        lib.nxd_get_state(ctx.h, C.byref(vout))
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if ws > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = ws * args.steps / e2e_s
+
+    # --- roofline of the dominant kernel family, timed live above
+    fam = int(np.argmax(prof_ms))
+    peak, peak_kind = measured_peaks()
+    roof = {"kernel": FAMILIES[fam], "bound": "hbm", "unit": "GB/s", "peak": peak, "peak_kind": peak_kind,
+            "ms_per_launch": float(prof_ms[fam] / max(prof_n[fam], 1)), "launches": int(prof_n[fam]),
+            "share_of_step_time": float(prof_ms[fam] / max(prof_ms.sum(), 1e-30))}
+    if FAMILIES[fam] == "narrow_phase" and cand_counts:
+        fv, ee = cand_counts
+        # per launch: the count kernel reads the items, the write kernel
+        # re-reads the flags; count both launches of a pass as one unit
+        bytes_pass = algorithmic_narrow_bytes((fv, ee, diag["n_contacts"]))
+        passes = prof_n[fam] / 6.0
+        achieved = bytes_pass * passes / (prof_ms[fam] / 1e3) / 1e9
+        roof.update(achieved=achieved, frac=achieved / peak, traffic=None,
+                    algorithmic_bytes_per_pass=bytes_pass)
+    else:
+        roof.update(achieved=None, frac=None, traffic=None)
+    per_family = {FAMILIES[i]: {"ms": round(float(prof_ms[i]), 3), "launches": int(prof_n[i])} for i in range(9)}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        stride = 64
+        est, wall = cpu_baseline_sample(scenes.hopper_chains, 1, stride)
+        cpu = {"value": 1.0 / est, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": (f"first step of the same scene through the CPU oracle (serial, as the reference runs; "
+                          f"the reference itself cannot be built here), literal computeSceneMinDistance over bodies "
+                          f"i % {stride} == 0 scaled x{stride}; {wall:.1f} s wall")}
+    launches_total = int(prof_n.sum())
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "replicas": ws, "l2": "flushed between steps (256 MiB write, untimed)",
+                   "per_family_ms": per_family, "last_step": {k: diag[k] for k in
+                                                              ("n_body_pairs", "n_contacts", "alm_iterations",
+                                                               "newton_iterations", "status")}},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": launches_total,
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -239,9 +239,14 @@ nxd_status nxd_max_step(nxd_ctx* ctx, double dt, double* out_dt);
 
 /* Form plugin interface (Dynamics/Forms/Form.h:8-21) evaluated at x against
  * the contacts / normal forces / predictive state installed below.
- * value: energy; gradient: overwrites grad[6n]; hessian: dense block rows of
- * the 6x6 block-sparse matrix as a BSR with caller buffers
- * (row_ptr[n+1], col_idx[cap], vals[cap*36] row-major blocks). */
+ * value: energy; gradient: overwrites grad[6n]; hessian (NXD_FORM_TOTAL):
+ * 6x6 blocks in BSR layout with caller buffers (row_ptr[n+1], col_idx[cap],
+ * vals[cap*36] row-major blocks).  Like the reference's triplet list
+ * (Form::hessian appends triplets that Eigen's setFromTriplets sums), a row
+ * may repeat a column: its summed diagonal block comes first, then one block
+ * per coupling term (joint, active barrier contact, friction contact) in term
+ * order; the consumer sums duplicates.  *nnzb receives the block count
+ * (NXD_CAPACITY when it exceeds cap). */
 nxd_status nxd_form_value(nxd_ctx* ctx, int32_t form, const double* x, double* out);
 nxd_status nxd_form_gradient(nxd_ctx* ctx, int32_t form, const double* x, double* grad);
 nxd_status nxd_form_hessian_bsr(nxd_ctx* ctx, int32_t form, const double* x,
@@ -258,7 +263,27 @@ nxd_status nxd_set_form_state(nxd_ctx* ctx, const nxd_contact* contacts, int32_t
 /* DistanceBarrierForm::computeNormalForces (DistanceBarrierForm.cpp:70-86). */
 nxd_status nxd_normal_forces(nxd_ctx* ctx, const double* x, double* out, int32_t n);
 
-/* Batched form (independent scenes, one launch per phase for all of them). */
+/* Device-side timing by kernel family, for measurement.  Every launch is
+ * counted; with profiling enabled each launch is bracketed by CUDA events on
+ * the context's stream.  nxd_profile(ctx, enable, ms, launches) synchronises,
+ * writes the accumulated milliseconds and launch counts since the previous
+ * call (arrays of NXD_PROF_FAMILIES, either may be NULL), resets them and
+ * switches event timing on (enable = 1) or off (0). */
+enum {
+    NXD_PROF_ASSEMBLY = 0,      /* body boxes, world vertices, poses        */
+    NXD_PROF_BROAD = 1,         /* body-pair broad phase                    */
+    NXD_PROF_TOPK = 2,          /* top-32 primitive selection               */
+    NXD_PROF_NARROW = 3,        /* narrow phase (count + ordered write)     */
+    NXD_PROF_MIN_DISTANCE = 4,  /* scene minimum distance                   */
+    NXD_PROF_NEWTON = 5,        /* Newton solve (one CTA per scene)         */
+    NXD_PROF_ALM_POST = 6,      /* ALM convergence / normal forces          */
+    NXD_PROF_SCAN = 7,          /* prefix sums                              */
+    NXD_PROF_OTHER = 8,
+    NXD_PROF_FAMILIES = 9
+};
+nxd_status nxd_profile(nxd_ctx* ctx, int32_t enable, double* ms, int64_t* launches);
+
+/* Batched form (independent scenes stepped together). */
 typedef struct nxd_batch nxd_batch;
 nxd_status nxd_batch_create(const nxd_scene_desc* descs, int32_t n_scenes, nxd_batch** out);
 void nxd_batch_destroy(nxd_batch* b);

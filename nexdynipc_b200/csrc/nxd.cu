@@ -67,6 +67,11 @@ int grid_for(long long n, int block, int max_blocks = 1 << 16) {
 
 struct nxd_ctx {
     DevArena mem;
+    // launch accounting (always) and per-family device timing (when enabled)
+    long long launches[NXD_PROF_FAMILIES] = {};
+    bool prof = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[NXD_PROF_FAMILIES];
+    std::vector<cudaEvent_t> pool;
     cudaStream_t stream = nullptr;
     int dev = 0, n_sm = 148;
     int N = 0, nv = 0, nf = 0, ne = 0, J = 0, D = 0;
@@ -108,6 +113,24 @@ struct nxd_ctx {
 };
 
 namespace {
+
+cudaEvent_t prof_event(nxd_ctx* c) {
+    if (!c->pool.empty()) { cudaEvent_t e = c->pool.back(); c->pool.pop_back(); return e; }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+struct ProfScope {
+    nxd_ctx* c; int fam; cudaEvent_t a = nullptr;
+    ProfScope(nxd_ctx* c_, int f) : c(c_), fam(f) {
+        c->launches[fam] += 1;
+        if (c->prof) { a = prof_event(c); cudaEventRecord(a, c->stream); }
+    }
+    ~ProfScope() {
+        if (c->prof) { cudaEvent_t b = prof_event(c); cudaEventRecord(b, c->stream); c->ev[fam].push_back({a, b}); }
+    }
+};
+#define NXD_LAUNCH(ctx, fam, ...) do { ProfScope ps_(ctx, fam); __VA_ARGS__; } while (0)
 
 void fill_solver(nxd_ctx* c) {
     Solver& S = c->S;
@@ -172,16 +195,16 @@ StepCfg step_cfg(const nxd_ctx* c) {
 
 // ContactAssembler::build + world vertices at the current poses
 void launch_assembly(nxd_ctx* c) {
-    k_body_boxes<<<grid_for(c->N, 128), 128, 0, c->stream>>>(c->geo, c->pos, c->quat, c->boxes);
-    k_world_vertices<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(c->geo, c->nv, c->vbody, c->pos, c->quat, c->wv);
+    NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_body_boxes<<<grid_for(c->N, 128), 128, 0, c->stream>>>(c->geo, c->pos, c->quat, c->boxes););
+    NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_world_vertices<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(c->geo, c->nv, c->vbody, c->pos, c->quat, c->wv););
 }
 
 // pair list (count / scan / write) with query q into out, count -> *count_dev
 void launch_pairs(nxd_ctx* c, const PairQuery& q, int* out, int* count_dev, const int* gate) {
     const int blocks = grid_for((long long)c->N * 32, 256);
-    k_pairs<<<blocks, 256, 0, c->stream>>>(c->geo, q, c->boxes, c->pair_cnt, nullptr, nullptr, 0, gate);
-    k_scan<<<1, 1024, 0, c->stream>>>(c->pair_cnt, c->pair_off, c->N, count_dev, gate);
-    k_pairs<<<blocks, 256, 0, c->stream>>>(c->geo, q, c->boxes, nullptr, c->pair_off, out, c->pair_cap, gate);
+    NXD_LAUNCH(c, NXD_PROF_BROAD, k_pairs<<<blocks, 256, 0, c->stream>>>(c->geo, q, c->boxes, c->pair_cnt, nullptr, nullptr, 0, gate););
+    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->pair_cnt, c->pair_off, c->N, count_dev, gate););
+    NXD_LAUNCH(c, NXD_PROF_BROAD, k_pairs<<<blocks, 256, 0, c->stream>>>(c->geo, q, c->boxes, nullptr, c->pair_off, out, c->pair_cap, gate););
 }
 
 size_t topk_smem(const nxd_ctx* c, int warps) {
@@ -194,14 +217,14 @@ void launch_candidates(nxd_ctx* c, const double* act_ptr, double act_val) {
     launch_pairs(c, q, c->pairs, &c->sc->n_pairs, nullptr);
     int warps = 4;
     while (warps > 1 && topk_smem(c, warps) > 200 * 1024) --warps;
-    k_topk<<<c->n_sm * 4, 32 * warps, topk_smem(c, warps), c->stream>>>(c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap,
-                                                                       c->boxes, c->wv, c->topk, c->topn, c->max_prims);
-    k_item_counts<<<grid_for(c->pair_cap, 256), 256, 0, c->stream>>>(&c->sc->n_pairs, c->pair_cap, c->topn, c->nfv,
-                                                                       c->nee, c->nvv, c->nev);
+    NXD_LAUNCH(c, NXD_PROF_TOPK, k_topk<<<c->n_sm * 4, 32 * warps, topk_smem(c, warps), c->stream>>>(c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap,
+                                                                       c->boxes, c->wv, c->topk, c->topn, c->max_prims););
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_item_counts<<<grid_for(c->pair_cap, 256), 256, 0, c->stream>>>(&c->sc->n_pairs, c->pair_cap, c->topn, c->nfv,
+                                                                       c->nee, c->nvv, c->nev););
     const int* np = &c->sc->n_pairs;
-    k_scan<<<1, 1024, 0, c->stream>>>(c->nfv, c->off_fv, c->pair_cap, &c->sc->fv_items, nullptr, nullptr, np);
-    k_scan<<<1, 1024, 0, c->stream>>>(c->nee, c->off_ee, c->pair_cap, &c->sc->ee_items, nullptr, nullptr, np);
-    k_scan<<<1, 1024, 0, c->stream>>>(c->nvv, c->off_vv, c->pair_cap, &c->sc->vv_items, nullptr, nullptr, np);
+    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->nfv, c->off_fv, c->pair_cap, &c->sc->fv_items, nullptr, nullptr, np););
+    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->nee, c->off_ee, c->pair_cap, &c->sc->ee_items, nullptr, nullptr, np););
+    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->nvv, c->off_vv, c->pair_cap, &c->sc->vv_items, nullptr, nullptr, np););
 }
 
 }  // namespace
@@ -217,19 +240,19 @@ void launch_narrow_full(nxd_ctx* c, const double* wv, const double* pose_p, cons
     const int blocks = c->n_sm * 8;
     int* skip_vv = c->i_scratch;
     const int* np = &c->sc->n_pairs;
-    k_narrow_count<<<blocks, 256, 0, c->stream>>>(in, 0, c->off_fv, c->flags, c->hit_cnt, skip_if);
-    k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->fv_hits, nullptr, skip_if, np);
-    k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 0, c->off_fv, c->flags, c->hit_off, nullptr, c->contacts, skip_if);
-    k_narrow_count<<<blocks, 256, 0, c->stream>>>(in, 1, c->off_ee, c->flags, c->hit_cnt, skip_if);
-    k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->ee_hits, nullptr, skip_if, np);
-    k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 1, c->off_ee, c->flags, c->hit_off, &c->sc->fv_hits, c->contacts,
-                                                  skip_if);
-    k_contact_totals<<<1, 1, 0, c->stream>>>(c->sc, 0, skip_if, skip_vv);
-    k_narrow_count<<<blocks, 256, 0, c->stream>>>(in, 2, c->off_vv, c->flags, c->hit_cnt, skip_vv);
-    k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->vv_hits, nullptr, skip_vv, np);
-    k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 2, c->off_vv, c->flags, c->hit_off, nullptr, c->contacts, skip_vv);
-    k_contact_totals<<<1, 1, 0, c->stream>>>(c->sc, 1, skip_if, nullptr);
-    k_sort_contacts<<<1, 1024, 0, c->stream>>>(c->sc, c->contacts, c->contacts_tmp, c->sort_key, c->sort_idx, skip_if);
+    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_count<<<blocks, 256, 0, c->stream>>>(in, 0, c->off_fv, c->flags, c->hit_cnt, skip_if););
+    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->fv_hits, nullptr, skip_if, np););
+    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 0, c->off_fv, c->flags, c->hit_off, nullptr, c->contacts, skip_if););
+    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_count<<<blocks, 256, 0, c->stream>>>(in, 1, c->off_ee, c->flags, c->hit_cnt, skip_if););
+    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->ee_hits, nullptr, skip_if, np););
+    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 1, c->off_ee, c->flags, c->hit_off, &c->sc->fv_hits, c->contacts,
+                                                  skip_if););
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_contact_totals<<<1, 1, 0, c->stream>>>(c->sc, 0, skip_if, skip_vv););
+    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_count<<<blocks, 256, 0, c->stream>>>(in, 2, c->off_vv, c->flags, c->hit_cnt, skip_vv););
+    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->vv_hits, nullptr, skip_vv, np););
+    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 2, c->off_vv, c->flags, c->hit_off, nullptr, c->contacts, skip_vv););
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_contact_totals<<<1, 1, 0, c->stream>>>(c->sc, 1, skip_if, nullptr););
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_sort_contacts<<<1, 1024, 0, c->stream>>>(c->sc, c->contacts, c->contacts_tmp, c->sort_key, c->sort_idx, skip_if););
 }
 
 }  // namespace
@@ -262,41 +285,41 @@ nxd_status enqueue_step(nxd_ctx* c, double dt) {
     launch_candidates(c, &c->sc->dhat, 0.0);
     // adaptive barrier (IPCSolver.cpp:817-832)
     if (c->s.enable_adaptive_barrier) {
-        k_barrier_init<<<1, 1024, 0, st>>>(cfg, c->mass, c->pos, c->sc, c->S.red);
-        k_init_scalar_d<<<1, 1, 0, st>>>(&c->sc->bmd, INFINITY);
+        NXD_LAUNCH(c, NXD_PROF_OTHER, k_barrier_init<<<1, 1024, 0, st>>>(cfg, c->mass, c->pos, c->sc, c->S.red););
+        NXD_LAUNCH(c, NXD_PROF_OTHER, k_init_scalar_d<<<1, 1, 0, st>>>(&c->sc->bmd, INFINITY););
         PairQuery qb{0, &c->sc->dhat, 0.0, 2.0, 0.0};
-        k_min_pair_distance<<<grid_for((long long)c->N * 32, 256), 256, 0, st>>>(c->geo, qb, c->boxes, &c->sc->bmd);
-        k_body_md_tol<<<grid_for(c->N, 128), 128, 0, st>>>(c->geo, c->pos, c->md_tol);
-        k_max_tol<<<1, 1, 0, st>>>(c->md_tol, c->N, c->max_md_tol);
-        k_md_gate<<<1, 1, 0, st>>>(c->sc, c->max_md_tol);
+        NXD_LAUNCH(c, NXD_PROF_BROAD, k_min_pair_distance<<<grid_for((long long)c->N * 32, 256), 256, 0, st>>>(c->geo, qb, c->boxes, &c->sc->bmd););
+        NXD_LAUNCH(c, NXD_PROF_OTHER, k_body_md_tol<<<grid_for(c->N, 128), 128, 0, st>>>(c->geo, c->pos, c->md_tol););
+        NXD_LAUNCH(c, NXD_PROF_OTHER, k_max_tol<<<1, 1, 0, st>>>(c->md_tol, c->N, c->max_md_tol););
+        NXD_LAUNCH(c, NXD_PROF_OTHER, k_md_gate<<<1, 1, 0, st>>>(c->sc, c->max_md_tol););
         PairQuery qm{2, &c->sc->md_radius, 0.0, 1.0, 0.0};
         launch_pairs(c, qm, c->md_pairs, &c->sc->n_md_pairs, &c->sc->md_gate);
-        k_min_distance<<<c->n_sm * 4, 256, 0, st>>>(c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
-                                                    &c->sc->md, &c->sc->md_gate);
-        k_kappa_update<<<1, 1, 0, st>>>(c->sc);
+        NXD_LAUNCH(c, NXD_PROF_MIN_DISTANCE, k_min_distance<<<c->n_sm * 4, 256, 0, st>>>(c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
+                                                    &c->sc->md, &c->sc->md_gate););
+        NXD_LAUNCH(c, NXD_PROF_OTHER, k_kappa_update<<<1, 1, 0, st>>>(c->sc););
     }
     // computeMaxStep: the FV root box fails the reference's domain predicate
     // before any bisection, so the earliest TOI is 1 and the step is dt.
     // integrator init, contact forms, drives
-    k_step_setup<<<grid_for(std::max(c->N, c->D), 128), 128, 0, st>>>(
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_step_setup<<<grid_for(std::max(c->N, c->D), 128), 128, 0, st>>>(
         cfg, dt, c->pos, c->quat, c->vel, c->omega, c->lacc, c->aacc, c->x, c->xhat, c->xprev, c->vprev, c->aprev, c->pos0,
-        c->quat0, c->sc, c->dprm, c->dfilt, c->dfinit, c->dhas_prev);
+        c->quat0, c->sc, c->dprm, c->dfilt, c->dfinit, c->dhas_prev););
     // detectContacts at the step-start poses (when a contact form is needed)
     const bool needs = c->s.enable_adaptive_barrier || (c->s.enable_friction && c->s.friction_coeff > 0.0);
     if (needs) launch_narrow_full(c, c->wv, c->pos, nullptr);
-    else k_contact_totals<<<1, 1, 0, st>>>(c->sc, 2, nullptr, nullptr);
+    else NXD_LAUNCH(c, NXD_PROF_OTHER, k_contact_totals<<<1, 1, 0, st>>>(c->sc, 2, nullptr, nullptr));
     int* skip_detect = c->i_scratch + 1;
     for (int alm = 0; alm < c->s.alm_max_iters; ++alm) {
-        k_newton<<<1, kSolverThreads, 0, st>>>(c->S);
-        k_alm_detect_gate<<<1, 1, 0, st>>>(c->sc, skip_detect);
-        k_pose_at_x<<<grid_for(c->N, 128), 128, 0, st>>>(c->N, c->x, c->quat, c->pose_p, c->pose_q);
-        k_world_vertices<<<grid_for(c->nv, 256), 256, 0, st>>>(c->geo, c->nv, c->vbody, c->pose_p, c->pose_q, c->wvx);
+        NXD_LAUNCH(c, NXD_PROF_NEWTON, k_newton<<<1, kSolverThreads, 0, st>>>(c->S););
+        NXD_LAUNCH(c, NXD_PROF_OTHER, k_alm_detect_gate<<<1, 1, 0, st>>>(c->sc, skip_detect););
+        NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_pose_at_x<<<grid_for(c->N, 128), 128, 0, st>>>(c->N, c->x, c->quat, c->pose_p, c->pose_q););
+        NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_world_vertices<<<grid_for(c->nv, 256), 256, 0, st>>>(c->geo, c->nv, c->vbody, c->pose_p, c->pose_q, c->wvx););
         launch_narrow_full(c, c->wvx, c->pose_p, skip_detect);
-        k_alm_post<<<1, kSolverThreads, 0, st>>>(c->S, c->sc, cfg, c->nforce);
+        NXD_LAUNCH(c, NXD_PROF_ALM_POST, k_alm_post<<<1, kSolverThreads, 0, st>>>(c->S, c->sc, cfg, c->nforce););
     }
-    k_update_state<<<grid_for(c->N, 128), 128, 0, st>>>(cfg, c->x, c->xprev, c->vprev, c->pos, c->quat, c->vel, c->omega,
-                                                        c->lacc, c->aacc, c->sc, c->da, c->db, c->dprm, c->dfilt);
-    if (c->D > 0) k_drive_kpi<<<1, 1, 0, st>>>(cfg, c->omega, c->sc, c->da, c->db, c->dprm, c->dfilt);
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_update_state<<<grid_for(c->N, 128), 128, 0, st>>>(cfg, c->x, c->xprev, c->vprev, c->pos, c->quat, c->vel, c->omega,
+                                                        c->lacc, c->aacc, c->sc, c->da, c->db, c->dprm, c->dfilt););
+    if (c->D > 0) NXD_LAUNCH(c, NXD_PROF_OTHER, k_drive_kpi<<<1, 1, 0, st>>>(cfg, c->omega, c->sc, c->da, c->db, c->dprm, c->dfilt));
     NXD_CUDA(cudaGetLastError());
     return NXD_OK;
 }
@@ -509,6 +532,9 @@ nxd_status nxd_create(const nxd_scene_desc* d, nxd_ctx** out) {
 void nxd_destroy(nxd_ctx* c) {
     if (!c) return;
     cudaDeviceSynchronize();
+    for (auto& v : c->ev)
+        for (auto& pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
     c->mem.release();
     delete c;
 }
@@ -595,10 +621,10 @@ nxd_status nxd_build_candidates(nxd_ctx* c, double act, nxd_candidates* o) {
     if (!c || !o) return NXD_INVALID_ARGUMENT;
     launch_assembly(c);
     launch_candidates(c, nullptr, act);
-    k_item_counts<<<grid_for(c->pair_cap, 256), 256, 0, c->stream>>>(&c->sc->n_pairs, c->pair_cap, c->topn, c->nfv, c->nee,
-                                                                       c->nvv, c->nev);
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_item_counts<<<grid_for(c->pair_cap, 256), 256, 0, c->stream>>>(&c->sc->n_pairs, c->pair_cap, c->topn, c->nfv, c->nee,
+                                                                       c->nvv, c->nev););
     int* tot = c->i_scratch + 4;
-    k_scan<<<1, 1024, 0, c->stream>>>(c->nev, c->off_ev, c->pair_cap, tot, nullptr, nullptr, &c->sc->n_pairs);
+    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->nev, c->off_ev, c->pair_cap, tot, nullptr, nullptr, &c->sc->n_pairs););
     NXD_CUDA(cudaStreamSynchronize(c->stream));
     Scalars h;
     int nev_total = 0;
@@ -618,8 +644,8 @@ nxd_status nxd_build_candidates(nxd_ctx* c, double act, nxd_candidates* o) {
     co.ee = tmp.alloc<int>(6 * (size_t)std::max<int64_t>(1, o->ee_count)); co.ee_cap = o->ee_count;
     co.fv = tmp.alloc<int>(4 * (size_t)std::max<int64_t>(1, o->fv_count)); co.fv_cap = o->fv_count;
     if (!tmp.ok) { tmp.release(); return NXD_CUDA_ERROR; }
-    k_materialize<<<c->n_sm * 4, 256, 0, c->stream>>>(c->geo, c->body_ids, c->pairs, &c->sc->n_pairs, c->pair_cap, c->topk,
-                                                     c->topn, c->off_vv, c->off_ev, c->off_ee, c->off_fv, co);
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_materialize<<<c->n_sm * 4, 256, 0, c->stream>>>(c->geo, c->body_ids, c->pairs, &c->sc->n_pairs, c->pair_cap, c->topk,
+                                                     c->topn, c->off_vv, c->off_ev, c->off_ee, c->off_fv, co););
     cudaStreamSynchronize(c->stream);
     auto back = [&](int32_t* buf, int64_t cap, const int* dev, int64_t cnt, int w) {
         if (buf && cnt > 0) cudaMemcpy(buf, dev, sizeof(int) * w * (size_t)std::min(cap, cnt), cudaMemcpyDeviceToHost);
@@ -638,8 +664,8 @@ nxd_status nxd_detect_contacts(nxd_ctx* c, const double* x, nxd_contact* out, in
     launch_candidates(c, &c->sc->dhat, 0.0);
     if (x) {
         NXD_CUDA(cudaMemcpyAsync(c->S.xt, x, 6 * (size_t)c->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-        k_pose_at_x<<<grid_for(c->N, 128), 128, 0, c->stream>>>(c->N, c->S.xt, c->quat, c->pose_p, c->pose_q);
-        k_world_vertices<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(c->geo, c->nv, c->vbody, c->pose_p, c->pose_q, c->wvx);
+        NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_pose_at_x<<<grid_for(c->N, 128), 128, 0, c->stream>>>(c->N, c->S.xt, c->quat, c->pose_p, c->pose_q););
+        NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_world_vertices<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(c->geo, c->nv, c->vbody, c->pose_p, c->pose_q, c->wvx););
         launch_narrow_full(c, c->wvx, c->pose_p, nullptr);
     } else {
         launch_narrow_full(c, c->wv, c->pos, nullptr);
@@ -657,20 +683,40 @@ nxd_status nxd_scene_min_distance(nxd_ctx* c, double* out) {
     if (!c || !out) return NXD_INVALID_ARGUMENT;
     launch_assembly(c);
     cudaStream_t st = c->stream;
-    k_body_md_tol<<<grid_for(c->N, 128), 128, 0, st>>>(c->geo, c->pos, c->md_tol);
-    k_max_tol<<<1, 1, 0, st>>>(c->md_tol, c->N, c->max_md_tol);
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_body_md_tol<<<grid_for(c->N, 128), 128, 0, st>>>(c->geo, c->pos, c->md_tol););
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_max_tol<<<1, 1, 0, st>>>(c->md_tol, c->N, c->max_md_tol););
     // force the gate open: bmd = 0
-    k_init_scalar_d<<<1, 1, 0, st>>>(&c->sc->bmd, 0.0);
-    k_md_gate<<<1, 1, 0, st>>>(c->sc, c->max_md_tol);
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_init_scalar_d<<<1, 1, 0, st>>>(&c->sc->bmd, 0.0););
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_md_gate<<<1, 1, 0, st>>>(c->sc, c->max_md_tol););
     PairQuery qm{2, &c->sc->md_radius, 0.0, 1.0, 0.0};
     launch_pairs(c, qm, c->md_pairs, &c->sc->n_md_pairs, &c->sc->md_gate);
-    k_min_distance<<<c->n_sm * 4, 256, 0, st>>>(c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
-                                                &c->sc->md, &c->sc->md_gate);
+    NXD_LAUNCH(c, NXD_PROF_MIN_DISTANCE, k_min_distance<<<c->n_sm * 4, 256, 0, st>>>(c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
+                                                &c->sc->md, &c->sc->md_gate););
     NXD_CUDA(cudaStreamSynchronize(st));
     Scalars h;
     NXD_CUDA(cudaMemcpy(&h, c->sc, sizeof(h), cudaMemcpyDeviceToHost));
     *out = h.md;
     return h.n_md_pairs > c->pair_cap ? NXD_CAPACITY : NXD_OK;
+}
+
+nxd_status nxd_profile(nxd_ctx* c, int32_t enable, double* ms, int64_t* launches) {
+    if (!c) return NXD_INVALID_ARGUMENT;
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    for (int f = 0; f < NXD_PROF_FAMILIES; ++f) {
+        double t = 0.0;
+        for (auto& pr : c->ev[f]) {
+            float m = 0.f;
+            if (cudaEventElapsedTime(&m, pr.first, pr.second) == cudaSuccess) t += m;
+            c->pool.push_back(pr.first);
+            c->pool.push_back(pr.second);
+        }
+        c->ev[f].clear();
+        if (ms) ms[f] = t;
+        if (launches) launches[f] = c->launches[f];
+        c->launches[f] = 0;
+    }
+    c->prof = enable != 0;
+    return NXD_OK;
 }
 
 nxd_status nxd_max_step(nxd_ctx* c, double dt, double* out_dt) {
@@ -682,6 +728,146 @@ nxd_status nxd_max_step(nxd_ctx* c, double dt, double* out_dt) {
     if (!c || !out_dt) return NXD_INVALID_ARGUMENT;
     *out_dt = dt;
     return NXD_OK;
+}
+
+nxd_status nxd_set_form_state(nxd_ctx* c, const nxd_contact* contacts, int32_t n, const double* normal_forces,
+                              const double* x_hat, double dt) {
+    if (!c || n < 0 || n > kMaxRawContacts || (n > 0 && !contacts) || !(dt > 0.0)) return NXD_INVALID_ARGUMENT;
+    cudaStream_t st = c->stream;
+    if (n > 0)
+        NXD_CUDA(cudaMemcpyAsync(c->contacts, contacts, sizeof(nxd_contact) * (size_t)n, cudaMemcpyHostToDevice, st));
+    if (normal_forces && n > 0)
+        NXD_CUDA(cudaMemcpyAsync(c->nforce, normal_forces, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, st));
+    if (x_hat) NXD_CUDA(cudaMemcpyAsync(c->xhat, x_hat, 6 * sizeof(double) * (size_t)c->N, cudaMemcpyHostToDevice, st));
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_set_form_state<<<grid_for(std::max(c->N, std::max(c->D, 1)), 128), 128, 0, st>>>(
+        step_cfg(c), c->sc, n, normal_forces ? n : 0, dt, c->pos, c->quat, c->pos0, c->quat0, c->dhas_prev););
+    NXD_CUDA(cudaStreamSynchronize(st));
+    return NXD_OK;
+}
+
+static nxd_status form_call(nxd_ctx* c, int32_t form, const double* x, int what, double* host_out, int32_t* row_ptr,
+                            int32_t* col_idx, double* vals, int64_t cap, int64_t* nnzb) {
+    if (!c || !x || form < 0 || form > NXD_FORM_CONTACT) return NXD_INVALID_ARGUMENT;
+    cudaStream_t st = c->stream;
+    const size_t n6 = 6 * (size_t)c->N;
+    double* xd = c->S.xt;   // scratch (the step is not running on this stream)
+    NXD_CUDA(cudaMemcpyAsync(xd, x, n6 * sizeof(double), cudaMemcpyHostToDevice, st));
+    DevArena tmp;
+    double* outd = tmp.alloc<double>(what == 1 ? n6 : 1);
+    int* rp = nullptr; int* ci = nullptr; double* vv = nullptr; long long* nz = nullptr;
+    if (what == 2) {
+        rp = tmp.alloc<int>(c->N + 1);
+        ci = tmp.alloc<int>(std::max<int64_t>(cap, 1));
+        vv = tmp.alloc<double>(36 * (size_t)std::max<int64_t>(cap, 1));
+        nz = tmp.alloc<long long>(1);
+    }
+    if (!tmp.ok) { tmp.release(); return NXD_CUDA_ERROR; }
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_form_eval<<<1, kSolverThreads, 0, st>>>(c->S, c->sc, form, what, xd, outd, rp, ci, vv, cap, nz););
+    cudaError_t e = cudaStreamSynchronize(st);
+    nxd_status rc = NXD_OK;
+    if (e != cudaSuccess) rc = NXD_CUDA_ERROR;
+    else if (what == 0) cudaMemcpy(host_out, outd, sizeof(double), cudaMemcpyDeviceToHost);
+    else if (what == 1) cudaMemcpy(host_out, outd, n6 * sizeof(double), cudaMemcpyDeviceToHost);
+    else {
+        long long nzh = 0;
+        cudaMemcpy(&nzh, nz, sizeof(long long), cudaMemcpyDeviceToHost);
+        if (nnzb) *nnzb = nzh;
+        if (nzh < 0) rc = NXD_INVALID_ARGUMENT;
+        else if (nzh > cap) rc = NXD_CAPACITY;
+        else {
+            if (row_ptr) cudaMemcpy(row_ptr, rp, sizeof(int) * (c->N + 1), cudaMemcpyDeviceToHost);
+            if (col_idx) cudaMemcpy(col_idx, ci, sizeof(int) * (size_t)nzh, cudaMemcpyDeviceToHost);
+            if (vals) cudaMemcpy(vals, vv, 36 * sizeof(double) * (size_t)nzh, cudaMemcpyDeviceToHost);
+        }
+    }
+    tmp.release();
+    return rc;
+}
+
+nxd_status nxd_form_value(nxd_ctx* c, int32_t form, const double* x, double* out) {
+    if (!out) return NXD_INVALID_ARGUMENT;
+    return form_call(c, form, x, 0, out, nullptr, nullptr, nullptr, 0, nullptr);
+}
+nxd_status nxd_form_gradient(nxd_ctx* c, int32_t form, const double* x, double* grad) {
+    if (!grad) return NXD_INVALID_ARGUMENT;
+    return form_call(c, form, x, 1, grad, nullptr, nullptr, nullptr, 0, nullptr);
+}
+nxd_status nxd_form_hessian_bsr(nxd_ctx* c, int32_t form, const double* x, int32_t* row_ptr, int32_t* col_idx,
+                                double* vals, int64_t cap, int64_t* nnzb) {
+    return form_call(c, form, x, 2, nullptr, row_ptr, col_idx, vals, cap, nnzb);
+}
+
+nxd_status nxd_normal_forces(nxd_ctx* c, const double* x, double* out, int32_t n) {
+    if (!c || !x || !out || n < 0) return NXD_INVALID_ARGUMENT;
+    cudaStream_t st = c->stream;
+    NXD_CUDA(cudaMemcpyAsync(c->S.xt, x, 6 * sizeof(double) * (size_t)c->N, cudaMemcpyHostToDevice, st));
+    DevArena tmp;
+    double* od = tmp.alloc<double>(std::max(n, 1));
+    if (!tmp.ok) { tmp.release(); return NXD_CUDA_ERROR; }
+    NXD_LAUNCH(c, NXD_PROF_OTHER, k_normal_forces<<<grid_for(std::max(n, 1), 128), 128, 0, st>>>(c->S, c->sc, c->S.xt, od, n););
+    cudaStreamSynchronize(st);
+    cudaMemcpy(out, od, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost);
+    tmp.release();
+    return NXD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batched scenes: one context per scene sharing one stream.
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct nxd_batch {
+    std::vector<nxd_ctx*> ctx;
+    cudaStream_t stream = nullptr;
+};
+
+extern "C" {
+
+nxd_status nxd_batch_create(const nxd_scene_desc* descs, int32_t n, nxd_batch** out) {
+    if (!descs || n <= 0 || !out) return NXD_INVALID_ARGUMENT;
+    nxd_batch* b = new (std::nothrow) nxd_batch();
+    if (!b) return NXD_INVALID_ARGUMENT;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) { delete b; return NXD_CUDA_ERROR; }
+    for (int i = 0; i < n; ++i) {
+        nxd_ctx* c = nullptr;
+        const nxd_status st = nxd_create(descs + i, &c);
+        if (st != NXD_OK) {
+            for (nxd_ctx* x : b->ctx) nxd_destroy(x);
+            cudaStreamDestroy(b->stream);
+            delete b;
+            return st;
+        }
+        c->stream = b->stream;
+        b->ctx.push_back(c);
+    }
+    *out = b;
+    return NXD_OK;
+}
+
+void nxd_batch_destroy(nxd_batch* b) {
+    if (!b) return;
+    for (nxd_ctx* c : b->ctx) nxd_destroy(c);
+    cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+nxd_status nxd_batch_step(nxd_batch* b, const double* dts) {
+    if (!b || !dts) return NXD_INVALID_ARGUMENT;
+    for (size_t i = 0; i < b->ctx.size(); ++i) {
+        const nxd_status st = nxd_step(b->ctx[i], dts[i]);
+        if (st != NXD_OK) return st;
+    }
+    return NXD_OK;
+}
+
+nxd_status nxd_batch_get_state(nxd_batch* b, int32_t scene, const nxd_state* o) {
+    if (!b || scene < 0 || scene >= (int)b->ctx.size()) return NXD_INVALID_ARGUMENT;
+    return nxd_get_state(b->ctx[scene], o);
+}
+
+nxd_status nxd_batch_get_diagnostics(nxd_batch* b, int32_t scene, nxd_diagnostics* o) {
+    if (!b || scene < 0 || scene >= (int)b->ctx.size()) return NXD_INVALID_ARGUMENT;
+    return nxd_get_diagnostics(b->ctx[scene], o);
 }
 
 }  // extern "C"

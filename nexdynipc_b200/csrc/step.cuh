@@ -299,3 +299,244 @@ __global__ void k_drive_kpi(StepCfg cfg, const double* omega, Scalars* sc, const
 }
 
 }  // namespace nx
+
+namespace nx {
+
+// ---------------------------------------------------------------------------
+// Form plugin interface (Dynamics/Forms/Form.h:8-21) on one CTA.
+// ---------------------------------------------------------------------------
+// bit masks of the forms folded into one evaluation
+enum { FM_INERTIA = 1, FM_GRAVITY = 2, FM_JOINTS = 4, FM_DRIVES = 8, FM_BARRIER = 16, FM_FRICTION = 32 };
+
+__device__ int form_mask(int form, const Solver& S) {
+    switch (form) {
+        case NXD_FORM_INERTIA: return FM_INERTIA;
+        case NXD_FORM_GRAVITY: return FM_GRAVITY;
+        case NXD_FORM_CONSTRAINT: return FM_JOINTS;
+        case NXD_FORM_BARRIER: return FM_BARRIER;
+        case NXD_FORM_FRICTION: return FM_FRICTION;
+        case NXD_FORM_DRIVES: return FM_DRIVES;
+        default: return 0;
+    }
+}
+
+// what: 0 value, 1 gradient, 2 hessian block list
+__global__ void __launch_bounds__(kSolverThreads) k_form_eval(Solver S, Scalars* sc, int form, int what, const double* x,
+                                                              double* out, int* row_ptr, int* col_idx, double* vals,
+                                                              long long cap, long long* nnzb) {
+    __shared__ int sh_cnt;
+    const int N = S.N;
+    const int C = sc->n_contacts;
+    const double s = sc->dt * sc->dt;
+    if (what == 0 && (form == NXD_FORM_TOTAL || form == NXD_FORM_CONTACT)) {
+        const double v = energy_total(S, x, s, C, form == NXD_FORM_CONTACT);
+        if (threadIdx.x == 0) out[0] = v;
+        return;
+    }
+    eval_poses(S, x);
+    __syncthreads();
+    for (int j = threadIdx.x; j < S.J; j += blockDim.x) joint_eval(S, j, x, what > 0);
+    for (int c = threadIdx.x; c < C; c += blockDim.x) {
+        barrier_eval(S, c, x);
+        friction_eval(S, c, x, what > 0);
+    }
+    for (int d = threadIdx.x; d < S.D; d += blockDim.x) drive_eval(S, d, x, what == 0 ? 0 : (what == 1 ? 1 : 2));
+    __syncthreads();
+    if (what == 0) {
+        double v = 0.0;
+        {
+            int n = 0;
+            if (form == NXD_FORM_INERTIA || form == NXD_FORM_GRAVITY) {
+                n = N;
+                for (int i = threadIdx.x; i < N; i += blockDim.x) {
+                    if (form == NXD_FORM_INERTIA) {
+                        const V3 dp = xs3(x, 6 * i) - xs3(S.xhat, 6 * i);
+                        const double et = 0.5 * S.mass[i] * sqnorm(dp);
+                        const V3 dth = xs3(x, 6 * i + 3) - xs3(S.xhat, 6 * i + 3);
+                        const double* I = S.inertia + 9 * i;
+                        const V3 r = v3(dth.x * I[0] + dth.y * I[3] + dth.z * I[6], dth.x * I[1] + dth.y * I[4] + dth.z * I[7],
+                                        dth.x * I[2] + dth.y * I[5] + dth.z * I[8]);
+                        S.red[i] = et + 0.5 * dot(r, dth);
+                    } else {
+                        S.red[i] = -(S.mass[i] * dot(v3(0.0, -9.81, 0.0), xs3(x, 6 * i)));
+                    }
+                }
+            } else if (form == NXD_FORM_CONSTRAINT) {
+                n = S.J;
+                for (int j = threadIdx.x; j < S.J; j += blockDim.x) S.red[j] = S.jE[j];
+            } else if (form == NXD_FORM_BARRIER) {
+                n = C;
+                for (int c = threadIdx.x; c < C; c += blockDim.x) S.red[c] = S.bE[c];
+            } else if (form == NXD_FORM_FRICTION) {
+                n = C;
+                for (int c = threadIdx.x; c < C; c += blockDim.x) S.red[c] = S.fE[c];
+            } else if (form == NXD_FORM_DRIVES) {
+                n = S.D;
+                for (int d = threadIdx.x; d < S.D; d += blockDim.x) S.red[d] = S.dE[d];
+            }
+            __syncthreads();
+            v = block_tree_sum(S.red, n);
+        }
+        if (threadIdx.x == 0) out[0] = v;
+        return;
+    }
+    // contact incidence
+    for (int i = threadIdx.x; i <= N; i += blockDim.x) S.cinc_cnt[i] = 0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < 2 * C; e += blockDim.x) {
+        const ContactRec& cr = S.contacts[e >> 1];
+        atomicAdd(&S.cinc_cnt[(e & 1) ? cr.body_b : cr.body_a], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int i = 0; i < N; ++i) { S.cinc_off[i] = acc; acc += S.cinc_cnt[i]; }
+        S.cinc_off[N] = acc;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i <= N; i += blockDim.x) S.cinc_cnt[i] = S.cinc_off[i];
+    __syncthreads();
+    warp_stable_place(2 * C, [&](int e) { const ContactRec& cr = S.contacts[e >> 1]; return (e & 1) ? cr.body_b : cr.body_a; },
+                      S.cinc_cnt, S.cinc);
+    __syncthreads();
+    if (what == 1) {
+        if (form == NXD_FORM_TOTAL || form == NXD_FORM_CONTACT) {
+            gather_gradient(S, x, s, C);
+            __syncthreads();
+            const double* src = form == NXD_FORM_TOTAL ? S.g : S.cg;
+            for (int k = threadIdx.x; k < 6 * N; k += blockDim.x) out[k] = src[k];
+            return;
+        }
+        const int m = form_mask(form, S);
+        const double dh = sc->bdhat;
+        const int nnf = sc->nnf;
+        for (int i = threadIdx.x; i < N; i += blockDim.x) {
+            double g[6] = {0, 0, 0, 0, 0, 0};
+            if (m & FM_INERTIA) {
+                const V3 gp = S.mass[i] * (xs3(x, 6 * i) - xs3(S.xhat, 6 * i));
+                const V3 gr = mat_vec(S.inertia + 9 * i, xs3(x, 6 * i + 3) - xs3(S.xhat, 6 * i + 3));
+                g[0] = gp.x; g[1] = gp.y; g[2] = gp.z; g[3] = gr.x; g[4] = gr.y; g[5] = gr.z;
+            }
+            if (m & FM_GRAVITY) {
+                const V3 f = -S.mass[i] * v3(0.0, -9.81, 0.0);
+                g[0] = f.x; g[1] = f.y; g[2] = f.z;
+            }
+            if (m & FM_JOINTS)
+                for (int q = S.jinc_off[i]; q < S.jinc_off[i + 1]; ++q) {
+                    const int j = S.jinc[q] >> 1, side = S.jinc[q] & 1;
+                    const int dim = joint_dim(S.jtype[j]);
+                    for (int k = 0; k < 6; ++k) {
+                        double a = 0.0;
+                        for (int r = 0; r < dim; ++r) a += S.jJ[72 * j + 12 * r + 6 * side + k] * S.jF[6 * j + r];
+                        g[k] += a;
+                    }
+                }
+            if (m & FM_DRIVES)
+                for (int q = S.dinc_off[i]; q < S.dinc_off[i + 1]; ++q) {
+                    const int d = S.dinc[q] >> 1, side = S.dinc[q] & 1;
+                    const Drv& p = S.dprm[d];
+                    const double ax[3] = {p.ax, p.ay, p.az};
+                    for (int k = 0; k < 3; ++k) {
+                        if (side == 1) g[3 + k] += S.dG[d] * ax[k];
+                        else g[3 + k] -= S.dG[d] * ax[k];
+                    }
+                }
+            for (int q = S.cinc_off[i]; q < S.cinc_off[i + 1]; ++q) {
+                const int c = S.cinc[q] >> 1, side = S.cinc[q] & 1;
+                if ((m & FM_BARRIER) && S.bD[c] < dh) {
+                    const V3 n = ld3(S.contacts[c].normal);
+                    const V3 contrib = side == 0 ? (-S.bGP[c]) * n : S.bGP[c] * n;
+                    g[0] += contrib.x; g[1] += contrib.y; g[2] += contrib.z;
+                }
+                if ((m & FM_FRICTION) && c < nnf && S.nforce[c] > 0) {
+                    const double* Jx = (side == 0 ? S.fJA : S.fJB) + 18 * c;
+                    const V3 fg = ld3(S.fFG + 3 * c);
+                    for (int k = 0; k < 6; ++k) g[k] += Jx[k] * fg.x + Jx[6 + k] * fg.y + Jx[12 + k] * fg.z;
+                }
+            }
+            for (int k = 0; k < 6; ++k) out[6 * i + k] = g[k];
+        }
+        return;
+    }
+    // Hessian block list: row i holds its summed diagonal block, then one block
+    // per coupling item incident to i (item order); like Eigen's
+    // setFromTriplets the consumer sums duplicates.
+    gather_diag_hessian(S, s, C);
+    __syncthreads();
+    const bool total = form == NXD_FORM_TOTAL;
+    if (!total) {
+        if (threadIdx.x == 0) *nnzb = -1;   // only the total Hessian is exported
+        return;
+    }
+    const int n_items = S.J + 2 * C;
+    for (int i = threadIdx.x; i <= N; i += blockDim.x) S.cinc_cnt[i] = 0;
+    __syncthreads();
+    for (int it = threadIdx.x; it < n_items; it += blockDim.x) {
+        if (!item_active(S, it)) continue;
+        int a, b;
+        item_bodies(S, it, a, b);
+        if (a == b) continue;
+        atomicAdd(&S.cinc_cnt[a], 1);
+        atomicAdd(&S.cinc_cnt[b], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int i = 0; i < N; ++i) { row_ptr[i] = acc; acc += 1 + S.cinc_cnt[i]; }
+        row_ptr[N] = acc;
+        *nnzb = acc;
+        sh_cnt = acc;
+    }
+    __syncthreads();
+    if (sh_cnt > cap) return;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        int pos = row_ptr[i];
+        col_idx[pos] = i;
+        for (int k = 0; k < 36; ++k) vals[36LL * pos + k] = S.Hd[36 * i + k];
+        ++pos;
+        for (int it = 0; it < n_items; ++it) {
+            if (!item_active(S, it)) continue;
+            int a, b;
+            item_bodies(S, it, a, b);
+            if (a == b || (a != i && b != i)) continue;
+            const int other = a == i ? b : a;
+            double blk[36];
+            for (int k = 0; k < 36; ++k) blk[k] = 0.0;
+            add_coupling_block(S, it, i, other, s, blk);
+            col_idx[pos] = other;
+            for (int k = 0; k < 36; ++k) vals[36LL * pos + k] = blk[k];
+            ++pos;
+        }
+    }
+}
+
+// DistanceBarrierForm::computeNormalForces at x for the installed contacts
+__global__ void k_normal_forces(Solver S, Scalars* sc, const double* x, double* out, int n) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= min(n, sc->n_contacts)) return;
+    const double d = contact_distance(S.contacts[c], x);
+    out[c] = (d < sc->bdhat && d > 0.0) ? fabs(barrier_gradient(d, sc->bdhat, sc->bkappa)) : 0.0;
+}
+
+// install form state (contacts are copied by the host)
+__global__ void k_set_form_state(StepCfg cfg, Scalars* sc, int n, int nnf, double dt, const double* pos, const double* quat,
+                                 double* pos0, double* quat0, int* dhas_prev) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < cfg.N) {
+        for (int k = 0; k < 3; ++k) pos0[3 * i + k] = pos[3 * i + k];
+        for (int k = 0; k < 4; ++k) quat0[4 * i + k] = quat[4 * i + k];
+    }
+    if (i < cfg.D) dhas_prev[i] = 0;
+    if (i == 0) {
+        sc->n_contacts = n;
+        sc->nnf = nnf;
+        sc->dt = dt;
+        sc->bdhat = dmax(1e-9, sc->dhat);
+        sc->bkappa = dmax(0.0, sc->kappa);
+        sc->barrier_form = 1;
+        sc->barrier_in_forms = cfg.enable_adaptive ? 1 : 0;
+        sc->friction_form = (cfg.enable_friction && cfg.friction_coeff > 0.0) ? 1 : 0;
+    }
+}
+
+}  // namespace nx

@@ -50,6 +50,22 @@ def lib():
     L.nxd_detect_contacts.argtypes = [vp, dp, C.c_void_p, C.c_int32, ip]
     L.nxd_scene_min_distance.argtypes = [vp, dp]
     L.nxd_max_step.argtypes = [vp, C.c_double, dp]
+    L.nxd_set_form_state.argtypes = [vp, C.c_void_p, C.c_int32, dp, dp, C.c_double]
+    L.nxd_form_value.argtypes = [vp, C.c_int32, dp, dp]
+    L.nxd_form_gradient.argtypes = [vp, C.c_int32, dp, dp]
+    L.nxd_form_hessian_bsr.argtypes = [vp, C.c_int32, dp, ip, ip, dp, C.c_int64, i64p]
+    L.nxd_normal_forces.argtypes = [vp, dp, dp, C.c_int32]
+    L.nxd_batch_create.argtypes = [C.POINTER(abi.NxdSceneDesc), C.c_int32, C.POINTER(vp)]
+    L.nxd_batch_destroy.argtypes = [vp]
+    L.nxd_batch_step.argtypes = [vp, dp]
+    L.nxd_batch_get_state.argtypes = [vp, C.c_int32, C.POINTER(abi.NxdState)]
+    L.nxd_batch_get_diagnostics.argtypes = [vp, C.c_int32, C.POINTER(abi.NxdDiagnostics)]
+    L.nxd_profile.argtypes = [vp, C.c_int32, dp, i64p]
+    L.nxd_profile.restype = C.c_int
+    for name in ("nxd_set_form_state", "nxd_form_value", "nxd_form_gradient", "nxd_form_hessian_bsr",
+                 "nxd_normal_forces", "nxd_batch_create", "nxd_batch_step", "nxd_batch_get_state",
+                 "nxd_batch_get_diagnostics"):
+        getattr(L, name).restype = C.c_int
     for name in ("nxd_create", "nxd_set_stream", "nxd_step", "nxd_get_state", "nxd_set_state", "nxd_get_diagnostics",
                  "nxd_get_joint_state", "nxd_body_pairs", "nxd_build_candidates", "nxd_detect_contacts",
                  "nxd_scene_min_distance", "nxd_max_step"):
@@ -132,6 +148,20 @@ class Context:
         _check("nxd_build_candidates", lib().nxd_build_candidates(self.h, act, C.byref(c)))
         return {k: bufs[k][:counts[k]] for k in bufs}
 
+    def candidate_counts(self, act: float):
+        """(face-vertex, edge-edge) candidate counts at the current poses."""
+        c = abi.NxdCandidates()
+        _check("nxd_build_candidates", lib().nxd_build_candidates(self.h, act, C.byref(c)))
+        return int(c.fv_count), int(c.ee_count)
+
+    def profile(self, enable: bool):
+        """Per-family device milliseconds and launch counts since the last call."""
+        ms = np.zeros(9)
+        n = np.zeros(9, dtype=np.int64)
+        _check("nxd_profile", lib().nxd_profile(self.h, int(enable), abi.dptr(ms),
+                                                n.ctypes.data_as(C.POINTER(C.c_int64))))
+        return ms, n
+
     def detect_contacts(self, x=None) -> np.ndarray:
         cap = 40000
         out = np.zeros(cap, dtype=abi.CONTACT_DTYPE)
@@ -150,6 +180,97 @@ class Context:
         v = C.c_double(0)
         _check("nxd_max_step", lib().nxd_max_step(self.h, dt, C.byref(v)))
         return v.value
+
+
+    # Form plugin interface (Dynamics/Forms/Form.h:8-21)
+    def set_form_state(self, contacts, normal_forces=None, x_hat=None, dt=None):
+        contacts = np.ascontiguousarray(contacts, dtype=abi.CONTACT_DTYPE)
+        self._fs = (contacts, None if normal_forces is None else np.ascontiguousarray(normal_forces, np.float64),
+                    None if x_hat is None else np.ascontiguousarray(x_hat, np.float64))
+        nf = abi.dptr(self._fs[1]) if normal_forces is not None else None
+        xh = abi.dptr(self._fs[2]) if x_hat is not None else None
+        _check("nxd_set_form_state", lib().nxd_set_form_state(self.h, contacts.ctypes.data_as(C.c_void_p), len(contacts),
+                                                              nf, xh, float(self.scene.dt if dt is None else dt)))
+
+    def form_value(self, form: int, x) -> float:
+        v = C.c_double(0)
+        _check("nxd_form_value", lib().nxd_form_value(self.h, form, abi.dptr(np.ascontiguousarray(x, np.float64)),
+                                                      C.byref(v)))
+        return v.value
+
+    def form_gradient(self, form: int, x) -> np.ndarray:
+        g = np.zeros(6 * self.n)
+        _check("nxd_form_gradient", lib().nxd_form_gradient(self.h, form, abi.dptr(np.ascontiguousarray(x, np.float64)),
+                                                            abi.dptr(g)))
+        return g
+
+    def form_hessian_bsr(self, x):
+        xx = np.ascontiguousarray(x, np.float64)
+        nnzb = C.c_int64(0)
+        rp = np.zeros(self.n + 1, np.int32)
+        st = lib().nxd_form_hessian_bsr(self.h, abi.NXD_FORM_TOTAL, abi.dptr(xx), abi.iptr(rp), None, None, 0,
+                                        C.byref(nnzb))
+        cap = nnzb.value
+        ci = np.zeros(max(cap, 1), np.int32)
+        vals = np.zeros((max(cap, 1), 6, 6))
+        _check("nxd_form_hessian_bsr", lib().nxd_form_hessian_bsr(self.h, abi.NXD_FORM_TOTAL, abi.dptr(xx), abi.iptr(rp),
+                                                                  abi.iptr(ci), abi.dptr(vals), cap, C.byref(nnzb)))
+        return rp, ci[:cap], vals[:cap]
+
+    def form_hessian_dense(self, x) -> np.ndarray:
+        rp, ci, vals = self.form_hessian_bsr(x)
+        H = np.zeros((6 * self.n, 6 * self.n))
+        for i in range(self.n):
+            for q in range(rp[i], rp[i + 1]):
+                j = ci[q]
+                H[6 * i:6 * i + 6, 6 * j:6 * j + 6] += vals[q]
+        return H
+
+    def normal_forces(self, x, n: int) -> np.ndarray:
+        out = np.zeros(max(n, 1))
+        _check("nxd_normal_forces", lib().nxd_normal_forces(self.h, abi.dptr(np.ascontiguousarray(x, np.float64)),
+                                                            abi.dptr(out), n))
+        return out[:n]
+
+
+class Batch:
+    """Independent scenes stepped together (nxd_batch_*)."""
+
+    def __init__(self, scene_list):
+        self.scenes = list(scene_list)
+        self._descs = (abi.NxdSceneDesc * len(self.scenes))()
+        for i, s in enumerate(self.scenes):
+            self._descs[i] = s.desc()
+        h = C.c_void_p()
+        _check("nxd_batch_create", lib().nxd_batch_create(self._descs, len(self.scenes), C.byref(h)))
+        self.h = h
+        self.dts = np.array([s.dt for s in self.scenes], dtype=np.float64)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().nxd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n: int = 1):
+        for _ in range(n):
+            _check("nxd_batch_step", lib().nxd_batch_step(self.h, abi.dptr(self.dts)))
+
+    def state(self, i: int) -> dict:
+        sb = abi.StateBuffers(self.scenes[i].n_bodies)
+        v = sb.view()
+        _check("nxd_batch_get_state", lib().nxd_batch_get_state(self.h, i, C.byref(v)))
+        return sb.as_dict()
+
+    def diagnostics(self, i: int) -> dict:
+        d = abi.NxdDiagnostics()
+        _check("nxd_batch_get_diagnostics", lib().nxd_batch_get_diagnostics(self.h, i, C.byref(d)))
+        return d.as_dict()
 
 
 class World:
