@@ -8,11 +8,14 @@
 //   AngleAxis(angle, axis) -> (cos(angle/2), sin(angle/2) axis)
 //   Quaternion -> AngleAxis: angle = 2 atan2(|vec|, |w|), axis = vec / (+-|vec|)
 // Every kernel is compiled with --fmad=false, so each product and sum is
-// separately rounded, as on the host side.
+// separately rounded, as on the host side; sin, cos, atan2 and log come from
+// nx_libm.h, the same code the CPU oracle uses.
 #pragma once
 
 #include <cmath>
 #include <cstdint>
+
+#include "nx_libm.h"
 
 #ifdef __CUDACC__
 #define NX_HD __host__ __device__ __forceinline__
@@ -72,13 +75,14 @@ NX_HD Q qnormalized(Q q) {
 }
 NX_HD Q q_from_angle_axis(double angle, V3 axis) {
     const double ha = 0.5 * angle;
-    const double s = sin(ha);
-    return q4(cos(ha), s * axis.x, s * axis.y, s * axis.z);
+    double s, c;
+    nxm::sincos(ha, &s, &c);
+    return q4(c, s * axis.x, s * axis.y, s * axis.z);
 }
 NX_HD void q_to_angle_axis(Q q, double& angle, V3& axis) {
     double n = norm(qvec(q));
     if (n != 0.0) {
-        angle = 2.0 * atan2(n, fabs(q.w));
+        angle = 2.0 * nxm::atan2(n, fabs(q.w));
         if (q.w < 0.0) n = -n;
         axis = qvec(q) / n;
     } else {
@@ -173,20 +177,20 @@ NX_HD double barrier_value(double d, double dh, double k) {
     if (d >= dh) return 0.0;
     if (d <= 0.0) return INFINITY;
     const double r = d / dh;
-    return -k * (d - dh) * (d - dh) * log(r);
+    return -k * (d - dh) * (d - dh) * nxm::log(r);
 }
 NX_HD double barrier_gradient(double d, double dh, double k) {
     if (d >= dh) return 0.0;
     if (d <= 0.0) return -INFINITY;
     const double diff = d - dh;
-    const double lr = log(d / dh);
+    const double lr = nxm::log(d / dh);
     return -k * (2 * diff * lr + diff * diff / d);
 }
 NX_HD double barrier_hessian(double d, double dh, double k) {
     if (d >= dh) return 0.0;
     if (d <= 0.0) return INFINITY;
     const double diff = d - dh;
-    const double lr = log(d / dh);
+    const double lr = nxm::log(d / dh);
     return -k * (2 * lr + 4 * diff / d - (diff * diff) / (d * d));
 }
 

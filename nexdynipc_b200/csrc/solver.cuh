@@ -318,7 +318,7 @@ __device__ double drive_sat(const Drv& p, double e) {
     const double raw = p.kv * e;
     if (!isfinite(p.maxT)) return raw;
     if (p.maxT <= 0.0) return raw;
-    return p.maxT * tanh(raw / p.maxT);
+    return p.maxT * nxm::tanh(raw / p.maxT);
 }
 __device__ double drive_velocity(const Solver& S, int d, const double* x) {
     const int A = S.da[d], B = S.db[d];
@@ -348,7 +348,7 @@ __device__ void drive_eval(const Solver& S, int d, const double* x, int mode) {
         double val;
         if (!isfinite(p.maxT)) val = 0.5 * p.kv * e * e;
         else if (p.kv <= 0.0 || p.maxT <= 0.0) val = 0.0;
-        else { const double s = (p.kv * e) / p.maxT; val = (p.maxT * p.maxT / p.kv) * log(cosh(s)); }
+        else { const double s = (p.kv * e) / p.maxT; val = (p.maxT * p.maxT / p.kv) * nxm::log(nxm::cosh(s)); }
         S.dE[d] = val;
     } else if (mode == 1) {
         const double v = drive_velocity(S, d, x);
@@ -364,7 +364,7 @@ __device__ void drive_eval(const Solver& S, int d, const double* x, int mode) {
             else {
                 const double ee = drive_dead(p, e);
                 const double s = (p.kv * ee) / p.maxT;
-                const double th = tanh(s);
+                const double th = nxm::tanh(s);
                 H = (p.kv * (1.0 - th * th)) / (dt * dt);
             }
         }

@@ -19,6 +19,10 @@
 
 #include "refcpu.h"
 
+// Elementary functions: the same portable implementations the device code
+// uses (Cody-Waite reduction + Taylor series), so the two sides round alike.
+#include "../nexdynipc_b200/csrc/nx_libm.h"
+
 #include <algorithm>
 #include <array>
 #include <chrono>
@@ -97,13 +101,14 @@ inline Q qnormalized(Q q) {
 }
 inline Q q_from_angle_axis(double angle, V3 axis) {
     const double ha = 0.5 * angle;
-    const double s = std::sin(ha);
-    return mkq(std::cos(ha), s * axis.x, s * axis.y, s * axis.z);
+    double s, c;
+    nxm::sincos(ha, &s, &c);
+    return mkq(c, s * axis.x, s * axis.y, s * axis.z);
 }
 inline void q_to_angle_axis(Q q, double& angle, V3& axis) {
     double n = norm(qvec(q));
     if (n != 0.0) {
-        angle = 2.0 * std::atan2(n, std::fabs(q.w));
+        angle = 2.0 * nxm::atan2(n, std::fabs(q.w));
         if (q.w < 0.0) n = -n;
         axis = qvec(q) / n;
     } else {
@@ -560,20 +565,20 @@ double barrier_value(double d, double dh, double k) {
     if (d >= dh) return 0.0;
     if (d <= 0.0) return kInf;
     double r = d / dh;
-    return -k * (d - dh) * (d - dh) * std::log(r);
+    return -k * (d - dh) * (d - dh) * nxm::log(r);
 }
 double barrier_gradient(double d, double dh, double k) {
     if (d >= dh) return 0.0;
     if (d <= 0.0) return -kInf;
     double diff = d - dh;
-    double lr = std::log(d / dh);
+    double lr = nxm::log(d / dh);
     return -k * (2 * diff * lr + diff * diff / d);
 }
 double barrier_hessian(double d, double dh, double k) {
     if (d >= dh) return 0.0;
     if (d <= 0.0) return kInf;
     double diff = d - dh;
-    double lr = std::log(d / dh);
+    double lr = nxm::log(d / dh);
     return -k * (2 * lr + 4 * diff / d - (diff * diff) / (d * d));
 }
 
@@ -1207,7 +1212,7 @@ double drive_sat_torque(const Drive& d, double e) {
     const double raw = d.kv * e;
     if (!std::isfinite(d.max_torque)) return raw;
     if (d.max_torque <= 0.0) return raw;
-    return d.max_torque * std::tanh(raw / d.max_torque);
+    return d.max_torque * nxm::tanh(raw / d.max_torque);
 }
 V3 drive_theta(const std::vector<double>& x, int g) {
     if (g < 0 || g + 5 >= (int)x.size()) return mk(0, 0, 0);
@@ -1230,7 +1235,7 @@ double drive_value(Drive& d, const std::vector<double>& x) {
     if (!std::isfinite(d.max_torque)) return 0.5 * d.kv * e * e;
     if (d.kv <= 0.0 || d.max_torque <= 0.0) return 0.0;
     const double s = (d.kv * e) / d.max_torque;
-    return (d.max_torque * d.max_torque / d.kv) * std::log(std::cosh(s));
+    return (d.max_torque * d.max_torque / d.kv) * nxm::log(nxm::cosh(s));
 }
 void drive_gradient(Drive& d, const std::vector<double>& x, std::vector<double>& g) {
     const double v = drive_joint_velocity(d, x);
@@ -1252,7 +1257,7 @@ void drive_hessian(Drive& d, const std::vector<double>& x, std::vector<Trip>& t)
         else {
             const double ee = drive_deadzone(d, e);
             const double s = (d.kv * ee) / d.max_torque;
-            const double th = std::tanh(s);
+            const double th = nxm::tanh(s);
             H = (d.kv * (1.0 - th * th)) / (d.dt * d.dt);
         }
     }
@@ -2277,6 +2282,20 @@ int nxo_ldlt_solve(const double* H, int32_t n, const double* b, double* x) {
     if (!solve_system(n, t, rhs, sol)) return NXD_FACTOR_FAILED;
     std::copy(sol.begin(), sol.end(), x);
     return NXD_OK;
+}
+
+void nxo_libm(int32_t fn, const double* x, const double* y, double* out, int32_t n) {
+    for (int i = 0; i < n; ++i) {
+        switch (fn) {
+            case 0: out[i] = nxm::sin(x[i]); break;
+            case 1: out[i] = nxm::cos(x[i]); break;
+            case 2: out[i] = nxm::atan2(x[i], y[i]); break;
+            case 3: out[i] = nxm::log(x[i]); break;
+            case 4: out[i] = nxm::exp(x[i]); break;
+            case 5: out[i] = nxm::tanh(x[i]); break;
+            default: out[i] = nxm::cosh(x[i]); break;
+        }
+    }
 }
 
 void nxo_select_top_k(const double* scores, int32_t n, int32_t k, int32_t* out) {

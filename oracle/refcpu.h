@@ -67,6 +67,10 @@ void nxo_select_top_k(const double* scores, int32_t n, int32_t k, int32_t* out_i
 /* std::sort of an index array by score (IPCSolver.cpp:571-577 uses it). */
 void nxo_std_sort(const double* keys, int32_t n, int32_t* idx_inout);
 
+/* The shared elementary functions (nexdynipc_b200/csrc/nx_libm.h):
+ * fn 0 sin, 1 cos, 2 atan2(x, y), 3 log, 4 exp, 5 tanh, 6 cosh. */
+void nxo_libm(int32_t fn, const double* x, const double* y, double* out, int32_t n);
+
 /* Stand-alone pieces used by the ported known-answer tests. */
 double nxo_barrier_value(double d, double dhat, double kappa);
 double nxo_barrier_gradient(double d, double dhat, double kappa);

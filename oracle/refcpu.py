@@ -57,6 +57,7 @@ def lib():
     L.nxo_normal_forces.argtypes = [vp, dp, dp, C.c_int32]
     L.nxo_ldlt_solve.argtypes = [dp, C.c_int32, dp, dp]
     L.nxo_select_top_k.argtypes = [dp, C.c_int32, C.c_int32, ip]
+    L.nxo_libm.argtypes = [C.c_int32, dp, dp, dp, C.c_int32]
     L.nxo_std_sort.argtypes = [dp, C.c_int32, ip]
     for nm in ("nxo_barrier_value", "nxo_barrier_gradient", "nxo_barrier_hessian"):
         getattr(L, nm).restype = C.c_double
@@ -194,6 +195,14 @@ class OracleWorld:
         out = np.zeros(max(n, 1))
         lib().nxo_normal_forces(self.h, _d(x), abi.dptr(out), n)
         return out[:n]
+
+
+def libm(fn: int, x, y=None) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(np.zeros_like(x) if y is None else y, dtype=np.float64)
+    out = np.zeros_like(x)
+    lib().nxo_libm(fn, abi.dptr(x), abi.dptr(y), abi.dptr(out), len(x))
+    return out
 
 
 def select_top_k(scores, k: int) -> np.ndarray:
