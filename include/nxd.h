@@ -291,6 +291,27 @@ nxd_status nxd_batch_step(nxd_batch* b, const double* dts);
 nxd_status nxd_batch_get_state(nxd_batch* b, int32_t scene, const nxd_state* out);
 nxd_status nxd_batch_get_diagnostics(nxd_batch* b, int32_t scene, nxd_diagnostics* out);
 
+/* Body-pair broad phase for callers that cannot allocate device memory.
+ * No counterpart in the reference.  Callers that manage every device byte
+ * themselves (a host engine's memory pool, a hard memory cap, a real-time
+ * loop that forbids allocator calls) pass device buffers they own:
+ * position [n*3], orientation [n*4] (w,x,y,z), local_box [n*6] (local AABB
+ * min xyz, max xyz, i.e. MeshShape::computeAABB) and pairs [cap*2].  The
+ * result equals nxd_body_pairs on the same poses (reference order); *count
+ * (host) gets the pair count, NXD_CAPACITY if it exceeds cap.
+ * The call allocates nothing: its scratch (world boxes, per-body counts and
+ * offsets, about 0.9 MB) is a fixed array in the library that every GPU which
+ * loads it holds until exit, so n is limited to NXD_NOALLOC_MAX_BODIES
+ * (larger n -> NXD_INVALID_ARGUMENT).  The first call on a device looks up
+ * that array's device address; make it before any stream capture.  All calls
+ * share the one array: calls that overlap on the GPU (different streams)
+ * race.  The call synchronises `stream` (a cudaStream_t, may be NULL) before
+ * returning the count. */
+#define NXD_NOALLOC_MAX_BODIES 16384
+nxd_status nxd_body_pairs_noalloc(const double* position, const double* orientation, const double* local_box,
+                                  int32_t n, double inflation_radius, int32_t* pairs, int64_t cap,
+                                  int64_t* count, void* stream);
+
 /* Library version string. */
 const char* nxd_version(void);
 

@@ -12,7 +12,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libnxd_b200.so")
-SRC = os.path.join(HERE, "csrc", "nxd.cu")
+SRCS = [os.path.join(HERE, "csrc", f) for f in ("nxd.cu", "noalloc.cu")]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17", "--fmad=false",
@@ -22,7 +22,7 @@ NVCC_FLAGS = [
 
 def build(verbose: bool = False, extra=()) -> str:
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, *extra, "-o", LIB, SRC]
+    cmd = [nvcc, *NVCC_FLAGS, *extra, "-o", LIB, *SRCS]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)

@@ -60,6 +60,8 @@ def lib():
     L.nxd_batch_step.argtypes = [vp, dp]
     L.nxd_batch_get_state.argtypes = [vp, C.c_int32, C.POINTER(abi.NxdState)]
     L.nxd_batch_get_diagnostics.argtypes = [vp, C.c_int32, C.POINTER(abi.NxdDiagnostics)]
+    L.nxd_body_pairs_noalloc.argtypes = [vp, vp, vp, C.c_int32, C.c_double, vp, C.c_int64, i64p, vp]
+    L.nxd_body_pairs_noalloc.restype = C.c_int
     L.nxd_profile.argtypes = [vp, C.c_int32, dp, i64p]
     L.nxd_profile.restype = C.c_int
     for name in ("nxd_set_form_state", "nxd_form_value", "nxd_form_gradient", "nxd_form_hessian_bsr",
@@ -271,6 +273,17 @@ class Batch:
         d = abi.NxdDiagnostics()
         _check("nxd_batch_get_diagnostics", lib().nxd_batch_get_diagnostics(self.h, i, C.byref(d)))
         return d.as_dict()
+
+
+def body_pairs_noalloc(position_ptr: int, orientation_ptr: int, local_box_ptr: int, n: int, r: float,
+                       pairs_ptr: int, cap: int, stream_ptr: int = 0) -> int:
+    """nxd_body_pairs_noalloc on caller-owned device buffers (raw pointers);
+    returns the pair count."""
+    cnt = C.c_int64(0)
+    _check("nxd_body_pairs_noalloc", lib().nxd_body_pairs_noalloc(
+        C.c_void_p(position_ptr), C.c_void_p(orientation_ptr), C.c_void_p(local_box_ptr), n, r,
+        C.c_void_p(pairs_ptr), cap, C.byref(cnt), C.c_void_p(stream_ptr) if stream_ptr else None))
+    return cnt.value
 
 
 class World:
