@@ -1669,7 +1669,21 @@ bool solve_system(int ndof, const std::vector<Trip>& trips, const std::vector<do
     for (int i = 0; i < nb; ++i) comps[find_root(parent, i)].push_back(i);
     sol.assign(ndof, 0.0);
     for (auto& kv : comps) {
-        const std::vector<int>& members = kv.second;   // ascending
+        // members ordered by (number of distinct coupled bodies, index): leaves
+        // of stars and the ends of chains come first, so they factor without
+        // fill; the device solver uses the same order
+        std::vector<int> members = kv.second;   // ascending
+        if (members.size() > 1) {
+            std::vector<std::pair<int, int>> key;
+            for (int b : members) {
+                int deg = 0;
+                for (int o : members)
+                    if (o != b && (H.blocks.count((long long)b * nb + o) || H.blocks.count((long long)o * nb + b))) ++deg;
+                key.push_back({deg, b});
+            }
+            std::sort(key.begin(), key.end());
+            for (size_t t = 0; t < key.size(); ++t) members[t] = key[t].second;
+        }
         const int m = (int)members.size(), n = 6 * m;
         std::vector<double> A((size_t)n * n, 0.0);
         for (int bi = 0; bi < m; ++bi)
