@@ -50,11 +50,6 @@ struct DevArena {
     }
 };
 
-int pow2_ceil_host(int n) {
-    int p = 1;
-    while (p < n) p <<= 1;
-    return p;
-}
 
 int grid_for(long long n, int block, int max_blocks = 1 << 16) {
     long long g = (n + block - 1) / block;
@@ -146,7 +141,7 @@ void fill_solver(nxd_ctx* c) {
     S.dhas_prev = c->dhas_prev; S.dfilt = c->dfilt; S.dinc_off = c->dinc_off; S.dinc = c->dinc;
     S.contacts = c->contacts; S.ncontacts_ptr = &c->sc->n_contacts;
     S.nforce = c->nforce; S.nnf_ptr = &c->sc->nnf;
-    S.cinc_off = m.alloc<int>(N + 1); S.cinc = m.alloc<int>(2 * C); S.cinc_cnt = m.alloc<int>(N + 1);
+    S.cinc_off = m.alloc<int>(N + 1); S.cinc = m.alloc<int>(2 * C);
     S.dt_ptr = &c->sc->dt; S.bdhat_ptr = &c->sc->bdhat; S.bkappa_ptr = &c->sc->bkappa;
     S.barrier_in_forms_ptr = &c->sc->barrier_in_forms; S.friction_form_ptr = &c->sc->friction_form;
     S.friction_mu = c->s.friction_coeff; S.friction_eps = 1e-8;
@@ -154,9 +149,8 @@ void fill_solver(nxd_ctx* c) {
     S.newton_tol = c->s.newton_tol; S.ls_c1 = c->s.ls_c1; S.ls_rho = c->s.ls_rho;
     S.alm_constraint_tol = c->s.alm_constraint_tol; S.alm_hardening_trigger = c->s.alm_hardening_trigger;
     S.alm_hardening_ratio = c->s.alm_hardening_ratio;
-    const int redn = pow2_ceil_host(std::max({6 * N, J, 2 * C, 1}));
     S.g = m.alloc<double>(6 * N); S.cg = m.alloc<double>(6 * N); S.dx = m.alloc<double>(6 * N);
-    S.xt = m.alloc<double>(6 * N); S.red = m.alloc<double>(redn);
+    S.xt = m.alloc<double>(6 * N);
     S.qj = m.alloc<double>(4 * N); S.qg = m.alloc<double>(4 * N);
     S.jC = m.alloc<double>(6 * J); S.jF = m.alloc<double>(6 * J); S.jJ = m.alloc<double>(72 * J);
     S.jE = m.alloc<double>(J); S.jact = m.alloc<int>(J);
@@ -165,17 +159,18 @@ void fill_solver(nxd_ctx* c) {
     S.fJB = m.alloc<double>(18 * C); S.fE = m.alloc<double>(C);
     S.dE = m.alloc<double>(D); S.dG = m.alloc<double>(D); S.dH = m.alloc<double>(D);
     S.Hd = m.alloc<double>(36 * N);
-    S.parent = m.alloc<int>(N); S.comp = m.alloc<int>(N); S.comp_size = m.alloc<int>(N + 1);
-    S.comp_off = m.alloc<int>(N + 1); S.members = m.alloc<int>(N); S.local = m.alloc<int>(N);
-    S.items = m.alloc<int>(J + 2 * C); S.item_comp_off = m.alloc<int>(N + 1); S.item_list = m.alloc<int>(J + 2 * C);
-    S.n_items_ptr = m.alloc<int>(1); S.deg = m.alloc<int>(N + 1);
-    const long long pool_doubles = std::min<long long>(64LL * 1024 * 1024, std::max<long long>(1 << 20, 36LL * N * 64));
+    S.parent = m.alloc<int>(N + 1); S.comp = m.alloc<int>(N);
+    S.mcnt = m.alloc<int>(N + 1); S.icnt = m.alloc<int>(N + 1); S.rflag = m.alloc<int>(N + 1);
+    S.comp_root = m.alloc<int>(N + 1); S.n_comp = m.alloc<int>(1); S.comp_next = m.alloc<int>(1);
+    S.members = m.alloc<int>(N); S.items = m.alloc<int>(J + 2 * kMaxContacts); S.local = m.alloc<int>(N + 1);
+    // per-component structure masks (3 k ceil(k/32) words + lists) and factors
+    // (36 (k + nnz(L)) + 6k doubles, nnz(L) <= k(k-1)/2): room for the whole
+    // scene as one dense component, the factor pool capped at 768 MB
+    const long long kk = std::min<long long>(N, kMaxComponentBodies);
+    const long long mwords = 3LL * kk * ((kk + 31) / 32) + 16LL * N + 4LL * (J + 2 * kMaxContacts) + 4096;
+    S.mpool = m.alloc<unsigned>(mwords); S.mpool_cap = mwords; S.mpool_off = m.alloc<long long>(1);
+    const long long pool_doubles = std::min<long long>(96LL << 20, 18LL * N * N + 64LL * N + 4096);
     S.pool = m.alloc<double>(pool_doubles); S.pool_cap = pool_doubles; S.pool_off = m.alloc<long long>(1);
-    const long long nzb_bytes = std::max<long long>(1 << 20, (long long)N * 64);
-    S.nzb = m.alloc<unsigned char>(nzb_bytes); S.nzb_cap = nzb_bytes; S.nzb_off = m.alloc<long long>(1);
-    c->cand_stride = 6 * kMaxComponentBodies + 2 * kMaxComponentBodies;
-    S.cand = m.alloc<int>((size_t)c->cand_stride * (kSolverThreads / 32)); S.cand_stride = c->cand_stride;
-    S.dvec = m.alloc<double>(12 * N);
     S.alm_done = &c->sc->alm_done; S.status = &c->sc->status; S.newton_iters = &c->sc->newton_iters;
     S.converged = &c->sc->converged; S.ls_fail = &c->sc->ls_fail;
     S.alm_mcv = m.alloc<double>(1); S.alm_dual = m.alloc<double>(1);
@@ -285,7 +280,7 @@ nxd_status enqueue_step(nxd_ctx* c, double dt) {
     launch_candidates(c, &c->sc->dhat, 0.0);
     // adaptive barrier (IPCSolver.cpp:817-832)
     if (c->s.enable_adaptive_barrier) {
-        NXD_LAUNCH(c, NXD_PROF_OTHER, k_barrier_init<<<1, 1024, 0, st>>>(cfg, c->mass, c->pos, c->sc, c->S.red););
+        NXD_LAUNCH(c, NXD_PROF_OTHER, k_barrier_init<<<1, kSolverThreads, 0, st>>>(cfg, c->mass, c->pos, c->sc););
         NXD_LAUNCH(c, NXD_PROF_OTHER, k_init_scalar_d<<<1, 1, 0, st>>>(&c->sc->bmd, INFINITY););
         PairQuery qb{0, &c->sc->dhat, 0.0, 2.0, 0.0};
         NXD_LAUNCH(c, NXD_PROF_BROAD, k_min_pair_distance<<<grid_for((long long)c->N * 32, 256), 256, 0, st>>>(c->geo, qb, c->boxes, &c->sc->bmd););

@@ -13,9 +13,10 @@
 //  * reductions over bodies / joints / contacts / DOFs use one fixed pairwise
 //    tree (pad to a power of two, v[i] += v[i+h], h = P/2 .. 1);
 //  * the linear solve is an LDL^T per connected block component, members
-//    ordered by (distinct coupled neighbours, body index), right-looking
-//    updates A_ic -= (L_ij L_cj) d_j in ascending j, forward substitution in
-//    ascending and backward substitution in descending column order.
+//    ordered by (distinct coupled neighbours, body index); every entry of L
+//    takes its updates (L_ik L_jk) d_k in ascending k over the structurally
+//    nonzero k (left-looking), forward substitution subtracts in ascending and
+//    backward substitution in descending column order.
 #pragma once
 
 #include "nx_math.cuh"
@@ -23,8 +24,22 @@
 
 namespace nx {
 
+// Optional per-phase cycle counters of k_newton (build with -DNXD_PHASE_TIMERS;
+// thread 0 prints one line per launch).  Off in the product build.
+#ifdef NXD_PHASE_TIMERS
+__shared__ long long nx_ph_acc[8];
+__shared__ long long nx_ph_last;
+#define NX_PHASE_START() do { if (threadIdx.x == 0) { for (int q_ = 0; q_ < 8; ++q_) nx_ph_acc[q_] = 0; nx_ph_last = clock64(); } } while (0)
+#define NX_PHASE(k) do { if (threadIdx.x == 0) { const long long t_ = clock64(); nx_ph_acc[k] += t_ - nx_ph_last; nx_ph_last = t_; } } while (0)
+#else
+#define NX_PHASE_START() do {} while (0)
+#define NX_PHASE(k) do {} while (0)
+#endif
+
 constexpr int kSolverThreads = 1024;
-constexpr int kMaxComponentBodies = 256;
+constexpr int kMaxComponentBodies = 2048;   // structure masks of <= 64 words per row
+constexpr int kMaxIncidence = 4096;          // 2 x kMaxContacts contact ends, sorted in shared memory
+static_assert(2 * kMaxContacts <= kMaxIncidence, "contact incidence sort buffer too small");
 
 struct Drv {   // velocity drive parameters (VelocityDriveForm)
     double ax, ay, az, kv, vt, maxT, delay, tau;
@@ -47,7 +62,7 @@ struct Solver {
     // contacts
     const ContactRec* contacts; const int* ncontacts_ptr;
     const double* nforce; const int* nnf_ptr;
-    int* cinc_off; int* cinc; int* cinc_cnt;      // built per ALM iteration
+    int* cinc_off; int* cinc;                     // body -> contact*2+side, ascending; built per kernel
     // scalars
     const double* dt_ptr; const double* bdhat_ptr; const double* bkappa_ptr;
     const int* barrier_in_forms_ptr; const int* friction_form_ptr;
@@ -56,20 +71,21 @@ struct Solver {
     double newton_tol, ls_c1, ls_rho;
     double alm_constraint_tol, alm_hardening_trigger, alm_hardening_ratio;
     // scratch
-    double* g; double* cg; double* dx; double* xt; double* red;   // red: >= pow2(max(N,J,C, 6N)) doubles
+    double* g; double* cg; double* dx; double* xt;                 // [6N]
     double* qj; double* qg;                                        // [N*4] poses at the evaluation point
-    double* jC; double* jF; double* jJ; double* jE; int* jact;     // joints
+    double* jC; double* jF; double* jJ; double* jE; int* jact;     // joints (jJ: 6 x 12 per joint)
     double* bD; double* bGP; double* bHP; double* bE;               // barrier per contact
     double* fFG; double* fHF; double* fJA; double* fJB; double* fE; // friction per contact
     double* dE; double* dG; double* dH;                            // drives
     double* Hd;                                                    // [N*36] diagonal blocks
-    int* parent; int* comp; int* comp_size; int* comp_off; int* members; int* local;
-    int* items; int* item_comp_off; int* item_list; int* n_items_ptr;
-    int* deg;
-    double* pool; long long pool_cap; long long* pool_off;
-    unsigned char* nzb; long long nzb_cap; long long* nzb_off;
-    int* cand; int cand_stride;
-    double* dvec;                                                  // [12N] per-component rhs and pivots
+    // linear solve
+    int* parent; int* comp;                       // [N] union-find parent, component root per body
+    int* mcnt; int* icnt; int* rflag;             // [N+1] per root: members, coupling items, multi-body flag
+    int* comp_root; int* n_comp; int* comp_next;  // multi-body components by ordinal; work counter
+    int* members; int* items;                     // [N], [J+2C] grouped per component
+    int* local;                                   // [N] body -> member index inside its component
+    unsigned* mpool; long long mpool_cap; long long* mpool_off;   // per-component masks and lists
+    double* pool; long long pool_cap; long long* pool_off;        // per-component L, D and rhs
     // outputs / state
     int* alm_done; int* status; int* newton_iters; int* converged; int* ls_fail;
     double* alm_mcv; double* alm_dual;
@@ -80,79 +96,217 @@ struct Solver {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int pow2_ceil(int n) { int p = 1; while (p < n) p <<= 1; return p; }
 
-// Fixed-tree sum of buf[0..n) (buf capacity >= pow2_ceil(n)); all threads call.
-__device__ double block_tree_sum(double* buf, int n) {
-    const int P = pow2_ceil(max(n, 1));
-    for (int i = n + threadIdx.x; i < P; i += blockDim.x) buf[i] = 0.0;
-    __syncthreads();
-    for (int h = P / 2; h >= 1; h >>= 1) {
-        for (int i = threadIdx.x; i < h; i += blockDim.x) buf[i] = buf[i] + buf[i + h];
-        __syncthreads();
+// Block reductions for 1024-thread CTAs.
+//
+// The fixed tree over n values pads to P = pow2 >= n with zeros and runs
+// v[i] += v[i + h] for h = P/2 .. 1.  Padding further (to P >= 1024) only adds
+// exact zeros at the top levels, so take P >= 1024.  After the levels with
+// h >= 32, v[r] (r < 32) is the same tree over the residue class
+// {r + 32 m}; after the levels with h >= 1024 inside that class, its element
+// m = l + 32 j reduces to the tree over j of v[r + 32 l + 1024 j].  So warp r,
+// lane l folds j (K = P / 1024 values, the stride tree = the contiguous
+// pairwise tree over the bit-reversed index, kept as a stack of partial sums),
+// the lanes finish class r with shuffles (h = 16 .. 1), and the 32 class sums
+// go through shared memory once for the last five levels.  The result is the
+// same double as the plain loop, with one __syncthreads per call.
+constexpr int kRedMaxQ = 6;
+
+template <typename F>
+__device__ __forceinline__ double lane_fold(int n, int base, F f) {
+    const int P = max(pow2_ceil(max(n, 1)), 1024);
+    const int K = P >> 10;
+    if (K == 1) return base < n ? f(base) : 0.0;
+    const int lg = 31 - __clz(K);
+    double stk[24];
+    int top = 0;
+    for (int j = 0; j < K; ++j) {
+        const int e = base + (int)((__brev((unsigned)j) >> (32 - lg)) << 10);
+        double v = e < n ? f(e) : 0.0;
+        for (int c = j + 1; !(c & 1); c >>= 1) v = stk[--top] + v;
+        stk[top++] = v;
     }
-    const double r = buf[0];
-    __syncthreads();
-    return r;
+    return stk[0];
+}
+__device__ __forceinline__ double warp_tree(double v) {
+    for (int h = 16; h >= 1; h >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, h);
+    return __shfl_sync(0xffffffffu, v, 0);
 }
 
-__device__ double block_max(double v, double* sh) {
-    for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        double w = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+// Reduction scratch of one CTA: two alternating buffers of kRedMaxQ x 32
+// class sums, so that a call's writes never meet the previous call's reads.
+struct BlockRed {
+    double* sh;      // 2 * kRedMaxQ * 32 doubles of shared memory
+    int parity;
+    template <int Q, typename F>
+    __device__ void sums(const int (&n)[Q], F f, double (&out)[Q]) {
+        static_assert(Q <= kRedMaxQ, "too many simultaneous reductions");
+        const int r = threadIdx.x >> 5, l = threadIdx.x & 31;
+        double* buf = sh + parity * (kRedMaxQ * 32);
+        parity ^= 1;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const double v = warp_tree(lane_fold(n[q], r + 32 * l, [&](int e) { return f(q, e); }));
+            if (l == 0) buf[q * 32 + r] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < Q; ++q) out[q] = warp_tree(buf[q * 32 + l]);
+    }
+    template <typename F>
+    __device__ double sum(int n, F f) {
+        const int nn[1] = {n};
+        double o[1];
+        sums<1>(nn, [&](int, int e) { return f(e); }, o);
+        return o[0];
+    }
+    __device__ double max(double v) {
+        for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        double* buf = sh + parity * (kRedMaxQ * 32);
+        parity ^= 1;
+        if ((threadIdx.x & 31) == 0) buf[threadIdx.x >> 5] = v;
+        __syncthreads();
+        double w = buf[threadIdx.x & 31];
         for (int o = 16; o > 0; o >>= 1) w = dmax(w, __shfl_xor_sync(0xffffffffu, w, o));
-        if (threadIdx.x == 0) sh[0] = w;
+        return w;
+    }
+};
+#define NX_BLOCK_RED(name)                                   \
+    __shared__ double name##_buf[2 * kRedMaxQ * 32];         \
+    BlockRed name;                                           \
+    name.sh = name##_buf;                                    \
+    name.parity = 0
+
+// Exclusive prefix sums of Q int arrays of length n, in place allowed; a[n]
+// receives the total.  Thread t scans the chunk [t c, t c + c), c = ceil(n /
+// 1024).  sh: 32 Q ints.  The caller synchronises before reading the result.
+template <int Q>
+__device__ void block_scan_excl(int* const (&a)[Q], int n, int* sh) {
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int c = (n + 1023) >> 10;
+    const int b0 = min(n, t * c), b1 = min(n, b0 + c);
+    int v[Q], incl[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        int acc = 0;
+        for (int i = b0; i < b1; ++i) acc += a[q][i];
+        v[q] = acc;
+        int x = acc;
+        for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+        incl[q] = x;
+        if (lane == 31) sh[q * 32 + w] = x;
     }
     __syncthreads();
-    const double r = sh[0];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        int x = sh[q * 32 + lane];
+        for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+        const int wbase = __shfl_sync(0xffffffffu, x, (w + 31) & 31) * (w > 0 ? 1 : 0);
+        const int total = __shfl_sync(0xffffffffu, x, 31);
+        int run = wbase + incl[q] - v[q];
+        for (int i = b0; i < b1; ++i) { const int e = a[q][i]; a[q][i] = run; run += e; }
+        if (t == 0) a[q][n] = total;
+    }
+}
+
+// Ascending bitonic sort of n <= kMaxIncidence 64-bit keys in shared memory.
+__device__ void block_sort_u64(unsigned long long* a, int n) {
+    const int P = pow2_ceil(max(n, 1));
+    for (int i = n + threadIdx.x; i < P; i += blockDim.x) a[i] = ~0ull;
     __syncthreads();
-    return r;
+    for (int k = 2; k <= P; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const unsigned long long x = a[i], y = a[l];
+                    if ((x > y) == ((i & k) == 0)) { a[i] = y; a[l] = x; }
+                }
+            }
+            __syncthreads();
+        }
+}
+
+// Warp-level helpers on global scratch (one warp, all lanes call).
+__device__ void warp_sort_int(int* a, int n, int* buf) {
+    const int lane = threadIdx.x & 31;
+    const int P = pow2_ceil(max(n, 1));
+    for (int i = lane; i < P; i += 32) buf[i] = i < n ? a[i] : 0x7fffffff;
+    __syncwarp();
+    for (int k = 2; k <= P; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < P; i += 32) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const int x = buf[i], y = buf[l];
+                    if ((x > y) == ((i & k) == 0)) { buf[i] = y; buf[l] = x; }
+                }
+            }
+            __syncwarp();
+        }
+    for (int i = lane; i < n; i += 32) a[i] = buf[i];
+    __syncwarp();
+}
+__device__ int warp_scan_excl(int* a, int n) {
+    const int lane = threadIdx.x & 31;
+    int carry = 0;
+    for (int base = 0; base < n; base += 32) {
+        const int i = base + lane;
+        const int v = i < n ? a[i] : 0;
+        int x = v;
+        for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+        if (i < n) a[i] = carry + x - v;
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+    __syncwarp();
+    return carry;
 }
 
 // ---------------------------------------------------------------------------
 // Per-item evaluation
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ V3 xs3(const double* x, int i) { return ld3(x + i); }
+__device__ __forceinline__ int joint_dim(int t) {
+    return t == NXD_JOINT_HINGE || t == NXD_JOINT_FIXED ? 6 : (t == NXD_JOINT_SPHERICAL ? 3 : 2);
+}
 
-// Joint C (and J, f if full).  J is dim x 12: columns 0-5 body A, 6-11 body B.
-__device__ void joint_eval(const Solver& S, int j, const double* x, bool full) {
+// Joint residual C at x; with Jd != null also the Jacobian (6 x 12 row-major:
+// columns 0-5 body A, 6-11 body B; unused rows zero).  Returns the row count.
+__device__ int joint_residual(const Solver& S, int j, const double* x, double* C, double* Jd) {
     const int t = S.jtype[j];
     const int A = S.ja[j], B = S.jb[j];
     const double* P = S.jparams + 16 * j;
-    double C[6] = {0, 0, 0, 0, 0, 0};
-    double Jm[6][12];
-    if (full) for (int r = 0; r < 6; ++r) for (int c = 0; c < 12; ++c) Jm[r][c] = 0.0;
-    int dim = 6;
+    for (int i = 0; i < 6; ++i) C[i] = 0.0;
+    if (Jd) for (int e = 0; e < 72; ++e) Jd[e] = 0.0;
     if (t == NXD_JOINT_HINGE || t == NXD_JOINT_SPHERICAL) {
-        dim = t == NXD_JOINT_HINGE ? 6 : 3;
         const V3 pA = xs3(x, 6 * A), pB = xs3(x, 6 * B);
         const Q qA = ldq(S.qj + 4 * A), qB = ldq(S.qj + 4 * B);
         const V3 rA = qrot(qA, ld3(P)), rB = qrot(qB, ld3(P + 3));
         const V3 v = (pA + rA) - (pB + rB);
         C[0] = v.x; C[1] = v.y; C[2] = v.z;
-        if (full) {
+        if (Jd) {
             // PointPrimitive::addJacobianRows (JointPrimitives.h:58-90)
             const M3 dA = cross_mat(rA), dB = cross_mat(rB);
             for (int i = 0; i < 3; ++i) {
-                Jm[i][i] = 1.0; Jm[i][6 + i] = -1.0;
-                for (int k = 0; k < 3; ++k) { Jm[i][3 + k] = -at(dA, i, k); Jm[i][9 + k] = at(dB, i, k); }
+                Jd[12 * i + i] = 1.0; Jd[12 * i + 6 + i] = -1.0;
+                for (int k = 0; k < 3; ++k) { Jd[12 * i + 3 + k] = -at(dA, i, k); Jd[12 * i + 9 + k] = at(dB, i, k); }
             }
         }
-        if (t == NXD_JOINT_HINGE) {
-            const V3 nA = qrot(qA, ld3(P + 6)), nB = qrot(qB, ld3(P + 9));
-            const V3 c = cross(nA, nB);
-            C[3] = c.x; C[4] = c.y; C[5] = c.z;
-            if (full) {
-                // AxisCrossPrimitive::addJacobianRows (JointPrimitives.h:212-240)
-                const M3 mA = mat_mul(cross_mat(nB), cross_mat(nA));
-                M3 na = cross_mat(nA);
-                for (int k = 0; k < 9; ++k) na.m[k] = -na.m[k];
-                const M3 mB = mat_mul(na, cross_mat(nB));
-                for (int i = 0; i < 3; ++i)
-                    for (int k = 0; k < 3; ++k) { Jm[3 + i][3 + k] = at(mA, i, k); Jm[3 + i][9 + k] = at(mB, i, k); }
-            }
+        if (t == NXD_JOINT_SPHERICAL) return 3;
+        const V3 nA = qrot(qA, ld3(P + 6)), nB = qrot(qB, ld3(P + 9));
+        const V3 c = cross(nA, nB);
+        C[3] = c.x; C[4] = c.y; C[5] = c.z;
+        if (Jd) {
+            // AxisCrossPrimitive::addJacobianRows (JointPrimitives.h:212-240)
+            const M3 mA = mat_mul(cross_mat(nB), cross_mat(nA));
+            M3 na = cross_mat(nA);
+            for (int k = 0; k < 9; ++k) na.m[k] = -na.m[k];
+            const M3 mB = mat_mul(na, cross_mat(nB));
+            for (int i = 0; i < 3; ++i)
+                for (int k = 0; k < 3; ++k) { Jd[12 * (3 + i) + 3 + k] = at(mA, i, k); Jd[12 * (3 + i) + 9 + k] = at(mB, i, k); }
         }
-    } else if (t == NXD_JOINT_FIXED) {
+        return 6;
+    }
+    if (t == NXD_JOINT_FIXED) {
         // FixedJoint::computeC / computeJ (FixedJoint.cpp:23-56)
         const V3 p = xs3(x, 6 * A);
         const V3 d = p - ld3(P);
@@ -163,54 +317,57 @@ __device__ void joint_eval(const Solver& S, int j, const double* x, bool full) {
         const V3 tt = ax * ang;
         const V3 th = xs3(x, 6 * A + 3);
         C[3] = th.x - tt.x; C[4] = th.y - tt.y; C[5] = th.z - tt.z;
-        if (full) for (int i = 0; i < 6; ++i) Jm[i][i] = 1.0;
-    } else {
-        // AngleLimitJoint (AngleLimitJoint.cpp:45-96)
-        dim = 2;
-        const Q qA = ldq(S.qj + 4 * A), qB = ldq(S.qj + 4 * B);
-        const Q qr = qmul(qconj(qA), qB);
-        double ang; V3 ax;
-        q_to_angle_axis(qr, ang, ax);
-        const V3 axis = ld3(P);
-        const double a = ang * dot(ax, axis);
-        C[0] = P[3] - a;
-        C[1] = a - P[4];
-        if (full) {
-            for (int k = 0; k < 3; ++k) {
-                Jm[0][3 + k] = get(axis, k); Jm[1][3 + k] = -get(axis, k);
-                Jm[0][9 + k] = -get(axis, k); Jm[1][9 + k] = get(axis, k);
-            }
-        }
+        if (Jd) for (int i = 0; i < 6; ++i) Jd[12 * i + i] = 1.0;
+        return 6;
     }
+    // AngleLimitJoint (AngleLimitJoint.cpp:45-96)
+    const Q qA = ldq(S.qj + 4 * A), qB = ldq(S.qj + 4 * B);
+    const Q qr = qmul(qconj(qA), qB);
+    double ang; V3 ax;
+    q_to_angle_axis(qr, ang, ax);
+    const V3 axis = ld3(P);
+    const double a = ang * dot(ax, axis);
+    C[0] = P[3] - a;
+    C[1] = a - P[4];
+    if (Jd)
+        for (int k = 0; k < 3; ++k) {
+            Jd[3 + k] = get(axis, k); Jd[12 + 3 + k] = -get(axis, k);
+            Jd[9 + k] = -get(axis, k); Jd[12 + 9 + k] = get(axis, k);
+        }
+    return 2;
+}
+// Joint::value (Joint.cpp:5-18); AngleLimitJoint::value (AngleLimitJoint.cpp:98-109)
+__device__ double joint_energy(const Solver& S, int j, const double* C, int dim) {
     const double mu = S.jmu[j];
     const double* lam = S.jlam + 6 * j;
-    double* Cj = S.jC + 6 * j;
-    for (int i = 0; i < 6; ++i) Cj[i] = C[i];
-    // energy (Joint::value, Joint.cpp:5-18; AngleLimitJoint::value, AngleLimitJoint.cpp:98-109)
-    if (t == NXD_JOINT_ANGLE_LIMIT) {
+    if (S.jtype[j] == NXD_JOINT_ANGLE_LIMIT) {
         double e = 0.0;
         for (int i = 0; i < 2; ++i) { const double gp = dmax(C[i], 0.0); e += lam[i] * gp + 0.5 * mu * gp * gp; }
-        S.jE[j] = e;
-    } else {
-        double t1 = 0.0, sq = 0.0;
-        for (int i = 0; i < dim; ++i) { t1 += lam[i] * C[i]; sq += C[i] * C[i]; }
-        S.jE[j] = t1 + 0.5 * mu * sq;
+        return e;
     }
+    double t1 = 0.0, sq = 0.0;
+    for (int i = 0; i < dim; ++i) { t1 += lam[i] * C[i]; sq += C[i] * C[i]; }
+    return t1 + 0.5 * mu * sq;
+}
+// C, energy and (full) J and f = mu C + lambda into the per-joint arrays
+__device__ void joint_eval(const Solver& S, int j, const double* x, bool full) {
+    double C[6];
+    const int dim = joint_residual(S, j, x, C, full ? S.jJ + 72 * j : nullptr);
+    double* Cj = S.jC + 6 * j;
+    for (int i = 0; i < 6; ++i) Cj[i] = C[i];
+    S.jE[j] = joint_energy(S, j, C, dim);
     if (!full) return;
+    const double mu = S.jmu[j];
+    const double* lam = S.jlam + 6 * j;
     double* F = S.jF + 6 * j;
     for (int i = 0; i < 6; ++i) F[i] = 0.0;
-    if (t == NXD_JOINT_ANGLE_LIMIT) {
+    if (S.jtype[j] == NXD_JOINT_ANGLE_LIMIT) {
         for (int i = 0; i < 2; ++i) F[i] = C[i] > 0.0 ? lam[i] + mu * C[i] : 0.0;
         S.jact[j] = (C[0] > 0.0 ? 1 : 0) | (C[1] > 0.0 ? 2 : 0);
     } else {
         for (int i = 0; i < dim; ++i) F[i] = mu * C[i] + lam[i];
         S.jact[j] = 0;
     }
-    double* Jd = S.jJ + 72 * j;
-    for (int r = 0; r < 6; ++r) for (int c = 0; c < 12; ++c) Jd[12 * r + c] = Jm[r][c];
-}
-__device__ __forceinline__ int joint_dim(int t) {
-    return t == NXD_JOINT_HINGE || t == NXD_JOINT_FIXED ? 6 : (t == NXD_JOINT_SPHERICAL ? 3 : 2);
 }
 __device__ __forceinline__ bool joint_couples(const Solver& S, int j) {
     const int t = S.jtype[j];
@@ -224,7 +381,6 @@ __device__ __forceinline__ double contact_distance(const ContactRec& c, const do
     const V3 pA = xs3(x, 6 * c.body_a), pB = xs3(x, 6 * c.body_b);
     return dmax(1e-9, dot(pB - pA, ld3(c.normal)));
 }
-
 __device__ void barrier_eval(const Solver& S, int c, const double* x) {
     const ContactRec& cr = S.contacts[c];
     const double dh = *S.bdhat_ptr, k = *S.bkappa_ptr;
@@ -264,10 +420,24 @@ __device__ V3 fric_tangent(const Solver& S, const ContactRec& c, const FricGeom&
     const V3 tv = rel - dot(rel, G.n) * G.n;
     return tv * dt;
 }
+__device__ __forceinline__ bool friction_on(const Solver& S, int c) {
+    return c < *S.nnf_ptr && S.nforce[c] > 0;
+}
+// FrictionPotential::value (Friction.cpp:5-20) of contact c at x
+__device__ double friction_value(const Solver& S, int c, const double* x) {
+    if (!friction_on(S, c)) return 0.0;
+    const double N = S.nforce[c];
+    const ContactRec& cr = S.contacts[c];
+    FricGeom G;
+    fric_geom(S, cr, G);
+    const V3 u = fric_tangent(S, cr, G, x, *S.dt_ptr);
+    const double un = norm(u);
+    const double sn = sqrt(un * un + S.friction_eps * S.friction_eps);
+    return S.friction_mu * N * (sn - S.friction_eps);
+}
 __device__ void friction_eval(const Solver& S, int c, const double* x, bool full) {
-    const int nnf = *S.nnf_ptr;
-    const double N = c < nnf ? S.nforce[c] : 0.0;
-    if (!(c < nnf) || N <= 0) { S.fE[c] = 0.0; return; }
+    if (!friction_on(S, c)) { S.fE[c] = 0.0; return; }
+    const double N = S.nforce[c];
     const ContactRec& cr = S.contacts[c];
     const double dt = *S.dt_ptr;
     FricGeom G;
@@ -280,10 +450,10 @@ __device__ void friction_eval(const Solver& S, int c, const double* x, bool full
     S.fE[c] = mu * N * (sn - eps);
     if (!full) return;
     V3 fg = v3(0, 0, 0);
-    double Hf[9];
+    double* Hf = S.fHF + 9 * c;
     if (un < 1e-12) {
-        const double s = mu * N / eps;
-        for (int i = 0; i < 9; ++i) Hf[i] = (i % 4 == 0) ? s : 0.0;
+        const double sc = mu * N / eps;
+        for (int i = 0; i < 9; ++i) Hf[i] = (i % 4 == 0) ? sc : 0.0;
     } else {
         const double sc = mu * N / sn;
         fg = sc * u;
@@ -292,7 +462,6 @@ __device__ void friction_eval(const Solver& S, int c, const double* x, bool full
             for (int j = 0; j < 3; ++j) Hf[3 * i + j] = sc * ((i == j ? 1.0 : 0.0) - get(u, i) * get(u, j) / s2);
     }
     st3(S.fFG + 3 * c, fg);
-    for (int i = 0; i < 9; ++i) S.fHF[9 * c + i] = Hf[i];
     // J_A = [-P, P [rA]x], J_B = [P, -P [rB]x]
     M3 P;
     for (int i = 0; i < 9; ++i) P.m[i] = G.P[i];
@@ -382,250 +551,271 @@ __device__ void eval_poses(const Solver& S, const double* x) {
     }
 }
 
+// InertiaForm::value (InertiaForm.cpp:14-33) and GravityForm::value
+// (GravityForm.cpp:8-16) of body i
+__device__ __forceinline__ double inertia_value(const Solver& S, int i, const double* x) {
+    const V3 dp = xs3(x, 6 * i) - xs3(S.xhat, 6 * i);
+    const double et = 0.5 * S.mass[i] * sqnorm(dp);
+    const V3 dth = xs3(x, 6 * i + 3) - xs3(S.xhat, 6 * i + 3);
+    const double* I = S.inertia + 9 * i;
+    const V3 r = v3(dth.x * I[0] + dth.y * I[3] + dth.z * I[6], dth.x * I[1] + dth.y * I[4] + dth.z * I[7],
+                    dth.x * I[2] + dth.y * I[5] + dth.z * I[8]);
+    return et + 0.5 * dot(r, dth);
+}
+__device__ __forceinline__ double gravity_value(const Solver& S, int i, const double* x) {
+    return -(S.mass[i] * dot(v3(0.0, -9.81, 0.0), xs3(x, 6 * i)));
+}
+
 // ---------------------------------------------------------------------------
-// Energies (computeValue / computeContactValue) at x
+// Energies (computeValue / computeContactValue) at x: every per-item term is
+// evaluated inside the fixed-tree reduction that sums it (no staging arrays).
+// Drives are stateful and evaluated once each before the sums.
 // ---------------------------------------------------------------------------
-__device__ double energy_total(const Solver& S, const double* x, double s, int C, bool contact_only) {
+__device__ double energy_total(const Solver& S, const double* x, double s, int C, bool contact_only, BlockRed& R) {
     eval_poses(S, x);
+    if (!contact_only)
+        for (int d = threadIdx.x; d < S.D; d += blockDim.x) drive_eval(S, d, x, 0);
     __syncthreads();
     const bool bar = *S.barrier_in_forms_ptr != 0, fr = *S.friction_form_ptr != 0;
-    if (!contact_only) {
-        for (int j = threadIdx.x; j < S.J; j += blockDim.x) joint_eval(S, j, x, false);
-        for (int d = threadIdx.x; d < S.D; d += blockDim.x) drive_eval(S, d, x, 0);
-    }
-    for (int c = threadIdx.x; c < C; c += blockDim.x) {
-        if (bar) barrier_eval(S, c, x);
-        if (fr) friction_eval(S, c, x, false);
-    }
-    __syncthreads();
+    const double dh = *S.bdhat_ptr, kap = *S.bkappa_ptr;
+    const int n[5] = {contact_only ? 0 : S.N, contact_only ? 0 : S.N, contact_only ? 0 : S.J, bar ? C : 0, fr ? C : 0};
+    double sum[5];
+    R.sums<5>(n, [&](int q, int e) -> double {
+        switch (q) {
+            case 0: return inertia_value(S, e, x);
+            case 1: return gravity_value(S, e, x);
+            case 2: { double Cj[6]; const int dim = joint_residual(S, e, x, Cj, nullptr); return joint_energy(S, e, Cj, dim); }
+            case 3: return barrier_value(contact_distance(S.contacts[e], x), dh, kap);
+            default: return friction_value(S, e, x);
+        }
+    }, sum);
     double v = 0.0;
     if (!contact_only) {
-        for (int i = threadIdx.x; i < S.N; i += blockDim.x) {
-            const V3 dp = xs3(x, 6 * i) - xs3(S.xhat, 6 * i);
-            const double et = 0.5 * S.mass[i] * sqnorm(dp);
-            const V3 dth = xs3(x, 6 * i + 3) - xs3(S.xhat, 6 * i + 3);
-            const double* I = S.inertia + 9 * i;
-            const V3 r = v3(dth.x * I[0] + dth.y * I[3] + dth.z * I[6], dth.x * I[1] + dth.y * I[4] + dth.z * I[7],
-                            dth.x * I[2] + dth.y * I[5] + dth.z * I[8]);
-            S.red[i] = et + 0.5 * dot(r, dth);
-        }
-        const double inert = block_tree_sum(S.red, S.N);
-        for (int i = threadIdx.x; i < S.N; i += blockDim.x)
-            S.red[i] = -(S.mass[i] * dot(v3(0.0, -9.81, 0.0), xs3(x, 6 * i)));
-        const double grav = block_tree_sum(S.red, S.N);
-        for (int j = threadIdx.x; j < S.J; j += blockDim.x) S.red[j] = S.jE[j];
-        const double cons = block_tree_sum(S.red, S.J);
-        v = inert;
-        v += s * grav;
-        v += cons;
+        v = sum[0];
+        v += s * sum[1];
+        v += sum[2];
         for (int d = 0; d < S.D; ++d) v += s * S.dE[d];
+        if (S.D > 0) __syncthreads();   // dE is rewritten by the next evaluation
     }
-    if (bar) {
-        for (int c = threadIdx.x; c < C; c += blockDim.x) S.red[c] = S.bE[c];
-        v += s * block_tree_sum(S.red, C);
-    }
-    if (fr) {
-        for (int c = threadIdx.x; c < C; c += blockDim.x) S.red[c] = S.fE[c];
-        v += s * block_tree_sum(S.red, C);
-    }
+    if (bar) v += s * sum[3];
+    if (fr) v += s * sum[4];
     return v;
 }
 
 // ---------------------------------------------------------------------------
-// Gradient gather per body (item order), plus the contact-only gradient
+// Gradient per DOF (item order within each entry), plus the contact-only part
 // ---------------------------------------------------------------------------
+__device__ void gradient_dof(const Solver& S, const double* x, double s, int i, int k, bool bar, bool fr, double dh,
+                             double& g_out, double& cg_out) {
+    const double m = S.mass[i];
+    double g;
+    if (k < 3) {
+        g = 0.0 + m * (x[6 * i + k] - S.xhat[6 * i + k]);
+        const double fgv = k == 1 ? (-m) * -9.81 : (-m) * 0.0;
+        g += s * fgv;
+    } else {
+        const double* I = S.inertia + 9 * i + 3 * (k - 3);
+        const double d0 = x[6 * i + 3] - S.xhat[6 * i + 3], d1 = x[6 * i + 4] - S.xhat[6 * i + 4],
+                     d2 = x[6 * i + 5] - S.xhat[6 * i + 5];
+        g = 0.0 + (I[0] * d0 + I[1] * d1 + I[2] * d2);
+        g += s * 0.0;
+    }
+    // ConstraintForm: J^T (mu C + lambda), joints in order
+    double t = 0.0;
+    for (int q = S.jinc_off[i]; q < S.jinc_off[i + 1]; ++q) {
+        const int j = S.jinc[q] >> 1, side = S.jinc[q] & 1;
+        const int dim = joint_dim(S.jtype[j]);
+        const double* Jd = S.jJ + 72 * j + 6 * side + k;
+        const double* F = S.jF + 6 * j;
+        double a = 0.0;
+        for (int r = 0; r < dim; ++r) a += Jd[12 * r] * F[r];
+        t += a;
+    }
+    g += t;
+    // drives, each its own form
+    for (int q = S.dinc_off[i]; q < S.dinc_off[i + 1]; ++q) {
+        if (k < 3) { g += s * 0.0; continue; }
+        const int d = S.dinc[q] >> 1, side = S.dinc[q] & 1;
+        const Drv& p = S.dprm[d];
+        const double c = S.dG[d] * (k == 3 ? p.ax : (k == 4 ? p.ay : p.az));
+        const double tk = side == 1 ? 0.0 + c : 0.0 - c;
+        g += s * tk;
+    }
+    double cb = 0.0, cf = 0.0;
+    if (bar || fr) {
+        for (int q = S.cinc_off[i]; q < S.cinc_off[i + 1]; ++q) {
+            const int c = S.cinc[q] >> 1, side = S.cinc[q] & 1;
+            if (bar && k < 3 && S.bD[c] < dh) {
+                const double gpv = S.bGP[c];
+                const double nk = S.contacts[c].normal[k];
+                cb += side == 0 ? (-gpv) * nk : gpv * nk;
+            }
+            if (fr && friction_on(S, c)) {
+                const double* Jx = (side == 0 ? S.fJA : S.fJB) + 18 * c;
+                const double* fg = S.fFG + 3 * c;
+                cf += Jx[k] * fg[0] + Jx[6 + k] * fg[1] + Jx[12 + k] * fg[2];
+            }
+        }
+    }
+    double cgv = 0.0;
+    if (bar) { g += s * cb; cgv += s * cb; }
+    if (fr) { g += s * cf; cgv += s * cf; }
+    g_out = g;
+    cg_out = cgv;
+}
 __device__ void gather_gradient(const Solver& S, const double* x, double s, int C) {
     const bool bar = *S.barrier_in_forms_ptr != 0, fr = *S.friction_form_ptr != 0;
     const double dh = *S.bdhat_ptr;
-    const int nnf = *S.nnf_ptr;
-    for (int i = threadIdx.x; i < S.N; i += blockDim.x) {
-        double g[6], t[6];
-        const double m = S.mass[i];
-        const V3 gp = m * (xs3(x, 6 * i) - xs3(S.xhat, 6 * i));
-        const V3 gr = mat_vec(S.inertia + 9 * i, xs3(x, 6 * i + 3) - xs3(S.xhat, 6 * i + 3));
-        g[0] = 0.0 + gp.x; g[1] = 0.0 + gp.y; g[2] = 0.0 + gp.z;
-        g[3] = 0.0 + gr.x; g[4] = 0.0 + gr.y; g[5] = 0.0 + gr.z;
-        const V3 fgv = -m * v3(0.0, -9.81, 0.0);
-        g[0] += s * fgv.x; g[1] += s * fgv.y; g[2] += s * fgv.z;
-        g[3] += s * 0.0; g[4] += s * 0.0; g[5] += s * 0.0;
-        // ConstraintForm: J^T (mu C + lambda), joints in order
-        for (int k = 0; k < 6; ++k) t[k] = 0.0;
-        for (int q = S.jinc_off[i]; q < S.jinc_off[i + 1]; ++q) {
-            const int j = S.jinc[q] >> 1, side = S.jinc[q] & 1;
-            const int dim = joint_dim(S.jtype[j]);
-            const double* Jd = S.jJ + 72 * j;
-            const double* F = S.jF + 6 * j;
-            for (int k = 0; k < 6; ++k) {
-                double a = 0.0;
-                for (int r = 0; r < dim; ++r) a += Jd[12 * r + 6 * side + k] * F[r];
-                t[k] += a;
-            }
-        }
-        for (int k = 0; k < 6; ++k) g[k] += t[k];
-        // drives, each its own form
-        for (int q = S.dinc_off[i]; q < S.dinc_off[i + 1]; ++q) {
-            const int d = S.dinc[q] >> 1, side = S.dinc[q] & 1;
-            const Drv& p = S.dprm[d];
-            const double dEdq = S.dG[d];
-            const V3 ax = v3(p.ax, p.ay, p.az);
-            for (int k = 0; k < 3; ++k) {
-                const double c = dEdq * get(ax, k);
-                const double tk = side == 1 ? 0.0 + c : 0.0 - c;
-                g[3 + k] += s * tk;
-            }
-            for (int k = 0; k < 3; ++k) g[k] += s * 0.0;
-        }
-        double cb[6] = {0, 0, 0, 0, 0, 0}, cf[6] = {0, 0, 0, 0, 0, 0};
-        if (bar || fr) {
-            for (int q = S.cinc_off[i]; q < S.cinc_off[i + 1]; ++q) {
-                const int c = S.cinc[q] >> 1, side = S.cinc[q] & 1;
-                const ContactRec& cr = S.contacts[c];
-                if (bar && S.bD[c] < dh) {
-                    const double gpv = S.bGP[c];
-                    const V3 n = ld3(cr.normal);
-                    const V3 contrib = side == 0 ? (-gpv) * n : gpv * n;
-                    cb[0] += contrib.x; cb[1] += contrib.y; cb[2] += contrib.z;
-                }
-                if (fr && c < nnf && S.nforce[c] > 0) {
-                    const double* Jx = (side == 0 ? S.fJA : S.fJB) + 18 * c;
-                    const V3 fg = ld3(S.fFG + 3 * c);
-                    for (int k = 0; k < 6; ++k) cf[k] += Jx[k] * fg.x + Jx[6 + k] * fg.y + Jx[12 + k] * fg.z;
-                }
-            }
-        }
-        double cgv[6];
-        for (int k = 0; k < 6; ++k) cgv[k] = 0.0;
-        if (bar) for (int k = 0; k < 6; ++k) { g[k] += s * cb[k]; cgv[k] += s * cb[k]; }
-        if (fr) for (int k = 0; k < 6; ++k) { g[k] += s * cf[k]; cgv[k] += s * cf[k]; }
-        for (int k = 0; k < 6; ++k) { S.g[6 * i + k] = g[k]; S.cg[6 * i + k] = cgv[k]; }
+    for (int e = threadIdx.x; e < 6 * S.N; e += blockDim.x) {
+        double g, cg;
+        gradient_dof(S, x, s, e / 6, e % 6, bar, fr, dh, g, cg);
+        S.g[e] = g;
+        S.cg[e] = cg;
     }
 }
 
 // ---------------------------------------------------------------------------
-// Hessian: diagonal block per body, coupling blocks per item
+// Hessian: diagonal block per body (one thread per block row), coupling
+// blocks per item
 // ---------------------------------------------------------------------------
-// 6x6 block contribution of a base joint to rows of side ra and cols of side ca
-__device__ void joint_block(const Solver& S, int j, int ra, int ca, double* out) {
+// row a of the 6x6 block mu J_ra^T J_ca of a base joint
+__device__ __forceinline__ void joint_block_row(const Solver& S, int j, int ra, int ca, int a, double* out) {
     const int dim = joint_dim(S.jtype[j]);
     const double* Jd = S.jJ + 72 * j;
     const double mu = S.jmu[j];
-    for (int a = 0; a < 6; ++a)
-        for (int b = 0; b < 6; ++b) {
-            double sacc = 0.0;
-            for (int r = 0; r < dim; ++r) sacc += Jd[12 * r + 6 * ra + a] * Jd[12 * r + 6 * ca + b];
-            out[6 * a + b] = sacc * mu;
-        }
+    for (int b = 0; b < 6; ++b) {
+        double sacc = 0.0;
+        for (int r = 0; r < dim; ++r) sacc += Jd[12 * r + 6 * ra + a] * Jd[12 * r + 6 * ca + b];
+        out[b] = sacc * mu;
+    }
 }
-__device__ void angle_limit_H(const Solver& S, int j, double* H3) {
+__device__ void joint_block(const Solver& S, int j, int ra, int ca, double* out) {
+    for (int a = 0; a < 6; ++a) joint_block_row(S, j, ra, ca, a, out + 6 * a);
+}
+// entry (a, b) of the 3x3 rotational AngleLimit block sum_active mu axis axis^T
+__device__ __forceinline__ double angle_limit_h(const Solver& S, int j, int a, int b) {
     const double* ax = S.jparams + 16 * j;
     const double mu = S.jmu[j];
-    for (int i = 0; i < 9; ++i) H3[i] = 0.0;
+    double h = 0.0;
     for (int rep = 0; rep < 2; ++rep)
-        if (S.jact[j] & (1 << rep))
-            for (int a = 0; a < 3; ++a)
-                for (int b = 0; b < 3; ++b) H3[3 * a + b] += mu * (ax[a] * ax[b]);
+        if (S.jact[j] & (1 << rep)) h += mu * (ax[a] * ax[b]);
+    return h;
 }
-// friction block J_X^T Hf J_Y, evaluated (J_X^T Hf) J_Y
-__device__ void friction_block(const Solver& S, int c, int sx, int sy, double* out) {
+__device__ void angle_limit_H(const Solver& S, int j, double* H3) {
+    for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) H3[3 * a + b] = angle_limit_h(S, j, a, b);
+}
+// row r of the friction block J_X^T Hf J_Y, evaluated (J_X^T Hf) J_Y
+__device__ __forceinline__ void friction_block_row(const Solver& S, int c, int sx, int sy, int r, double* out) {
     const double* Jx = (sx == 0 ? S.fJA : S.fJB) + 18 * c;
     const double* Jy = (sy == 0 ? S.fJA : S.fJB) + 18 * c;
     const double* Hf = S.fHF + 9 * c;
-    for (int r = 0; r < 6; ++r) {
-        const double T0 = Jx[r] * Hf[0] + Jx[6 + r] * Hf[3] + Jx[12 + r] * Hf[6];
-        const double T1 = Jx[r] * Hf[1] + Jx[6 + r] * Hf[4] + Jx[12 + r] * Hf[7];
-        const double T2 = Jx[r] * Hf[2] + Jx[6 + r] * Hf[5] + Jx[12 + r] * Hf[8];
-        for (int cc = 0; cc < 6; ++cc) out[6 * r + cc] = T0 * Jy[cc] + T1 * Jy[6 + cc] + T2 * Jy[12 + cc];
-    }
+    const double T0 = Jx[r] * Hf[0] + Jx[6 + r] * Hf[3] + Jx[12 + r] * Hf[6];
+    const double T1 = Jx[r] * Hf[1] + Jx[6 + r] * Hf[4] + Jx[12 + r] * Hf[7];
+    const double T2 = Jx[r] * Hf[2] + Jx[6 + r] * Hf[5] + Jx[12 + r] * Hf[8];
+    for (int cc = 0; cc < 6; ++cc) out[cc] = T0 * Jy[cc] + T1 * Jy[6 + cc] + T2 * Jy[12 + cc];
+}
+__device__ void friction_block(const Solver& S, int c, int sx, int sy, double* out) {
+    for (int r = 0; r < 6; ++r) friction_block_row(S, c, sx, sy, r, out + 6 * r);
+}
+// drive Hessian entry (ra, ca) of the rotational block (upper entries use
+// (H a_r) a_c with r <= c, the mirrored lower ones repeat them)
+__device__ __forceinline__ double drive_h(const Solver& S, int d, int ra, int ca, double s) {
+    const Drv& p = S.dprm[d];
+    const double ax[3] = {p.ax, p.ay, p.az};
+    const double Hd = S.dH[d];
+    const int lo = min(ra, ca), hi = max(ra, ca);
+    return (Hd * ax[lo] * ax[hi]) * s;
 }
 
+// row a of body i's diagonal block, contributions in item order
+__device__ void diag_hessian_row(const Solver& S, double s, int i, int a, bool bar, bool fr, double dh, double* H) {
+    for (int b = 0; b < 6; ++b) H[b] = 0.0;
+    if (a < 3) H[a] += S.mass[i];
+    else for (int b = 0; b < 3; ++b) H[3 + b] += S.inertia[9 * i + 3 * (a - 3) + b];
+    double blk[6];
+    for (int q = S.jinc_off[i]; q < S.jinc_off[i + 1]; ++q) {
+        const int j = S.jinc[q] >> 1, side = S.jinc[q] & 1;
+        if (S.jtype[j] == NXD_JOINT_ANGLE_LIMIT) {
+            if (!S.jact[j]) continue;
+            if (a >= 3) for (int b = 0; b < 3; ++b) H[3 + b] += angle_limit_h(S, j, a - 3, b);
+        } else {
+            joint_block_row(S, j, side, side, a, blk);
+            for (int b = 0; b < 6; ++b) H[b] += blk[b];
+        }
+    }
+    for (int q = S.dinc_off[i]; q < S.dinc_off[i + 1]; ++q) {
+        const int d = S.dinc[q] >> 1;
+        if (S.dH[d] == 0.0) continue;
+        if (a >= 3) for (int b = 0; b < 3; ++b) H[3 + b] += drive_h(S, d, a - 3, b, s);
+    }
+    if (!(bar || fr)) return;
+    if (bar && a < 3)
+        for (int q = S.cinc_off[i]; q < S.cinc_off[i + 1]; ++q) {
+            const int c = S.cinc[q] >> 1;
+            if (!(S.bD[c] < dh)) continue;
+            const double hp = S.bHP[c];
+            const double* n = S.contacts[c].normal;
+            for (int cc = 0; cc < 3; ++cc) H[cc] += (hp * (n[a] * n[cc])) * s;
+        }
+    if (fr)
+        for (int q = S.cinc_off[i]; q < S.cinc_off[i + 1]; ++q) {
+            const int c = S.cinc[q] >> 1, side = S.cinc[q] & 1;
+            if (!friction_on(S, c)) continue;
+            friction_block_row(S, c, side, side, a, blk);
+            for (int b = 0; b < 6; ++b) H[b] += blk[b] * s;
+        }
+}
 __device__ void gather_diag_hessian(const Solver& S, double s, int C) {
     const bool bar = *S.barrier_in_forms_ptr != 0, fr = *S.friction_form_ptr != 0;
     const double dh = *S.bdhat_ptr;
-    const int nnf = *S.nnf_ptr;
-    for (int i = threadIdx.x; i < S.N; i += blockDim.x) {
-        double H[36];
-        for (int k = 0; k < 36; ++k) H[k] = 0.0;
-        const double m = S.mass[i];
-        H[0] += m; H[7] += m; H[14] += m;
-        for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) H[6 * (3 + a) + 3 + b] += S.inertia[9 * i + 3 * a + b];
-        double blk[36];
-        for (int q = S.jinc_off[i]; q < S.jinc_off[i + 1]; ++q) {
-            const int j = S.jinc[q] >> 1, side = S.jinc[q] & 1;
-            if (S.jtype[j] == NXD_JOINT_ANGLE_LIMIT) {
-                if (!S.jact[j]) continue;
-                double H3[9];
-                angle_limit_H(S, j, H3);
-                for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) H[6 * (3 + a) + 3 + b] += H3[3 * a + b];
-            } else {
-                joint_block(S, j, side, side, blk);
-                for (int k = 0; k < 36; ++k) H[k] += blk[k];
-            }
-        }
-        for (int q = S.dinc_off[i]; q < S.dinc_off[i + 1]; ++q) {
-            const int d = S.dinc[q] >> 1;
-            const double Hd = S.dH[d];
-            if (Hd == 0.0) continue;
-            const Drv& p = S.dprm[d];
-            const double ax[3] = {p.ax, p.ay, p.az};
-            for (int a = 0; a < 3; ++a) H[6 * (3 + a) + 3 + a] += (Hd * ax[a] * ax[a]) * s;
-            for (int a = 0; a < 3; ++a)
-                for (int b = a + 1; b < 3; ++b) {
-                    const double od = Hd * ax[a] * ax[b];
-                    H[6 * (3 + a) + 3 + b] += od * s;
-                    H[6 * (3 + b) + 3 + a] += od * s;
-                }
-        }
-        if (bar || fr) {
-            for (int q = S.cinc_off[i]; q < S.cinc_off[i + 1]; ++q) {
-                const int c = S.cinc[q] >> 1;
-                if (!bar || !(S.bD[c] < dh)) continue;
-                const double hp = S.bHP[c];
-                const V3 n = ld3(S.contacts[c].normal);
-                for (int r = 0; r < 3; ++r)
-                    for (int cc = 0; cc < 3; ++cc) H[6 * r + cc] += (hp * (get(n, r) * get(n, cc))) * s;
-            }
-            for (int q = S.cinc_off[i]; q < S.cinc_off[i + 1]; ++q) {
-                const int c = S.cinc[q] >> 1, side = S.cinc[q] & 1;
-                if (!fr || !(c < nnf && S.nforce[c] > 0)) continue;
-                friction_block(S, c, side, side, blk);
-                for (int k = 0; k < 36; ++k) H[k] += blk[k] * s;
-            }
-        }
-        for (int k = 0; k < 36; ++k) S.Hd[36 * i + k] = H[k];
+    for (int e = threadIdx.x; e < 6 * S.N; e += blockDim.x) {
+        double H[6];
+        diag_hessian_row(S, s, e / 6, e % 6, bar, fr, dh, H);
+        for (int b = 0; b < 6; ++b) S.Hd[6 * e + b] = H[b];
     }
 }
 
-// Coupling block of item `it` with rows of body R and cols of body Cb (R != Cb),
-// added into out (6x6, row-major).  Items: [0,J) joints, [J, J+C) barrier
+// Coupling block entry e (row-major 6x6) of item `it` with rows of body R
+// and cols of body Cb (R != Cb).  Items: [0,J) joints, [J, J+C) barrier
 // contacts, [J+C, J+2C) friction contacts.
-__device__ void add_coupling_block(const Solver& S, int it, int R, int Cb, double s, double* out) {
-    double blk[36];
+__device__ double coupling_entry(const Solver& S, int it, int R, int Cb, double s, int C, int e) {
+    const int ra = e / 6, cb = e % 6;
     if (it < S.J) {
         const int j = it;
-        const int ra = S.ja[j] == R ? 0 : 1, ca = S.ja[j] == Cb ? 0 : 1;
-        if (S.jtype[j] == NXD_JOINT_ANGLE_LIMIT) {
-            double H3[9];
-            angle_limit_H(S, j, H3);
-            for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) out[6 * (3 + a) + 3 + b] += -H3[3 * a + b];
-        } else {
-            joint_block(S, j, ra, ca, blk);
-            for (int k = 0; k < 36; ++k) out[k] += blk[k];
-        }
-        return;
+        if (S.jtype[j] == NXD_JOINT_ANGLE_LIMIT)
+            return (ra >= 3 && cb >= 3) ? -angle_limit_h(S, j, ra - 3, cb - 3) : 0.0;
+        const int sr = S.ja[j] == R ? 0 : 1, sc = S.ja[j] == Cb ? 0 : 1;
+        const int dim = joint_dim(S.jtype[j]);
+        const double* Jd = S.jJ + 72 * j;
+        double acc = 0.0;
+        for (int r = 0; r < dim; ++r) acc += Jd[12 * r + 6 * sr + ra] * Jd[12 * r + 6 * sc + cb];
+        return acc * S.jmu[j];
     }
-    const int C = *S.ncontacts_ptr;
     if (it < S.J + C) {
+        if (ra >= 3 || cb >= 3) return 0.0;
         const int c = it - S.J;
-        const double hp = S.bHP[c];
-        const V3 n = ld3(S.contacts[c].normal);
-        for (int r = 0; r < 3; ++r)
-            for (int cc = 0; cc < 3; ++cc) out[6 * r + cc] += (-(hp * (get(n, r) * get(n, cc)))) * s;
-        return;
+        const double* n = S.contacts[c].normal;
+        return (-(S.bHP[c] * (n[ra] * n[cb]))) * s;
     }
     const int c = it - S.J - C;
     const int sx = S.contacts[c].body_a == R ? 0 : 1, sy = S.contacts[c].body_a == Cb ? 0 : 1;
-    friction_block(S, c, sx, sy, blk);
-    for (int k = 0; k < 36; ++k) out[k] += blk[k] * s;
+    const double* Jx = (sx == 0 ? S.fJA : S.fJB) + 18 * c;
+    const double* Jy = (sy == 0 ? S.fJA : S.fJB) + 18 * c;
+    const double* Hf = S.fHF + 9 * c;
+    const double T0 = Jx[ra] * Hf[0] + Jx[6 + ra] * Hf[3] + Jx[12 + ra] * Hf[6];
+    const double T1 = Jx[ra] * Hf[1] + Jx[6 + ra] * Hf[4] + Jx[12 + ra] * Hf[7];
+    const double T2 = Jx[ra] * Hf[2] + Jx[6 + ra] * Hf[5] + Jx[12 + ra] * Hf[8];
+    return (T0 * Jy[cb] + T1 * Jy[6 + cb] + T2 * Jy[12 + cb]) * s;
+}
+// whole block, added into out (used by the form interface)
+__device__ void add_coupling_block(const Solver& S, int it, int R, int Cb, double s, double* out) {
+    const int C = *S.ncontacts_ptr;
+    for (int e = 0; e < 36; ++e) {
+        const int ra = e / 6, cb = e % 6;
+        const bool touches = it < S.J ? (S.jtype[it] != NXD_JOINT_ANGLE_LIMIT || (ra >= 3 && cb >= 3))
+                                      : (it < S.J + C ? (ra < 3 && cb < 3) : true);
+        if (touches) out[e] += coupling_entry(S, it, R, Cb, s, C, e);
+    }
 }
 __device__ __forceinline__ void item_bodies(const Solver& S, int it, int& a, int& b) {
     if (it < S.J) { a = S.ja[it]; b = S.jb[it]; return; }
@@ -638,7 +828,28 @@ __device__ __forceinline__ bool item_active(const Solver& S, int it) {
     const int C = *S.ncontacts_ptr;
     if (it < S.J + C) return *S.barrier_in_forms_ptr != 0 && S.bD[it - S.J] < *S.bdhat_ptr;
     const int c = it - S.J - C;
-    return *S.friction_form_ptr != 0 && c < *S.nnf_ptr && S.nforce[c] > 0;
+    return *S.friction_form_ptr != 0 && friction_on(S, c);
+}
+
+// ---------------------------------------------------------------------------
+// Contact incidence: body -> (contact * 2 + side), ascending, from one sort of
+// (body, end) keys; cinc_off[b] = first key of body >= b.
+// ---------------------------------------------------------------------------
+__device__ void build_contact_incidence(const Solver& S, int C, unsigned long long* keys) {
+    const int n = 2 * C;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const ContactRec& cr = S.contacts[e >> 1];
+        const int b = (e & 1) ? cr.body_b : cr.body_a;
+        keys[e] = ((unsigned long long)(unsigned)b << 32) | (unsigned)e;
+    }
+    block_sort_u64(keys, n);
+    for (int p = threadIdx.x; p <= n; p += blockDim.x) {
+        const int lo = p == 0 ? -1 : (int)(keys[p - 1] >> 32);
+        const int hi = p == n ? S.N : (int)(keys[p] >> 32);
+        for (int b = lo + 1; b <= hi; ++b) S.cinc_off[b] = p;
+        if (p < n) S.cinc[p] = (int)(keys[p] & 0xffffffffu);
+    }
+    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -665,118 +876,355 @@ __device__ void uf_union(int* par, int a, int b) {
     }
 }
 
-// stable bucket placement, warp 0, entries e in [0, n): key(e) -> out position
-// offs[key] holds the running start per key (already the exclusive scan).
-template <typename KeyFn>
-__device__ void warp_stable_place(int n, KeyFn key, int* offs, int* out) {
-    if (threadIdx.x >= 32) return;
-    const int lane = threadIdx.x;
-    const unsigned lt = (1u << lane) - 1u;
-    for (int base = 0; base < n; base += 32) {
-        const int e = base + lane;
-        const bool valid = e < n;
-        const int k = valid ? key(e) : -1 - lane;
-        const unsigned mask = __match_any_sync(0xffffffffu, k);
-        const int rank = __popc(mask & lt);
-        int start = 0;
-        if (valid) start = offs[k];
-        __syncwarp();
-        if (valid) out[start + rank] = e;
-        const int leader = __ffs(mask) - 1;
-        if (valid && lane == leader) offs[k] = start + __popc(mask);
-        __syncwarp();
-    }
-}
-
-}  // namespace nx
-
-namespace nx {
-
 // LDL^T of one 6x6 block (lower part of H), left-looking exactly as the dense
-// oracle loop; solves rhs in place.  Returns false on a zero pivot.
-__device__ bool ldlt6_solve(double* A, double* b) {
+// oracle loop, solving rhs in place.  Fully unrolled: A stays in registers.
+// Returns false on a zero pivot.
+__device__ __forceinline__ bool ldlt6_solve(double (&A)[36], double (&b)[6]) {
     double d[6];
+#pragma unroll
     for (int j = 0; j < 6; ++j) {
         double dj = A[6 * j + j];
+#pragma unroll
         for (int k = 0; k < j; ++k) { const double l = A[6 * j + k]; dj -= l * l * d[k]; }
         if (dj == 0.0) return false;
         d[j] = dj;
         A[6 * j + j] = dj;
+#pragma unroll
         for (int i = j + 1; i < 6; ++i) {
             double s = A[6 * i + j];
+#pragma unroll
             for (int k = 0; k < j; ++k) s -= A[6 * i + k] * A[6 * j + k] * d[k];
             A[6 * i + j] = s / dj;
         }
     }
-    for (int i = 0; i < 6; ++i) { double s = b[i]; for (int k = 0; k < i; ++k) s -= A[6 * i + k] * b[k]; b[i] = s; }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double s = b[i];
+#pragma unroll
+        for (int k = 0; k < i; ++k) s -= A[6 * i + k] * b[k];
+        b[i] = s;
+    }
+#pragma unroll
     for (int i = 0; i < 6; ++i) b[i] /= A[6 * i + i];
-    for (int i = 5; i >= 0; --i) { double s = b[i]; for (int k = 5; k > i; --k) s -= A[6 * k + i] * b[k]; b[i] = s; }
+#pragma unroll
+    for (int i = 5; i >= 0; --i) {
+        double s = b[i];
+#pragma unroll
+        for (int k = 5; k > i; --k) s -= A[6 * k + i] * b[k];
+        b[i] = s;
+    }
     return true;
 }
 
-__device__ __forceinline__ void tri_index(int t, int& a, int& b) {
-    int r = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-    while ((r + 1) * (r + 2) / 2 <= t) ++r;
-    while (r * (r + 1) / 2 > t) --r;
-    a = r;
-    b = t - r * (r + 1) / 2;
+// ---------------------------------------------------------------------------
+// Block-sparse LDL^T of one multi-body component, one warp.
+//
+// Members are put in elimination order by (distinct coupled neighbours, body
+// index).  The block structure of L (with fill) comes from bit masks:
+// colm[p] = rows below p, filled by merging each column into its parent (the
+// first row below it); rowm[i] = the columns of row i.  L is stored by block
+// rows (row i's blocks in ascending column order), D with the strictly lower
+// part of each diagonal block.  Column p is computed left-looking: every entry
+// first takes the updates (L_ik L_pk) d_k of all earlier structurally nonzero
+// block columns k in ascending order, then those of the columns of block p
+// before it, in registers (one lane per row of the panel, 30 rows per pass).
+// Forward substitution is fused into the column loop; backward substitution
+// runs in descending block order.  Every entry sees the same sequence of
+// operations as the dense oracle loop (its skipped terms are exact zeros).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int mask_rank(const unsigned* row, int b) {
+    int r = 0;
+    for (int w = 0; w < (b >> 5); ++w) r += __popc(row[w]);
+    return r + __popc(row[b >> 5] & ((1u << (b & 31)) - 1u));
 }
+__device__ __forceinline__ bool mask_test(const unsigned* row, int b) { return (row[b >> 5] >> (b & 31)) & 1u; }
 
-// Warp-level block-skipping right-looking LDL^T + solve of one component
-// matrix A (n x n row-major, lower part valid), nzb (k x k, lower, with fill).
-__device__ bool warp_ldlt_solve(double* A, int n, int k, const unsigned char* nzb, int* cand, double* dpiv, double* rhs) {
+// returns 0 ok, 1 zero pivot, 2 capacity
+__device__ int solve_component(const Solver& S, int root, double s, int C) {
     const int lane = threadIdx.x & 31;
-    bool ok = true;
-    for (int j = 0; j < n; ++j) {
-        const int bj = j / 6;
-        int m = 0;
-        for (int i = j + 1; i < 6 * bj + 6; ++i) { if (lane == 0) cand[m] = i; ++m; }
-        for (int bi = bj + 1; bi < k; ++bi)
-            if (nzb[(size_t)bi * k + bj]) { if (lane < 6) cand[m + lane] = 6 * bi + lane; m += 6; }
-        __syncwarp();
-        const double dj = A[(size_t)j * n + j];
-        if (dj == 0.0) { ok = false; break; }
-        for (int t = lane; t < m; t += 32) { const int i = cand[t]; A[(size_t)i * n + j] = A[(size_t)i * n + j] / dj; }
-        __syncwarp();
-        const int np = m * (m + 1) / 2;
-        for (int t = lane; t < np; t += 32) {
-            int a, b;
-            tri_index(t, a, b);
-            const int i = cand[a], c = cand[b];
-            A[(size_t)i * n + c] -= (A[(size_t)i * n + j] * A[(size_t)c * n + j]) * dj;
-        }
-        if (lane == 0) dpiv[j] = dj;
-        __syncwarp();
-    }
-    if (!ok) return false;
-    for (int j = 0; j < n; ++j) {
-        const int bj = j / 6;
-        const double yj = rhs[j];
-        for (int i = j + 1 + lane; i < 6 * bj + 6; i += 32) rhs[i] -= A[(size_t)i * n + j] * yj;
-        for (int bi = bj + 1; bi < k; ++bi)
-            if (nzb[(size_t)bi * k + bj] && lane < 6) { const int i = 6 * bi + lane; rhs[i] -= A[(size_t)i * n + j] * yj; }
-        __syncwarp();
-    }
-    for (int i = lane; i < n; i += 32) rhs[i] /= dpiv[i];
+    const unsigned full = 0xffffffffu;
+    const int k = S.mcnt[root + 1] - S.mcnt[root];
+    const int m = S.icnt[root + 1] - S.icnt[root];
+    int* mem = S.members + S.mcnt[root];
+    int* its = S.items + S.icnt[root];
+    if (k > kMaxComponentBodies) return 2;
+    const int W = (k + 31) >> 5;
+    const int Psort = max(pow2_ceil(k), pow2_ceil(max(m, 1)));
+    const long long nwords = Psort + 3LL * k * W + 6LL * k + 2;
+    long long off = 0;
+    if (lane == 0) off = (long long)atomicAdd((unsigned long long*)S.mpool_off, (unsigned long long)nwords);
+    off = __shfl_sync(full, off, 0);
+    if (off + nwords > S.mpool_cap) return 2;
+    unsigned* base = S.mpool + off;
+    int* sortbuf = (int*)base;
+    unsigned* adj = base + Psort;
+    unsigned* colm = adj + (size_t)k * W;
+    unsigned* rowm = colm + (size_t)k * W;
+    int* deg = (int*)(rowm + (size_t)k * W);
+    int* degcnt = deg + k;
+    int* pos_of = degcnt + k + 1;
+    int* body_at = pos_of + k;
+    int* rowptr = body_at + k;
+    int* rows = rowptr + k + 1;
+
+    // members ascending, items in item order
+    warp_sort_int(mem, k, sortbuf);
+    warp_sort_int(its, m, sortbuf);
+    for (int t = lane; t < k; t += 32) S.local[mem[t]] = t;
+    for (long long e = lane; e < 3LL * k * W; e += 32) adj[e] = 0u;
+    for (int t = lane; t <= k; t += 32) degcnt[t] = 0;
     __syncwarp();
-    for (int j = n - 1; j >= 0; --j) {
-        const int bj = j / 6;
-        const double xj = rhs[j];
-        for (int i = 6 * bj + lane; i < j; i += 32) rhs[i] -= A[(size_t)j * n + i] * xj;
-        for (int bc = 0; bc < bj; ++bc)
-            if (nzb[(size_t)bj * k + bc] && lane < 6) { const int i = 6 * bc + lane; rhs[i] -= A[(size_t)j * n + i] * xj; }
+    for (int q = lane; q < m; q += 32) {
+        int a, b;
+        item_bodies(S, its[q], a, b);
+        const int la = S.local[a], lb = S.local[b];
+        atomicOr(&adj[la * W + (lb >> 5)], 1u << (lb & 31));
+        atomicOr(&adj[lb * W + (la >> 5)], 1u << (la & 31));
+    }
+    __syncwarp();
+    for (int t = lane; t < k; t += 32) {
+        int d = 0;
+        for (int w = 0; w < W; ++w) d += __popc(adj[t * W + w]);
+        deg[t] = d;
+        atomicAdd(&degcnt[d], 1);
+    }
+    __syncwarp();
+    warp_scan_excl(degcnt, k + 1);
+    // stable counting placement by degree (members already ascending)
+    const unsigned lt = (1u << lane) - 1u;
+    for (int b0 = 0; b0 < k; b0 += 32) {
+        const int t = b0 + lane;
+        const int key = t < k ? deg[t] : -1 - lane;
+        const unsigned mask = __match_any_sync(full, key);
+        const int rank = __popc(mask & lt);
+        const int start = t < k ? degcnt[key] : 0;
+        __syncwarp();
+        if (t < k) { pos_of[t] = start + rank; body_at[start + rank] = mem[t]; }
+        if (t < k && lane == __ffs(mask) - 1) degcnt[key] = start + __popc(mask);
         __syncwarp();
     }
-    return true;
+    // lower structure in elimination positions
+    for (int t = lane; t < k; t += 32) {
+        const int pt = pos_of[t];
+        for (int w = 0; w < W; ++w) {
+            unsigned mm = adj[t * W + w];
+            while (mm) {
+                const int u = 32 * w + __ffs(mm) - 1;
+                mm &= mm - 1;
+                const int pu = pos_of[u];
+                if (pu > pt) atomicOr(&colm[pt * W + (pu >> 5)], 1u << (pu & 31));
+            }
+        }
+    }
+    __syncwarp();
+    // symbolic fill: column p merges into its parent
+    for (int p = 0; p < k; ++p) {
+        const unsigned w0 = lane < W ? colm[p * W + lane] : 0u;
+        const unsigned w1 = lane + 32 < W ? colm[p * W + lane + 32] : 0u;
+        const unsigned b0 = __ballot_sync(full, w0 != 0u), b1 = __ballot_sync(full, w1 != 0u);
+        if (!b0 && !b1) continue;
+        int wi;
+        unsigned word;
+        if (b0) { wi = __ffs(b0) - 1; word = __shfl_sync(full, w0, wi); }
+        else { const int l1 = __ffs(b1) - 1; word = __shfl_sync(full, w1, l1); wi = 32 + l1; }
+        const int par = 32 * wi + __ffs(word) - 1;
+        unsigned v0 = w0, v1 = w1;
+        if (lane == wi) v0 &= ~(1u << (par & 31));
+        if (lane + 32 == wi) v1 &= ~(1u << (par & 31));
+        if (v0) colm[par * W + lane] |= v0;
+        if (v1) colm[par * W + lane + 32] |= v1;
+        __syncwarp();
+    }
+    for (int p = lane; p < k; p += 32)
+        for (int w = 0; w < W; ++w) {
+            unsigned mm = colm[p * W + w];
+            while (mm) {
+                const int i = 32 * w + __ffs(mm) - 1;
+                mm &= mm - 1;
+                atomicOr(&rowm[i * W + (p >> 5)], 1u << (p & 31));
+            }
+        }
+    __syncwarp();
+    for (int i = lane; i < k; i += 32) {
+        int c = 0;
+        for (int w = 0; w < W; ++w) c += __popc(rowm[i * W + w]);
+        rowptr[i] = c;
+    }
+    __syncwarp();
+    const int nnz = warp_scan_excl(rowptr, k);
+    if (lane == 0) rowptr[k] = nnz;
+    const long long ndoubles = 36LL * (k + nnz) + 6LL * k;
+    long long doff = 0;
+    if (lane == 0) doff = (long long)atomicAdd((unsigned long long*)S.pool_off, (unsigned long long)ndoubles);
+    doff = __shfl_sync(full, doff, 0);
+    if (doff + ndoubles > S.pool_cap) return 2;
+    double* Dg = S.pool + doff;
+    double* Lv = Dg + 36LL * k;
+    double* vec = Lv + 36LL * nnz;
+    for (int e = lane; e < 36 * k; e += 32) Dg[e] = S.Hd[36 * body_at[e / 36] + e % 36];
+    for (long long e = lane; e < 36LL * nnz; e += 32) Lv[e] = 0.0;
+    for (int e = lane; e < 6 * k; e += 32) vec[e] = -S.g[6 * body_at[e / 6] + e % 6];
+    __syncwarp();
+    // coupling blocks, items in item order (lane e owns entry e of every block)
+    for (int q = 0; q < m; ++q) {
+        const int it = its[q];
+        int a, b;
+        item_bodies(S, it, a, b);
+        const int pa = pos_of[S.local[a]], pb = pos_of[S.local[b]];
+        const int R = pa > pb ? a : b, Cb = pa > pb ? b : a;
+        const int I = max(pa, pb), Jc = min(pa, pb);
+        double* blk = Lv + 36LL * (rowptr[I] + mask_rank(rowm + (size_t)I * W, Jc));
+        for (int e = lane; e < 36; e += 32) blk[e] += coupling_entry(S, it, R, Cb, s, C, e);
+    }
+    __syncwarp();
+
+    // numeric factorisation with fused forward substitution
+    for (int p = 0; p < k; ++p) {
+        const unsigned* rp = rowm + (size_t)p * W;
+        // rows of column p, ascending
+        int nb = 0;
+        for (int b0 = ((p + 1) >> 5) << 5; b0 < k; b0 += 32) {
+            const int bit = b0 + lane;
+            const bool set = bit > p && bit < k && mask_test(colm + (size_t)p * W, bit);
+            const unsigned bal = __ballot_sync(full, set);
+            if (set) rows[nb + __popc(bal & lt)] = bit;
+            nb += __popc(bal);
+        }
+        __syncwarp();
+        double Lr[6], dJ[6];
+        for (int chunk = 0;; ++chunk) {
+            const bool diag = chunk == 0 && lane < 6;
+            const int bi = chunk == 0 ? (lane - 6) / 6 : 4 + 5 * (chunk - 1) + lane / 6;
+            const int r = diag ? lane : (chunk == 0 ? (lane - 6) % 6 : lane % 6);
+            const bool valid = diag || (lane < 30 && (chunk > 0 || lane >= 6) && bi < nb);
+            const int I = diag || !valid ? p : rows[bi];
+            double T[6];
+            double* Lrow = nullptr;
+            for (int c = 0; c < 6; ++c) Lr[c] = 0.0;
+            if (valid) {
+                if (diag) {
+                    for (int c = 0; c < 6; ++c) T[c] = Dg[36LL * p + 6 * r + c];
+                } else {
+                    Lrow = Lv + 36LL * (rowptr[I] + mask_rank(rowm + (size_t)I * W, p)) + 6 * r;
+                    for (int c = 0; c < 6; ++c) T[c] = Lrow[c];
+                }
+                // updates of the earlier block columns K in rowm[I] & rowm[p]
+                const unsigned* ri = rowm + (size_t)I * W;
+                int cI = 0, cP = 0;
+                for (int w = 0; w < W; ++w) {
+                    const unsigned mi = ri[w], mp = rp[w];
+                    unsigned both = mi & mp;
+                    while (both) {
+                        const int bb = __ffs(both) - 1;
+                        both &= both - 1;
+                        const unsigned below = (1u << bb) - 1u;
+                        const double* Lik = Lv + 36LL * (rowptr[I] + cI + __popc(mi & below)) + 6 * r;
+                        const double* Lpk = Lv + 36LL * (rowptr[p] + cP + __popc(mp & below));
+                        const double* dK = Dg + 36LL * (32 * w + bb);
+                        for (int kk = 0; kk < 6; ++kk) {
+                            const double lik = Lik[kk], dk = dK[7 * kk];
+                            for (int c = 0; c < 6; ++c) T[c] -= (lik * Lpk[6 * c + kk]) * dk;
+                        }
+                    }
+                    cI += __popc(mi);
+                    cP += __popc(mp);
+                }
+            } else {
+                for (int c = 0; c < 6; ++c) T[c] = 0.0;
+            }
+            // the six columns of block p
+            for (int c = 0; c < 6; ++c) {
+                double val = T[c];
+                if (chunk == 0) {
+                    for (int c2 = 0; c2 < c; ++c2) {
+                        const double lcc = __shfl_sync(full, Lr[c2], c);
+                        val -= (Lr[c2] * lcc) * dJ[c2];
+                    }
+                    dJ[c] = __shfl_sync(full, val, c);
+                } else {
+                    for (int c2 = 0; c2 < c; ++c2) val -= (Lr[c2] * Dg[36LL * p + 6 * c + c2]) * dJ[c2];
+                }
+                if (dJ[c] == 0.0) return 1;
+                if (valid && !(diag && r <= c)) Lr[c] = val / dJ[c];
+            }
+            if (valid) {
+                if (diag) {
+                    for (int c = 0; c < r; ++c) Dg[36LL * p + 6 * r + c] = Lr[c];
+                    Dg[36LL * p + 7 * r] = dJ[r];
+                } else {
+                    for (int c = 0; c < 6; ++c) Lrow[c] = Lr[c];
+                }
+            }
+            __syncwarp();
+            if (chunk == 0) {
+                // forward substitution for block p (lanes 0-5 hold its rows)
+                double yv = 0.0;
+                if (lane < 6) {
+                    yv = vec[6 * p + lane];
+                    int cP = 0;
+                    for (int w = 0; w < W; ++w) {
+                        const unsigned mp = rp[w];
+                        unsigned mm = mp;
+                        while (mm) {
+                            const int bb = __ffs(mm) - 1;
+                            mm &= mm - 1;
+                            const double* Lpk = Lv + 36LL * (rowptr[p] + cP + __popc(mp & ((1u << bb) - 1u))) + 6 * lane;
+                            const double* yk = vec + 6 * (32 * w + bb);
+                            for (int kk = 0; kk < 6; ++kk) yv -= Lpk[kk] * yk[kk];
+                        }
+                        cP += __popc(mp);
+                    }
+                }
+                for (int c = 0; c < 6; ++c) {
+                    const double yc = __shfl_sync(full, yv, c);
+                    if (lane < 6 && lane > c) yv -= Lr[c] * yc;
+                }
+                if (lane < 6) vec[6 * p + lane] = yv;
+                __syncwarp();
+            }
+            const int done = chunk == 0 ? 4 : 4 + 5 * chunk;
+            if (done >= nb) break;
+        }
+    }
+    // backward substitution, descending blocks
+    for (int p = k - 1; p >= 0; --p) {
+        double xv = 0.0;
+        if (lane < 6) {
+            xv = vec[6 * p + lane] / Dg[36LL * p + 7 * lane];
+            const unsigned* cp = colm + (size_t)p * W;
+            for (int w = W - 1; w >= 0; --w) {
+                unsigned mm = cp[w];
+                while (mm) {
+                    const int bb = 31 - __clz(mm);
+                    mm &= ~(1u << bb);
+                    const int I = 32 * w + bb;
+                    const double* Lip = Lv + 36LL * (rowptr[I] + mask_rank(rowm + (size_t)I * W, p));
+                    const double* xi = vec + 6 * I;
+                    for (int r = 5; r >= 0; --r) xv -= Lip[6 * r + lane] * xi[r];
+                }
+            }
+        }
+        for (int c = 5; c >= 0; --c) {
+            const double xc = __shfl_sync(full, xv, c);
+            if (lane < c) xv -= Dg[36LL * p + 6 * c + lane] * xc;
+        }
+        if (lane < 6) vec[6 * p + lane] = xv;
+        __syncwarp();
+    }
+    for (int e = lane; e < 6 * k; e += 32) S.dx[6 * body_at[e / 6] + e % 6] = vec[e];
+    __syncwarp();
+    return 0;
 }
 
 // Solve H dx = -g.  Returns false (all threads) on failure.
-__device__ bool solve_newton_system(const Solver& S, double s, int C, int* sh_flag) {
+__device__ bool solve_newton_system(const Solver& S, double s, int C, int* sh_flag, int* sh_next, int* sh_scan) {
     const int N = S.N;
     const int n_items = S.J + 2 * C;
-    // union-find
-    for (int i = threadIdx.x; i < N; i += blockDim.x) S.parent[i] = i;
-    if (threadIdx.x == 0) *sh_flag = 0;
+    for (int i = threadIdx.x; i <= N; i += blockDim.x) {
+        if (i < N) S.parent[i] = i;
+        S.mcnt[i] = 0; S.icnt[i] = 0; S.rflag[i] = 0;
+    }
+    if (threadIdx.x == 0) { *sh_flag = 0; *sh_next = 0; *S.mpool_off = 0; *S.pool_off = 0; }
     __syncthreads();
     for (int it = threadIdx.x; it < n_items; it += blockDim.x) {
         if (!item_active(S, it)) continue;
@@ -785,193 +1233,78 @@ __device__ bool solve_newton_system(const Solver& S, double s, int C, int* sh_fl
         if (a != b) uf_union(S.parent, a, b);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < N; i += blockDim.x) S.comp[i] = uf_find(S.parent, i);
-    __syncthreads();
-    // component sizes (indexed by root) and member lists (bodies ascending)
-    for (int i = threadIdx.x; i < N; i += blockDim.x) S.comp_size[i] = 0;
-    __syncthreads();
-    for (int i = threadIdx.x; i < N; i += blockDim.x) atomicAdd(&S.comp_size[S.comp[i]], 1);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int r = 0; r < N; ++r) { S.comp_off[r] = acc; acc += S.comp_size[r]; }
-        S.comp_off[N] = acc;
-        *S.pool_off = 0;
-        *S.nzb_off = 0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        const int r = uf_find(S.parent, i);
+        S.comp[i] = r;
+        atomicAdd(&S.mcnt[r], 1);
+    }
+    for (int it = threadIdx.x; it < n_items; it += blockDim.x) {
+        if (!item_active(S, it)) continue;
+        int a, b;
+        item_bodies(S, it, a, b);
+        if (a != b) atomicAdd(&S.icnt[uf_find(S.parent, a)], 1);
     }
     __syncthreads();
-    // running starts live in item_comp_off temporarily for the placement
-    for (int r = threadIdx.x; r <= N; r += blockDim.x) S.item_comp_off[r] = S.comp_off[r];
+    // singletons: one thread each, in registers
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        const bool multi = S.comp[i] == i && S.mcnt[i] >= 2;
+        S.rflag[i] = multi ? 1 : 0;
+        if (S.comp[i] != i || S.mcnt[i] != 1) continue;
+        double A[36], b[6];
+#pragma unroll
+        for (int e = 0; e < 36; ++e) A[e] = S.Hd[36 * i + e];
+#pragma unroll
+        for (int e = 0; e < 6; ++e) b[e] = -S.g[6 * i + e];
+        if (!ldlt6_solve(A, b)) { atomicExch(sh_flag, 1); continue; }
+#pragma unroll
+        for (int e = 0; e < 6; ++e) S.dx[6 * i + e] = b[e];
+    }
     __syncthreads();
-    warp_stable_place(N, [&](int e) { return S.comp[e]; }, S.item_comp_off, S.members);
+    NX_PHASE(3);
+    for (int i = threadIdx.x; i < N; i += blockDim.x)
+        if (!S.rflag[i]) S.mcnt[i] = 0;
     __syncthreads();
-    // active coupling items grouped by component root, item order kept
-    for (int r = threadIdx.x; r <= N; r += blockDim.x) S.deg[r] = 0;
+    {
+        int* const arr[3] = {S.mcnt, S.icnt, S.rflag};
+        block_scan_excl<3>(arr, N, sh_scan);
+    }
     __syncthreads();
+    const int n_comp = S.rflag[N];
+    for (int r = threadIdx.x; r < N; r += blockDim.x) {
+        if (S.rflag[r + 1] != S.rflag[r]) S.comp_root[S.rflag[r]] = r;
+        S.local[r] = 0;    // member cursor per root
+        S.parent[r] = 0;   // item cursor per root
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        const int r = S.comp[i];
+        if (S.mcnt[r + 1] - S.mcnt[r] >= 2) S.members[S.mcnt[r] + atomicAdd(&S.local[r], 1)] = i;
+    }
     for (int it = threadIdx.x; it < n_items; it += blockDim.x) {
-        S.items[it] = -1;
         if (!item_active(S, it)) continue;
         int a, b;
         item_bodies(S, it, a, b);
         if (a == b) continue;
-        S.items[it] = S.comp[a];
-        atomicAdd(&S.deg[S.comp[a]], 1);
+        const int r = S.comp[a];
+        S.items[S.icnt[r] + atomicAdd(&S.parent[r], 1)] = it;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int r = 0; r < N; ++r) { const int c = S.deg[r]; S.deg[r] = acc; acc += c; }
-        S.deg[N] = acc;
-        *S.n_items_ptr = acc;
-    }
-    __syncthreads();
-    for (int r = threadIdx.x; r <= N; r += blockDim.x) S.item_comp_off[r] = S.deg[r];
-    __syncthreads();
-    {
-        // compact active items in order, then stable-place by component
-        // (items[] holds the component root or -1)
-        if (threadIdx.x < 32) {
-            const int lane = threadIdx.x;
-            const unsigned lt = (1u << lane) - 1u;
-            for (int base = 0; base < n_items; base += 32) {
-                const int e = base + lane;
-                const int key = e < n_items ? S.items[e] : -1;
-                const bool valid = key >= 0;
-                const unsigned mask = __match_any_sync(0xffffffffu, valid ? key : -1 - lane);
-                const int rank = __popc(mask & lt);
-                int start = 0;
-                if (valid) start = S.item_comp_off[key];
-                __syncwarp();
-                if (valid) S.item_list[start + rank] = e;
-                const int leader = __ffs(mask) - 1;
-                if (valid && lane == leader) S.item_comp_off[key] = start + __popc(mask);
-                __syncwarp();
-            }
+    NX_PHASE(3);
+    // multi-body components: one warp each, taken from a shared counter
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int o = 0;
+        if (lane == 0) o = atomicAdd(sh_next, 1);
+        o = __shfl_sync(0xffffffffu, o, 0);
+        if (o >= n_comp) break;
+        const int rc = solve_component(S, S.comp_root[o], s, C);
+        if (rc != 0 && lane == 0) {
+            atomicExch(sh_flag, 1);
+            if (rc == 2) atomicExch(S.status, NXD_CAPACITY);
         }
     }
     __syncthreads();
-    // singletons: one thread each
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
-        if (S.comp[i] != i || S.comp_size[i] != 1) continue;
-        double A[36], b[6];
-        for (int k = 0; k < 36; ++k) A[k] = S.Hd[36 * i + k];
-        for (int k = 0; k < 6; ++k) b[k] = -S.g[6 * i + k];
-        if (!ldlt6_solve(A, b)) { atomicExch(sh_flag, 1); continue; }
-        for (int k = 0; k < 6; ++k) S.dx[6 * i + k] = b[k];
-    }
-    // multi-body components: one warp each
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    int* cand = S.cand + (size_t)wid * S.cand_stride;
-    int ci = 0;
-    for (int r = 0; r < N; ++r) {
-        if (S.comp_size[r] < 2 || S.comp[r] != r) continue;
-        if ((ci++ % nw) != wid) continue;
-        const int k = S.comp_size[r];
-        const int* mem = S.members + S.comp_off[r];
-        if (k > kMaxComponentBodies) { if (lane == 0) { atomicExch(sh_flag, 1); atomicExch(S.status, NXD_CAPACITY); } continue; }
-        const int n = 6 * k;
-        long long aoff = 0, zoff = 0;
-        if (lane == 0) {
-            aoff = atomicAdd((unsigned long long*)S.pool_off, (unsigned long long)n * n);
-            zoff = atomicAdd((unsigned long long*)S.nzb_off, (unsigned long long)k * k);
-        }
-        aoff = __shfl_sync(0xffffffffu, aoff, 0);
-        zoff = __shfl_sync(0xffffffffu, zoff, 0);
-        if (aoff + (long long)n * n > S.pool_cap || zoff + (long long)k * k > S.nzb_cap) {
-            if (lane == 0) { atomicExch(sh_flag, 1); atomicExch(S.status, NXD_CAPACITY); }
-            continue;
-        }
-        double* A = S.pool + aoff;
-        unsigned char* nz = S.nzb + zoff;
-        const int i0 = S.deg[r], i1 = S.deg[r + 1];
-        // provisional local index = rank in ascending member order
-        for (int t = lane; t < k; t += 32) S.local[mem[t]] = t;
-        for (int t = lane; t < k * k; t += 32) nz[t] = 0;
-        __syncwarp();
-        for (int q = i0 + lane; q < i1; q += 32) {
-            int a, b;
-            item_bodies(S, S.item_list[q], a, b);
-            const int la = S.local[a], lb = S.local[b];
-            nz[la * k + lb] = 1; nz[lb * k + la] = 1;
-        }
-        __syncwarp();
-        // order members by (distinct neighbours, body index)
-        int* ord = cand + 6 * kMaxComponentBodies;       // k ints
-        int* dg = ord + kMaxComponentBodies;             // k ints
-        for (int t = lane; t < k; t += 32) {
-            int c = 0;
-            for (int u = 0; u < k; ++u) c += (u != t && nz[t * k + u]) ? 1 : 0;
-            dg[t] = c;
-            ord[t] = mem[t];
-        }
-        __syncwarp();
-        if (lane == 0) {
-            for (int a = 1; a < k; ++a) {
-                const int vb = ord[a], vd = dg[a];
-                int b = a - 1;
-                while (b >= 0 && (dg[b] > vd || (dg[b] == vd && ord[b] > vb))) { ord[b + 1] = ord[b]; dg[b + 1] = dg[b]; --b; }
-                ord[b + 1] = vb; dg[b + 1] = vd;
-            }
-        }
-        __syncwarp();
-        for (int t = lane; t < k; t += 32) S.local[ord[t]] = t;
-        for (int t = lane; t < k * k; t += 32) nz[t] = 0;
-        __syncwarp();
-        for (int q = i0 + lane; q < i1; q += 32) {
-            int a, b;
-            item_bodies(S, S.item_list[q], a, b);
-            const int la = S.local[a], lb = S.local[b];
-            nz[max(la, lb) * k + min(la, lb)] = 1;
-        }
-        __syncwarp();
-        // symbolic fill, column by column
-        for (int bj = 0; bj < k; ++bj) {
-            for (int t = lane; t < k * k; t += 32) {
-                const int b2 = t / k, b1 = t % k;
-                if (b1 > bj && b2 > b1 && nz[(size_t)b1 * k + bj] && nz[(size_t)b2 * k + bj]) nz[(size_t)b2 * k + b1] = 1;
-            }
-            __syncwarp();
-        }
-        // zero used blocks, place diagonal blocks (lower part)
-        for (int t = lane; t < k * k; t += 32) {
-            const int bi = t / k, bc = t % k;
-            if (bc > bi) continue;
-            if (bc != bi && !nz[t]) continue;
-            for (int e = 0; e < 36; ++e) {
-                const int rr = e / 6, cc = e % 6;
-                double v = 0.0;
-                if (bc == bi && cc <= rr) v = S.Hd[36 * ord[bi] + e];
-                A[(size_t)(6 * bi + rr) * n + 6 * bc + cc] = v;
-            }
-        }
-        __syncwarp();
-        // coupling items in item order, lower orientation in local order
-        if (lane == 0) {
-            for (int q = i0; q < i1; ++q) {
-                const int it = S.item_list[q];
-                int a, b;
-                item_bodies(S, it, a, b);
-                const int la = S.local[a], lb = S.local[b];
-                const int R = la > lb ? a : b, Cb = la > lb ? b : a;
-                const int lr = max(la, lb), lc = min(la, lb);
-                double blk[36];
-                for (int e = 0; e < 36; ++e) blk[e] = 0.0;
-                add_coupling_block(S, it, R, Cb, s, blk);
-                for (int e = 0; e < 36; ++e) A[(size_t)(6 * lr + e / 6) * n + 6 * lc + e % 6] += blk[e];
-            }
-        }
-        __syncwarp();
-        // rhs and pivots: the component's members own DOF range
-        // [6 comp_off, 6 comp_off + n) of dvec ([12N] doubles)
-        double* b = S.dvec + 6 * (size_t)S.comp_off[r];
-        double* dp = S.dvec + 6 * (size_t)N + 6 * (size_t)S.comp_off[r];
-        for (int t = lane; t < n; t += 32) b[t] = -S.g[6 * ord[t / 6] + t % 6];
-        __syncwarp();
-        if (!warp_ldlt_solve(A, n, k, nz, cand, dp, b)) { if (lane == 0) atomicExch(sh_flag, 1); continue; }
-        for (int t = lane; t < n; t += 32) S.dx[6 * ord[t / 6] + t % 6] = b[t];
-        __syncwarp();
-    }
-    __syncthreads();
+    NX_PHASE(4);
     const bool fail = *sh_flag != 0;
     __syncthreads();
     return !fail;
@@ -981,34 +1314,21 @@ __device__ bool solve_newton_system(const Solver& S, double s, int C, int* sh_fl
 // The kernel: one ALM iteration's Newton solve + joint bookkeeping.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kSolverThreads) k_newton(Solver S) {
-    __shared__ double sh_red[32];
-    __shared__ int sh_flag;
-    __shared__ int sh_done;
+    __shared__ unsigned long long sh_keys[kMaxIncidence];
+    __shared__ int sh_scan[3 * 32];
+    __shared__ int sh_flag, sh_next;
+    NX_BLOCK_RED(R);
     if (*S.alm_done) return;
+    NX_PHASE_START();
     const int N = S.N;
     const int C = *S.ncontacts_ptr;
     const double dt = *S.dt_ptr;
     const double s = dt * dt;
     const int n6 = 6 * N;
-    // contact incidence (body -> contact*2+side), contact order kept
-    for (int i = threadIdx.x; i <= N; i += blockDim.x) S.cinc_cnt[i] = 0;
-    __syncthreads();
-    for (int e = threadIdx.x; e < 2 * C; e += blockDim.x) {
-        const ContactRec& cr = S.contacts[e >> 1];
-        atomicAdd(&S.cinc_cnt[(e & 1) ? cr.body_b : cr.body_a], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int i = 0; i < N; ++i) { S.cinc_off[i] = acc; acc += S.cinc_cnt[i]; }
-        S.cinc_off[N] = acc;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i <= N; i += blockDim.x) S.cinc_cnt[i] = S.cinc_off[i];
-    __syncthreads();
-    warp_stable_place(2 * C, [&](int e) { const ContactRec& cr = S.contacts[e >> 1]; return (e & 1) ? cr.body_b : cr.body_a; },
-                      S.cinc_cnt, S.cinc);
-    __syncthreads();
+    const bool bar = *S.barrier_in_forms_ptr != 0, fr = *S.friction_form_ptr != 0;
+    const double dh = *S.bdhat_ptr;
+    build_contact_incidence(S, C, sh_keys);
+    NX_PHASE(0);
 
     bool converged = false;
     int iters = 0;
@@ -1016,50 +1336,57 @@ __global__ void __launch_bounds__(kSolverThreads) k_newton(Solver S) {
         iters = iter;
         // gradient at x (drives: gradient call)
         eval_poses(S, S.x);
+        for (int d = threadIdx.x; d < S.D; d += blockDim.x) drive_eval(S, d, S.x, 1);
         __syncthreads();
         for (int j = threadIdx.x; j < S.J; j += blockDim.x) joint_eval(S, j, S.x, true);
-        for (int d = threadIdx.x; d < S.D; d += blockDim.x) drive_eval(S, d, S.x, 1);
-        const bool bar = *S.barrier_in_forms_ptr != 0, fr = *S.friction_form_ptr != 0;
         for (int c = threadIdx.x; c < C; c += blockDim.x) {
             if (bar) barrier_eval(S, c, S.x);
             if (fr) friction_eval(S, c, S.x, true);
         }
         __syncthreads();
-        gather_gradient(S, S.x, s, C);
-        __syncthreads();
         double gm = 0.0;
-        for (int k = threadIdx.x; k < n6; k += blockDim.x) gm = dmax(gm, fabs(S.g[k]));
-        gm = block_max(gm, sh_red);
+        for (int e = threadIdx.x; e < n6; e += blockDim.x) {
+            double g, cg;
+            gradient_dof(S, S.x, s, e / 6, e % 6, bar, fr, dh, g, cg);
+            S.g[e] = g;
+            S.cg[e] = cg;
+            gm = dmax(gm, fabs(g));
+        }
+        gm = R.max(gm);
+        NX_PHASE(1);
         if (gm < S.newton_tol) { converged = true; break; }
         // Hessian (drives: hessian call)
         for (int d = threadIdx.x; d < S.D; d += blockDim.x) drive_eval(S, d, S.x, 2);
         __syncthreads();
         gather_diag_hessian(S, s, C);
         __syncthreads();
-        if (!solve_newton_system(S, s, C, &sh_flag)) break;
+        NX_PHASE(2);
+        if (!solve_newton_system(S, s, C, &sh_flag, &sh_next, sh_scan)) break;
         // line search (max step 1)
-        const double fx = energy_total(S, S.x, s, C, false);
-        for (int k = threadIdx.x; k < n6; k += blockDim.x) S.red[k] = S.g[k] * S.dx[k];
-        const double descent = block_tree_sum(S.red, n6);
-        const double fc = energy_total(S, S.x, s, C, true);
-        for (int k = threadIdx.x; k < n6; k += blockDim.x) S.red[k] = S.cg[k] * S.dx[k];
-        const double cdesc = block_tree_sum(S.red, n6);
+        const double fx = energy_total(S, S.x, s, C, false, R);
+        double dd[2];
+        {
+            const int nn[2] = {n6, n6};
+            R.sums<2>(nn, [&](int q, int e) { return (q == 0 ? S.g[e] : S.cg[e]) * S.dx[e]; }, dd);
+        }
+        const double descent = dd[0], cdesc = dd[1];
+        const double fc = energy_total(S, S.x, s, C, true, R);
+        NX_PHASE(5);
         if (descent > 0) { if (threadIdx.x == 0) atomicAdd(S.ls_fail, 1); break; }
         double alpha = 1.0;
-        if (threadIdx.x == 0) sh_done = 0;
-        __syncthreads();
+        bool done = false;
         for (int ls = 0; ls < S.ls_max_iters; ++ls) {
-            for (int k = threadIdx.x; k < n6; k += blockDim.x) S.xt[k] = S.x[k] + alpha * S.dx[k];
+            for (int e = threadIdx.x; e < n6; e += blockDim.x) S.xt[e] = S.x[e] + alpha * S.dx[e];
             __syncthreads();
-            const double fn = energy_total(S, S.xt, s, C, false);
-            const double fcn = energy_total(S, S.xt, s, C, true);
+            const double fn = energy_total(S, S.xt, s, C, false, R);
+            const double fcn = energy_total(S, S.xt, s, C, true, R);
             const bool cok = cdesc <= 0.0 ? (fcn <= fc + S.ls_c1 * alpha * cdesc) : (fcn <= fc);
-            if (fn <= fx + S.ls_c1 * alpha * descent && cok) { sh_done = 1; break; }
+            if (fn <= fx + S.ls_c1 * alpha * descent && cok) { done = true; break; }
             alpha *= S.ls_rho;
         }
-        __syncthreads();
-        if (!sh_done) { if (threadIdx.x == 0) atomicAdd(S.ls_fail, 1); break; }
-        for (int k = threadIdx.x; k < n6; k += blockDim.x) S.x[k] = S.xt[k];
+        NX_PHASE(6);
+        if (!done) { if (threadIdx.x == 0) atomicAdd(S.ls_fail, 1); break; }
+        for (int e = threadIdx.x; e < n6; e += blockDim.x) S.x[e] = S.xt[e];
         __syncthreads();
         if (iter == S.newton_max_iters - 1) iters = S.newton_max_iters;
     }
@@ -1068,38 +1395,44 @@ __global__ void __launch_bounds__(kSolverThreads) k_newton(Solver S) {
         atomicAdd(S.newton_iters, iters);
         *S.converged = converged ? 1 : 0;
     }
-    // ALM: violation, hardening, lambda update (IPCSolver.cpp:1084-1110)
+    // ALM: violation, hardening, lambda update (IPCSolver.cpp:1084-1110);
+    // each joint hardens with its own pre-update stiffness, then takes
+    // lambda += mu_new C
     eval_poses(S, S.x);
     __syncthreads();
-    for (int j = threadIdx.x; j < S.J; j += blockDim.x) joint_eval(S, j, S.x, false);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double mcv = 0.0, dual = 0.0;
-        for (int j = 0; j < S.J; ++j) {
-            const int dim = joint_dim(S.jtype[j]);
-            double inf = 0.0;
-            for (int k = 0; k < dim; ++k) inf = dmax(inf, fabs(S.jC[6 * j + k]));
-            mcv = dmax(mcv, inf);
-            const double dc = S.jmu[j] * inf;
-            if (isfinite(dc)) dual = dmax(dual, dmin(dc, 1e12));
-            else dual = dmax(dual, 1e12);
-            if (inf > S.alm_hardening_trigger * S.alm_constraint_tol) {
-                const double ns = S.jmu[j] * S.alm_hardening_ratio;
-                S.jmu[j] = isfinite(ns) ? dmin(ns, 1e12) : 1e12;
-            }
-        }
-        *S.alm_mcv = mcv;
-        *S.alm_dual = dual;
-    }
-    __syncthreads();
+    double mcv = 0.0, dual = 0.0;
     for (int j = threadIdx.x; j < S.J; j += blockDim.x) {
-        const int dim = joint_dim(S.jtype[j]);
-        const double* Cj = S.jC + 6 * j;
+        double Cj[6];
+        const int dim = joint_residual(S, j, S.x, Cj, nullptr);
+        for (int k = 0; k < 6; ++k) S.jC[6 * j + k] = Cj[k];
+        double inf = 0.0;
+        for (int k = 0; k < dim; ++k) inf = dmax(inf, fabs(Cj[k]));
+        mcv = dmax(mcv, inf);
+        double mu = S.jmu[j];
+        const double dc = mu * inf;
+        if (isfinite(dc)) dual = dmax(dual, dmin(dc, 1e12));
+        else dual = dmax(dual, 1e12);
+        if (inf > S.alm_hardening_trigger * S.alm_constraint_tol) {
+            const double ns = mu * S.alm_hardening_ratio;
+            mu = isfinite(ns) ? dmin(ns, 1e12) : 1e12;
+            S.jmu[j] = mu;
+        }
         double* lam = S.jlam + 6 * j;
-        const double mu = S.jmu[j];
         if (S.jtype[j] == NXD_JOINT_ANGLE_LIMIT) for (int k = 0; k < dim; ++k) lam[k] = dmax(0.0, lam[k] + mu * Cj[k]);
         else for (int k = 0; k < dim; ++k) lam[k] += mu * Cj[k];
     }
+    mcv = R.max(mcv);
+    dual = R.max(dual);
+    if (threadIdx.x == 0) {
+        *S.alm_mcv = mcv;
+        *S.alm_dual = dual;
+    }
+    NX_PHASE(7);
+#ifdef NXD_PHASE_TIMERS
+    if (threadIdx.x == 0)
+        printf("PH C=%d it=%d init=%lld grad=%lld hess=%lld symb=%lld comp=%lld ls0=%lld ls=%lld post=%lld\n", C, iters,
+               nx_ph_acc[0], nx_ph_acc[1], nx_ph_acc[2], nx_ph_acc[3], nx_ph_acc[4], nx_ph_acc[5], nx_ph_acc[6], nx_ph_acc[7]);
+#endif
 }
 
 }  // namespace nx

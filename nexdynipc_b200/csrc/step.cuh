@@ -44,11 +44,11 @@ struct StepCfg {
 
 // IPCSolver::initializeAdaptiveBarrier (IPCSolver.cpp:327-353) +
 // AdaptiveBarrier::initialize (AdaptiveBarrier.h:27-31); runs once per context.
-__global__ void k_barrier_init(StepCfg cfg, const double* mass, const double* pos, Scalars* sc, double* red) {
+__global__ void __launch_bounds__(kSolverThreads) k_barrier_init(StepCfg cfg, const double* mass, const double* pos, Scalars* sc) {
     __shared__ double bb[6];
+    NX_BLOCK_RED(R);
     if (!cfg.enable_adaptive || sc->barrier_initialized || cfg.N == 0) return;
-    for (int i = threadIdx.x; i < cfg.N; i += blockDim.x) red[i] = mass[i];
-    const double tm = block_tree_sum(red, cfg.N);
+    const double tm = R.sum(cfg.N, [&](int i) { return mass[i]; });
     if (threadIdx.x == 0) {
         V3 mn = v3(INFINITY, INFINITY, INFINITY), mx = v3(-INFINITY, -INFINITY, -INFINITY);
         for (int i = 0; i < cfg.N; ++i) { mn = cwmin(mn, ld3(pos + 3 * i)); mx = cwmax(mx, ld3(pos + 3 * i)); }
@@ -175,16 +175,18 @@ __global__ void k_sort_contacts(Scalars* sc, ContactRec* c, ContactRec* tmp, dou
 // After the Newton solve and the detection at x_new (IPCSolver.cpp:1112-1165):
 // normal forces, contact residual, ALM convergence.
 __global__ void __launch_bounds__(kSolverThreads) k_alm_post(Solver S, Scalars* sc, StepCfg cfg, double* nforce_out) {
-    __shared__ double sh_red[32];
+    __shared__ unsigned long long sh_keys[kMaxIncidence];
+    NX_BLOCK_RED(R);
     if (sc->alm_done) return;
     const int C = sc->n_contacts;
     const bool bform = sc->barrier_form != 0, fform = sc->friction_form != 0;
+    const bool fric = cfg.enable_friction && fform;
     if (bform || fform) {
         eval_poses(S, S.x);
         __syncthreads();
         for (int c = threadIdx.x; c < C; c += blockDim.x) barrier_eval(S, c, S.x);
         __syncthreads();
-        if (cfg.enable_friction && fform) {
+        if (fric) {
             // DistanceBarrierForm::computeNormalForces (DistanceBarrierForm.cpp:70-86)
             for (int c = threadIdx.x; c < C; c += blockDim.x) {
                 double nf = 0.0;
@@ -197,54 +199,34 @@ __global__ void __launch_bounds__(kSolverThreads) k_alm_post(Solver S, Scalars* 
             if (threadIdx.x == 0) sc->nnf = C;
         }
         __syncthreads();
-        if (cfg.enable_friction && fform)
+        if (fric)
             for (int c = threadIdx.x; c < C; c += blockDim.x) friction_eval(S, c, S.x, true);
-        // contact incidence for the gather
-        for (int i = threadIdx.x; i <= S.N; i += blockDim.x) S.cinc_cnt[i] = 0;
-        __syncthreads();
-        for (int e = threadIdx.x; e < 2 * C; e += blockDim.x) {
-            const ContactRec& cr = S.contacts[e >> 1];
-            atomicAdd(&S.cinc_cnt[(e & 1) ? cr.body_b : cr.body_a], 1);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int acc = 0;
-            for (int i = 0; i < S.N; ++i) { S.cinc_off[i] = acc; acc += S.cinc_cnt[i]; }
-            S.cinc_off[S.N] = acc;
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i <= S.N; i += blockDim.x) S.cinc_cnt[i] = S.cinc_off[i];
-        __syncthreads();
-        warp_stable_place(2 * C, [&](int e) { const ContactRec& cr = S.contacts[e >> 1]; return (e & 1) ? cr.body_b : cr.body_a; },
-                          S.cinc_cnt, S.cinc);
-        __syncthreads();
+        build_contact_incidence(S, C, sh_keys);
+        // max |barrier + friction gradient| over all DOFs
         double m = 0.0;
         const double dh = sc->bdhat;
-        const int nnf = sc->nnf;
-        for (int i = threadIdx.x; i < S.N; i += blockDim.x) {
-            double cb[6] = {0, 0, 0, 0, 0, 0}, cf[6] = {0, 0, 0, 0, 0, 0};
+        for (int e = threadIdx.x; e < 6 * S.N; e += blockDim.x) {
+            const int i = e / 6, k = e % 6;
+            double cb = 0.0, cf = 0.0;
             for (int q = S.cinc_off[i]; q < S.cinc_off[i + 1]; ++q) {
                 const int c = S.cinc[q] >> 1, side = S.cinc[q] & 1;
-                if (bform && S.bD[c] < dh) {
+                if (bform && k < 3 && S.bD[c] < dh) {
                     const double gpv = S.bGP[c];
-                    const V3 n = ld3(S.contacts[c].normal);
-                    const V3 contrib = side == 0 ? (-gpv) * n : gpv * n;
-                    cb[0] += contrib.x; cb[1] += contrib.y; cb[2] += contrib.z;
+                    const double nk = S.contacts[c].normal[k];
+                    cb += side == 0 ? (-gpv) * nk : gpv * nk;
                 }
-                if (cfg.enable_friction && fform && c < nnf && S.nforce[c] > 0) {
+                if (fric && friction_on(S, c)) {
                     const double* Jx = (side == 0 ? S.fJA : S.fJB) + 18 * c;
-                    const V3 fg = ld3(S.fFG + 3 * c);
-                    for (int k = 0; k < 6; ++k) cf[k] += Jx[k] * fg.x + Jx[6 + k] * fg.y + Jx[12 + k] * fg.z;
+                    const double* fg = S.fFG + 3 * c;
+                    cf += Jx[k] * fg[0] + Jx[6 + k] * fg[1] + Jx[12 + k] * fg[2];
                 }
             }
-            for (int k = 0; k < 6; ++k) {
-                double v = 0.0;
-                if (bform) v += cb[k];
-                if (cfg.enable_friction && fform) v += cf[k];
-                m = dmax(m, fabs(v));
-            }
+            double v = 0.0;
+            if (bform) v += cb;
+            if (fric) v += cf;
+            m = dmax(m, fabs(v));
         }
-        m = block_max(m, sh_red);
+        m = R.max(m);
         if (threadIdx.x == 0) sc->alm_cres = isfinite(m) ? m : 1e12;
     } else if (threadIdx.x == 0) {
         sc->alm_cres = 0.0;
@@ -324,12 +306,14 @@ __device__ int form_mask(int form, const Solver& S) {
 __global__ void __launch_bounds__(kSolverThreads) k_form_eval(Solver S, Scalars* sc, int form, int what, const double* x,
                                                               double* out, int* row_ptr, int* col_idx, double* vals,
                                                               long long cap, long long* nnzb) {
-    __shared__ int sh_cnt;
+    __shared__ unsigned long long sh_keys[kMaxIncidence];
+    __shared__ int sh_scan[32];
+    NX_BLOCK_RED(R);
     const int N = S.N;
     const int C = sc->n_contacts;
     const double s = sc->dt * sc->dt;
     if (what == 0 && (form == NXD_FORM_TOTAL || form == NXD_FORM_CONTACT)) {
-        const double v = energy_total(S, x, s, C, form == NXD_FORM_CONTACT);
+        const double v = energy_total(S, x, s, C, form == NXD_FORM_CONTACT, R);
         if (threadIdx.x == 0) out[0] = v;
         return;
     }
@@ -344,61 +328,16 @@ __global__ void __launch_bounds__(kSolverThreads) k_form_eval(Solver S, Scalars*
     __syncthreads();
     if (what == 0) {
         double v = 0.0;
-        {
-            int n = 0;
-            if (form == NXD_FORM_INERTIA || form == NXD_FORM_GRAVITY) {
-                n = N;
-                for (int i = threadIdx.x; i < N; i += blockDim.x) {
-                    if (form == NXD_FORM_INERTIA) {
-                        const V3 dp = xs3(x, 6 * i) - xs3(S.xhat, 6 * i);
-                        const double et = 0.5 * S.mass[i] * sqnorm(dp);
-                        const V3 dth = xs3(x, 6 * i + 3) - xs3(S.xhat, 6 * i + 3);
-                        const double* I = S.inertia + 9 * i;
-                        const V3 r = v3(dth.x * I[0] + dth.y * I[3] + dth.z * I[6], dth.x * I[1] + dth.y * I[4] + dth.z * I[7],
-                                        dth.x * I[2] + dth.y * I[5] + dth.z * I[8]);
-                        S.red[i] = et + 0.5 * dot(r, dth);
-                    } else {
-                        S.red[i] = -(S.mass[i] * dot(v3(0.0, -9.81, 0.0), xs3(x, 6 * i)));
-                    }
-                }
-            } else if (form == NXD_FORM_CONSTRAINT) {
-                n = S.J;
-                for (int j = threadIdx.x; j < S.J; j += blockDim.x) S.red[j] = S.jE[j];
-            } else if (form == NXD_FORM_BARRIER) {
-                n = C;
-                for (int c = threadIdx.x; c < C; c += blockDim.x) S.red[c] = S.bE[c];
-            } else if (form == NXD_FORM_FRICTION) {
-                n = C;
-                for (int c = threadIdx.x; c < C; c += blockDim.x) S.red[c] = S.fE[c];
-            } else if (form == NXD_FORM_DRIVES) {
-                n = S.D;
-                for (int d = threadIdx.x; d < S.D; d += blockDim.x) S.red[d] = S.dE[d];
-            }
-            __syncthreads();
-            v = block_tree_sum(S.red, n);
-        }
+        if (form == NXD_FORM_INERTIA) v = R.sum(N, [&](int i) { return inertia_value(S, i, x); });
+        else if (form == NXD_FORM_GRAVITY) v = R.sum(N, [&](int i) { return gravity_value(S, i, x); });
+        else if (form == NXD_FORM_CONSTRAINT) v = R.sum(S.J, [&](int j) { return S.jE[j]; });
+        else if (form == NXD_FORM_BARRIER) v = R.sum(C, [&](int c) { return S.bE[c]; });
+        else if (form == NXD_FORM_FRICTION) v = R.sum(C, [&](int c) { return S.fE[c]; });
+        else if (form == NXD_FORM_DRIVES) v = R.sum(S.D, [&](int d) { return S.dE[d]; });
         if (threadIdx.x == 0) out[0] = v;
         return;
     }
-    // contact incidence
-    for (int i = threadIdx.x; i <= N; i += blockDim.x) S.cinc_cnt[i] = 0;
-    __syncthreads();
-    for (int e = threadIdx.x; e < 2 * C; e += blockDim.x) {
-        const ContactRec& cr = S.contacts[e >> 1];
-        atomicAdd(&S.cinc_cnt[(e & 1) ? cr.body_b : cr.body_a], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int i = 0; i < N; ++i) { S.cinc_off[i] = acc; acc += S.cinc_cnt[i]; }
-        S.cinc_off[N] = acc;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i <= N; i += blockDim.x) S.cinc_cnt[i] = S.cinc_off[i];
-    __syncthreads();
-    warp_stable_place(2 * C, [&](int e) { const ContactRec& cr = S.contacts[e >> 1]; return (e & 1) ? cr.body_b : cr.body_a; },
-                      S.cinc_cnt, S.cinc);
-    __syncthreads();
+    build_contact_incidence(S, C, sh_keys);
     if (what == 1) {
         if (form == NXD_FORM_TOTAL || form == NXD_FORM_CONTACT) {
             gather_gradient(S, x, s, C);
@@ -469,26 +408,25 @@ __global__ void __launch_bounds__(kSolverThreads) k_form_eval(Solver S, Scalars*
         return;
     }
     const int n_items = S.J + 2 * C;
-    for (int i = threadIdx.x; i <= N; i += blockDim.x) S.cinc_cnt[i] = 0;
+    for (int i = threadIdx.x; i <= N; i += blockDim.x) row_ptr[i] = i < N ? 1 : 0;
     __syncthreads();
     for (int it = threadIdx.x; it < n_items; it += blockDim.x) {
         if (!item_active(S, it)) continue;
         int a, b;
         item_bodies(S, it, a, b);
         if (a == b) continue;
-        atomicAdd(&S.cinc_cnt[a], 1);
-        atomicAdd(&S.cinc_cnt[b], 1);
+        atomicAdd(&row_ptr[a], 1);
+        atomicAdd(&row_ptr[b], 1);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int i = 0; i < N; ++i) { row_ptr[i] = acc; acc += 1 + S.cinc_cnt[i]; }
-        row_ptr[N] = acc;
-        *nnzb = acc;
-        sh_cnt = acc;
+    {
+        int* const arr[1] = {row_ptr};
+        block_scan_excl<1>(arr, N, sh_scan);
     }
     __syncthreads();
-    if (sh_cnt > cap) return;
+    const int nblocks = row_ptr[N];
+    if (threadIdx.x == 0) *nnzb = nblocks;
+    if (nblocks > cap) return;
     for (int i = threadIdx.x; i < N; i += blockDim.x) {
         int pos = row_ptr[i];
         col_idx[pos] = i;
