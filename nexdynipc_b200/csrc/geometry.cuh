@@ -316,10 +316,12 @@ struct ContactRec {   // nxd_contact layout
 
 __device__ __forceinline__ double clamp01(double v) { return (v < 0.0) ? 0.0 : ((1.0 < v) ? 1.0 : v); }
 
-__device__ void closest_points_on_segments(V3 p1, V3 q1, V3 p2, V3 q2, V3& c1, V3& c2) {
+// closestPointsOnSegments (IPCSolver.cpp:32-90) given d1 = q1 - p1,
+// a = |d1|^2, d2 = q2 - p2, e = |d2|^2
+__device__ __forceinline__ void closest_points_core(V3 p1, V3 d1, double a, V3 p2, V3 d2, double e, V3& c1, V3& c2) {
     const double eps = 1e-12;
-    const V3 d1 = q1 - p1, d2 = q2 - p2, r = p1 - p2;
-    const double a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+    const V3 r = p1 - p2;
+    const double f = dot(d2, r);
     double s, t;
     if (a <= eps && e <= eps) { c1 = p1; c2 = p2; return; }
     if (a <= eps) {
@@ -340,6 +342,10 @@ __device__ void closest_points_on_segments(V3 p1, V3 q1, V3 p2, V3 q2, V3& c1, V
     }
     c1 = p1 + d1 * s;
     c2 = p2 + d2 * t;
+}
+__device__ __forceinline__ void closest_points_on_segments(V3 p1, V3 q1, V3 p2, V3 q2, V3& c1, V3& c2) {
+    const V3 d1 = q1 - p1, d2 = q2 - p2;
+    closest_points_core(p1, d1, dot(d1, d1), p2, d2, dot(d2, d2), c1, c2);
 }
 __device__ __forceinline__ V3 safe_normalized(V3 v, V3 fb) {
     const double n = norm(v);
@@ -501,6 +507,104 @@ __global__ void k_narrow_write(NarrowIn in, int kind, const int* item_off, const
             }
             __syncthreads();
         }
+    }
+}
+
+// Pass 1 for FV and EE with the pair's selected primitives staged in shared
+// memory: per face its first vertex, edge vectors, unit normal and the
+// barycentric Gram terms; per edge its start, direction, |d|^2, midpoint and
+// half length; per vertex its position.  Each item then repeats only the
+// per-item arithmetic of narrow_item, on the same operands, so its decision
+// equals narrow_item's.  An EE item whose segments' bounding spheres are
+// farther apart than dhat + 1e-9 cannot pass (the closest-point pair lies on
+// the segments up to rounding far below 1e-9) and is rejected first.
+constexpr int kFaceStage = 16, kEdgeStage = 12;
+__global__ void __launch_bounds__(256) k_narrow_count_staged(NarrowIn in, int kind, const int* item_off, unsigned char* flags,
+                                                             int* hit_cnt, const int* gate_zero) {
+    if (gate_zero && *gate_zero != 0) return;
+    __shared__ double prim[2][kTopK][kFaceStage];
+    __shared__ double vtx[2][kTopK][3];
+    __shared__ int red[8];
+    const int np = min(*in.npairs_ptr, in.cap);
+    const double dh = *in.dhat_ptr;
+    for (int p = blockIdx.x; p < np; p += gridDim.x) {
+        const int AB[2] = {in.pairs[2 * p], in.pairs[2 * p + 1]};
+        const int* T = in.topk + (size_t)p * 6 * kTopK;
+        const int* n = in.topn + 6 * p;
+        const int t0 = threadIdx.x;
+        if (t0 < 64) {
+            const int side = t0 >> 5, k = t0 & 31, body = AB[side];
+            const int vo = in.g.voff[body];
+            double* P = prim[side][k];
+            if (kind == 0 && k < n[4 + side]) {
+                const int* F = in.g.faces + 3 * (in.g.foff[body] + T[(4 + side) * kTopK + k]);
+                const V3 v0 = ld3(in.wv + 3 * (vo + F[0])), v1 = ld3(in.wv + 3 * (vo + F[1])), v2 = ld3(in.wv + 3 * (vo + F[2]));
+                const V3 e0 = v1 - v0, e1 = v2 - v0;
+                const V3 nn = safe_normalized(cross(e0, e1), v3(0, 1, 0));
+                const double d00 = dot(e0, e0), d01 = dot(e0, e1), d11 = dot(e1, e1);
+                st3(P, v0); st3(P + 3, e0); st3(P + 6, e1); st3(P + 9, nn);
+                P[12] = d00; P[13] = d01; P[14] = d11; P[15] = d00 * d11 - d01 * d01;
+            } else if (kind == 1 && k < n[2 + side]) {
+                const int* E = in.g.edges + 2 * (in.g.eoff[body] + T[(2 + side) * kTopK + k]);
+                const V3 a0 = ld3(in.wv + 3 * (vo + E[0])), a1 = ld3(in.wv + 3 * (vo + E[1]));
+                const V3 d = a1 - a0;
+                st3(P, a0); st3(P + 3, d); P[6] = dot(d, d);
+                st3(P + 7, 0.5 * (a0 + a1)); P[10] = 0.5 * norm(d);
+            }
+        } else if (t0 < 128 && kind == 0) {
+            const int side = (t0 - 64) >> 5, k = t0 & 31, body = AB[side];
+            if (k < n[side]) st3(vtx[side][k], ld3(in.wv + 3 * (in.g.voff[body] + T[side * kTopK + k])));
+        }
+        __syncthreads();
+        const int cnt = kind == 0 ? n[4] * n[1] + n[5] * n[0] : n[2] * n[3];
+        const int fv1 = n[4] * n[1];
+        const int off = item_off[p];
+        int h = 0;
+        for (int t = t0; t < cnt; t += blockDim.x) {
+            bool hit = false;
+            if (kind == 0) {
+                int fs, fi, vs_, vi;
+                if (t < fv1) { fs = 0; fi = t / n[1]; vs_ = 1; vi = t % n[1]; }
+                else { const int u = t - fv1; fs = 1; fi = u / n[0]; vs_ = 0; vi = u % n[0]; }
+                const double* P = prim[fs][fi];
+                const V3 a = ld3(P), nn = ld3(P + 9);
+                const V3 pp = ld3(vtx[vs_][vi]);
+                const double sd = dot(pp - a, nn);
+                if (!(fabs(sd) >= dh)) {
+                    // point_in_triangle(proj, v0, v1, v2) (IPCSolver.cpp:107-134)
+                    const V3 proj = pp - sd * nn;
+                    const V3 v2 = proj - a;
+                    const double d20 = dot(v2, ld3(P + 3)), d21 = dot(v2, ld3(P + 6));
+                    const double d00 = P[12], d01 = P[13], d11 = P[14], denom = P[15];
+                    if (!(fabs(denom) < 1e-16)) {
+                        const double v = (d11 * d20 - d01 * d21) / denom;
+                        const double w = (d00 * d21 - d01 * d20) / denom;
+                        const double u = 1.0 - v - w;
+                        hit = u >= -1e-8 && v >= -1e-8 && w >= -1e-8;
+                    }
+                }
+            } else {
+                const double* EA = prim[0][t / n[3]];
+                const double* EB = prim[1][t % n[3]];
+                const double lb = norm(ld3(EA + 7) - ld3(EB + 7)) - EA[10] - EB[10];
+                if (!(lb >= dh + 1e-9)) {
+                    V3 c0, c1;
+                    closest_points_core(ld3(EA), ld3(EA + 3), EA[6], ld3(EB), ld3(EB + 3), EB[6], c0, c1);
+                    hit = !(norm(c1 - c0) >= dh);
+                }
+            }
+            flags[off + t] = hit ? 1 : 0;
+            h += hit ? 1 : 0;
+        }
+        for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+        if ((t0 & 31) == 0) red[t0 >> 5] = h;
+        __syncthreads();
+        if (t0 == 0) {
+            int sum = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
+            hit_cnt[p] = sum;
+        }
+        __syncthreads();
     }
 }
 

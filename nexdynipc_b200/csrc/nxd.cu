@@ -69,6 +69,7 @@ struct nxd_ctx {
     std::vector<cudaEvent_t> pool;
     cudaStream_t stream = nullptr;
     int dev = 0, n_sm = 148;
+    int newton_grid = 1;   // co-resident CTAs of k_newton (power of two)
     int N = 0, nv = 0, nf = 0, ne = 0, J = 0, D = 0;
     int max_prims = 0;
     int pair_cap = 0;
@@ -174,6 +175,17 @@ void fill_solver(nxd_ctx* c) {
     S.alm_done = &c->sc->alm_done; S.status = &c->sc->status; S.newton_iters = &c->sc->newton_iters;
     S.converged = &c->sc->converged; S.ls_fail = &c->sc->ls_fail;
     S.alm_mcv = m.alloc<double>(1); S.alm_dual = m.alloc<double>(1);
+    S.solve_fail = m.alloc<int>(1);
+    S.bar_count = m.alloc<unsigned>(2); S.bar_abort = (int*)(S.bar_count + 1);
+    S.gpart = m.alloc<double>(2 * kRedMaxQ * kMaxNewtonGrid);
+    // one CTA of kNewtonThreads per 512 DOFs, a power of two no larger than
+    // what the device keeps co-resident
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newton, kNewtonThreads, 0);
+    const int coresident = std::max(1, per_sm * c->n_sm);
+    int g = 1;
+    while (g < kMaxNewtonGrid && g * 2 <= coresident && (long long)g * kNewtonThreads < 6LL * N) g *= 2;
+    c->newton_grid = g;
 }
 
 StepCfg step_cfg(const nxd_ctx* c) {
@@ -186,6 +198,15 @@ StepCfg step_cfg(const nxd_ctx* c) {
     k.alm_dual_tol = c->s.alm_dual_tol;
     k.alm_contact_tol = c->s.alm_contact_tol;
     return k;
+}
+
+// one ALM iteration's Newton solve: barrier counters zeroed, then a
+// cooperative launch of k_newton on c->newton_grid CTAs
+void launch_newton(nxd_ctx* c) {
+    ProfScope ps_(c, NXD_PROF_NEWTON);
+    cudaMemsetAsync(c->S.bar_count, 0, 2 * sizeof(unsigned), c->stream);
+    void* args[] = {(void*)&c->S};
+    cudaLaunchCooperativeKernel((const void*)k_newton, dim3(c->newton_grid), dim3(kNewtonThreads), args, 0, c->stream);
 }
 
 // ContactAssembler::build + world vertices at the current poses
@@ -235,10 +256,10 @@ void launch_narrow_full(nxd_ctx* c, const double* wv, const double* pose_p, cons
     const int blocks = c->n_sm * 8;
     int* skip_vv = c->i_scratch;
     const int* np = &c->sc->n_pairs;
-    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_count<<<blocks, 256, 0, c->stream>>>(in, 0, c->off_fv, c->flags, c->hit_cnt, skip_if););
+    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_count_staged<<<blocks, 256, 0, c->stream>>>(in, 0, c->off_fv, c->flags, c->hit_cnt, skip_if););
     NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->fv_hits, nullptr, skip_if, np););
     NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 0, c->off_fv, c->flags, c->hit_off, nullptr, c->contacts, skip_if););
-    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_count<<<blocks, 256, 0, c->stream>>>(in, 1, c->off_ee, c->flags, c->hit_cnt, skip_if););
+    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_count_staged<<<blocks, 256, 0, c->stream>>>(in, 1, c->off_ee, c->flags, c->hit_cnt, skip_if););
     NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->ee_hits, nullptr, skip_if, np););
     NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 1, c->off_ee, c->flags, c->hit_off, &c->sc->fv_hits, c->contacts,
                                                   skip_if););
@@ -305,7 +326,7 @@ nxd_status enqueue_step(nxd_ctx* c, double dt) {
     else NXD_LAUNCH(c, NXD_PROF_OTHER, k_contact_totals<<<1, 1, 0, st>>>(c->sc, 2, nullptr, nullptr));
     int* skip_detect = c->i_scratch + 1;
     for (int alm = 0; alm < c->s.alm_max_iters; ++alm) {
-        NXD_LAUNCH(c, NXD_PROF_NEWTON, k_newton<<<1, kSolverThreads, 0, st>>>(c->S););
+        launch_newton(c);
         NXD_LAUNCH(c, NXD_PROF_OTHER, k_alm_detect_gate<<<1, 1, 0, st>>>(c->sc, skip_detect););
         NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_pose_at_x<<<grid_for(c->N, 128), 128, 0, st>>>(c->N, c->x, c->quat, c->pose_p, c->pose_q););
         NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_world_vertices<<<grid_for(c->nv, 256), 256, 0, st>>>(c->geo, c->nv, c->vbody, c->pose_p, c->pose_q, c->wvx););

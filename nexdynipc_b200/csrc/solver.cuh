@@ -86,6 +86,10 @@ struct Solver {
     int* local;                                   // [N] body -> member index inside its component
     unsigned* mpool; long long mpool_cap; long long* mpool_off;   // per-component masks and lists
     double* pool; long long pool_cap; long long* pool_off;        // per-component L, D and rhs
+    int* solve_fail;                              // [1] zero pivot or capacity in this solve
+    // grid execution of k_newton
+    unsigned* bar_count; int* bar_abort;          // barrier arrivals and give-up flag, zeroed per launch
+    double* gpart;                                // [2 * kRedMaxQ * kMaxNewtonGrid] per-CTA partial sums
     // outputs / state
     int* alm_done; int* status; int* newton_iters; int* converged; int* ls_fail;
     double* alm_mcv; double* alm_dual;
@@ -96,31 +100,35 @@ struct Solver {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int pow2_ceil(int n) { int p = 1; while (p < n) p <<= 1; return p; }
 
-// Block reductions for 1024-thread CTAs.
+// Block reductions.
 //
 // The fixed tree over n values pads to P = pow2 >= n with zeros and runs
-// v[i] += v[i + h] for h = P/2 .. 1.  Padding further (to P >= 1024) only adds
-// exact zeros at the top levels, so take P >= 1024.  After the levels with
-// h >= 32, v[r] (r < 32) is the same tree over the residue class
-// {r + 32 m}; after the levels with h >= 1024 inside that class, its element
-// m = l + 32 j reduces to the tree over j of v[r + 32 l + 1024 j].  So warp r,
-// lane l folds j (K = P / 1024 values, the stride tree = the contiguous
-// pairwise tree over the bit-reversed index, kept as a stack of partial sums),
-// the lanes finish class r with shuffles (h = 16 .. 1), and the 32 class sums
-// go through shared memory once for the last five levels.  The result is the
-// same double as the plain loop, with one __syncthreads per call.
-constexpr int kRedMaxQ = 6;
+// v[i] += v[i + h] for h = P/2 .. 1.  Padding further only adds exact zeros
+// at the top levels, so take P >= the number of threads T.  After the levels
+// with h >= nw (the warp count), v[w] is the same tree over the residue class
+// {w + nw m}; inside that class, after its levels with stride >= 32 nw,
+// element m = l + 32 j reduces to the tree over j of v[w + nw l + T j].  So
+// warp w, lane l folds j (K = P / T values; the stride tree is the
+// contiguous pairwise tree over the bit-reversed index, kept as a stack of
+// partial sums), the lanes finish class w with shuffles (h = 16 .. 1), and
+// the nw class sums go through shared memory once for the last levels.  The
+// result is the same double as the plain loop, with one __syncthreads.
+constexpr int kRedMaxQ = 8;
 
+// Fold of the K = P / stride values f(base + stride * m), m < K (P = the
+// padded length, a power of two >= stride), in stride-tree order: the
+// contiguous pairwise tree over the bit-reversed m, kept as a stack of
+// partial sums.  Elements at or past n are zero.
 template <typename F>
-__device__ __forceinline__ double lane_fold(int n, int base, F f) {
-    const int P = max(pow2_ceil(max(n, 1)), 1024);
-    const int K = P >> 10;
+__device__ __forceinline__ double lane_fold(int n, int base, int stride, F f) {
+    const int P = max(pow2_ceil(max(n, 1)), stride);
+    const int K = P / stride;
     if (K == 1) return base < n ? f(base) : 0.0;
     const int lg = 31 - __clz(K);
     double stk[24];
     int top = 0;
     for (int j = 0; j < K; ++j) {
-        const int e = base + (int)((__brev((unsigned)j) >> (32 - lg)) << 10);
+        const int e = base + stride * (int)(__brev((unsigned)j) >> (32 - lg));
         double v = e < n ? f(e) : 0.0;
         for (int c = j + 1; !(c & 1); c >>= 1) v = stk[--top] + v;
         stk[top++] = v;
@@ -132,25 +140,28 @@ __device__ __forceinline__ double warp_tree(double v) {
     return __shfl_sync(0xffffffffu, v, 0);
 }
 
-// Reduction scratch of one CTA: two alternating buffers of kRedMaxQ x 32
-// class sums, so that a call's writes never meet the previous call's reads.
+// Reduction scratch of one CTA (blockDim a power of two >= 32, nw warps):
+// warp w, lane l folds the elements w + nw l + blockDim j; two alternating
+// buffers of class sums, so that a call's writes never meet the previous
+// call's reads.
 struct BlockRed {
     double* sh;      // 2 * kRedMaxQ * 32 doubles of shared memory
     int parity;
     template <int Q, typename F>
     __device__ void sums(const int (&n)[Q], F f, double (&out)[Q]) {
         static_assert(Q <= kRedMaxQ, "too many simultaneous reductions");
-        const int r = threadIdx.x >> 5, l = threadIdx.x & 31;
+        const int B = blockDim.x, nw = B >> 5;
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
         double* buf = sh + parity * (kRedMaxQ * 32);
         parity ^= 1;
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            const double v = warp_tree(lane_fold(n[q], r + 32 * l, [&](int e) { return f(q, e); }));
-            if (l == 0) buf[q * 32 + r] = v;
+            const double v = warp_tree(lane_fold(n[q], w + nw * l, B, [&](int e) { return f(q, e); }));
+            if (l == 0) buf[q * 32 + w] = v;
         }
         __syncthreads();
 #pragma unroll
-        for (int q = 0; q < Q; ++q) out[q] = warp_tree(buf[q * 32 + l]);
+        for (int q = 0; q < Q; ++q) out[q] = warp_tree(l < nw ? buf[q * 32 + l] : 0.0);
     }
     template <typename F>
     __device__ double sum(int n, F f) {
@@ -165,7 +176,7 @@ struct BlockRed {
         parity ^= 1;
         if ((threadIdx.x & 31) == 0) buf[threadIdx.x >> 5] = v;
         __syncthreads();
-        double w = buf[threadIdx.x & 31];
+        double w = (threadIdx.x & 31) < (blockDim.x >> 5) ? buf[threadIdx.x & 31] : 0.0;
         for (int o = 16; o > 0; o >>= 1) w = dmax(w, __shfl_xor_sync(0xffffffffu, w, o));
         return w;
     }
@@ -177,12 +188,13 @@ struct BlockRed {
     name.parity = 0
 
 // Exclusive prefix sums of Q int arrays of length n, in place allowed; a[n]
-// receives the total.  Thread t scans the chunk [t c, t c + c), c = ceil(n /
-// 1024).  sh: 32 Q ints.  The caller synchronises before reading the result.
+// receives the total.  Thread t of the CTA scans the chunk [t c, t c + c),
+// c = ceil(n / blockDim).  sh: 32 Q ints.  The caller synchronises before
+// reading the result.
 template <int Q>
 __device__ void block_scan_excl(int* const (&a)[Q], int n, int* sh) {
-    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    const int c = (n + 1023) >> 10;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5, nw = blockDim.x >> 5;
+    const int c = (n + blockDim.x - 1) / blockDim.x;
     const int b0 = min(n, t * c), b1 = min(n, b0 + c);
     int v[Q], incl[Q];
 #pragma unroll
@@ -198,9 +210,10 @@ __device__ void block_scan_excl(int* const (&a)[Q], int n, int* sh) {
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-        int x = sh[q * 32 + lane];
+        int x = lane < nw ? sh[q * 32 + lane] : 0;
         for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
-        const int wbase = __shfl_sync(0xffffffffu, x, (w + 31) & 31) * (w > 0 ? 1 : 0);
+        const int prev = __shfl_sync(0xffffffffu, x, (w + 31) & 31);
+        const int wbase = w > 0 ? prev : 0;
         const int total = __shfl_sync(0xffffffffu, x, 31);
         int run = wbase + incl[q] - v[q];
         for (int i = b0; i < b1; ++i) { const int e = a[q][i]; a[q][i] = run; run += e; }
@@ -1216,37 +1229,190 @@ __device__ int solve_component(const Solver& S, int root, double s, int C) {
     return 0;
 }
 
-// Solve H dx = -g.  Returns false (all threads) on failure.
-__device__ bool solve_newton_system(const Solver& S, double s, int C, int* sh_flag, int* sh_next, int* sh_scan) {
+// ---------------------------------------------------------------------------
+// Grid-wide execution of the Newton solve: G co-resident CTAs (cooperative
+// launch, G a power of two), one counting barrier in global memory with a
+// bounded wait.  G = 1 degenerates to __syncthreads.
+// ---------------------------------------------------------------------------
+constexpr int kNewtonThreads = 512;
+constexpr int kMaxNewtonGrid = 64;
+constexpr unsigned kBarrierSpinLimit = 1u << 24;   // x >= 64 ns sleeps: about a second
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+struct GridCtx {
+    int G, b, gtid, gthreads;
+    unsigned* count;      // arrivals, zeroed before each launch
+    int* abort;           // set by a CTA whose wait ran out
+    int* status;
+    unsigned target;
+    int* sh_ok;           // shared: 0 once this CTA has given up
+    __device__ bool sync() {
+        if (G == 1) { __syncthreads(); return true; }
+        target += G;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int ok = *sh_ok;
+            if (ok) {
+                __threadfence();
+                atomicAdd(count, 1u);
+                unsigned spins = 0;
+                while (ld_acquire_u32(count) < target) {
+                    if (++spins > kBarrierSpinLimit || *(volatile int*)abort) {
+                        ok = 0;
+                        atomicExch(abort, 1);
+                        atomicExch(status, NXD_TIMEOUT);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                __threadfence();
+            }
+            *sh_ok = ok;
+        }
+        __syncthreads();
+        return *sh_ok != 0;
+    }
+};
+
+// Fixed-tree sums over the grid: CTA b reduces the residue class b mod G
+// (elements b + G m) with the block scheme, the G class sums go through
+// global memory once (one barrier), every CTA finishes the last log2 G
+// levels itself.  Same double as the plain loop over the padded length.
+struct GridRed {
+    GridCtx* gc;
+    double* sh;           // shared: kRedMaxQ * 32
+    double* part;         // global: 2 * kRedMaxQ * kMaxNewtonGrid
+    int parity;
+    template <int Q, typename F>
+    __device__ void sums(const int (&n)[Q], F f, double (&out)[Q]) {
+        static_assert(Q <= kRedMaxQ, "too many simultaneous reductions");
+        const int G = gc->G, b = gc->b, B = blockDim.x, nw = B >> 5;
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        double* gp = part + parity * (kRedMaxQ * kMaxNewtonGrid);
+        parity ^= 1;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const double v = warp_tree(lane_fold(n[q], b + G * (w + nw * l), G * B, [&](int e) { return f(q, e); }));
+            if (l == 0) sh[q * 32 + w] = v;
+        }
+        __syncthreads();
+        if (w == 0) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const double t = warp_tree(l < nw ? sh[q * 32 + l] : 0.0);
+                if (l == 0) { if (G == 1) sh[q * 32] = t; else gp[q * kMaxNewtonGrid + b] = t; }
+            }
+        }
+        gc->sync();
+        if (G == 1) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) out[q] = sh[q * 32];
+            __syncthreads();
+            return;
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            out[q] = warp_tree(lane_fold(G, l, 32, [&](int e) { return __ldcg(gp + q * kMaxNewtonGrid + e); }));
+    }
+    __device__ double max(double v) {
+        const int G = gc->G, b = gc->b;
+        for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        double* gp = part + parity * (kRedMaxQ * kMaxNewtonGrid);
+        parity ^= 1;
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double w = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) w = dmax(w, __shfl_xor_sync(0xffffffffu, w, o));
+            if (threadIdx.x == 0) { if (G == 1) sh[0] = w; else gp[b] = w; }
+        }
+        gc->sync();
+        if (G == 1) { const double r = sh[0]; __syncthreads(); return r; }
+        double w = 0.0;
+        for (int e = threadIdx.x & 31; e < G; e += 32) w = dmax(w, __ldcg(gp + e));
+        for (int o = 16; o > 0; o >>= 1) w = dmax(w, __shfl_xor_sync(0xffffffffu, w, o));
+        return w;
+    }
+};
+
+// grid-strided loop over [0, n)
+#define NX_GRID_FOR(e, n, gc) for (int e = (gc).gtid; e < (n); e += (gc).gthreads)
+
+// poses (and the x <- xt copy after an accepted step) for every body
+__device__ void grid_poses(const Solver& S, const double* x, const GridCtx& gc) {
+    NX_GRID_FOR(i, S.N, gc) {
+        const Q q0 = ldq(S.quat0 + 4 * i);
+        const V3 th = xs3(x, 6 * i + 3);
+        stq(S.qj + 4 * i, rot_joint(q0, th));
+        stq(S.qg + 4 * i, rot_gt(q0, th));
+    }
+}
+
+// computeValue and computeContactValue at x from one set of fixed-tree sums;
+// poses at x and the drives' value call must be done.
+__device__ void grid_energies(const Solver& S, const double* x, double s, int C, GridRed& R, double& full,
+                              double& contact) {
+    const bool bar = *S.barrier_in_forms_ptr != 0, fr = *S.friction_form_ptr != 0;
+    const double dh = *S.bdhat_ptr, kap = *S.bkappa_ptr;
+    const int n[5] = {S.N, S.N, S.J, bar ? C : 0, fr ? C : 0};
+    double sum[5];
+    R.sums<5>(n, [&](int q, int e) -> double {
+        switch (q) {
+            case 0: return inertia_value(S, e, x);
+            case 1: return gravity_value(S, e, x);
+            case 2: { double Cj[6]; const int dim = joint_residual(S, e, x, Cj, nullptr); return joint_energy(S, e, Cj, dim); }
+            case 3: return barrier_value(contact_distance(S.contacts[e], x), dh, kap);
+            default: return friction_value(S, e, x);
+        }
+    }, sum);
+    double v = sum[0];
+    v += s * sum[1];
+    v += sum[2];
+    for (int d = 0; d < S.D; ++d) v += s * S.dE[d];
+    if (S.D > 0) R.gc->sync();   // dE is rewritten by the next value call
+    double c = 0.0;
+    if (bar) { v += s * sum[3]; c += s * sum[3]; }
+    if (fr) { v += s * sum[4]; c += s * sum[4]; }
+    full = v;
+    contact = c;
+}
+
+// Solve H dx = -g over the grid.  Returns false (all threads) on failure.
+__device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, int* sh_scan, int* sh_flag) {
     const int N = S.N;
     const int n_items = S.J + 2 * C;
-    for (int i = threadIdx.x; i <= N; i += blockDim.x) {
+    NX_GRID_FOR(i, N + 1, gc) {
         if (i < N) S.parent[i] = i;
         S.mcnt[i] = 0; S.icnt[i] = 0; S.rflag[i] = 0;
     }
-    if (threadIdx.x == 0) { *sh_flag = 0; *sh_next = 0; *S.mpool_off = 0; *S.pool_off = 0; }
-    __syncthreads();
-    for (int it = threadIdx.x; it < n_items; it += blockDim.x) {
+    if (gc.gtid == 0) { *S.comp_next = 0; *S.mpool_off = 0; *S.pool_off = 0; *S.solve_fail = 0; }
+    gc.sync();
+    NX_GRID_FOR(it, n_items, gc) {
         if (!item_active(S, it)) continue;
         int a, b;
         item_bodies(S, it, a, b);
         if (a != b) uf_union(S.parent, a, b);
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    gc.sync();
+    NX_GRID_FOR(i, N, gc) {
         const int r = uf_find(S.parent, i);
         S.comp[i] = r;
         atomicAdd(&S.mcnt[r], 1);
     }
-    for (int it = threadIdx.x; it < n_items; it += blockDim.x) {
+    NX_GRID_FOR(it, n_items, gc) {
         if (!item_active(S, it)) continue;
         int a, b;
         item_bodies(S, it, a, b);
         if (a != b) atomicAdd(&S.icnt[uf_find(S.parent, a)], 1);
     }
-    __syncthreads();
+    gc.sync();
     // singletons: one thread each, in registers
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    NX_GRID_FOR(i, N, gc) {
         const bool multi = S.comp[i] == i && S.mcnt[i] >= 2;
         S.rflag[i] = multi ? 1 : 0;
         if (S.comp[i] != i || S.mcnt[i] != 1) continue;
@@ -1255,32 +1421,32 @@ __device__ bool solve_newton_system(const Solver& S, double s, int C, int* sh_fl
         for (int e = 0; e < 36; ++e) A[e] = S.Hd[36 * i + e];
 #pragma unroll
         for (int e = 0; e < 6; ++e) b[e] = -S.g[6 * i + e];
-        if (!ldlt6_solve(A, b)) { atomicExch(sh_flag, 1); continue; }
+        if (!ldlt6_solve(A, b)) { atomicExch(S.solve_fail, 1); continue; }
 #pragma unroll
         for (int e = 0; e < 6; ++e) S.dx[6 * i + e] = b[e];
     }
-    __syncthreads();
+    gc.sync();
     NX_PHASE(3);
-    for (int i = threadIdx.x; i < N; i += blockDim.x)
-        if (!S.rflag[i]) S.mcnt[i] = 0;
-    __syncthreads();
-    {
+    if (gc.b == 0) {
+        for (int i = threadIdx.x; i < N; i += blockDim.x)
+            if (!S.rflag[i]) S.mcnt[i] = 0;
+        __syncthreads();
         int* const arr[3] = {S.mcnt, S.icnt, S.rflag};
         block_scan_excl<3>(arr, N, sh_scan);
     }
-    __syncthreads();
-    const int n_comp = S.rflag[N];
-    for (int r = threadIdx.x; r < N; r += blockDim.x) {
+    gc.sync();
+    const int n_comp = __ldcg(S.rflag + N);
+    NX_GRID_FOR(r, N, gc) {
         if (S.rflag[r + 1] != S.rflag[r]) S.comp_root[S.rflag[r]] = r;
         S.local[r] = 0;    // member cursor per root
         S.parent[r] = 0;   // item cursor per root
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    gc.sync();
+    NX_GRID_FOR(i, N, gc) {
         const int r = S.comp[i];
         if (S.mcnt[r + 1] - S.mcnt[r] >= 2) S.members[S.mcnt[r] + atomicAdd(&S.local[r], 1)] = i;
     }
-    for (int it = threadIdx.x; it < n_items; it += blockDim.x) {
+    NX_GRID_FOR(it, n_items, gc) {
         if (!item_active(S, it)) continue;
         int a, b;
         item_bodies(S, it, a, b);
@@ -1288,38 +1454,50 @@ __device__ bool solve_newton_system(const Solver& S, double s, int C, int* sh_fl
         const int r = S.comp[a];
         S.items[S.icnt[r] + atomicAdd(&S.parent[r], 1)] = it;
     }
-    __syncthreads();
+    gc.sync();
     NX_PHASE(3);
-    // multi-body components: one warp each, taken from a shared counter
+    // multi-body components: one warp each, taken from a global counter
     const int lane = threadIdx.x & 31;
     for (;;) {
         int o = 0;
-        if (lane == 0) o = atomicAdd(sh_next, 1);
+        if (lane == 0) o = atomicAdd(S.comp_next, 1);
         o = __shfl_sync(0xffffffffu, o, 0);
         if (o >= n_comp) break;
         const int rc = solve_component(S, S.comp_root[o], s, C);
         if (rc != 0 && lane == 0) {
-            atomicExch(sh_flag, 1);
+            atomicExch(S.solve_fail, 1);
             if (rc == 2) atomicExch(S.status, NXD_CAPACITY);
         }
     }
-    __syncthreads();
+    gc.sync();
     NX_PHASE(4);
+    if (threadIdx.x == 0) *sh_flag = __ldcg(S.solve_fail);
+    __syncthreads();
     const bool fail = *sh_flag != 0;
     __syncthreads();
     return !fail;
 }
 
 // ---------------------------------------------------------------------------
-// The kernel: one ALM iteration's Newton solve + joint bookkeeping.
+// The kernel: one ALM iteration's Newton solve + joint bookkeeping, on G
+// co-resident CTAs (every branch below depends only on grid-reduced values,
+// so all CTAs take the same path and meet at every barrier).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kSolverThreads) k_newton(Solver S) {
+__global__ void __launch_bounds__(kNewtonThreads) k_newton(Solver S) {
     __shared__ unsigned long long sh_keys[kMaxIncidence];
+    __shared__ double sh_red[kRedMaxQ * 32];
     __shared__ int sh_scan[3 * 32];
-    __shared__ int sh_flag, sh_next;
-    NX_BLOCK_RED(R);
+    __shared__ int sh_flag, sh_ok;
     if (*S.alm_done) return;
     NX_PHASE_START();
+    GridCtx gc;
+    gc.G = gridDim.x; gc.b = blockIdx.x;
+    gc.gtid = blockIdx.x * blockDim.x + threadIdx.x; gc.gthreads = gridDim.x * blockDim.x;
+    gc.count = S.bar_count; gc.abort = S.bar_abort; gc.status = S.status; gc.target = 0; gc.sh_ok = &sh_ok;
+    if (threadIdx.x == 0) sh_ok = 1;
+    __syncthreads();
+    GridRed R;
+    R.gc = &gc; R.sh = sh_red; R.part = S.gpart; R.parity = 0;
     const int N = S.N;
     const int C = *S.ncontacts_ptr;
     const double dt = *S.dt_ptr;
@@ -1327,25 +1505,28 @@ __global__ void __launch_bounds__(kSolverThreads) k_newton(Solver S) {
     const int n6 = 6 * N;
     const bool bar = *S.barrier_in_forms_ptr != 0, fr = *S.friction_form_ptr != 0;
     const double dh = *S.bdhat_ptr;
-    build_contact_incidence(S, C, sh_keys);
+    if (gc.b == 0) build_contact_incidence(S, C, sh_keys);
+    if (!gc.sync()) return;
     NX_PHASE(0);
 
-    bool converged = false;
+    bool converged = false, poses_at_x = false, aborted = false;
     int iters = 0;
     for (int iter = 0; iter < S.newton_max_iters; ++iter) {
         iters = iter;
         // gradient at x (drives: gradient call)
-        eval_poses(S, S.x);
-        for (int d = threadIdx.x; d < S.D; d += blockDim.x) drive_eval(S, d, S.x, 1);
-        __syncthreads();
-        for (int j = threadIdx.x; j < S.J; j += blockDim.x) joint_eval(S, j, S.x, true);
-        for (int c = threadIdx.x; c < C; c += blockDim.x) {
+        if (!poses_at_x) grid_poses(S, S.x, gc);
+        poses_at_x = true;
+        NX_GRID_FOR(d, S.D, gc) drive_eval(S, d, S.x, 1);
+        if (!gc.sync()) { aborted = true; break; }
+        NX_GRID_FOR(e, S.J + C, gc) {
+            if (e < S.J) { joint_eval(S, e, S.x, true); continue; }
+            const int c = e - S.J;
             if (bar) barrier_eval(S, c, S.x);
             if (fr) friction_eval(S, c, S.x, true);
         }
-        __syncthreads();
+        if (!gc.sync()) { aborted = true; break; }
         double gm = 0.0;
-        for (int e = threadIdx.x; e < n6; e += blockDim.x) {
+        NX_GRID_FOR(e, n6, gc) {
             double g, cg;
             gradient_dof(S, S.x, s, e / 6, e % 6, bar, fr, dh, g, cg);
             S.g[e] = g;
@@ -1356,52 +1537,76 @@ __global__ void __launch_bounds__(kSolverThreads) k_newton(Solver S) {
         NX_PHASE(1);
         if (gm < S.newton_tol) { converged = true; break; }
         // Hessian (drives: hessian call)
-        for (int d = threadIdx.x; d < S.D; d += blockDim.x) drive_eval(S, d, S.x, 2);
-        __syncthreads();
-        gather_diag_hessian(S, s, C);
-        __syncthreads();
-        NX_PHASE(2);
-        if (!solve_newton_system(S, s, C, &sh_flag, &sh_next, sh_scan)) break;
-        // line search (max step 1)
-        const double fx = energy_total(S, S.x, s, C, false, R);
-        double dd[2];
-        {
-            const int nn[2] = {n6, n6};
-            R.sums<2>(nn, [&](int q, int e) { return (q == 0 ? S.g[e] : S.cg[e]) * S.dx[e]; }, dd);
+        if (S.D > 0) {
+            NX_GRID_FOR(d, S.D, gc) drive_eval(S, d, S.x, 2);
+            gc.sync();
         }
-        const double descent = dd[0], cdesc = dd[1];
-        const double fc = energy_total(S, S.x, s, C, true, R);
+        {
+            const bool b2 = bar, f2 = fr;
+            NX_GRID_FOR(e, n6, gc) {
+                double H[6];
+                diag_hessian_row(S, s, e / 6, e % 6, b2, f2, dh, H);
+                for (int k = 0; k < 6; ++k) S.Hd[6 * e + k] = H[k];
+            }
+        }
+        if (!gc.sync()) { aborted = true; break; }
+        NX_PHASE(2);
+        if (!grid_solve(S, s, C, gc, sh_scan, &sh_flag)) break;
+        // line search (max step 1): the value calls at x, then descent terms
+        if (S.D > 0) {
+            NX_GRID_FOR(d, S.D, gc) drive_eval(S, d, S.x, 0);
+            gc.sync();
+        }
+        double fx, fc, descent, cdesc;
+        {
+            grid_energies(S, S.x, s, C, R, fx, fc);
+            const int nn[2] = {n6, n6};
+            double dd[2];
+            R.sums<2>(nn, [&](int q, int e) { return (q == 0 ? S.g[e] : S.cg[e]) * S.dx[e]; }, dd);
+            descent = dd[0];
+            cdesc = dd[1];
+        }
         NX_PHASE(5);
-        if (descent > 0) { if (threadIdx.x == 0) atomicAdd(S.ls_fail, 1); break; }
+        if (descent > 0) { if (gc.gtid == 0) atomicAdd(S.ls_fail, 1); poses_at_x = true; break; }
         double alpha = 1.0;
         bool done = false;
         for (int ls = 0; ls < S.ls_max_iters; ++ls) {
-            for (int e = threadIdx.x; e < n6; e += blockDim.x) S.xt[e] = S.x[e] + alpha * S.dx[e];
-            __syncthreads();
-            const double fn = energy_total(S, S.xt, s, C, false, R);
-            const double fcn = energy_total(S, S.xt, s, C, true, R);
+            NX_GRID_FOR(i, N, gc) {
+                for (int k = 0; k < 6; ++k) S.xt[6 * i + k] = S.x[6 * i + k] + alpha * S.dx[6 * i + k];
+                const Q q0 = ldq(S.quat0 + 4 * i);
+                const V3 th = xs3(S.xt, 6 * i + 3);
+                stq(S.qj + 4 * i, rot_joint(q0, th));
+                stq(S.qg + 4 * i, rot_gt(q0, th));
+            }
+            NX_GRID_FOR(d, S.D, gc) drive_eval(S, d, S.xt, 0);
+            gc.sync();
+            double fn, fcn;
+            grid_energies(S, S.xt, s, C, R, fn, fcn);
             const bool cok = cdesc <= 0.0 ? (fcn <= fc + S.ls_c1 * alpha * cdesc) : (fcn <= fc);
             if (fn <= fx + S.ls_c1 * alpha * descent && cok) { done = true; break; }
             alpha *= S.ls_rho;
         }
         NX_PHASE(6);
-        if (!done) { if (threadIdx.x == 0) atomicAdd(S.ls_fail, 1); break; }
-        for (int e = threadIdx.x; e < n6; e += blockDim.x) S.x[e] = S.xt[e];
-        __syncthreads();
+        if (!done) { if (gc.gtid == 0) atomicAdd(S.ls_fail, 1); poses_at_x = false; break; }
+        // accept: x <- xt (each body by the thread that posed it)
+        NX_GRID_FOR(i, N, gc)
+            for (int k = 0; k < 6; ++k) S.x[6 * i + k] = S.xt[6 * i + k];
+        poses_at_x = true;
+        if (S.D > 0) gc.sync();   // the drives' next gradient call reads any body's x
         if (iter == S.newton_max_iters - 1) iters = S.newton_max_iters;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    if (aborted) return;
+    if (gc.gtid == 0) {
         atomicAdd(S.newton_iters, iters);
         *S.converged = converged ? 1 : 0;
     }
     // ALM: violation, hardening, lambda update (IPCSolver.cpp:1084-1110);
     // each joint hardens with its own pre-update stiffness, then takes
     // lambda += mu_new C
-    eval_poses(S, S.x);
-    __syncthreads();
+    if (!poses_at_x) grid_poses(S, S.x, gc);
+    if (!gc.sync()) return;
     double mcv = 0.0, dual = 0.0;
-    for (int j = threadIdx.x; j < S.J; j += blockDim.x) {
+    NX_GRID_FOR(j, S.J, gc) {
         double Cj[6];
         const int dim = joint_residual(S, j, S.x, Cj, nullptr);
         for (int k = 0; k < 6; ++k) S.jC[6 * j + k] = Cj[k];
@@ -1423,15 +1628,16 @@ __global__ void __launch_bounds__(kSolverThreads) k_newton(Solver S) {
     }
     mcv = R.max(mcv);
     dual = R.max(dual);
-    if (threadIdx.x == 0) {
+    if (gc.gtid == 0) {
         *S.alm_mcv = mcv;
         *S.alm_dual = dual;
     }
     NX_PHASE(7);
 #ifdef NXD_PHASE_TIMERS
-    if (threadIdx.x == 0)
-        printf("PH C=%d it=%d init=%lld grad=%lld hess=%lld symb=%lld comp=%lld ls0=%lld ls=%lld post=%lld\n", C, iters,
-               nx_ph_acc[0], nx_ph_acc[1], nx_ph_acc[2], nx_ph_acc[3], nx_ph_acc[4], nx_ph_acc[5], nx_ph_acc[6], nx_ph_acc[7]);
+    if (gc.gtid == 0)
+        printf("PH G=%d C=%d it=%d init=%lld grad=%lld hess=%lld symb=%lld comp=%lld ls0=%lld ls=%lld post=%lld\n", gc.G, C,
+               iters, nx_ph_acc[0], nx_ph_acc[1], nx_ph_acc[2], nx_ph_acc[3], nx_ph_acc[4], nx_ph_acc[5], nx_ph_acc[6],
+               nx_ph_acc[7]);
 #endif
 }
 
