@@ -441,170 +441,274 @@ __device__ bool narrow_item(const NarrowIn& in, int kind, int p, int t, ContactR
     return true;
 }
 
-// Pass 1: hit flags per item and hit counts per pair.  One block per pair.
-__global__ void k_narrow_count(NarrowIn in, int kind, const int* item_off, unsigned char* flags, int* hit_cnt,
-                               const int* gate_zero) {
-    if (gate_zero && *gate_zero != 0) return;
-    const int np = min(*in.npairs_ptr, in.cap);
-    __shared__ int red[32];
-    for (int p = blockIdx.x; p < np; p += gridDim.x) {
-        const int* n = in.topn + 6 * p;
-        const int cnt = kind == 0 ? n[4] * n[1] + n[5] * n[0] : (kind == 1 ? n[2] * n[3] : n[0] * n[1]);
-        const int off = item_off[p];
-        int h = 0;
-        for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-            const bool hit = narrow_item(in, kind, p, t, nullptr);
-            flags[off + t] = hit ? 1 : 0;
-            h += hit ? 1 : 0;
-        }
-        for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = h;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int s = 0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-            hit_cnt[p] = s;
-        }
-        __syncthreads();
-    }
+// ---------------------------------------------------------------------------
+// Narrow-phase passes over the implicit candidate grids of each pair.
+//
+// A pair's items form grids in the order of ContactAssembler.cpp:304-341:
+// FV side 0 = faces of A x vertices of B, FV side 1 = faces of B x vertices
+// of A, EE = edges of A x edges of B, VV = vertices of A x vertices of B;
+// item t = row * ncols + col.  One warp owns a pair.  Each lane keeps one row
+// primitive (a face, an A-edge or an A-vertex) in registers and walks the
+// columns, whose operands the warp stages in shared memory (SoA) and reads
+// as broadcasts.  The hits of column c form one 32-bit ballot (bit = row);
+// lane c keeps that word in a register and the warp stores its masks only
+// when the pair has hits.  Every decision repeats narrow_item's arithmetic on
+// the same operands, so the two always agree.
+// ---------------------------------------------------------------------------
+constexpr int kMaskWords = 3 * kTopK;   // per pair: FV side 0 | FV side 1 | EE (VV reuses the first 32)
+constexpr int kRowsWarps = 4;           // warps per block of k_narrow_rows
+constexpr int kEmitWarps = 8;           // warps per block of k_narrow_emit
+
+struct NarrowScratch {
+    unsigned* mask;        // [cap * kMaskWords] column hit masks
+    int* cnt;              // [2 * cap] hits per pair: FV | EE (VV uses the FV half)
+    int* off;              // [2 * cap] exclusive prefixes of cnt, per half
+};
+
+struct FaceRegs { V3 v0, e0, e1, nn; double d00, d01, d11, denom; };
+
+__device__ __forceinline__ FaceRegs load_face(const NarrowIn& in, int body, int face) {
+    const int* F = in.g.faces + 3 * (in.g.foff[body] + face);
+    const int vo = in.g.voff[body];
+    FaceRegs f;
+    f.v0 = ld3(in.wv + 3 * (vo + F[0]));
+    const V3 v1 = ld3(in.wv + 3 * (vo + F[1])), v2 = ld3(in.wv + 3 * (vo + F[2]));
+    f.e0 = v1 - f.v0; f.e1 = v2 - f.v0;
+    f.nn = safe_normalized(cross(f.e0, f.e1), v3(0, 1, 0));
+    f.d00 = dot(f.e0, f.e0); f.d01 = dot(f.e0, f.e1); f.d11 = dot(f.e1, f.e1);
+    f.denom = f.d00 * f.d11 - f.d01 * f.d01;
+    return f;
 }
 
-// Pass 2: write hits in item order at base + hit_off[p] (positions past the
-// raw cap are dropped, as append_contact does).
-__global__ void k_narrow_write(NarrowIn in, int kind, const int* item_off, const unsigned char* flags, const int* hit_off,
-                               const int* base_ptr, ContactRec* out, const int* gate_zero) {
-    if (gate_zero && *gate_zero != 0) return;
-    const int np = min(*in.npairs_ptr, in.cap);
-    __shared__ int wsum[32];
-    __shared__ int carry;
-    const int base = base_ptr ? *base_ptr : 0;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int p = blockIdx.x; p < np; p += gridDim.x) {
-        const int* n = in.topn + 6 * p;
-        const int cnt = kind == 0 ? n[4] * n[1] + n[5] * n[0] : (kind == 1 ? n[2] * n[3] : n[0] * n[1]);
-        const int off = item_off[p];
-        if (threadIdx.x == 0) carry = base + hit_off[p];
-        __syncthreads();
-        for (int b0 = 0; b0 < cnt; b0 += blockDim.x) {
-            const int t = b0 + threadIdx.x;
-            const int f = t < cnt ? flags[off + t] : 0;
-            const unsigned bal = __ballot_sync(0xffffffffu, f);
-            if (lane == 0) wsum[wid] = __popc(bal);
-            __syncthreads();
-            int pre = 0;
-            for (int w = 0; w < wid; ++w) pre += wsum[w];
-            const int pos = carry + pre + __popc(bal & ((1u << lane) - 1u));
-            if (f && pos < kMaxRawContacts) {
-                ContactRec r;
-                narrow_item(in, kind, p, t, &r);
-                out[pos] = r;
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                int tot = 0;
-                for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += wsum[w];
-                carry += tot;
-            }
-            __syncthreads();
-        }
-    }
+// FV decision of narrow_item: |plane distance| < dhat and the projection
+// passes point_in_triangle (IPCSolver.cpp:107-134).
+__device__ __forceinline__ bool fv_hit(const FaceRegs& f, V3 pp, double dh) {
+    const double sd = dot(pp - f.v0, f.nn);
+    if (fabs(sd) >= dh) return false;
+    const V3 proj = pp - sd * f.nn;
+    const V3 w2 = proj - f.v0;
+    const double d20 = dot(w2, f.e0), d21 = dot(w2, f.e1);
+    if (fabs(f.denom) < 1e-16) return false;
+    const double v = (f.d11 * d20 - f.d01 * d21) / f.denom;
+    const double w = (f.d00 * d21 - f.d01 * d20) / f.denom;
+    const double u = 1.0 - v - w;
+    return u >= -1e-8 && v >= -1e-8 && w >= -1e-8;
 }
 
-// Pass 1 for FV and EE with the pair's selected primitives staged in shared
-// memory: per face its first vertex, edge vectors, unit normal and the
-// barycentric Gram terms; per edge its start, direction, |d|^2, midpoint and
-// half length; per vertex its position.  Each item then repeats only the
-// per-item arithmetic of narrow_item, on the same operands, so its decision
-// equals narrow_item's.  An EE item whose segments' bounding spheres are
-// farther apart than dhat + 1e-9 cannot pass (the closest-point pair lies on
-// the segments up to rounding far below 1e-9) and is rejected first.
-constexpr int kFaceStage = 16, kEdgeStage = 12;
-__global__ void __launch_bounds__(256) k_narrow_count_staged(NarrowIn in, int kind, const int* item_off, unsigned char* flags,
-                                                             int* hit_cnt, const int* gate_zero) {
-    if (gate_zero && *gate_zero != 0) return;
-    __shared__ double prim[2][kTopK][kFaceStage];
-    __shared__ double vtx[2][kTopK][3];
-    __shared__ int red[8];
+struct WarpStage {
+    double va[3][kTopK], vb[3][kTopK];                 // selected vertices of A and B
+    double b0[3][kTopK], bd[3][kTopK], bmid[3][kTopK]; // selected edges of B: start, direction, midpoint
+    double bdd[kTopK], bhalf[kTopK];                   // |direction|^2, half length
+};
+
+__device__ __forceinline__ V3 ld_col(const double (&a)[3][kTopK], int c) { return v3(a[0][c], a[1][c], a[2][c]); }
+__device__ __forceinline__ void st_col(double (&a)[3][kTopK], int c, V3 v) { a[0][c] = v.x; a[1][c] = v.y; a[2][c] = v.z; }
+
+// Pass 1.  mode 0: FV and EE hit masks and counts; mode 1: the VV fallback.
+__global__ void __launch_bounds__(32 * kRowsWarps) k_narrow_rows(NarrowIn in, int mode, NarrowScratch s, const int* skip_if) {
+    if (skip_if && *skip_if != 0) return;
+    __shared__ WarpStage stage[kRowsWarps];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    WarpStage& W = stage[threadIdx.x >> 5];
     const int np = min(*in.npairs_ptr, in.cap);
     const double dh = *in.dhat_ptr;
-    for (int p = blockIdx.x; p < np; p += gridDim.x) {
-        const int AB[2] = {in.pairs[2 * p], in.pairs[2 * p + 1]};
+    const int nwarps = gridDim.x * kRowsWarps;
+    for (int p = blockIdx.x * kRowsWarps + (threadIdx.x >> 5); p < np; p += nwarps) {
+        const int A = in.pairs[2 * p], B = in.pairs[2 * p + 1];
         const int* T = in.topk + (size_t)p * 6 * kTopK;
         const int* n = in.topn + 6 * p;
-        const int t0 = threadIdx.x;
-        if (t0 < 64) {
-            const int side = t0 >> 5, k = t0 & 31, body = AB[side];
-            const int vo = in.g.voff[body];
-            double* P = prim[side][k];
-            if (kind == 0 && k < n[4 + side]) {
-                const int* F = in.g.faces + 3 * (in.g.foff[body] + T[(4 + side) * kTopK + k]);
-                const V3 v0 = ld3(in.wv + 3 * (vo + F[0])), v1 = ld3(in.wv + 3 * (vo + F[1])), v2 = ld3(in.wv + 3 * (vo + F[2]));
-                const V3 e0 = v1 - v0, e1 = v2 - v0;
-                const V3 nn = safe_normalized(cross(e0, e1), v3(0, 1, 0));
-                const double d00 = dot(e0, e0), d01 = dot(e0, e1), d11 = dot(e1, e1);
-                st3(P, v0); st3(P + 3, e0); st3(P + 6, e1); st3(P + 9, nn);
-                P[12] = d00; P[13] = d01; P[14] = d11; P[15] = d00 * d11 - d01 * d01;
-            } else if (kind == 1 && k < n[2 + side]) {
-                const int* E = in.g.edges + 2 * (in.g.eoff[body] + T[(2 + side) * kTopK + k]);
-                const V3 a0 = ld3(in.wv + 3 * (vo + E[0])), a1 = ld3(in.wv + 3 * (vo + E[1]));
-                const V3 d = a1 - a0;
-                st3(P, a0); st3(P + 3, d); P[6] = dot(d, d);
-                st3(P + 7, 0.5 * (a0 + a1)); P[10] = 0.5 * norm(d);
+        const int n0 = n[0], n1 = n[1], n2 = n[2], n3 = n[3], n4 = n[4], n5 = n[5];
+        const int voA = in.g.voff[A], voB = in.g.voff[B];
+        __syncwarp();
+        if (lane < n0) st_col(W.va, lane, ld3(in.wv + 3 * (voA + T[lane])));
+        if (lane < n1) st_col(W.vb, lane, ld3(in.wv + 3 * (voB + T[kTopK + lane])));
+        if (mode == 1) {
+            const V3 a = lane < n0 ? ld3(in.wv + 3 * (voA + T[lane])) : v3(0, 0, 0);
+            __syncwarp();
+            unsigned mv = 0;
+            int cv = 0;
+            for (int c = 0; c < n1; ++c) {
+                const V3 d = ld_col(W.vb, c) - a;
+                const unsigned b = __ballot_sync(full, lane < n0 && !(norm(d) >= dh));
+                if (lane == c) mv = b;
+                cv += __popc(b);
             }
-        } else if (t0 < 128 && kind == 0) {
-            const int side = (t0 - 64) >> 5, k = t0 & 31, body = AB[side];
-            if (k < n[side]) st3(vtx[side][k], ld3(in.wv + 3 * (in.g.voff[body] + T[side * kTopK + k])));
+            if (lane == 0) s.cnt[p] = cv;
+            if (cv) s.mask[(size_t)p * kMaskWords + lane] = mv;
+            continue;
         }
-        __syncthreads();
-        const int cnt = kind == 0 ? n[4] * n[1] + n[5] * n[0] : n[2] * n[3];
-        const int fv1 = n[4] * n[1];
-        const int off = item_off[p];
-        int h = 0;
-        for (int t = t0; t < cnt; t += blockDim.x) {
-            bool hit = false;
-            if (kind == 0) {
-                int fs, fi, vs_, vi;
-                if (t < fv1) { fs = 0; fi = t / n[1]; vs_ = 1; vi = t % n[1]; }
-                else { const int u = t - fv1; fs = 1; fi = u / n[0]; vs_ = 0; vi = u % n[0]; }
-                const double* P = prim[fs][fi];
-                const V3 a = ld3(P), nn = ld3(P + 9);
-                const V3 pp = ld3(vtx[vs_][vi]);
-                const double sd = dot(pp - a, nn);
-                if (!(fabs(sd) >= dh)) {
-                    // point_in_triangle(proj, v0, v1, v2) (IPCSolver.cpp:107-134)
-                    const V3 proj = pp - sd * nn;
-                    const V3 v2 = proj - a;
-                    const double d20 = dot(v2, ld3(P + 3)), d21 = dot(v2, ld3(P + 6));
-                    const double d00 = P[12], d01 = P[13], d11 = P[14], denom = P[15];
-                    if (!(fabs(denom) < 1e-16)) {
-                        const double v = (d11 * d20 - d01 * d21) / denom;
-                        const double w = (d00 * d21 - d01 * d20) / denom;
-                        const double u = 1.0 - v - w;
-                        hit = u >= -1e-8 && v >= -1e-8 && w >= -1e-8;
+        // edges of B (columns of the EE grid)
+        if (lane < n3) {
+            const int* E = in.g.edges + 2 * (in.g.eoff[B] + T[3 * kTopK + lane]);
+            const V3 b0 = ld3(in.wv + 3 * (voB + E[0])), b1 = ld3(in.wv + 3 * (voB + E[1]));
+            const V3 d = b1 - b0;
+            st_col(W.b0, lane, b0); st_col(W.bd, lane, d); st_col(W.bmid, lane, 0.5 * (b0 + b1));
+            W.bdd[lane] = dot(d, d); W.bhalf[lane] = 0.5 * norm(d);
+        }
+        int cf = 0, ce = 0;
+        unsigned m0 = 0, m1 = 0, m2 = 0;
+        // FV side 0: lane = face of A, columns = vertices of B
+        {
+            const FaceRegs f = lane < n4 ? load_face(in, A, T[4 * kTopK + lane]) : FaceRegs{};
+            __syncwarp();
+            for (int c = 0; c < n1; ++c) {
+                const unsigned b = __ballot_sync(full, lane < n4 && fv_hit(f, ld_col(W.vb, c), dh));
+                if (lane == c) m0 = b;
+                cf += __popc(b);
+            }
+        }
+        // FV side 1: lane = face of B, columns = vertices of A
+        {
+            const FaceRegs f = lane < n5 ? load_face(in, B, T[5 * kTopK + lane]) : FaceRegs{};
+            for (int c = 0; c < n0; ++c) {
+                const unsigned b = __ballot_sync(full, lane < n5 && fv_hit(f, ld_col(W.va, c), dh));
+                if (lane == c) m1 = b;
+                cf += __popc(b);
+            }
+        }
+        // EE: lane = edge of A, columns = edges of B.  An item whose segments'
+        // bounding spheres are farther apart than dhat + 1e-9 cannot pass (the
+        // closest points lie on the segments up to rounding far below 1e-9).
+        {
+            V3 a0 = v3(0, 0, 0), d1 = v3(0, 0, 0), ma = v3(0, 0, 0);
+            double aa = 0.0, ha = 0.0;
+            if (lane < n2) {
+                const int* E = in.g.edges + 2 * (in.g.eoff[A] + T[2 * kTopK + lane]);
+                a0 = ld3(in.wv + 3 * (voA + E[0]));
+                const V3 a1 = ld3(in.wv + 3 * (voA + E[1]));
+                d1 = a1 - a0; aa = dot(d1, d1); ma = 0.5 * (a0 + a1); ha = 0.5 * norm(d1);
+            }
+            for (int c = 0; c < n3; ++c) {
+                bool hit = false;
+                if (lane < n2) {
+                    const V3 dm = ma - ld_col(W.bmid, c);
+                    const double r = dh + 1e-9 + ha + W.bhalf[c];
+                    if (!(dot(dm, dm) >= r * r)) {
+                        V3 c0, c1;
+                        closest_points_core(a0, d1, aa, ld_col(W.b0, c), ld_col(W.bd, c), W.bdd[c], c0, c1);
+                        hit = !(norm(c1 - c0) >= dh);
                     }
                 }
-            } else {
-                const double* EA = prim[0][t / n[3]];
-                const double* EB = prim[1][t % n[3]];
-                const double lb = norm(ld3(EA + 7) - ld3(EB + 7)) - EA[10] - EB[10];
-                if (!(lb >= dh + 1e-9)) {
-                    V3 c0, c1;
-                    closest_points_core(ld3(EA), ld3(EA + 3), EA[6], ld3(EB), ld3(EB + 3), EB[6], c0, c1);
-                    hit = !(norm(c1 - c0) >= dh);
-                }
+                const unsigned b = __ballot_sync(full, hit);
+                if (lane == c) m2 = b;
+                ce += __popc(b);
             }
-            flags[off + t] = hit ? 1 : 0;
-            h += hit ? 1 : 0;
         }
-        for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
-        if ((t0 & 31) == 0) red[t0 >> 5] = h;
+        if (lane == 0) { s.cnt[p] = cf; s.cnt[in.cap + p] = ce; }
+        if (cf + ce) {
+            unsigned* M = s.mask + (size_t)p * kMaskWords;
+            M[lane] = m0; M[kTopK + lane] = m1; M[2 * kTopK + lane] = m2;
+        }
+    }
+}
+
+// Exclusive scan of n ints by one block; returns the total (all threads).
+__device__ int block_scan(const int* in, int* out, int n) {
+    __shared__ int warp_sums[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = i < n ? in[i] : 0;
+        int x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sums[wid] = x;
         __syncthreads();
-        if (t0 == 0) {
-            int sum = 0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
-            hit_cnt[p] = sum;
+        if (wid == 0) {
+            int sv = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, sv, o);
+                if (lane >= o) sv += y;
+            }
+            warp_sums[lane] = sv;
         }
         __syncthreads();
+        const int excl = carry + (wid > 0 ? warp_sums[wid - 1] : 0) + x - v;
+        if (i < n) out[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+        __syncthreads();
+    }
+    const int total = carry;
+    __syncthreads();
+    return total;
+}
+
+// Prefixes of the hit counts: nseg halves of cap entries each (FV, EE), the
+// first *npairs_ptr of each; totals -> tot[0..nseg).
+__global__ void k_hit_scan(const int* cnt, int* off, int cap, const int* npairs_ptr, int nseg, int* tot0, int* tot1,
+                           const int* skip_if) {
+    if (skip_if && *skip_if != 0) return;
+    const int np = min(*npairs_ptr, cap);
+    for (int sgm = 0; sgm < nseg; ++sgm) {
+        const int t = block_scan(cnt + (size_t)sgm * cap, off + (size_t)sgm * cap, np);
+        if (threadIdx.x == 0) *(sgm == 0 ? tot0 : tot1) = t;
+    }
+}
+
+// Pass 2: the hits of each pair in item order, written at their global
+// position (FV list, then EE at *ee_base; positions past the raw cap are
+// dropped, as append_contact does).  One warp per pair; pairs without hits
+// return at once.
+__device__ __forceinline__ void emit_grid(const NarrowIn& in, int kind, int p, const unsigned* M, int rows, int cols,
+                                          int item_base, int& pos, ContactRec* out) {
+    const int lane = threadIdx.x & 31;
+    const unsigned w = lane < cols ? M[lane] : 0u;
+    int mine = 0;
+    for (int c = 0; c < cols; ++c) mine += (__shfl_sync(0xffffffffu, w, c) >> lane) & 1u;
+    if (lane >= rows) mine = 0;
+    int x = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, x, 31);
+    int q = pos + x - mine;
+    for (int c = 0; c < cols; ++c) {
+        const unsigned mc = __shfl_sync(0xffffffffu, w, c);
+        if (lane < rows && ((mc >> lane) & 1u)) {
+            if (q < kMaxRawContacts) {
+                ContactRec r;
+                narrow_item(in, kind, p, item_base + lane * cols + c, &r);
+                out[q] = r;
+            }
+            ++q;
+        }
+    }
+    pos += total;
+}
+
+__global__ void __launch_bounds__(32 * kEmitWarps) k_narrow_emit(NarrowIn in, int mode, NarrowScratch s, const int* ee_base,
+                                                                 ContactRec* out, const int* skip_if) {
+    if (skip_if && *skip_if != 0) return;
+    const int np = min(*in.npairs_ptr, in.cap);
+    const int nwarps = gridDim.x * kEmitWarps;
+    for (int p = blockIdx.x * kEmitWarps + (threadIdx.x >> 5); p < np; p += nwarps) {
+        const int* n = in.topn + 6 * p;
+        const unsigned* M = s.mask + (size_t)p * kMaskWords;
+        if (mode == 1) {
+            if (s.cnt[p] == 0) continue;
+            int pos = s.off[p];
+            if (pos < kMaxRawContacts) emit_grid(in, 2, p, M, n[0], n[1], 0, pos, out);
+            continue;
+        }
+        if (s.cnt[p] > 0) {
+            int pos = s.off[p];
+            if (pos < kMaxRawContacts) {
+                emit_grid(in, 0, p, M, n[4], n[1], 0, pos, out);
+                emit_grid(in, 0, p, M + kTopK, n[5], n[0], n[4] * n[1], pos, out);
+            }
+        }
+        if (s.cnt[in.cap + p] > 0) {
+            int pos = *ee_base + s.off[in.cap + p];
+            if (pos < kMaxRawContacts) emit_grid(in, 1, p, M + 2 * kTopK, n[2], n[3], 0, pos, out);
+        }
     }
 }
 

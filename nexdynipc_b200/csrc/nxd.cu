@@ -73,7 +73,6 @@ struct nxd_ctx {
     int N = 0, nv = 0, nf = 0, ne = 0, J = 0, D = 0;
     int max_prims = 0;
     int pair_cap = 0;
-    long long item_cap = 0;
     nxd_settings s{};
     std::vector<int> h_body_ids;
     std::vector<int> h_voff, h_foff, h_eoff;
@@ -95,8 +94,8 @@ struct nxd_ctx {
     int *pair_cnt, *pair_off, *pairs, *md_pairs;
     int *topk, *topn;
     int *nfv, *nee, *nvv, *nev, *off_fv, *off_ee, *off_vv, *off_ev;
-    int *hit_cnt, *hit_off;
-    unsigned char* flags;
+    int *hit_cnt, *hit_off;          // narrow-phase hits per pair: FV | EE halves, and their prefixes
+    unsigned* hmask;                 // narrow-phase column hit masks, kMaskWords per pair
     ContactRec *contacts, *contacts_tmp;
     double* sort_key;
     int* sort_idx;
@@ -253,20 +252,20 @@ namespace {
 // skip_if (device flag, may be null) skips the whole detection.
 void launch_narrow_full(nxd_ctx* c, const double* wv, const double* pose_p, const int* skip_if) {
     NarrowIn in{c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap, c->topk, c->topn, wv, pose_p, &c->sc->dhat};
-    const int blocks = c->n_sm * 8;
+    const NarrowScratch ns{c->hmask, c->hit_cnt, c->hit_off};
+    const int rows_blocks = c->n_sm * 8, emit_blocks = c->n_sm * 2;
     int* skip_vv = c->i_scratch;
     const int* np = &c->sc->n_pairs;
-    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_count_staged<<<blocks, 256, 0, c->stream>>>(in, 0, c->off_fv, c->flags, c->hit_cnt, skip_if););
-    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->fv_hits, nullptr, skip_if, np););
-    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 0, c->off_fv, c->flags, c->hit_off, nullptr, c->contacts, skip_if););
-    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_count_staged<<<blocks, 256, 0, c->stream>>>(in, 1, c->off_ee, c->flags, c->hit_cnt, skip_if););
-    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->ee_hits, nullptr, skip_if, np););
-    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 1, c->off_ee, c->flags, c->hit_off, &c->sc->fv_hits, c->contacts,
-                                                  skip_if););
+    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_rows<<<rows_blocks, 32 * kRowsWarps, 0, c->stream>>>(in, 0, ns, skip_if););
+    NXD_LAUNCH(c, NXD_PROF_SCAN, k_hit_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, np, 2, &c->sc->fv_hits,
+                                                                      &c->sc->ee_hits, skip_if););
+    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_emit<<<emit_blocks, 32 * kEmitWarps, 0, c->stream>>>(in, 0, ns, &c->sc->fv_hits, c->contacts,
+                                                                                                skip_if););
     NXD_LAUNCH(c, NXD_PROF_OTHER, k_contact_totals<<<1, 1, 0, c->stream>>>(c->sc, 0, skip_if, skip_vv););
-    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_count<<<blocks, 256, 0, c->stream>>>(in, 2, c->off_vv, c->flags, c->hit_cnt, skip_vv););
-    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, &c->sc->vv_hits, nullptr, skip_vv, np););
-    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_write<<<blocks, 256, 0, c->stream>>>(in, 2, c->off_vv, c->flags, c->hit_off, nullptr, c->contacts, skip_vv););
+    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_rows<<<rows_blocks, 32 * kRowsWarps, 0, c->stream>>>(in, 1, ns, skip_vv););
+    NXD_LAUNCH(c, NXD_PROF_SCAN, k_hit_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, np, 1, &c->sc->vv_hits,
+                                                                      nullptr, skip_vv););
+    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_emit<<<emit_blocks, 32 * kEmitWarps, 0, c->stream>>>(in, 1, ns, nullptr, c->contacts, skip_vv););
     NXD_LAUNCH(c, NXD_PROF_OTHER, k_contact_totals<<<1, 1, 0, c->stream>>>(c->sc, 1, skip_if, nullptr););
     NXD_LAUNCH(c, NXD_PROF_OTHER, k_sort_contacts<<<1, 1024, 0, c->stream>>>(c->sc, c->contacts, c->contacts_tmp, c->sort_key, c->sort_idx, skip_if););
 }
@@ -518,9 +517,8 @@ nxd_status nxd_create(const nxd_scene_desc* d, nxd_ctx** out) {
     c->nev = m.alloc<int>(c->pair_cap);
     c->off_fv = m.alloc<int>(c->pair_cap); c->off_ee = m.alloc<int>(c->pair_cap); c->off_vv = m.alloc<int>(c->pair_cap);
     c->off_ev = m.alloc<int>(c->pair_cap);
-    c->hit_cnt = m.alloc<int>(c->pair_cap); c->hit_off = m.alloc<int>(c->pair_cap);
-    c->item_cap = (long long)c->pair_cap * 2 * kTopK * kTopK;
-    c->flags = m.alloc<unsigned char>((size_t)c->item_cap);
+    c->hit_cnt = m.alloc<int>(2 * (size_t)c->pair_cap); c->hit_off = m.alloc<int>(2 * (size_t)c->pair_cap);
+    c->hmask = m.alloc<unsigned>((size_t)c->pair_cap * kMaskWords);
     c->contacts = m.alloc<ContactRec>(kMaxRawContacts);
     c->contacts_tmp = m.alloc<ContactRec>(kMaxContacts);
     c->sort_key = m.alloc<double>(65536); c->sort_idx = m.alloc<int>(65536);
