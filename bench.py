@@ -124,6 +124,58 @@ def cpu_baseline_sample(scene_fn, threads: int, stride: int):
     return est, wall
 
 
+def batched_leg(torch, steps: int, warmup: int, flush):
+    """256 independent scenes of 2-63 bodies (the batched configuration, seed
+    4000): aggregate scene-steps/s of the batched form (one graph of batched
+    launches per step) next to the plain path (the same scenes, one context
+    each, stepped one after another on one stream).  Both device-timed with
+    CUDA events per step, L2 flushed between steps."""
+    from nexdynipc_b200 import runtime, scenes
+    scs = scenes.batched_scenes(256)
+    stream = torch.cuda.Stream()
+    lib = runtime.lib()
+    b = runtime.Batch(scs)
+    b.set_stream(stream.cuda_stream)
+    singles = [runtime.Context(s) for s in scs]
+    for c in singles:
+        lib.nxd_set_stream(c.h, C.c_void_p(stream.cuda_stream))
+
+    def plain_step():
+        for c, s in zip(singles, scs):
+            st = lib.nxd_step(c.h, s.dt)
+            if st != 0:
+                raise runtime.NxdError("nxd_step", st)
+
+    def timed(fn):
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                fn()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        with torch.cuda.stream(stream):
+            for k in range(steps):
+                flush.fill_(k & 0xFF)
+                ev[k][0].record(stream)
+                fn()
+                ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(e) for a, e in ev) / 1e3
+
+    t_batched = timed(b.step)
+    t_plain = timed(plain_step)
+    status = max(b.diagnostics(i)["status"] for i in range(len(scs)))
+    same = all(np.array_equal(b.state(i)["position"], singles[i].state()["position"]) for i in range(0, len(scs), 17))
+    n = len(scs)
+    out = {"scenes": n, "bodies": int(sum(s.n_bodies for s in scs)), "steps": steps,
+           "value": n * steps / t_batched, "plain_value": n * steps / t_plain, "unit": "scene-steps/s",
+           "batched_over_plain": t_plain / t_batched, "groups": b.groups(), "status": int(status),
+           "equal_to_plain_sample": bool(same)}
+    for c in singles:
+        c.close()
+    b.close()
+    return out
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
@@ -159,6 +211,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.impl == "reference":
@@ -271,6 +324,10 @@ def main():
         roof.update(achieved=None, frac=None, traffic=None)
     per_family = {FAMILIES[i]: {"ms": round(float(prof_ms[i]), 3), "launches": int(prof_n[i])} for i in range(9)}
 
+    batched = None
+    if not args.no_batched:
+        batched = batched_leg(torch, min(args.steps, 10), 2, flush)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         stride = 64
@@ -287,7 +344,8 @@ def main():
         "config": {"workload": WORKLOAD, "replicas": ws, "l2": "flushed between steps (256 MiB write, untimed)",
                    "per_family_ms": per_family, "last_step": {k: diag[k] for k in
                                                               ("n_body_pairs", "n_contacts", "alm_iterations",
-                                                               "newton_iterations", "status")}},
+                                                               "newton_iterations", "status")},
+                   "batched": batched},
         "roofline": roof,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},

@@ -283,13 +283,24 @@ enum {
 };
 nxd_status nxd_profile(nxd_ctx* ctx, int32_t enable, double* ms, int64_t* launches);
 
-/* Batched form (independent scenes stepped together). */
+/* Batched form: independent scenes (each an IPCSolver::step of its own World,
+ * IPCSolver.cpp:808) stepped together.  nxd_batch_step records each scene's
+ * step sequence once per set of dts; scenes whose sequences match form a
+ * group, and each group's step runs as one CUDA graph of batched launches,
+ * one launch per kernel for all its scenes (the Newton solve is one CTA per
+ * scene).  Each scene's result equals nxd_step on its own context.
+ * nxd_batch_step returns without synchronising; get_state synchronises.
+ * nxd_batch_groups reports the number of groups; nxd_batch_set_stream makes
+ * the batch issue its work on a caller's cudaStream_t (after synchronising
+ * the previous one).  Neither has a reference counterpart. */
 typedef struct nxd_batch nxd_batch;
 nxd_status nxd_batch_create(const nxd_scene_desc* descs, int32_t n_scenes, nxd_batch** out);
 void nxd_batch_destroy(nxd_batch* b);
 nxd_status nxd_batch_step(nxd_batch* b, const double* dts);
 nxd_status nxd_batch_get_state(nxd_batch* b, int32_t scene, const nxd_state* out);
 nxd_status nxd_batch_get_diagnostics(nxd_batch* b, int32_t scene, nxd_diagnostics* out);
+int32_t nxd_batch_groups(nxd_batch* b);
+nxd_status nxd_batch_set_stream(nxd_batch* b, void* stream);
 
 /* Body-pair broad phase for callers that cannot allocate device memory.
  * No counterpart in the reference.  Callers that manage every device byte

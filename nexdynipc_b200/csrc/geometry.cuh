@@ -36,28 +36,34 @@ __device__ __forceinline__ void st_box(double* b, const Box& x) { st3(b, x.mn); 
 // ---------------------------------------------------------------------------
 // ContactAssembler::build (ContactAssembler.cpp:124-154): world boxes
 // ---------------------------------------------------------------------------
-__global__ void k_body_boxes(Geo g, const double* pos, const double* quat, double* boxes) {
+__device__ __forceinline__ void body_boxes_body(const Geo& g, const double* pos, const double* quat, double* boxes) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.N) return;
     const Box b = transform_local_box(ld3(g.lmin + 3 * i), ld3(g.lmax + 3 * i), ld3(pos + 3 * i), ldq(quat + 4 * i));
     st_box(boxes + 6 * i, b);
 }
+constexpr int kLB_body_boxes = 0;
+__global__ void k_body_boxes(const __grid_constant__ Geo g, const double* pos, const double* quat, double* boxes) { body_boxes_body(g, pos, quat, boxes); }
 
 // pose of body i at x: p = x[6i..], q = exp(theta) q_ref ('>' threshold)
-__global__ void k_pose_at_x(int N, const double* x, const double* quat_ref, double* pp, double* pq) {
+__device__ __forceinline__ void pose_at_x_body(int N, const double* x, const double* quat_ref, double* pp, double* pq) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     st3(pp + 3 * i, ld3(x + 6 * i));
     stq(pq + 4 * i, rot_gt(ldq(quat_ref + 4 * i), ld3(x + 6 * i + 3)));
 }
+constexpr int kLB_pose_at_x = 0;
+__global__ void k_pose_at_x(int N, const double* x, const double* quat_ref, double* pp, double* pq) { pose_at_x_body(N, x, quat_ref, pp, pq); }
 
 // world vertex = p + q * v_local (one thread per vertex)
-__global__ void k_world_vertices(Geo g, int nv, const int* vbody, const double* pos, const double* quat, double* wv) {
+__device__ __forceinline__ void world_vertices_body(const Geo& g, int nv, const int* vbody, const double* pos, const double* quat, double* wv) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nv) return;
     const int b = vbody[v];
     st3(wv + 3 * v, ld3(pos + 3 * b) + qrot(ldq(quat + 4 * b), ld3(g.verts + 3 * v)));
 }
+constexpr int kLB_world_vertices = 0;
+__global__ void k_world_vertices(const __grid_constant__ Geo g, int nv, const int* vbody, const double* pos, const double* quat, double* wv) { world_vertices_body(g, nv, vbody, pos, quat, wv); }
 
 // ---------------------------------------------------------------------------
 // Broad phase (ContactAssembler::detectBodyPairs, ContactAssembler.cpp:156-178
@@ -92,8 +98,7 @@ __device__ __forceinline__ bool pair_test(const Geo& g, const PairQuery& q, cons
 }
 
 // one warp per i: count (out == nullptr) or write pairs in descending j
-__global__ void k_pairs(Geo g, PairQuery q, const double* boxes, int* counts, const int* offsets, int* out, int cap,
-                        const int* gate) {
+__device__ __forceinline__ void pairs_body(const Geo& g, const PairQuery& q, const double* boxes, int* counts, const int* offsets, int* out, int cap, const int* gate) {
     if (gate && *gate == 0) return;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -116,13 +121,14 @@ __global__ void k_pairs(Geo g, PairQuery q, const double* boxes, int* counts, co
         if (!out && lane == 0) counts[i] = c;
     }
 }
+constexpr int kLB_pairs = 0;
+__global__ void k_pairs(const __grid_constant__ Geo g, const __grid_constant__ PairQuery q, const double* boxes, int* counts, const int* offsets, int* out, int cap, const int* gate) { pairs_body(g, q, boxes, counts, offsets, out, cap, gate); }
 
 // Exclusive scan of n ints (single block, 1024 threads); total -> *total.
 // n_dev (optional) caps n at a device-side count.  The scan runs only when
 // run_if is null or non-zero and skip_if is null or zero; when run_if is zero
 // the total is cleared, when skip_if is set nothing is written.
-__global__ void k_scan(const int* in, int* out, int n, int* total, const int* run_if, const int* skip_if = nullptr,
-                       const int* n_dev = nullptr) {
+__device__ __forceinline__ void scan_body(const int* in, int* out, int n, int* total, const int* run_if, const int* skip_if, const int* n_dev) {
     if (skip_if && *skip_if != 0) return;
     if (run_if && *run_if == 0) { if (threadIdx.x == 0 && total) *total = 0; return; }
     if (n_dev) n = min(n, *n_dev);
@@ -158,6 +164,8 @@ __global__ void k_scan(const int* in, int* out, int n, int* total, const int* ru
     }
     if (threadIdx.x == 0 && total) *total = carry;
 }
+constexpr int kLB_scan = 0;
+__global__ void k_scan(const int* in, int* out, int n, int* total, const int* run_if, const int* skip_if = nullptr, const int* n_dev = nullptr) { scan_body(in, out, n, total, run_if, skip_if, n_dev); }
 
 // ---------------------------------------------------------------------------
 // estimateMinBodyPairDistance (ContactAssembler.cpp:180-212): min over the
@@ -167,7 +175,7 @@ __device__ __forceinline__ void atomic_min_pos_double(double* addr, double v) {
     // non-negative doubles order like their bit patterns
     atomicMin(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
 }
-__global__ void k_min_pair_distance(Geo g, PairQuery q, const double* boxes, double* out) {
+__device__ __forceinline__ void min_pair_distance_body(const Geo& g, const PairQuery& q, const double* boxes, double* out) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -179,14 +187,15 @@ __global__ void k_min_pair_distance(Geo g, PairQuery q, const double* boxes, dou
     for (int o = 16; o > 0; o >>= 1) m = dmin(m, __shfl_xor_sync(0xffffffffu, m, o));
     if (lane == 0 && m < INFINITY) atomic_min_pos_double(out, m);
 }
+constexpr int kLB_min_pair_distance = 0;
+__global__ void k_min_pair_distance(const __grid_constant__ Geo g, const __grid_constant__ PairQuery q, const double* boxes, double* out) { min_pair_distance_body(g, q, boxes, out); }
 
 // ---------------------------------------------------------------------------
 // Top-k selection (ContactAssembler.cpp:214-303): one warp per (pair, list),
 // list s = 0 vA, 1 vB, 2 eA, 3 eB, 4 fA, 5 fB.  Scores are point-to-box
 // distances of the primitive's world vertices to the other body's box.
 // ---------------------------------------------------------------------------
-__global__ void k_topk(Geo g, const int* pairs, const int* npairs_ptr, int cap, const double* boxes, const double* wv,
-                       int* topk, int* topn, int max_prims) {
+__device__ __forceinline__ void topk_body(const Geo& g, const int* pairs, const int* npairs_ptr, int cap, const double* boxes, const double* wv, int* topk, int* topn, int max_prims) {
     extern __shared__ unsigned char smem_raw[];
     const int wpb = blockDim.x >> 5;
     const int wid = threadIdx.x >> 5;
@@ -235,12 +244,14 @@ __global__ void k_topk(Geo g, const int* pairs, const int* npairs_ptr, int cap, 
         __syncwarp();
     }
 }
+constexpr int kLB_topk = 0;
+__global__ void k_topk(const __grid_constant__ Geo g, const int* pairs, const int* npairs_ptr, int cap, const double* boxes, const double* wv, int* topk, int* topn, int max_prims) { topk_body(g, pairs, npairs_ptr, cap, boxes, wv, topk, topn, max_prims); }
 
 // ---------------------------------------------------------------------------
 // Candidate item counts per pair and the materialised candidate lists
 // (ContactAssembler.cpp:304-341 order).
 // ---------------------------------------------------------------------------
-__global__ void k_item_counts(const int* npairs_ptr, int cap, const int* topn, int* nfv, int* nee, int* nvv, int* nev) {
+__device__ __forceinline__ void item_counts_body(const int* npairs_ptr, int cap, const int* topn, int* nfv, int* nee, int* nvv, int* nev) {
     const int np = min(*npairs_ptr, cap);
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
         const int* t = topn + 6 * p;
@@ -250,6 +261,8 @@ __global__ void k_item_counts(const int* npairs_ptr, int cap, const int* topn, i
         if (nev) nev[p] = t[2] * t[1] + t[3] * t[0];
     }
 }
+constexpr int kLB_item_counts = 0;
+__global__ void k_item_counts(const int* npairs_ptr, int cap, const int* topn, int* nfv, int* nee, int* nvv, int* nev) { item_counts_body(npairs_ptr, cap, topn, nfv, nee, nvv, nev); }
 
 struct CandOut {
     int* vv; long long vv_cap;
@@ -505,7 +518,7 @@ __device__ __forceinline__ V3 ld_col(const double (&a)[3][kTopK], int c) { retur
 __device__ __forceinline__ void st_col(double (&a)[3][kTopK], int c, V3 v) { a[0][c] = v.x; a[1][c] = v.y; a[2][c] = v.z; }
 
 // Pass 1.  mode 0: FV and EE hit masks and counts; mode 1: the VV fallback.
-__global__ void __launch_bounds__(32 * kRowsWarps) k_narrow_rows(NarrowIn in, int mode, NarrowScratch s, const int* skip_if) {
+__device__ __forceinline__ void narrow_rows_body(const NarrowIn& in, int mode, const NarrowScratch& s, const int* skip_if) {
     if (skip_if && *skip_if != 0) return;
     __shared__ WarpStage stage[kRowsWarps];
     const unsigned full = 0xffffffffu;
@@ -602,6 +615,8 @@ __global__ void __launch_bounds__(32 * kRowsWarps) k_narrow_rows(NarrowIn in, in
         }
     }
 }
+constexpr int kLB_narrow_rows = 32 * kRowsWarps;
+__global__ void __launch_bounds__(32 * kRowsWarps) k_narrow_rows(const __grid_constant__ NarrowIn in, int mode, const __grid_constant__ NarrowScratch s, const int* skip_if) { narrow_rows_body(in, mode, s, skip_if); }
 
 // Exclusive scan of n ints by one block; returns the total (all threads).
 __device__ int block_scan(const int* in, int* out, int n) {
@@ -642,8 +657,7 @@ __device__ int block_scan(const int* in, int* out, int n) {
 
 // Prefixes of the hit counts: nseg halves of cap entries each (FV, EE), the
 // first *npairs_ptr of each; totals -> tot[0..nseg).
-__global__ void k_hit_scan(const int* cnt, int* off, int cap, const int* npairs_ptr, int nseg, int* tot0, int* tot1,
-                           const int* skip_if) {
+__device__ __forceinline__ void hit_scan_body(const int* cnt, int* off, int cap, const int* npairs_ptr, int nseg, int* tot0, int* tot1, const int* skip_if) {
     if (skip_if && *skip_if != 0) return;
     const int np = min(*npairs_ptr, cap);
     for (int sgm = 0; sgm < nseg; ++sgm) {
@@ -651,6 +665,8 @@ __global__ void k_hit_scan(const int* cnt, int* off, int cap, const int* npairs_
         if (threadIdx.x == 0) *(sgm == 0 ? tot0 : tot1) = t;
     }
 }
+constexpr int kLB_hit_scan = 0;
+__global__ void k_hit_scan(const int* cnt, int* off, int cap, const int* npairs_ptr, int nseg, int* tot0, int* tot1, const int* skip_if) { hit_scan_body(cnt, off, cap, npairs_ptr, nseg, tot0, tot1, skip_if); }
 
 // Pass 2: the hits of each pair in item order, written at their global
 // position (FV list, then EE at *ee_base; positions past the raw cap are
@@ -684,8 +700,7 @@ __device__ __forceinline__ void emit_grid(const NarrowIn& in, int kind, int p, c
     pos += total;
 }
 
-__global__ void __launch_bounds__(32 * kEmitWarps) k_narrow_emit(NarrowIn in, int mode, NarrowScratch s, const int* ee_base,
-                                                                 ContactRec* out, const int* skip_if) {
+__device__ __forceinline__ void narrow_emit_body(const NarrowIn& in, int mode, const NarrowScratch& s, const int* ee_base, ContactRec* out, const int* skip_if) {
     if (skip_if && *skip_if != 0) return;
     const int np = min(*in.npairs_ptr, in.cap);
     const int nwarps = gridDim.x * kEmitWarps;
@@ -711,6 +726,8 @@ __global__ void __launch_bounds__(32 * kEmitWarps) k_narrow_emit(NarrowIn in, in
         }
     }
 }
+constexpr int kLB_narrow_emit = 32 * kEmitWarps;
+__global__ void __launch_bounds__(32 * kEmitWarps) k_narrow_emit(const __grid_constant__ NarrowIn in, int mode, const __grid_constant__ NarrowScratch s, const int* ee_base, ContactRec* out, const int* skip_if) { narrow_emit_body(in, mode, s, ee_base, out, skip_if); }
 
 // ---------------------------------------------------------------------------
 // Scene minimum distance, pruned (computeSceneMinDistance,
@@ -744,8 +761,7 @@ __device__ double vertex_face_plane_distance(V3 p, V3 v0, V3 v1, V3 v2) {
     return INFINITY;
 }
 
-__global__ void k_min_distance(Geo g, const int* pairs, const int* npairs_ptr, int cap, const double* boxes,
-                               const double* wv, double* out, const int* gate) {
+__device__ __forceinline__ void min_distance_body(const Geo& g, const int* pairs, const int* npairs_ptr, int cap, const double* boxes, const double* wv, double* out, const int* gate) {
     if (gate && *gate == 0) return;
     const int np = min(*npairs_ptr, cap);
     double m = INFINITY;
@@ -771,5 +787,7 @@ __global__ void k_min_distance(Geo g, const int* pairs, const int* npairs_ptr, i
     for (int o = 16; o > 0; o >>= 1) m = dmin(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0 && m < INFINITY) atomic_min_pos_double(out, m);
 }
+constexpr int kLB_min_distance = 0;
+__global__ void k_min_distance(const __grid_constant__ Geo g, const int* pairs, const int* npairs_ptr, int cap, const double* boxes, const double* wv, double* out, const int* gate) { min_distance_body(g, pairs, npairs_ptr, cap, boxes, wv, out, gate); }
 
 }  // namespace nx

@@ -12,6 +12,7 @@
 
 #include "../../include/nxd.h"
 #include "step.cuh"
+#include "batch.cuh"
 
 using namespace nx;
 
@@ -105,6 +106,8 @@ struct nxd_ctx {
     // solver scratch
     Solver S{};
     int cand_stride = 0;
+    // when set, launches are recorded here (batched replay) instead of issued
+    std::vector<LaunchRec>* rec = nullptr;
 };
 
 namespace {
@@ -126,6 +129,18 @@ struct ProfScope {
     }
 };
 #define NXD_LAUNCH(ctx, fam, ...) do { ProfScope ps_(ctx, fam); __VA_ARGS__; } while (0)
+// Launch of a step kernel k_<name> (body <name>_body): issued on the
+// context's stream, or recorded for a batched replay.
+#define NXD_K(ctx, fam, name, grid, block, smem, ...)                                                     \
+    do {                                                                                                \
+        if ((ctx)->rec) {                                                                               \
+            record_into<&name##_body, kLB_##name>(*(ctx)->rec, fam, (decltype(&name##_body))nullptr,    \
+                                                   dim3(grid), dim3(block), (size_t)(smem), __VA_ARGS__); \
+        } else {                                                                                        \
+            ProfScope ps_(ctx, fam);                                                                    \
+            k_##name<<<grid, block, smem, (ctx)->stream>>>(__VA_ARGS__);                                \
+        }                                                                                               \
+    } while (0)
 
 void fill_solver(nxd_ctx* c) {
     Solver& S = c->S;
@@ -199,9 +214,14 @@ StepCfg step_cfg(const nxd_ctx* c) {
     return k;
 }
 
-// one ALM iteration's Newton solve: barrier counters zeroed, then a
-// cooperative launch of k_newton on c->newton_grid CTAs
+// one ALM iteration's Newton solve: one CTA (a plain launch; the grid
+// barrier degenerates to __syncthreads), or barrier counters zeroed and a
+// cooperative launch of k_newton on c->newton_grid co-resident CTAs
 void launch_newton(nxd_ctx* c) {
+    if (c->rec || c->newton_grid == 1) {
+        NXD_K(c, NXD_PROF_NEWTON, newton, (1), (kNewtonThreads), (0), c->S);
+        return;
+    }
     ProfScope ps_(c, NXD_PROF_NEWTON);
     cudaMemsetAsync(c->S.bar_count, 0, 2 * sizeof(unsigned), c->stream);
     void* args[] = {(void*)&c->S};
@@ -210,16 +230,16 @@ void launch_newton(nxd_ctx* c) {
 
 // ContactAssembler::build + world vertices at the current poses
 void launch_assembly(nxd_ctx* c) {
-    NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_body_boxes<<<grid_for(c->N, 128), 128, 0, c->stream>>>(c->geo, c->pos, c->quat, c->boxes););
-    NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_world_vertices<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(c->geo, c->nv, c->vbody, c->pos, c->quat, c->wv););
+    NXD_K(c, NXD_PROF_ASSEMBLY, body_boxes, (grid_for(c->N, 128)), (128), (0), c->geo, c->pos, c->quat, c->boxes);
+    NXD_K(c, NXD_PROF_ASSEMBLY, world_vertices, (grid_for(c->nv, 256)), (256), (0), c->geo, c->nv, c->vbody, c->pos, c->quat, c->wv);
 }
 
 // pair list (count / scan / write) with query q into out, count -> *count_dev
 void launch_pairs(nxd_ctx* c, const PairQuery& q, int* out, int* count_dev, const int* gate) {
     const int blocks = grid_for((long long)c->N * 32, 256);
-    NXD_LAUNCH(c, NXD_PROF_BROAD, k_pairs<<<blocks, 256, 0, c->stream>>>(c->geo, q, c->boxes, c->pair_cnt, nullptr, nullptr, 0, gate););
-    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->pair_cnt, c->pair_off, c->N, count_dev, gate););
-    NXD_LAUNCH(c, NXD_PROF_BROAD, k_pairs<<<blocks, 256, 0, c->stream>>>(c->geo, q, c->boxes, nullptr, c->pair_off, out, c->pair_cap, gate););
+    NXD_K(c, NXD_PROF_BROAD, pairs, (blocks), (256), (0), c->geo, q, c->boxes, c->pair_cnt, nullptr, nullptr, 0, gate);
+    NXD_K(c, NXD_PROF_SCAN, scan, (1), (1024), (0), c->pair_cnt, c->pair_off, c->N, count_dev, gate, nullptr, nullptr);
+    NXD_K(c, NXD_PROF_BROAD, pairs, (blocks), (256), (0), c->geo, q, c->boxes, nullptr, c->pair_off, out, c->pair_cap, gate);
 }
 
 size_t topk_smem(const nxd_ctx* c, int warps) {
@@ -232,14 +252,14 @@ void launch_candidates(nxd_ctx* c, const double* act_ptr, double act_val) {
     launch_pairs(c, q, c->pairs, &c->sc->n_pairs, nullptr);
     int warps = 4;
     while (warps > 1 && topk_smem(c, warps) > 200 * 1024) --warps;
-    NXD_LAUNCH(c, NXD_PROF_TOPK, k_topk<<<c->n_sm * 4, 32 * warps, topk_smem(c, warps), c->stream>>>(c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap,
-                                                                       c->boxes, c->wv, c->topk, c->topn, c->max_prims););
-    NXD_LAUNCH(c, NXD_PROF_OTHER, k_item_counts<<<grid_for(c->pair_cap, 256), 256, 0, c->stream>>>(&c->sc->n_pairs, c->pair_cap, c->topn, c->nfv,
-                                                                       c->nee, c->nvv, c->nev););
+    NXD_K(c, NXD_PROF_TOPK, topk, (c->n_sm * 4), (32 * warps), (topk_smem(c, warps)), c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap,
+                                                                       c->boxes, c->wv, c->topk, c->topn, c->max_prims);
+    NXD_K(c, NXD_PROF_OTHER, item_counts, (grid_for(c->pair_cap, 256)), (256), (0), &c->sc->n_pairs, c->pair_cap, c->topn, c->nfv,
+                                                                       c->nee, c->nvv, c->nev);
     const int* np = &c->sc->n_pairs;
-    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->nfv, c->off_fv, c->pair_cap, &c->sc->fv_items, nullptr, nullptr, np););
-    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->nee, c->off_ee, c->pair_cap, &c->sc->ee_items, nullptr, nullptr, np););
-    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->nvv, c->off_vv, c->pair_cap, &c->sc->vv_items, nullptr, nullptr, np););
+    NXD_K(c, NXD_PROF_SCAN, scan, (1), (1024), (0), c->nfv, c->off_fv, c->pair_cap, &c->sc->fv_items, nullptr, nullptr, np);
+    NXD_K(c, NXD_PROF_SCAN, scan, (1), (1024), (0), c->nee, c->off_ee, c->pair_cap, &c->sc->ee_items, nullptr, nullptr, np);
+    NXD_K(c, NXD_PROF_SCAN, scan, (1), (1024), (0), c->nvv, c->off_vv, c->pair_cap, &c->sc->vv_items, nullptr, nullptr, np);
 }
 
 }  // namespace
@@ -256,85 +276,91 @@ void launch_narrow_full(nxd_ctx* c, const double* wv, const double* pose_p, cons
     const int rows_blocks = c->n_sm * 8, emit_blocks = c->n_sm * 2;
     int* skip_vv = c->i_scratch;
     const int* np = &c->sc->n_pairs;
-    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_rows<<<rows_blocks, 32 * kRowsWarps, 0, c->stream>>>(in, 0, ns, skip_if););
-    NXD_LAUNCH(c, NXD_PROF_SCAN, k_hit_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, np, 2, &c->sc->fv_hits,
-                                                                      &c->sc->ee_hits, skip_if););
-    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_emit<<<emit_blocks, 32 * kEmitWarps, 0, c->stream>>>(in, 0, ns, &c->sc->fv_hits, c->contacts,
-                                                                                                skip_if););
-    NXD_LAUNCH(c, NXD_PROF_OTHER, k_contact_totals<<<1, 1, 0, c->stream>>>(c->sc, 0, skip_if, skip_vv););
-    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_rows<<<rows_blocks, 32 * kRowsWarps, 0, c->stream>>>(in, 1, ns, skip_vv););
-    NXD_LAUNCH(c, NXD_PROF_SCAN, k_hit_scan<<<1, 1024, 0, c->stream>>>(c->hit_cnt, c->hit_off, c->pair_cap, np, 1, &c->sc->vv_hits,
-                                                                      nullptr, skip_vv););
-    NXD_LAUNCH(c, NXD_PROF_NARROW, k_narrow_emit<<<emit_blocks, 32 * kEmitWarps, 0, c->stream>>>(in, 1, ns, nullptr, c->contacts, skip_vv););
-    NXD_LAUNCH(c, NXD_PROF_OTHER, k_contact_totals<<<1, 1, 0, c->stream>>>(c->sc, 1, skip_if, nullptr););
-    NXD_LAUNCH(c, NXD_PROF_OTHER, k_sort_contacts<<<1, 1024, 0, c->stream>>>(c->sc, c->contacts, c->contacts_tmp, c->sort_key, c->sort_idx, skip_if););
+    NXD_K(c, NXD_PROF_NARROW, narrow_rows, (rows_blocks), (32 * kRowsWarps), (0), in, 0, ns, skip_if);
+    NXD_K(c, NXD_PROF_SCAN, hit_scan, (1), (1024), (0), c->hit_cnt, c->hit_off, c->pair_cap, np, 2, &c->sc->fv_hits,
+                                                                      &c->sc->ee_hits, skip_if);
+    NXD_K(c, NXD_PROF_NARROW, narrow_emit, (emit_blocks), (32 * kEmitWarps), (0), in, 0, ns, &c->sc->fv_hits, c->contacts,
+                                                                                                skip_if);
+    NXD_K(c, NXD_PROF_OTHER, contact_totals, (1), (1), (0), c->sc, 0, skip_if, skip_vv);
+    NXD_K(c, NXD_PROF_NARROW, narrow_rows, (rows_blocks), (32 * kRowsWarps), (0), in, 1, ns, skip_vv);
+    NXD_K(c, NXD_PROF_SCAN, hit_scan, (1), (1024), (0), c->hit_cnt, c->hit_off, c->pair_cap, np, 1, &c->sc->vv_hits,
+                                                                      nullptr, skip_vv);
+    NXD_K(c, NXD_PROF_NARROW, narrow_emit, (emit_blocks), (32 * kEmitWarps), (0), in, 1, ns, nullptr, c->contacts, skip_vv);
+    NXD_K(c, NXD_PROF_OTHER, contact_totals, (1), (1), (0), c->sc, 1, skip_if, nullptr);
+    NXD_K(c, NXD_PROF_OTHER, sort_contacts, (1), (1024), (0), c->sc, c->contacts, c->contacts_tmp, c->sort_key, c->sort_idx, skip_if);
 }
 
 }  // namespace
 
 // A detection pass inside an ALM iteration runs only when the iteration runs
 // and a contact form exists; fold both conditions into one skip flag.
-__global__ void k_alm_detect_gate(const Scalars* sc, int* skip) {
+__device__ __forceinline__ void alm_detect_gate_body(const Scalars* sc, int* skip) {
     *skip = (sc->alm_done || !(sc->barrier_form || sc->friction_form)) ? 1 : 0;
 }
-__global__ void k_init_scalar_d(double* p, double v) { *p = v; }
-__global__ void k_max_tol(const double* tol, int n, double* out) {
+constexpr int kLB_alm_detect_gate = 0;
+__global__ void k_alm_detect_gate(const Scalars* sc, int* skip) { alm_detect_gate_body(sc, skip); }
+__device__ __forceinline__ void init_scalar_d_body(double* p, double v) { *p = v; }
+constexpr int kLB_init_scalar_d = 0;
+__global__ void k_init_scalar_d(double* p, double v) { init_scalar_d_body(p, v); }
+__device__ __forceinline__ void max_tol_body(const double* tol, int n, double* out) {
     double m = 0.0;
     for (int i = 0; i < n; ++i) m = dmax(m, tol[i]);
     *out = m;
 }
-__global__ void k_body_md_tol(Geo g, const double* pos, double* tol) {
+constexpr int kLB_max_tol = 0;
+__global__ void k_max_tol(const double* tol, int n, double* out) { max_tol_body(tol, n, out); }
+__device__ __forceinline__ void body_md_tol_body(const Geo& g, const double* pos, double* tol) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.N) return;
     const double diag = norm(ld3(g.lmax + 3 * i) - ld3(g.lmin + 3 * i));
     tol[i] = 4e-6 * diag + 1e-9 * (1.0 + norm(ld3(pos + 3 * i)) + diag);
 }
+constexpr int kLB_body_md_tol = 0;
+__global__ void k_body_md_tol(const __grid_constant__ Geo g, const double* pos, double* tol) { body_md_tol_body(g, pos, tol); }
 
 namespace {
 
 nxd_status enqueue_step(nxd_ctx* c, double dt) {
-    cudaStream_t st = c->stream;
     const StepCfg cfg = step_cfg(c);
     // ContactAssembler::build + buildCandidateSet(currentDhat)
     launch_assembly(c);
     launch_candidates(c, &c->sc->dhat, 0.0);
     // adaptive barrier (IPCSolver.cpp:817-832)
     if (c->s.enable_adaptive_barrier) {
-        NXD_LAUNCH(c, NXD_PROF_OTHER, k_barrier_init<<<1, kSolverThreads, 0, st>>>(cfg, c->mass, c->pos, c->sc););
-        NXD_LAUNCH(c, NXD_PROF_OTHER, k_init_scalar_d<<<1, 1, 0, st>>>(&c->sc->bmd, INFINITY););
+        NXD_K(c, NXD_PROF_OTHER, barrier_init, (1), (kSolverThreads), (0), cfg, c->mass, c->pos, c->sc);
+        NXD_K(c, NXD_PROF_OTHER, init_scalar_d, (1), (1), (0), &c->sc->bmd, INFINITY);
         PairQuery qb{0, &c->sc->dhat, 0.0, 2.0, 0.0};
-        NXD_LAUNCH(c, NXD_PROF_BROAD, k_min_pair_distance<<<grid_for((long long)c->N * 32, 256), 256, 0, st>>>(c->geo, qb, c->boxes, &c->sc->bmd););
-        NXD_LAUNCH(c, NXD_PROF_OTHER, k_body_md_tol<<<grid_for(c->N, 128), 128, 0, st>>>(c->geo, c->pos, c->md_tol););
-        NXD_LAUNCH(c, NXD_PROF_OTHER, k_max_tol<<<1, 1, 0, st>>>(c->md_tol, c->N, c->max_md_tol););
-        NXD_LAUNCH(c, NXD_PROF_OTHER, k_md_gate<<<1, 1, 0, st>>>(c->sc, c->max_md_tol););
+        NXD_K(c, NXD_PROF_BROAD, min_pair_distance, (grid_for((long long)c->N * 32, 256)), (256), (0), c->geo, qb, c->boxes, &c->sc->bmd);
+        NXD_K(c, NXD_PROF_OTHER, body_md_tol, (grid_for(c->N, 128)), (128), (0), c->geo, c->pos, c->md_tol);
+        NXD_K(c, NXD_PROF_OTHER, max_tol, (1), (1), (0), c->md_tol, c->N, c->max_md_tol);
+        NXD_K(c, NXD_PROF_OTHER, md_gate, (1), (1), (0), c->sc, c->max_md_tol);
         PairQuery qm{2, &c->sc->md_radius, 0.0, 1.0, 0.0};
         launch_pairs(c, qm, c->md_pairs, &c->sc->n_md_pairs, &c->sc->md_gate);
-        NXD_LAUNCH(c, NXD_PROF_MIN_DISTANCE, k_min_distance<<<c->n_sm * 4, 256, 0, st>>>(c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
-                                                    &c->sc->md, &c->sc->md_gate););
-        NXD_LAUNCH(c, NXD_PROF_OTHER, k_kappa_update<<<1, 1, 0, st>>>(c->sc););
+        NXD_K(c, NXD_PROF_MIN_DISTANCE, min_distance, (c->n_sm * 4), (256), (0), c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
+                                                    &c->sc->md, &c->sc->md_gate);
+        NXD_K(c, NXD_PROF_OTHER, kappa_update, (1), (1), (0), c->sc);
     }
     // computeMaxStep: the FV root box fails the reference's domain predicate
     // before any bisection, so the earliest TOI is 1 and the step is dt.
     // integrator init, contact forms, drives
-    NXD_LAUNCH(c, NXD_PROF_OTHER, k_step_setup<<<grid_for(std::max(c->N, c->D), 128), 128, 0, st>>>(
-        cfg, dt, c->pos, c->quat, c->vel, c->omega, c->lacc, c->aacc, c->x, c->xhat, c->xprev, c->vprev, c->aprev, c->pos0,
-        c->quat0, c->sc, c->dprm, c->dfilt, c->dfinit, c->dhas_prev););
+    NXD_K(c, NXD_PROF_OTHER, step_setup, (grid_for(std::max(c->N, c->D), 128)), (128), (0), cfg, dt, c->pos, c->quat, c->vel, c->omega, c->lacc, c->aacc, c->x, c->xhat, c->xprev, c->vprev, c->aprev, c->pos0,
+        c->quat0, c->sc, c->dprm, c->dfilt, c->dfinit, c->dhas_prev);
     // detectContacts at the step-start poses (when a contact form is needed)
     const bool needs = c->s.enable_adaptive_barrier || (c->s.enable_friction && c->s.friction_coeff > 0.0);
     if (needs) launch_narrow_full(c, c->wv, c->pos, nullptr);
-    else NXD_LAUNCH(c, NXD_PROF_OTHER, k_contact_totals<<<1, 1, 0, st>>>(c->sc, 2, nullptr, nullptr));
+    else NXD_K(c, NXD_PROF_OTHER, contact_totals, (1), (1), (0), c->sc, 2, nullptr, nullptr);
     int* skip_detect = c->i_scratch + 1;
     for (int alm = 0; alm < c->s.alm_max_iters; ++alm) {
         launch_newton(c);
-        NXD_LAUNCH(c, NXD_PROF_OTHER, k_alm_detect_gate<<<1, 1, 0, st>>>(c->sc, skip_detect););
-        NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_pose_at_x<<<grid_for(c->N, 128), 128, 0, st>>>(c->N, c->x, c->quat, c->pose_p, c->pose_q););
-        NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_world_vertices<<<grid_for(c->nv, 256), 256, 0, st>>>(c->geo, c->nv, c->vbody, c->pose_p, c->pose_q, c->wvx););
+        NXD_K(c, NXD_PROF_OTHER, alm_detect_gate, (1), (1), (0), c->sc, skip_detect);
+        NXD_K(c, NXD_PROF_ASSEMBLY, pose_at_x, (grid_for(c->N, 128)), (128), (0), c->N, c->x, c->quat, c->pose_p, c->pose_q);
+        NXD_K(c, NXD_PROF_ASSEMBLY, world_vertices, (grid_for(c->nv, 256)), (256), (0), c->geo, c->nv, c->vbody, c->pose_p, c->pose_q, c->wvx);
         launch_narrow_full(c, c->wvx, c->pose_p, skip_detect);
-        NXD_LAUNCH(c, NXD_PROF_ALM_POST, k_alm_post<<<1, kSolverThreads, 0, st>>>(c->S, c->sc, cfg, c->nforce););
+        NXD_K(c, NXD_PROF_ALM_POST, alm_post, (1), (kSolverThreads), (0), c->S, c->sc, cfg, c->nforce);
     }
-    NXD_LAUNCH(c, NXD_PROF_OTHER, k_update_state<<<grid_for(c->N, 128), 128, 0, st>>>(cfg, c->x, c->xprev, c->vprev, c->pos, c->quat, c->vel, c->omega,
-                                                        c->lacc, c->aacc, c->sc, c->da, c->db, c->dprm, c->dfilt););
-    if (c->D > 0) NXD_LAUNCH(c, NXD_PROF_OTHER, k_drive_kpi<<<1, 1, 0, st>>>(cfg, c->omega, c->sc, c->da, c->db, c->dprm, c->dfilt));
+    NXD_K(c, NXD_PROF_OTHER, update_state, (grid_for(c->N, 128)), (128), (0), cfg, c->x, c->xprev, c->vprev, c->pos, c->quat, c->vel, c->omega,
+                                                        c->lacc, c->aacc, c->sc, c->da, c->db, c->dprm, c->dfilt);
+    if (c->D > 0) NXD_K(c, NXD_PROF_OTHER, drive_kpi, (1), (1), (0), cfg, c->omega, c->sc, c->da, c->db, c->dprm, c->dfilt);
     NXD_CUDA(cudaGetLastError());
     return NXD_OK;
 }
@@ -635,10 +661,10 @@ nxd_status nxd_build_candidates(nxd_ctx* c, double act, nxd_candidates* o) {
     if (!c || !o) return NXD_INVALID_ARGUMENT;
     launch_assembly(c);
     launch_candidates(c, nullptr, act);
-    NXD_LAUNCH(c, NXD_PROF_OTHER, k_item_counts<<<grid_for(c->pair_cap, 256), 256, 0, c->stream>>>(&c->sc->n_pairs, c->pair_cap, c->topn, c->nfv, c->nee,
-                                                                       c->nvv, c->nev););
+    NXD_K(c, NXD_PROF_OTHER, item_counts, (grid_for(c->pair_cap, 256)), (256), (0), &c->sc->n_pairs, c->pair_cap, c->topn, c->nfv, c->nee,
+                                                                       c->nvv, c->nev);
     int* tot = c->i_scratch + 4;
-    NXD_LAUNCH(c, NXD_PROF_SCAN, k_scan<<<1, 1024, 0, c->stream>>>(c->nev, c->off_ev, c->pair_cap, tot, nullptr, nullptr, &c->sc->n_pairs););
+    NXD_K(c, NXD_PROF_SCAN, scan, (1), (1024), (0), c->nev, c->off_ev, c->pair_cap, tot, nullptr, nullptr, &c->sc->n_pairs);
     NXD_CUDA(cudaStreamSynchronize(c->stream));
     Scalars h;
     int nev_total = 0;
@@ -678,8 +704,8 @@ nxd_status nxd_detect_contacts(nxd_ctx* c, const double* x, nxd_contact* out, in
     launch_candidates(c, &c->sc->dhat, 0.0);
     if (x) {
         NXD_CUDA(cudaMemcpyAsync(c->S.xt, x, 6 * (size_t)c->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-        NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_pose_at_x<<<grid_for(c->N, 128), 128, 0, c->stream>>>(c->N, c->S.xt, c->quat, c->pose_p, c->pose_q););
-        NXD_LAUNCH(c, NXD_PROF_ASSEMBLY, k_world_vertices<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(c->geo, c->nv, c->vbody, c->pose_p, c->pose_q, c->wvx););
+        NXD_K(c, NXD_PROF_ASSEMBLY, pose_at_x, (grid_for(c->N, 128)), (128), (0), c->N, c->S.xt, c->quat, c->pose_p, c->pose_q);
+        NXD_K(c, NXD_PROF_ASSEMBLY, world_vertices, (grid_for(c->nv, 256)), (256), (0), c->geo, c->nv, c->vbody, c->pose_p, c->pose_q, c->wvx);
         launch_narrow_full(c, c->wvx, c->pose_p, nullptr);
     } else {
         launch_narrow_full(c, c->wv, c->pos, nullptr);
@@ -697,15 +723,15 @@ nxd_status nxd_scene_min_distance(nxd_ctx* c, double* out) {
     if (!c || !out) return NXD_INVALID_ARGUMENT;
     launch_assembly(c);
     cudaStream_t st = c->stream;
-    NXD_LAUNCH(c, NXD_PROF_OTHER, k_body_md_tol<<<grid_for(c->N, 128), 128, 0, st>>>(c->geo, c->pos, c->md_tol););
-    NXD_LAUNCH(c, NXD_PROF_OTHER, k_max_tol<<<1, 1, 0, st>>>(c->md_tol, c->N, c->max_md_tol););
+    NXD_K(c, NXD_PROF_OTHER, body_md_tol, (grid_for(c->N, 128)), (128), (0), c->geo, c->pos, c->md_tol);
+    NXD_K(c, NXD_PROF_OTHER, max_tol, (1), (1), (0), c->md_tol, c->N, c->max_md_tol);
     // force the gate open: bmd = 0
-    NXD_LAUNCH(c, NXD_PROF_OTHER, k_init_scalar_d<<<1, 1, 0, st>>>(&c->sc->bmd, 0.0););
-    NXD_LAUNCH(c, NXD_PROF_OTHER, k_md_gate<<<1, 1, 0, st>>>(c->sc, c->max_md_tol););
+    NXD_K(c, NXD_PROF_OTHER, init_scalar_d, (1), (1), (0), &c->sc->bmd, 0.0);
+    NXD_K(c, NXD_PROF_OTHER, md_gate, (1), (1), (0), c->sc, c->max_md_tol);
     PairQuery qm{2, &c->sc->md_radius, 0.0, 1.0, 0.0};
     launch_pairs(c, qm, c->md_pairs, &c->sc->n_md_pairs, &c->sc->md_gate);
-    NXD_LAUNCH(c, NXD_PROF_MIN_DISTANCE, k_min_distance<<<c->n_sm * 4, 256, 0, st>>>(c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
-                                                &c->sc->md, &c->sc->md_gate););
+    NXD_K(c, NXD_PROF_MIN_DISTANCE, min_distance, (c->n_sm * 4), (256), (0), c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
+                                                &c->sc->md, &c->sc->md_gate);
     NXD_CUDA(cudaStreamSynchronize(st));
     Scalars h;
     NXD_CUDA(cudaMemcpy(&h, c->sc, sizeof(h), cudaMemcpyDeviceToHost));
@@ -826,14 +852,113 @@ nxd_status nxd_normal_forces(nxd_ctx* c, const double* x, double* out, int32_t n
 }
 
 // ---------------------------------------------------------------------------
-// Batched scenes: one context per scene sharing one stream.
+// Batched scenes: one context per scene; the step sequences of all scenes are
+// recorded, scenes with identical sequences form a group, and each group's
+// step is one CUDA graph of batched launches (one launch per kernel position
+// for all of the group's scenes, gridDim.y = scenes).
 // ---------------------------------------------------------------------------
 }  // extern "C"
+
+namespace {
+
+struct BatchGroup {
+    std::vector<int> scenes;
+    std::vector<const void*> kern;
+    std::vector<dim3> grid, block;
+    std::vector<size_t> smem, table_off;
+    void* table = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+}  // namespace
 
 struct nxd_batch {
     std::vector<nxd_ctx*> ctx;
     cudaStream_t stream = nullptr;
+    std::vector<double> dts;           // the dts the groups were recorded with
+    std::vector<BatchGroup> groups;
+    bool own_stream = true;
 };
+
+namespace {
+
+void release_groups(nxd_batch* b) {
+    for (BatchGroup& g : b->groups) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+        if (g.table) cudaFree(g.table);
+    }
+    b->groups.clear();
+}
+
+// Records every scene's step with its dt and builds the group graphs.
+nxd_status build_groups(nxd_batch* b, const double* dts) {
+    release_groups(b);
+    const int n = (int)b->ctx.size();
+    std::vector<std::vector<LaunchRec>> recs(n);
+    for (int i = 0; i < n; ++i) {
+        nxd_ctx* c = b->ctx[i];
+        c->rec = &recs[i];
+        const nxd_status st = enqueue_step(c, dts[i]);
+        c->rec = nullptr;
+        if (st != NXD_OK) return st;
+    }
+    auto same_seq = [&](int i, int j) {
+        if (recs[i].size() != recs[j].size()) return false;
+        for (size_t k = 0; k < recs[i].size(); ++k) {
+            const LaunchRec &x = recs[i][k], &y = recs[j][k];
+            if (x.kern != y.kern || x.block.x != y.block.x || x.block.y != y.block.y || x.block.z != y.block.z) return false;
+        }
+        return true;
+    };
+    for (int i = 0; i < n; ++i) {
+        bool placed = false;
+        for (BatchGroup& g : b->groups)
+            if (same_seq(g.scenes[0], i)) { g.scenes.push_back(i); placed = true; break; }
+        if (!placed) { b->groups.emplace_back(); b->groups.back().scenes.push_back(i); }
+    }
+    for (BatchGroup& g : b->groups) {
+        const std::vector<LaunchRec>& r0 = recs[g.scenes[0]];
+        const size_t L = r0.size(), ns = g.scenes.size();
+        size_t bytes = 0;
+        for (size_t k = 0; k < L; ++k) {
+            g.table_off.push_back(bytes);
+            bytes += (r0[k].args.size() * ns + 255) / 256 * 256;
+        }
+        std::vector<unsigned char> host(std::max<size_t>(bytes, 1));
+        for (size_t k = 0; k < L; ++k) {
+            unsigned gx = 1;
+            size_t smem = 0;
+            for (size_t q = 0; q < ns; ++q) {
+                const LaunchRec& r = recs[g.scenes[q]][k];
+                gx = std::max(gx, r.grid.x);
+                smem = std::max(smem, r.smem);
+                std::memcpy(host.data() + g.table_off[k] + q * r.args.size(), r.args.data(), r.args.size());
+            }
+            g.kern.push_back(r0[k].kern);
+            g.grid.push_back(dim3(gx, (unsigned)ns, 1));
+            g.block.push_back(r0[k].block);
+            g.smem.push_back(smem);
+            if (smem > 48 * 1024)
+                NXD_CUDA(cudaFuncSetAttribute(r0[k].kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        }
+        NXD_CUDA(cudaMalloc(&g.table, host.size()));
+        NXD_CUDA(cudaMemcpy(g.table, host.data(), host.size(), cudaMemcpyHostToDevice));
+        NXD_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        for (size_t k = 0; k < L; ++k) {
+            void* tab = (unsigned char*)g.table + g.table_off[k];
+            void* args[] = {&tab};
+            cudaLaunchKernel(g.kern[k], g.grid[k], g.block[k], args, g.smem[k], b->stream);
+        }
+        NXD_CUDA(cudaStreamEndCapture(b->stream, &g.graph));
+        NXD_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+    }
+    b->dts.assign(dts, dts + n);
+    return NXD_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -852,6 +977,7 @@ nxd_status nxd_batch_create(const nxd_scene_desc* descs, int32_t n, nxd_batch** 
             return st;
         }
         c->stream = b->stream;
+        c->newton_grid = 1;   // one CTA per scene in the batched Newton launch
         b->ctx.push_back(c);
     }
     *out = b;
@@ -860,17 +986,36 @@ nxd_status nxd_batch_create(const nxd_scene_desc* descs, int32_t n, nxd_batch** 
 
 void nxd_batch_destroy(nxd_batch* b) {
     if (!b) return;
-    for (nxd_ctx* c : b->ctx) nxd_destroy(c);
-    cudaStreamDestroy(b->stream);
+    cudaStreamSynchronize(b->stream);
+    release_groups(b);
+    for (nxd_ctx* c : b->ctx) { c->stream = nullptr; nxd_destroy(c); }
+    if (b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
 }
 
 nxd_status nxd_batch_step(nxd_batch* b, const double* dts) {
     if (!b || !dts) return NXD_INVALID_ARGUMENT;
-    for (size_t i = 0; i < b->ctx.size(); ++i) {
-        const nxd_status st = nxd_step(b->ctx[i], dts[i]);
+    for (size_t i = 0; i < b->ctx.size(); ++i)
+        if (!(dts[i] > 0.0)) return NXD_INVALID_ARGUMENT;
+    bool same = b->dts.size() == b->ctx.size() && !b->groups.empty();
+    for (size_t i = 0; same && i < b->ctx.size(); ++i) same = b->dts[i] == dts[i];
+    if (!same) {
+        NXD_CUDA(cudaStreamSynchronize(b->stream));
+        const nxd_status st = build_groups(b, dts);
         if (st != NXD_OK) return st;
     }
+    for (BatchGroup& g : b->groups) NXD_CUDA(cudaGraphLaunch(g.exec, b->stream));
+    return NXD_OK;
+}
+
+int32_t nxd_batch_groups(nxd_batch* b) { return b ? (int32_t)b->groups.size() : 0; }
+
+nxd_status nxd_batch_set_stream(nxd_batch* b, void* stream) {
+    if (!b || !stream) return NXD_INVALID_ARGUMENT;
+    NXD_CUDA(cudaStreamSynchronize(b->stream));
+    b->stream = (cudaStream_t)stream;
+    b->own_stream = false;
+    for (nxd_ctx* c : b->ctx) c->stream = b->stream;
     return NXD_OK;
 }
 

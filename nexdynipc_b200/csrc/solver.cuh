@@ -1483,7 +1483,7 @@ __device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, int* s
 // co-resident CTAs (every branch below depends only on grid-reduced values,
 // so all CTAs take the same path and meet at every barrier).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kNewtonThreads) k_newton(Solver S) {
+__device__ __forceinline__ void newton_body(const Solver& S) {
     __shared__ unsigned long long sh_keys[kMaxIncidence];
     __shared__ double sh_red[kRedMaxQ * 32];
     __shared__ int sh_scan[3 * 32];
@@ -1640,5 +1640,7 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton(Solver S) {
                nx_ph_acc[7]);
 #endif
 }
+constexpr int kLB_newton = kNewtonThreads;
+__global__ void __launch_bounds__(kNewtonThreads) k_newton(const __grid_constant__ Solver S) { newton_body(S); }
 
 }  // namespace nx

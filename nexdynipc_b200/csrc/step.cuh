@@ -44,7 +44,7 @@ struct StepCfg {
 
 // IPCSolver::initializeAdaptiveBarrier (IPCSolver.cpp:327-353) +
 // AdaptiveBarrier::initialize (AdaptiveBarrier.h:27-31); runs once per context.
-__global__ void __launch_bounds__(kSolverThreads) k_barrier_init(StepCfg cfg, const double* mass, const double* pos, Scalars* sc) {
+__device__ __forceinline__ void barrier_init_body(const StepCfg& cfg, const double* mass, const double* pos, Scalars* sc) {
     __shared__ double bb[6];
     NX_BLOCK_RED(R);
     if (!cfg.enable_adaptive || sc->barrier_initialized || cfg.N == 0) return;
@@ -61,26 +61,29 @@ __global__ void __launch_bounds__(kSolverThreads) k_barrier_init(StepCfg cfg, co
         sc->barrier_initialized = 1;
     }
 }
+constexpr int kLB_barrier_init = kSolverThreads;
+__global__ void __launch_bounds__(kSolverThreads) k_barrier_init(const __grid_constant__ StepCfg cfg, const double* mass, const double* pos, Scalars* sc) { barrier_init_body(cfg, mass, pos, sc); }
 
-__global__ void k_md_gate(Scalars* sc, const double* max_md_tol) {
+__device__ __forceinline__ void md_gate_body(Scalars* sc, const double* max_md_tol) {
     sc->md_gate = (sc->bmd < sc->dhat * 2.0) ? 1 : 0;
     sc->md = INFINITY;
     sc->md_radius = 0.5 * (kPruneBand + *max_md_tol) + 1e-12;
 }
+constexpr int kLB_md_gate = 0;
+__global__ void k_md_gate(Scalars* sc, const double* max_md_tol) { md_gate_body(sc, max_md_tol); }
 
 // AdaptiveBarrier::updateStiffness (AdaptiveBarrier.h:33-37)
-__global__ void k_kappa_update(Scalars* sc) {
+__device__ __forceinline__ void kappa_update_body(Scalars* sc) {
     if (!sc->md_gate) return;
     const double md = sc->md;
     if (md < INFINITY && md < 1e-9 && sc->kappa < 1e20) sc->kappa = dmin(sc->kappa * 2.0, 1e20);
 }
+constexpr int kLB_kappa_update = 0;
+__global__ void k_kappa_update(Scalars* sc) { kappa_update_body(sc); }
 
 // Integrator init / x_tilde (IPCSolver.cpp:839-861, ImplicitEulerIntegrator.cpp:5-11),
 // contact-form flags (IPCSolver.cpp:873-921) and drive set-up (IPCSolver.cpp:923-958).
-__global__ void k_step_setup(StepCfg cfg, double dt, const double* pos, const double* quat, const double* vel,
-                             const double* omega, const double* lacc, const double* aacc, double* x, double* xhat,
-                             double* xprev, double* vprev, double* aprev, double* pos0, double* quat0, Scalars* sc,
-                             const Drv* dprm, double* dfilt, int* dfinit, int* dhas_prev) {
+__device__ __forceinline__ void step_setup_body(const StepCfg& cfg, double dt, const double* pos, const double* quat, const double* vel, const double* omega, const double* lacc, const double* aacc, double* x, double* xhat, double* xprev, double* vprev, double* aprev, double* pos0, double* quat0, Scalars* sc, const Drv* dprm, double* dfilt, int* dfinit, int* dhas_prev) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < cfg.N) {
         for (int k = 0; k < 3; ++k) {
@@ -121,10 +124,12 @@ __global__ void k_step_setup(StepCfg cfg, double dt, const double* pos, const do
         sc->alm_mcv = 0.0; sc->alm_dual = 0.0; sc->alm_cres = 0.0;
     }
 }
+constexpr int kLB_step_setup = 0;
+__global__ void k_step_setup(const __grid_constant__ StepCfg cfg, double dt, const double* pos, const double* quat, const double* vel, const double* omega, const double* lacc, const double* aacc, double* x, double* xhat, double* xprev, double* vprev, double* aprev, double* pos0, double* quat0, Scalars* sc, const Drv* dprm, double* dfilt, int* dfinit, int* dhas_prev) { step_setup_body(cfg, dt, pos, quat, vel, omega, lacc, aacc, x, xhat, xprev, vprev, aprev, pos0, quat0, sc, dprm, dfilt, dfinit, dhas_prev); }
 
 // Contact totals after FV + EE (+VV) passes; gates the VV fallback.
 // stage 2 clears the counts (no detection this step).
-__global__ void k_contact_totals(Scalars* sc, int stage, const int* skip_if, int* skip_vv) {
+__device__ __forceinline__ void contact_totals_body(Scalars* sc, int stage, const int* skip_if, int* skip_vv) {
     if (skip_if && *skip_if != 0) { if (skip_vv) *skip_vv = 1; return; }
     if (stage == 2) { sc->n_contacts = 0; sc->n_contacts_raw = 0; return; }
     if (stage == 0) {
@@ -138,11 +143,13 @@ __global__ void k_contact_totals(Scalars* sc, int stage, const int* skip_if, int
         sc->n_contacts = raw > kMaxContacts ? kMaxContacts : raw;
     }
 }
+constexpr int kLB_contact_totals = 0;
+__global__ void k_contact_totals(Scalars* sc, int stage, const int* skip_if, int* skip_vv) { contact_totals_body(sc, stage, skip_if, skip_vv); }
 
 // std::sort by distance + truncation to 2000 (IPCSolver.cpp:571-577): a
 // bitonic sort on (distance, original position); equal distances keep their
 // detection order.  One CTA; runs only when more than 2000 contacts exist.
-__global__ void k_sort_contacts(Scalars* sc, ContactRec* c, ContactRec* tmp, double* key, int* idx, const int* skip_if) {
+__device__ __forceinline__ void sort_contacts_body(Scalars* sc, ContactRec* c, ContactRec* tmp, double* key, int* idx, const int* skip_if) {
     if (skip_if && *skip_if != 0) return;
     const int raw = sc->n_contacts_raw;
     if (raw <= kMaxContacts) return;
@@ -171,10 +178,12 @@ __global__ void k_sort_contacts(Scalars* sc, ContactRec* c, ContactRec* tmp, dou
     __syncthreads();
     for (int i = threadIdx.x; i < kMaxContacts; i += blockDim.x) c[i] = tmp[i];
 }
+constexpr int kLB_sort_contacts = 0;
+__global__ void k_sort_contacts(Scalars* sc, ContactRec* c, ContactRec* tmp, double* key, int* idx, const int* skip_if) { sort_contacts_body(sc, c, tmp, key, idx, skip_if); }
 
 // After the Newton solve and the detection at x_new (IPCSolver.cpp:1112-1165):
 // normal forces, contact residual, ALM convergence.
-__global__ void __launch_bounds__(kSolverThreads) k_alm_post(Solver S, Scalars* sc, StepCfg cfg, double* nforce_out) {
+__device__ __forceinline__ void alm_post_body(const Solver& S, Scalars* sc, const StepCfg& cfg, double* nforce_out) {
     __shared__ unsigned long long sh_keys[kMaxIncidence];
     NX_BLOCK_RED(R);
     if (sc->alm_done) return;
@@ -240,12 +249,12 @@ __global__ void __launch_bounds__(kSolverThreads) k_alm_post(Solver S, Scalars* 
             sc->alm_done = 1;
     }
 }
+constexpr int kLB_alm_post = kSolverThreads;
+__global__ void __launch_bounds__(kSolverThreads) k_alm_post(const __grid_constant__ Solver S, Scalars* sc, const __grid_constant__ StepCfg cfg, double* nforce_out) { alm_post_body(S, sc, cfg, nforce_out); }
 
 // ImplicitEuler::update_quantities + write-back (IPCSolver.cpp:1168-1195)
 // and the velocity-drive KPIs (IPCSolver.cpp:1197-1215).
-__global__ void k_update_state(StepCfg cfg, const double* x, const double* xprev, const double* vprev, double* pos,
-                               double* quat, double* vel, double* omega, double* lacc, double* aacc, Scalars* sc,
-                               const int* da, const int* db, const Drv* dprm, const double* dfilt) {
+__device__ __forceinline__ void update_state_body(const StepCfg& cfg, const double* x, const double* xprev, const double* vprev, double* pos, double* quat, double* vel, double* omega, double* lacc, double* aacc, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const double dt = sc->dt;
     if (i < cfg.N) {
@@ -260,9 +269,10 @@ __global__ void k_update_state(StepCfg cfg, const double* x, const double* xprev
         stq(quat + 4 * i, rot_gt(ldq(quat + 4 * i), ld3(x + 6 * i + 3)));
     }
 }
+constexpr int kLB_update_state = 0;
+__global__ void k_update_state(const __grid_constant__ StepCfg cfg, const double* x, const double* xprev, const double* vprev, double* pos, double* quat, double* vel, double* omega, double* lacc, double* aacc, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt) { update_state_body(cfg, x, xprev, vprev, pos, quat, vel, omega, lacc, aacc, sc, da, db, dprm, dfilt); }
 
-__global__ void k_drive_kpi(StepCfg cfg, const double* omega, Scalars* sc, const int* da, const int* db, const Drv* dprm,
-                            const double* dfilt) {
+__device__ __forceinline__ void drive_kpi_body(const StepCfg& cfg, const double* omega, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt) {
     double max_vw = 0.0;
     int sat = 0;
     for (int d = 0; d < cfg.D; ++d) {
@@ -279,6 +289,8 @@ __global__ void k_drive_kpi(StepCfg cfg, const double* omega, Scalars* sc, const
     sc->last_vw = max_vw;
     sc->last_tsat = cfg.D > 0 ? (double)sat / cfg.D : 0.0;
 }
+constexpr int kLB_drive_kpi = 0;
+__global__ void k_drive_kpi(const __grid_constant__ StepCfg cfg, const double* omega, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt) { drive_kpi_body(cfg, omega, sc, da, db, dprm, dfilt); }
 
 }  // namespace nx
 

@@ -60,6 +60,10 @@ def lib():
     L.nxd_batch_step.argtypes = [vp, dp]
     L.nxd_batch_get_state.argtypes = [vp, C.c_int32, C.POINTER(abi.NxdState)]
     L.nxd_batch_get_diagnostics.argtypes = [vp, C.c_int32, C.POINTER(abi.NxdDiagnostics)]
+    L.nxd_batch_groups.argtypes = [vp]
+    L.nxd_batch_groups.restype = C.c_int32
+    L.nxd_batch_set_stream.argtypes = [vp, vp]
+    L.nxd_batch_set_stream.restype = C.c_int
     L.nxd_body_pairs_noalloc.argtypes = [vp, vp, vp, C.c_int32, C.c_double, vp, C.c_int64, i64p, vp]
     L.nxd_body_pairs_noalloc.restype = C.c_int
     L.nxd_profile.argtypes = [vp, C.c_int32, dp, i64p]
@@ -262,6 +266,14 @@ class Batch:
     def step(self, n: int = 1):
         for _ in range(n):
             _check("nxd_batch_step", lib().nxd_batch_step(self.h, abi.dptr(self.dts)))
+
+    def set_stream(self, stream_ptr: int):
+        """Issue the batch's work on a caller's CUDA stream (raw cudaStream_t)."""
+        _check("nxd_batch_set_stream", lib().nxd_batch_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def groups(self) -> int:
+        """Number of launch groups (scenes with identical step sequences)."""
+        return int(lib().nxd_batch_groups(self.h))
 
     def state(self, i: int) -> dict:
         sb = abi.StateBuffers(self.scenes[i].n_bodies)

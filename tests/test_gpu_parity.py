@@ -244,14 +244,25 @@ def test_trajectory_double_pendulum_meshless():
 
 
 def test_batch_matches_single_scenes():
-    scs = scenes.batched_scenes(n_scenes=6)
-    b = runtime().Batch(scs)
+    # batched launches (one launch per kernel for all scenes of a group)
+    # against the same scenes stepped one context at a time: identical bits;
+    # against the oracle: the trajectory tolerance
+    scs = scenes.batched_scenes(n_scenes=12)
+    rt = runtime()
+    b = rt.Batch(scs)
+    singles = [rt.Context(s) for s in scs]
     ows = [refcpu.OracleWorld(s) for s in scs]
     for _ in range(10):
         b.step()
+        for c in singles:
+            c.step()
         for o in ows:
             o.step()
-    for i, (s, o) in enumerate(zip(scs, ows)):
-        sg, so = b.state(i), o.state()
+    assert 1 <= b.groups() <= len(scs)
+    for i, (s, c, o) in enumerate(zip(scs, singles, ows)):
+        sg, sc_, so = b.state(i), c.state(), o.state()
+        for k in sg:
+            assert np.array_equal(sg[k], sc_[k]), (i, k)
+        assert b.diagnostics(i)["status"] == 0
         assert np.abs(sg["position"] - so["position"]).max() <= 1e-6
         assert quat_angle(sg["orientation"], so["orientation"]).max() <= 1e-6
