@@ -99,13 +99,43 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def algorithmic_narrow_bytes(ctx_diag_items):
-    """Compulsory bytes of one narrow-phase pass: per face-vertex candidate
-    16 B of ids + 4 x 24 B of vertex coordinates, per edge-edge candidate
-    24 B + 4 x 24 B, plus the 1 B hit flag written and read back; 88 B per
-    contact written."""
-    fv, ee, contacts = ctx_diag_items
-    return fv * (16 + 96 + 2) + ee * (24 + 96 + 2) + contacts * 88
+def candidate_operand_bytes(fv: int, ee: int, contacts: int) -> int:
+    """Operand bytes of one narrow-phase pass counted per candidate: per
+    face-vertex candidate 16 B of ids + 4 x 24 B of vertex coordinates, per
+    edge-edge candidate 24 B + 4 x 24 B; 88 B per contact written."""
+    return fv * (16 + 96) + ee * (24 + 96) + contacts * 88
+
+
+def staged_pair_bytes(n_pairs: int, contacts: int) -> int:
+    """Bytes one narrow-phase pass must move: per body pair its two ids, the
+    six top-32 id lists (768 B + 24 B of sizes), the coordinates of the 64
+    selected vertices (24 B each), the 64 selected faces (12 B of ids + 3 x
+    24 B of coordinates) and the 64 selected edges (8 B + 2 x 24 B), each
+    read once per pair; 88 B per contact written."""
+    return n_pairs * (8 + 768 + 24 + 64 * 24 + 64 * 84 + 64 * 56) + contacts * 88
+
+
+def ncu_traffic():
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    from the ncu summaries under profiles/ ('traffic <kernel> <bytes>')."""
+    out = {}
+    pdir = os.path.join(ROOT, "profiles")
+    for fn in sorted(os.listdir(pdir)) if os.path.isdir(pdir) else []:
+        with open(os.path.join(pdir, fn)) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) == 3 and parts[0] == "traffic":
+                    out[parts[1]] = int(parts[2])
+    return out
+
+
+def newton_bytes(n_bodies: int, n_joints: int, n_contacts: float) -> float:
+    """Compulsory bytes of one Newton iteration of the block-sparse direct
+    solve: every 6x6 Hessian block (bodies, joint and contact couplings)
+    written and read once (2 x 288 B), seven passes over 6N-vectors (x, g,
+    contact gradient, dx, trial x: 8 B x 6N each), 88 B per contact and about
+    800 B of parameters, multipliers and Jacobian per joint."""
+    return 2 * 288.0 * (n_bodies + n_joints + n_contacts) + 7 * 48.0 * n_bodies + 88.0 * n_contacts + 800.0 * n_joints
 
 
 def cpu_baseline_sample(scene_fn, threads: int, stride: int):
@@ -227,28 +257,34 @@ def main():
     from nexdynipc_b200 import abi, runtime, scenes
 
     sc = scenes.hopper_chains()
+    # two contexts of the same scene: the step is deterministic, so both pass
+    # through identical states; ctx is timed (graph replay), ctx_prof steps
+    # the same step indices with CUDA events around every launch
     ctx = runtime.Context(sc)
+    ctx_prof = runtime.Context(sc)
     lib = runtime.lib()
     stream = torch.cuda.Stream()
     lib.nxd_set_stream(ctx.h, C.c_void_p(stream.cuda_stream))
+    lib.nxd_set_stream(ctx_prof.h, C.c_void_p(stream.cuda_stream))
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")   # > 126 MB L2
     dt = sc.dt
 
-    def step():
-        st = lib.nxd_step(ctx.h, dt)
+    def step(c=ctx):
+        st = lib.nxd_step(c.h, dt)
         if st != 0:
             raise runtime.NxdError("nxd_step", st)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             step()
+            step(ctx_prof)
     torch.cuda.synchronize()
     init_state = ctx.state()
 
-    # --- device-timed steps (inputs resident in HBM), L2 flushed between steps
-    prof_ms = np.zeros(9)
-    prof_n = np.zeros(9, dtype=np.int64)
-    lib.nxd_profile(ctx.h, 1, None, None)
+    # --- device-timed steps (inputs resident in HBM), L2 flushed between
+    # steps; each step is the context's captured CUDA graph (no per-launch
+    # events inside the timed region)
+    lib.nxd_profile(ctx.h, 0, None, None)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     if ws > 1:
@@ -262,9 +298,24 @@ def main():
                 step()
                 ends[k].record(stream)
         torch.cuda.synchronize()
-    lib.nxd_profile(ctx.h, 0, abi.dptr(prof_ms), prof_n.ctypes.data_as(C.POINTER(C.c_int64)))
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = float(sum(step_ms))
+    timed_n = np.zeros(9, dtype=np.int64)
+    lib.nxd_profile(ctx.h, 0, None, timed_n.ctypes.data_as(C.POINTER(C.c_int64)))
+    # --- the same step indices on the twin context with CUDA events around
+    # every launch (direct launches): per-family device time
+    prof_ms = np.zeros(9)
+    prof_n = np.zeros(9, dtype=np.int64)
+    lib.nxd_profile(ctx_prof.h, 1, None, None)
+    prof_steps = []
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            step(ctx_prof)
+            prof_steps.append(ctx_prof.diagnostics())   # synchronises; events bracket the launches only
+    torch.cuda.synchronize()
+    lib.nxd_profile(ctx_prof.h, 0, abi.dptr(prof_ms), prof_n.ctypes.data_as(C.POINTER(C.c_int64)))
+    twin_equal = bool(np.array_equal(ctx.state()["position"], ctx_prof.state()["position"]))
     diag = ctx.diagnostics()
     if ws > 1:
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
@@ -305,23 +356,46 @@ def main():
         e2e_s = float(t.item())
     e2e = ws * args.steps / e2e_s
 
-    # --- roofline of the dominant kernel family, timed live above
-    fam = int(np.argmax(prof_ms))
+    # --- roofline of the dominant kernel family (timed on the twin context
+    # over the same step indices) and of the narrow phase
     peak, peak_kind = measured_peaks()
-    roof = {"kernel": FAMILIES[fam], "bound": "hbm", "unit": "GB/s", "peak": peak, "peak_kind": peak_kind,
-            "ms_per_launch": float(prof_ms[fam] / max(prof_n[fam], 1)), "launches": int(prof_n[fam]),
-            "share_of_step_time": float(prof_ms[fam] / max(prof_ms.sum(), 1e-30))}
-    if FAMILIES[fam] == "narrow_phase" and cand_counts:
+
+    def family_roof(i):
+        return {"kernel": FAMILIES[i], "bound": "hbm", "unit": "GB/s", "peak": peak, "peak_kind": peak_kind,
+                "ms_per_launch": float(prof_ms[i] / max(prof_n[i], 1)), "launches": int(prof_n[i]),
+                "share_of_step_time": float(prof_ms[i] / max(prof_ms.sum(), 1e-30)), "traffic": None}
+
+    n_joints = int(sc.joint_type.shape[0])
+    newton_iters = int(sum(d["newton_iterations"] for d in prof_steps))
+    mean_contacts = float(np.mean([d["n_contacts"] for d in prof_steps]))
+    traffic = ncu_traffic()
+    roof_newton = family_roof(FAMILIES.index("newton"))
+    roof_newton["traffic"] = traffic.get("k_newton")
+    nb = newton_bytes(sc.n_bodies, n_joints, mean_contacts)
+    ach = nb * newton_iters / (prof_ms[FAMILIES.index("newton")] / 1e3) / 1e9
+    roof_newton.update(achieved=ach, frac=ach / peak, algorithmic_bytes_per_newton_iteration=nb,
+                       newton_iterations=newton_iters,
+                       note=("latency-bound: one Newton solve per ALM iteration on a cooperative grid of CTAs, "
+                             "about 25 grid barriers per Newton iteration; HBM is not the limiter"))
+    roof_narrow = family_roof(FAMILIES.index("narrow_phase"))
+    roof_narrow["traffic"] = traffic.get("k_narrow_rows")
+    if cand_counts:
         fv, ee = cand_counts
-        # per launch: the count kernel reads the items, the write kernel
-        # re-reads the flags; count both launches of a pass as one unit
-        bytes_pass = algorithmic_narrow_bytes((fv, ee, diag["n_contacts"]))
-        passes = prof_n[fam] / 6.0
-        achieved = bytes_pass * passes / (prof_ms[fam] / 1e3) / 1e9
-        roof.update(achieved=achieved, frac=achieved / peak, traffic=None,
-                    algorithmic_bytes_per_pass=bytes_pass)
-    else:
-        roof.update(achieved=None, frac=None, traffic=None)
+        # a detection pass is 4 launches (FV+EE rows, their hit emission, and
+        # the gated VV rows / emission); count the pass as one unit
+        passes = prof_n[FAMILIES.index("narrow_phase")] / 4.0
+        secs = prof_ms[FAMILIES.index("narrow_phase")] / 1e3
+        bytes_pass = staged_pair_bytes(diag["n_body_pairs"], diag["n_contacts"])
+        per_cand = candidate_operand_bytes(fv, ee, diag["n_contacts"])
+        ach = bytes_pass * passes / secs / 1e9
+        roof_narrow.update(achieved=ach, frac=ach / peak, algorithmic_bytes_per_pass=bytes_pass,
+                           per_candidate_operand_gbs=per_cand * passes / secs / 1e9,
+                           note=("compute-bound: each pair's selected primitives are staged once and every "
+                                 "candidate is tested from registers / shared memory (ncu: FP64 pipe ~40 % "
+                                 "active); per_candidate_operand_gbs counts every candidate's operands"))
+    fam = int(np.argmax(prof_ms))
+    roof = roof_newton if FAMILIES[fam] == "newton" else (roof_narrow if FAMILIES[fam] == "narrow_phase"
+                                                          else dict(family_roof(fam), achieved=None, frac=None))
     per_family = {FAMILIES[i]: {"ms": round(float(prof_ms[i]), 3), "launches": int(prof_n[i])} for i in range(9)}
 
     batched = None
@@ -336,17 +410,22 @@ def main():
                "sample": (f"first step of the same scene through the CPU oracle (serial, as the reference runs; "
                           f"the reference itself cannot be built here), literal computeSceneMinDistance over bodies "
                           f"i % {stride} == 0 scaled x{stride}; {wall:.1f} s wall")}
-    launches_total = int(prof_n.sum())
+    launches_total = int(timed_n.sum())
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "replicas": ws, "l2": "flushed between steps (256 MiB write, untimed)",
+                   "timing": ("value: K steps, each the step's CUDA graph, CUDA events per step; per_family_ms and "
+                              "roofline: the same K step indices on a twin context of the same scene with CUDA "
+                              "events around every launch"),
+                   "twin_state_equal": twin_equal,
                    "per_family_ms": per_family, "last_step": {k: diag[k] for k in
                                                               ("n_body_pairs", "n_contacts", "alm_iterations",
                                                                "newton_iterations", "status")},
                    "batched": batched},
         "roofline": roof,
+        "roofline_narrow_phase": roof_narrow,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": launches_total,
@@ -355,6 +434,7 @@ def main():
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
+    ctx_prof.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
 

@@ -108,6 +108,13 @@ struct nxd_ctx {
     int cand_stride = 0;
     // when set, launches are recorded here (batched replay) instead of issued
     std::vector<LaunchRec>* rec = nullptr;
+    // nxd_step as a CUDA graph, captured per dt on a private stream
+    cudaStream_t cap_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    double graph_dt = 0.0;
+    bool graph_off = false;
+    long long graph_launches[NXD_PROF_FAMILIES] = {};
 };
 
 namespace {
@@ -254,12 +261,6 @@ void launch_candidates(nxd_ctx* c, const double* act_ptr, double act_val) {
     while (warps > 1 && topk_smem(c, warps) > 200 * 1024) --warps;
     NXD_K(c, NXD_PROF_TOPK, topk, (c->n_sm * 4), (32 * warps), (topk_smem(c, warps)), c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap,
                                                                        c->boxes, c->wv, c->topk, c->topn, c->max_prims);
-    NXD_K(c, NXD_PROF_OTHER, item_counts, (grid_for(c->pair_cap, 256)), (256), (0), &c->sc->n_pairs, c->pair_cap, c->topn, c->nfv,
-                                                                       c->nee, c->nvv, c->nev);
-    const int* np = &c->sc->n_pairs;
-    NXD_K(c, NXD_PROF_SCAN, scan, (1), (1024), (0), c->nfv, c->off_fv, c->pair_cap, &c->sc->fv_items, nullptr, nullptr, np);
-    NXD_K(c, NXD_PROF_SCAN, scan, (1), (1024), (0), c->nee, c->off_ee, c->pair_cap, &c->sc->ee_items, nullptr, nullptr, np);
-    NXD_K(c, NXD_PROF_SCAN, scan, (1), (1024), (0), c->nvv, c->off_vv, c->pair_cap, &c->sc->vv_items, nullptr, nullptr, np);
 }
 
 }  // namespace
@@ -370,6 +371,10 @@ nxd_status enqueue_step(nxd_ctx* c, double dt) {
 // ===========================================================================
 // C ABI
 // ===========================================================================
+namespace {
+void drop_step_graph(nxd_ctx* c);
+}  // namespace
+
 extern "C" {
 
 void nxd_default_settings(nxd_settings* s) {
@@ -575,6 +580,8 @@ void nxd_destroy(nxd_ctx* c) {
     for (auto& v : c->ev)
         for (auto& pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
     for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
+    drop_step_graph(c);
+    if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     c->mem.release();
     delete c;
 }
@@ -585,9 +592,64 @@ nxd_status nxd_set_stream(nxd_ctx* c, void* stream) {
     return NXD_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+void drop_step_graph(nxd_ctx* c) {
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->graph_exec = nullptr;
+    c->graph = nullptr;
+}
+
+// Captures enqueue_step(c, dt) into c->graph_exec; false if the capture or
+// the instantiation is refused (the step then runs as direct launches).
+bool capture_step(nxd_ctx* c, double dt) {
+    drop_step_graph(c);
+    if (!c->cap_stream && cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking) != cudaSuccess) return false;
+    long long before[NXD_PROF_FAMILIES];
+    std::memcpy(before, c->launches, sizeof(before));
+    cudaStream_t saved = c->stream;
+    c->stream = c->cap_stream;
+    bool ok = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+        const nxd_status st = enqueue_step(c, dt);
+        const cudaError_t e = cudaStreamEndCapture(c->cap_stream, &c->graph);
+        ok = st == NXD_OK && e == cudaSuccess && c->graph;
+    }
+    c->stream = saved;
+    for (int f = 0; f < NXD_PROF_FAMILIES; ++f) {
+        c->graph_launches[f] = c->launches[f] - before[f];
+        c->launches[f] = before[f];
+    }
+    if (ok) ok = cudaGraphInstantiate(&c->graph_exec, c->graph, 0) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        drop_step_graph(c);
+        return false;
+    }
+    c->graph_dt = dt;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
 nxd_status nxd_step(nxd_ctx* c, double dt) {
     if (!c || !(dt > 0.0)) return NXD_INVALID_ARGUMENT;
-    return enqueue_step(c, dt);
+    // per-family event timing needs direct launches
+    if (c->prof || c->graph_off) return enqueue_step(c, dt);
+    if (!c->graph_exec || c->graph_dt != dt) {
+        if (!capture_step(c, dt)) {
+            c->graph_off = true;
+            return enqueue_step(c, dt);
+        }
+    }
+    for (int f = 0; f < NXD_PROF_FAMILIES; ++f) c->launches[f] += c->graph_launches[f];
+    NXD_CUDA(cudaGraphLaunch(c->graph_exec, c->stream));
+    return NXD_OK;
 }
 
 nxd_status nxd_get_state(nxd_ctx* c, const nxd_state* o) {
@@ -661,8 +723,13 @@ nxd_status nxd_build_candidates(nxd_ctx* c, double act, nxd_candidates* o) {
     if (!c || !o) return NXD_INVALID_ARGUMENT;
     launch_assembly(c);
     launch_candidates(c, nullptr, act);
+    // per-pair item counts and offsets of the four candidate lists
     NXD_K(c, NXD_PROF_OTHER, item_counts, (grid_for(c->pair_cap, 256)), (256), (0), &c->sc->n_pairs, c->pair_cap, c->topn, c->nfv, c->nee,
                                                                        c->nvv, c->nev);
+    const int* np = &c->sc->n_pairs;
+    NXD_K(c, NXD_PROF_SCAN, scan, (1), (1024), (0), c->nfv, c->off_fv, c->pair_cap, &c->sc->fv_items, nullptr, nullptr, np);
+    NXD_K(c, NXD_PROF_SCAN, scan, (1), (1024), (0), c->nee, c->off_ee, c->pair_cap, &c->sc->ee_items, nullptr, nullptr, np);
+    NXD_K(c, NXD_PROF_SCAN, scan, (1), (1024), (0), c->nvv, c->off_vv, c->pair_cap, &c->sc->vv_items, nullptr, nullptr, np);
     int* tot = c->i_scratch + 4;
     NXD_K(c, NXD_PROF_SCAN, scan, (1), (1024), (0), c->nev, c->off_ev, c->pair_cap, tot, nullptr, nullptr, &c->sc->n_pairs);
     NXD_CUDA(cudaStreamSynchronize(c->stream));
