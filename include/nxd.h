@@ -302,6 +302,40 @@ nxd_status nxd_batch_get_diagnostics(nxd_batch* b, int32_t scene, nxd_diagnostic
 int32_t nxd_batch_groups(nxd_batch* b);
 nxd_status nxd_batch_set_stream(nxd_batch* b, void* stream);
 
+/* Primitive-level contact model (full IPC).  No counterpart in the
+ * reference, which only has the body-COM barrier (its design notes plan
+ * this replacement: documents/2026.02.28, rigid-ipc replacement plan).
+ * Primitives are numbered over bodies in world order: vertices, faces and
+ * the unique edges of each body's mesh (as in nxd_build_candidates).
+ * x is the 6N optimisation vector (NULL: the current poses).  Calls
+ * synchronise the context's stream and return host results; device
+ * buffers grow on demand.
+ *
+ * nxd_ipc_candidates: point-triangle pairs (vertex, face) and edge-edge
+ * pairs (edge i < edge j) of different bodies whose boxes overlap, the
+ * primitive box inflated by `inflation` (swept over x -> x + dx when dx is
+ * given); LBVH over Morton codes.  Sorted by (first, second). */
+nxd_status nxd_ipc_candidates(nxd_ctx* ctx, const double* x, const double* dx, double inflation,
+                              int32_t* pt, int64_t pt_cap, int32_t* ee, int64_t ee_cap,
+                              int64_t* n_pt, int64_t* n_ee);
+/* nxd_ipc_barrier: the barrier form over the candidates at x (boxes
+ * inflated by dhat), in the Form interface's three parts (Form.h:8-21):
+ * energy sum_pairs b(d^2), b(s) = -kappa (s - dhat^2)^2 ln(s / dhat^2); the
+ * gradient over the 6N DOFs (overwritten); the Hessian with each pair's
+ * 12x12 block projected to PSD, chained to the two bodies' DOFs through
+ * [I, -[R r]x], as BSR (row_ptr[N+1], col_idx[nnzb], vals[nnzb*36]
+ * row-major).  *nnzb gets the block count (NXD_CAPACITY if > cap_blocks). */
+nxd_status nxd_ipc_barrier(nxd_ctx* ctx, const double* x, double dhat, double kappa, double* energy,
+                           double* grad, int32_t* row_ptr, int32_t* col_idx, double* vals,
+                           int64_t cap_blocks, int64_t* nnzb, int64_t* n_pairs, int64_t* n_active);
+/* nxd_ipc_max_step: the line-search bound OptimizationProblem::maxStep
+ * (Math/NewtonSolver.h:42) for the step x -> x + dx: the smallest additive-CCD
+ * time of impact in [0, 1] over the pairs whose swept boxes overlap, each
+ * pair keeping eta of its initial distance (points move on the chords
+ * between their positions at x and x + dx). */
+nxd_status nxd_ipc_max_step(nxd_ctx* ctx, const double* x, const double* dx, double eta, double* alpha,
+                            int64_t* n_pairs);
+
 /* Body-pair broad phase for callers that cannot allocate device memory.
  * No counterpart in the reference.  Callers that manage every device byte
  * themselves (a host engine's memory pool, a hard memory cap, a real-time

@@ -1,0 +1,514 @@
+// ipc.cuh — device side of the primitive-level contact model (full IPC,
+// "Mode I"): a linear BVH over dhat-inflated triangle / edge boxes, rebuilt
+// from Morton codes for every evaluation state, stack traversal that emits
+// the compacted point-triangle and edge-edge candidate lists, the per-pair
+// barrier with PSD-projected Hessians chained to 6x6 body blocks (segment
+// reduction into BSR), and additive CCD with a block min-reduce.
+//
+// HBM layout (per context, grown on demand):
+//   wq[nv*3], wq1[nv*3]      world vertices at x and at x + dx
+//   leaf boxes [n*6]          face / edge boxes, inflated (min xyz, max xyz)
+//   keys / ids [n]            (Morton << 32 | index), sorted by a stable LSD
+//                             radix sort on the Morton bits
+//   nodes: child[2(n-1)], parent[2n-1], box[(2n-1)*6], flags[n-1]
+//   pairs pt[n_pt*2] (vertex, face), ee[n_ee*2] (edge i < edge j)
+//   per active pair: energy, chained gradient (12), up to 5 (lambda, z[12])
+#pragma once
+
+#include "geometry.cuh"
+#include "ipc_pair.h"
+
+namespace nx {
+
+// ---------------------------------------------------------------------------
+// Stable LSD radix sort of (64-bit key, int value) pairs on key bits
+// [lo, hi), 8 bits per pass.  A block sorts a tile of kRsTile items: digit
+// histogram, a global digit-major exclusive scan, then a stable scatter
+// (rounds of 256 items in tile order; ranks inside a warp from
+// __match_any_sync, across warps from per-round digit counts).
+// ---------------------------------------------------------------------------
+constexpr int kRsThreads = 256;
+constexpr int kRsRounds = 16;
+constexpr int kRsTile = kRsThreads * kRsRounds;
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const unsigned long long* keys, int n, int shift, int* hist, int nblocks) {
+    __shared__ int h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kRsTile;
+    for (int r = 0; r < kRsRounds; ++r) {
+        const int i = base + r * kRsThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & 0xFF], 1);
+    }
+    __syncthreads();
+    hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void k_rs_scan(int* hist, int n) { block_scan(hist, hist, n); }
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const unsigned long long* kin, const int* vin, unsigned long long* kout,
+                                                           int* vout, int n, int shift, const int* hist, int nblocks) {
+    __shared__ int run[256];
+    __shared__ int wcnt[kRsThreads / 32][256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    run[threadIdx.x] = hist[threadIdx.x * nblocks + blockIdx.x];
+    for (int k = 0; k < kRsThreads / 32; ++k) wcnt[k][threadIdx.x] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kRsTile;
+    for (int r = 0; r < kRsRounds; ++r) {
+        const int i = base + r * kRsThreads + threadIdx.x;
+        const bool ok = i < n;
+        const unsigned long long key = ok ? kin[i] : 0ull;
+        const int d = ok ? (int)((key >> shift) & 0xFF) : 256 + lane;   // idle lanes never match
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const int rank = __popc(peers & ((1u << lane) - 1u));
+        const int leader = __ffs(peers) - 1;
+        if (ok && lane == leader) wcnt[w][d] = __popc(peers);
+        __syncthreads();
+        if (ok) {
+            int pos = run[d] + rank;
+            for (int k = 0; k < w; ++k) pos += wcnt[k][d];
+            kout[pos] = key;
+            vout[pos] = vin[i];
+        }
+        __syncthreads();
+        // advance the running offsets; clear the counts of this round
+        int add = 0;
+        for (int k = 0; k < kRsThreads / 32; ++k) { add += wcnt[k][threadIdx.x]; wcnt[k][threadIdx.x] = 0; }
+        run[threadIdx.x] += add;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Boxes
+// ---------------------------------------------------------------------------
+struct PrimGeo {
+    int nv, nf, ne;
+    const int* vbody;          // [nv]
+    const int* fbody;          // [nf]
+    const int* ebody;          // [ne]
+    const int* fvert;          // [nf*3] global vertex ids
+    const int* evert;          // [ne*2] global vertex ids
+};
+
+__device__ __forceinline__ void box_of(const double* w0, const double* w1, const int* vid, int nvid, double infl, double* out) {
+    V3 mn = ld3(w0 + 3 * vid[0]), mx = mn;
+    for (int k = 0; k < nvid; ++k) {
+        const V3 a = ld3(w0 + 3 * vid[k]);
+        mn = cwmin(mn, a); mx = cwmax(mx, a);
+        if (w1) { const V3 b = ld3(w1 + 3 * vid[k]); mn = cwmin(mn, b); mx = cwmax(mx, b); }
+    }
+    const V3 e = v3(infl, infl, infl);
+    st3(out, mn - e);
+    st3(out + 3, mx + e);
+}
+
+// kind 0: face leaves, 1: edge leaves, 2: vertex queries, 3: edge queries
+__global__ void k_ipc_boxes(PrimGeo pg, int kind, const double* w0, const double* w1, double infl, double* out) {
+    const int n = kind == 0 ? pg.nf : (kind == 2 ? pg.nv : pg.ne);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (kind == 0) box_of(w0, w1, pg.fvert + 3 * i, 3, infl, out + 6 * i);
+        else if (kind == 2) box_of(w0, w1, &i, 1, infl, out + 6 * i);
+        else box_of(w0, w1, pg.evert + 2 * i, 2, infl, out + 6 * i);
+    }
+}
+
+// Global primitive topology from the body-local meshes: one thread per body.
+__global__ void k_prim_topology(Geo g, int* fbody, int* fvert, int* ebody, int* evert) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < g.N; b += gridDim.x * blockDim.x) {
+        const int vo = g.voff[b];
+        for (int f = g.foff[b]; f < g.foff[b + 1]; ++f) {
+            fbody[f] = b;
+            for (int k = 0; k < 3; ++k) fvert[3 * f + k] = vo + g.faces[3 * f + k];
+        }
+        for (int e = g.eoff[b]; e < g.eoff[b + 1]; ++e) {
+            ebody[e] = b;
+            for (int k = 0; k < 2; ++k) evert[2 * e + k] = vo + g.edges[2 * e + k];
+        }
+    }
+}
+
+__global__ void k_axpy_vec(const double* x, const double* dx, int n, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = x[i] + dx[i];
+}
+
+// list[pos[i]] = i for every flagged i (pos = exclusive scan of flag)
+__global__ void k_compact(const int* flag, const int* pos, int n, int* list) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (flag[i]) list[pos[i]] = i;
+}
+
+// Scene bounds of the leaf-box centroids (one block, fixed order).
+__global__ void k_centroid_bounds(const double* box, int n, double* out6) {
+    __shared__ double sm[6][32];
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        for (int a = 0; a < 3; ++a) {
+            const double c = 0.5 * (box[6 * i + a] + box[6 * i + 3 + a]);
+            lo[a] = dmin(lo[a], c); hi[a] = dmax(hi[a], c);
+        }
+    for (int a = 0; a < 3; ++a)
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[a] = dmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+            hi[a] = dmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (l == 0) for (int a = 0; a < 3; ++a) { sm[a][w] = lo[a]; sm[3 + a][w] = hi[a]; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int a = 0; a < 3; ++a) {
+            double L = INFINITY, H = -INFINITY;
+            for (int k = 0; k < nw; ++k) { L = dmin(L, sm[a][k]); H = dmax(H, sm[3 + a][k]); }
+            out6[a] = L; out6[3 + a] = H;
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned expand_bits10(unsigned v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+// key = (30-bit Morton code of the box centroid) << 32 | leaf index
+__global__ void k_morton(const double* box, int n, const double* bounds, unsigned long long* keys, int* ids) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        unsigned q[3];
+        for (int a = 0; a < 3; ++a) {
+            const double ext = bounds[3 + a] - bounds[a];
+            const double c = 0.5 * (box[6 * i + a] + box[6 * i + 3 + a]);
+            double u = ext > 0.0 ? (c - bounds[a]) / ext : 0.0;
+            u = u < 0.0 ? 0.0 : (u > 1.0 ? 1.0 : u);
+            unsigned v = (unsigned)(u * 1023.0);
+            q[a] = v > 1023u ? 1023u : v;
+        }
+        const unsigned m = (expand_bits10(q[0]) << 2) | (expand_bits10(q[1]) << 1) | expand_bits10(q[2]);
+        keys[i] = ((unsigned long long)m << 32) | (unsigned)i;
+        ids[i] = i;
+    }
+}
+
+// Karras (2012) hierarchy over sorted unique keys: internal node i spans a
+// key range that starts or ends at i; its split is the highest differing bit.
+// Children >= 0 are internal nodes, ~leaf for leaves (leaf slot in sorted order).
+__device__ __forceinline__ int kdelta(const unsigned long long* k, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    return __clzll(k[i] ^ k[j]);
+}
+
+__global__ void k_karras(const unsigned long long* k, int n, int* child, int* parent) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x) {
+        const int d = (kdelta(k, n, i, i + 1) - kdelta(k, n, i, i - 1)) >= 0 ? 1 : -1;
+        const int dmin_ = kdelta(k, n, i, i - d);
+        int lmax = 2;
+        while (lmax < 2 * n && kdelta(k, n, i, i + lmax * d) > dmin_) lmax <<= 1;
+        int l = 0;
+        for (int t = lmax >> 1; t >= 1; t >>= 1)
+            if (kdelta(k, n, i, i + (l + t) * d) > dmin_) l += t;
+        const int j = i + l * d;
+        const int dnode = kdelta(k, n, i, j);
+        int s = 0, t = l;
+        while (t > 1) {
+            t = (t + 1) >> 1;
+            if (kdelta(k, n, i, i + (s + t) * d) > dnode) s += t;
+        }
+        const int gamma = i + s * d + (d < 0 ? -1 : 0);
+        const int lo = i < j ? i : j, hi = i < j ? j : i;
+        const int left = lo == gamma ? ~gamma : gamma;
+        const int right = hi == gamma + 1 ? ~(gamma + 1) : gamma + 1;
+        child[2 * i] = left;
+        child[2 * i + 1] = right;
+        parent[left >= 0 ? left : (n - 1) + ~left] = i;
+        parent[right >= 0 ? right : (n - 1) + ~right] = i;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) parent[0] = -1;   // the root (internal node 0, or the only leaf)
+}
+
+// Bottom-up boxes: node slots 0..n-2 internal, n-1+s leaf s (sorted order).
+// The second child to arrive at a node (atomic counter) merges its two boxes.
+__global__ void k_refit(const double* leaf_box, const int* ids, int n, const int* child, const int* parent, double* nbox,
+                        int* flags) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        double* lb = nbox + 6 * ((n - 1) + s);
+        const double* src = leaf_box + 6 * ids[s];
+        for (int a = 0; a < 6; ++a) lb[a] = src[a];
+        if (n == 1) continue;
+        __threadfence();
+        int node = parent[(n - 1) + s];
+        for (int guard = 0; node >= 0 && guard < 64 + n; ++guard) {
+            if (atomicAdd(&flags[node], 1) == 0) break;   // first arrival: the sibling finishes
+            __threadfence();
+            const int c0 = child[2 * node], c1 = child[2 * node + 1];
+            const double* b0 = nbox + 6 * (c0 >= 0 ? c0 : (n - 1) + ~c0);
+            const double* b1 = nbox + 6 * (c1 >= 0 ? c1 : (n - 1) + ~c1);
+            double* bn = nbox + 6 * node;
+            for (int a = 0; a < 3; ++a) {
+                bn[a] = dmin(__ldcg(b0 + a), __ldcg(b1 + a));
+                bn[3 + a] = dmax(__ldcg(b0 + 3 + a), __ldcg(b1 + 3 + a));
+            }
+            __threadfence();
+            node = parent[node];
+        }
+    }
+}
+
+__device__ __forceinline__ bool boxes_overlap(const double* a, const double* b) {
+    return a[0] <= b[3] && b[0] <= a[3] && a[1] <= b[4] && b[1] <= a[4] && a[2] <= b[5] && b[2] <= a[5];
+}
+
+// Traversal of one query box against the tree; mode 0 counts, mode 1 writes
+// (prim ids ascending within the query: insertion into the query's slice).
+// kind 0: vertex queries vs faces (other body); 1: edge queries vs edges
+// (other body, query < prim).
+constexpr int kTravStack = 96;
+__global__ void k_traverse(PrimGeo pg, int kind, const double* qbox, int nq, const double* nbox, const int* child, const int* ids,
+                           int n, int* cnt, const int* off, int* out, int* status) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        double qb[6];
+        for (int a = 0; a < 6; ++a) qb[a] = qbox[6 * q + a];
+        const int qbody = kind == 0 ? pg.vbody[q] : pg.ebody[q];
+        int c = 0;
+        int* dst = out ? out + 2 * (size_t)off[q] : nullptr;
+        int stack[kTravStack];
+        int top = 0;
+        stack[top++] = n == 1 ? ~0 : 0;
+        while (top > 0) {
+            const int node = stack[--top];
+            const int slot = node >= 0 ? node : (n - 1) + ~node;
+            if (!boxes_overlap(qb, nbox + 6 * slot)) continue;
+            if (node < 0) {
+                const int prim = ids[~node];
+                const int pbody = kind == 0 ? pg.fbody[prim] : pg.ebody[prim];
+                if (pbody == qbody || (kind == 1 && !(q < prim))) continue;
+                if (dst) {
+                    int k = c;
+                    while (k > 0 && dst[2 * (k - 1) + 1] > prim) {
+                        dst[2 * k] = dst[2 * (k - 1)];
+                        dst[2 * k + 1] = dst[2 * (k - 1) + 1];
+                        --k;
+                    }
+                    dst[2 * k] = q;
+                    dst[2 * k + 1] = prim;
+                }
+                ++c;
+                continue;
+            }
+            if (top + 2 > kTravStack) { atomicExch(status, NXD_CAPACITY); continue; }
+            stack[top++] = child[2 * node + 1];
+            stack[top++] = child[2 * node];
+        }
+        if (!out) cnt[q] = c;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per-pair barrier (PT list then EE list), chained to body DOFs.
+// ---------------------------------------------------------------------------
+struct IpcPairs {
+    const int* pt; int n_pt;
+    const int* ee; int n_ee;
+};
+
+struct IpcPose {
+    const double* wq;      // world vertices at x [nv*3]
+    const double* pp;      // body positions at x [N*3]
+};
+
+__device__ __forceinline__ void pair_points(const PrimGeo& pg, const IpcPairs& P, const IpcPose& ps, int p, int& kind,
+                                            V3* X, int* side, V3* arm, int& bA, int& bB) {
+    int vid[4];
+    if (p < P.n_pt) {
+        kind = ipc::kPairPT;
+        const int v = P.pt[2 * p], f = P.pt[2 * p + 1];
+        vid[0] = v; vid[1] = pg.fvert[3 * f]; vid[2] = pg.fvert[3 * f + 1]; vid[3] = pg.fvert[3 * f + 2];
+        bA = pg.vbody[v]; bB = pg.fbody[f];
+        side[0] = 0; side[1] = 1; side[2] = 1; side[3] = 1;
+    } else {
+        kind = ipc::kPairEE;
+        const int q = p - P.n_pt;
+        const int e0 = P.ee[2 * q], e1 = P.ee[2 * q + 1];
+        vid[0] = pg.evert[2 * e0]; vid[1] = pg.evert[2 * e0 + 1]; vid[2] = pg.evert[2 * e1]; vid[3] = pg.evert[2 * e1 + 1];
+        bA = pg.ebody[e0]; bB = pg.ebody[e1];
+        side[0] = 0; side[1] = 0; side[2] = 1; side[3] = 1;
+    }
+    for (int k = 0; k < 4; ++k) {
+        X[k] = ld3(ps.wq + 3 * vid[k]);
+        arm[k] = X[k] - ld3(ps.pp + 3 * (side[k] ? bB : bA));
+    }
+}
+
+struct IpcEvalOut {
+    double* e;         // [n] pair energy
+    double* grad;      // [n*12] chained gradient (A 0..5, B 6..11)
+    double* lam;       // [n*5]
+    double* z;         // [n*5*12]
+    int* nterm;        // [n]
+    int* body;         // [n*2]
+    int* active;       // [n] 1 when d^2 < dhat^2
+    int* type;         // [n] distance type
+};
+
+__global__ void k_ipc_pair_eval(PrimGeo pg, IpcPairs P, IpcPose ps, double dhat, double kappa, IpcEvalOut o) {
+    const int n = P.n_pt + P.n_ee;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        int kind, side[4], bA, bB;
+        V3 X[4], arm[4];
+        pair_points(pg, P, ps, p, kind, X, side, arm, bA, bB);
+        const ipc::DistForm f = ipc::classify(kind, X);
+        const ipc::PairEval ev = ipc::pair_barrier(f, X, dhat, kappa);
+        o.e[p] = ev.e;
+        o.body[2 * p] = bA; o.body[2 * p + 1] = bB;
+        o.type[p] = f.type;
+        o.active[p] = ev.d2 < dhat * dhat ? 1 : 0;
+        ipc::chain12(ev.grad, side, arm, o.grad + 12 * (size_t)p);
+        o.nterm[p] = ev.n_terms;
+        for (int k = 0; k < ev.n_terms; ++k) {
+            o.lam[5 * (size_t)p + k] = ev.lam[k];
+            ipc::chain12(ev.y[k], side, arm, o.z + 60 * (size_t)p + 12 * k);
+        }
+    }
+}
+
+// Contributions of the active pairs: gradient (body, pair, side) and
+// Hessian blocks (row body, col body, pair, block) with their segment keys.
+__global__ void k_ipc_contrib(const int* active_list, int na, const int* body, int N, unsigned long long* gkey, int* gval,
+                              unsigned long long* hkey, int* hval) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
+        const int p = active_list[a];
+        const int b[2] = {body[2 * p], body[2 * p + 1]};
+        for (int s = 0; s < 2; ++s) {
+            gkey[2 * a + s] = (unsigned long long)b[s];
+            gval[2 * a + s] = 2 * p + s;
+        }
+        for (int r = 0; r < 2; ++r)
+            for (int c = 0; c < 2; ++c) {
+                hkey[4 * a + 2 * r + c] = (unsigned long long)b[r] * (unsigned long long)N + (unsigned long long)b[c];
+                hval[4 * a + 2 * r + c] = 4 * p + 2 * r + c;
+            }
+    }
+}
+
+// Segment starts of sorted keys: flag[i] = key changes at i.
+__global__ void k_seg_flags(const unsigned long long* key, int n, int* flag) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        flag[i] = (i == 0 || key[i] != key[i - 1]) ? 1 : 0;
+}
+__global__ void k_seg_starts(const int* flag, const int* pos, int n, int* start, int* nseg) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (flag[i]) start[pos[i]] = i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int m = n > 0 ? pos[n - 1] + flag[n - 1] : 0;
+        *nseg = m;
+        start[m] = n;
+    }
+}
+
+// Gradient: thread per (segment, dof) sums its contributions in pair order.
+__global__ void k_ipc_grad(const unsigned long long* gkey, const int* gval, const int* start, const int* nseg, const double* pgrad,
+                           double* grad) {
+    const int ns = *nseg;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 6 * ns; t += gridDim.x * blockDim.x) {
+        const int sgm = t / 6, dof = t % 6;
+        double acc = 0.0;
+        for (int i = start[sgm]; i < start[sgm + 1]; ++i) {
+            const int v = gval[i];
+            acc += pgrad[12 * (size_t)(v >> 1) + 6 * (v & 1) + dof];
+        }
+        grad[6 * gkey[start[sgm]] + dof] = acc;
+    }
+}
+
+// Hessian blocks: thread per (segment, entry); block (r, c) of pair p is
+// sum_k (lam_k z_k[r-side i]) z_k[c-side j], summed over the segment's pairs
+// in pair order.  Writes BSR col_idx / vals in sorted (row, col) order.
+__global__ void k_ipc_hess(const unsigned long long* hkey, const int* hval, const int* start, const int* nseg, int N,
+                           const double* lam, const double* z, const int* nterm, int* col_idx, double* vals, long long cap) {
+    const int ns = *nseg;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 36 * ns; t += gridDim.x * blockDim.x) {
+        const int sgm = t / 36, e = t % 36, i = e / 6, j = e % 6;
+        if (sgm >= cap) continue;
+        double acc = 0.0;
+        for (int s = start[sgm]; s < start[sgm + 1]; ++s) {
+            const int v = hval[s];
+            const int p = v >> 2, r = (v >> 1) & 1, c = v & 1;
+            double blk = 0.0;
+            for (int k = 0; k < nterm[p]; ++k) {
+                const double* zk = z + 60 * (size_t)p + 12 * k;
+                blk += (lam[5 * (size_t)p + k] * zk[6 * r + i]) * zk[6 * c + j];
+            }
+            acc += blk;
+        }
+        vals[36 * (size_t)sgm + e] = acc;
+        if (e == 0) col_idx[sgm] = (int)(hkey[start[sgm]] % (unsigned long long)N);
+    }
+}
+
+__global__ void k_ipc_rowptr(const unsigned long long* hkey, const int* start, const int* nseg, int N, int* row_ptr) {
+    const int ns = *nseg;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r <= N; r += gridDim.x * blockDim.x) {
+        // first segment whose row >= r (binary search over sorted segment keys)
+        int lo = 0, hi = ns;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((long long)(hkey[start[mid]] / (unsigned long long)N) < r) lo = mid + 1;
+            else hi = mid;
+        }
+        row_ptr[r] = lo;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Additive CCD over the candidate pairs (swept boxes): per pair the time of
+// impact along the chords of its points, then the minimum (one block).
+// ---------------------------------------------------------------------------
+__global__ void k_ipc_accd(PrimGeo pg, IpcPairs P, const double* wq0, const double* wq1, double eta, int max_iter, double* toi) {
+    const int n = P.n_pt + P.n_ee;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        int vid[4], kind;
+        if (p < P.n_pt) {
+            kind = ipc::kPairPT;
+            const int v = P.pt[2 * p], f = P.pt[2 * p + 1];
+            vid[0] = v; vid[1] = pg.fvert[3 * f]; vid[2] = pg.fvert[3 * f + 1]; vid[3] = pg.fvert[3 * f + 2];
+        } else {
+            kind = ipc::kPairEE;
+            const int q = p - P.n_pt;
+            const int e0 = P.ee[2 * q], e1 = P.ee[2 * q + 1];
+            vid[0] = pg.evert[2 * e0]; vid[1] = pg.evert[2 * e0 + 1]; vid[2] = pg.evert[2 * e1]; vid[3] = pg.evert[2 * e1 + 1];
+        }
+        V3 X[4], D[4];
+        for (int k = 0; k < 4; ++k) {
+            X[k] = ld3(wq0 + 3 * vid[k]);
+            D[k] = ld3(wq1 + 3 * vid[k]) - X[k];
+        }
+        toi[p] = ipc::accd_toi(kind, X, D, 1.0, eta, 1000, nullptr);
+    }
+}
+
+__global__ void k_min_reduce(const double* v, int n, double init, double* out) {
+    __shared__ double sm[32];
+    double m = init;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = dmin(m, v[i]);
+    for (int o = 16; o > 0; o >>= 1) m = dmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = init;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r = dmin(r, sm[k]);
+        *out = r;
+    }
+}
+
+// Fixed-tree sum of n doubles (the padded pairwise tree), one block.
+__global__ void __launch_bounds__(1024) k_tree_sum(const double* v, int n, double* out) {
+    __shared__ double sh[2 * kRedMaxQ * 32];
+    BlockRed R;
+    R.sh = sh;
+    R.parity = 0;
+    const double s = R.sum(n, [&](int e) { return v[e]; });
+    if (threadIdx.x == 0) *out = s;
+}
+
+}  // namespace nx

@@ -1,0 +1,384 @@
+// ipc_pair.h — per-pair arithmetic of the primitive-level contact model
+// (full IPC, "Mode I"): distance-type classification, squared distance with
+// its gradient and Hessian, the log barrier on squared distance, the PSD
+// projection of the pair Hessian, the chain to rigid-body DOFs, and additive
+// CCD.  Shared by the sm_100a kernels and the CPU oracle (compiled without
+// FMA contraction on both sides).  The reference has no such model; the
+// formulas follow the published methods:
+//   Li et al. 2020, "Incremental Potential Contact" (barrier on squared
+//     distance, distance types, PSD-projected Hessians);
+//   Ericson 2005, "Real-Time Collision Detection" 5.1.9 (clamped closest
+//     points of two segments), 5.1.5 (closest point on a triangle by regions);
+//   Li et al. 2021, "Codimensional Incremental Potential Contact" (additive
+//     CCD: conservative advancement with a Lipschitz bound on the distance).
+//
+// Every pair has four points X[0..3]: point-triangle (p, t0, t1, t2),
+// edge-edge (a0, a1, b0, b1).  A classified pair is a DistForm: the squared
+// distance is |r|^2 with r = sum_k w_k X_k, the weights affine in nu <= 2
+// parameters u whose optimum the type fixes (c[k][j] = dw_k / du_j).  With
+// g(x, u) = |r|^2 and f(x) = min_u g:
+//   grad_k f = 2 w_k r,
+//   hess f   = g_xx - g_xu g_uu^-1 g_ux,  g_xx = 2 (w w^T) (x) I3,
+//   g_uu = 2 A^T A (A = [a_j], a_j = sum_k c_kj X_k),
+//   g_{x_k u_j} = 2 (w_k a_j + c_kj r).
+// The Hessian's range lies in span{w (x) e_1..3, c_1 (x) r, c_2 (x) r}, so
+// the barrier Hessian b'' grad grad^T + b' hess is projected to PSD exactly
+// by an eigen-decomposition in that <= 5-dimensional basis.
+#pragma once
+
+#include "nx_math.cuh"
+
+namespace nx {
+namespace ipc {
+
+enum { kPairPT = 0, kPairEE = 1 };
+
+// Type codes.  PT: 0..2 point-vertex (t0, t1, t2), 3..5 point-edge (t0t1,
+// t1t2, t2t0), 6 point-interior.  EE: 0..3 vertex-vertex (a0b0, a0b1, a1b0,
+// a1b1), 4..5 a-edge vs b0 / b1, 6..7 b-edge vs a0 / a1, 8 interior.
+struct DistForm {
+    double w[4];
+    double c[4][2];
+    int nu;
+    int type;
+};
+
+struct V12 { V3 v[4]; };
+
+NX_HD DistForm form_zero() {
+    DistForm f;
+    for (int k = 0; k < 4; ++k) { f.w[k] = 0.0; f.c[k][0] = 0.0; f.c[k][1] = 0.0; }
+    f.nu = 0; f.type = 0;
+    return f;
+}
+NX_HD double clamp01(double v) { return v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v); }
+
+// Point p = X[0] against the segment X[i] X[j]: clamped parameter and d^2.
+NX_HD double point_segment(const V3* X, int i, int j, double& t) {
+    const V3 e = X[j] - X[i];
+    const double ee = dot(e, e);
+    t = ee > 0.0 ? clamp01(dot(X[0] - X[i], e) / ee) : 0.0;
+    const V3 r = X[0] - X[i] - t * e;
+    return dot(r, r);
+}
+
+// Point-triangle classification (p, t0, t1, t2).
+NX_HD DistForm classify_pt(const V3* X) {
+    DistForm f = form_zero();
+    const V3 e1 = X[2] - X[1], e2 = X[3] - X[1], q = X[0] - X[1];
+    const double a = dot(e1, e1), b = dot(e1, e2), c = dot(e2, e2), d = dot(e1, q), e = dot(e2, q);
+    const double det = a * c - b * b;
+    if (det > 1e-14 * a * c) {
+        const double b1 = (c * d - b * e) / det, b2 = (a * e - b * d) / det;
+        if (b1 >= 0.0 && b2 >= 0.0 && b1 + b2 <= 1.0) {
+            f.w[0] = 1.0; f.w[1] = -(1.0 - b1 - b2); f.w[2] = -b1; f.w[3] = -b2;
+            f.c[1][0] = 1.0; f.c[1][1] = 1.0; f.c[2][0] = -1.0; f.c[3][1] = -1.0;
+            f.nu = 2; f.type = 6;
+            return f;
+        }
+    }
+    // boundary: the nearest of the three edges (first minimum in order)
+    const int ei[3] = {1, 2, 3}, ej[3] = {2, 3, 1};
+    double best = 0.0, bt = 0.0;
+    int be = -1;
+    for (int k = 0; k < 3; ++k) {
+        double t;
+        const double d2 = point_segment(X, ei[k], ej[k], t);
+        if (be < 0 || d2 < best) { best = d2; bt = t; be = k; }
+    }
+    const int i = ei[be], j = ej[be];
+    f.w[0] = 1.0;
+    if (bt > 0.0 && bt < 1.0) {
+        f.w[i] = -(1.0 - bt); f.w[j] = -bt;
+        f.c[i][0] = 1.0; f.c[j][0] = -1.0;
+        f.nu = 1; f.type = 3 + be;
+    } else {
+        const int v = bt <= 0.0 ? i : j;
+        f.w[v] = -1.0;
+        f.nu = 0; f.type = v - 1;
+    }
+    return f;
+}
+
+// Edge-edge classification (a0, a1, b0, b1), clamped closest points.
+// Nearly parallel edges (A E - B^2 <= 1e-10 A E) take s = 0, so they never
+// classify as interior.
+NX_HD DistForm classify_ee(const V3* X) {
+    DistForm f = form_zero();
+    const V3 d1 = X[1] - X[0], d2 = X[3] - X[2], r = X[0] - X[2];
+    const double A = dot(d1, d1), E = dot(d2, d2), F = dot(d2, r);
+    double s = 0.0, t = 0.0;
+    if (A <= 1e-30 && E <= 1e-30) {
+        s = 0.0; t = 0.0;
+    } else if (A <= 1e-30) {
+        s = 0.0; t = clamp01(F / E);
+    } else {
+        const double C = dot(d1, r);
+        if (E <= 1e-30) {
+            t = 0.0; s = clamp01(-C / A);
+        } else {
+            const double B = dot(d1, d2);
+            const double den = A * E - B * B;
+            s = den > 1e-10 * A * E ? clamp01((B * F - C * E) / den) : 0.0;
+            t = (B * s + F) / E;
+            if (t < 0.0) { t = 0.0; s = clamp01(-C / A); }
+            else if (t > 1.0) { t = 1.0; s = clamp01((B - C) / A); }
+        }
+    }
+    const bool si = s > 0.0 && s < 1.0, ti = t > 0.0 && t < 1.0;
+    if (si && ti) {
+        f.w[0] = 1.0 - s; f.w[1] = s; f.w[2] = -(1.0 - t); f.w[3] = -t;
+        f.c[0][0] = -1.0; f.c[1][0] = 1.0; f.c[2][1] = 1.0; f.c[3][1] = -1.0;
+        f.nu = 2; f.type = 8;
+    } else if (si) {
+        const int pb = t <= 0.0 ? 2 : 3;
+        f.w[0] = 1.0 - s; f.w[1] = s; f.w[pb] = -1.0;
+        f.c[0][0] = -1.0; f.c[1][0] = 1.0;
+        f.nu = 1; f.type = 4 + (pb - 2);
+    } else if (ti) {
+        const int pa = s <= 0.0 ? 0 : 1;
+        f.w[pa] = 1.0; f.w[2] = -(1.0 - t); f.w[3] = -t;
+        f.c[2][0] = 1.0; f.c[3][0] = -1.0;
+        f.nu = 1; f.type = 6 + pa;
+    } else {
+        const int pa = s <= 0.0 ? 0 : 1, pb = t <= 0.0 ? 2 : 3;
+        f.w[pa] = 1.0; f.w[pb] = -1.0;
+        f.nu = 0; f.type = 2 * pa + (pb - 2);
+    }
+    return f;
+}
+
+NX_HD DistForm classify(int kind, const V3* X) { return kind == kPairPT ? classify_pt(X) : classify_ee(X); }
+
+NX_HD V3 form_r(const DistForm& f, const V3* X) {
+    return f.w[0] * X[0] + f.w[1] * X[1] + f.w[2] * X[2] + f.w[3] * X[3];
+}
+NX_HD double dist2(int kind, const V3* X) {
+    const DistForm f = classify(kind, X);
+    const V3 r = form_r(f, X);
+    return dot(r, r);
+}
+
+// Log barrier on squared distance s with support s < sh = dhat^2:
+// b(s) = -kappa (s - sh)^2 ln(s / sh), and its first two derivatives in s.
+NX_HD double barrier_s(double s, double sh, double kappa) {
+    if (!(s < sh)) return 0.0;
+    if (!(s > 0.0)) return INFINITY;
+    const double q = s - sh;
+    return -kappa * q * q * nxm::log(s / sh);
+}
+NX_HD double barrier_s1(double s, double sh, double kappa) {
+    if (!(s < sh) || !(s > 0.0)) return 0.0;
+    const double q = s - sh;
+    return -kappa * (2.0 * q * nxm::log(s / sh) + q * q / s);
+}
+NX_HD double barrier_s2(double s, double sh, double kappa) {
+    if (!(s < sh) || !(s > 0.0)) return 0.0;
+    const double q = s - sh;
+    return -kappa * (2.0 * nxm::log(s / sh) + 4.0 * q / s - (q * q) / (s * s));
+}
+
+// Cyclic Jacobi eigen-decomposition of a symmetric m x m matrix (m <= 5),
+// in place: on return A holds the eigenvalues on its diagonal and V the
+// eigenvectors (columns).  At most 16 sweeps.
+template <int M>
+NX_HD void jacobi_eigen(double (&A)[M][M], double (&V)[M][M], int m) {
+    for (int i = 0; i < M; ++i)
+        for (int j = 0; j < M; ++j) V[i][j] = i == j ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 16; ++sweep) {
+        double off = 0.0, tot = 0.0;
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) {
+                tot += A[i][j] * A[i][j];
+                if (i != j) off += A[i][j] * A[i][j];
+            }
+        if (!(off > 1e-30 * tot)) break;
+        for (int p = 0; p < m - 1; ++p)
+            for (int q = p + 1; q < m; ++q) {
+                const double apq = A[p][q];
+                if (apq == 0.0) continue;
+                const double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
+                const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                for (int k = 0; k < m; ++k) {
+                    const double akp = A[k][p], akq = A[k][q];
+                    A[k][p] = c * akp - s * akq;
+                    A[k][q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < m; ++k) {
+                    const double apk = A[p][k], aqk = A[q][k];
+                    A[p][k] = c * apk - s * aqk;
+                    A[q][k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < m; ++k) {
+                    const double vkp = V[k][p], vkq = V[k][q];
+                    V[k][p] = c * vkp - s * vkq;
+                    V[k][q] = s * vkp + c * vkq;
+                }
+            }
+    }
+}
+
+// 12-vectors as four V3 blocks.
+NX_HD double dot12(const V12& a, const V12& b) {
+    return (dot(a.v[0], b.v[0]) + dot(a.v[1], b.v[1])) + (dot(a.v[2], b.v[2]) + dot(a.v[3], b.v[3]));
+}
+NX_HD void axpy12(double s, const V12& x, V12& y) {
+    for (int k = 0; k < 4; ++k) y.v[k] = y.v[k] + s * x.v[k];
+}
+NX_HD V12 scale12(double s, const V12& x) {
+    V12 y;
+    for (int k = 0; k < 4; ++k) y.v[k] = s * x.v[k];
+    return y;
+}
+NX_HD V12 outer_wv(const double* w, V3 v) {   // w (x) v
+    V12 y;
+    for (int k = 0; k < 4; ++k) y.v[k] = w[k] * v;
+    return y;
+}
+
+// Barrier of one classified pair.  Outputs: e = b(d^2); grad (12) =
+// b' grad d^2; the PSD part of the Hessian as sum_k lam[k] y_k y_k^T with
+// at most 5 terms (n_terms).  Returns d^2.
+struct PairEval {
+    double d2, e;
+    V12 grad;
+    int n_terms;
+    double lam[5];
+    V12 y[5];
+};
+
+NX_HD PairEval pair_barrier(const DistForm& f, const V3* X, double dhat, double kappa) {
+    PairEval o;
+    const V3 r = form_r(f, X);
+    const double s = dot(r, r), sh = dhat * dhat;
+    o.d2 = s;
+    o.e = barrier_s(s, sh, kappa);
+    o.n_terms = 0;
+    for (int k = 0; k < 4; ++k) o.grad.v[k] = v3(0, 0, 0);
+    if (!(s < sh) || !(s > 0.0)) return o;
+    const double b1 = barrier_s1(s, sh, kappa), b2 = barrier_s2(s, sh, kappa);
+    const V12 gs = outer_wv(f.w, 2.0 * r);          // grad d^2
+    o.grad = scale12(b1, gs);
+    // a_j, g_uu = 2 A^T A, its inverse
+    V3 a[2] = {v3(0, 0, 0), v3(0, 0, 0)};
+    for (int j = 0; j < f.nu; ++j)
+        a[j] = f.c[0][j] * X[0] + f.c[1][j] * X[1] + f.c[2][j] * X[2] + f.c[3][j] * X[3];
+    double Minv[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    if (f.nu == 1) {
+        Minv[0][0] = 1.0 / (2.0 * dot(a[0], a[0]));
+    } else if (f.nu == 2) {
+        const double m00 = 2.0 * dot(a[0], a[0]), m01 = 2.0 * dot(a[0], a[1]), m11 = 2.0 * dot(a[1], a[1]);
+        const double det = m00 * m11 - m01 * m01;
+        Minv[0][0] = m11 / det; Minv[0][1] = -m01 / det; Minv[1][0] = -m01 / det; Minv[1][1] = m00 / det;
+    }
+    // G_j = 2 (w (x) a_j + c_j (x) r)
+    V12 G[2];
+    for (int j = 0; j < f.nu; ++j) {
+        const double cj[4] = {f.c[0][j], f.c[1][j], f.c[2][j], f.c[3][j]};
+        G[j] = outer_wv(f.w, 2.0 * a[j]);
+        axpy12(1.0, outer_wv(cj, 2.0 * r), G[j]);
+    }
+    // orthonormal basis: w (x) e_a / |w| (a = x, y, z), then the c_j (x) r
+    // directions orthogonalised against it (twice, modified Gram-Schmidt)
+    const double wn = sqrt((f.w[0] * f.w[0] + f.w[1] * f.w[1]) + (f.w[2] * f.w[2] + f.w[3] * f.w[3]));
+    V12 B[5];
+    int m = 0;
+    const V3 ex = v3(1, 0, 0), ey = v3(0, 1, 0), ez = v3(0, 0, 1);
+    B[m++] = outer_wv(f.w, (1.0 / wn) * ex);
+    B[m++] = outer_wv(f.w, (1.0 / wn) * ey);
+    B[m++] = outer_wv(f.w, (1.0 / wn) * ez);
+    for (int j = 0; j < f.nu; ++j) {
+        const double cj[4] = {f.c[0][j], f.c[1][j], f.c[2][j], f.c[3][j]};
+        V12 v = outer_wv(cj, r);
+        const double n0 = sqrt(dot12(v, v));
+        for (int pass = 0; pass < 2; ++pass)
+            for (int k = 0; k < m; ++k) axpy12(-dot12(B[k], v), B[k], v);
+        const double n1 = sqrt(dot12(v, v));
+        if (n1 > 1e-9 * n0 && n1 > 0.0) B[m++] = scale12(1.0 / n1, v);
+    }
+    // coordinates of grad d^2 and G_j in the basis; the basis image of
+    // 2 (w w^T) (x) I3 is 2 |w|^2 on the first three coordinates
+    double gam[5], Gam[2][5];
+    for (int k = 0; k < m; ++k) {
+        gam[k] = dot12(B[k], gs);
+        for (int j = 0; j < f.nu; ++j) Gam[j][k] = dot12(B[k], G[j]);
+    }
+    double S[5][5], V[5][5];
+    for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 5; ++j) S[i][j] = 0.0;
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) {
+            double hs = (i == j && i < 3) ? 2.0 * wn * wn : 0.0;
+            for (int p = 0; p < f.nu; ++p)
+                for (int q = 0; q < f.nu; ++q) hs -= Gam[p][i] * Minv[p][q] * Gam[q][j];
+            S[i][j] = b2 * gam[i] * gam[j] + b1 * hs;
+        }
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < i; ++j) {   // exact symmetry before the rotations
+            const double avg = 0.5 * (S[i][j] + S[j][i]);
+            S[i][j] = avg; S[j][i] = avg;
+        }
+    jacobi_eigen<5>(S, V, m);
+    int n = 0;
+    for (int k = 0; k < m; ++k) {
+        const double lam = S[k][k];
+        if (!(lam > 0.0)) continue;
+        V12 y = scale12(V[0][k], B[0]);
+        for (int i = 1; i < m; ++i) axpy12(V[i][k], B[i], y);
+        o.lam[n] = lam;
+        o.y[n] = y;
+        ++n;
+    }
+    o.n_terms = n;
+    return o;
+}
+
+// Rigid chain: point k of the pair belongs to body side[k] (0 = body A,
+// 1 = body B) at lever arm arm[k] = R r_k (world offset from the body's
+// position); its DOF Jacobian is [I3, -[arm]x].  The transposed Jacobian
+// maps a 12-vector of point forces to 12 body DOFs (A: 0..5, B: 6..11).
+NX_HD void chain12(const V12& z, const int* side, const V3* arm, double* out12) {
+    for (int i = 0; i < 12; ++i) out12[i] = 0.0;
+    for (int k = 0; k < 4; ++k) {
+        double* o = out12 + 6 * side[k];
+        const V3 t = cross(arm[k], z.v[k]);
+        o[0] += z.v[k].x; o[1] += z.v[k].y; o[2] += z.v[k].z;
+        o[3] += t.x; o[4] += t.y; o[5] += t.z;
+    }
+}
+
+// Additive CCD along linear point trajectories X + t P, t in [0, t_max]:
+// the relative motion of the pair (common translation removed) changes the
+// distance by at most lp per unit t, so from distance d at t the step
+// 0.9 (d - g) / lp keeps the distance above g = eta d(0).  Returns the
+// largest t reached (t_max when no approach below g happens); at most
+// max_iter advancements.  Every returned t keeps the distance >= g on [0, t].
+NX_HD double accd_toi(int kind, const V3* X0, const V3* P0, double t_max, double eta, int max_iter, int* iters) {
+    V3 P[4];
+    const V3 mean = 0.25 * ((P0[0] + P0[1]) + (P0[2] + P0[3]));
+    for (int k = 0; k < 4; ++k) P[k] = P0[k] - mean;
+    double lp;
+    if (kind == kPairPT) lp = norm(P[0]) + dmax(norm(P[1]), dmax(norm(P[2]), norm(P[3])));
+    else lp = dmax(norm(P[0]), norm(P[1])) + dmax(norm(P[2]), norm(P[3]));
+    if (iters) *iters = 0;
+    const double d0 = sqrt(dist2(kind, X0));
+    if (!(lp > 0.0)) return t_max;
+    if (!(d0 > 0.0)) return 0.0;
+    const double g = eta * d0;
+    double t = 0.0, d = d0;
+    for (int it = 0; it < max_iter; ++it) {
+        if (iters) *iters = it + 1;
+        const double tl = 0.9 * (d - g) / lp;
+        if (t + tl >= t_max) return t_max;
+        if (!(tl > 1e-12 * t_max)) return t;
+        t += tl;
+        V3 X[4];
+        for (int k = 0; k < 4; ++k) X[k] = X0[k] + t * P0[k];
+        d = sqrt(dist2(kind, X));
+    }
+    return t;
+}
+
+}  // namespace ipc
+}  // namespace nx

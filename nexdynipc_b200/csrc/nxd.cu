@@ -13,6 +13,7 @@
 #include "../../include/nxd.h"
 #include "step.cuh"
 #include "batch.cuh"
+#include "ipc.cuh"
 
 using namespace nx;
 
@@ -108,6 +109,8 @@ struct nxd_ctx {
     int cand_stride = 0;
     // when set, launches are recorded here (batched replay) instead of issued
     std::vector<LaunchRec>* rec = nullptr;
+    // primitive-level (full IPC) model state, created on first use
+    struct IpcState* ipc = nullptr;
     // nxd_step as a CUDA graph, captured per dt on a private stream
     cudaStream_t cap_stream = nullptr;
     cudaGraph_t graph = nullptr;
@@ -373,6 +376,7 @@ nxd_status enqueue_step(nxd_ctx* c, double dt) {
 // ===========================================================================
 namespace {
 void drop_step_graph(nxd_ctx* c);
+void release_ipc(nxd_ctx* c);
 }  // namespace
 
 extern "C" {
@@ -581,6 +585,7 @@ void nxd_destroy(nxd_ctx* c) {
         for (auto& pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
     for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
     drop_step_graph(c);
+    release_ipc(c);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     c->mem.release();
     delete c;
@@ -915,6 +920,355 @@ nxd_status nxd_normal_forces(nxd_ctx* c, const double* x, double* out, int32_t n
     cudaStreamSynchronize(st);
     cudaMemcpy(out, od, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost);
     tmp.release();
+    return NXD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Primitive-level contact model (full IPC): LBVH candidates, barrier form
+// (energy, gradient, PSD BSR Hessian), additive-CCD step bound.  Buffers are
+// created on first use and grown to the counts a call needs; these calls
+// synchronise and return host results.
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+struct GrowBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    bool ensure(size_t bytes) {
+        bytes = std::max<size_t>(bytes, 256);
+        if (bytes <= cap) return true;
+        if (p) {
+            cudaDeviceSynchronize();   // queued kernels may still read the old buffer
+            cudaFree(p);
+        }
+        p = nullptr;
+        cap = 0;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) { p = nullptr; return false; }
+        cap = bytes;
+        return true;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+    void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+};
+
+struct Bvh {
+    int n = 0;
+    GrowBuf k0, k1, i0, i1, leaf, nbox, child, parent, flags, bounds;
+};
+
+}  // namespace
+
+struct IpcState {
+    PrimGeo pg{};
+    GrowBuf fbody, fvert, ebody, evert;
+    GrowBuf x0, x1, pp0, pq0, pp1, pq1, wq0, wq1, qv, qe;
+    Bvh faces, edges;
+    GrowBuf cnt, off, pt, ee, scal, hist;
+    int n_pt = 0, n_ee = 0;
+    GrowBuf e, grad12, lam, z, nterm, body, active, type, apos, alist;
+    GrowBuf gkey, gval, gkey1, gval1, hkey, hval, hkey1, hval1;
+    GrowBuf sflag, spos, sstart, gout, rowptr, colidx, vals, toi;
+    std::vector<GrowBuf*> all() {
+        return {&fbody, &fvert, &ebody, &evert, &x0, &x1, &pp0, &pq0, &pp1, &pq1, &wq0, &wq1, &qv, &qe,
+                &faces.k0, &faces.k1, &faces.i0, &faces.i1, &faces.leaf, &faces.nbox, &faces.child, &faces.parent,
+                &faces.flags, &faces.bounds, &edges.k0, &edges.k1, &edges.i0, &edges.i1, &edges.leaf, &edges.nbox,
+                &edges.child, &edges.parent, &edges.flags, &edges.bounds, &cnt, &off, &pt, &ee, &scal, &hist, &e,
+                &grad12, &lam, &z, &nterm, &body, &active, &type, &apos, &alist, &gkey, &gval, &gkey1, &gval1, &hkey,
+                &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi};
+    }
+    void release() { for (GrowBuf* b : all()) b->release(); }
+};
+
+namespace {
+
+#define IPC_ENSURE(buf, bytes) do { if (!(buf).ensure(bytes)) return NXD_CUDA_ERROR; } while (0)
+
+void release_ipc(nxd_ctx* c) {
+    if (!c->ipc) return;
+    c->ipc->release();
+    delete c->ipc;
+    c->ipc = nullptr;
+}
+
+nxd_status ipc_prepare(nxd_ctx* c) {
+    if (c->ipc) return NXD_OK;
+    IpcState* s = new (std::nothrow) IpcState();
+    if (!s) return NXD_CUDA_ERROR;
+    c->ipc = s;
+    IPC_ENSURE(s->fbody, 4 * (size_t)c->nf); IPC_ENSURE(s->fvert, 12 * (size_t)c->nf);
+    IPC_ENSURE(s->ebody, 4 * (size_t)c->ne); IPC_ENSURE(s->evert, 8 * (size_t)c->ne);
+    k_prim_topology<<<grid_for(c->N, 128), 128, 0, c->stream>>>(c->geo, s->fbody.as<int>(), s->fvert.as<int>(),
+                                                              s->ebody.as<int>(), s->evert.as<int>());
+    s->pg = PrimGeo{c->nv, c->nf, c->ne, c->vbody, s->fbody.as<int>(), s->ebody.as<int>(), s->fvert.as<int>(),
+                    s->evert.as<int>()};
+    IPC_ENSURE(s->scal, 64);
+    NXD_CUDA(cudaGetLastError());
+    return NXD_OK;
+}
+
+// World vertices at x (host 6N; NULL = the current poses) into wq0, and at
+// x + dx into wq1 when dx is given.
+nxd_status ipc_pose(nxd_ctx* c, const double* x, const double* dx) {
+    IpcState* s = c->ipc;
+    const int N = c->N;
+    IPC_ENSURE(s->pp0, 24 * (size_t)N); IPC_ENSURE(s->pq0, 32 * (size_t)N); IPC_ENSURE(s->wq0, 24 * (size_t)c->nv);
+    IPC_ENSURE(s->x0, 48 * (size_t)N);
+    if (x) {
+        NXD_CUDA(cudaMemcpyAsync(s->x0.p, x, 48 * (size_t)N, cudaMemcpyHostToDevice, c->stream));
+        k_pose_at_x<<<grid_for(N, 128), 128, 0, c->stream>>>(N, s->x0.as<double>(), c->quat, s->pp0.as<double>(), s->pq0.as<double>());
+    } else {
+        NXD_CUDA(cudaMemcpyAsync(s->pp0.p, c->pos, 24 * (size_t)N, cudaMemcpyDeviceToDevice, c->stream));
+        NXD_CUDA(cudaMemcpyAsync(s->pq0.p, c->quat, 32 * (size_t)N, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    k_world_vertices<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(c->geo, c->nv, c->vbody, s->pp0.as<double>(), s->pq0.as<double>(),
+                                                                  s->wq0.as<double>());
+    if (dx) {
+        IPC_ENSURE(s->x1, 48 * (size_t)N); IPC_ENSURE(s->pp1, 24 * (size_t)N); IPC_ENSURE(s->pq1, 32 * (size_t)N);
+        IPC_ENSURE(s->wq1, 24 * (size_t)c->nv);
+        NXD_CUDA(cudaMemcpyAsync(s->x1.p, dx, 48 * (size_t)N, cudaMemcpyHostToDevice, c->stream));
+        k_axpy_vec<<<grid_for(6 * N, 256), 256, 0, c->stream>>>(s->x0.as<double>(), s->x1.as<double>(), 6 * N, s->x1.as<double>());
+        k_pose_at_x<<<grid_for(N, 128), 128, 0, c->stream>>>(N, s->x1.as<double>(), c->quat, s->pp1.as<double>(), s->pq1.as<double>());
+        k_world_vertices<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(c->geo, c->nv, c->vbody, s->pp1.as<double>(),
+                                                                      s->pq1.as<double>(), s->wq1.as<double>());
+    }
+    NXD_CUDA(cudaGetLastError());
+    return NXD_OK;
+}
+
+// Stable LSD radix sort of n (key, value) pairs on key bits [lo, hi); the
+// result ends in (k0, v0).
+nxd_status radix_sort(nxd_ctx* c, GrowBuf& k0, GrowBuf& v0, GrowBuf& k1, GrowBuf& v1, int n, int lo, int hi) {
+    if (n <= 1) return NXD_OK;
+    IpcState* s = c->ipc;
+    IPC_ENSURE(k1, 8 * (size_t)n); IPC_ENSURE(v1, 4 * (size_t)n);
+    const int nblocks = (n + kRsTile - 1) / kRsTile;
+    IPC_ENSURE(s->hist, 4 * 256 * (size_t)nblocks);
+    for (int shift = lo; shift < hi; shift += 8) {
+        k_rs_hist<<<nblocks, kRsThreads, 0, c->stream>>>(k0.as<unsigned long long>(), n, shift, s->hist.as<int>(), nblocks);
+        k_rs_scan<<<1, 1024, 0, c->stream>>>(s->hist.as<int>(), 256 * nblocks);
+        k_rs_scatter<<<nblocks, kRsThreads, 0, c->stream>>>(k0.as<unsigned long long>(), v0.as<int>(), k1.as<unsigned long long>(),
+                                                            v1.as<int>(), n, shift, s->hist.as<int>(), nblocks);
+        std::swap(k0, k1);
+        std::swap(v0, v1);
+    }
+    NXD_CUDA(cudaGetLastError());
+    return NXD_OK;
+}
+
+int bits_for(unsigned long long maxkey) {
+    int b = 0;
+    while (b < 64 && (maxkey >> b) != 0ull) ++b;
+    return (b + 7) / 8 * 8;
+}
+
+// LBVH over the face (kind 0) or edge (kind 1) boxes: Morton keys, stable
+// radix sort, Karras hierarchy, bottom-up boxes.
+nxd_status ipc_build_bvh(nxd_ctx* c, Bvh& B, int kind, bool swept, double infl) {
+    IpcState* s = c->ipc;
+    const int n = kind == 0 ? c->nf : c->ne;
+    B.n = n;
+    IPC_ENSURE(B.leaf, 48 * (size_t)n);
+    if (n == 0) return NXD_OK;
+    const double* w1 = swept ? s->wq1.as<double>() : nullptr;
+    k_ipc_boxes<<<grid_for(n, 256), 256, 0, c->stream>>>(s->pg, kind, s->wq0.as<double>(), w1, infl, B.leaf.as<double>());
+    IPC_ENSURE(B.bounds, 48);
+    k_centroid_bounds<<<1, 1024, 0, c->stream>>>(B.leaf.as<double>(), n, B.bounds.as<double>());
+    IPC_ENSURE(B.k0, 8 * (size_t)n); IPC_ENSURE(B.i0, 4 * (size_t)n);
+    k_morton<<<grid_for(n, 256), 256, 0, c->stream>>>(B.leaf.as<double>(), n, B.bounds.as<double>(), B.k0.as<unsigned long long>(),
+                                                      B.i0.as<int>());
+    nxd_status st = radix_sort(c, B.k0, B.i0, B.k1, B.i1, n, 32, 64);
+    if (st != NXD_OK) return st;
+    IPC_ENSURE(B.nbox, 48 * (size_t)(2 * n - 1)); IPC_ENSURE(B.child, 8 * (size_t)n);
+    IPC_ENSURE(B.parent, 4 * (size_t)(2 * n)); IPC_ENSURE(B.flags, 4 * (size_t)n);
+    NXD_CUDA(cudaMemsetAsync(B.flags.p, 0, 4 * (size_t)n, c->stream));
+    k_karras<<<grid_for(std::max(n - 1, 1), 128), 128, 0, c->stream>>>(B.k0.as<unsigned long long>(), n, B.child.as<int>(),
+                                                                        B.parent.as<int>());
+    k_refit<<<grid_for(n, 128), 128, 0, c->stream>>>(B.leaf.as<double>(), B.i0.as<int>(), n, B.child.as<int>(), B.parent.as<int>(),
+                                                     B.nbox.as<double>(), B.flags.as<int>());
+    NXD_CUDA(cudaGetLastError());
+    return NXD_OK;
+}
+
+// Queries against a tree: counts, offsets, then the pairs (query-major,
+// prim ascending) into out; *count gets the number of pairs.
+nxd_status ipc_traverse(nxd_ctx* c, int kind, Bvh& B, const double* qbox, int nq, GrowBuf& out, int* count) {
+    IpcState* s = c->ipc;
+    *count = 0;
+    if (nq == 0 || B.n == 0) return NXD_OK;
+    IPC_ENSURE(s->cnt, 4 * (size_t)nq); IPC_ENSURE(s->off, 4 * (size_t)nq);
+    int* d_tot = s->scal.as<int>();
+    int* d_status = d_tot + 1;
+    NXD_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), c->stream));
+    const int grid = grid_for(nq, 128);
+    k_traverse<<<grid, 128, 0, c->stream>>>(s->pg, kind, qbox, nq, B.nbox.as<double>(), B.child.as<int>(), B.i0.as<int>(), B.n,
+                                            s->cnt.as<int>(), nullptr, nullptr, d_status);
+    k_scan<<<1, 1024, 0, c->stream>>>(s->cnt.as<int>(), s->off.as<int>(), nq, d_tot, nullptr, nullptr, nullptr);
+    int h[2];
+    NXD_CUDA(cudaMemcpyAsync(h, d_tot, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    if (h[1] != 0) return (nxd_status)h[1];
+    *count = h[0];
+    IPC_ENSURE(out, 8 * (size_t)std::max(h[0], 1));
+    k_traverse<<<grid, 128, 0, c->stream>>>(s->pg, kind, qbox, nq, B.nbox.as<double>(), B.child.as<int>(), B.i0.as<int>(), B.n,
+                                            nullptr, s->off.as<int>(), out.as<int>(), d_status);
+    NXD_CUDA(cudaGetLastError());
+    return NXD_OK;
+}
+
+// Candidate point-triangle and edge-edge pairs at the posed world vertices:
+// leaf boxes inflated by infl (swept over wq0 -> wq1 when swept).
+nxd_status ipc_candidates(nxd_ctx* c, bool swept, double infl) {
+    IpcState* s = c->ipc;
+    nxd_status st = ipc_build_bvh(c, s->faces, 0, swept, infl);
+    if (st == NXD_OK) st = ipc_build_bvh(c, s->edges, 1, swept, infl);
+    if (st != NXD_OK) return st;
+    IPC_ENSURE(s->qv, 48 * (size_t)c->nv); IPC_ENSURE(s->qe, 48 * (size_t)c->ne);
+    const double* w1 = swept ? s->wq1.as<double>() : nullptr;
+    if (c->nv) k_ipc_boxes<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(s->pg, 2, s->wq0.as<double>(), w1, 0.0, s->qv.as<double>());
+    if (c->ne) k_ipc_boxes<<<grid_for(c->ne, 256), 256, 0, c->stream>>>(s->pg, 3, s->wq0.as<double>(), w1, 0.0, s->qe.as<double>());
+    st = ipc_traverse(c, 0, s->faces, s->qv.as<double>(), c->nv, s->pt, &s->n_pt);
+    if (st == NXD_OK) st = ipc_traverse(c, 1, s->edges, s->qe.as<double>(), c->ne, s->ee, &s->n_ee);
+    return st;
+}
+
+// Sorted segments of keys[0..m): starts in s->sstart (m_seg + 1 entries).
+nxd_status ipc_segments(nxd_ctx* c, const unsigned long long* keys, int m, int* nseg_host) {
+    IpcState* s = c->ipc;
+    IPC_ENSURE(s->sflag, 4 * (size_t)m); IPC_ENSURE(s->spos, 4 * (size_t)m); IPC_ENSURE(s->sstart, 4 * (size_t)(m + 1));
+    int* d_n = s->scal.as<int>() + 2;
+    k_seg_flags<<<grid_for(m, 256), 256, 0, c->stream>>>(keys, m, s->sflag.as<int>());
+    k_scan<<<1, 1024, 0, c->stream>>>(s->sflag.as<int>(), s->spos.as<int>(), m, d_n, nullptr, nullptr, nullptr);
+    k_seg_starts<<<grid_for(m, 256), 256, 0, c->stream>>>(s->sflag.as<int>(), s->spos.as<int>(), m, s->sstart.as<int>(), d_n);
+    NXD_CUDA(cudaMemcpyAsync(nseg_host, d_n, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    return NXD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+nxd_status nxd_ipc_candidates(nxd_ctx* c, const double* x, const double* dx, double inflation, int32_t* pt, int64_t pt_cap,
+                              int32_t* ee, int64_t ee_cap, int64_t* n_pt, int64_t* n_ee) {
+    if (!c || !n_pt || !n_ee || !(inflation >= 0.0) || (dx && !x)) return NXD_INVALID_ARGUMENT;
+    nxd_status st = ipc_prepare(c);
+    if (st == NXD_OK) st = ipc_pose(c, x, dx);
+    if (st == NXD_OK) st = ipc_candidates(c, dx != nullptr, inflation);
+    if (st != NXD_OK) return st;
+    IpcState* s = c->ipc;
+    *n_pt = s->n_pt;
+    *n_ee = s->n_ee;
+    if (pt && s->n_pt)
+        NXD_CUDA(cudaMemcpy(pt, s->pt.p, 8 * (size_t)std::min<int64_t>(pt_cap, s->n_pt), cudaMemcpyDeviceToHost));
+    if (ee && s->n_ee)
+        NXD_CUDA(cudaMemcpy(ee, s->ee.p, 8 * (size_t)std::min<int64_t>(ee_cap, s->n_ee), cudaMemcpyDeviceToHost));
+    return (pt && s->n_pt > pt_cap) || (ee && s->n_ee > ee_cap) ? NXD_CAPACITY : NXD_OK;
+}
+
+nxd_status nxd_ipc_barrier(nxd_ctx* c, const double* x, double dhat, double kappa, double* energy, double* grad, int32_t* row_ptr,
+                           int32_t* col_idx, double* vals, int64_t cap_blocks, int64_t* nnzb, int64_t* n_pairs,
+                           int64_t* n_active) {
+    if (!c || !(dhat > 0.0) || !(kappa >= 0.0)) return NXD_INVALID_ARGUMENT;
+    nxd_status st = ipc_prepare(c);
+    if (st == NXD_OK) st = ipc_pose(c, x, nullptr);
+    if (st == NXD_OK) st = ipc_candidates(c, false, dhat);
+    if (st != NXD_OK) return st;
+    IpcState* s = c->ipc;
+    const int N = c->N, n = s->n_pt + s->n_ee;
+    if (n_pairs) *n_pairs = n;
+    const IpcPairs P{s->pt.as<int>(), s->n_pt, s->ee.as<int>(), s->n_ee};
+    const IpcPose ps{s->wq0.as<double>(), s->pp0.as<double>()};
+    const size_t nn = std::max(n, 1);
+    IPC_ENSURE(s->e, 8 * nn); IPC_ENSURE(s->grad12, 96 * nn); IPC_ENSURE(s->lam, 40 * nn); IPC_ENSURE(s->z, 480 * nn);
+    IPC_ENSURE(s->nterm, 4 * nn); IPC_ENSURE(s->body, 8 * nn); IPC_ENSURE(s->active, 4 * nn); IPC_ENSURE(s->type, 4 * nn);
+    IPC_ENSURE(s->apos, 4 * nn); IPC_ENSURE(s->alist, 4 * nn);
+    const IpcEvalOut o{s->e.as<double>(), s->grad12.as<double>(), s->lam.as<double>(), s->z.as<double>(), s->nterm.as<int>(),
+                       s->body.as<int>(), s->active.as<int>(), s->type.as<int>()};
+    double* d_energy = reinterpret_cast<double*>(s->scal.as<char>() + 32);
+    int* d_na = s->scal.as<int>() + 3;
+    if (n) k_ipc_pair_eval<<<grid_for(n, 128), 128, 0, c->stream>>>(s->pg, P, ps, dhat, kappa, o);
+    k_tree_sum<<<1, 1024, 0, c->stream>>>(s->e.as<double>(), n, d_energy);
+    k_scan<<<1, 1024, 0, c->stream>>>(s->active.as<int>(), s->apos.as<int>(), n, d_na, nullptr, nullptr, nullptr);
+    if (n) k_compact<<<grid_for(n, 256), 256, 0, c->stream>>>(s->active.as<int>(), s->apos.as<int>(), n, s->alist.as<int>());
+    int na = 0;
+    double eh = 0.0;
+    NXD_CUDA(cudaMemcpyAsync(&na, d_na, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    NXD_CUDA(cudaMemcpyAsync(&eh, d_energy, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    if (energy) *energy = eh;
+    if (n_active) *n_active = na;
+    // contributions, stable-sorted by body / by (row body, col body)
+    IPC_ENSURE(s->gkey, 16 * (size_t)std::max(na, 1)); IPC_ENSURE(s->gval, 8 * (size_t)std::max(na, 1));
+    IPC_ENSURE(s->hkey, 32 * (size_t)std::max(na, 1)); IPC_ENSURE(s->hval, 16 * (size_t)std::max(na, 1));
+    if (na)
+        k_ipc_contrib<<<grid_for(na, 128), 128, 0, c->stream>>>(s->alist.as<int>(), na, s->body.as<int>(), N,
+                                                                 s->gkey.as<unsigned long long>(), s->gval.as<int>(),
+                                                                 s->hkey.as<unsigned long long>(), s->hval.as<int>());
+    st = radix_sort(c, s->gkey, s->gval, s->gkey1, s->gval1, 2 * na, 0, bits_for((unsigned long long)N));
+    if (st == NXD_OK)
+        st = radix_sort(c, s->hkey, s->hval, s->hkey1, s->hval1, 4 * na, 0, bits_for((unsigned long long)N * (unsigned long long)N));
+    if (st != NXD_OK) return st;
+    IPC_ENSURE(s->gout, 48 * (size_t)N);
+    NXD_CUDA(cudaMemsetAsync(s->gout.p, 0, 48 * (size_t)N, c->stream));
+    IPC_ENSURE(s->sflag, 16 * (size_t)std::max(na, 1)); IPC_ENSURE(s->spos, 16 * (size_t)std::max(na, 1));
+    IPC_ENSURE(s->sstart, 16 * (size_t)std::max(na, 1) + 4);
+    int ng = 0;
+    if (na) {
+        st = ipc_segments(c, s->gkey.as<unsigned long long>(), 2 * na, &ng);
+        if (st != NXD_OK) return st;
+        k_ipc_grad<<<grid_for(6LL * ng, 128), 128, 0, c->stream>>>(s->gkey.as<unsigned long long>(), s->gval.as<int>(),
+                                                                    s->sstart.as<int>(), s->scal.as<int>() + 2,
+                                                                    s->grad12.as<double>(), s->gout.as<double>());
+    }
+    if (grad) {
+        NXD_CUDA(cudaMemcpyAsync(grad, s->gout.p, 48 * (size_t)N, cudaMemcpyDeviceToHost, c->stream));
+        NXD_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    int nh = 0;
+    if (na) {
+        st = ipc_segments(c, s->hkey.as<unsigned long long>(), 4 * na, &nh);
+        if (st != NXD_OK) return st;
+    }
+    if (nnzb) *nnzb = nh;
+    if (nh > cap_blocks && (col_idx || vals)) return NXD_CAPACITY;
+    IPC_ENSURE(s->rowptr, 4 * (size_t)(N + 1)); IPC_ENSURE(s->colidx, 4 * (size_t)std::max(nh, 1));
+    IPC_ENSURE(s->vals, 288 * (size_t)std::max(nh, 1));
+    if (nh)
+        k_ipc_hess<<<grid_for(36LL * nh, 128), 128, 0, c->stream>>>(s->hkey.as<unsigned long long>(), s->hval.as<int>(),
+                                                                     s->sstart.as<int>(), s->scal.as<int>() + 2, N,
+                                                                     s->lam.as<double>(), s->z.as<double>(), s->nterm.as<int>(),
+                                                                     s->colidx.as<int>(), s->vals.as<double>(), nh);
+    if (nh) k_ipc_rowptr<<<grid_for(N + 1, 128), 128, 0, c->stream>>>(s->hkey.as<unsigned long long>(), s->sstart.as<int>(),
+                                                                        s->scal.as<int>() + 2, N, s->rowptr.as<int>());
+    else NXD_CUDA(cudaMemsetAsync(s->rowptr.p, 0, 4 * (size_t)(N + 1), c->stream));
+    if (row_ptr) NXD_CUDA(cudaMemcpyAsync(row_ptr, s->rowptr.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, c->stream));
+    if (col_idx && nh) NXD_CUDA(cudaMemcpyAsync(col_idx, s->colidx.p, 4 * (size_t)nh, cudaMemcpyDeviceToHost, c->stream));
+    if (vals && nh) NXD_CUDA(cudaMemcpyAsync(vals, s->vals.p, 288 * (size_t)nh, cudaMemcpyDeviceToHost, c->stream));
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    NXD_CUDA(cudaGetLastError());
+    return NXD_OK;
+}
+
+nxd_status nxd_ipc_max_step(nxd_ctx* c, const double* x, const double* dx, double eta, double* alpha, int64_t* n_pairs) {
+    if (!c || !x || !dx || !alpha || !(eta > 0.0 && eta < 1.0)) return NXD_INVALID_ARGUMENT;
+    nxd_status st = ipc_prepare(c);
+    if (st == NXD_OK) st = ipc_pose(c, x, dx);
+    if (st == NXD_OK) st = ipc_candidates(c, true, 0.0);
+    if (st != NXD_OK) return st;
+    IpcState* s = c->ipc;
+    const int n = s->n_pt + s->n_ee;
+    if (n_pairs) *n_pairs = n;
+    IPC_ENSURE(s->toi, 8 * (size_t)std::max(n, 1));
+    const IpcPairs P{s->pt.as<int>(), s->n_pt, s->ee.as<int>(), s->n_ee};
+    double* d_a = reinterpret_cast<double*>(s->scal.as<char>() + 40);
+    if (n) k_ipc_accd<<<grid_for(n, 128), 128, 0, c->stream>>>(s->pg, P, s->wq0.as<double>(), s->wq1.as<double>(), eta, 1000,
+                                                                s->toi.as<double>());
+    k_min_reduce<<<1, 1024, 0, c->stream>>>(s->toi.as<double>(), n, 1.0, d_a);
+    NXD_CUDA(cudaMemcpyAsync(alpha, d_a, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    NXD_CUDA(cudaGetLastError());
     return NXD_OK;
 }
 

@@ -60,6 +60,12 @@ def lib():
     L.nxd_batch_step.argtypes = [vp, dp]
     L.nxd_batch_get_state.argtypes = [vp, C.c_int32, C.POINTER(abi.NxdState)]
     L.nxd_batch_get_diagnostics.argtypes = [vp, C.c_int32, C.POINTER(abi.NxdDiagnostics)]
+    L.nxd_ipc_candidates.argtypes = [vp, vp, vp, C.c_double, ip, C.c_int64, ip, C.c_int64, i64p, i64p]
+    L.nxd_ipc_candidates.restype = C.c_int
+    L.nxd_ipc_barrier.argtypes = [vp, vp, C.c_double, C.c_double, dp, dp, ip, ip, dp, C.c_int64, i64p, i64p, i64p]
+    L.nxd_ipc_barrier.restype = C.c_int
+    L.nxd_ipc_max_step.argtypes = [vp, vp, vp, C.c_double, dp, i64p]
+    L.nxd_ipc_max_step.restype = C.c_int
     L.nxd_batch_groups.argtypes = [vp]
     L.nxd_batch_groups.restype = C.c_int32
     L.nxd_batch_set_stream.argtypes = [vp, vp]
@@ -237,6 +243,55 @@ class Context:
         _check("nxd_normal_forces", lib().nxd_normal_forces(self.h, abi.dptr(np.ascontiguousarray(x, np.float64)),
                                                             abi.dptr(out), n))
         return out[:n]
+
+
+    # --- primitive-level contact model (full IPC): nxd_ipc_*
+    def ipc_candidates(self, x=None, dx=None, inflation: float = 0.0):
+        """Point-triangle (vertex, face) and edge-edge (edge, edge) pairs,
+        int32 arrays of shape (n, 2), sorted (LBVH on the device)."""
+        L = lib()
+        npt, nee = C.c_int64(), C.c_int64()
+        xa = None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+        da = None if dx is None else np.ascontiguousarray(dx, dtype=np.float64)
+        xp = C.c_void_p(xa.ctypes.data) if xa is not None else None
+        dp_ = C.c_void_p(da.ctypes.data) if da is not None else None
+        _check("nxd_ipc_candidates", L.nxd_ipc_candidates(self.h, xp, dp_, inflation, None, 0, None, 0, C.byref(npt),
+                                                          C.byref(nee)))
+        pt = np.zeros((max(npt.value, 1), 2), dtype=np.int32)
+        ee = np.zeros((max(nee.value, 1), 2), dtype=np.int32)
+        _check("nxd_ipc_candidates", L.nxd_ipc_candidates(self.h, xp, dp_, inflation, abi.iptr(pt), npt.value,
+                                                          abi.iptr(ee), nee.value, C.byref(npt), C.byref(nee)))
+        return pt[:npt.value], ee[:nee.value]
+
+    def ipc_barrier(self, x, dhat: float, kappa: float):
+        """(energy, gradient[6N], (row_ptr, col_idx, vals[nnzb, 6, 6]), n_pairs, n_active)."""
+        L = lib()
+        n = self.scene.n_bodies
+        xa = np.ascontiguousarray(x, dtype=np.float64)
+        e = C.c_double()
+        g = np.zeros(6 * n)
+        nnzb, npairs, nact = C.c_int64(), C.c_int64(), C.c_int64()
+        rp = np.zeros(n + 1, dtype=np.int32)
+        _check("nxd_ipc_barrier", L.nxd_ipc_barrier(self.h, C.c_void_p(xa.ctypes.data), dhat, kappa, C.byref(e), abi.dptr(g),
+                                                    abi.iptr(rp), None, None, 0, C.byref(nnzb), C.byref(npairs),
+                                                    C.byref(nact)))
+        ci = np.zeros(max(nnzb.value, 1), dtype=np.int32)
+        vv = np.zeros((max(nnzb.value, 1), 6, 6))
+        _check("nxd_ipc_barrier", L.nxd_ipc_barrier(self.h, C.c_void_p(xa.ctypes.data), dhat, kappa, C.byref(e), abi.dptr(g),
+                                                    abi.iptr(rp), abi.iptr(ci), abi.dptr(vv), nnzb.value, C.byref(nnzb),
+                                                    C.byref(npairs), C.byref(nact)))
+        m = nnzb.value
+        return e.value, g, (rp, ci[:m], vv[:m]), npairs.value, nact.value
+
+    def ipc_max_step(self, x, dx, eta: float = 0.1):
+        """(alpha, n_pairs): additive-CCD bound of the step x -> x + dx."""
+        a = C.c_double()
+        n = C.c_int64()
+        xa = np.ascontiguousarray(x, dtype=np.float64)
+        da = np.ascontiguousarray(dx, dtype=np.float64)
+        _check("nxd_ipc_max_step", lib().nxd_ipc_max_step(self.h, C.c_void_p(xa.ctypes.data), C.c_void_p(da.ctypes.data),
+                                                          eta, C.byref(a), C.byref(n)))
+        return a.value, n.value
 
 
 class Batch:

@@ -7,4 +7,4 @@ here="$(cd "$(dirname "$0")" && pwd)"
 mkdir -p "$here/_build"
 g++ -std=c++17 -O3 -march=x86-64-v3 -ffp-contract=off -fno-fast-math -fopenmp -fPIC -shared \
     -Wall -Wextra -Wno-unused-parameter \
-    -o "$here/_build/librefcpu.so" "$here/refcpu.cpp"
+    -o "$here/_build/librefcpu.so" "$here/refcpu.cpp" "$here/ipc_cpu.cpp"

@@ -1,0 +1,334 @@
+// ipc_cpu.cpp — CPU checker for the primitive-level contact model (full IPC).
+//
+// Test infrastructure, like refcpu.cpp: only tests/ and bench.py's CPU leg
+// load it.  The reference has no primitive-level model, so this restates
+// the published method (Li et al. 2020 IPC; Li et al. 2021 additive CCD)
+// with the per-pair arithmetic shared with the kernels (ipc_pair.h), and
+// checks everything around it independently:
+//   - candidate sets by an exact sweep over x-sorted boxes (no BVH);
+//   - the subspace PSD projection against a full 12x12 Jacobi projection
+//     of the raw pair Hessian (nxo_ipc_pair);
+//   - derivatives by finite differences (in tests/).
+// Sums follow the device's fixed orders: energies through the padded
+// pairwise tree, gradients and Hessian blocks in pair order.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "refcpu.h"
+#include "../nexdynipc_b200/csrc/ipc_pair.h"
+
+using nx::V3;
+namespace ipc = nx::ipc;
+
+namespace {
+
+struct Geo {
+    int64_t nv = 0, nf = 0, ne = 0;
+    int N = 0;
+    std::vector<int32_t> vbody, fbody, fvert, ebody, evert;
+    std::vector<double> wv, wv1, pos;
+};
+
+Geo load(nxo_world* w, const double* x, const double* dx) {
+    Geo g;
+    nxo_prim_counts(w, &g.nv, &g.nf, &g.ne);
+    g.N = nxo_body_count(w);
+    g.vbody.resize(g.nv); g.fbody.resize(g.nf); g.fvert.resize(3 * g.nf); g.ebody.resize(g.ne); g.evert.resize(2 * g.ne);
+    nxo_prim_topology(w, g.vbody.data(), g.fbody.data(), g.fvert.data(), g.ebody.data(), g.evert.data());
+    g.wv.resize(3 * g.nv); g.pos.resize(3 * g.N);
+    nxo_world_vertices_at(w, x, g.wv.data(), g.pos.data());
+    if (dx) {
+        std::vector<double> x1(6 * (size_t)g.N);
+        for (size_t i = 0; i < x1.size(); ++i) x1[i] = x[i] + dx[i];
+        g.wv1.resize(3 * g.nv);
+        nxo_world_vertices_at(w, x1.data(), g.wv1.data(), nullptr);
+    }
+    return g;
+}
+
+struct Box { double mn[3], mx[3]; };
+
+Box box_of(const Geo& g, const int32_t* vid, int nvid, double infl) {
+    V3 mn = nx::ld3(&g.wv[3 * vid[0]]), mx = mn;
+    for (int k = 0; k < nvid; ++k) {
+        const V3 a = nx::ld3(&g.wv[3 * vid[k]]);
+        mn = nx::cwmin(mn, a); mx = nx::cwmax(mx, a);
+        if (!g.wv1.empty()) { const V3 b = nx::ld3(&g.wv1[3 * vid[k]]); mn = nx::cwmin(mn, b); mx = nx::cwmax(mx, b); }
+    }
+    const V3 e = nx::v3(infl, infl, infl);
+    const V3 lo = mn - e, hi = mx + e;
+    return Box{{lo.x, lo.y, lo.z}, {hi.x, hi.y, hi.z}};
+}
+
+bool overlap(const Box& a, const Box& b) {
+    return a.mn[0] <= b.mx[0] && b.mn[0] <= a.mx[0] && a.mn[1] <= b.mx[1] && b.mn[1] <= a.mx[1] && a.mn[2] <= b.mx[2] &&
+           b.mn[2] <= a.mx[2];
+}
+
+// All (query, leaf) pairs with overlapping boxes that `keep` accepts, query
+// ascending, leaf ascending: leaves sorted by min x; a query scans the
+// leaves whose min x lies in [q.min.x - widest, q.max.x]; leaves much wider
+// than the typical one are tested against every query.
+template <typename Keep>
+std::vector<int32_t> sweep(const std::vector<Box>& q, const std::vector<Box>& leaf, Keep keep) {
+    std::vector<double> widths;
+    for (const Box& b : leaf) widths.push_back(b.mx[0] - b.mn[0]);
+    std::vector<double> ws = widths;
+    std::sort(ws.begin(), ws.end());
+    const double typical = ws.empty() ? 0.0 : ws[ws.size() / 2];
+    std::vector<int> small, big;
+    for (int i = 0; i < (int)leaf.size(); ++i) (widths[i] > 8.0 * typical + 1e-12 ? big : small).push_back(i);
+    std::sort(small.begin(), small.end(), [&](int a, int b) { return leaf[a].mn[0] < leaf[b].mn[0] || (leaf[a].mn[0] == leaf[b].mn[0] && a < b); });
+    double widest = 0.0;
+    std::vector<double> smin;
+    for (int i : small) { widest = std::max(widest, widths[i]); smin.push_back(leaf[i].mn[0]); }
+    std::vector<std::vector<int32_t>> hits(q.size());
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long long qi = 0; qi < (long long)q.size(); ++qi) {
+        const Box& Q = q[qi];
+        std::vector<int32_t>& h = hits[qi];
+        const auto lo = std::lower_bound(smin.begin(), smin.end(), Q.mn[0] - widest) - smin.begin();
+        for (size_t k = lo; k < small.size() && smin[k] <= Q.mx[0]; ++k) {
+            const int L = small[k];
+            if (overlap(Q, leaf[L]) && keep((int)qi, L)) h.push_back(L);
+        }
+        for (int L : big)
+            if (overlap(Q, leaf[L]) && keep((int)qi, L)) h.push_back(L);
+        std::sort(h.begin(), h.end());
+    }
+    std::vector<int32_t> out;
+    for (size_t qi = 0; qi < q.size(); ++qi)
+        for (int32_t L : hits[qi]) { out.push_back((int32_t)qi); out.push_back(L); }
+    return out;
+}
+
+void candidates(const Geo& g, double infl, std::vector<int32_t>& pt, std::vector<int32_t>& ee) {
+    std::vector<Box> fb(g.nf), eb(g.ne), qv(g.nv), qe(g.ne);
+    for (int64_t f = 0; f < g.nf; ++f) fb[f] = box_of(g, &g.fvert[3 * f], 3, infl);
+    for (int64_t e = 0; e < g.ne; ++e) { eb[e] = box_of(g, &g.evert[2 * e], 2, infl); qe[e] = box_of(g, &g.evert[2 * e], 2, 0.0); }
+    for (int64_t v = 0; v < g.nv; ++v) { const int32_t id = (int32_t)v; qv[v] = box_of(g, &id, 1, 0.0); }
+    pt = sweep(qv, fb, [&](int v, int f) { return g.vbody[v] != g.fbody[f]; });
+    ee = sweep(qe, eb, [&](int a, int b) { return a < b && g.ebody[a] != g.ebody[b]; });
+}
+
+void pair_points(const Geo& g, const std::vector<int32_t>& pt, const std::vector<int32_t>& ee, size_t p, int& kind, V3* X,
+                 int* side, V3* arm, int& bA, int& bB) {
+    int vid[4];
+    const size_t npt = pt.size() / 2;
+    if (p < npt) {
+        kind = ipc::kPairPT;
+        const int v = pt[2 * p], f = pt[2 * p + 1];
+        vid[0] = v; vid[1] = g.fvert[3 * f]; vid[2] = g.fvert[3 * f + 1]; vid[3] = g.fvert[3 * f + 2];
+        bA = g.vbody[v]; bB = g.fbody[f];
+        side[0] = 0; side[1] = 1; side[2] = 1; side[3] = 1;
+    } else {
+        kind = ipc::kPairEE;
+        const size_t q = p - npt;
+        const int e0 = ee[2 * q], e1 = ee[2 * q + 1];
+        vid[0] = g.evert[2 * e0]; vid[1] = g.evert[2 * e0 + 1]; vid[2] = g.evert[2 * e1]; vid[3] = g.evert[2 * e1 + 1];
+        bA = g.ebody[e0]; bB = g.ebody[e1];
+        side[0] = 0; side[1] = 0; side[2] = 1; side[3] = 1;
+    }
+    for (int k = 0; k < 4; ++k) {
+        X[k] = nx::ld3(&g.wv[3 * vid[k]]);
+        arm[k] = X[k] - nx::ld3(&g.pos[3 * (side[k] ? bB : bA)]);
+    }
+}
+
+// the device's fixed pairwise tree (pad to a power of two, halve)
+double tree_sum(std::vector<double> v) {
+    size_t P = 1;
+    while (P < v.size()) P <<= 1;
+    v.resize(P, 0.0);
+    for (size_t h = P / 2; h >= 1; h /= 2) {
+        for (size_t i = 0; i < h; ++i) v[i] = v[i] + v[i + h];
+        if (h == 1) break;
+    }
+    return v.empty() ? 0.0 : v[0];
+}
+
+// Raw 12x12 pair Hessian b'' grad grad^T + b' hess(d^2), written out densely.
+void raw_hessian(const ipc::DistForm& f, const V3* X, double dhat, double kappa, double* H) {
+    for (int i = 0; i < 144; ++i) H[i] = 0.0;
+    const V3 r = ipc::form_r(f, X);
+    const double s = nx::dot(r, r), sh = dhat * dhat;
+    if (!(s < sh) || !(s > 0.0)) return;
+    const double b1 = ipc::barrier_s1(s, sh, kappa), b2 = ipc::barrier_s2(s, sh, kappa);
+    double gs[12];
+    for (int k = 0; k < 4; ++k) { gs[3 * k] = 2.0 * f.w[k] * r.x; gs[3 * k + 1] = 2.0 * f.w[k] * r.y; gs[3 * k + 2] = 2.0 * f.w[k] * r.z; }
+    V3 a[2] = {nx::v3(0, 0, 0), nx::v3(0, 0, 0)};
+    for (int j = 0; j < f.nu; ++j) a[j] = f.c[0][j] * X[0] + f.c[1][j] * X[1] + f.c[2][j] * X[2] + f.c[3][j] * X[3];
+    double M[2][2] = {{0, 0}, {0, 0}}, Mi[2][2] = {{0, 0}, {0, 0}};
+    for (int i = 0; i < f.nu; ++i)
+        for (int j = 0; j < f.nu; ++j) M[i][j] = 2.0 * nx::dot(a[i], a[j]);
+    if (f.nu == 1) Mi[0][0] = 1.0 / M[0][0];
+    if (f.nu == 2) {
+        const double det = M[0][0] * M[1][1] - M[0][1] * M[1][0];
+        Mi[0][0] = M[1][1] / det; Mi[1][1] = M[0][0] / det; Mi[0][1] = -M[0][1] / det; Mi[1][0] = -M[1][0] / det;
+    }
+    double G[2][12];
+    for (int j = 0; j < f.nu; ++j)
+        for (int k = 0; k < 4; ++k)
+            for (int c = 0; c < 3; ++c) G[j][3 * k + c] = 2.0 * (f.w[k] * nx::get(a[j], c) + f.c[k][j] * nx::get(r, c));
+    for (int I = 0; I < 12; ++I)
+        for (int J = 0; J < 12; ++J) {
+            double hs = (I % 3 == J % 3) ? 2.0 * f.w[I / 3] * f.w[J / 3] : 0.0;
+            for (int p = 0; p < f.nu; ++p)
+                for (int q = 0; q < f.nu; ++q) hs -= G[p][I] * Mi[p][q] * G[q][J];
+            H[12 * I + J] = b2 * gs[I] * gs[J] + b1 * hs;
+        }
+}
+
+}  // namespace
+
+extern "C" {
+
+int nxo_ipc_candidates(nxo_world* w, const double* x, const double* dx, double infl, int32_t* pt, int64_t pt_cap, int32_t* ee,
+                       int64_t ee_cap, int64_t* n_pt, int64_t* n_ee) {
+    const Geo g = load(w, x, dx);
+    std::vector<int32_t> P, E;
+    candidates(g, infl, P, E);
+    *n_pt = (int64_t)P.size() / 2;
+    *n_ee = (int64_t)E.size() / 2;
+    if (pt) std::memcpy(pt, P.data(), sizeof(int32_t) * (size_t)std::min<int64_t>(2 * pt_cap, (int64_t)P.size()));
+    if (ee) std::memcpy(ee, E.data(), sizeof(int32_t) * (size_t)std::min<int64_t>(2 * ee_cap, (int64_t)E.size()));
+    return (*n_pt > pt_cap && pt) || (*n_ee > ee_cap && ee) ? NXD_CAPACITY : NXD_OK;
+}
+
+// Barrier over the candidates at x (boxes inflated by dhat): energy (fixed
+// tree over all pairs, PT then EE), gradient (6N, pair order) and, when H is
+// not NULL, the dense 6N x 6N PSD-projected Hessian (pair order per block).
+int nxo_ipc_barrier(nxo_world* w, const double* x, double dhat, double kappa, double* energy, double* grad, double* H,
+                    int64_t* n_pairs, int64_t* n_active) {
+    const Geo g = load(w, x, nullptr);
+    std::vector<int32_t> P, E;
+    candidates(g, dhat, P, E);
+    const size_t n = P.size() / 2 + E.size() / 2;
+    const int N6 = 6 * g.N;
+    std::vector<double> e(n);
+    if (grad) std::fill(grad, grad + N6, 0.0);
+    if (H) std::fill(H, H + (size_t)N6 * N6, 0.0);
+    int64_t na = 0;
+    for (size_t p = 0; p < n; ++p) {
+        int kind, side[4], bA, bB;
+        V3 X[4], arm[4];
+        pair_points(g, P, E, p, kind, X, side, arm, bA, bB);
+        const ipc::DistForm f = ipc::classify(kind, X);
+        const ipc::PairEval ev = ipc::pair_barrier(f, X, dhat, kappa);
+        e[p] = ev.e;
+        if (!(ev.d2 < dhat * dhat)) continue;
+        ++na;
+        double g12[12];
+        ipc::chain12(ev.grad, side, arm, g12);
+        const int b[2] = {bA, bB};
+        if (grad)
+            for (int s = 0; s < 2; ++s)
+                for (int d = 0; d < 6; ++d) grad[6 * b[s] + d] += g12[6 * s + d];
+        if (!H) continue;
+        double z[5][12];
+        for (int k = 0; k < ev.n_terms; ++k) ipc::chain12(ev.y[k], side, arm, z[k]);
+        for (int r = 0; r < 2; ++r)
+            for (int c = 0; c < 2; ++c)
+                for (int i = 0; i < 6; ++i)
+                    for (int j = 0; j < 6; ++j) {
+                        double blk = 0.0;
+                        for (int k = 0; k < ev.n_terms; ++k) blk += (ev.lam[k] * z[k][6 * r + i]) * z[k][6 * c + j];
+                        H[(size_t)(6 * b[r] + i) * N6 + 6 * b[c] + j] += blk;
+                    }
+    }
+    if (energy) *energy = tree_sum(e);
+    if (n_pairs) *n_pairs = (int64_t)n;
+    if (n_active) *n_active = na;
+    return NXD_OK;
+}
+
+// Largest step fraction in [0, 1] along x -> x + dx that additive CCD allows
+// (eta: kept fraction of each pair's initial distance), over the pairs whose
+// swept boxes overlap.
+double nxo_ipc_max_step(nxo_world* w, const double* x, const double* dx, double eta, int64_t* n_pairs) {
+    const Geo g = load(w, x, dx);
+    std::vector<int32_t> P, E;
+    candidates(g, 0.0, P, E);
+    const size_t n = P.size() / 2 + E.size() / 2;
+    if (n_pairs) *n_pairs = (int64_t)n;
+    double t = 1.0;
+    for (size_t p = 0; p < n; ++p) {
+        int kind, side[4], bA, bB;
+        V3 X[4], arm[4];
+        pair_points(g, P, E, p, kind, X, side, arm, bA, bB);
+        int vid[4];
+        if (p < P.size() / 2) {
+            const int v = P[2 * p], f = P[2 * p + 1];
+            vid[0] = v; vid[1] = g.fvert[3 * f]; vid[2] = g.fvert[3 * f + 1]; vid[3] = g.fvert[3 * f + 2];
+        } else {
+            const size_t q = p - P.size() / 2;
+            vid[0] = g.evert[2 * E[2 * q]]; vid[1] = g.evert[2 * E[2 * q] + 1];
+            vid[2] = g.evert[2 * E[2 * q + 1]]; vid[3] = g.evert[2 * E[2 * q + 1] + 1];
+        }
+        V3 D[4];
+        for (int k = 0; k < 4; ++k) D[k] = nx::ld3(&g.wv1[3 * vid[k]]) - X[k];
+        t = nx::dmin(t, ipc::accd_toi(kind, X, D, 1.0, eta, 1000, nullptr));
+    }
+    return t;
+}
+
+// One pair (X12 = four points): d^2, type, energy, gradient (12), the
+// subspace PSD Hessian (144), the raw Hessian (144) and its PSD projection
+// by a full 12x12 Jacobi decomposition (144).  Any output may be NULL.
+int nxo_ipc_pair(int32_t kind, const double* X12, double dhat, double kappa, double* d2, int32_t* type, double* e, double* g12,
+                 double* H_sub, double* H_raw, double* H_full) {
+    V3 X[4];
+    for (int k = 0; k < 4; ++k) X[k] = nx::ld3(X12 + 3 * k);
+    const ipc::DistForm f = ipc::classify(kind, X);
+    const ipc::PairEval ev = ipc::pair_barrier(f, X, dhat, kappa);
+    if (d2) *d2 = ev.d2;
+    if (type) *type = f.type;
+    if (e) *e = ev.e;
+    if (g12)
+        for (int k = 0; k < 4; ++k) nx::st3(g12 + 3 * k, ev.grad.v[k]);
+    if (H_sub) {
+        for (int i = 0; i < 144; ++i) H_sub[i] = 0.0;
+        for (int k = 0; k < ev.n_terms; ++k)
+            for (int I = 0; I < 12; ++I)
+                for (int J = 0; J < 12; ++J)
+                    H_sub[12 * I + J] += ev.lam[k] * nx::get(ev.y[k].v[I / 3], I % 3) * nx::get(ev.y[k].v[J / 3], J % 3);
+    }
+    double R[144];
+    raw_hessian(f, X, dhat, kappa, R);
+    if (H_raw) std::memcpy(H_raw, R, sizeof(R));
+    if (H_full) {
+        double A[12][12], V[12][12];
+        for (int i = 0; i < 12; ++i)
+            for (int j = 0; j < 12; ++j) A[i][j] = 0.5 * (R[12 * i + j] + R[12 * j + i]);
+        ipc::jacobi_eigen<12>(A, V, 12);
+        for (int i = 0; i < 12; ++i)
+            for (int j = 0; j < 12; ++j) {
+                double h = 0.0;
+                for (int k = 0; k < 12; ++k)
+                    if (A[k][k] > 0.0) h += A[k][k] * V[i][k] * V[j][k];
+                H_full[12 * i + j] = h;
+            }
+    }
+    return NXD_OK;
+}
+
+double nxo_ipc_accd(int32_t kind, const double* X12, const double* D12, double t_max, double eta, int32_t max_iter,
+                    int32_t* iters) {
+    V3 X[4], D[4];
+    for (int k = 0; k < 4; ++k) { X[k] = nx::ld3(X12 + 3 * k); D[k] = nx::ld3(D12 + 3 * k); }
+    int it = 0;
+    const double t = ipc::accd_toi(kind, X, D, t_max, eta, max_iter, &it);
+    if (iters) *iters = it;
+    return t;
+}
+
+double nxo_ipc_dist2(int32_t kind, const double* X12) {
+    V3 X[4];
+    for (int k = 0; k < 4; ++k) X[k] = nx::ld3(X12 + 3 * k);
+    return ipc::dist2(kind, X);
+}
+
+}  // extern "C"

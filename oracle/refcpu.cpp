@@ -2386,4 +2386,65 @@ int nxo_interval_root_poly(const double* c, int32_t deg, double lo, double hi, d
     return found ? 1 : 0;
 }
 
+// ---------------------------------------------------------------------------
+// Geometry accessors for the primitive-level (full IPC) checker in
+// ipc_cpu.cpp: primitives numbered over bodies in world order (vertices,
+// faces, unique edges of each body's mesh; meshless bodies have none), the
+// same numbering the device uses.
+// ---------------------------------------------------------------------------
+int32_t nxo_body_count(nxo_world* w) { return (int32_t)w->bodies.size(); }
+
+void nxo_prim_counts(nxo_world* w, int64_t* nv, int64_t* nf, int64_t* ne) {
+    int64_t a = 0, b = 0, c = 0;
+    for (const Body& B : w->bodies) {
+        if (B.mesh < 0) continue;
+        const Mesh& M = w->meshes[B.mesh];
+        a += (int64_t)M.V.size(); b += (int64_t)M.F.size(); c += (int64_t)M.E.size();
+    }
+    *nv = a; *nf = b; *ne = c;
+}
+
+void nxo_prim_topology(nxo_world* w, int32_t* vbody, int32_t* fbody, int32_t* fvert, int32_t* ebody, int32_t* evert) {
+    int vo = 0, fo = 0, eo = 0;
+    for (int i = 0; i < (int)w->bodies.size(); ++i) {
+        const Body& B = w->bodies[i];
+        if (B.mesh < 0) continue;
+        const Mesh& M = w->meshes[B.mesh];
+        for (size_t v = 0; v < M.V.size(); ++v) vbody[vo + v] = i;
+        for (size_t f = 0; f < M.F.size(); ++f) {
+            fbody[fo + f] = i;
+            for (int k = 0; k < 3; ++k) fvert[3 * (fo + f) + k] = vo + M.F[f][k];
+        }
+        for (size_t e = 0; e < M.E.size(); ++e) {
+            ebody[eo + e] = i;
+            for (int k = 0; k < 2; ++k) evert[2 * (eo + e) + k] = vo + M.E[e][k];
+        }
+        vo += (int)M.V.size(); fo += (int)M.F.size(); eo += (int)M.E.size();
+    }
+}
+
+// World vertices and body positions at state x (6N; p = x[6i..], q =
+// exp(theta) q_body as in detectContactsAtState), or at the current poses
+// when x is NULL.
+void nxo_world_vertices_at(nxo_world* w, const double* x, double* wv, double* pos) {
+    int vo = 0;
+    for (int i = 0; i < (int)w->bodies.size(); ++i) {
+        const Body& B = w->bodies[i];
+        V3 p = B.position;
+        Q q = B.orientation;
+        if (x) {
+            p = V3{x[6 * i], x[6 * i + 1], x[6 * i + 2]};
+            q = update_rotation_gt(B.orientation, V3{x[6 * i + 3], x[6 * i + 4], x[6 * i + 5]});
+        }
+        if (pos) { pos[3 * i] = p.x; pos[3 * i + 1] = p.y; pos[3 * i + 2] = p.z; }
+        if (B.mesh < 0) continue;
+        const Mesh& M = w->meshes[B.mesh];
+        for (size_t v = 0; v < M.V.size(); ++v) {
+            const V3 a = p + qrot(q, M.V[v]);
+            wv[3 * (vo + v)] = a.x; wv[3 * (vo + v) + 1] = a.y; wv[3 * (vo + v) + 2] = a.z;
+        }
+        vo += (int)M.V.size();
+    }
+}
+
 }  // extern "C"

@@ -86,6 +86,24 @@ void nxo_friction_hessian_smooth(const double* u, double N, double mu, double ep
 int nxo_interval_root_poly(const double* coeffs, int32_t degree, double lo, double hi,
                            double tol, double* root_lo, double* root_hi);
 
+/* Geometry accessors (primitives numbered over bodies in world order). */
+int32_t nxo_body_count(nxo_world* w);
+void nxo_prim_counts(nxo_world* w, int64_t* nv, int64_t* nf, int64_t* ne);
+void nxo_prim_topology(nxo_world* w, int32_t* vbody, int32_t* fbody, int32_t* fvert, int32_t* ebody, int32_t* evert);
+void nxo_world_vertices_at(nxo_world* w, const double* x, double* wv, double* pos);
+
+/* Primitive-level contact model (full IPC), ipc_cpu.cpp. */
+int nxo_ipc_candidates(nxo_world* w, const double* x, const double* dx, double inflation, int32_t* pt, int64_t pt_cap,
+                       int32_t* ee, int64_t ee_cap, int64_t* n_pt, int64_t* n_ee);
+int nxo_ipc_barrier(nxo_world* w, const double* x, double dhat, double kappa, double* energy, double* grad, double* H,
+                    int64_t* n_pairs, int64_t* n_active);
+double nxo_ipc_max_step(nxo_world* w, const double* x, const double* dx, double eta, int64_t* n_pairs);
+int nxo_ipc_pair(int32_t kind, const double* X12, double dhat, double kappa, double* d2, int32_t* type, double* e,
+                 double* g12, double* H_sub, double* H_raw, double* H_full);
+double nxo_ipc_accd(int32_t kind, const double* X12, const double* D12, double t_max, double eta, int32_t max_iter,
+                    int32_t* iters);
+double nxo_ipc_dist2(int32_t kind, const double* X12);
+
 #ifdef __cplusplus
 }
 #endif

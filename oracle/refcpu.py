@@ -71,6 +71,16 @@ def lib():
         getattr(L, nm).argtypes = [dp, C.c_double, C.c_double, C.c_double, dp]
     L.nxo_interval_root_poly.restype = C.c_int
     L.nxo_interval_root_poly.argtypes = [dp, C.c_int32, C.c_double, C.c_double, C.c_double, dp, dp]
+    i64p = C.POINTER(C.c_int64)
+    L.nxo_ipc_candidates.argtypes = [vp, dp, dp, C.c_double, ip, i64, ip, i64, i64p, i64p]
+    L.nxo_ipc_barrier.argtypes = [vp, dp, C.c_double, C.c_double, dp, dp, dp, i64p, i64p]
+    L.nxo_ipc_max_step.restype = C.c_double
+    L.nxo_ipc_max_step.argtypes = [vp, dp, dp, C.c_double, i64p]
+    L.nxo_ipc_pair.argtypes = [C.c_int32, dp, C.c_double, C.c_double, dp, ip, dp, dp, dp, dp, dp]
+    L.nxo_ipc_accd.restype = C.c_double
+    L.nxo_ipc_accd.argtypes = [C.c_int32, dp, dp, C.c_double, C.c_double, C.c_int32, ip]
+    L.nxo_ipc_dist2.restype = C.c_double
+    L.nxo_ipc_dist2.argtypes = [C.c_int32, dp]
     _lib = L
     return L
 
@@ -195,6 +205,63 @@ class OracleWorld:
         out = np.zeros(max(n, 1))
         lib().nxo_normal_forces(self.h, _d(x), abi.dptr(out), n)
         return out[:n]
+
+
+    # --- primitive-level contact model (full IPC), ipc_cpu.cpp
+    def ipc_candidates(self, x=None, dx=None, inflation: float = 0.0):
+        """(pt, ee) int32 arrays of shape (n, 2), sorted."""
+        L = lib()
+        npt, nee = C.c_int64(), C.c_int64()
+        xa = None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+        da = None if dx is None else np.ascontiguousarray(dx, dtype=np.float64)
+        xp = abi.dptr(xa) if xa is not None else None
+        dp_ = abi.dptr(da) if da is not None else None
+        L.nxo_ipc_candidates(self.h, xp, dp_, inflation, None, 0, None, 0, C.byref(npt), C.byref(nee))
+        pt = np.zeros((max(npt.value, 1), 2), dtype=np.int32)
+        ee = np.zeros((max(nee.value, 1), 2), dtype=np.int32)
+        L.nxo_ipc_candidates(self.h, xp, dp_, inflation, abi.iptr(pt), npt.value, abi.iptr(ee), nee.value, C.byref(npt),
+                             C.byref(nee))
+        return pt[:npt.value], ee[:nee.value]
+
+    def ipc_barrier(self, x, dhat: float, kappa: float, hessian: bool = True):
+        """(energy, gradient[6N], dense Hessian[6N, 6N] or None, n_pairs, n_active)."""
+        n6 = 6 * self.scene.n_bodies
+        g = np.zeros(n6)
+        H = np.zeros((n6, n6)) if hessian else None
+        e = C.c_double()
+        npairs, nact = C.c_int64(), C.c_int64()
+        lib().nxo_ipc_barrier(self.h, _d(x), dhat, kappa, C.byref(e), abi.dptr(g), abi.dptr(H) if hessian else None,
+                              C.byref(npairs), C.byref(nact))
+        return e.value, g, H, npairs.value, nact.value
+
+    def ipc_max_step(self, x, dx, eta: float = 0.1):
+        n = C.c_int64()
+        a = lib().nxo_ipc_max_step(self.h, _d(x), _d(dx), eta, C.byref(n))
+        return a, n.value
+
+
+def ipc_pair(kind: int, X, dhat: float, kappa: float) -> dict:
+    """One pair of four points (kind 0 point-triangle, 1 edge-edge)."""
+    X = np.ascontiguousarray(X, dtype=np.float64).reshape(12)
+    d2, e = C.c_double(), C.c_double()
+    t = C.c_int32()
+    g = np.zeros(12)
+    Hs, Hr, Hf = np.zeros(144), np.zeros(144), np.zeros(144)
+    lib().nxo_ipc_pair(kind, abi.dptr(X), dhat, kappa, C.byref(d2), C.byref(t), C.byref(e), abi.dptr(g), abi.dptr(Hs),
+                       abi.dptr(Hr), abi.dptr(Hf))
+    return {"d2": d2.value, "type": t.value, "e": e.value, "g": g, "H_sub": Hs.reshape(12, 12),
+            "H_raw": Hr.reshape(12, 12), "H_full": Hf.reshape(12, 12)}
+
+
+def ipc_dist2(kind: int, X) -> float:
+    return lib().nxo_ipc_dist2(kind, _d(np.asarray(X, dtype=np.float64).reshape(12)))
+
+
+def ipc_accd(kind: int, X, D, t_max: float = 1.0, eta: float = 0.1, max_iter: int = 1000):
+    it = C.c_int32()
+    t = lib().nxo_ipc_accd(kind, _d(np.asarray(X, dtype=np.float64).reshape(12)),
+                           _d(np.asarray(D, dtype=np.float64).reshape(12)), t_max, eta, max_iter, C.byref(it))
+    return t, it.value
 
 
 def libm(fn: int, x, y=None) -> np.ndarray:
