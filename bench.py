@@ -206,6 +206,43 @@ def batched_leg(torch, steps: int, warmup: int, flush):
     return out
 
 
+def mode_i_leg(ctx, sc, reps: int = 5):
+    """Primitive-level contact model on the workload's current state, through
+    the C ABI (host arrays in and out, each call synchronising): LBVH
+    candidates (boxes inflated by dhat), the barrier form (energy, gradient,
+    BSR Hessian) and the additive-CCD bound of the velocity step x -> x +
+    dt v.  Median wall time of `reps` calls after one warm-up call."""
+    st = ctx.state()
+    n = sc.n_bodies
+    x = np.zeros(6 * n)
+    dx = np.zeros(6 * n)
+    for i in range(n):
+        x[6 * i:6 * i + 3] = st["position"][i]
+        dx[6 * i:6 * i + 3] = sc.dt * st["velocity"][i]
+        dx[6 * i + 3:6 * i + 6] = sc.dt * st["angular_velocity"][i]
+    dhat, kappa = sc.settings.dhat, 1e6
+
+    def timed(fn):
+        fn()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            out = fn()
+            ts.append(time.perf_counter() - t0)
+        return float(np.median(ts)), out
+
+    t_c, (pt, ee) = timed(lambda: ctx.ipc_candidates(x, None, dhat))
+    t_b, (e, g, bsr, npairs, nact) = timed(lambda: ctx.ipc_barrier(x, dhat, kappa))
+    t_s, (alpha, nccd) = timed(lambda: ctx.ipc_max_step(x, dx, 0.1))
+    return {"candidates": {"ms": 1e3 * t_c, "pt_pairs": int(len(pt)), "ee_pairs": int(len(ee)),
+                           "pairs_per_s": (len(pt) + len(ee)) / t_c},
+            "barrier": {"ms": 1e3 * t_b, "pairs": int(npairs), "active": int(nact), "bsr_blocks": int(len(bsr[1])),
+                        "pairs_per_s": npairs / t_b},
+            "max_step": {"ms": 1e3 * t_s, "pairs": int(nccd), "alpha": alpha, "pairs_per_s": nccd / t_s},
+            "timing": "wall clock per C-ABI call (host copies included), median of %d after a warm-up call" % reps,
+            "primitives": {"vertices": int(sc.n_vertices), "faces": int(sc.n_faces)}}
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
@@ -242,6 +279,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-mode-i", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.impl == "reference":
@@ -398,6 +436,8 @@ def main():
                                                           else dict(family_roof(fam), achieved=None, frac=None))
     per_family = {FAMILIES[i]: {"ms": round(float(prof_ms[i]), 3), "launches": int(prof_n[i])} for i in range(9)}
 
+    mode_i = None if args.no_mode_i else mode_i_leg(ctx, sc)
+
     batched = None
     if not args.no_batched:
         batched = batched_leg(torch, min(args.steps, 10), 2, flush)
@@ -423,7 +463,8 @@ def main():
                    "per_family_ms": per_family, "last_step": {k: diag[k] for k in
                                                               ("n_body_pairs", "n_contacts", "alm_iterations",
                                                                "newton_iterations", "status")},
-                   "batched": batched},
+                   "batched": batched,
+                   "mode_i": mode_i},
         "roofline": roof,
         "roofline_narrow_phase": roof_narrow,
         "cpu_baseline": cpu,
