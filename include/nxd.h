@@ -84,7 +84,16 @@ typedef struct nxd_settings {
     double newton_tol;               /* Options::tolerance                     */
     double ls_c1;                    /* Options::line_search_c1                */
     double ls_rho;                   /* Options::line_search_rho               */
+    int32_t integrator;              /* NXD_INTEGRATOR_* (setIntegrator)       */
+    int32_t reserved0;
+    double newmark_beta;             /* ImplicitNewmark(beta, gamma)           */
+    double newmark_gamma;
 } nxd_settings;
+
+/* Time integrators (TimeIntegration/ImplicitTimeIntegrator.cpp:15-33):
+ * implicit Euler (the IPCSolver default) and Newmark (the Simulation
+ * default, beta 0.25, gamma 0.5). */
+enum { NXD_INTEGRATOR_IMPLICIT_EULER = 0, NXD_INTEGRATOR_IMPLICIT_NEWMARK = 1 };
 
 /* Fill an nxd_settings with the reference's defaults
  * (IPCSolver.h:97-119, NewtonSolver.h:58-64, LineSearch.h:36-38). */
@@ -118,6 +127,13 @@ typedef struct nxd_scene_desc {
     const int32_t* drive_body_b;         /* [n_drives] body id                    */
     const double* drive_params;          /* [n_drives*8]                          */
     nxd_settings settings;
+    /* IPCSolver::addAllowedContactPair (IPCSolver.cpp:275-289): when
+     * n_contact_pairs > 0 only these body pairs make contacts, and a pair's
+     * friction >= 0 overrides the friction coefficient in the per-step mean
+     * over the active contacts (IPCSolver.cpp:891-911). */
+    int32_t n_contact_pairs;
+    const int32_t* contact_pair_bodies;  /* [n_contact_pairs*2] body ids         */
+    const double* contact_pair_friction; /* [n_contact_pairs] (< 0: none) or NULL */
 } nxd_scene_desc;
 
 /* Body state as written back by IPCSolver::step (IPCSolver.cpp:1174-1195). */

@@ -55,7 +55,14 @@ class NxdSettings(C.Structure):
         ("newton_tol", C.c_double),
         ("ls_c1", C.c_double),
         ("ls_rho", C.c_double),
+        ("integrator", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("newmark_beta", C.c_double),
+        ("newmark_gamma", C.c_double),
     ]
+
+INTEGRATOR_IMPLICIT_EULER = 0
+INTEGRATOR_IMPLICIT_NEWMARK = 1
 
 
 def default_settings() -> NxdSettings:
@@ -80,6 +87,9 @@ def default_settings() -> NxdSettings:
     s.newton_tol = 1e-6
     s.ls_c1 = 1e-4
     s.ls_rho = 0.5
+    s.integrator = INTEGRATOR_IMPLICIT_EULER     # IPCSolver's own default (IPCSolver.cpp:264-266)
+    s.newmark_beta = 0.25                        # ImplicitTimeIntegrator::create defaults
+    s.newmark_gamma = 0.5
     return s
 
 
@@ -110,6 +120,9 @@ class NxdSceneDesc(C.Structure):
         ("drive_body_b", _ip),
         ("drive_params", _dp),
         ("settings", NxdSettings),
+        ("n_contact_pairs", C.c_int32),
+        ("contact_pair_bodies", _ip),
+        ("contact_pair_friction", _dp),
     ]
 
 

@@ -386,7 +386,25 @@ struct NarrowIn {
     const double* wv;                 // world vertices at the tested pose
     const double* pose_p;             // body positions at the tested pose [N*3]
     const double* dhat_ptr;
+    const unsigned long long* allowed;  // sorted (lo world index << 32 | hi) keys of the allowed
+    int n_allowed;                      // contact pairs; 0: every pair is allowed
 };
+
+__device__ __forceinline__ unsigned long long body_pair_key(int a, int b) {
+    const int lo = a < b ? a : b, hi = a < b ? b : a;
+    return ((unsigned long long)(unsigned)lo << 32) | (unsigned)hi;
+}
+// IPCSolver::isContactPairAllowed (IPCSolver.cpp:283-289) by binary search
+__device__ __forceinline__ int allowed_index(const unsigned long long* keys, int n, int a, int b) {
+    const unsigned long long k = body_pair_key(a, b);
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (keys[mid] < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < n && keys[lo] == k ? lo : -1;
+}
 
 // kind 0 = FV, 1 = EE, 2 = VV; item t of pair p.  Returns hit and fills rec.
 __device__ bool narrow_item(const NarrowIn& in, int kind, int p, int t, ContactRec* rec) {
@@ -529,6 +547,11 @@ __device__ __forceinline__ void narrow_rows_body(const NarrowIn& in, int mode, c
     const int nwarps = gridDim.x * kRowsWarps;
     for (int p = blockIdx.x * kRowsWarps + (threadIdx.x >> 5); p < np; p += nwarps) {
         const int A = in.pairs[2 * p], B = in.pairs[2 * p + 1];
+        if (in.n_allowed > 0 && allowed_index(in.allowed, in.n_allowed, A, B) < 0) {
+            // detectContacts drops every contact of a pair that is not allowed
+            if (lane == 0) { s.cnt[p] = 0; if (mode == 0) s.cnt[in.cap + p] = 0; }
+            continue;
+        }
         const int* T = in.topk + (size_t)p * 6 * kTopK;
         const int* n = in.topn + 6 * p;
         const int n0 = n[0], n1 = n[1], n2 = n[2], n3 = n[3], n4 = n[4], n5 = n[5];

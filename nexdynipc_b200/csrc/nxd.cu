@@ -107,6 +107,11 @@ struct nxd_ctx {
     // solver scratch
     Solver S{};
     int cand_stride = 0;
+    // allowed contact pairs (sorted keys) and their friction overrides
+    unsigned long long* allowed_keys = nullptr;
+    double* allowed_mu = nullptr;
+    int n_allowed = 0;
+    bool has_mu_override = false;
     // when set, launches are recorded here (batched replay) instead of issued
     std::vector<LaunchRec>* rec = nullptr;
     // primitive-level (full IPC) model state, created on first use
@@ -167,9 +172,9 @@ void fill_solver(nxd_ctx* c) {
     S.contacts = c->contacts; S.ncontacts_ptr = &c->sc->n_contacts;
     S.nforce = c->nforce; S.nnf_ptr = &c->sc->nnf;
     S.cinc_off = m.alloc<int>(N + 1); S.cinc = m.alloc<int>(2 * C);
-    S.dt_ptr = &c->sc->dt; S.bdhat_ptr = &c->sc->bdhat; S.bkappa_ptr = &c->sc->bkappa;
+    S.dt_ptr = &c->sc->dt; S.scale_ptr = &c->sc->scale; S.bdhat_ptr = &c->sc->bdhat; S.bkappa_ptr = &c->sc->bkappa;
     S.barrier_in_forms_ptr = &c->sc->barrier_in_forms; S.friction_form_ptr = &c->sc->friction_form;
-    S.friction_mu = c->s.friction_coeff; S.friction_eps = 1e-8;
+    S.friction_mu_ptr = &c->sc->friction_mu; S.friction_eps = 1e-8;
     S.newton_max_iters = c->s.newton_max_iters; S.ls_max_iters = c->s.ls_max_iters;
     S.newton_tol = c->s.newton_tol; S.ls_c1 = c->s.ls_c1; S.ls_rho = c->s.ls_rho;
     S.alm_constraint_tol = c->s.alm_constraint_tol; S.alm_hardening_trigger = c->s.alm_hardening_trigger;
@@ -221,6 +226,9 @@ StepCfg step_cfg(const nxd_ctx* c) {
     k.alm_constraint_tol = c->s.alm_constraint_tol;
     k.alm_dual_tol = c->s.alm_dual_tol;
     k.alm_contact_tol = c->s.alm_contact_tol;
+    k.newmark = c->s.integrator == NXD_INTEGRATOR_IMPLICIT_NEWMARK ? 1 : 0;
+    k.beta = c->s.newmark_beta;
+    k.gamma = c->s.newmark_gamma;
     return k;
 }
 
@@ -275,7 +283,8 @@ namespace {
 // fallback when both found nothing, then the raw cap and the 2000 cap.
 // skip_if (device flag, may be null) skips the whole detection.
 void launch_narrow_full(nxd_ctx* c, const double* wv, const double* pose_p, const int* skip_if) {
-    NarrowIn in{c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap, c->topk, c->topn, wv, pose_p, &c->sc->dhat};
+    NarrowIn in{c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap, c->topk, c->topn, wv, pose_p, &c->sc->dhat,
+                c->allowed_keys, c->n_allowed};
     const NarrowScratch ns{c->hmask, c->hit_cnt, c->hit_off};
     const int rows_blocks = c->n_sm * 8, emit_blocks = c->n_sm * 2;
     int* skip_vv = c->i_scratch;
@@ -353,6 +362,10 @@ nxd_status enqueue_step(nxd_ctx* c, double dt) {
     const bool needs = c->s.enable_adaptive_barrier || (c->s.enable_friction && c->s.friction_coeff > 0.0);
     if (needs) launch_narrow_full(c, c->wv, c->pos, nullptr);
     else NXD_K(c, NXD_PROF_OTHER, contact_totals, (1), (1), (0), c->sc, 2, nullptr, nullptr);
+    // the friction form's coefficient with per-pair overrides, from the
+    // step-start contacts (IPCSolver.cpp:891-911)
+    if (c->has_mu_override && c->s.enable_friction && c->s.friction_coeff > 0.0)
+        NXD_K(c, NXD_PROF_OTHER, friction_mu, (1), (1), (0), cfg, c->sc, c->contacts, c->allowed_keys, c->allowed_mu, c->n_allowed);
     int* skip_detect = c->i_scratch + 1;
     for (int alm = 0; alm < c->s.alm_max_iters; ++alm) {
         launch_newton(c);
@@ -362,7 +375,7 @@ nxd_status enqueue_step(nxd_ctx* c, double dt) {
         launch_narrow_full(c, c->wvx, c->pose_p, skip_detect);
         NXD_K(c, NXD_PROF_ALM_POST, alm_post, (1), (kSolverThreads), (0), c->S, c->sc, cfg, c->nforce);
     }
-    NXD_K(c, NXD_PROF_OTHER, update_state, (grid_for(c->N, 128)), (128), (0), cfg, c->x, c->xprev, c->vprev, c->pos, c->quat, c->vel, c->omega,
+    NXD_K(c, NXD_PROF_OTHER, update_state, (grid_for(c->N, 128)), (128), (0), cfg, c->x, c->xprev, c->vprev, c->xhat, c->aprev, c->pos, c->quat, c->vel, c->omega,
                                                         c->lacc, c->aacc, c->sc, c->da, c->db, c->dprm, c->dfilt);
     if (c->D > 0) NXD_K(c, NXD_PROF_OTHER, drive_kpi, (1), (1), (0), cfg, c->omega, c->sc, c->da, c->db, c->dprm, c->dfilt);
     NXD_CUDA(cudaGetLastError());
@@ -401,6 +414,9 @@ void nxd_default_settings(nxd_settings* s) {
     s->newton_tol = 1e-6;
     s->ls_c1 = 1e-4;
     s->ls_rho = 0.5;
+    s->integrator = NXD_INTEGRATOR_IMPLICIT_EULER;
+    s->newmark_beta = 0.25;
+    s->newmark_gamma = 0.5;
 }
 
 const char* nxd_version(void) { return "nxd-b200 0.1 (sm_100a, FP64)"; }
@@ -516,6 +532,30 @@ nxd_status nxd_create(const nxd_scene_desc* d, nxd_ctx** out) {
     c->vbody = m.upload(vbody.data(), vbody.size());
     c->has_mesh = m.upload(has_mesh.data(), N);
     c->body_ids = m.upload(c->h_body_ids.data(), N);
+    // IPCSolver::addAllowedContactPair: keys of world-index pairs, sorted,
+    // with the last non-negative friction given for a pair as its override
+    if (d->n_contact_pairs > 0 && d->contact_pair_bodies) {
+        std::vector<std::pair<unsigned long long, double>> kv;
+        for (int q = 0; q < d->n_contact_pairs; ++q) {
+            const int a = idx_of(d->contact_pair_bodies[2 * q]), b = idx_of(d->contact_pair_bodies[2 * q + 1]);
+            if (a < 0 || b < 0) continue;
+            const int lo = std::min(a, b), hi = std::max(a, b);
+            const double f = d->contact_pair_friction ? d->contact_pair_friction[q] : -1.0;
+            kv.push_back({((unsigned long long)(unsigned)lo << 32) | (unsigned)hi, f});
+        }
+        std::stable_sort(kv.begin(), kv.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+        std::vector<unsigned long long> keys;
+        std::vector<double> mu;
+        for (const auto& e : kv) {
+            if (!keys.empty() && keys.back() == e.first) { if (e.second >= 0.0) mu.back() = e.second; continue; }
+            keys.push_back(e.first);
+            mu.push_back(e.second >= 0.0 ? e.second : -1.0);
+        }
+        for (double f : mu) c->has_mu_override = c->has_mu_override || f >= 0.0;
+        c->n_allowed = (int)keys.size();
+        c->allowed_keys = m.upload(keys.data(), keys.size());
+        c->allowed_mu = m.upload(mu.data(), mu.size());
+    }
     c->lmin = m.upload(lmin.data(), 3 * N);
     c->lmax = m.upload(lmax.data(), 3 * N);
     c->md_tol = m.alloc<double>(N);

@@ -64,9 +64,10 @@ struct Solver {
     const double* nforce; const int* nnf_ptr;
     int* cinc_off; int* cinc;                     // body -> contact*2+side, ascending; built per kernel
     // scalars
-    const double* dt_ptr; const double* bdhat_ptr; const double* bkappa_ptr;
+    const double* dt_ptr; const double* scale_ptr; const double* bdhat_ptr; const double* bkappa_ptr;
     const int* barrier_in_forms_ptr; const int* friction_form_ptr;
-    double friction_mu, friction_eps;
+    const double* friction_mu_ptr;                // FrictionForm coefficient of the step
+    double friction_eps;
     int newton_max_iters, ls_max_iters;
     double newton_tol, ls_c1, ls_rho;
     double alm_constraint_tol, alm_hardening_trigger, alm_hardening_ratio;
@@ -446,7 +447,7 @@ __device__ double friction_value(const Solver& S, int c, const double* x) {
     const V3 u = fric_tangent(S, cr, G, x, *S.dt_ptr);
     const double un = norm(u);
     const double sn = sqrt(un * un + S.friction_eps * S.friction_eps);
-    return S.friction_mu * N * (sn - S.friction_eps);
+    return *S.friction_mu_ptr * N * (sn - S.friction_eps);
 }
 __device__ void friction_eval(const Solver& S, int c, const double* x, bool full) {
     if (!friction_on(S, c)) { S.fE[c] = 0.0; return; }
@@ -456,7 +457,7 @@ __device__ void friction_eval(const Solver& S, int c, const double* x, bool full
     FricGeom G;
     fric_geom(S, cr, G);
     const V3 u = fric_tangent(S, cr, G, x, dt);
-    const double mu = S.friction_mu, eps = S.friction_eps;
+    const double mu = *S.friction_mu_ptr, eps = S.friction_eps;
     // FrictionPotential (Friction.cpp:5-61)
     const double un = norm(u);
     const double sn = sqrt(un * un + eps * eps);
@@ -1500,8 +1501,7 @@ __device__ __forceinline__ void newton_body(const Solver& S) {
     R.gc = &gc; R.sh = sh_red; R.part = S.gpart; R.parity = 0;
     const int N = S.N;
     const int C = *S.ncontacts_ptr;
-    const double dt = *S.dt_ptr;
-    const double s = dt * dt;
+    const double s = *S.scale_ptr;   // ImplicitTimeIntegrator::acceleration_scaling
     const int n6 = 6 * N;
     const bool bar = *S.barrier_in_forms_ptr != 0, fr = *S.friction_form_ptr != 0;
     const double dh = *S.bdhat_ptr;

@@ -14,6 +14,8 @@ struct Scalars {
     double dhat;            // AdaptiveBarrier::currentDhat
     double kappa;           // AdaptiveBarrier::currentStiffness
     double dt;              // step dt (computeMaxStep result)
+    double scale;           // ImplicitTimeIntegrator::acceleration_scaling
+    double friction_mu;     // FrictionForm coefficient of this step
     double bdhat, bkappa;   // DistanceBarrierForm parameters
     double bmd;             // estimateBroadPhaseMinDistance(2 dhat)
     double md;              // computeSceneMinDistance (pruned)
@@ -40,6 +42,8 @@ struct StepCfg {
     int enable_adaptive, enable_friction;
     double friction_coeff;
     double alm_constraint_tol, alm_dual_tol, alm_contact_tol;
+    int newmark;            // 1: ImplicitNewmark(beta, gamma), 0: ImplicitEuler
+    double beta, gamma;
 };
 
 // IPCSolver::initializeAdaptiveBarrier (IPCSolver.cpp:327-353) +
@@ -94,8 +98,12 @@ __device__ __forceinline__ void step_setup_body(const StepCfg& cfg, double dt, c
             pos0[3 * i + k] = p;
         }
         for (int k = 0; k < 4; ++k) quat0[4 * i + k] = quat[4 * i + k];
+        // x_tilde: ImplicitEuler (ImplicitEulerIntegrator.cpp:5-7) or
+        // ImplicitNewmark (ImplicitNewmark.cpp:8-10), Eigen's evaluation order
+        const double s1 = (dt * dt) * (0.5 - cfg.beta);
         for (int k = 0; k < 6; ++k) {
-            const double xh = xprev[6 * i + k] + dt * vprev[6 * i + k];
+            double xh = xprev[6 * i + k] + dt * vprev[6 * i + k];
+            if (cfg.newmark) xh = xh + s1 * aprev[6 * i + k];
             xhat[6 * i + k] = xh;
             x[6 * i + k] = xh;
         }
@@ -109,6 +117,8 @@ __device__ __forceinline__ void step_setup_body(const StepCfg& cfg, double dt, c
     }
     if (i == 0) {
         sc->dt = dt;
+        sc->scale = cfg.newmark ? (cfg.beta * dt) * dt : dt * dt;
+        sc->friction_mu = cfg.friction_coeff;
         const bool needs = cfg.enable_adaptive || (cfg.enable_friction && cfg.friction_coeff > 0.0);
         sc->barrier_form = needs ? 1 : 0;
         sc->barrier_in_forms = (cfg.enable_adaptive && needs) ? 1 : 0;
@@ -126,6 +136,28 @@ __device__ __forceinline__ void step_setup_body(const StepCfg& cfg, double dt, c
 }
 constexpr int kLB_step_setup = 0;
 __global__ void k_step_setup(const __grid_constant__ StepCfg cfg, double dt, const double* pos, const double* quat, const double* vel, const double* omega, const double* lacc, const double* aacc, double* x, double* xhat, double* xprev, double* vprev, double* aprev, double* pos0, double* quat0, Scalars* sc, const Drv* dprm, double* dfilt, int* dfinit, int* dhas_prev) { step_setup_body(cfg, dt, pos, quat, vel, omega, lacc, aacc, x, xhat, xprev, vprev, aprev, pos0, quat0, sc, dprm, dfilt, dfinit, dhas_prev); }
+
+// Friction coefficient of the step with per-pair overrides
+// (IPCSolver.cpp:891-911): the mean over the active contacts of each
+// contact's pair override, else the global coefficient, summed in contact
+// order.  Runs only when overrides exist.
+__device__ __forceinline__ void friction_mu_body(const StepCfg& cfg, Scalars* sc, const ContactRec* contacts,
+                                                 const unsigned long long* keys, const double* mu, int n_keys) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int n = sc->n_contacts;
+    if (n <= 0) { sc->friction_mu = cfg.friction_coeff; return; }
+    double sum = 0.0;
+    for (int c = 0; c < n; ++c) {
+        const int k = allowed_index(keys, n_keys, contacts[c].body_a, contacts[c].body_b);
+        sum += (k >= 0 && mu[k] >= 0.0) ? mu[k] : cfg.friction_coeff;
+    }
+    sc->friction_mu = sum / (double)n;
+}
+constexpr int kLB_friction_mu = 0;
+__global__ void k_friction_mu(const __grid_constant__ StepCfg cfg, Scalars* sc, const ContactRec* contacts,
+                              const unsigned long long* keys, const double* mu, int n_keys) {
+    friction_mu_body(cfg, sc, contacts, keys, mu, n_keys);
+}
 
 // Contact totals after FV + EE (+VV) passes; gates the VV fallback.
 // stage 2 clears the counts (no detection this step).
@@ -252,15 +284,22 @@ __device__ __forceinline__ void alm_post_body(const Solver& S, Scalars* sc, cons
 constexpr int kLB_alm_post = kSolverThreads;
 __global__ void __launch_bounds__(kSolverThreads) k_alm_post(const __grid_constant__ Solver S, Scalars* sc, const __grid_constant__ StepCfg cfg, double* nforce_out) { alm_post_body(S, sc, cfg, nforce_out); }
 
-// ImplicitEuler::update_quantities + write-back (IPCSolver.cpp:1168-1195)
-// and the velocity-drive KPIs (IPCSolver.cpp:1197-1215).
-__device__ __forceinline__ void update_state_body(const StepCfg& cfg, const double* x, const double* xprev, const double* vprev, double* pos, double* quat, double* vel, double* omega, double* lacc, double* aacc, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt) {
+// update_quantities (ImplicitEulerIntegrator.cpp:13-25 or ImplicitNewmark.cpp:16-30)
+// + write-back (IPCSolver.cpp:1168-1195).
+__device__ __forceinline__ void update_state_body(const StepCfg& cfg, const double* x, const double* xprev, const double* vprev, const double* xhat, const double* aprev, double* pos, double* quat, double* vel, double* omega, double* lacc, double* aacc, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const double dt = sc->dt;
     if (i < cfg.N) {
         double vn[6], an[6];
-        for (int k = 0; k < 6; ++k) vn[k] = (x[6 * i + k] - xprev[6 * i + k]) / dt;
-        for (int k = 0; k < 6; ++k) an[k] = (vn[k] - vprev[6 * i + k]) / dt;
+        if (cfg.newmark) {
+            const double den = (cfg.beta * dt) * dt;
+            for (int k = 0; k < 6; ++k) an[k] = (x[6 * i + k] - xhat[6 * i + k]) / den;
+            for (int k = 0; k < 6; ++k)
+                vn[k] = vprev[6 * i + k] + dt * ((1.0 - cfg.gamma) * aprev[6 * i + k] + cfg.gamma * an[k]);
+        } else {
+            for (int k = 0; k < 6; ++k) vn[k] = (x[6 * i + k] - xprev[6 * i + k]) / dt;
+            for (int k = 0; k < 6; ++k) an[k] = (vn[k] - vprev[6 * i + k]) / dt;
+        }
         for (int k = 0; k < 3; ++k) {
             lacc[3 * i + k] = an[k]; aacc[3 * i + k] = an[3 + k];
             vel[3 * i + k] = vn[k]; omega[3 * i + k] = vn[3 + k];
@@ -270,7 +309,7 @@ __device__ __forceinline__ void update_state_body(const StepCfg& cfg, const doub
     }
 }
 constexpr int kLB_update_state = 0;
-__global__ void k_update_state(const __grid_constant__ StepCfg cfg, const double* x, const double* xprev, const double* vprev, double* pos, double* quat, double* vel, double* omega, double* lacc, double* aacc, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt) { update_state_body(cfg, x, xprev, vprev, pos, quat, vel, omega, lacc, aacc, sc, da, db, dprm, dfilt); }
+__global__ void k_update_state(const __grid_constant__ StepCfg cfg, const double* x, const double* xprev, const double* vprev, const double* xhat, const double* aprev, double* pos, double* quat, double* vel, double* omega, double* lacc, double* aacc, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt) { update_state_body(cfg, x, xprev, vprev, xhat, aprev, pos, quat, vel, omega, lacc, aacc, sc, da, db, dprm, dfilt); }
 
 __device__ __forceinline__ void drive_kpi_body(const StepCfg& cfg, const double* omega, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt) {
     double max_vw = 0.0;
@@ -323,7 +362,7 @@ __global__ void __launch_bounds__(kSolverThreads) k_form_eval(Solver S, Scalars*
     NX_BLOCK_RED(R);
     const int N = S.N;
     const int C = sc->n_contacts;
-    const double s = sc->dt * sc->dt;
+    const double s = sc->scale;
     if (what == 0 && (form == NXD_FORM_TOTAL || form == NXD_FORM_CONTACT)) {
         const double v = energy_total(S, x, s, C, form == NXD_FORM_CONTACT, R);
         if (threadIdx.x == 0) out[0] = v;
@@ -481,6 +520,8 @@ __global__ void k_set_form_state(StepCfg cfg, Scalars* sc, int n, int nnf, doubl
         sc->n_contacts = n;
         sc->nnf = nnf;
         sc->dt = dt;
+        sc->scale = cfg.newmark ? (cfg.beta * dt) * dt : dt * dt;
+        sc->friction_mu = cfg.friction_coeff;
         sc->bdhat = dmax(1e-9, sc->dhat);
         sc->bkappa = dmax(0.0, sc->kappa);
         sc->barrier_form = 1;

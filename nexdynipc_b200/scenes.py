@@ -181,6 +181,10 @@ class Scene:
     settings: abi.NxdSettings
     dt: float
     steps: int
+    body_ids: np.ndarray = None                 # RigidBody::id per body (default: the world index)
+    body_names: list = None
+    contact_pairs: np.ndarray = None            # [n, 2] body ids (IPCSolver::addAllowedContactPair)
+    contact_pair_friction: np.ndarray = None    # [n], < 0: no override
 
     @property
     def n_bodies(self) -> int:
@@ -196,7 +200,8 @@ class Scene:
 
     def desc(self) -> abi.NxdSceneDesc:
         """NxdSceneDesc viewing this scene's arrays (keep the Scene alive)."""
-        self._ids = np.arange(self.n_bodies, dtype=np.int32)
+        self._ids = (np.arange(self.n_bodies, dtype=np.int32) if self.body_ids is None
+                     else np.ascontiguousarray(self.body_ids, dtype=np.int32))
         self._zeros3 = np.zeros((self.n_bodies, 3))
         d = abi.NxdSceneDesc()
         d.n_bodies = self.n_bodies
@@ -224,6 +229,14 @@ class Scene:
         d.drive_body_b = abi.iptr(self.drive_body_b)
         d.drive_params = abi.dptr(self.drive_params)
         d.settings = self.settings
+        if self.contact_pairs is not None and len(self.contact_pairs):
+            self._cp = np.ascontiguousarray(self.contact_pairs, dtype=np.int32).reshape(-1, 2)
+            fr = (np.full(len(self._cp), -1.0) if self.contact_pair_friction is None
+                  else self.contact_pair_friction)
+            self._cpf = np.ascontiguousarray(fr, dtype=np.float64)
+            d.n_contact_pairs = len(self._cp)
+            d.contact_pair_bodies = abi.iptr(self._cp)
+            d.contact_pair_friction = abi.dptr(self._cpf)
         return d
 
     def initial_state(self) -> dict:

@@ -350,6 +350,17 @@ struct nxo_world {
     std::vector<double> normal_forces;
     bool barrier_form = false, friction_form = false, barrier_in_forms = false;
     double barrier_dhat = 1e-3, barrier_kappa = 0.0, friction_mu = 0.0, friction_eps = 1e-8, friction_dt = 0.01;
+    // IPCSolver::allowed_contact_pair_keys_ / pair_friction_overrides_ (by body id)
+    std::unordered_set<std::uint64_t> allowed_pairs;
+    std::unordered_map<std::uint64_t, double> pair_friction;
+    bool pair_allowed(int id_a, int id_b) const {
+        if (allowed_pairs.empty()) return true;
+        return allowed_pairs.count(pair_key(id_a, id_b)) != 0;
+    }
+    static std::uint64_t pair_key(int a, int b) {   // IPCSolver::makePairKey (IPCSolver.cpp:268-273)
+        const int lo = std::min(a, b), hi = std::max(a, b);
+        return ((std::uint64_t)(std::uint32_t)lo << 32) | (std::uint32_t)hi;
+    }
     std::vector<double> x_hat;
     double dt = 0.01;               // integrator dt
     std::vector<double> x_prev, v_prev, a_prev;
@@ -893,6 +904,7 @@ std::vector<Contact> detect_contacts(nxo_world* w, const std::vector<double>* x,
     auto finish = [&](const Raw& r, std::vector<Contact>& out) {
         auto ait = id2i.find(r.a), bit = id2i.find(r.b);
         if (ait == id2i.end() || bit == id2i.end()) return;
+        if (!w->pair_allowed(r.a, r.b)) return;   // IPCSolver.cpp:448, 668
         V3 pa, pb; Q qa, qb;
         pose(ait->second, pa, qa); pose(bit->second, pb, qb);
         V3 n = safe_normalized(r.normal, pb - pa);
@@ -1518,7 +1530,12 @@ double drives_value(nxo_world* w, const std::vector<double>& x) {
     return tree_sum(ev);
 }
 
-double scaling(nxo_world* w) { return w->dt * w->dt; }   // ImplicitEuler::acceleration_scaling
+// acceleration_scaling: ImplicitEuler dt^2 (ImplicitEulerIntegrator.cpp:9-11),
+// ImplicitNewmark beta dt^2 (ImplicitNewmark.cpp:12-14)
+double scaling(nxo_world* w) {
+    if (w->s.integrator == NXD_INTEGRATOR_IMPLICIT_NEWMARK) return (w->s.newmark_beta * w->dt) * w->dt;
+    return w->dt * w->dt;
+}
 
 double problem_value(nxo_world* w, const std::vector<double>& x) {
     double v = inertia_value(w, x);
@@ -1823,10 +1840,16 @@ void step(nxo_world* w, double dt) {
             a[i * 6 + k] = b.linear_acceleration[k]; a[i * 6 + 3 + k] = b.angular_acceleration[k];
         }
     }
-    // ImplicitTimeIntegrator::init + ImplicitEuler::x_tilde
+    // ImplicitTimeIntegrator::init + x_tilde (ImplicitEulerIntegrator.cpp:5-7,
+    // ImplicitNewmark.cpp:8-10)
     w->x_prev = x; w->v_prev = v; w->a_prev = a; w->dt = actual_dt;
+    const bool newmark = s.integrator == NXD_INTEGRATOR_IMPLICIT_NEWMARK;
+    const double nm_s1 = (actual_dt * actual_dt) * (0.5 - s.newmark_beta);
     std::vector<double> x_hat(n);
-    for (int i = 0; i < n; ++i) x_hat[i] = x[i] + actual_dt * v[i];
+    for (int i = 0; i < n; ++i) {
+        x_hat[i] = x[i] + actual_dt * v[i];
+        if (newmark) x_hat[i] = x_hat[i] + nm_s1 * a[i];
+    }
     std::vector<double> x_new = x_hat;
     w->x_hat = x_hat;
 
@@ -1849,7 +1872,19 @@ void step(nxo_world* w, double dt) {
     if (s.enable_adaptive_barrier && w->barrier_form) w->barrier_in_forms = true;
     if (s.enable_friction && s.friction_coeff > 0) {
         w->friction_form = true;
-        w->friction_mu = s.friction_coeff;   // no per-pair overrides
+        // effective coefficient with per-pair overrides (IPCSolver.cpp:891-911)
+        double mu = s.friction_coeff;
+        if (!active.empty() && !w->pair_friction.empty()) {
+            double sum = 0.0;
+            int cnt = 0;
+            for (const Contact& c : active) {
+                auto it = w->pair_friction.find(nxo_world::pair_key(w->bodies[c.bodyA].id, w->bodies[c.bodyB].id));
+                sum += it != w->pair_friction.end() ? it->second : s.friction_coeff;
+                ++cnt;
+            }
+            if (cnt > 0) mu = sum / (double)cnt;
+        }
+        w->friction_mu = mu;
         w->friction_eps = 1e-8;
         w->friction_dt = std::max(0.0, actual_dt);
         w->friction_contacts = active;
@@ -1945,10 +1980,18 @@ void step(nxo_world* w, double dt) {
     w->diag.newton_converged = conv_last ? 1 : 0;
     const double t5 = now_s();
 
-    // ImplicitEuler::update_quantities + write-back (IPCSolver.cpp:1168-1195)
+    // update_quantities (ImplicitEulerIntegrator.cpp:13-25, ImplicitNewmark.cpp:16-30)
+    // + write-back (IPCSolver.cpp:1168-1195)
     std::vector<double> vn(n), an(n);
-    for (int i = 0; i < n; ++i) vn[i] = (x_new[i] - w->x_prev[i]) / actual_dt;
-    for (int i = 0; i < n; ++i) an[i] = (vn[i] - w->v_prev[i]) / actual_dt;
+    if (newmark) {
+        const double den = (s.newmark_beta * actual_dt) * actual_dt;
+        for (int i = 0; i < n; ++i) an[i] = (x_new[i] - w->x_hat[i]) / den;
+        for (int i = 0; i < n; ++i)
+            vn[i] = w->v_prev[i] + actual_dt * ((1.0 - s.newmark_gamma) * w->a_prev[i] + s.newmark_gamma * an[i]);
+    } else {
+        for (int i = 0; i < n; ++i) vn[i] = (x_new[i] - w->x_prev[i]) / actual_dt;
+        for (int i = 0; i < n; ++i) an[i] = (vn[i] - w->v_prev[i]) / actual_dt;
+    }
     for (int i = 0; i < N; ++i) {
         Body& b = w->bodies[i];
         const int idx = i * 6;
@@ -1999,6 +2042,13 @@ nxo_world* nxo_create(const nxd_scene_desc* d) {
     auto* w = new nxo_world();
     w->s = d->settings;
     const int N = d->n_bodies;
+    // IPCSolver::addAllowedContactPair (IPCSolver.cpp:275-281)
+    for (int q = 0; d->contact_pair_bodies && q < d->n_contact_pairs; ++q) {
+        const auto key = nxo_world::pair_key(d->contact_pair_bodies[2 * q], d->contact_pair_bodies[2 * q + 1]);
+        w->allowed_pairs.insert(key);
+        const double f = d->contact_pair_friction ? d->contact_pair_friction[q] : -1.0;
+        if (f >= 0.0) w->pair_friction[key] = f;
+    }
     w->bodies.resize(N);
     w->meshes.resize(N);
     for (int i = 0; i < N; ++i) {

@@ -39,7 +39,7 @@ def test_version_and_default_settings():
 def test_struct_sizes():
     assert C.sizeof(abi.NxdContact) == 80
     assert C.sizeof(abi.NxdCandidates) == 96
-    assert C.sizeof(abi.NxdSettings) == 120
+    assert C.sizeof(abi.NxdSettings) == 144
 
 
 def test_create_without_device_reports_no_device():

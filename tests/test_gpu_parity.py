@@ -243,6 +243,15 @@ def test_trajectory_double_pendulum_meshless():
     assert wp <= 1e-6 and wr <= 1e-6, (wp, wr)
 
 
+def test_trajectory_newmark():
+    # the reference's Simulation default integrator (ImplicitNewmark, beta
+    # 0.25, gamma 0.5) on the double pendulum and the cube stack
+    for sc, steps in ((double_pendulum(), 100), (scenes.cube_stack(), 50)):
+        sc.settings.integrator = abi.INTEGRATOR_IMPLICIT_NEWMARK
+        wp, wr, _ = run_pair(sc, steps, check_every=10)
+        assert wp <= 1e-6 and wr <= 1e-6, (sc.name, wp, wr)
+
+
 def test_batch_matches_single_scenes():
     # batched launches (one launch per kernel for all scenes of a group)
     # against the same scenes stepped one context at a time: identical bits;
@@ -266,3 +275,40 @@ def test_batch_matches_single_scenes():
         assert b.diagnostics(i)["status"] == 0
         assert np.abs(sg["position"] - so["position"]).max() <= 1e-6
         assert quat_angle(sg["orientation"], so["orientation"]).max() <= 1e-6
+
+
+def test_scene_file_fixture():
+    # a scene file in the reference's schema (Newmark, allowed contact pairs
+    # with friction overrides, hinge + angle limit + velocity drive)
+    import os
+    from nexdynipc_b200 import sceneio
+    fixture = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "scene_contact_hinge.json")
+    sc, cfg = sceneio.load_scene(fixture)
+    ctx = runtime().Context(sc)
+    ow = refcpu.OracleWorld(sc)
+    cg = ctx.detect_contacts()
+    co, _ = ow.detect_contacts()
+    assert len(cg) > 0
+    contacts_equal(cg, co)
+    wp, wr, _ = run_pair(sc, 20, check_every=5)
+    assert wp <= 1e-6 and wr <= 1e-6, (wp, wr)
+    # a pair list without Ground-Cube drops those contacts on the device too
+    sc2, _ = sceneio.load_scene(fixture)
+    sc2.contact_pairs = np.array([[11, 13]], dtype=np.int32)
+    sc2.contact_pair_friction = np.array([0.6])
+    assert len(runtime().Context(sc2).detect_contacts()) == 0
+
+
+def test_scene_file_run_writes_reference_csv(tmp_path):
+    import os
+    from nexdynipc_b200 import sceneio
+    fixture = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "scene_contact_hinge.json")
+    sc, cfg, out = sceneio.run(fixture, output_dir=str(tmp_path))
+    d = sceneio.read_state_csv(out.path)
+    frames = int(d["frame_idx"].max())
+    assert frames == 20                                   # t < 0.1 with dt 0.005
+    ow = refcpu.OracleWorld(sc)
+    for _ in range(frames):
+        ow.step(cfg.dt)
+    last = d["frame_idx"] == frames
+    assert np.abs(d["pos_y"][last] - ow.state()["position"][:, 1]).max() <= 1e-6

@@ -282,3 +282,32 @@ def test_literal_and_pruned_min_distance_agree_below_band():
     pr = w.scene_min_distance(False)
     assert lit == pr
     assert lit < 1e-9
+
+
+def test_newmark_free_fall_recurrence():
+    # ImplicitNewmark (TimeIntegration/ImplicitNewmark.cpp): for a free body
+    # the Newton solve gives x' = x_tilde + beta h^2 g, so a' = g and
+    # v' = v + h ((1 - gamma) a + gamma a'), with a_0 = 0 as the scene starts.
+    from nexdynipc_b200 import abi, scenes
+    sb = scenes.SceneBuilder("free_fall")
+    sb.add_body(np.zeros((0, 3)), np.zeros((0, 3), np.int32), (0.0, 2.0, 0.0), mass=2.0, inertia=np.eye(3),
+                vel=(0.3, 1.0, 0.0))
+    s = abi.default_settings()
+    s.integrator = abi.INTEGRATOR_IMPLICIT_NEWMARK
+    s.newmark_beta, s.newmark_gamma = 0.25, 0.5
+    h = 0.01
+    sc = sb.build(s, h, 50)
+    ow = refcpu.OracleWorld(sc)
+    g = np.array([0.0, -9.81, 0.0])
+    p, v, a = np.array([0.0, 2.0, 0.0]), np.array([0.3, 1.0, 0.0]), np.zeros(3)
+    for _ in range(50):
+        ow.step()
+        xt = p + h * v + h * h * (0.5 - 0.25) * a
+        p_new = xt + 0.25 * h * h * g
+        a_new = (p_new - xt) / (0.25 * h * h)
+        v = v + h * (0.5 * a + 0.5 * a_new)
+        p, a = p_new, a_new
+    st = ow.state()
+    assert np.allclose(st["position"][0], p, rtol=0, atol=1e-10)
+    assert np.allclose(st["velocity"][0], v, rtol=0, atol=1e-8)
+    assert np.allclose(st["linear_acceleration"][0], g, rtol=0, atol=1e-5)
