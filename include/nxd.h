@@ -48,7 +48,10 @@ enum {
     NXD_JOINT_HINGE = 0,        /* HingeJoint       (Joints/HingeJoint.cpp)       */
     NXD_JOINT_FIXED = 1,        /* FixedJoint       (Joints/FixedJoint.cpp)       */
     NXD_JOINT_SPHERICAL = 2,    /* SphericalJoint   (Joints/SphericalJoint.cpp)   */
-    NXD_JOINT_ANGLE_LIMIT = 3   /* AngleLimitJoint  (Joints/AngleLimitJoint.cpp)  */
+    NXD_JOINT_ANGLE_LIMIT = 3,  /* AngleLimitJoint  (Joints/AngleLimitJoint.cpp)  */
+    NXD_JOINT_PRISMATIC = 4,    /* PrismaticJoint   (Joints/PrismaticJoint.cpp)   */
+    NXD_JOINT_CYLINDRICAL = 5,  /* CylindricalJoint (Joints/CylindricalJoint.cpp) */
+    NXD_JOINT_DISTANCE_LIMIT = 6 /* DistanceLimitJoint (Joints/DistanceLimitJoint.cpp) */
 };
 #define NXD_JOINT_PARAMS 16
 
@@ -57,6 +60,8 @@ enum {
  *   fixed:       target_position[3] target_orientation[4] (w,x,y,z) (FixedJoint ctor)
  *   spherical:   anchorA[3] anchorB[3]                        (SphericalJoint ctor)
  *   angle limit: axis[3] min_angle_rad max_angle_rad          (AngleLimitJoint ctor)
+ *   prismatic, cylindrical: anchorA[3] anchorB[3] axisA[3] axisB[3] (ctors)
+ *   distance limit: min_distance max_distance                 (DistanceLimitJoint ctor)
  */
 
 #define NXD_DRIVE_PARAMS 8

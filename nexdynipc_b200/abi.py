@@ -13,6 +13,9 @@ NXD_JOINT_HINGE = 0
 NXD_JOINT_FIXED = 1
 NXD_JOINT_SPHERICAL = 2
 NXD_JOINT_ANGLE_LIMIT = 3
+NXD_JOINT_PRISMATIC = 4
+NXD_JOINT_CYLINDRICAL = 5
+NXD_JOINT_DISTANCE_LIMIT = 6
 NXD_JOINT_PARAMS = 16
 NXD_DRIVE_PARAMS = 8
 

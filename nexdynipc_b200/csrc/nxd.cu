@@ -488,7 +488,7 @@ nxd_status nxd_create(const nxd_scene_desc* d, nxd_ctx** out) {
         jtype[j] = d->joint_type[j];
         ja[j] = idx_of(d->joint_body_a[j]);
         jb[j] = jtype[j] == NXD_JOINT_FIXED ? -1 : idx_of(d->joint_body_b[j]);
-        if (ja[j] < 0 || (jtype[j] != NXD_JOINT_FIXED && jb[j] < 0) || jtype[j] < 0 || jtype[j] > 3) {
+        if (ja[j] < 0 || (jtype[j] != NXD_JOINT_FIXED && jb[j] < 0) || jtype[j] < 0 || jtype[j] > NXD_JOINT_DISTANCE_LIMIT) {
             c->mem.release(); delete c; return NXD_INVALID_ARGUMENT;
         }
         for (int k = 0; k < 16; ++k) jparams[16 * j + k] = d->joint_params[16 * j + k];

@@ -280,7 +280,20 @@ __device__ int warp_scan_excl(int* a, int n) {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ V3 xs3(const double* x, int i) { return ld3(x + i); }
 __device__ __forceinline__ int joint_dim(int t) {
-    return t == NXD_JOINT_HINGE || t == NXD_JOINT_FIXED ? 6 : (t == NXD_JOINT_SPHERICAL ? 3 : 2);
+    if (t == NXD_JOINT_HINGE || t == NXD_JOINT_FIXED) return 6;
+    if (t == NXD_JOINT_PRISMATIC) return 5;
+    if (t == NXD_JOINT_CYLINDRICAL) return 4;
+    return t == NXD_JOINT_SPHERICAL ? 3 : 2;
+}
+// inequality joints: value max(C, 0), projected multipliers, active-set Hessian
+__device__ __forceinline__ bool joint_is_limit(int t) { return t == NXD_JOINT_ANGLE_LIMIT || t == NXD_JOINT_DISTANCE_LIMIT; }
+
+// JointPrimitives::computeBasis (JointPrimitives.h:29-37) of an axis that the
+// joint's constructor has already normalised
+__device__ __forceinline__ void joint_basis(V3 axis, V3& u, V3& v) {
+    const V3 a = normalized(axis);
+    u = fabs(a.x) < 0.8 ? normalized(cross(a, v3(1, 0, 0))) : normalized(cross(a, v3(0, 1, 0)));
+    v = normalized(cross(a, u));
 }
 
 // Joint residual C at x; with Jd != null also the Jacobian (6 x 12 row-major:
@@ -334,6 +347,60 @@ __device__ int joint_residual(const Solver& S, int j, const double* x, double* C
         if (Jd) for (int i = 0; i < 6; ++i) Jd[12 * i + i] = 1.0;
         return 6;
     }
+    if (t == NXD_JOINT_PRISMATIC || t == NXD_JOINT_CYLINDRICAL) {
+        // PrismaticJoint / CylindricalJoint::computeC, computeJ (PrismaticJoint.cpp:30-66,
+        // CylindricalJoint.cpp:30-62) from PointOnAxis, Direction and RollLock
+        // primitives (JointPrimitives.h:111-265)
+        const V3 axA = normalized(ld3(P + 6)), axB = normalized(ld3(P + 9));
+        V3 uA, vA, uB, vB;
+        joint_basis(axA, uA, vA);
+        joint_basis(axB, uB, vB);
+        const V3 pA = xs3(x, 6 * A), pB = xs3(x, 6 * B);
+        const Q qA = ldq(S.qj + 4 * A), qB = ldq(S.qj + 4 * B);
+        const V3 rA = qrot(qA, ld3(P)), rB = qrot(qB, ld3(P + 3));
+        const V3 d = (pB + rB) - (pA + rA);
+        const V3 uAw = qrot(qA, uA), vAw = qrot(qA, vA);
+        C[0] = dot(d, uAw); C[1] = dot(d, vAw);
+        const V3 nA = qrot(qA, axA), uBw = qrot(qB, uB), vBw = qrot(qB, vB);
+        C[2] = dot(nA, uBw); C[3] = dot(nA, vBw);
+        if (Jd) {
+            const V3 dirs[2] = {uAw, vAw};
+            for (int r = 0; r < 2; ++r) {
+                const V3 dir = dirs[r];
+                const V3 gA = cross(dir, rA) + cross(dir, d), gB = cross(rB, dir);
+                for (int k = 0; k < 3; ++k) {
+                    Jd[12 * r + k] = -get(dir, k); Jd[12 * r + 3 + k] = get(gA, k);
+                    Jd[12 * r + 6 + k] = get(dir, k); Jd[12 * r + 9 + k] = get(gB, k);
+                }
+            }
+            const V3 bdirs[2] = {uBw, vBw};
+            for (int r = 0; r < 2; ++r) {
+                const V3 gA = cross(nA, bdirs[r]), gB = cross(bdirs[r], nA);
+                for (int k = 0; k < 3; ++k) { Jd[12 * (2 + r) + 3 + k] = get(gA, k); Jd[12 * (2 + r) + 9 + k] = get(gB, k); }
+            }
+        }
+        if (t == NXD_JOINT_CYLINDRICAL) return 4;
+        C[4] = dot(uAw, vBw);
+        if (Jd) {
+            const V3 gA = cross(uAw, vBw), gB = cross(vBw, uAw);
+            for (int k = 0; k < 3; ++k) { Jd[12 * 4 + 3 + k] = get(gA, k); Jd[12 * 4 + 9 + k] = get(gB, k); }
+        }
+        return 5;
+    }
+    if (t == NXD_JOINT_DISTANCE_LIMIT) {
+        // DistanceLimitJoint::computeC / computeJ (DistanceLimitJoint.cpp:38-89)
+        const V3 dd = xs3(x, 6 * B) - xs3(x, 6 * A);
+        const double dist = norm(dd);
+        const V3 dir = dist < 1e-12 ? v3(1, 0, 0) : dd / dist;
+        C[0] = P[0] - dist;
+        C[1] = dist - dmax(P[1], P[0]);
+        if (Jd)
+            for (int k = 0; k < 3; ++k) {
+                Jd[k] = get(dir, k); Jd[12 + k] = -get(dir, k);
+                Jd[6 + k] = -get(dir, k); Jd[12 + 6 + k] = get(dir, k);
+            }
+        return 2;
+    }
     // AngleLimitJoint (AngleLimitJoint.cpp:45-96)
     const Q qA = ldq(S.qj + 4 * A), qB = ldq(S.qj + 4 * B);
     const Q qr = qmul(qconj(qA), qB);
@@ -354,7 +421,7 @@ __device__ int joint_residual(const Solver& S, int j, const double* x, double* C
 __device__ double joint_energy(const Solver& S, int j, const double* C, int dim) {
     const double mu = S.jmu[j];
     const double* lam = S.jlam + 6 * j;
-    if (S.jtype[j] == NXD_JOINT_ANGLE_LIMIT) {
+    if (joint_is_limit(S.jtype[j])) {
         double e = 0.0;
         for (int i = 0; i < 2; ++i) { const double gp = dmax(C[i], 0.0); e += lam[i] * gp + 0.5 * mu * gp * gp; }
         return e;
@@ -375,7 +442,7 @@ __device__ void joint_eval(const Solver& S, int j, const double* x, bool full) {
     const double* lam = S.jlam + 6 * j;
     double* F = S.jF + 6 * j;
     for (int i = 0; i < 6; ++i) F[i] = 0.0;
-    if (S.jtype[j] == NXD_JOINT_ANGLE_LIMIT) {
+    if (joint_is_limit(S.jtype[j])) {
         for (int i = 0; i < 2; ++i) F[i] = C[i] > 0.0 ? lam[i] + mu * C[i] : 0.0;
         S.jact[j] = (C[0] > 0.0 ? 1 : 0) | (C[1] > 0.0 ? 2 : 0);
     } else {
@@ -386,7 +453,7 @@ __device__ void joint_eval(const Solver& S, int j, const double* x, bool full) {
 __device__ __forceinline__ bool joint_couples(const Solver& S, int j) {
     const int t = S.jtype[j];
     if (t == NXD_JOINT_FIXED) return false;
-    if (t == NXD_JOINT_ANGLE_LIMIT) return S.jact[j] != 0;
+    if (joint_is_limit(t)) return S.jact[j] != 0;
     return true;
 }
 
@@ -715,6 +782,16 @@ __device__ __forceinline__ double angle_limit_h(const Solver& S, int j, int a, i
         if (S.jact[j] & (1 << rep)) h += mu * (ax[a] * ax[b]);
     return h;
 }
+// entry (a, b) of the translational DistanceLimit block sum_active mu dir dir^T
+// (DistanceLimitJoint.cpp:113-160); dir is row 0 of the stored Jacobian
+__device__ __forceinline__ double distance_limit_h(const Solver& S, int j, int a, int b) {
+    const double* dir = S.jJ + 72 * j;
+    const double mu = S.jmu[j];
+    double h = 0.0;
+    for (int rep = 0; rep < 2; ++rep)
+        if (S.jact[j] & (1 << rep)) h += mu * (dir[a] * dir[b]);
+    return h;
+}
 __device__ void angle_limit_H(const Solver& S, int j, double* H3) {
     for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) H3[3 * a + b] = angle_limit_h(S, j, a, b);
 }
@@ -752,6 +829,9 @@ __device__ void diag_hessian_row(const Solver& S, double s, int i, int a, bool b
         if (S.jtype[j] == NXD_JOINT_ANGLE_LIMIT) {
             if (!S.jact[j]) continue;
             if (a >= 3) for (int b = 0; b < 3; ++b) H[3 + b] += angle_limit_h(S, j, a - 3, b);
+        } else if (S.jtype[j] == NXD_JOINT_DISTANCE_LIMIT) {
+            if (!S.jact[j]) continue;
+            if (a < 3) for (int b = 0; b < 3; ++b) H[b] += distance_limit_h(S, j, a, b);
         } else {
             joint_block_row(S, j, side, side, a, blk);
             for (int b = 0; b < 6; ++b) H[b] += blk[b];
@@ -798,6 +878,8 @@ __device__ double coupling_entry(const Solver& S, int it, int R, int Cb, double 
         const int j = it;
         if (S.jtype[j] == NXD_JOINT_ANGLE_LIMIT)
             return (ra >= 3 && cb >= 3) ? -angle_limit_h(S, j, ra - 3, cb - 3) : 0.0;
+        if (S.jtype[j] == NXD_JOINT_DISTANCE_LIMIT)
+            return (ra < 3 && cb < 3) ? -distance_limit_h(S, j, ra, cb) : 0.0;
         const int sr = S.ja[j] == R ? 0 : 1, sc = S.ja[j] == Cb ? 0 : 1;
         const int dim = joint_dim(S.jtype[j]);
         const double* Jd = S.jJ + 72 * j;
@@ -826,7 +908,8 @@ __device__ void add_coupling_block(const Solver& S, int it, int R, int Cb, doubl
     const int C = *S.ncontacts_ptr;
     for (int e = 0; e < 36; ++e) {
         const int ra = e / 6, cb = e % 6;
-        const bool touches = it < S.J ? (S.jtype[it] != NXD_JOINT_ANGLE_LIMIT || (ra >= 3 && cb >= 3))
+        const bool touches = it < S.J ? (S.jtype[it] == NXD_JOINT_ANGLE_LIMIT ? (ra >= 3 && cb >= 3)
+                                         : (S.jtype[it] == NXD_JOINT_DISTANCE_LIMIT ? (ra < 3 && cb < 3) : true))
                                       : (it < S.J + C ? (ra < 3 && cb < 3) : true);
         if (touches) out[e] += coupling_entry(S, it, R, Cb, s, C, e);
     }
@@ -1623,7 +1706,7 @@ __device__ __forceinline__ void newton_body(const Solver& S) {
             S.jmu[j] = mu;
         }
         double* lam = S.jlam + 6 * j;
-        if (S.jtype[j] == NXD_JOINT_ANGLE_LIMIT) for (int k = 0; k < dim; ++k) lam[k] = dmax(0.0, lam[k] + mu * Cj[k]);
+        if (joint_is_limit(S.jtype[j])) for (int k = 0; k < dim; ++k) lam[k] = dmax(0.0, lam[k] + mu * Cj[k]);
         else for (int k = 0; k < dim; ++k) lam[k] += mu * Cj[k];
     }
     mcv = R.max(mcv);

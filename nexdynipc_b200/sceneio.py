@@ -13,10 +13,10 @@
   KPIs) on the device.
 
 Joint and constraint kinds the device step implements: hinge (and its
-deprecated alias revolute), spherical, fixed, angle_limit,
-angular_velocity_drive.  Scenes using the others (prismatic, cylindrical,
-distance_limit(s), linear_velocity_drive, position_drive, force_drive,
-damped_spring) raise NotImplementedError naming them.
+deprecated alias revolute), spherical, prismatic, cylindrical, fixed,
+angle_limit, distance_limit(s), angular_velocity_drive.  Scenes using the
+others (linear_velocity_drive, position_drive, force_drive, damped_spring)
+raise NotImplementedError naming them.
 """
 from __future__ import annotations
 
@@ -30,9 +30,9 @@ import numpy as np
 from . import abi
 from .scenes import Scene
 
-_SUPPORTED = {"hinge", "revolute", "spherical", "fixed", "angle_limit", "angular_velocity_drive"}
-_KNOWN_UNSUPPORTED = {"prismatic", "cylindrical", "distance_limit", "distance_limits", "linear_velocity_drive",
-                      "position_drive", "force_drive", "damped_spring"}
+_SUPPORTED = {"hinge", "revolute", "spherical", "fixed", "angle_limit", "angular_velocity_drive", "prismatic",
+              "cylindrical", "distance_limit", "distance_limits"}
+_KNOWN_UNSUPPORTED = {"linear_velocity_drive", "position_drive", "force_drive", "damped_spring"}
 
 
 def load_obj(path: str):
@@ -173,6 +173,21 @@ def load_scene(path: str, dt: float | None = None):
             jt.append(abi.NXD_JOINT_HINGE if t == "hinge" else abi.NXD_JOINT_SPHERICAL)
             ja.append(int(entry["body_a"])); jb.append(int(entry["body_b"]))
             js.append(float(entry.get("stiffness", 1e8)))
+        elif t in ("prismatic", "cylindrical"):
+            p[0:3], p[3:6] = _vec(entry["anchor_a"]), _vec(entry["anchor_b"])
+            p[6:9], p[9:12] = _vec(entry["axis_a"]), _vec(entry["axis_b"])
+            jt.append(abi.NXD_JOINT_PRISMATIC if t == "prismatic" else abi.NXD_JOINT_CYLINDRICAL)
+            ja.append(int(entry["body_a"])); jb.append(int(entry["body_b"]))
+            js.append(float(entry.get("stiffness", 1e8)))
+        elif t in ("distance_limit", "distance_limits"):
+            a, b2 = int(entry.get("body_a", -1)), int(entry.get("body_b", -1))
+            if a not in index or b2 not in index:
+                continue
+            mn = float(entry.get("min_distance_m", entry.get("min_translation_m", 0.0)))
+            mx = float(entry.get("max_distance_m", entry.get("max_translation_m", mn)))
+            p[0], p[1] = mn, mx
+            jt.append(abi.NXD_JOINT_DISTANCE_LIMIT); ja.append(a); jb.append(b2)
+            js.append(float(entry.get("stiffness", 1e5)))
         elif t == "fixed":
             p[0:3] = _vec(entry["position"])
             o = entry.get("orientation")

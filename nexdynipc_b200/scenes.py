@@ -290,6 +290,21 @@ class SceneBuilder:
         p[3], p[4] = lo, hi
         self.joints.append((abi.NXD_JOINT_ANGLE_LIMIT, a, b, p, stiffness))
 
+    def prismatic(self, a, b, anchor_a, anchor_b, axis_a, axis_b, stiffness=1e8):
+        p = np.zeros(16)
+        p[0:3], p[3:6], p[6:9], p[9:12] = anchor_a, anchor_b, axis_a, axis_b
+        self.joints.append((abi.NXD_JOINT_PRISMATIC, a, b, p, stiffness))
+
+    def cylindrical(self, a, b, anchor_a, anchor_b, axis_a, axis_b, stiffness=1e8):
+        p = np.zeros(16)
+        p[0:3], p[3:6], p[6:9], p[9:12] = anchor_a, anchor_b, axis_a, axis_b
+        self.joints.append((abi.NXD_JOINT_CYLINDRICAL, a, b, p, stiffness))
+
+    def distance_limit(self, a, b, min_d, max_d, stiffness=1e5):
+        p = np.zeros(16)
+        p[0], p[1] = min_d, max_d
+        self.joints.append((abi.NXD_JOINT_DISTANCE_LIMIT, a, b, p, stiffness))
+
     def velocity_drive(self, a, b, axis, kv, v_target, max_torque=0.0, delay=0.0, delay_tau=0.0):
         p = np.zeros(8)
         p[0:3] = axis

@@ -294,7 +294,15 @@ struct Joint {
     // updateState
     int gA = -1, gB = -1;
     V3 pA_ref, pB_ref; Q qA_ref, qB_ref;
-    int dim() const { return type == NXD_JOINT_HINGE || type == NXD_JOINT_FIXED ? 6 : (type == NXD_JOINT_SPHERICAL ? 3 : 2); }
+    V3 uA, vA, uB, vB;                   // prismatic / cylindrical bases (computeBasis)
+    double min_dist = 0, max_dist = 0;   // distance limit
+    int dim() const {
+        if (type == NXD_JOINT_HINGE || type == NXD_JOINT_FIXED) return 6;
+        if (type == NXD_JOINT_PRISMATIC) return 5;
+        if (type == NXD_JOINT_CYLINDRICAL) return 4;
+        return type == NXD_JOINT_SPHERICAL ? 3 : 2;
+    }
+    bool is_limit() const { return type == NXD_JOINT_ANGLE_LIMIT || type == NXD_JOINT_DISTANCE_LIMIT; }
 };
 
 struct Drive {
@@ -1001,6 +1009,13 @@ inline M3 mat_mul(const M3& A, const M3& B) {
     return C;
 }
 
+// JointPrimitives::computeBasis (JointPrimitives.h:29-37)
+void compute_basis(V3 axis, V3& u, V3& v) {
+    const V3 a = normalized(axis);
+    u = std::abs(a.x) < 0.8 ? normalized(cross(a, mk(1, 0, 0))) : normalized(cross(a, mk(0, 1, 0)));
+    v = normalized(cross(a, u));
+}
+
 // C(x) per joint kind
 void joint_C(const Joint& J, const std::vector<double>& x, double* C) {
     switch (J.type) {
@@ -1032,6 +1047,30 @@ void joint_C(const Joint& J, const std::vector<double>& x, double* C) {
             const V3 tt = ax * ang;
             const V3 th = xseg(x, J.gA + 3);
             C[3] = th.x - tt.x; C[4] = th.y - tt.y; C[5] = th.z - tt.z;
+            break;
+        }
+        case NXD_JOINT_PRISMATIC:
+        case NXD_JOINT_CYLINDRICAL: {
+            const EvalBody A = eval_body(J.gA, J.pA_ref, J.qA_ref, x);
+            const EvalBody B = eval_body(J.gB, J.pB_ref, J.qB_ref, x);
+            // PointOnAxisPrimitive::value (JointPrimitives.h:117-124)
+            const V3 rA = qrot(A.q, J.anchorA), rB = qrot(B.q, J.anchorB);
+            const V3 d = (B.p + rB) - (A.p + rA);
+            const V3 uAw = qrot(A.q, J.uA), vAw = qrot(A.q, J.vA);
+            C[0] = dot(d, uAw); C[1] = dot(d, vAw);
+            // DirectionPrimitive::value (JointPrimitives.h:170-175)
+            const V3 nA = qrot(A.q, J.axisA), uBw = qrot(B.q, J.uB), vBw = qrot(B.q, J.vB);
+            C[2] = dot(nA, uBw); C[3] = dot(nA, vBw);
+            // RollLockPrimitive::value (JointPrimitives.h:245-249)
+            if (J.type == NXD_JOINT_PRISMATIC) C[4] = dot(uAw, vBw);
+            break;
+        }
+        case NXD_JOINT_DISTANCE_LIMIT: {
+            // DistanceLimitJoint::computeC (DistanceLimitJoint.cpp:49-58)
+            const V3 pA = J.gA >= 0 ? xseg(x, J.gA) : J.pA_ref, pB = J.gB >= 0 ? xseg(x, J.gB) : J.pB_ref;
+            const double dist = norm(pB - pA);
+            C[0] = J.min_dist - dist;
+            C[1] = dist - J.max_dist;
             break;
         }
         case NXD_JOINT_ANGLE_LIMIT: {
@@ -1110,6 +1149,52 @@ JacRows joint_J(const Joint& J, const std::vector<double>& x) {
             }
             break;
         }
+        case NXD_JOINT_PRISMATIC:
+        case NXD_JOINT_CYLINDRICAL: {
+            const EvalBody A = eval_body(J.gA, J.pA_ref, J.qA_ref, x);
+            const EvalBody B = eval_body(J.gB, J.pB_ref, J.qB_ref, x);
+            const V3 rA = qrot(A.q, J.anchorA), rB = qrot(B.q, J.anchorB);
+            const V3 d = (B.p + rB) - (A.p + rA);
+            const V3 uAw = qrot(A.q, J.uA), vAw = qrot(A.q, J.vA);
+            // PointOnAxisPrimitive::addJacobianRows (JointPrimitives.h:126-163)
+            const V3 dirs[2] = {uAw, vAw};
+            for (int r = 0; r < 2; ++r) {
+                const V3 dir = dirs[r];
+                if (J.gA >= 0) {
+                    for (int k = 0; k < 3; ++k) jac_add(t, r, J.gA + k, -dir[k]);
+                    const V3 gA = cross(dir, rA) + cross(dir, d);
+                    for (int k = 0; k < 3; ++k) jac_add(t, r, J.gA + 3 + k, gA[k]);
+                }
+                if (J.gB >= 0) {
+                    for (int k = 0; k < 3; ++k) jac_add(t, r, J.gB + k, dir[k]);
+                    const V3 gB = cross(rB, dir);
+                    for (int k = 0; k < 3; ++k) jac_add(t, r, J.gB + 3 + k, gB[k]);
+                }
+            }
+            // DirectionPrimitive::addJacobianRows (JointPrimitives.h:177-200)
+            const V3 nA = qrot(A.q, J.axisA), uBw = qrot(B.q, J.uB), vBw = qrot(B.q, J.vB);
+            const V3 bdirs[2] = {uBw, vBw};
+            for (int r = 0; r < 2; ++r) {
+                if (J.gA >= 0) { const V3 gA = cross(nA, bdirs[r]); for (int k = 0; k < 3; ++k) jac_add(t, 2 + r, J.gA + 3 + k, gA[k]); }
+                if (J.gB >= 0) { const V3 gB = cross(bdirs[r], nA); for (int k = 0; k < 3; ++k) jac_add(t, 2 + r, J.gB + 3 + k, gB[k]); }
+            }
+            // RollLockPrimitive::addJacobianRow (JointPrimitives.h:251-265)
+            if (J.type == NXD_JOINT_PRISMATIC) {
+                if (J.gA >= 0) { const V3 gA = cross(uAw, vBw); for (int k = 0; k < 3; ++k) jac_add(t, 4, J.gA + 3 + k, gA[k]); }
+                if (J.gB >= 0) { const V3 gB = cross(vBw, uAw); for (int k = 0; k < 3; ++k) jac_add(t, 4, J.gB + 3 + k, gB[k]); }
+            }
+            break;
+        }
+        case NXD_JOINT_DISTANCE_LIMIT: {
+            // DistanceLimitJoint::direction / computeJ (DistanceLimitJoint.cpp:37-47, 60-89)
+            const V3 pA = J.gA >= 0 ? xseg(x, J.gA) : J.pA_ref, pB = J.gB >= 0 ? xseg(x, J.gB) : J.pB_ref;
+            const V3 dd = pB - pA;
+            const double dist = norm(dd);
+            const V3 dir = dist < 1e-12 ? mk(1, 0, 0) : dd / dist;
+            if (J.gA >= 0) for (int k = 0; k < 3; ++k) { jac_add(t, 0, J.gA + k, dir[k]); jac_add(t, 1, J.gA + k, -dir[k]); }
+            if (J.gB >= 0) for (int k = 0; k < 3; ++k) { jac_add(t, 0, J.gB + k, -dir[k]); jac_add(t, 1, J.gB + k, dir[k]); }
+            break;
+        }
         case NXD_JOINT_ANGLE_LIMIT: {
             // AngleLimitJoint::computeJ (AngleLimitJoint.cpp:74-96)
             if (J.gA >= 0) for (int k = 0; k < 3; ++k) { jac_add(t, 0, J.gA + 3 + k, J.axis[k]); jac_add(t, 1, J.gA + 3 + k, -J.axis[k]); }
@@ -1129,8 +1214,8 @@ double joint_value(const Joint& J, const std::vector<double>& x) {
     double C[6];
     joint_C(J, x, C);
     const int d = J.dim();
-    if (J.type == NXD_JOINT_ANGLE_LIMIT) {
-        // AngleLimitJoint::value (AngleLimitJoint.cpp:98-109)
+    if (J.is_limit()) {
+        // AngleLimitJoint::value (AngleLimitJoint.cpp:98-109), DistanceLimitJoint::value (:91-100)
         double e = 0.0;
         for (int i = 0; i < d; ++i) { const double gp = std::max(C[i], 0.0); e += J.lambda[i] * gp + 0.5 * J.mu * gp * gp; }
         return e;
@@ -1145,7 +1230,7 @@ void joint_gradient(const Joint& J, const std::vector<double>& x, std::vector<do
     joint_C(J, x, C);
     const int d = J.dim();
     double f[6];
-    if (J.type == NXD_JOINT_ANGLE_LIMIT) {
+    if (J.is_limit()) {
         for (int i = 0; i < d; ++i) f[i] = C[i] > 0.0 ? J.lambda[i] + J.mu * C[i] : 0.0;
     } else {
         for (int i = 0; i < d; ++i) f[i] = J.mu * C[i] + J.lambda[i];
@@ -1179,6 +1264,29 @@ void joint_hessian(const Joint& J, const std::vector<double>& x, std::vector<Tri
             }
         return;
     }
+    if (J.type == NXD_JOINT_DISTANCE_LIMIT) {
+        // DistanceLimitJoint::hessian (DistanceLimitJoint.cpp:113-160)
+        double C[2];
+        joint_C(J, x, C);
+        const bool amin = C[0] > 0.0, amax = C[1] > 0.0;
+        if (!amin && !amax) return;
+        const V3 pA = J.gA >= 0 ? xseg(x, J.gA) : J.pA_ref, pB = J.gB >= 0 ? xseg(x, J.gB) : J.pB_ref;
+        const V3 dd = pB - pA;
+        const double dist = norm(dd);
+        const V3 dir = dist < 1e-12 ? mk(1, 0, 0) : dd / dist;
+        double H[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int rep = 0; rep < 2; ++rep)
+            if ((rep == 0 && amin) || (rep == 1 && amax))
+                for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) H[i][j] += J.mu * (dir[i] * dir[j]);
+        if (J.gA >= 0) for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) t.push_back({J.gA + i, J.gA + j, H[i][j]});
+        if (J.gB >= 0) for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) t.push_back({J.gB + i, J.gB + j, H[i][j]});
+        if (J.gA >= 0 && J.gB >= 0)
+            for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) {
+                t.push_back({J.gA + i, J.gB + j, -H[i][j]});
+                t.push_back({J.gB + i, J.gA + j, -H[i][j]});
+            }
+        return;
+    }
     // Joint::hessian (Joint.cpp:34-55): H = (J^T J) * mu, column-major entries
     JacRows R = joint_J(J, x);
     const size_t nc = R.cols.size();
@@ -1199,7 +1307,7 @@ void joint_update_lambda(Joint& J, const std::vector<double>& x) {
     double C[6];
     joint_C(J, x, C);
     const int d = J.dim();
-    if (J.type == NXD_JOINT_ANGLE_LIMIT) {
+    if (J.is_limit()) {
         for (int i = 0; i < d; ++i) J.lambda[i] = std::max(0.0, J.lambda[i] + J.mu * C[i]);
     } else {
         for (int i = 0; i < d; ++i) J.lambda[i] += J.mu * C[i];
@@ -2093,6 +2201,19 @@ nxo_world* nxo_create(const nxd_scene_desc* d) {
                 break;
             case NXD_JOINT_ANGLE_LIMIT:
                 J.axis = normalized(mk(p[0], p[1], p[2])); J.min_angle = p[3]; J.max_angle = p[4];
+                break;
+            case NXD_JOINT_PRISMATIC:
+            case NXD_JOINT_CYLINDRICAL:
+                // PrismaticJoint / CylindricalJoint ctors: normalised axes, then
+                // JointPrimitives::computeBasis of each
+                J.anchorA = mk(p[0], p[1], p[2]); J.anchorB = mk(p[3], p[4], p[5]);
+                J.axisA = normalized(mk(p[6], p[7], p[8])); J.axisB = normalized(mk(p[9], p[10], p[11]));
+                compute_basis(J.axisA, J.uA, J.vA);
+                compute_basis(J.axisB, J.uB, J.vB);
+                break;
+            case NXD_JOINT_DISTANCE_LIMIT:
+                // DistanceLimitJoint ctor (DistanceLimitJoint.cpp:6-15)
+                J.min_dist = p[0]; J.max_dist = std::max(p[1], p[0]);
                 break;
             default: delete w; return nullptr;
         }

@@ -252,6 +252,27 @@ def test_trajectory_newmark():
         assert wp <= 1e-6 and wr <= 1e-6, (sc.name, wp, wr)
 
 
+def test_trajectory_prismatic_cylindrical_distance_joints():
+    # PrismaticJoint, CylindricalJoint and DistanceLimitJoint on falling
+    # bodies hanging from a fixed anchor (ALM terms, hardening, active sets)
+    sb = scenes.SceneBuilder("sliders")
+    v, f = scenes.box_mesh(0.05, 0.05, 0.05)
+    a = sb.add_body(v, f, (0.0, 1.0, 0.0), mass=1.0, inertia=0.01 * np.eye(3))
+    sb.fix(a)
+    b = sb.add_body(v, f, (0.2, 1.0, 0.0), mass=0.5, inertia=0.01 * np.eye(3), vel=(0.1, 0.0, 0.2))
+    c = sb.add_body(v, f, (0.2, 0.7, 0.0), mass=0.5, inertia=0.01 * np.eye(3), omega=(0.0, 1.0, 0.0))
+    d = sb.add_body(v, f, (0.5, 0.7, 0.1), mass=0.5, inertia=0.01 * np.eye(3), vel=(0.0, 0.3, 0.0))
+    sb.prismatic(a, b, (0.1, 0, 0), (-0.1, 0, 0), (1, 0, 0), (1, 0, 0), stiffness=1e6)
+    sb.cylindrical(b, c, (0, -0.15, 0), (0, 0.15, 0), (0, 1, 0), (0, 1, 0), stiffness=1e6)
+    sb.distance_limit(c, d, 0.2, 0.32, stiffness=1e6)
+    s = abi.default_settings()
+    s.alm_max_iters = 6
+    sc = sb.build(s, 0.01, 60)
+    wp, wr, (lg, mg, lo, mo) = run_pair(sc, 60, check_every=10)
+    assert wp <= 1e-6 and wr <= 1e-6, (wp, wr)
+    assert np.abs(lg - lo).max() <= 1e-6 * max(1.0, np.abs(lo).max())
+
+
 def test_batch_matches_single_scenes():
     # batched launches (one launch per kernel for all scenes of a group)
     # against the same scenes stepped one context at a time: identical bits;

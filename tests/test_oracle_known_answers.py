@@ -311,3 +311,46 @@ def test_newmark_free_fall_recurrence():
     assert np.allclose(st["position"][0], p, rtol=0, atol=1e-10)
     assert np.allclose(st["velocity"][0], v, rtol=0, atol=1e-8)
     assert np.allclose(st["linear_acceleration"][0], g, rtol=0, atol=1e-5)
+
+
+def slider_scene(kind):
+    """Two boxes joined by a prismatic / cylindrical joint, or kept within a
+    distance band (PrismaticJoint, CylindricalJoint, DistanceLimitJoint)."""
+    sb = scenes.SceneBuilder(kind)
+    v, f = scenes.box_mesh(0.1, 0.1, 0.1)
+    sb.add_body(v, f, (0, 0, 0), mass=1.0, inertia=np.eye(3))
+    sb.add_body(v, f, (0.3, 0.1, 0), quat=scenes.quat_from_axis_angle((0, 0, 1), 0.2), mass=1.0, inertia=np.eye(3))
+    if kind == "prismatic":
+        sb.prismatic(0, 1, (0.1, 0, 0), (-0.1, 0, 0), (1, 0.2, 0), (1, 0, 0.1), stiffness=1e4)
+    elif kind == "cylindrical":
+        sb.cylindrical(0, 1, (0.1, 0, 0), (-0.1, 0, 0), (0.3, 1, 0), (0, 1, 0), stiffness=1e4)
+    else:
+        sb.distance_limit(0, 1, 0.4, 0.5, stiffness=1e4)
+    return sb.build(abi.default_settings(), 0.01, 1)
+
+
+@pytest.mark.parametrize("kind", ["prismatic", "cylindrical", "distance"])
+def test_new_joints_constraint_fd_gradient(kind):
+    # PrismaticJoint / CylindricalJoint / DistanceLimitJoint: the constraint
+    # form's gradient J^T (mu C + lambda) against central differences of its
+    # value (the rotational columns are the left-perturbation Jacobian,
+    # exact at theta = 0)
+    sc = slider_scene(kind)
+    w = refcpu.OracleWorld(sc)
+    w.set_form_state(np.zeros(0, dtype=abi.CONTACT_DTYPE), None, np.zeros(12))
+    x = np.zeros(12)
+    x[0:3] = sc.position[0]
+    x[6:9] = sc.position[1] + (0.0, 0.0, 0.0 if kind != "distance" else 0.5)   # distance 0.59 > max 0.5
+    e0 = w.form_value(abi.NXD_FORM_CONSTRAINT, x)
+    assert e0 > 0.0
+    g = w.form_gradient(abi.NXD_FORM_CONSTRAINT, x)
+    h = 1e-7
+    for k in range(12):
+        xp, xm = x.copy(), x.copy()
+        xp[k] += h
+        xm[k] -= h
+        fd = (w.form_value(abi.NXD_FORM_CONSTRAINT, xp) - w.form_value(abi.NXD_FORM_CONSTRAINT, xm)) / (2 * h)
+        assert abs(g[k] - fd) <= 1e-5 * np.abs(g).max(), (kind, k, g[k], fd)
+    H = w.form_hessian(abi.NXD_FORM_CONSTRAINT, x)
+    assert np.allclose(H, H.T, rtol=0, atol=1e-9 * np.abs(H).max())
+    assert np.linalg.eigvalsh(H).min() >= -1e-9 * np.abs(H).max()

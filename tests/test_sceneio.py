@@ -58,13 +58,12 @@ def test_fixture_scene_mapping():
 
 def test_unsupported_joint_type_is_refused(tmp_path):
     doc = json.load(open(FIXTURE))
-    doc["joints"].append({"type": "prismatic", "body_a": 12, "body_b": 13, "anchor_a": [0, 0, 0],
-                          "anchor_b": [0, 0, 0], "axis_a": [1, 0, 0], "axis_b": [1, 0, 0]})
+    doc["joints"].append({"type": "damped_spring", "body_a": 12, "body_b": 13, "stiffness_npm": 10.0})
     p = tmp_path / "s.json"
     p.write_text(json.dumps(doc))
     for name in ("ground.obj", "cube.obj", "link.obj"):
         (tmp_path / name).write_text(open(os.path.join(GOLDEN, name)).read())
-    with pytest.raises(NotImplementedError, match="prismatic"):
+    with pytest.raises(NotImplementedError, match="damped_spring"):
         sceneio.load_scene(str(p))
 
 
