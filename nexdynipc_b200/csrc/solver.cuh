@@ -1330,6 +1330,7 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 
 struct GridCtx {
     int G, b, gtid, gthreads;
+    int lin;              // element index of this thread in NX_GRID_FOR: CTA-interleaved
     unsigned* count;      // arrivals, zeroed before each launch
     int* abort;           // set by a CTA whose wait ran out
     int* status;
@@ -1425,7 +1426,10 @@ struct GridRed {
 };
 
 // grid-strided loop over [0, n)
-#define NX_GRID_FOR(e, n, gc) for (int e = (gc).gtid; e < (n); e += (gc).gthreads)
+// Grid-stride loop with consecutive elements on consecutive CTAs (element e
+// on CTA e mod G), so that short lists of heavy elements (joints, bodies)
+// spread over all SMs instead of filling the first CTAs.
+#define NX_GRID_FOR(e, n, gc) for (int e = (gc).lin; e < (n); e += (gc).gthreads)
 
 // poses (and the x <- xt copy after an accepted step) for every body
 __device__ void grid_poses(const Solver& S, const double* x, const GridCtx& gc) {
@@ -1540,13 +1544,11 @@ __device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, int* s
     }
     gc.sync();
     NX_PHASE(3);
-    // multi-body components: one warp each, taken from a global counter
+    // multi-body components: one warp each, consecutive components on
+    // consecutive CTAs (warp w of CTA b takes components w G + b, + G nw, ...)
     const int lane = threadIdx.x & 31;
-    for (;;) {
-        int o = 0;
-        if (lane == 0) o = atomicAdd(S.comp_next, 1);
-        o = __shfl_sync(0xffffffffu, o, 0);
-        if (o >= n_comp) break;
+    const int nwarps = gc.G * (blockDim.x >> 5);
+    for (int o = (threadIdx.x >> 5) * gc.G + gc.b; o < n_comp; o += nwarps) {
         const int rc = solve_component(S, S.comp_root[o], s, C);
         if (rc != 0 && lane == 0) {
             atomicExch(S.solve_fail, 1);
@@ -1577,6 +1579,7 @@ __device__ __forceinline__ void newton_body(const Solver& S) {
     GridCtx gc;
     gc.G = gridDim.x; gc.b = blockIdx.x;
     gc.gtid = blockIdx.x * blockDim.x + threadIdx.x; gc.gthreads = gridDim.x * blockDim.x;
+    gc.lin = threadIdx.x * gc.G + gc.b;
     gc.count = S.bar_count; gc.abort = S.bar_abort; gc.status = S.status; gc.target = 0; gc.sh_ok = &sh_ok;
     if (threadIdx.x == 0) sh_ok = 1;
     __syncthreads();
