@@ -191,61 +191,73 @@ constexpr int kLB_min_pair_distance = 0;
 __global__ void k_min_pair_distance(const __grid_constant__ Geo g, const __grid_constant__ PairQuery q, const double* boxes, double* out) { min_pair_distance_body(g, q, boxes, out); }
 
 // ---------------------------------------------------------------------------
-// Top-k selection (ContactAssembler.cpp:214-303): one warp per (pair, list),
-// list s = 0 vA, 1 vB, 2 eA, 3 eB, 4 fA, 5 fB.  Scores are point-to-box
-// distances of the primitive's world vertices to the other body's box.
+// Top-k selection (ContactAssembler.cpp:214-303), lists s = 0 vA, 1 vB, 2 eA,
+// 3 eB, 4 fA, 5 fB.  Scores are point-to-box distances of the primitive's
+// world vertices to the other body's box.  One warp per (pair, side): the
+// side's vertex scores are computed once, and an edge's (face's) score is the
+// std::min of its vertices' scores, the same value the per-list evaluation
+// gives.  Shared memory per warp: vertex scores, one list's scores, and the
+// selection's idx / G / L arrays.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void topk_body(const Geo& g, const int* pairs, const int* npairs_ptr, int cap, const double* boxes, const double* wv, int* topk, int* topn, int max_prims) {
-    extern __shared__ unsigned char smem_raw[];
+__host__ __device__ inline size_t topk_warp_bytes(int max_prims, int max_verts) {
+    return ((size_t)max_verts * sizeof(double) + (size_t)max_prims * (sizeof(double) + 3 * sizeof(int)) + 31) / 16 * 16;
+}
+__device__ __forceinline__ void topk_body(const Geo& g, const int* pairs, const int* npairs_ptr, int cap, const double* boxes, const double* wv, int* topk, int* topn, int max_prims, int max_verts) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int wpb = blockDim.x >> 5;
     const int wid = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const size_t per_warp = ((size_t)max_prims * (sizeof(double) + 3 * sizeof(int)) + 31) / 16 * 16;
-    unsigned char* base = smem_raw + per_warp * wid;
-    double* key = reinterpret_cast<double*>(base);
+    unsigned char* base = smem_raw + topk_warp_bytes(max_prims, max_verts) * wid;
+    double* vkey = reinterpret_cast<double*>(base);
+    double* key = vkey + max_verts;
     int* idx = reinterpret_cast<int*>(key + max_prims);
-    SelView v{idx, key, idx + max_prims, idx + 2 * max_prims};
     const int np = min(*npairs_ptr, cap);
-    for (int item = blockIdx.x * wpb + wid; item < np * 6; item += gridDim.x * wpb) {
-        const int p = item / 6, s = item % 6;
+    for (int item = blockIdx.x * wpb + wid; item < np * 2; item += gridDim.x * wpb) {
+        const int p = item >> 1, side = item & 1;
         const int a = pairs[2 * p], b = pairs[2 * p + 1];
-        const int X = (s & 1) ? b : a;
-        const int Y = (s & 1) ? a : b;
+        const int X = side ? b : a;
+        const int Y = side ? a : b;
         const Box other = ld_box(boxes + 6 * Y);
-        const int vo = g.voff[X];
-        int n;
-        if (s < 2) {
-            n = g.voff[X + 1] - vo;
-            for (int e = lane; e < n; e += 32) key[e] = point_box_distance(ld3(wv + 3 * (vo + e)), other);
-        } else if (s < 4) {
-            const int eo = g.eoff[X];
-            n = g.eoff[X + 1] - eo;
-            for (int e = lane; e < n; e += 32) {
-                const int* ed = g.edges + 2 * (eo + e);
-                key[e] = dmin(point_box_distance(ld3(wv + 3 * (vo + ed[0])), other),
-                              point_box_distance(ld3(wv + 3 * (vo + ed[1])), other));
+        const int vo = g.voff[X], nv = g.voff[X + 1] - vo;
+        for (int e = lane; e < nv; e += 32) vkey[e] = point_box_distance(ld3(wv + 3 * (vo + e)), other);
+        __syncwarp();
+        for (int list = 0; list < 3; ++list) {
+            const double* kk = key;
+            int n, s;
+            if (list == 0) {
+                s = 2 + side;
+                const int eo = g.eoff[X];
+                n = g.eoff[X + 1] - eo;
+                for (int e = lane; e < n; e += 32) {
+                    const int* ed = g.edges + 2 * (eo + e);
+                    key[e] = dmin(vkey[ed[0]], vkey[ed[1]]);
+                }
+            } else if (list == 1) {
+                s = 4 + side;
+                const int fo = g.foff[X];
+                n = g.foff[X + 1] - fo;
+                for (int e = lane; e < n; e += 32) {
+                    const int* f = g.faces + 3 * (fo + e);
+                    key[e] = dmin(dmin(vkey[f[0]], vkey[f[1]]), vkey[f[2]]);
+                }
+            } else {
+                s = side;
+                n = nv;
+                kk = vkey;
             }
-        } else {
-            const int fo = g.foff[X];
-            n = g.foff[X + 1] - fo;
-            for (int e = lane; e < n; e += 32) {
-                const int* f = g.faces + 3 * (fo + e);
-                const double d0 = point_box_distance(ld3(wv + 3 * (vo + f[0])), other);
-                const double d1 = point_box_distance(ld3(wv + 3 * (vo + f[1])), other);
-                const double d2 = point_box_distance(ld3(wv + 3 * (vo + f[2])), other);
-                key[e] = dmin(dmin(d0, d1), d2);
-            }
+            __syncwarp();
+            const SelView v{idx, kk, idx + max_prims, idx + 2 * max_prims};
+            const int k = min(kTopK, n);
+            sel_top_k_warp(v, n, k);
+            const size_t out = (size_t)p * 6 + s;
+            if (lane < k) topk[out * kTopK + lane] = idx[lane];
+            if (lane == 0) topn[out] = k;
+            __syncwarp();
         }
-        __syncwarp();
-        const int k = min(kTopK, n);
-        sel_top_k_warp(v, n, k);
-        if (lane < k) topk[(size_t)item * kTopK + lane] = idx[lane];
-        if (lane == 0) topn[item] = k;
-        __syncwarp();
     }
 }
 constexpr int kLB_topk = 0;
-__global__ void k_topk(const __grid_constant__ Geo g, const int* pairs, const int* npairs_ptr, int cap, const double* boxes, const double* wv, int* topk, int* topn, int max_prims) { topk_body(g, pairs, npairs_ptr, cap, boxes, wv, topk, topn, max_prims); }
+__global__ void k_topk(const __grid_constant__ Geo g, const int* pairs, const int* npairs_ptr, int cap, const double* boxes, const double* wv, int* topk, int* topn, int max_prims, int max_verts) { topk_body(g, pairs, npairs_ptr, cap, boxes, wv, topk, topn, max_prims, max_verts); }
 
 // ---------------------------------------------------------------------------
 // Candidate item counts per pair and the materialised candidate lists
@@ -784,31 +796,48 @@ __device__ double vertex_face_plane_distance(V3 p, V3 v0, V3 v1, V3 v2) {
     return INFINITY;
 }
 
+// One warp per pair: lanes test 32 vertices of body i against body j's box at
+// a time; each vertex that passes is broadcast and the lanes sweep j's faces.
+// The two prune tests and the plane distance are those of the per-(vertex,
+// face) formulation, so the minimum over the surviving pairs is the same value.
 __device__ __forceinline__ void min_distance_body(const Geo& g, const int* pairs, const int* npairs_ptr, int cap, const double* boxes, const double* wv, double* out, const int* gate) {
     if (gate && *gate == 0) return;
+    const unsigned full = 0xffffffffu;
     const int np = min(*npairs_ptr, cap);
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
     double m = INFINITY;
-    for (int p = blockIdx.x; p < np; p += gridDim.x) {
+    for (int p = blockIdx.x * wpb + (threadIdx.x >> 5); p < np; p += gridDim.x * wpb) {
         const int i = pairs[2 * p], j = pairs[2 * p + 1];
         const Box bj = ld_box(boxes + 6 * j);
         const double band = kPruneBand + g.md_tol[j];
         const int vi0 = g.voff[i], nvi = g.voff[i + 1] - vi0;
         const int vj0 = g.voff[j];
         const int fj0 = g.foff[j], nfj = g.foff[j + 1] - fj0;
-        for (int w = threadIdx.x; w < nvi * nfj; w += blockDim.x) {
-            const int vi = w / nfj, fi = w % nfj;
-            const V3 pp = ld3(wv + 3 * (vi0 + vi));
-            if (point_box_distance(pp, bj) > band) continue;
-            const int* F = g.faces + 3 * (fj0 + fi);
-            const V3 a = ld3(wv + 3 * (vj0 + F[0])), b = ld3(wv + 3 * (vj0 + F[1])), c = ld3(wv + 3 * (vj0 + F[2]));
-            Box fb = box_empty();
-            box_expand(fb, a); box_expand(fb, b); box_expand(fb, c);
-            if (point_box_distance(pp, fb) > band) continue;
-            m = dmin(m, vertex_face_plane_distance(pp, a, b, c));
+        for (int v0 = 0; v0 < nvi; v0 += 32) {
+            V3 pp = v3(0.0, 0.0, 0.0);
+            bool near = false;
+            if (v0 + lane < nvi) {
+                pp = ld3(wv + 3 * (vi0 + v0 + lane));
+                near = !(point_box_distance(pp, bj) > band);
+            }
+            unsigned live = __ballot_sync(full, near);
+            while (live) {
+                const int src = __ffs(live) - 1;
+                live &= live - 1;
+                const V3 q = v3(__shfl_sync(full, pp.x, src), __shfl_sync(full, pp.y, src), __shfl_sync(full, pp.z, src));
+                for (int fi = lane; fi < nfj; fi += 32) {
+                    const int* F = g.faces + 3 * (fj0 + fi);
+                    const V3 a = ld3(wv + 3 * (vj0 + F[0])), b = ld3(wv + 3 * (vj0 + F[1])), c = ld3(wv + 3 * (vj0 + F[2]));
+                    Box fb = box_empty();
+                    box_expand(fb, a); box_expand(fb, b); box_expand(fb, c);
+                    if (point_box_distance(q, fb) > band) continue;
+                    m = dmin(m, vertex_face_plane_distance(q, a, b, c));
+                }
+            }
         }
     }
-    for (int o = 16; o > 0; o >>= 1) m = dmin(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0 && m < INFINITY) atomic_min_pos_double(out, m);
+    for (int o = 16; o > 0; o >>= 1) m = dmin(m, __shfl_xor_sync(full, m, o));
+    if (lane == 0 && m < INFINITY) atomic_min_pos_double(out, m);
 }
 constexpr int kLB_min_distance = 0;
 __global__ void k_min_distance(const __grid_constant__ Geo g, const int* pairs, const int* npairs_ptr, int cap, const double* boxes, const double* wv, double* out, const int* gate) { min_distance_body(g, pairs, npairs_ptr, cap, boxes, wv, out, gate); }

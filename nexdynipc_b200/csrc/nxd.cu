@@ -74,6 +74,7 @@ struct nxd_ctx {
     int newton_grid = 1;   // co-resident CTAs of k_newton (power of two)
     int N = 0, nv = 0, nf = 0, ne = 0, J = 0, D = 0;
     int max_prims = 0;
+    int max_verts = 0;
     int pair_cap = 0;
     nxd_settings s{};
     std::vector<int> h_body_ids;
@@ -209,8 +210,10 @@ void fill_solver(nxd_ctx* c) {
     S.gpart = m.alloc<double>(2 * kRedMaxQ * kMaxNewtonGrid);
     // one CTA of kNewtonThreads per 512 DOFs, a power of two no larger than
     // what the device keeps co-resident
+    S.slab_bytes = kNewtonSlabBytes;
+    cudaFuncSetAttribute(k_newton, cudaFuncAttributeMaxDynamicSharedMemorySize, kNewtonDynSmem);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newton, kNewtonThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newton, kNewtonThreads, kNewtonDynSmem);
     const int coresident = std::max(1, per_sm * c->n_sm);
     int g = 1;
     while (g < kMaxNewtonGrid && g * 2 <= coresident && (long long)g * kNewtonThreads < 6LL * N) g *= 2;
@@ -237,13 +240,13 @@ StepCfg step_cfg(const nxd_ctx* c) {
 // cooperative launch of k_newton on c->newton_grid co-resident CTAs
 void launch_newton(nxd_ctx* c) {
     if (c->rec || c->newton_grid == 1) {
-        NXD_K(c, NXD_PROF_NEWTON, newton, (1), (kNewtonThreads), (0), c->S);
+        NXD_K(c, NXD_PROF_NEWTON, newton, (1), (kNewtonThreads), (kNewtonDynSmem), c->S);
         return;
     }
     ProfScope ps_(c, NXD_PROF_NEWTON);
     cudaMemsetAsync(c->S.bar_count, 0, 2 * sizeof(unsigned), c->stream);
     void* args[] = {(void*)&c->S};
-    cudaLaunchCooperativeKernel((const void*)k_newton, dim3(c->newton_grid), dim3(kNewtonThreads), args, 0, c->stream);
+    cudaLaunchCooperativeKernel((const void*)k_newton, dim3(c->newton_grid), dim3(kNewtonThreads), args, kNewtonDynSmem, c->stream);
 }
 
 // ContactAssembler::build + world vertices at the current poses
@@ -261,17 +264,17 @@ void launch_pairs(nxd_ctx* c, const PairQuery& q, int* out, int* count_dev, cons
 }
 
 size_t topk_smem(const nxd_ctx* c, int warps) {
-    return (size_t)warps * (((size_t)c->max_prims * (sizeof(double) + 3 * sizeof(int)) + 31) / 16 * 16);
+    return (size_t)warps * topk_warp_bytes(c->max_prims, c->max_verts);
 }
 
 // buildCandidateSet with activation distance = *dhat (device) -> pairs, topk, item offsets
 void launch_candidates(nxd_ctx* c, const double* act_ptr, double act_val) {
     PairQuery q{1, act_ptr, act_val, 1.0, 1.0};
     launch_pairs(c, q, c->pairs, &c->sc->n_pairs, nullptr);
-    int warps = 4;
+    int warps = 8;
     while (warps > 1 && topk_smem(c, warps) > 200 * 1024) --warps;
     NXD_K(c, NXD_PROF_TOPK, topk, (c->n_sm * 4), (32 * warps), (topk_smem(c, warps)), c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap,
-                                                                       c->boxes, c->wv, c->topk, c->topn, c->max_prims);
+                                                                       c->boxes, c->wv, c->topk, c->topn, c->max_prims, c->max_verts);
 }
 
 }  // namespace
@@ -315,13 +318,17 @@ __global__ void k_alm_detect_gate(const Scalars* sc, int* skip) { alm_detect_gat
 __device__ __forceinline__ void init_scalar_d_body(double* p, double v) { *p = v; }
 constexpr int kLB_init_scalar_d = 0;
 __global__ void k_init_scalar_d(double* p, double v) { init_scalar_d_body(p, v); }
+// max(0, tol[0..n)) over one CTA (the tolerances are positive and finite, so
+// the maximum does not depend on the order)
 __device__ __forceinline__ void max_tol_body(const double* tol, int n, double* out) {
+    NX_BLOCK_RED(R);
     double m = 0.0;
-    for (int i = 0; i < n; ++i) m = dmax(m, tol[i]);
-    *out = m;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = dmax(m, tol[i]);
+    m = R.max(m);
+    if (threadIdx.x == 0) *out = m;
 }
-constexpr int kLB_max_tol = 0;
-__global__ void k_max_tol(const double* tol, int n, double* out) { max_tol_body(tol, n, out); }
+constexpr int kLB_max_tol = kSolverThreads;
+__global__ void __launch_bounds__(kSolverThreads) k_max_tol(const double* tol, int n, double* out) { max_tol_body(tol, n, out); }
 __device__ __forceinline__ void body_md_tol_body(const Geo& g, const double* pos, double* tol) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.N) return;
@@ -345,7 +352,7 @@ nxd_status enqueue_step(nxd_ctx* c, double dt) {
         PairQuery qb{0, &c->sc->dhat, 0.0, 2.0, 0.0};
         NXD_K(c, NXD_PROF_BROAD, min_pair_distance, (grid_for((long long)c->N * 32, 256)), (256), (0), c->geo, qb, c->boxes, &c->sc->bmd);
         NXD_K(c, NXD_PROF_OTHER, body_md_tol, (grid_for(c->N, 128)), (128), (0), c->geo, c->pos, c->md_tol);
-        NXD_K(c, NXD_PROF_OTHER, max_tol, (1), (1), (0), c->md_tol, c->N, c->max_md_tol);
+        NXD_K(c, NXD_PROF_OTHER, max_tol, (1), (kSolverThreads), (0), c->md_tol, c->N, c->max_md_tol);
         NXD_K(c, NXD_PROF_OTHER, md_gate, (1), (1), (0), c->sc, c->max_md_tol);
         PairQuery qm{2, &c->sc->md_radius, 0.0, 1.0, 0.0};
         launch_pairs(c, qm, c->md_pairs, &c->sc->n_md_pairs, &c->sc->md_gate);
@@ -476,6 +483,7 @@ nxd_status nxd_create(const nxd_scene_desc* d, nxd_ctx** out) {
         }
         const int nvb = v1 - v0, nfb = f1 - f0, neb = (int)(edges.size() / 2) - eoff[i];
         c->max_prims = std::max({c->max_prims, nvb, nfb, neb});
+        c->max_verts = std::max(c->max_verts, nvb);
     }
     eoff[N] = (int)(edges.size() / 2);
     c->ne = eoff[N];
@@ -836,7 +844,7 @@ nxd_status nxd_scene_min_distance(nxd_ctx* c, double* out) {
     launch_assembly(c);
     cudaStream_t st = c->stream;
     NXD_K(c, NXD_PROF_OTHER, body_md_tol, (grid_for(c->N, 128)), (128), (0), c->geo, c->pos, c->md_tol);
-    NXD_K(c, NXD_PROF_OTHER, max_tol, (1), (1), (0), c->md_tol, c->N, c->max_md_tol);
+    NXD_K(c, NXD_PROF_OTHER, max_tol, (1), (kSolverThreads), (0), c->md_tol, c->N, c->max_md_tol);
     // force the gate open: bmd = 0
     NXD_K(c, NXD_PROF_OTHER, init_scalar_d, (1), (1), (0), &c->sc->bmd, 0.0);
     NXD_K(c, NXD_PROF_OTHER, md_gate, (1), (1), (0), c->sc, c->max_md_tol);

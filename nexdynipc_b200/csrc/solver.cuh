@@ -87,6 +87,7 @@ struct Solver {
     int* local;                                   // [N] body -> member index inside its component
     unsigned* mpool; long long mpool_cap; long long* mpool_off;   // per-component masks and lists
     double* pool; long long pool_cap; long long* pool_off;        // per-component L, D and rhs
+    int slab_bytes;                               // per-warp shared workspace of a component solve (0: none)
     int* solve_fail;                              // [1] zero pivot or capacity in this solve
     // grid execution of k_newton
     unsigned* bar_count; int* bar_abort;          // barrier arrivals and give-up flag, zeroed per launch
@@ -1037,7 +1038,9 @@ __device__ __forceinline__ int mask_rank(const unsigned* row, int b) {
 __device__ __forceinline__ bool mask_test(const unsigned* row, int b) { return (row[b >> 5] >> (b & 31)) & 1u; }
 
 // returns 0 ok, 1 zero pivot, 2 capacity
-__device__ int solve_component(const Solver& S, int root, double s, int C) {
+// Workspace: the structure words, then the factor doubles, each in the warp's
+// shared-memory slab when it fits there, else in the global pools.
+__device__ int solve_component(const Solver& S, int root, double s, int C, unsigned char* slab) {
     const int lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
     const int k = S.mcnt[root + 1] - S.mcnt[root];
@@ -1048,11 +1051,18 @@ __device__ int solve_component(const Solver& S, int root, double s, int C) {
     const int W = (k + 31) >> 5;
     const int Psort = max(pow2_ceil(k), pow2_ceil(max(m, 1)));
     const long long nwords = Psort + 3LL * k * W + 6LL * k + 2;
-    long long off = 0;
-    if (lane == 0) off = (long long)atomicAdd((unsigned long long*)S.mpool_off, (unsigned long long)nwords);
-    off = __shfl_sync(full, off, 0);
-    if (off + nwords > S.mpool_cap) return 2;
-    unsigned* base = S.mpool + off;
+    unsigned* base;
+    size_t slab_used = 0;
+    if (slab && 4 * nwords <= S.slab_bytes) {
+        base = reinterpret_cast<unsigned*>(slab);
+        slab_used = (size_t)(4 * nwords + 15) & ~(size_t)15;
+    } else {
+        long long off = 0;
+        if (lane == 0) off = (long long)atomicAdd((unsigned long long*)S.mpool_off, (unsigned long long)nwords);
+        off = __shfl_sync(full, off, 0);
+        if (off + nwords > S.mpool_cap) return 2;
+        base = S.mpool + off;
+    }
     int* sortbuf = (int*)base;
     unsigned* adj = base + Psort;
     unsigned* colm = adj + (size_t)k * W;
@@ -1151,11 +1161,16 @@ __device__ int solve_component(const Solver& S, int root, double s, int C) {
     const int nnz = warp_scan_excl(rowptr, k);
     if (lane == 0) rowptr[k] = nnz;
     const long long ndoubles = 36LL * (k + nnz) + 6LL * k;
-    long long doff = 0;
-    if (lane == 0) doff = (long long)atomicAdd((unsigned long long*)S.pool_off, (unsigned long long)ndoubles);
-    doff = __shfl_sync(full, doff, 0);
-    if (doff + ndoubles > S.pool_cap) return 2;
-    double* Dg = S.pool + doff;
+    double* Dg;
+    if (slab && (long long)slab_used + 8 * ndoubles <= S.slab_bytes) {
+        Dg = reinterpret_cast<double*>(slab + slab_used);
+    } else {
+        long long doff = 0;
+        if (lane == 0) doff = (long long)atomicAdd((unsigned long long*)S.pool_off, (unsigned long long)ndoubles);
+        doff = __shfl_sync(full, doff, 0);
+        if (doff + ndoubles > S.pool_cap) return 2;
+        Dg = S.pool + doff;
+    }
     double* Lv = Dg + 36LL * k;
     double* vec = Lv + 36LL * nnz;
     for (int e = lane; e < 36 * k; e += 32) Dg[e] = S.Hd[36 * body_at[e / 36] + e % 36];
@@ -1319,6 +1334,8 @@ __device__ int solve_component(const Solver& S, int root, double s, int C) {
 // bounded wait.  G = 1 degenerates to __syncthreads.
 // ---------------------------------------------------------------------------
 constexpr int kNewtonThreads = 512;
+constexpr int kNewtonSlabBytes = 11 * 1024;   // per warp: a chain-sized component factors in shared memory
+constexpr int kNewtonDynSmem = (kNewtonThreads / 32) * kNewtonSlabBytes;
 constexpr int kMaxNewtonGrid = 64;
 constexpr unsigned kBarrierSpinLimit = 1u << 24;   // x >= 64 ns sleeps: about a second
 
@@ -1548,8 +1565,10 @@ __device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, int* s
     // consecutive CTAs (warp w of CTA b takes components w G + b, + G nw, ...)
     const int lane = threadIdx.x & 31;
     const int nwarps = gc.G * (blockDim.x >> 5);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char* const slab = S.slab_bytes > 0 ? smem_raw + (size_t)(threadIdx.x >> 5) * S.slab_bytes : nullptr;
     for (int o = (threadIdx.x >> 5) * gc.G + gc.b; o < n_comp; o += nwarps) {
-        const int rc = solve_component(S, S.comp_root[o], s, C);
+        const int rc = solve_component(S, S.comp_root[o], s, C, slab);
         if (rc != 0 && lane == 0) {
             atomicExch(S.solve_fail, 1);
             if (rc == 2) atomicExch(S.status, NXD_CAPACITY);

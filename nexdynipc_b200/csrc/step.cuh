@@ -53,9 +53,19 @@ __device__ __forceinline__ void barrier_init_body(const StepCfg& cfg, const doub
     NX_BLOCK_RED(R);
     if (!cfg.enable_adaptive || sc->barrier_initialized || cfg.N == 0) return;
     const double tm = R.sum(cfg.N, [&](int i) { return mass[i]; });
+    // scene bounds: per-thread, per-warp, then across warps (min / max are
+    // exact; a +-0 tie only changes the sign of a zero, which mx - mn absorbs)
+    __shared__ double wb[32 * 6];
+    V3 mn = v3(INFINITY, INFINITY, INFINITY), mx = v3(-INFINITY, -INFINITY, -INFINITY);
+    for (int i = threadIdx.x; i < cfg.N; i += blockDim.x) { mn = cwmin(mn, ld3(pos + 3 * i)); mx = cwmax(mx, ld3(pos + 3 * i)); }
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = cwmin(mn, v3(__shfl_xor_sync(0xffffffffu, mn.x, o), __shfl_xor_sync(0xffffffffu, mn.y, o), __shfl_xor_sync(0xffffffffu, mn.z, o)));
+        mx = cwmax(mx, v3(__shfl_xor_sync(0xffffffffu, mx.x, o), __shfl_xor_sync(0xffffffffu, mx.y, o), __shfl_xor_sync(0xffffffffu, mx.z, o)));
+    }
+    if ((threadIdx.x & 31) == 0) { st3(wb + 6 * (threadIdx.x >> 5), mn); st3(wb + 6 * (threadIdx.x >> 5) + 3, mx); }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        V3 mn = v3(INFINITY, INFINITY, INFINITY), mx = v3(-INFINITY, -INFINITY, -INFINITY);
-        for (int i = 0; i < cfg.N; ++i) { mn = cwmin(mn, ld3(pos + 3 * i)); mx = cwmax(mx, ld3(pos + 3 * i)); }
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) { mn = cwmin(mn, ld3(wb + 6 * w)); mx = cwmax(mx, ld3(wb + 6 * w + 3)); }
         st3(bb, mn); st3(bb + 3, mx);
         const double am = tm / (double)cfg.N;
         double diag = norm(mx - mn);
