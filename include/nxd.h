@@ -64,9 +64,24 @@ enum {
  *   distance limit: min_distance max_distance                 (DistanceLimitJoint ctor)
  */
 
+/* Control forms of World::forms, in load order (src/Control). */
+enum {
+    NXD_DRIVE_ANGULAR_VELOCITY = 0, /* VelocityDriveForm        (VelocityDriveForm.cpp)       */
+    NXD_DRIVE_LINEAR_VELOCITY = 1,  /* LinearVelocityDriveForm  (LinearVelocityDriveForm.cpp) */
+    NXD_DRIVE_POSITION = 2,         /* PositionDriveForm        (PositionDriveForm.cpp)       */
+    NXD_DRIVE_FORCE = 3,            /* ForceDriveForm           (ForceDriveForm.cpp)          */
+    NXD_DRIVE_DAMPED_SPRING = 4     /* DampedSpringForm         (DampedSpringForm.cpp)        */
+};
 #define NXD_DRIVE_PARAMS 8
-/* Velocity drive (Control/VelocityDriveForm.cpp) parameter layout, 8 doubles:
- *   axis[3] kv v_target max_torque(<=0: unlimited) delay_radps delay_tau_s */
+/* Per-drive parameter layout inside nxd_scene_desc.drive_params (8 doubles):
+ *   angular velocity: axis[3] kv v_target max_torque(<=0: unlimited) delay_radps delay_tau_s
+ *   linear velocity:  axis[3] kv v_target max_force(<=0: unlimited)  delay_mps   delay_tau_s
+ *   position:         axis[3] kp target_position max_force(<=0: unlimited) deadzone_m 0
+ *   force:            force_world[3] torque_world[3] 0 0   (body_b is the body, body_a -1)
+ *   damped spring:    rest_length stiffness damping 0 0 0 0 0
+ * Axes are normalised at creation, as the constructors do.  body_a may be -1
+ * (world) for the angular, linear and position drives; the spring needs two
+ * distinct bodies. */
 
 /* Solver settings: IPCSolver setters (Dynamics/IPCSolver.h:34-79) and
  * NewtonSolver::Options (Math/NewtonSolver.h:58-64). */
@@ -127,7 +142,7 @@ typedef struct nxd_scene_desc {
     const int32_t* joint_body_b;         /* [n_joints] body id (fixed: -1)        */
     const double* joint_params;          /* [n_joints*16]                         */
     const double* joint_stiffness;       /* [n_joints] ALM penalty mu             */
-    int32_t n_drives;                    /* VelocityDriveForm entries of World::forms */
+    int32_t n_drives;                    /* control forms of World::forms, load order */
     const int32_t* drive_body_a;         /* [n_drives] body id or -1 (world)      */
     const int32_t* drive_body_b;         /* [n_drives] body id                    */
     const double* drive_params;          /* [n_drives*8]                          */
@@ -139,6 +154,7 @@ typedef struct nxd_scene_desc {
     int32_t n_contact_pairs;
     const int32_t* contact_pair_bodies;  /* [n_contact_pairs*2] body ids         */
     const double* contact_pair_friction; /* [n_contact_pairs] (< 0: none) or NULL */
+    const int32_t* drive_kind;           /* [n_drives] NXD_DRIVE_* or NULL (all angular velocity) */
 } nxd_scene_desc;
 
 /* Body state as written back by IPCSolver::step (IPCSolver.cpp:1174-1195). */
@@ -205,7 +221,7 @@ enum {
     NXD_FORM_CONSTRAINT = 2,  /* ConstraintForm over all joints  */
     NXD_FORM_BARRIER = 3,     /* DistanceBarrierForm (unscaled)  */
     NXD_FORM_FRICTION = 4,    /* FrictionForm (unscaled)         */
-    NXD_FORM_DRIVES = 5,      /* sum of VelocityDriveForms       */
+    NXD_FORM_DRIVES = 5,      /* sum of the control forms        */
     NXD_FORM_TOTAL = 6,       /* SimulationProblem::computeValue / computeGradient */
     NXD_FORM_CONTACT = 7      /* SimulationProblem::computeContactValue / Gradient */
 };

@@ -18,6 +18,11 @@ NXD_JOINT_CYLINDRICAL = 5
 NXD_JOINT_DISTANCE_LIMIT = 6
 NXD_JOINT_PARAMS = 16
 NXD_DRIVE_PARAMS = 8
+NXD_DRIVE_ANGULAR_VELOCITY = 0
+NXD_DRIVE_LINEAR_VELOCITY = 1
+NXD_DRIVE_POSITION = 2
+NXD_DRIVE_FORCE = 3
+NXD_DRIVE_DAMPED_SPRING = 4
 
 NXD_FORM_INERTIA = 0
 NXD_FORM_GRAVITY = 1
@@ -126,6 +131,7 @@ class NxdSceneDesc(C.Structure):
         ("n_contact_pairs", C.c_int32),
         ("contact_pair_bodies", _ip),
         ("contact_pair_friction", _dp),
+        ("drive_kind", _ip),
     ]
 
 

@@ -88,6 +88,8 @@ struct nxd_ctx {
     double *jparams, *jmu, *jlam;
     int *da, *db, *dinc_off, *dinc, *dfinit, *dhas_prev;
     Drv* dprm;
+    int* dkind;
+    double* dDir;
     double *dfilt, *dprevA, *dprevB;
     // state
     double *pos, *quat, *vel, *omega, *lacc, *aacc;
@@ -169,6 +171,7 @@ void fill_solver(nxd_ctx* c) {
     S.jtype = c->jtype; S.ja = c->ja; S.jb = c->jb; S.jparams = c->jparams; S.jmu = c->jmu; S.jlam = c->jlam;
     S.jinc_off = c->jinc_off; S.jinc = c->jinc;
     S.da = c->da; S.db = c->db; S.dprm = c->dprm; S.dprevA = c->dprevA; S.dprevB = c->dprevB;
+    S.dkind = c->dkind; S.dDir = c->dDir; S.bvel = c->vel;
     S.dhas_prev = c->dhas_prev; S.dfilt = c->dfilt; S.dinc_off = c->dinc_off; S.dinc = c->dinc;
     S.contacts = c->contacts; S.ncontacts_ptr = &c->sc->n_contacts;
     S.nforce = c->nforce; S.nnf_ptr = &c->sc->nnf;
@@ -193,12 +196,12 @@ void fill_solver(nxd_ctx* c) {
     S.parent = m.alloc<int>(N + 1); S.comp = m.alloc<int>(N);
     S.mcnt = m.alloc<int>(N + 1); S.icnt = m.alloc<int>(N + 1); S.rflag = m.alloc<int>(N + 1);
     S.comp_root = m.alloc<int>(N + 1); S.n_comp = m.alloc<int>(1); S.comp_next = m.alloc<int>(1);
-    S.members = m.alloc<int>(N); S.items = m.alloc<int>(J + 2 * kMaxContacts); S.local = m.alloc<int>(N + 1);
+    S.members = m.alloc<int>(N); S.items = m.alloc<int>(J + D + 2 * kMaxContacts); S.local = m.alloc<int>(N + 1);
     // per-component structure masks (3 k ceil(k/32) words + lists) and factors
     // (36 (k + nnz(L)) + 6k doubles, nnz(L) <= k(k-1)/2): room for the whole
     // scene as one dense component, the factor pool capped at 768 MB
     const long long kk = std::min<long long>(N, kMaxComponentBodies);
-    const long long mwords = 3LL * kk * ((kk + 31) / 32) + 16LL * N + 4LL * (J + 2 * kMaxContacts) + 4096;
+    const long long mwords = 3LL * kk * ((kk + 31) / 32) + 16LL * N + 4LL * (J + D + 2 * kMaxContacts) + 4096;
     S.mpool = m.alloc<unsigned>(mwords); S.mpool_cap = mwords; S.mpool_off = m.alloc<long long>(1);
     const long long pool_doubles = std::min<long long>(96LL << 20, 18LL * N * N + 64LL * N + 4096);
     S.pool = m.alloc<double>(pool_doubles); S.pool_cap = pool_doubles; S.pool_off = m.alloc<long long>(1);
@@ -384,7 +387,7 @@ nxd_status enqueue_step(nxd_ctx* c, double dt) {
     }
     NXD_K(c, NXD_PROF_OTHER, update_state, (grid_for(c->N, 128)), (128), (0), cfg, c->x, c->xprev, c->vprev, c->xhat, c->aprev, c->pos, c->quat, c->vel, c->omega,
                                                         c->lacc, c->aacc, c->sc, c->da, c->db, c->dprm, c->dfilt);
-    if (c->D > 0) NXD_K(c, NXD_PROF_OTHER, drive_kpi, (1), (1), (0), cfg, c->omega, c->sc, c->da, c->db, c->dprm, c->dfilt);
+    if (c->D > 0) NXD_K(c, NXD_PROF_OTHER, drive_kpi, (1), (1), (0), cfg, c->omega, c->sc, c->da, c->db, c->dprm, c->dfilt, c->dkind);
     NXD_CUDA(cudaGetLastError());
     return NXD_OK;
 }
@@ -511,13 +514,29 @@ nxd_status nxd_create(const nxd_scene_desc* d, nxd_ctx** out) {
     std::vector<int> da(c->D), db(c->D);
     std::vector<Drv> dprm(c->D);
     std::vector<double> dfilt(c->D);
+    std::vector<int> dkind(c->D, NXD_DRIVE_ANGULAR_VELOCITY);
     for (int k = 0; k < c->D; ++k) {
+        const int kind = d->drive_kind ? d->drive_kind[k] : NXD_DRIVE_ANGULAR_VELOCITY;
+        dkind[k] = kind;
         da[k] = d->drive_body_a[k] >= 0 ? idx_of(d->drive_body_a[k]) : -1;
         db[k] = idx_of(d->drive_body_b[k]);
-        if (db[k] < 0) { c->mem.release(); delete c; return NXD_INVALID_ARGUMENT; }
+        // the loader's checks (SceneLoader.cpp:274-446): body_b must exist (an
+        // unknown body_a is the world), a spring needs both bodies; a form
+        // coupling a body to itself is refused
+        const bool bad = kind < NXD_DRIVE_ANGULAR_VELOCITY || kind > NXD_DRIVE_DAMPED_SPRING || db[k] < 0 ||
+                         da[k] == db[k] ||
+                         (kind == NXD_DRIVE_DAMPED_SPRING && da[k] < 0) || (kind == NXD_DRIVE_FORCE && da[k] >= 0);
+        if (bad) { c->mem.release(); delete c; return NXD_INVALID_ARGUMENT; }
         const double* p = d->drive_params + 8 * k;
-        const V3 ax = normalized(v3(p[0], p[1], p[2]));
-        dprm[k] = Drv{ax.x, ax.y, ax.z, p[3], p[4], p[5] <= 0.0 ? INFINITY : p[5], std::max(0.0, p[6]), std::max(0.0, p[7])};
+        if (kind == NXD_DRIVE_FORCE || kind == NXD_DRIVE_DAMPED_SPRING) {
+            dprm[k] = Drv{p[0], p[1], p[2], p[3], p[4], p[5], 0.0, 0.0};
+        } else {
+            // constructors normalise the axis; setMaxForce / setMaxTorque map
+            // <= 0 to unlimited; setDelay / setDeadzone / setDelayTau clamp at 0
+            const V3 ax = normalized(v3(p[0], p[1], p[2]));
+            const double tau = kind == NXD_DRIVE_POSITION ? 0.0 : std::max(0.0, p[7]);
+            dprm[k] = Drv{ax.x, ax.y, ax.z, p[3], p[4], p[5] <= 0.0 ? INFINITY : p[5], std::max(0.0, p[6]), tau};
+        }
         dfilt[k] = p[4];
         if (da[k] >= 0) dinc_l[da[k]].push_back(2 * k);
         dinc_l[db[k]].push_back(2 * k + 1);
@@ -575,6 +594,7 @@ nxd_status nxd_create(const nxd_scene_desc* d, nxd_ctx** out) {
     c->jlam = m.upload(jlam.data(), jlam.size());
     c->jinc_off = m.upload(jinc_off.data(), N + 1); c->jinc = m.upload(jinc.data(), jinc.size());
     c->da = m.upload(da.data(), c->D); c->db = m.upload(db.data(), c->D); c->dprm = m.upload(dprm.data(), c->D);
+    c->dkind = m.upload(dkind.data(), c->D); c->dDir = m.alloc<double>(3 * c->D);
     c->dfilt = m.upload(dfilt.data(), c->D); c->dfinit = m.alloc<int>(c->D); c->dhas_prev = m.alloc<int>(c->D);
     c->dprevA = m.alloc<double>(3 * c->D); c->dprevB = m.alloc<double>(3 * c->D);
     c->dinc_off = m.upload(dinc_off.data(), N + 1); c->dinc = m.upload(dinc.data(), dinc.size());

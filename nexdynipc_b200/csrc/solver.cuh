@@ -41,7 +41,15 @@ constexpr int kMaxComponentBodies = 2048;   // structure masks of <= 64 words pe
 constexpr int kMaxIncidence = 4096;          // 2 x kMaxContacts contact ends, sorted in shared memory
 static_assert(2 * kMaxContacts <= kMaxIncidence, "contact incidence sort buffer too small");
 
-struct Drv {   // velocity drive parameters (VelocityDriveForm)
+// Control-form parameters (8 doubles, the nxd_scene_desc layout after the
+// creation-time normalisation):
+//   angular / linear velocity drive: axis, kv, v_target, max torque / force
+//     (inf: unlimited), delay deadzone, delay filter time constant
+//   position drive: axis, kp (kv), target position (vt), max force (maxT),
+//     deadzone (delay)
+//   force drive: force (ax, ay, az), torque (kv, vt, maxT)
+//   damped spring: rest length (ax), stiffness (ay), damping (az)
+struct Drv {
     double ax, ay, az, kv, vt, maxT, delay, tau;
 };
 
@@ -59,6 +67,9 @@ struct Solver {
     const int* da; const int* db; const Drv* dprm;
     double* dprevA; double* dprevB; int* dhas_prev; const double* dfilt;
     const int* dinc_off; const int* dinc;         // body -> (drive*2+side)
+    const int* dkind;                             // [D] NXD_DRIVE_*
+    double* dDir;                                 // [3D] spring direction of the last gradient / Hessian call
+    const double* bvel;                           // [3N] body velocities of the step start (DampedSpringForm)
     // contacts
     const ContactRec* contacts; const int* ncontacts_ptr;
     const double* nforce; const int* nnf_ptr;
@@ -557,7 +568,12 @@ __device__ void friction_eval(const Solver& S, int c, const double* x, bool full
         }
 }
 
-// VelocityDriveForm (VelocityDriveForm.cpp:61-417), stateful joint velocity.
+// Control forms.  VelocityDriveForm (VelocityDriveForm.cpp:61-417) and
+// LinearVelocityDriveForm (LinearVelocityDriveForm.cpp:56-280) share the
+// stateful joint velocity, on the rotation or the translation part of x;
+// PositionDriveForm (PositionDriveForm.cpp:66-172), ForceDriveForm
+// (ForceDriveForm.cpp:22-40) and DampedSpringForm (DampedSpringForm.cpp:30-112)
+// are stateless.
 __device__ double drive_target(const Drv& p, double filt) { return p.tau <= 0.0 ? p.vt : filt; }
 __device__ double drive_dead(const Drv& p, double e) {
     if (p.delay <= 0.0) return e;
@@ -573,8 +589,9 @@ __device__ double drive_sat(const Drv& p, double e) {
 }
 __device__ double drive_velocity(const Solver& S, int d, const double* x) {
     const int A = S.da[d], B = S.db[d];
-    const V3 tA = A >= 0 ? xs3(x, 6 * A + 3) : v3(0, 0, 0);
-    const V3 tB = B >= 0 ? xs3(x, 6 * B + 3) : v3(0, 0, 0);
+    const int o = S.dkind[d] == NXD_DRIVE_LINEAR_VELOCITY ? 0 : 3;
+    const V3 tA = A >= 0 ? xs3(x, 6 * A + o) : v3(0, 0, 0);
+    const V3 tB = B >= 0 ? xs3(x, 6 * B + o) : v3(0, 0, 0);
     const double dt = *S.dt_ptr;
     V3 oA = v3(0, 0, 0), oB = v3(0, 0, 0);
     if (S.dhas_prev[d]) {
@@ -588,20 +605,84 @@ __device__ double drive_velocity(const Solver& S, int d, const double* x) {
     S.dhas_prev[d] = 1;
     return v;
 }
-// mode 0 value, 1 gradient, 2 hessian (stateful as in the reference)
+// PositionDriveForm::getPositionError
+__device__ double position_error(const Solver& S, int d, const double* x) {
+    const int A = S.da[d], B = S.db[d];
+    const V3 pA = A >= 0 ? xs3(x, 6 * A) : v3(0, 0, 0);
+    const V3 pB = B >= 0 ? xs3(x, 6 * B) : v3(0, 0, 0);
+    const Drv& p = S.dprm[d];
+    return p.vt - dot(pB - pA, v3(p.ax, p.ay, p.az));
+}
+// DampedSpringForm::springDirection: unit x for a degenerate spring
+__device__ V3 spring_direction(const Solver& S, int d, const double* x, double& length) {
+    const V3 dv = xs3(x, 6 * S.db[d]) - xs3(x, 6 * S.da[d]);
+    length = norm(dv);
+    if (length < 1e-12) return v3(1.0, 0.0, 0.0);
+    return dv / length;
+}
+// value of a drive with effective error e and the saturating potential
+// (m^2/k) log cosh(k e / m) when the limit m is finite
+__device__ double drive_potential(const Drv& p, double e) {
+    if (!isfinite(p.maxT)) return 0.5 * p.kv * e * e;
+    if (p.kv <= 0.0 || p.maxT <= 0.0) return 0.0;
+    const double s = (p.kv * e) / p.maxT;
+    return (p.maxT * p.maxT / p.kv) * nxm::log(nxm::cosh(s));
+}
+// mode 0 value (dE), 1 gradient scalar (dG), 2 Hessian scalar (dH); the
+// velocity drives are stateful as in the reference
 __device__ void drive_eval(const Solver& S, int d, const double* x, int mode) {
     const Drv& p = S.dprm[d];
+    const int kind = S.dkind[d];
     const double dt = *S.dt_ptr;
+    if (kind == NXD_DRIVE_FORCE) {
+        if (mode == 0) S.dE[d] = 0.0;
+        return;
+    }
+    if (kind == NXD_DRIVE_DAMPED_SPRING) {
+        double len;
+        const V3 dir = spring_direction(S, d, x, len);
+        const double e = len - p.ax;
+        if (mode == 0) { S.dE[d] = 0.5 * p.ay * e * e; return; }
+        st3(S.dDir + 3 * d, dir);
+        if (mode == 1) {
+            const double vrel = dot(ld3(S.bvel + 3 * S.db[d]) - ld3(S.bvel + 3 * S.da[d]), dir);
+            S.dG[d] = p.ay * e + p.az * vrel;
+        } else {
+            S.dH[d] = p.ay;
+        }
+        return;
+    }
+    if (kind == NXD_DRIVE_POSITION) {
+        const double err = position_error(S, d, x);
+        if (mode == 0) S.dE[d] = drive_potential(p, drive_dead(p, err));
+        else if (mode == 1) S.dG[d] = drive_sat(p, drive_dead(p, err));
+        else {
+            double h = p.kv;
+            if (isfinite(p.maxT) && p.kv > 0.0 && p.maxT > 0.0) {
+                if (fabs(err) <= p.delay) h = 0.0;
+                else {
+                    const double sv = (p.kv * drive_dead(p, err)) / p.maxT;
+                    const double th = nxm::tanh(sv);
+                    h = p.kv * (1.0 - th * th);
+                }
+            }
+            S.dH[d] = h;
+        }
+        return;
+    }
     const double tgt = drive_target(p, S.dfilt[d]);
+    const bool linear = kind == NXD_DRIVE_LINEAR_VELOCITY;
     if (mode == 0) {
         const double v = drive_velocity(S, d, x);
-        const double e = drive_dead(p, tgt - v);
-        double val;
-        if (!isfinite(p.maxT)) val = 0.5 * p.kv * e * e;
-        else if (p.kv <= 0.0 || p.maxT <= 0.0) val = 0.0;
-        else { const double s = (p.kv * e) / p.maxT; val = (p.maxT * p.maxT / p.kv) * nxm::log(nxm::cosh(s)); }
-        S.dE[d] = val;
+        S.dE[d] = drive_potential(p, drive_dead(p, tgt - v));
     } else if (mode == 1) {
+        if (linear) {
+            // LinearVelocityDriveForm::gradient: nothing (and no state update) for dt <= 0
+            if (dt <= 0) { S.dG[d] = 0.0; return; }
+            const double v = drive_velocity(S, d, x);
+            S.dG[d] = drive_sat(p, drive_dead(p, tgt - v)) / dt;
+            return;
+        }
         const double v = drive_velocity(S, d, x);
         const double e = drive_dead(p, tgt - v);
         const double tq = drive_sat(p, e);
@@ -614,13 +695,56 @@ __device__ void drive_eval(const Solver& S, int d, const double* x, int mode) {
             if (fabs(e) <= p.delay) H = 0.0;
             else {
                 const double ee = drive_dead(p, e);
-                const double s = (p.kv * ee) / p.maxT;
-                const double th = nxm::tanh(s);
+                const double sv = (p.kv * ee) / p.maxT;
+                const double th = nxm::tanh(sv);
                 H = (p.kv * (1.0 - th * th)) / (dt * dt);
             }
         }
         S.dH[d] = H;
     }
+}
+// Gradient term of drive d at DOF k of its body on `side` (1: body_b): the
+// value c the form adds (+1) to or subtracts (-1) from its zeroed gradient,
+// or 0 when the form leaves that DOF alone.
+__device__ int drive_grad_term(const Solver& S, int d, int side, int k, double& c) {
+    const Drv& p = S.dprm[d];
+    switch (S.dkind[d]) {
+        case NXD_DRIVE_ANGULAR_VELOCITY:
+            if (k < 3) return 0;
+            c = S.dG[d] * (k == 3 ? p.ax : (k == 4 ? p.ay : p.az));
+            return side == 1 ? 1 : -1;
+        case NXD_DRIVE_LINEAR_VELOCITY:
+        case NXD_DRIVE_POSITION:
+            if (k >= 3) return 0;
+            c = S.dG[d] * (k == 0 ? p.ax : (k == 1 ? p.ay : p.az));
+            return side == 1 ? -1 : 1;
+        case NXD_DRIVE_FORCE: {
+            const double f[6] = {p.ax, p.ay, p.az, p.kv, p.vt, p.maxT};
+            c = f[k];
+            return -1;
+        }
+        default:
+            if (k >= 3) return 0;
+            c = S.dG[d] * S.dDir[3 * d + k];
+            return side == 1 ? 1 : -1;
+    }
+}
+// Translational Hessian entry (h a_r) a_c of a two-body drive (linear and
+// position drives: axis; spring: direction), or false when the form emits no
+// block (h == 0 for the drives)
+__device__ __forceinline__ bool drive_trans_h(const Solver& S, int d, int r, int cc, double& h) {
+    const int kind = S.dkind[d];
+    if (kind == NXD_DRIVE_DAMPED_SPRING) {
+        const double* a = S.dDir + 3 * d;
+        h = (S.dH[d] * a[r]) * a[cc];
+        return true;
+    }
+    if (kind != NXD_DRIVE_LINEAR_VELOCITY && kind != NXD_DRIVE_POSITION) return false;
+    if (S.dH[d] == 0.0) return false;
+    const Drv& p = S.dprm[d];
+    const double a[3] = {p.ax, p.ay, p.az};
+    h = (S.dH[d] * a[r]) * a[cc];
+    return true;
 }
 
 // poses at x for every body (joint-style and friction-style rotations)
@@ -714,13 +838,12 @@ __device__ void gradient_dof(const Solver& S, const double* x, double s, int i, 
         t += a;
     }
     g += t;
-    // drives, each its own form
+    // control forms, each its own form (its zeroed gradient, scaled, added)
     for (int q = S.dinc_off[i]; q < S.dinc_off[i + 1]; ++q) {
-        if (k < 3) { g += s * 0.0; continue; }
         const int d = S.dinc[q] >> 1, side = S.dinc[q] & 1;
-        const Drv& p = S.dprm[d];
-        const double c = S.dG[d] * (k == 3 ? p.ax : (k == 4 ? p.ay : p.az));
-        const double tk = side == 1 ? 0.0 + c : 0.0 - c;
+        double c = 0.0;
+        const int sg = drive_grad_term(S, d, side, k, c);
+        const double tk = sg == 0 ? 0.0 : (sg > 0 ? 0.0 + c : 0.0 - c);
         g += s * tk;
     }
     double cb = 0.0, cf = 0.0;
@@ -840,8 +963,14 @@ __device__ void diag_hessian_row(const Solver& S, double s, int i, int a, bool b
     }
     for (int q = S.dinc_off[i]; q < S.dinc_off[i + 1]; ++q) {
         const int d = S.dinc[q] >> 1;
-        if (S.dH[d] == 0.0) continue;
-        if (a >= 3) for (int b = 0; b < 3; ++b) H[3 + b] += drive_h(S, d, a - 3, b, s);
+        if (S.dkind[d] == NXD_DRIVE_ANGULAR_VELOCITY) {
+            if (S.dH[d] == 0.0) continue;
+            if (a >= 3) for (int b = 0; b < 3; ++b) H[3 + b] += drive_h(S, d, a - 3, b, s);
+        } else if (a < 3) {
+            double h;
+            for (int b = 0; b < 3; ++b)
+                if (drive_trans_h(S, d, a, b, h)) H[b] += h * s;
+        }
     }
     if (!(bar || fr)) return;
     if (bar && a < 3)
@@ -871,10 +1000,17 @@ __device__ void gather_diag_hessian(const Solver& S, double s, int C) {
 }
 
 // Coupling block entry e (row-major 6x6) of item `it` with rows of body R
-// and cols of body Cb (R != Cb).  Items: [0,J) joints, [J, J+C) barrier
-// contacts, [J+C, J+2C) friction contacts.
+// and cols of body Cb (R != Cb).  Items, in the order their triplets reach
+// the Hessian: [0,J) joints, [J,J+D) control forms, [J+D, J+D+C) barrier
+// contacts, [J+D+C, J+D+2C) friction contacts.
 __device__ double coupling_entry(const Solver& S, int it, int R, int Cb, double s, int C, int e) {
     const int ra = e / 6, cb = e % 6;
+    if (it >= S.J && it < S.J + S.D) {
+        // two-body control form: -(h a_ra) a_cb in both off-diagonal blocks
+        double h;
+        if (ra >= 3 || cb >= 3 || !drive_trans_h(S, it - S.J, ra, cb, h)) return 0.0;
+        return (-h) * s;
+    }
     if (it < S.J) {
         const int j = it;
         if (S.jtype[j] == NXD_JOINT_ANGLE_LIMIT)
@@ -888,13 +1024,14 @@ __device__ double coupling_entry(const Solver& S, int it, int R, int Cb, double 
         for (int r = 0; r < dim; ++r) acc += Jd[12 * r + 6 * sr + ra] * Jd[12 * r + 6 * sc + cb];
         return acc * S.jmu[j];
     }
-    if (it < S.J + C) {
+    const int J2 = S.J + S.D;
+    if (it < J2 + C) {
         if (ra >= 3 || cb >= 3) return 0.0;
-        const int c = it - S.J;
+        const int c = it - J2;
         const double* n = S.contacts[c].normal;
         return (-(S.bHP[c] * (n[ra] * n[cb]))) * s;
     }
-    const int c = it - S.J - C;
+    const int c = it - J2 - C;
     const int sx = S.contacts[c].body_a == R ? 0 : 1, sy = S.contacts[c].body_a == Cb ? 0 : 1;
     const double* Jx = (sx == 0 ? S.fJA : S.fJB) + 18 * c;
     const double* Jy = (sy == 0 ? S.fJA : S.fJB) + 18 * c;
@@ -911,21 +1048,33 @@ __device__ void add_coupling_block(const Solver& S, int it, int R, int Cb, doubl
         const int ra = e / 6, cb = e % 6;
         const bool touches = it < S.J ? (S.jtype[it] == NXD_JOINT_ANGLE_LIMIT ? (ra >= 3 && cb >= 3)
                                          : (S.jtype[it] == NXD_JOINT_DISTANCE_LIMIT ? (ra < 3 && cb < 3) : true))
-                                      : (it < S.J + C ? (ra < 3 && cb < 3) : true);
+                                      : (it < S.J + S.D + C ? (ra < 3 && cb < 3) : true);
         if (touches) out[e] += coupling_entry(S, it, R, Cb, s, C, e);
     }
 }
 __device__ __forceinline__ void item_bodies(const Solver& S, int it, int& a, int& b) {
     if (it < S.J) { a = S.ja[it]; b = S.jb[it]; return; }
+    const int J2 = S.J + S.D;
+    if (it < J2) { a = S.da[it - S.J]; b = S.db[it - S.J]; return; }
     const int C = *S.ncontacts_ptr;
-    const int c = it < S.J + C ? it - S.J : it - S.J - C;
+    const int c = it < J2 + C ? it - J2 : it - J2 - C;
     a = S.contacts[c].body_a; b = S.contacts[c].body_b;
+}
+// a control form couples its two bodies when it emits off-diagonal blocks:
+// the spring always, the linear and position drives when h != 0
+__device__ __forceinline__ bool drive_couples(const Solver& S, int d) {
+    if (S.da[d] < 0) return false;
+    const int kind = S.dkind[d];
+    if (kind == NXD_DRIVE_DAMPED_SPRING) return true;
+    return (kind == NXD_DRIVE_LINEAR_VELOCITY || kind == NXD_DRIVE_POSITION) && S.dH[d] != 0.0;
 }
 __device__ __forceinline__ bool item_active(const Solver& S, int it) {
     if (it < S.J) return joint_couples(S, it);
+    const int J2 = S.J + S.D;
+    if (it < J2) return drive_couples(S, it - S.J);
     const int C = *S.ncontacts_ptr;
-    if (it < S.J + C) return *S.barrier_in_forms_ptr != 0 && S.bD[it - S.J] < *S.bdhat_ptr;
-    const int c = it - S.J - C;
+    if (it < J2 + C) return *S.barrier_in_forms_ptr != 0 && S.bD[it - J2] < *S.bdhat_ptr;
+    const int c = it - J2 - C;
     return *S.friction_form_ptr != 0 && friction_on(S, c);
 }
 
@@ -1490,7 +1639,7 @@ __device__ void grid_energies(const Solver& S, const double* x, double s, int C,
 // Solve H dx = -g over the grid.  Returns false (all threads) on failure.
 __device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, int* sh_scan, int* sh_flag) {
     const int N = S.N;
-    const int n_items = S.J + 2 * C;
+    const int n_items = S.J + S.D + 2 * C;
     NX_GRID_FOR(i, N + 1, gc) {
         if (i < N) S.parent[i] = i;
         S.mcnt[i] = 0; S.icnt[i] = 0; S.rflag[i] = 0;

@@ -321,10 +321,14 @@ __device__ __forceinline__ void update_state_body(const StepCfg& cfg, const doub
 constexpr int kLB_update_state = 0;
 __global__ void k_update_state(const __grid_constant__ StepCfg cfg, const double* x, const double* xprev, const double* vprev, const double* xhat, const double* aprev, double* pos, double* quat, double* vel, double* omega, double* lacc, double* aacc, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt) { update_state_body(cfg, x, xprev, vprev, xhat, aprev, pos, quat, vel, omega, lacc, aacc, sc, da, db, dprm, dfilt); }
 
-__device__ __forceinline__ void drive_kpi_body(const StepCfg& cfg, const double* omega, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt) {
+// angular-velocity-drive KPIs (IPCSolver.cpp:1197-1215): only
+// VelocityDriveForms are counted
+__device__ __forceinline__ void drive_kpi_body(const StepCfg& cfg, const double* omega, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt, const int* dkind) {
     double max_vw = 0.0;
-    int sat = 0;
+    int sat = 0, count = 0;
     for (int d = 0; d < cfg.D; ++d) {
+        if (dkind[d] != NXD_DRIVE_ANGULAR_VELOCITY) continue;
+        ++count;
         const Drv& p = dprm[d];
         const V3 oA = da[d] >= 0 ? ld3(omega + 3 * da[d]) : v3(0, 0, 0);
         const V3 oB = ld3(omega + 3 * db[d]);
@@ -336,10 +340,10 @@ __device__ __forceinline__ void drive_kpi_body(const StepCfg& cfg, const double*
         }
     }
     sc->last_vw = max_vw;
-    sc->last_tsat = cfg.D > 0 ? (double)sat / cfg.D : 0.0;
+    sc->last_tsat = count > 0 ? (double)sat / count : 0.0;
 }
 constexpr int kLB_drive_kpi = 0;
-__global__ void k_drive_kpi(const __grid_constant__ StepCfg cfg, const double* omega, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt) { drive_kpi_body(cfg, omega, sc, da, db, dprm, dfilt); }
+__global__ void k_drive_kpi(const __grid_constant__ StepCfg cfg, const double* omega, Scalars* sc, const int* da, const int* db, const Drv* dprm, const double* dfilt, const int* dkind) { drive_kpi_body(cfg, omega, sc, da, db, dprm, dfilt, dkind); }
 
 }  // namespace nx
 
@@ -434,11 +438,11 @@ __global__ void __launch_bounds__(kSolverThreads) k_form_eval(Solver S, Scalars*
             if (m & FM_DRIVES)
                 for (int q = S.dinc_off[i]; q < S.dinc_off[i + 1]; ++q) {
                     const int d = S.dinc[q] >> 1, side = S.dinc[q] & 1;
-                    const Drv& p = S.dprm[d];
-                    const double ax[3] = {p.ax, p.ay, p.az};
-                    for (int k = 0; k < 3; ++k) {
-                        if (side == 1) g[3 + k] += S.dG[d] * ax[k];
-                        else g[3 + k] -= S.dG[d] * ax[k];
+                    for (int k = 0; k < 6; ++k) {
+                        double c = 0.0;
+                        const int sg = drive_grad_term(S, d, side, k, c);
+                        if (sg > 0) g[k] += c;
+                        else if (sg < 0) g[k] -= c;
                     }
                 }
             for (int q = S.cinc_off[i]; q < S.cinc_off[i + 1]; ++q) {
@@ -468,7 +472,7 @@ __global__ void __launch_bounds__(kSolverThreads) k_form_eval(Solver S, Scalars*
         if (threadIdx.x == 0) *nnzb = -1;   // only the total Hessian is exported
         return;
     }
-    const int n_items = S.J + 2 * C;
+    const int n_items = S.J + S.D + 2 * C;
     for (int i = threadIdx.x; i <= N; i += blockDim.x) row_ptr[i] = i < N ? 1 : 0;
     __syncthreads();
     for (int it = threadIdx.x; it < n_items; it += blockDim.x) {

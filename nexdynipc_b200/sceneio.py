@@ -12,11 +12,13 @@
 * run(path): Simulation::run's loop (t < max_time: step, export frame and
   KPIs) on the device.
 
-Joint and constraint kinds the device step implements: hinge (and its
-deprecated alias revolute), spherical, prismatic, cylindrical, fixed,
-angle_limit, distance_limit(s), angular_velocity_drive.  Scenes using the
-others (linear_velocity_drive, position_drive, force_drive, damped_spring)
-raise NotImplementedError naming them.
+Every joint and constraint kind of SceneLoader::parseJoint is loaded: hinge
+(and its deprecated alias revolute), spherical, prismatic, cylindrical, fixed,
+angle_limit, distance_limit(s), and the control forms angular_velocity_drive,
+linear_velocity_drive, position_drive, force_drive and damped_spring (kept in
+load order, as World::forms holds them).  Another type raises
+NotImplementedError naming it, where the reference prints "Ignoring
+unsupported constraint type".
 """
 from __future__ import annotations
 
@@ -30,9 +32,71 @@ import numpy as np
 from . import abi
 from .scenes import Scene
 
-_SUPPORTED = {"hinge", "revolute", "spherical", "fixed", "angle_limit", "angular_velocity_drive", "prismatic",
-              "cylindrical", "distance_limit", "distance_limits"}
-_KNOWN_UNSUPPORTED = {"linear_velocity_drive", "position_drive", "force_drive", "damped_spring"}
+_DRIVES = {"angular_velocity_drive", "linear_velocity_drive", "position_drive", "force_drive", "damped_spring"}
+_SUPPORTED = {"hinge", "revolute", "spherical", "fixed", "angle_limit", "prismatic", "cylindrical",
+              "distance_limit", "distance_limits"} | _DRIVES
+
+
+def _normalized(v):
+    """Eigen's normalized(): v / sqrt((x^2 + y^2) + z^2), v itself when zero."""
+    x, y, z = (float(t) for t in v)
+    n2 = x * x + y * y + z * z
+    if n2 > 0.0:
+        n = math.sqrt(n2)
+        return [x / n, y / n, z / n]
+    return [x, y, z]
+
+
+def _drive_entry(t, entry, index):
+    """(kind, body_a id or -1, body_b id, params[8]) of a control-form entry
+    (SceneLoader.cpp:274-446), or None where the loader ignores it."""
+    q = np.zeros(8)
+    g = entry.get
+    if t == "force_drive":
+        b = int(g("body", g("body_b", -1)))
+        if b not in index:
+            return None               # "Ignoring force_drive with invalid body id"
+        if "force" in entry:
+            q[0:3] = _vec(entry["force"])
+        elif "axis" in entry:
+            fn = float(g("force_n", g("force_magnitude", 0.0)))
+            q[0:3] = [a * fn for a in _normalized(entry["axis"])]
+        if "torque" in entry:
+            q[3:6] = _vec(entry["torque"])
+        return abi.NXD_DRIVE_FORCE, -1, b, q
+    if t == "damped_spring":
+        a, b = int(g("body_a", -1)), int(g("body_b", -1))
+        if a not in index or b not in index:
+            return None               # "Ignoring damped_spring with invalid body id"
+        q[0] = float(g("rest_length_m", g("rest_length", 0.0)))
+        q[1] = float(g("stiffness_npm", g("stiffness", 0.0)))
+        q[2] = float(g("damping_nspm", g("damping", 0.0)))
+        return abi.NXD_DRIVE_DAMPED_SPRING, a, b, q
+    a, b = int(entry["body_a"]), int(entry["body_b"])
+    if b not in index:
+        return None                   # "Ignoring <drive> with invalid body_b id"
+    q[0:3] = _vec(entry["axis"])
+    if t == "position_drive":
+        q[3] = float(g("kp", g("stiffness", 100.0)))
+        q[4] = float(g("target_position_m", g("target_position", 0.0)))
+        q[5] = float(g("max_force", g("max_force_n", 0.0)))
+        q[6] = float(g("deadzone", g("deadzone_m", 0.0)))
+        kind = abi.NXD_DRIVE_POSITION
+    elif t == "linear_velocity_drive":
+        q[3] = float(g("kv", g("stiffness", 100.0)))
+        q[4] = float(g("target_velocity_mps", g("target_velocity", 0.0)))
+        q[5] = float(g("max_force", g("max_force_n", 0.0)))
+        q[6] = float(g("delay", g("delay_mps", 0.0)))
+        q[7] = float(g("delay_tau", g("delay_seconds", 0.0)))
+        kind = abi.NXD_DRIVE_LINEAR_VELOCITY
+    else:
+        q[3] = float(g("kv", g("stiffness", 100.0)))
+        q[4] = float(g("target_velocity_radps", 0.0))
+        q[5] = float(g("max_torque", g("max_torque_nm", 0.0)))
+        q[6] = float(g("delay", g("delay_radps", 0.0)))
+        q[7] = float(g("delay_tau", g("delay_seconds", 0.0)))
+        kind = abi.NXD_DRIVE_ANGULAR_VELOCITY
+    return kind, (a if a in index else -1), b, q
 
 
 def load_obj(path: str):
@@ -150,7 +214,7 @@ def load_scene(path: str, dt: float | None = None):
     index = {bid: i for i, bid in enumerate(ids)}
 
     jt, ja, jb, jp, js = [], [], [], [], []
-    da, db, dp = [], [], []
+    da, db, dp, dk = [], [], [], []
     seen = set()
     for entry in list(doc.get("joints", [])) + list(doc.get("constraints", [])):
         if "type" not in entry:
@@ -203,18 +267,10 @@ def load_scene(path: str, dt: float | None = None):
             p[4] = float(entry.get("max_angle_deg", 180.0)) * math.pi / 180.0
             jt.append(abi.NXD_JOINT_ANGLE_LIMIT); ja.append(a); jb.append(b2)
             js.append(float(entry.get("stiffness", 1e5)))
-        else:   # angular_velocity_drive
-            a, b2 = int(entry["body_a"]), int(entry["body_b"])
-            if b2 not in index:
-                continue              # "Ignoring angular_velocity_drive with invalid body_b id"
-            q = np.zeros(8)
-            q[0:3] = _vec(entry["axis"])
-            q[3] = float(entry.get("kv", entry.get("stiffness", 100.0)))
-            q[4] = float(entry.get("target_velocity_radps", 0.0))
-            q[5] = float(entry.get("max_torque", entry.get("max_torque_nm", 0.0)))
-            q[6] = float(entry.get("delay", entry.get("delay_radps", 0.0)))
-            q[7] = float(entry.get("delay_tau", entry.get("delay_seconds", 0.0)))
-            da.append(a if a in index else -1); db.append(b2); dp.append(q)
+        else:   # control forms
+            d = _drive_entry(t, entry, index)
+            if d is not None:
+                dk.append(d[0]); da.append(d[1]); db.append(d[2]); dp.append(d[3])
             continue
         jp.append(p)
 
@@ -290,6 +346,7 @@ def load_scene(path: str, dt: float | None = None):
         joint_stiffness=np.asarray(js, dtype=np.float64).reshape(nj),
         drive_body_a=np.asarray(da, dtype=np.int32).reshape(nd), drive_body_b=np.asarray(db, dtype=np.int32).reshape(nd),
         drive_params=np.ascontiguousarray(np.asarray(dp, dtype=np.float64).reshape(nd, 8)),
+        drive_kind=np.asarray(dk, dtype=np.int32).reshape(nd),
         settings=s, dt=float(cfg.dt if dt is None else dt), steps=int(math.ceil(cfg.max_time / cfg.dt - 1e-12)),
         body_ids=np.asarray(ids, dtype=np.int32), body_names=names,
         contact_pairs=np.asarray([(a, b) for a, b, _ in pairs], dtype=np.int32).reshape(-1, 2) if pairs else None,

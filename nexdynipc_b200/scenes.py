@@ -185,6 +185,7 @@ class Scene:
     body_names: list = None
     contact_pairs: np.ndarray = None            # [n, 2] body ids (IPCSolver::addAllowedContactPair)
     contact_pair_friction: np.ndarray = None    # [n], < 0: no override
+    drive_kind: np.ndarray = None               # [n_drives] NXD_DRIVE_* (default: all angular velocity)
 
     @property
     def n_bodies(self) -> int:
@@ -228,6 +229,9 @@ class Scene:
         d.drive_body_a = abi.iptr(self.drive_body_a)
         d.drive_body_b = abi.iptr(self.drive_body_b)
         d.drive_params = abi.dptr(self.drive_params)
+        if self.drive_kind is not None and len(self.drive_kind):
+            self._dk = np.ascontiguousarray(self.drive_kind, dtype=np.int32)
+            d.drive_kind = abi.iptr(self._dk)
         d.settings = self.settings
         if self.contact_pairs is not None and len(self.contact_pairs):
             self._cp = np.ascontiguousarray(self.contact_pairs, dtype=np.int32).reshape(-1, 2)
@@ -251,7 +255,7 @@ class SceneBuilder:
         self.name = name
         self.bodies = []     # dicts
         self.joints = []     # (type, a, b, params[16], stiffness)
-        self.drives = []     # (a, b, params[8])
+        self.drives = []     # (a, b, params[8], kind)
 
     def add_body(self, verts, faces, pos, quat=(1, 0, 0, 0), vel=(0, 0, 0), omega=(0, 0, 0),
                  mass=None, inertia=None, density=1000.0, recentre=True):
@@ -309,7 +313,29 @@ class SceneBuilder:
         p = np.zeros(8)
         p[0:3] = axis
         p[3:8] = (kv, v_target, max_torque, delay, delay_tau)
-        self.drives.append((a, b, p))
+        self.drives.append((a, b, p, abi.NXD_DRIVE_ANGULAR_VELOCITY))
+
+    def linear_velocity_drive(self, a, b, axis, kv, v_target, max_force=0.0, delay=0.0, delay_tau=0.0):
+        p = np.zeros(8)
+        p[0:3] = axis
+        p[3:8] = (kv, v_target, max_force, delay, delay_tau)
+        self.drives.append((a, b, p, abi.NXD_DRIVE_LINEAR_VELOCITY))
+
+    def position_drive(self, a, b, axis, kp, target, max_force=0.0, deadzone=0.0):
+        p = np.zeros(8)
+        p[0:3] = axis
+        p[3:7] = (kp, target, max_force, deadzone)
+        self.drives.append((a, b, p, abi.NXD_DRIVE_POSITION))
+
+    def force_drive(self, b, force, torque=(0.0, 0.0, 0.0)):
+        p = np.zeros(8)
+        p[0:3], p[3:6] = force, torque
+        self.drives.append((-1, b, p, abi.NXD_DRIVE_FORCE))
+
+    def damped_spring(self, a, b, rest_length, stiffness, damping):
+        p = np.zeros(8)
+        p[0:3] = (rest_length, stiffness, damping)
+        self.drives.append((a, b, p, abi.NXD_DRIVE_DAMPED_SPRING))
 
     def build(self, settings, dt, steps) -> Scene:
         n = len(self.bodies)
@@ -339,6 +365,7 @@ class SceneBuilder:
             drive_body_a=np.array([d[0] for d in self.drives], dtype=np.int32).reshape(nd),
             drive_body_b=np.array([d[1] for d in self.drives], dtype=np.int32).reshape(nd),
             drive_params=np.ascontiguousarray(np.array([d[2] for d in self.drives]).reshape(nd, 8)),
+            drive_kind=np.array([d[3] for d in self.drives], dtype=np.int32).reshape(nd),
             settings=settings, dt=dt, steps=steps)
 
 
@@ -500,6 +527,36 @@ def batched_scenes(seed: int = 4000, n_scenes: int = 256):
                     count += 1
         scenes.append(sb.build(_settings(1e-3, mu), dt=1e-2, steps=100))
     return scenes
+
+
+def control_forms(seed: int = 6000, dhat: float = 1e-3, mu: float = 0.4) -> Scene:
+    """Every control form of World::forms on 0.1 m boxes over a static ground
+    box: a damped spring from a fixed anchor, a saturating position drive
+    with a deadzone to the world and one between two boxes, a torque-limited
+    linear velocity drive with a target filter, an angular velocity drive, and
+    a force drive with a torque; dt 1e-2, 60 steps."""
+    rng = np.random.default_rng(seed)
+    sb = SceneBuilder("control_forms")
+    gv, gf = box_mesh(2.0, 0.25, 2.0)
+    g = sb.add_body(gv, gf, (0.0, -0.25, 0.0))
+    sb.fix(g)
+    bv, bf = box_mesh(0.05, 0.05, 0.05)
+    anchor = sb.add_body(bv, bf, (0.0, 1.2, 0.0))
+    sb.fix(anchor)
+    jit = lambda: rng.uniform(-0.02, 0.02, size=3)
+    hang = sb.add_body(bv, bf, (0.05, 0.85, 0.02) + jit(), vel=(0.2, 0.0, -0.1))
+    slide = sb.add_body(bv, bf, (0.4, 0.05 + dhat / 2, 0.0) + jit() * (1, 0, 1))
+    follow = sb.add_body(bv, bf, (0.7, 0.05 + dhat / 2, 0.1) + jit() * (1, 0, 1))
+    spin = sb.add_body(bv, bf, (-0.4, 0.05 + dhat / 2, -0.2) + jit() * (1, 0, 1))
+    push = sb.add_body(bv, bf, (-0.6, 0.3, 0.3) + jit(), omega=(0.0, 0.5, 0.0))
+    sb.damped_spring(anchor, hang, rest_length=0.3, stiffness=400.0, damping=2.0)
+    sb.position_drive(-1, slide, (1.0, 0.0, 0.2), kp=60.0, target=0.55, max_force=4.0, deadzone=0.01)
+    sb.linear_velocity_drive(slide, follow, (1.0, 0.0, 0.0), kv=0.05, v_target=-0.2, max_force=0.5,
+                             delay=0.01, delay_tau=0.05)
+    sb.velocity_drive(g, spin, (0.0, 1.0, 0.0), kv=0.002, v_target=0.5, max_torque=0.01)
+    sb.force_drive(push, (0.3, 4.0, 0.0), torque=(0.0, 0.0, 0.02))
+    sb.position_drive(hang, push, (0.0, 1.0, 0.0), kp=25.0, target=-0.4)
+    return sb.build(_settings(dhat, mu), dt=1e-2, steps=60)
 
 
 def diff_scene(seed: int = 5000) -> Scene:

@@ -305,9 +305,16 @@ struct Joint {
     bool is_limit() const { return type == NXD_JOINT_ANGLE_LIMIT || type == NXD_JOINT_DISTANCE_LIMIT; }
 };
 
+// Control form of World::forms.  The velocity and position drives use axis,
+// kv (kp), v_target (target position), max_torque (max force), delay
+// (deadzone) and delay_tau; the force drive force / torque; the spring
+// rest / k / c.
 struct Drive {
+    int kind = NXD_DRIVE_ANGULAR_VELOCITY;
     int bodyA = -1, bodyB = -1;    // world indices (-1: none)
     V3 axis; double kv = 0, v_target = 0, max_torque = kInf, delay = 0, delay_tau = 0;
+    V3 force, torque;
+    double rest = 0, k = 0, c = 0;
     double dt = 0.01;
     int gA = -1, gB = -1;
     V3 prevA, prevB; bool has_prev = false;
@@ -1334,12 +1341,18 @@ double drive_sat_torque(const Drive& d, double e) {
     if (d.max_torque <= 0.0) return raw;
     return d.max_torque * nxm::tanh(raw / d.max_torque);
 }
-V3 drive_theta(const std::vector<double>& x, int g) {
+// the joint coordinates a velocity drive differentiates: rotation vector
+// (VelocityDriveForm) or position (LinearVelocityDriveForm::extractPosition)
+V3 drive_coord(const Drive& d, const std::vector<double>& x, int g) {
+    if (d.kind == NXD_DRIVE_LINEAR_VELOCITY) {
+        if (g < 0 || g + 2 >= (int)x.size()) return mk(0, 0, 0);
+        return xseg(x, g);
+    }
     if (g < 0 || g + 5 >= (int)x.size()) return mk(0, 0, 0);
     return xseg(x, g + 3);
 }
 double drive_joint_velocity(Drive& d, const std::vector<double>& x) {
-    const V3 tA = drive_theta(x, d.gA), tB = drive_theta(x, d.gB);
+    const V3 tA = drive_coord(d, x, d.gA), tB = drive_coord(d, x, d.gB);
     V3 oA = mk(0, 0, 0), oB = mk(0, 0, 0);
     if (d.has_prev) {
         if (d.gA >= 0) oA = d.dt <= 0 ? mk(0, 0, 0) : (tA - d.prevA) / d.dt;
@@ -1349,15 +1362,84 @@ double drive_joint_velocity(Drive& d, const std::vector<double>& x) {
     d.prevA = tA; d.prevB = tB; d.has_prev = true;
     return v;
 }
-double drive_value(Drive& d, const std::vector<double>& x) {
-    const double v = drive_joint_velocity(d, x);
-    const double e = drive_deadzone(d, drive_effective_target(d) - v);
+// 0.5 k e^2, or (m^2/k) log cosh(k e / m) with a finite limit m
+// (VelocityDriveForm.cpp:300-318, LinearVelocityDriveForm.cpp:186-202,
+// PositionDriveForm.cpp:117-127)
+double drive_potential(const Drive& d, double e) {
     if (!std::isfinite(d.max_torque)) return 0.5 * d.kv * e * e;
     if (d.kv <= 0.0 || d.max_torque <= 0.0) return 0.0;
     const double s = (d.kv * e) / d.max_torque;
     return (d.max_torque * d.max_torque / d.kv) * nxm::log(nxm::cosh(s));
 }
-void drive_gradient(Drive& d, const std::vector<double>& x, std::vector<double>& g) {
+// PositionDriveForm::getPositionError (PositionDriveForm.cpp:66-81)
+double position_error(const Drive& d, const std::vector<double>& x) {
+    V3 pA = mk(0, 0, 0), pB = mk(0, 0, 0);
+    if (d.gA >= 0 && d.gA + 2 < (int)x.size()) pA = xseg(x, d.gA);
+    if (d.gB >= 0 && d.gB + 2 < (int)x.size()) pB = xseg(x, d.gB);
+    return d.v_target - dot(pB - pA, d.axis);
+}
+// DampedSpringForm::springDirection (DampedSpringForm.cpp:37-46)
+V3 spring_direction(const Drive& d, const std::vector<double>& x, double& length) {
+    const V3 dv = xseg(x, d.gB) - xseg(x, d.gA);
+    length = norm(dv);
+    if (length < 1e-12) return mk(1.0, 0.0, 0.0);
+    return dv / length;
+}
+double drive_value(nxo_world* w, Drive& d, const std::vector<double>& x) {
+    (void)w;
+    switch (d.kind) {
+        case NXD_DRIVE_FORCE: return 0.0;
+        case NXD_DRIVE_DAMPED_SPRING: {
+            double len;
+            (void)spring_direction(d, x, len);
+            const double e = len - d.rest;
+            return 0.5 * d.k * e * e;
+        }
+        case NXD_DRIVE_POSITION: return drive_potential(d, drive_deadzone(d, position_error(d, x)));
+        default: {
+            const double v = drive_joint_velocity(d, x);
+            return drive_potential(d, drive_deadzone(d, drive_effective_target(d) - v));
+        }
+    }
+}
+void drive_gradient(nxo_world* w, Drive& d, const std::vector<double>& x, std::vector<double>& g) {
+    switch (d.kind) {
+        case NXD_DRIVE_FORCE:
+            // ForceDriveForm.cpp:27-35
+            if (d.gB < 0) return;
+            for (int i = 0; i < 3; ++i) g[d.gB + i] -= d.force[i];
+            for (int i = 0; i < 3; ++i) g[d.gB + 3 + i] -= d.torque[i];
+            return;
+        case NXD_DRIVE_DAMPED_SPRING: {
+            // DampedSpringForm.cpp:67-82: velocities of the bodies' state
+            double len;
+            const V3 dir = spring_direction(d, x, len);
+            const double e = len - d.rest;
+            const double vrel = dot(w->bodies[d.bodyB].velocity - w->bodies[d.bodyA].velocity, dir);
+            const double sc = d.k * e + d.c * vrel;
+            for (int i = 0; i < 3; ++i) g[d.gB + i] += sc * dir[i];
+            for (int i = 0; i < 3; ++i) g[d.gA + i] -= sc * dir[i];
+            return;
+        }
+        case NXD_DRIVE_POSITION: {
+            // PositionDriveForm.cpp:129-137
+            const double f = drive_sat_torque(d, drive_deadzone(d, position_error(d, x)));
+            if (d.gB >= 0) for (int i = 0; i < 3; ++i) g[d.gB + i] -= f * d.axis[i];
+            if (d.gA >= 0) for (int i = 0; i < 3; ++i) g[d.gA + i] += f * d.axis[i];
+            return;
+        }
+        case NXD_DRIVE_LINEAR_VELOCITY: {
+            // LinearVelocityDriveForm.cpp:204-219
+            if (d.dt <= 0.0) return;
+            const double v = drive_joint_velocity(d, x);
+            const double f = drive_sat_torque(d, drive_deadzone(d, drive_effective_target(d) - v));
+            const double coeff = f / d.dt;
+            if (d.gB >= 0) for (int i = 0; i < 3; ++i) g[d.gB + i] -= coeff * d.axis[i];
+            if (d.gA >= 0) for (int i = 0; i < 3; ++i) g[d.gA + i] += coeff * d.axis[i];
+            return;
+        }
+        default: break;
+    }
     const double v = drive_joint_velocity(d, x);
     const double e = drive_deadzone(d, drive_effective_target(d) - v);
     const double tq = drive_sat_torque(d, e);
@@ -1367,7 +1449,46 @@ void drive_gradient(Drive& d, const std::vector<double>& x, std::vector<double>&
     if (d.gB >= 0 && d.gB + 5 < (int)g.size()) for (int i = 0; i < 3; ++i) g[d.gB + 3 + i] += dEdq * d.axis[i];
     if (d.gA >= 0 && d.gA + 5 < (int)g.size()) for (int i = 0; i < 3; ++i) g[d.gA + 3 + i] -= dEdq * d.axis[i];
 }
+// h (a a^T) on the translation blocks: B, A, then the two off-diagonal
+// blocks with -h (a a^T), entry by entry; Eigen evaluates s (a a^T) as
+// (s a) a^T, so entry (i, j) is (h a_i) a_j
+void push_two_body_translation(const Drive& d, double h, V3 a, std::vector<Trip>& t) {
+    double H[3][3];
+    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) H[i][j] = (h * a[i]) * a[j];
+    if (d.gB >= 0) for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) t.push_back({d.gB + i, d.gB + j, H[i][j]});
+    if (d.gA >= 0) for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) t.push_back({d.gA + i, d.gA + j, H[i][j]});
+    if (d.gA >= 0 && d.gB >= 0)
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                t.push_back({d.gA + i, d.gB + j, -H[i][j]});
+                t.push_back({d.gB + i, d.gA + j, -H[i][j]});
+            }
+}
 void drive_hessian(Drive& d, const std::vector<double>& x, std::vector<Trip>& t) {
+    if (d.kind == NXD_DRIVE_FORCE) return;
+    if (d.kind == NXD_DRIVE_DAMPED_SPRING) {
+        // DampedSpringForm.cpp:84-112
+        double len;
+        const V3 dir = spring_direction(d, x, len);
+        push_two_body_translation(d, d.k, dir, t);
+        return;
+    }
+    if (d.kind == NXD_DRIVE_POSITION) {
+        // PositionDriveForm.cpp:139-170
+        double h = d.kv;
+        const double err = position_error(d, x);
+        if (std::isfinite(d.max_torque) && d.kv > 0.0 && d.max_torque > 0.0) {
+            if (std::fabs(err) <= d.delay) h = 0.0;
+            else {
+                const double s = (d.kv * drive_deadzone(d, err)) / d.max_torque;
+                const double th = nxm::tanh(s);
+                h = d.kv * (1.0 - th * th);
+            }
+        }
+        if (h == 0.0) return;
+        push_two_body_translation(d, h, d.axis, t);
+        return;
+    }
     if (d.dt <= 0) return;
     double H = d.kv / (d.dt * d.dt);
     if (std::isfinite(d.max_torque) && d.kv > 0.0 && d.max_torque > 0.0) {
@@ -1382,6 +1503,11 @@ void drive_hessian(Drive& d, const std::vector<double>& x, std::vector<Trip>& t)
         }
     }
     if (H == 0.0) return;
+    if (d.kind == NXD_DRIVE_LINEAR_VELOCITY) {
+        // LinearVelocityDriveForm.cpp:221-270
+        push_two_body_translation(d, H, d.axis, t);
+        return;
+    }
     for (int side = 0; side < 2; ++side) {
         const int g = side == 0 ? d.gB : d.gA;
         if (g < 0) continue;
@@ -1634,7 +1760,7 @@ double constraint_value(nxo_world* w, const std::vector<double>& x) {
 }
 double drives_value(nxo_world* w, const std::vector<double>& x) {
     std::vector<double> ev;
-    for (auto& d : w->drives) ev.push_back(drive_value(d, x));
+    for (auto& d : w->drives) ev.push_back(drive_value(w, d, x));
     return tree_sum(ev);
 }
 
@@ -1651,7 +1777,7 @@ double problem_value(nxo_world* w, const std::vector<double>& x) {
     v += s * gravity_value(w, x);
     v += constraint_value(w, x);
     // world.forms: drives, then barrier (if pushed), then friction
-    for (auto& d : w->drives) v += s * drive_value(d, x);
+    for (auto& d : w->drives) v += s * drive_value(w, d, x);
     if (w->barrier_in_forms) v += s * barrier_form_value(w, x);
     if (w->friction_form) v += s * friction_form_value(w, x);
     return v;
@@ -1671,7 +1797,7 @@ void problem_gradient(nxo_world* w, const std::vector<double>& x, std::vector<do
     for (size_t i = 0; i < n; ++i) g[i] += t[i];
     for (auto& d : w->drives) {
         std::fill(t.begin(), t.end(), 0.0);
-        drive_gradient(d, x, t);
+        drive_gradient(w, d, x, t);
         for (size_t i = 0; i < n; ++i) g[i] += s * t[i];
     }
     if (w->barrier_in_forms) {
@@ -2114,6 +2240,7 @@ void step(nxo_world* w, double dt) {
     double max_vw = 0.0;
     int dc = 0, sat = 0;
     for (auto& d : w->drives) {
+        if (d.kind != NXD_DRIVE_ANGULAR_VELOCITY) continue;   // VelocityDriveForms only
         ++dc;
         V3 oA = d.bodyA >= 0 ? w->bodies[d.bodyA].angular_velocity : mk(0, 0, 0);
         V3 oB = w->bodies[d.bodyB].angular_velocity;
@@ -2224,13 +2351,24 @@ nxo_world* nxo_create(const nxd_scene_desc* d) {
     for (int k = 0; k < d->n_drives; ++k) {
         Drive D;
         const double* p = d->drive_params + (size_t)NXD_DRIVE_PARAMS * k;
+        D.kind = d->drive_kind ? d->drive_kind[k] : NXD_DRIVE_ANGULAR_VELOCITY;
         D.bodyA = d->drive_body_a[k] >= 0 ? body_index_of_id(w, d->drive_body_a[k]) : -1;
         D.bodyB = body_index_of_id(w, d->drive_body_b[k]);
-        D.axis = normalized(mk(p[0], p[1], p[2]));
-        D.kv = p[3]; D.v_target = p[4];
-        D.max_torque = p[5] <= 0.0 ? kInf : p[5];
-        D.delay = std::max(0.0, p[6]);
-        D.delay_tau = std::max(0.0, p[7]);
+        if (D.kind < NXD_DRIVE_ANGULAR_VELOCITY || D.kind > NXD_DRIVE_DAMPED_SPRING || D.bodyB < 0 ||
+            D.bodyA == D.bodyB || (D.kind == NXD_DRIVE_DAMPED_SPRING && D.bodyA < 0) ||
+            (D.kind == NXD_DRIVE_FORCE && D.bodyA >= 0)) { delete w; return nullptr; }
+        if (D.kind == NXD_DRIVE_FORCE) {
+            D.force = mk(p[0], p[1], p[2]);
+            D.torque = mk(p[3], p[4], p[5]);
+        } else if (D.kind == NXD_DRIVE_DAMPED_SPRING) {
+            D.rest = p[0]; D.k = p[1]; D.c = p[2];
+        } else {
+            D.axis = normalized(mk(p[0], p[1], p[2]));
+            D.kv = p[3]; D.v_target = p[4];
+            D.max_torque = p[5] <= 0.0 ? kInf : p[5];
+            D.delay = std::max(0.0, p[6]);
+            D.delay_tau = D.kind == NXD_DRIVE_POSITION ? 0.0 : std::max(0.0, p[7]);
+        }
         D.filtered = D.v_target;
         w->drives.push_back(D);
     }
@@ -2415,7 +2553,7 @@ int nxo_form_gradient(nxo_world* w, int32_t form, const double* xp, double* gp) 
         case NXD_FORM_CONSTRAINT: for (const auto& J : w->joints) joint_gradient(J, x, g); break;
         case NXD_FORM_BARRIER: barrier_form_gradient(w, x, g); break;
         case NXD_FORM_FRICTION: friction_form_gradient(w, x, g); break;
-        case NXD_FORM_DRIVES: for (auto& d : w->drives) drive_gradient(d, x, g); break;
+        case NXD_FORM_DRIVES: for (auto& d : w->drives) drive_gradient(w, d, x, g); break;
         case NXD_FORM_TOTAL: problem_gradient(w, x, g); break;
         case NXD_FORM_CONTACT: problem_contact_gradient(w, x, g); break;
         default: return NXD_INVALID_ARGUMENT;

@@ -32,6 +32,7 @@ SCENES = {
     "cube_stack": lambda: scenes.cube_stack(),
     "sphere_bowl": lambda: scenes.sphere_bowl(n_spheres=24),
     "hopper_small": lambda: scenes.hopper_chains(n_hulls=192, n_chains=6),
+    "control_forms": lambda: scenes.control_forms(),
 }
 
 
@@ -153,7 +154,7 @@ def random_state_and_contacts(sc, seed=3):
     return x, xh, c, nf
 
 
-@pytest.mark.parametrize("name", ["cube_stack", "hopper_small"])
+@pytest.mark.parametrize("name", ["cube_stack", "hopper_small", "control_forms"])
 def test_form_values_gradients_hessian(name):
     sc = SCENES[name]()
     x, xh, c, nf = random_state_and_contacts(sc)
@@ -271,6 +272,36 @@ def test_trajectory_prismatic_cylindrical_distance_joints():
     wp, wr, (lg, mg, lo, mo) = run_pair(sc, 60, check_every=10)
     assert wp <= 1e-6 and wr <= 1e-6, (wp, wr)
     assert np.abs(lg - lo).max() <= 1e-6 * max(1.0, np.abs(lo).max())
+
+
+def test_trajectory_control_forms():
+    # DampedSpringForm, PositionDriveForm (to the world and between bodies),
+    # LinearVelocityDriveForm, VelocityDriveForm and ForceDriveForm in one
+    # World::forms list, with contacts on a ground box
+    wp, wr, _ = run_pair(scenes.control_forms(), 60, check_every=10)
+    assert wp <= 1e-6 and wr <= 1e-6, (wp, wr)
+
+
+def test_control_forms_batched_and_refused():
+    rt = runtime()
+    scs = [scenes.control_forms(seed=6000 + k) for k in range(3)]
+    b = rt.Batch(scs)
+    singles = [rt.Context(s) for s in scs]
+    for _ in range(8):
+        b.step()
+        for c in singles:
+            c.step()
+    for i, c in enumerate(singles):
+        sg, sc_ = b.state(i), c.state()
+        for k in sg:
+            assert np.array_equal(sg[k], sc_[k]), (i, k)
+    # a spring needs two distinct bodies; a force drive acts on body_b only
+    bad = scenes.control_forms()
+    bad.drive_body_a = bad.drive_body_a.copy()
+    bad.drive_body_a[0] = bad.drive_body_b[0]
+    with pytest.raises(rt.NxdError) as e:
+        rt.Context(bad)
+    assert e.value.status == 7   # NXD_INVALID_ARGUMENT
 
 
 def test_batch_matches_single_scenes():

@@ -56,15 +56,50 @@ def test_fixture_scene_mapping():
     assert sc.dt == 0.005 and cfg.max_time == 0.1 and cfg.output_name == "fixture_run"
 
 
-def test_unsupported_joint_type_is_refused(tmp_path):
-    doc = json.load(open(FIXTURE))
-    doc["joints"].append({"type": "damped_spring", "body_a": 12, "body_b": 13, "stiffness_npm": 10.0})
+def _write_scene(tmp_path, doc):
     p = tmp_path / "s.json"
     p.write_text(json.dumps(doc))
     for name in ("ground.obj", "cube.obj", "link.obj"):
         (tmp_path / name).write_text(open(os.path.join(GOLDEN, name)).read())
-    with pytest.raises(NotImplementedError, match="damped_spring"):
-        sceneio.load_scene(str(p))
+    return str(p)
+
+
+def test_unsupported_joint_type_is_refused(tmp_path):
+    doc = json.load(open(FIXTURE))
+    doc["joints"].append({"type": "gear", "body_a": 12, "body_b": 13})
+    with pytest.raises(NotImplementedError, match="gear"):
+        sceneio.load_scene(_write_scene(tmp_path, doc))
+
+
+def test_control_form_entries(tmp_path):
+    # SceneLoader.cpp:274-446: key fallbacks, defaults, skipped entries and the
+    # load order of World::forms ("joints" before "constraints", where the
+    # fixture's velocity drive is)
+    doc = json.load(open(FIXTURE))
+    doc["joints"] += [
+        {"type": "damped_spring", "body_a": 12, "body_b": 13, "stiffness_npm": 10.0, "rest_length": 0.2,
+         "damping_nspm": 0.5},
+        {"type": "damped_spring", "body_a": 99, "body_b": 13, "stiffness_npm": 1.0},     # ignored
+        {"type": "position_drive", "body_a": -1, "body_b": 11, "axis": [0, 2, 0], "stiffness": 30.0,
+         "target_position_m": 0.4, "max_force_n": 5.0, "deadzone_m": 0.01},
+        {"type": "linear_velocity_drive", "body_a": 12, "body_b": 13, "axis": [1, 0, 0],
+         "target_velocity": -0.3, "delay_mps": 0.02, "delay_seconds": 0.1},
+        {"type": "force_drive", "body_b": 11, "axis": [3, 0, 4], "force_magnitude": 10.0, "torque": [0, 0.1, 0]},
+        {"type": "force_drive", "body": 77, "force": [1, 2, 3]},                          # ignored
+    ]
+    sc, _ = sceneio.load_scene(_write_scene(tmp_path, doc))
+    assert list(sc.drive_kind) == [abi.NXD_DRIVE_DAMPED_SPRING, abi.NXD_DRIVE_POSITION,
+                                   abi.NXD_DRIVE_LINEAR_VELOCITY, abi.NXD_DRIVE_FORCE, abi.NXD_DRIVE_ANGULAR_VELOCITY]
+    assert list(sc.drive_body_a) == [12, -1, 12, -1, 12] and list(sc.drive_body_b) == [13, 11, 13, 11, 13]
+    assert list(sc.drive_params[0][:3]) == [0.2, 10.0, 0.5]
+    assert list(sc.drive_params[1][3:7]) == [30.0, 0.4, 5.0, 0.01]
+    assert list(sc.drive_params[2][3:8]) == [100.0, -0.3, 0.0, 0.02, 0.1]     # kv defaults to 100
+    assert list(sc.drive_params[3][:6]) == [0.6 * 10.0, 0.0, 0.8 * 10.0, 0.0, 0.1, 0.0]
+    # the oracle builds and steps the scene
+    ow = refcpu.OracleWorld(sc)
+    for _ in range(3):
+        ow.step()
+    assert np.isfinite(ow.state()["position"]).all()
 
 
 def test_state_csv_columns_and_precision(tmp_path):
