@@ -266,6 +266,16 @@ void launch_pairs(nxd_ctx* c, const PairQuery& q, int* out, int* count_dev, cons
     NXD_K(c, NXD_PROF_BROAD, pairs, (blocks), (256), (0), c->geo, q, c->boxes, nullptr, c->pair_off, out, c->pair_cap, gate);
 }
 
+// CTAs of a grid-stride loop over the pair list: no more than the pair
+// capacity or N(N-1)/2 pairs can need a warp, so a small world (a batch
+// replays hundreds of them in one launch) launches only the CTAs it can use
+int pair_grid(const nxd_ctx* c, int warps_per_pair_item, int items_per_pair, int warps_per_block, int max_blocks) {
+    const long long maxp = std::min<long long>(c->pair_cap, (long long)c->N * (c->N - 1) / 2);
+    const long long warps = maxp * items_per_pair * warps_per_pair_item;
+    const long long need = (warps + warps_per_block - 1) / warps_per_block;
+    return (int)std::max<long long>(1, std::min<long long>(max_blocks, need));
+}
+
 size_t topk_smem(const nxd_ctx* c, int warps) {
     return (size_t)warps * topk_warp_bytes(c->max_prims, c->max_verts);
 }
@@ -276,7 +286,7 @@ void launch_candidates(nxd_ctx* c, const double* act_ptr, double act_val) {
     launch_pairs(c, q, c->pairs, &c->sc->n_pairs, nullptr);
     int warps = 8;
     while (warps > 1 && topk_smem(c, warps) > 200 * 1024) --warps;
-    NXD_K(c, NXD_PROF_TOPK, topk, (c->n_sm * 4), (32 * warps), (topk_smem(c, warps)), c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap,
+    NXD_K(c, NXD_PROF_TOPK, topk, (pair_grid(c, 1, 2, warps, c->n_sm * 4)), (32 * warps), (topk_smem(c, warps)), c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap,
                                                                        c->boxes, c->wv, c->topk, c->topn, c->max_prims, c->max_verts);
 }
 
@@ -292,7 +302,8 @@ void launch_narrow_full(nxd_ctx* c, const double* wv, const double* pose_p, cons
     NarrowIn in{c->geo, c->pairs, &c->sc->n_pairs, c->pair_cap, c->topk, c->topn, wv, pose_p, &c->sc->dhat,
                 c->allowed_keys, c->n_allowed};
     const NarrowScratch ns{c->hmask, c->hit_cnt, c->hit_off};
-    const int rows_blocks = c->n_sm * 8, emit_blocks = c->n_sm * 2;
+    const int rows_blocks = pair_grid(c, 1, 1, kRowsWarps, c->n_sm * 8);
+    const int emit_blocks = pair_grid(c, 1, 1, kEmitWarps, c->n_sm * 2);
     int* skip_vv = c->i_scratch;
     const int* np = &c->sc->n_pairs;
     NXD_K(c, NXD_PROF_NARROW, narrow_rows, (rows_blocks), (32 * kRowsWarps), (0), in, 0, ns, skip_if);
@@ -359,7 +370,7 @@ nxd_status enqueue_step(nxd_ctx* c, double dt) {
         NXD_K(c, NXD_PROF_OTHER, md_gate, (1), (1), (0), c->sc, c->max_md_tol);
         PairQuery qm{2, &c->sc->md_radius, 0.0, 1.0, 0.0};
         launch_pairs(c, qm, c->md_pairs, &c->sc->n_md_pairs, &c->sc->md_gate);
-        NXD_K(c, NXD_PROF_MIN_DISTANCE, min_distance, (c->n_sm * 4), (256), (0), c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
+        NXD_K(c, NXD_PROF_MIN_DISTANCE, min_distance, (pair_grid(c, 1, 1, 8, c->n_sm * 4)), (256), (0), c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
                                                     &c->sc->md, &c->sc->md_gate);
         NXD_K(c, NXD_PROF_OTHER, kappa_update, (1), (1), (0), c->sc);
     }
@@ -870,7 +881,7 @@ nxd_status nxd_scene_min_distance(nxd_ctx* c, double* out) {
     NXD_K(c, NXD_PROF_OTHER, md_gate, (1), (1), (0), c->sc, c->max_md_tol);
     PairQuery qm{2, &c->sc->md_radius, 0.0, 1.0, 0.0};
     launch_pairs(c, qm, c->md_pairs, &c->sc->n_md_pairs, &c->sc->md_gate);
-    NXD_K(c, NXD_PROF_MIN_DISTANCE, min_distance, (c->n_sm * 4), (256), (0), c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
+    NXD_K(c, NXD_PROF_MIN_DISTANCE, min_distance, (pair_grid(c, 1, 1, 8, c->n_sm * 4)), (256), (0), c->geo, c->md_pairs, &c->sc->n_md_pairs, c->pair_cap, c->boxes, c->wv,
                                                 &c->sc->md, &c->sc->md_gate);
     NXD_CUDA(cudaStreamSynchronize(st));
     Scalars h;

@@ -1764,6 +1764,11 @@ __device__ __forceinline__ void newton_body(const Solver& S) {
     NX_PHASE(0);
 
     bool converged = false, poses_at_x = false, aborted = false;
+    // energies at the accepted iterate: the next line search's starting
+    // values are the same function of the same x, so they are reused when no
+    // stateful form (a velocity drive) has to see its value call
+    bool have_fx = false;
+    double fx_acc = 0.0, fc_acc = 0.0;
     int iters = 0;
     for (int iter = 0; iter < S.newton_max_iters; ++iter) {
         iters = iter;
@@ -1813,7 +1818,8 @@ __device__ __forceinline__ void newton_body(const Solver& S) {
         }
         double fx, fc, descent, cdesc;
         {
-            grid_energies(S, S.x, s, C, R, fx, fc);
+            if (have_fx) { fx = fx_acc; fc = fc_acc; }
+            else grid_energies(S, S.x, s, C, R, fx, fc);
             const int nn[2] = {n6, n6};
             double dd[2];
             R.sums<2>(nn, [&](int q, int e) { return (q == 0 ? S.g[e] : S.cg[e]) * S.dx[e]; }, dd);
@@ -1837,7 +1843,7 @@ __device__ __forceinline__ void newton_body(const Solver& S) {
             double fn, fcn;
             grid_energies(S, S.xt, s, C, R, fn, fcn);
             const bool cok = cdesc <= 0.0 ? (fcn <= fc + S.ls_c1 * alpha * cdesc) : (fcn <= fc);
-            if (fn <= fx + S.ls_c1 * alpha * descent && cok) { done = true; break; }
+            if (fn <= fx + S.ls_c1 * alpha * descent && cok) { done = true; fx_acc = fn; fc_acc = fcn; break; }
             alpha *= S.ls_rho;
         }
         NX_PHASE(6);
@@ -1846,6 +1852,7 @@ __device__ __forceinline__ void newton_body(const Solver& S) {
         NX_GRID_FOR(i, N, gc)
             for (int k = 0; k < 6; ++k) S.x[6 * i + k] = S.xt[6 * i + k];
         poses_at_x = true;
+        have_fx = S.D == 0;
         if (S.D > 0) gc.sync();   // the drives' next gradient call reads any body's x
         if (iter == S.newton_max_iters - 1) iters = S.newton_max_iters;
     }
