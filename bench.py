@@ -206,6 +206,53 @@ def batched_leg(torch, steps: int, warmup: int, flush):
     return out
 
 
+def diff_leg(torch):
+    """Differentiable-rollout configuration: 16 icospheres colliding on a
+    ground box, 50 steps, final poses differentiated with respect to the 48
+    initial velocities, 16 masses and the friction coefficient by central
+    differences, i.e. 131 worlds stepped as one batch.  Reports the device
+    time of the 50 batched steps (CUDA events) and the wall time of the whole
+    Jacobian call (scene copies, batch creation, read-back)."""
+    import time
+    from nexdynipc_b200 import diff, runtime, scenes
+    sc = scenes.diff_scene()
+    bodies = list(range(1, sc.n_bodies))
+    spec = diff.ParamSpec(["velocity", "mass", "friction"], bodies=bodies)
+    theta = spec.get(sc)
+    steps = sc.steps
+    times = {}
+
+    def runner(worlds, n):
+        stream = torch.cuda.Stream()
+        b = runtime.Batch(worlds)
+        b.set_stream(stream.cuda_stream)
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            b.step(n)
+            e.record(stream)
+        torch.cuda.synchronize()
+        times["device_s"] = a.elapsed_time(e) / 1e3
+        out = [b.state(i) for i in range(len(worlds))]
+        status = max(b.diagnostics(i)["status"] for i in range(len(worlds)))
+        b.close()
+        times["status"] = status
+        return out
+
+    diff.rollout_jacobian(sc, spec, theta, 2, bodies, runner=runner)      # warm-up (module load, graphs)
+    t0 = time.perf_counter()
+    y, J = diff.rollout_jacobian(sc, spec, theta, steps, bodies, runner=runner)
+    wall = time.perf_counter() - t0
+    worlds = 2 * theta.size + 1
+    return {"workload": f"{sc.n_bodies - 1} icospheres (162 V) on a ground box, {steps} steps, dt {sc.dt}",
+            "parameters": int(theta.size), "outputs": int(y.size), "worlds": worlds,
+            "device_s": times["device_s"], "wall_s": wall,
+            "scene_steps_per_s": worlds * steps / times["device_s"],
+            "jacobians_per_s_wall": 1.0 / wall, "status": int(times["status"]),
+            "finite": bool(np.isfinite(J).all())}
+
+
 def mode_i_leg(ctx, sc, reps: int = 5):
     """Primitive-level contact model on the workload's current state, through
     the C ABI (host arrays in and out, each call synchronising): LBVH
@@ -280,6 +327,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-mode-i", action="store_true")
+    ap.add_argument("--no-diff", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.impl == "reference":
@@ -441,6 +489,7 @@ def main():
     batched = None
     if not args.no_batched:
         batched = batched_leg(torch, min(args.steps, 10), 2, flush)
+    diffl = None if args.no_diff else diff_leg(torch)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -464,6 +513,7 @@ def main():
                                                               ("n_body_pairs", "n_contacts", "alm_iterations",
                                                                "newton_iterations", "status")},
                    "batched": batched,
+                   "diff": diffl,
                    "mode_i": mode_i},
         "roofline": roof,
         "roofline_narrow_phase": roof_narrow,
