@@ -426,6 +426,9 @@ def main():
     vin, vout = view(pinned), view(out_pinned)
     h2d = sum(v.numel() * 8 for v in pinned.values())
     d2h = sum(v.numel() * 8 for v in out_pinned.values())
+    # a host-driven loop continuing the timed trajectory: each step uploads
+    # the state the previous step read back
+    lib.nxd_get_state(ctx.h, C.byref(vin))
     if ws > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -434,6 +437,7 @@ def main():
         lib.nxd_set_state(ctx.h, C.byref(vin))
         step()
         lib.nxd_get_state(ctx.h, C.byref(vout))
+        vin, vout = vout, vin
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     if ws > 1:
@@ -507,7 +511,8 @@ def main():
         "config": {"workload": WORKLOAD, "replicas": ws, "l2": "flushed between steps (256 MiB write, untimed)",
                    "timing": ("value: K steps, each the step's CUDA graph, CUDA events per step; per_family_ms and "
                               "roofline: the same K step indices on a twin context of the same scene with CUDA "
-                              "events around every launch"),
+                              "events around every launch; e2e: the next K steps of the trajectory, each "
+                              "nxd_set_state from pinned host memory, nxd_step, nxd_get_state back, wall clock"),
                    "twin_state_equal": twin_equal,
                    "per_family_ms": per_family, "last_step": {k: diag[k] for k in
                                                               ("n_body_pairs", "n_contacts", "alm_iterations",

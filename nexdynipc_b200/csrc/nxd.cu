@@ -209,6 +209,7 @@ void fill_solver(nxd_ctx* c) {
     S.converged = &c->sc->converged; S.ls_fail = &c->sc->ls_fail;
     S.alm_mcv = m.alloc<double>(1); S.alm_dual = m.alloc<double>(1);
     S.solve_fail = m.alloc<int>(1);
+    S.iact = m.alloc<int>(J + D + 2 * kMaxContacts);
     S.bar_count = m.alloc<unsigned>(2); S.bar_abort = (int*)(S.bar_count + 1);
     S.gpart = m.alloc<double>(2 * kRedMaxQ * kMaxNewtonGrid);
     // one CTA of kNewtonThreads per 512 DOFs, a power of two no larger than
@@ -736,29 +737,34 @@ nxd_status nxd_step(nxd_ctx* c, double dt) {
     return NXD_OK;
 }
 
+// State copies are queued on the context's stream behind the work already
+// there (one copy per array, no batched-copy API), then waited for once, so
+// the host buffers are free when the call returns.
 nxd_status nxd_get_state(nxd_ctx* c, const nxd_state* o) {
     if (!c || !o) return NXD_INVALID_ARGUMENT;
-    NXD_CUDA(cudaStreamSynchronize(c->stream));
     const size_t n3 = 3 * (size_t)c->N * sizeof(double), n4 = 4 * (size_t)c->N * sizeof(double);
-    if (o->position) NXD_CUDA(cudaMemcpy(o->position, c->pos, n3, cudaMemcpyDeviceToHost));
-    if (o->orientation) NXD_CUDA(cudaMemcpy(o->orientation, c->quat, n4, cudaMemcpyDeviceToHost));
-    if (o->velocity) NXD_CUDA(cudaMemcpy(o->velocity, c->vel, n3, cudaMemcpyDeviceToHost));
-    if (o->angular_velocity) NXD_CUDA(cudaMemcpy(o->angular_velocity, c->omega, n3, cudaMemcpyDeviceToHost));
-    if (o->linear_acceleration) NXD_CUDA(cudaMemcpy(o->linear_acceleration, c->lacc, n3, cudaMemcpyDeviceToHost));
-    if (o->angular_acceleration) NXD_CUDA(cudaMemcpy(o->angular_acceleration, c->aacc, n3, cudaMemcpyDeviceToHost));
+    const cudaMemcpyKind k = cudaMemcpyDeviceToHost;
+    if (o->position) NXD_CUDA(cudaMemcpyAsync(o->position, c->pos, n3, k, c->stream));
+    if (o->orientation) NXD_CUDA(cudaMemcpyAsync(o->orientation, c->quat, n4, k, c->stream));
+    if (o->velocity) NXD_CUDA(cudaMemcpyAsync(o->velocity, c->vel, n3, k, c->stream));
+    if (o->angular_velocity) NXD_CUDA(cudaMemcpyAsync(o->angular_velocity, c->omega, n3, k, c->stream));
+    if (o->linear_acceleration) NXD_CUDA(cudaMemcpyAsync(o->linear_acceleration, c->lacc, n3, k, c->stream));
+    if (o->angular_acceleration) NXD_CUDA(cudaMemcpyAsync(o->angular_acceleration, c->aacc, n3, k, c->stream));
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
     return NXD_OK;
 }
 
 nxd_status nxd_set_state(nxd_ctx* c, const nxd_state* o) {
     if (!c || !o) return NXD_INVALID_ARGUMENT;
-    NXD_CUDA(cudaStreamSynchronize(c->stream));
     const size_t n3 = 3 * (size_t)c->N * sizeof(double), n4 = 4 * (size_t)c->N * sizeof(double);
-    if (o->position) NXD_CUDA(cudaMemcpy(c->pos, o->position, n3, cudaMemcpyHostToDevice));
-    if (o->orientation) NXD_CUDA(cudaMemcpy(c->quat, o->orientation, n4, cudaMemcpyHostToDevice));
-    if (o->velocity) NXD_CUDA(cudaMemcpy(c->vel, o->velocity, n3, cudaMemcpyHostToDevice));
-    if (o->angular_velocity) NXD_CUDA(cudaMemcpy(c->omega, o->angular_velocity, n3, cudaMemcpyHostToDevice));
-    if (o->linear_acceleration) NXD_CUDA(cudaMemcpy(c->lacc, o->linear_acceleration, n3, cudaMemcpyHostToDevice));
-    if (o->angular_acceleration) NXD_CUDA(cudaMemcpy(c->aacc, o->angular_acceleration, n3, cudaMemcpyHostToDevice));
+    const cudaMemcpyKind k = cudaMemcpyHostToDevice;
+    if (o->position) NXD_CUDA(cudaMemcpyAsync(c->pos, o->position, n3, k, c->stream));
+    if (o->orientation) NXD_CUDA(cudaMemcpyAsync(c->quat, o->orientation, n4, k, c->stream));
+    if (o->velocity) NXD_CUDA(cudaMemcpyAsync(c->vel, o->velocity, n3, k, c->stream));
+    if (o->angular_velocity) NXD_CUDA(cudaMemcpyAsync(c->omega, o->angular_velocity, n3, k, c->stream));
+    if (o->linear_acceleration) NXD_CUDA(cudaMemcpyAsync(c->lacc, o->linear_acceleration, n3, k, c->stream));
+    if (o->angular_acceleration) NXD_CUDA(cudaMemcpyAsync(c->aacc, o->angular_acceleration, n3, k, c->stream));
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
     return NXD_OK;
 }
 

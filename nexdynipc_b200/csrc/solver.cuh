@@ -100,6 +100,7 @@ struct Solver {
     double* pool; long long pool_cap; long long* pool_off;        // per-component L, D and rhs
     int slab_bytes;                               // per-warp shared workspace of a component solve (0: none)
     int* solve_fail;                              // [1] zero pivot or capacity in this solve
+    int* iact;                                    // [J+D+2*Cmax] item active at the last structure build
     // grid execution of k_newton
     unsigned* bar_count; int* bar_abort;          // barrier arrivals and give-up flag, zeroed per launch
     double* gpart;                                // [2 * kRedMaxQ * kMaxNewtonGrid] per-CTA partial sums
@@ -1188,8 +1189,12 @@ __device__ __forceinline__ bool mask_test(const unsigned* row, int b) { return (
 
 // returns 0 ok, 1 zero pivot, 2 capacity
 // Workspace: the structure words, then the factor doubles, each in the warp's
-// shared-memory slab when it fits there, else in the global pools.
-__device__ int solve_component(const Solver& S, int root, double s, int C, unsigned char* slab) {
+// shared-memory slab when it fits there, else in the global pools.  With
+// reuse, the slab already holds this component's structure (same members,
+// items and coupling pattern): only the numeric part runs.  in_slab tells
+// the caller whether the structure now sits in the slab.
+__device__ int solve_component(const Solver& S, int root, double s, int C, unsigned char* slab, bool reuse,
+                               bool& in_slab) {
     const int lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
     const int k = S.mcnt[root + 1] - S.mcnt[root];
@@ -1202,10 +1207,13 @@ __device__ int solve_component(const Solver& S, int root, double s, int C, unsig
     const long long nwords = Psort + 3LL * k * W + 6LL * k + 2;
     unsigned* base;
     size_t slab_used = 0;
+    in_slab = false;
     if (slab && 4 * nwords <= S.slab_bytes) {
         base = reinterpret_cast<unsigned*>(slab);
         slab_used = (size_t)(4 * nwords + 15) & ~(size_t)15;
+        in_slab = true;
     } else {
+        reuse = false;
         long long off = 0;
         if (lane == 0) off = (long long)atomicAdd((unsigned long long*)S.mpool_off, (unsigned long long)nwords);
         off = __shfl_sync(full, off, 0);
@@ -1222,7 +1230,11 @@ __device__ int solve_component(const Solver& S, int root, double s, int C, unsig
     int* body_at = pos_of + k;
     int* rowptr = body_at + k;
     int* rows = rowptr + k + 1;
-
+    const unsigned lt = (1u << lane) - 1u;
+    int nnz;
+    if (reuse) {
+        nnz = rowptr[k];
+    } else {
     // members ascending, items in item order
     warp_sort_int(mem, k, sortbuf);
     warp_sort_int(its, m, sortbuf);
@@ -1247,7 +1259,6 @@ __device__ int solve_component(const Solver& S, int root, double s, int C, unsig
     __syncwarp();
     warp_scan_excl(degcnt, k + 1);
     // stable counting placement by degree (members already ascending)
-    const unsigned lt = (1u << lane) - 1u;
     for (int b0 = 0; b0 < k; b0 += 32) {
         const int t = b0 + lane;
         const int key = t < k ? deg[t] : -1 - lane;
@@ -1307,8 +1318,9 @@ __device__ int solve_component(const Solver& S, int root, double s, int C, unsig
         rowptr[i] = c;
     }
     __syncwarp();
-    const int nnz = warp_scan_excl(rowptr, k);
+    nnz = warp_scan_excl(rowptr, k);
     if (lane == 0) rowptr[k] = nnz;
+    }
     const long long ndoubles = 36LL * (k + nnz) + 6LL * k;
     double* Dg;
     if (slab && (long long)slab_used + 8 * ndoubles <= S.slab_bytes) {
@@ -1488,6 +1500,12 @@ constexpr int kNewtonDynSmem = (kNewtonThreads / 32) * kNewtonSlabBytes;
 constexpr int kMaxNewtonGrid = 64;
 constexpr unsigned kBarrierSpinLimit = 1u << 24;   // x >= 64 ns sleeps: about a second
 
+// arrival of a grid barrier: an acq_rel fence at GPU scope (cumulative over
+// the writes this thread has observed, i.e. its CTA's writes before the
+// preceding __syncthreads), then a relaxed add without a return value
+__device__ __forceinline__ void red_release_add_u32(unsigned* p, unsigned v) {
+    asm volatile("fence.acq_rel.gpu;\n\tred.relaxed.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     unsigned v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -1509,19 +1527,19 @@ struct GridCtx {
         if (threadIdx.x == 0) {
             int ok = *sh_ok;
             if (ok) {
-                __threadfence();
-                atomicAdd(count, 1u);
+                // release the CTA's writes, then poll with acquire loads
+                red_release_add_u32(count, 1u);
                 unsigned spins = 0;
                 while (ld_acquire_u32(count) < target) {
-                    if (++spins > kBarrierSpinLimit || *(volatile int*)abort) {
+                    ++spins;
+                    if (spins > kBarrierSpinLimit || ((spins & 63u) == 0 && *(volatile int*)abort)) {
                         ok = 0;
                         atomicExch(abort, 1);
                         atomicExch(status, NXD_TIMEOUT);
                         break;
                     }
-                    __nanosleep(64);
+                    if (spins > 32) __nanosleep(64);
                 }
-                __threadfence();
             }
             *sh_ok = ok;
         }
@@ -1636,10 +1654,43 @@ __device__ void grid_energies(const Solver& S, const double* x, double s, int C,
     contact = c;
 }
 
+// 6x6 LDL^T solve of body i's diagonal block (a body no item couples)
+__device__ __forceinline__ void solve_singleton(const Solver& S, int i) {
+    double A[36], b[6];
+#pragma unroll
+    for (int e = 0; e < 36; ++e) A[e] = S.Hd[36 * i + e];
+#pragma unroll
+    for (int e = 0; e < 6; ++e) b[e] = -S.g[6 * i + e];
+    if (!ldlt6_solve(A, b)) { atomicExch(S.solve_fail, 1); return; }
+#pragma unroll
+    for (int e = 0; e < 6; ++e) S.dx[6 * i + e] = b[e];
+}
+
 // Solve H dx = -g over the grid.  Returns false (all threads) on failure.
-__device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, int* sh_scan, int* sh_flag) {
+// The block structure (components, their member and item lists, each
+// component's elimination order and fill pattern) depends only on which
+// coupling items are active.  `cached` says an earlier call of this launch
+// built it; it is reused, after one grid reduction over the items' states,
+// when no item changed state since.  A component's own symbolic part is
+// reused when its warp's shared slab still holds it (one component per warp).
+__device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, GridRed& R, int* sh_scan, int* sh_flag,
+                           int* sh_wcomp, bool& cached) {
     const int N = S.N;
     const int n_items = S.J + S.D + 2 * C;
+    bool reuse = false;
+    if (cached) {
+        if (gc.gtid == 0) { *S.mpool_off = 0; *S.pool_off = 0; *S.solve_fail = 0; }
+        double ch = 0.0;
+        NX_GRID_FOR(it, n_items, gc) if ((item_active(S, it) ? 1 : 0) != S.iact[it]) ch = 1.0;
+        reuse = R.max(ch) == 0.0;
+    }
+    if (reuse) {
+        NX_GRID_FOR(i, N, gc) {
+            if (S.comp[i] != i || S.rflag[i + 1] != S.rflag[i]) continue;
+            solve_singleton(S, i);
+        }
+        NX_PHASE(3);
+    } else {
     NX_GRID_FOR(i, N + 1, gc) {
         if (i < N) S.parent[i] = i;
         S.mcnt[i] = 0; S.icnt[i] = 0; S.rflag[i] = 0;
@@ -1647,7 +1698,9 @@ __device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, int* s
     if (gc.gtid == 0) { *S.comp_next = 0; *S.mpool_off = 0; *S.pool_off = 0; *S.solve_fail = 0; }
     gc.sync();
     NX_GRID_FOR(it, n_items, gc) {
-        if (!item_active(S, it)) continue;
+        const bool act = item_active(S, it);
+        S.iact[it] = act ? 1 : 0;
+        if (!act) continue;
         int a, b;
         item_bodies(S, it, a, b);
         if (a != b) uf_union(S.parent, a, b);
@@ -1659,7 +1712,7 @@ __device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, int* s
         atomicAdd(&S.mcnt[r], 1);
     }
     NX_GRID_FOR(it, n_items, gc) {
-        if (!item_active(S, it)) continue;
+        if (!S.iact[it]) continue;
         int a, b;
         item_bodies(S, it, a, b);
         if (a != b) atomicAdd(&S.icnt[uf_find(S.parent, a)], 1);
@@ -1670,14 +1723,7 @@ __device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, int* s
         const bool multi = S.comp[i] == i && S.mcnt[i] >= 2;
         S.rflag[i] = multi ? 1 : 0;
         if (S.comp[i] != i || S.mcnt[i] != 1) continue;
-        double A[36], b[6];
-#pragma unroll
-        for (int e = 0; e < 36; ++e) A[e] = S.Hd[36 * i + e];
-#pragma unroll
-        for (int e = 0; e < 6; ++e) b[e] = -S.g[6 * i + e];
-        if (!ldlt6_solve(A, b)) { atomicExch(S.solve_fail, 1); continue; }
-#pragma unroll
-        for (int e = 0; e < 6; ++e) S.dx[6 * i + e] = b[e];
+        solve_singleton(S, i);
     }
     gc.sync();
     NX_PHASE(3);
@@ -1689,7 +1735,6 @@ __device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, int* s
         block_scan_excl<3>(arr, N, sh_scan);
     }
     gc.sync();
-    const int n_comp = __ldcg(S.rflag + N);
     NX_GRID_FOR(r, N, gc) {
         if (S.rflag[r + 1] != S.rflag[r]) S.comp_root[S.rflag[r]] = r;
         S.local[r] = 0;    // member cursor per root
@@ -1701,7 +1746,7 @@ __device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, int* s
         if (S.mcnt[r + 1] - S.mcnt[r] >= 2) S.members[S.mcnt[r] + atomicAdd(&S.local[r], 1)] = i;
     }
     NX_GRID_FOR(it, n_items, gc) {
-        if (!item_active(S, it)) continue;
+        if (!S.iact[it]) continue;
         int a, b;
         item_bodies(S, it, a, b);
         if (a == b) continue;
@@ -1710,20 +1755,26 @@ __device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, int* s
     }
     gc.sync();
     NX_PHASE(3);
+    }
+    const int n_comp = __ldcg(S.rflag + N);
     // multi-body components: one warp each, consecutive components on
     // consecutive CTAs (warp w of CTA b takes components w G + b, + G nw, ...)
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nwarps = gc.G * (blockDim.x >> 5);
+    const bool one_each = n_comp <= nwarps;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    unsigned char* const slab = S.slab_bytes > 0 ? smem_raw + (size_t)(threadIdx.x >> 5) * S.slab_bytes : nullptr;
-    for (int o = (threadIdx.x >> 5) * gc.G + gc.b; o < n_comp; o += nwarps) {
-        const int rc = solve_component(S, S.comp_root[o], s, C, slab);
+    unsigned char* const slab = S.slab_bytes > 0 ? smem_raw + (size_t)w * S.slab_bytes : nullptr;
+    for (int o = w * gc.G + gc.b; o < n_comp; o += nwarps) {
+        bool in_slab = false;
+        const int rc = solve_component(S, S.comp_root[o], s, C, slab, reuse && one_each && sh_wcomp[w] == o, in_slab);
+        if (lane == 0) sh_wcomp[w] = (rc == 0 && in_slab) ? o : -1;
         if (rc != 0 && lane == 0) {
             atomicExch(S.solve_fail, 1);
             if (rc == 2) atomicExch(S.status, NXD_CAPACITY);
         }
     }
     gc.sync();
+    cached = true;
     NX_PHASE(4);
     if (threadIdx.x == 0) *sh_flag = __ldcg(S.solve_fail);
     __syncthreads();
@@ -1742,7 +1793,9 @@ __device__ __forceinline__ void newton_body(const Solver& S) {
     __shared__ double sh_red[kRedMaxQ * 32];
     __shared__ int sh_scan[3 * 32];
     __shared__ int sh_flag, sh_ok;
+    __shared__ int sh_wcomp[kNewtonThreads / 32];   // component whose structure each warp's slab holds
     if (*S.alm_done) return;
+    if (threadIdx.x < kNewtonThreads / 32) sh_wcomp[threadIdx.x] = -1;
     NX_PHASE_START();
     GridCtx gc;
     gc.G = gridDim.x; gc.b = blockIdx.x;
@@ -1767,7 +1820,7 @@ __device__ __forceinline__ void newton_body(const Solver& S) {
     // energies at the accepted iterate: the next line search's starting
     // values are the same function of the same x, so they are reused when no
     // stateful form (a velocity drive) has to see its value call
-    bool have_fx = false;
+    bool have_fx = false, cached = false;
     double fx_acc = 0.0, fc_acc = 0.0;
     int iters = 0;
     for (int iter = 0; iter < S.newton_max_iters; ++iter) {
@@ -1810,7 +1863,7 @@ __device__ __forceinline__ void newton_body(const Solver& S) {
         }
         if (!gc.sync()) { aborted = true; break; }
         NX_PHASE(2);
-        if (!grid_solve(S, s, C, gc, sh_scan, &sh_flag)) break;
+        if (!grid_solve(S, s, C, gc, R, sh_scan, &sh_flag, sh_wcomp, cached)) break;
         // line search (max step 1): the value calls at x, then descent terms
         if (S.D > 0) {
             NX_GRID_FOR(d, S.D, gc) drive_eval(S, d, S.x, 0);
