@@ -290,6 +290,38 @@ nxd_status nxd_form_hessian_bsr(nxd_ctx* ctx, int32_t form, const double* x,
                                 int32_t* row_ptr, int32_t* col_idx, double* vals,
                                 int64_t cap, int64_t* nnzb);
 
+/* SimulationProblem's three calls in one: computeValue, computeGradient and
+ * computeHessian of the total energy at x (the NXD_FORM_TOTAL value,
+ * gradient and BSR Hessian above; stateful drives see the value call, then
+ * the gradient call, then the Hessian call). */
+nxd_status nxd_eval_all(nxd_ctx* ctx, const double* x, double* energy, double* grad,
+                        int32_t* row_ptr, int32_t* col_idx, double* vals, int64_t cap, int64_t* nnzb);
+
+/* A 6x6-block sparse matrix over the context's bodies (host pointers), in the
+ * layout nxd_form_hessian_bsr writes: repeated (row, col) blocks are summed in
+ * storage order, as setFromTriplets sums duplicate triplets. */
+typedef struct nxd_bsr {
+    int32_t n_rows;             /* block rows: the context's body count */
+    int64_t nnzb;               /* blocks */
+    const int32_t* row_ptr;     /* [n_rows+1] */
+    const int32_t* col_idx;     /* [nnzb] */
+    const double* vals;         /* [nnzb*36] row-major blocks */
+} nxd_bsr;
+
+typedef struct nxd_solve_stats {
+    int32_t components;         /* connected block components of 2+ bodies */
+    int32_t singletons;         /* bodies coupled to no other */
+    int32_t largest_component;  /* bodies in the largest component */
+    int32_t factor_failed;      /* 1: an exactly zero pivot (LinearSolver::info() false) */
+} nxd_solve_stats;
+
+/* LinearSolver::analyzePattern + factorize + solve (Math/LinearSolver.cpp:11-39):
+ * x = H^-1 b by block LDL^T per connected component, members ordered by
+ * (coupled bodies, index), reading each block of the lower triangle in that
+ * order as stored (SimplicialLDLT's UpLo = Lower).  b and x: [6 n] host
+ * arrays.  NXD_FACTOR_FAILED on a zero pivot; stats may be NULL. */
+nxd_status nxd_linear_solve(nxd_ctx* ctx, const nxd_bsr* H, const double* b, double* x, nxd_solve_stats* stats);
+
 /* DistanceBarrierForm::updateContacts + FrictionForm::updateContactPoints +
  * FrictionForm::updateNormalForces (normal_forces may be NULL: none) and
  * InertiaForm::setPredictiveState (x_hat may be NULL: keep). */

@@ -135,6 +135,25 @@ class NxdSceneDesc(C.Structure):
     ]
 
 
+class NxdBsr(C.Structure):
+    _fields_ = [
+        ("n_rows", C.c_int32),
+        ("nnzb", C.c_int64),
+        ("row_ptr", _ip),
+        ("col_idx", _ip),
+        ("vals", _dp),
+    ]
+
+
+class NxdSolveStats(C.Structure):
+    _fields_ = [
+        ("components", C.c_int32),
+        ("singletons", C.c_int32),
+        ("largest_component", C.c_int32),
+        ("factor_failed", C.c_int32),
+    ]
+
+
 class NxdState(C.Structure):
     _fields_ = [
         ("position", _dp),

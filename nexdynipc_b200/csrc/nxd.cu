@@ -210,12 +210,14 @@ void fill_solver(nxd_ctx* c) {
     S.alm_mcv = m.alloc<double>(1); S.alm_dual = m.alloc<double>(1);
     S.solve_fail = m.alloc<int>(1);
     S.iact = m.alloc<int>(J + D + 2 * kMaxContacts);
+    S.ext_n = -1; S.ext_row = nullptr; S.ext_col = nullptr; S.ext_vals = nullptr;
     S.bar_count = m.alloc<unsigned>(2); S.bar_abort = (int*)(S.bar_count + 1);
     S.gpart = m.alloc<double>(2 * kRedMaxQ * kMaxNewtonGrid);
     // one CTA of kNewtonThreads per 512 DOFs, a power of two no larger than
     // what the device keeps co-resident
     S.slab_bytes = kNewtonSlabBytes;
     cudaFuncSetAttribute(k_newton, cudaFuncAttributeMaxDynamicSharedMemorySize, kNewtonDynSmem);
+    cudaFuncSetAttribute(k_linear_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, kNewtonDynSmem);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newton, kNewtonThreads, kNewtonDynSmem);
     const int coresident = std::max(1, per_sm * c->n_sm);
@@ -992,6 +994,77 @@ nxd_status nxd_form_gradient(nxd_ctx* c, int32_t form, const double* x, double* 
 nxd_status nxd_form_hessian_bsr(nxd_ctx* c, int32_t form, const double* x, int32_t* row_ptr, int32_t* col_idx,
                                 double* vals, int64_t cap, int64_t* nnzb) {
     return form_call(c, form, x, 2, nullptr, row_ptr, col_idx, vals, cap, nnzb);
+}
+
+nxd_status nxd_eval_all(nxd_ctx* c, const double* x, double* energy, double* grad, int32_t* row_ptr,
+                        int32_t* col_idx, double* vals, int64_t cap, int64_t* nnzb) {
+    if (!energy || !grad) return NXD_INVALID_ARGUMENT;
+    nxd_status rc = form_call(c, NXD_FORM_TOTAL, x, 0, energy, nullptr, nullptr, nullptr, 0, nullptr);
+    if (rc == NXD_OK) rc = form_call(c, NXD_FORM_TOTAL, x, 1, grad, nullptr, nullptr, nullptr, 0, nullptr);
+    if (rc == NXD_OK) rc = form_call(c, NXD_FORM_TOTAL, x, 2, nullptr, row_ptr, col_idx, vals, cap, nnzb);
+    return rc;
+}
+
+nxd_status nxd_linear_solve(nxd_ctx* c, const nxd_bsr* H, const double* b, double* x, nxd_solve_stats* stats) {
+    if (!c || !H || !b || !x || H->n_rows != c->N || H->nnzb < 0 || H->nnzb > INT32_MAX ||
+        (H->nnzb > 0 && (!H->row_ptr || !H->col_idx || !H->vals)))
+        return NXD_INVALID_ARGUMENT;
+    const int N = c->N;
+    const long long nb = H->nnzb;
+    for (int i = 0; i < N; ++i)
+        if (H->row_ptr[i] > H->row_ptr[i + 1] || H->row_ptr[i] < 0) return NXD_INVALID_ARGUMENT;
+    if (H->row_ptr[0] != 0 || H->row_ptr[N] != nb) return NXD_INVALID_ARGUMENT;
+    for (long long k = 0; k < nb; ++k)
+        if (H->col_idx[k] < 0 || H->col_idx[k] >= N) return NXD_INVALID_ARGUMENT;
+    cudaStream_t st = c->stream;
+    DevArena tmp;
+    int* rp = tmp.alloc<int>(N + 1);
+    int* ci = tmp.alloc<int>(std::max<long long>(nb, 1));
+    int* er = tmp.alloc<int>(std::max<long long>(nb, 1));
+    double* vv = tmp.alloc<double>(36 * (size_t)std::max<long long>(nb, 1));
+    double* bd = tmp.alloc<double>(6 * (size_t)N);
+    int* items = tmp.alloc<int>(std::max<long long>(nb, 1));
+    int* iact = tmp.alloc<int>(std::max<long long>(nb, 1));
+    int* stat = tmp.alloc<int>(1);
+    if (!tmp.ok) { tmp.release(); return NXD_CUDA_ERROR; }
+    NXD_CUDA(cudaMemcpyAsync(rp, H->row_ptr, sizeof(int) * (N + 1), cudaMemcpyHostToDevice, st));
+    if (nb > 0) {
+        NXD_CUDA(cudaMemcpyAsync(ci, H->col_idx, sizeof(int) * nb, cudaMemcpyHostToDevice, st));
+        NXD_CUDA(cudaMemcpyAsync(vv, H->vals, 36 * sizeof(double) * nb, cudaMemcpyHostToDevice, st));
+    }
+    NXD_CUDA(cudaMemcpyAsync(bd, b, 6 * sizeof(double) * N, cudaMemcpyHostToDevice, st));
+    NXD_CUDA(cudaMemsetAsync(stat, 0, sizeof(int), st));
+    Solver S = c->S;
+    S.ext_n = (int)nb; S.ext_row = er; S.ext_col = ci; S.ext_vals = vv;
+    S.items = items; S.iact = iact; S.status = stat;
+    if (N > 0) k_bsr_prepare<<<grid_for(N, 128), 128, 0, st>>>(S, rp, bd, er);
+    if (N > 0) k_linear_solve<<<1, kNewtonThreads, kNewtonDynSmem, st>>>(S);
+    NXD_CUDA(cudaGetLastError());
+    NXD_CUDA(cudaStreamSynchronize(st));
+    int fail = 0, capst = 0;
+    cudaMemcpy(&fail, S.solve_fail, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(&capst, stat, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(x, S.dx, 6 * sizeof(double) * N, cudaMemcpyDeviceToHost);
+    if (stats) {
+        std::vector<int> rflag(N + 1), mcnt(N + 1), comp(N);
+        cudaMemcpy(rflag.data(), S.rflag, sizeof(int) * (N + 1), cudaMemcpyDeviceToHost);
+        cudaMemcpy(mcnt.data(), S.mcnt, sizeof(int) * (N + 1), cudaMemcpyDeviceToHost);
+        cudaMemcpy(comp.data(), S.comp, sizeof(int) * N, cudaMemcpyDeviceToHost);
+        stats->components = rflag[N];
+        int in_multi = 0, largest = N > 0 ? 1 : 0;
+        for (int r = 0; r < N; ++r)
+            if (rflag[r + 1] != rflag[r]) {
+                const int k = mcnt[r + 1] - mcnt[r];
+                in_multi += k;
+                largest = std::max(largest, k);
+            }
+        stats->singletons = N - in_multi;
+        stats->largest_component = largest;
+        stats->factor_failed = (fail && !capst) ? 1 : 0;
+    }
+    tmp.release();
+    if (capst) return NXD_CAPACITY;
+    return fail ? NXD_FACTOR_FAILED : NXD_OK;
 }
 
 nxd_status nxd_normal_forces(nxd_ctx* c, const double* x, double* out, int32_t n) {

@@ -101,6 +101,10 @@ struct Solver {
     int slab_bytes;                               // per-warp shared workspace of a component solve (0: none)
     int* solve_fail;                              // [1] zero pivot or capacity in this solve
     int* iact;                                    // [J+D+2*Cmax] item active at the last structure build
+    // external linear system (nxd_linear_solve): when ext_n >= 0 the coupling
+    // items are the caller's BSR blocks (row, col, 36 values), diagonal
+    // blocks inactive, instead of joints, control forms and contacts
+    int ext_n; const int* ext_row; const int* ext_col; const double* ext_vals;
     // grid execution of k_newton
     unsigned* bar_count; int* bar_abort;          // barrier arrivals and give-up flag, zeroed per launch
     double* gpart;                                // [2 * kRedMaxQ * kMaxNewtonGrid] per-CTA partial sums
@@ -1005,6 +1009,7 @@ __device__ void gather_diag_hessian(const Solver& S, double s, int C) {
 // the Hessian: [0,J) joints, [J,J+D) control forms, [J+D, J+D+C) barrier
 // contacts, [J+D+C, J+D+2C) friction contacts.
 __device__ double coupling_entry(const Solver& S, int it, int R, int Cb, double s, int C, int e) {
+    if (S.ext_n >= 0) return S.ext_row[it] == R ? S.ext_vals[36LL * it + e] : 0.0;   // block (R, Cb) as stored
     const int ra = e / 6, cb = e % 6;
     if (it >= S.J && it < S.J + S.D) {
         // two-body control form: -(h a_ra) a_cb in both off-diagonal blocks
@@ -1054,6 +1059,7 @@ __device__ void add_coupling_block(const Solver& S, int it, int R, int Cb, doubl
     }
 }
 __device__ __forceinline__ void item_bodies(const Solver& S, int it, int& a, int& b) {
+    if (S.ext_n >= 0) { a = S.ext_row[it]; b = S.ext_col[it]; return; }
     if (it < S.J) { a = S.ja[it]; b = S.jb[it]; return; }
     const int J2 = S.J + S.D;
     if (it < J2) { a = S.da[it - S.J]; b = S.db[it - S.J]; return; }
@@ -1070,6 +1076,7 @@ __device__ __forceinline__ bool drive_couples(const Solver& S, int d) {
     return (kind == NXD_DRIVE_LINEAR_VELOCITY || kind == NXD_DRIVE_POSITION) && S.dH[d] != 0.0;
 }
 __device__ __forceinline__ bool item_active(const Solver& S, int it) {
+    if (S.ext_n >= 0) return S.ext_row[it] != S.ext_col[it];
     if (it < S.J) return joint_couples(S, it);
     const int J2 = S.J + S.D;
     if (it < J2) return drive_couples(S, it - S.J);
@@ -1676,7 +1683,7 @@ __device__ __forceinline__ void solve_singleton(const Solver& S, int i) {
 __device__ bool grid_solve(const Solver& S, double s, int C, GridCtx& gc, GridRed& R, int* sh_scan, int* sh_flag,
                            int* sh_wcomp, bool& cached) {
     const int N = S.N;
-    const int n_items = S.J + S.D + 2 * C;
+    const int n_items = S.ext_n >= 0 ? S.ext_n : S.J + S.D + 2 * C;
     bool reuse = false;
     if (cached) {
         if (gc.gtid == 0) { *S.mpool_off = 0; *S.pool_off = 0; *S.solve_fail = 0; }
@@ -1956,5 +1963,41 @@ __device__ __forceinline__ void newton_body(const Solver& S) {
 }
 constexpr int kLB_newton = kNewtonThreads;
 __global__ void __launch_bounds__(kNewtonThreads) k_newton(const __grid_constant__ Solver S) { newton_body(S); }
+
+// ---------------------------------------------------------------------------
+// LinearSolver::analyzePattern + factorize + solve (LinearSolver.cpp:11-39) for
+// a caller's block matrix: diagonal blocks summed in storage order into Hd,
+// the right-hand side as -g, then the Newton solve's component LDL^T on one
+// CTA (the lower triangle in elimination order, as SimplicialLDLT's Lower).
+// ---------------------------------------------------------------------------
+__global__ void k_bsr_prepare(Solver S, const int* row_ptr, const double* b, int* ext_row) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.N) return;
+    double H[36];
+    for (int e = 0; e < 36; ++e) H[e] = 0.0;
+    for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
+        ext_row[k] = i;
+        if (S.ext_col[k] == i)
+            for (int e = 0; e < 36; ++e) H[e] += S.ext_vals[36LL * k + e];
+    }
+    for (int e = 0; e < 36; ++e) S.Hd[36 * i + e] = H[e];
+    for (int k = 0; k < 6; ++k) S.g[6 * i + k] = -b[6 * i + k];
+}
+__global__ void __launch_bounds__(kNewtonThreads) k_linear_solve(const __grid_constant__ Solver S) {
+    __shared__ double sh_red[kRedMaxQ * 32];
+    __shared__ int sh_scan[3 * 32];
+    __shared__ int sh_flag, sh_ok;
+    __shared__ int sh_wcomp[kNewtonThreads / 32];
+    if (threadIdx.x < kNewtonThreads / 32) sh_wcomp[threadIdx.x] = -1;
+    if (threadIdx.x == 0) sh_ok = 1;
+    GridCtx gc;
+    gc.G = 1; gc.b = 0; gc.gtid = threadIdx.x; gc.gthreads = blockDim.x; gc.lin = threadIdx.x;
+    gc.count = S.bar_count; gc.abort = S.bar_abort; gc.status = S.status; gc.target = 0; gc.sh_ok = &sh_ok;
+    __syncthreads();
+    GridRed R;
+    R.gc = &gc; R.sh = sh_red; R.part = S.gpart; R.parity = 0;
+    bool cached = false;
+    grid_solve(S, 1.0, 0, gc, R, sh_scan, &sh_flag, sh_wcomp, cached);
+}
 
 }  // namespace nx

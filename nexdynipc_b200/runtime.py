@@ -55,6 +55,8 @@ def lib():
     L.nxd_form_gradient.argtypes = [vp, C.c_int32, dp, dp]
     L.nxd_form_hessian_bsr.argtypes = [vp, C.c_int32, dp, ip, ip, dp, C.c_int64, i64p]
     L.nxd_normal_forces.argtypes = [vp, dp, dp, C.c_int32]
+    L.nxd_eval_all.argtypes = [vp, dp, dp, dp, ip, ip, dp, C.c_int64, i64p]
+    L.nxd_linear_solve.argtypes = [vp, C.POINTER(abi.NxdBsr), dp, dp, C.POINTER(abi.NxdSolveStats)]
     L.nxd_batch_create.argtypes = [C.POINTER(abi.NxdSceneDesc), C.c_int32, C.POINTER(vp)]
     L.nxd_batch_destroy.argtypes = [vp]
     L.nxd_batch_step.argtypes = [vp, dp]
@@ -237,6 +239,36 @@ class Context:
                 j = ci[q]
                 H[6 * i:6 * i + 6, 6 * j:6 * j + 6] += vals[q]
         return H
+
+    def eval_all(self, x):
+        """(energy, gradient, (row_ptr, col_idx, vals)) of the total energy at
+        x in one call (nxd_eval_all)."""
+        xx = np.ascontiguousarray(x, np.float64)
+        e = C.c_double(0)
+        g = np.zeros(6 * self.n)
+        rp = np.zeros(self.n + 1, np.int32)
+        # every row: its diagonal block plus one block per incident coupling
+        # term (joints, control forms, at most 2000 contacts twice)
+        cap = self.n + 2 * (len(self.scene.joint_type) + len(self.scene.drive_body_b) + 2 * 2000)
+        nnzb = C.c_int64(0)
+        ci = np.zeros(cap, np.int32)
+        vals = np.zeros((cap, 6, 6))
+        _check("nxd_eval_all", lib().nxd_eval_all(self.h, abi.dptr(xx), C.byref(e), abi.dptr(g), abi.iptr(rp),
+                                                  abi.iptr(ci), abi.dptr(vals), cap, C.byref(nnzb)))
+        return e.value, g, (rp, ci[:nnzb.value], vals[:nnzb.value])
+
+    def linear_solve(self, row_ptr, col_idx, vals, b):
+        """x = H^-1 b for a 6x6-block BSR H over this context's bodies
+        (nxd_linear_solve); returns (x, stats dict)."""
+        rp = np.ascontiguousarray(row_ptr, np.int32)
+        ci = np.ascontiguousarray(col_idx, np.int32)
+        vv = np.ascontiguousarray(vals, np.float64)
+        bb = np.ascontiguousarray(b, np.float64)
+        H = abi.NxdBsr(self.n, len(ci), abi.iptr(rp), abi.iptr(ci), abi.dptr(vv))
+        x = np.zeros(6 * self.n)
+        stt = abi.NxdSolveStats()
+        _check("nxd_linear_solve", lib().nxd_linear_solve(self.h, C.byref(H), abi.dptr(bb), abi.dptr(x), C.byref(stt)))
+        return x, {k: getattr(stt, k) for k, _ in abi.NxdSolveStats._fields_}
 
     def normal_forces(self, x, n: int) -> np.ndarray:
         out = np.zeros(max(n, 1))

@@ -2589,6 +2589,21 @@ int nxo_form_hessian_dense(nxo_world* w, int32_t form, const double* xp, double*
     return NXD_OK;
 }
 
+int nxo_linear_solve(int32_t n_rows, int64_t nnzb, const int32_t* row_ptr, const int32_t* col_idx,
+                     const double* vals, const double* b, double* x) {
+    std::vector<Trip> trips;
+    trips.reserve((size_t)nnzb * 36);
+    for (int i = 0; i < n_rows; ++i)
+        for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+            for (int r = 0; r < 6; ++r)
+                for (int cc = 0; cc < 6; ++cc) trips.push_back({6 * i + r, 6 * col_idx[k] + cc, vals[36 * k + 6 * r + cc]});
+    const int n = 6 * n_rows;
+    std::vector<double> rhs(b, b + n), sol;
+    if (!solve_system(n, trips, rhs, sol)) return NXD_FACTOR_FAILED;
+    for (int i = 0; i < n; ++i) x[i] = sol[i];
+    return NXD_OK;
+}
+
 int nxo_normal_forces(nxo_world* w, const double* xp, double* out, int32_t n) {
     const auto x = vec_from(xp, w->bodies.size() * 6);
     const auto nf = barrier_normal_forces(w, x);

@@ -58,6 +58,11 @@ int nxo_form_gradient(nxo_world* w, int32_t form, const double* x, double* grad)
 /* Dense (6n x 6n, row-major) Hessian of a form, duplicates summed. */
 int nxo_form_hessian_dense(nxo_world* w, int32_t form, const double* x, double* H);
 int nxo_normal_forces(nxo_world* w, const double* x, double* out, int32_t n);
+/* LinearSolver on a caller's 6x6-block BSR matrix: blocks become triplets
+ * in storage order, then the same per-component dense LDL^T as the Newton
+ * solve.  Returns NXD_OK or NXD_FACTOR_FAILED. */
+int nxo_linear_solve(int32_t n_rows, int64_t nnzb, const int32_t* row_ptr, const int32_t* col_idx,
+                     const double* vals, const double* b, double* x);
 /* LDL^T solve of H dx = b with the oracle's solver (dense H input). */
 int nxo_ldlt_solve(const double* H, int32_t n, const double* b, double* x);
 

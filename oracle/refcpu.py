@@ -55,6 +55,8 @@ def lib():
     L.nxo_form_gradient.argtypes = [vp, C.c_int32, dp, dp]
     L.nxo_form_hessian_dense.argtypes = [vp, C.c_int32, dp, dp]
     L.nxo_normal_forces.argtypes = [vp, dp, dp, C.c_int32]
+    ip = C.POINTER(C.c_int32)
+    L.nxo_linear_solve.argtypes = [C.c_int32, C.c_int64, ip, ip, dp, dp, dp]
     L.nxo_ldlt_solve.argtypes = [dp, C.c_int32, dp, dp]
     L.nxo_select_top_k.argtypes = [dp, C.c_int32, C.c_int32, ip]
     L.nxo_libm.argtypes = [C.c_int32, dp, dp, dp, C.c_int32]
@@ -262,6 +264,20 @@ def ipc_accd(kind: int, X, D, t_max: float = 1.0, eta: float = 0.1, max_iter: in
     t = lib().nxo_ipc_accd(kind, _d(np.asarray(X, dtype=np.float64).reshape(12)),
                            _d(np.asarray(D, dtype=np.float64).reshape(12)), t_max, eta, max_iter, C.byref(it))
     return t, it.value
+
+
+def linear_solve(row_ptr, col_idx, vals, b):
+    """LinearSolver restated: x = H^-1 b for a 6x6-block BSR matrix; None on
+    a zero pivot."""
+    row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    col_idx = np.ascontiguousarray(col_idx, dtype=np.int32)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.zeros_like(b)
+    ip = C.POINTER(C.c_int32)
+    rc = lib().nxo_linear_solve(len(row_ptr) - 1, len(col_idx), row_ptr.ctypes.data_as(ip),
+                                col_idx.ctypes.data_as(ip), _d(vals), _d(b), abi.dptr(x))
+    return x if rc == 0 else None
 
 
 def libm(fn: int, x, y=None) -> np.ndarray:
