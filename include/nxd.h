@@ -405,6 +405,35 @@ nxd_status nxd_ipc_barrier(nxd_ctx* ctx, const double* x, double dhat, double ka
 nxd_status nxd_ipc_max_step(nxd_ctx* ctx, const double* x, const double* dx, double eta, double* alpha,
                             int64_t* n_pairs);
 
+/* Full-IPC time step: the primitive-level model above inside a Newton step.
+ * x_tilde and the inertia, gravity, joint and control forms are nxd_step's
+ * (joints with their current multipliers, no ALM update); the
+ * primitive-pair barrier replaces the COM-distance contact forms.  Newton
+ * starts from the step-start configuration and uses the |g|_inf test and
+ * Armijo backtracking (settings.ls_c1, ls_rho) from min(1, CCD bound);
+ * candidates are rebuilt at every iterate and trial point; each system is
+ * solved by nxd_linear_solve; the state is written back as nxd_step does.
+ * No friction term. */
+typedef struct nxd_ipc_params {
+    double dhat;                /* barrier activation distance               */
+    double kappa;               /* barrier stiffness                         */
+    double eta;                 /* CCD: kept fraction of each pair's gap     */
+    double newton_tol;          /* |g|_inf                                   */
+    int32_t newton_max_iters;
+    int32_t ls_max_iters;
+} nxd_ipc_params;
+typedef struct nxd_ipc_stats {
+    int32_t newton_iterations;
+    int32_t converged;
+    int32_t line_search_failed;
+    int32_t solve_failed;
+    double last_alpha_max;      /* the last CCD bound                        */
+    double energy;              /* total energy at the last accepted iterate */
+    int64_t n_pairs;            /* candidate pairs at the last iterate       */
+    int64_t n_active;           /* pairs within dhat                         */
+} nxd_ipc_stats;
+nxd_status nxd_ipc_step(nxd_ctx* ctx, double dt, const nxd_ipc_params* p, nxd_ipc_stats* stats);
+
 /* Body-pair broad phase for callers that cannot allocate device memory.
  * No counterpart in the reference.  Callers that manage every device byte
  * themselves (a host engine's memory pool, a hard memory cap, a real-time

@@ -154,6 +154,37 @@ class NxdSolveStats(C.Structure):
     ]
 
 
+class NxdIpcParams(C.Structure):
+    _fields_ = [
+        ("dhat", C.c_double),
+        ("kappa", C.c_double),
+        ("eta", C.c_double),
+        ("newton_tol", C.c_double),
+        ("newton_max_iters", C.c_int32),
+        ("ls_max_iters", C.c_int32),
+    ]
+
+
+class NxdIpcStats(C.Structure):
+    _fields_ = [
+        ("newton_iterations", C.c_int32),
+        ("converged", C.c_int32),
+        ("line_search_failed", C.c_int32),
+        ("solve_failed", C.c_int32),
+        ("last_alpha_max", C.c_double),
+        ("energy", C.c_double),
+        ("n_pairs", C.c_int64),
+        ("n_active", C.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def ipc_params(dhat=1e-3, kappa=1e8, eta=0.1, newton_tol=1e-6, newton_max_iters=50, ls_max_iters=30) -> "NxdIpcParams":
+    return NxdIpcParams(dhat, kappa, eta, newton_tol, newton_max_iters, ls_max_iters)
+
+
 class NxdState(C.Structure):
     _fields_ = [
         ("position", _dp),

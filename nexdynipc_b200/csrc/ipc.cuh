@@ -133,6 +133,38 @@ __global__ void k_axpy_vec(const double* x, const double* dx, int n, double* out
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = x[i] + dx[i];
 }
 
+// full-IPC time step helpers: out = x + alpha dx; g = gr + s gb and its
+// negation; elementwise product; row-wise concatenation of two BSR matrices
+// (the second scaled by s), rows of the first before the second's
+__global__ void k_axpy_alpha(const double* x, const double* dx, double alpha, int n, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = x[i] + alpha * dx[i];
+}
+__global__ void k_grad_combine(const double* gr, const double* gb, double s, int n, double* g, double* neg) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double v = gr[i] + s * gb[i];
+        g[i] = v;
+        neg[i] = -v;
+    }
+}
+__global__ void k_mul_vec(const double* a, const double* b, int n, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = a[i] * b[i];
+}
+__global__ void k_bsr_concat(int N, const int* rpa, const int* cia, const double* va, const int* rpb, const int* cib,
+                             const double* vb, double s, const int* rpm, int* cim, double* vm) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int o = rpm[i];
+    for (int k = rpa[i]; k < rpa[i + 1]; ++k, ++o) {
+        cim[o] = cia[k];
+        for (int e = 0; e < 36; ++e) vm[36LL * o + e] = va[36LL * k + e];
+    }
+    if (!rpb) return;
+    for (int k = rpb[i]; k < rpb[i + 1]; ++k, ++o) {
+        cim[o] = cib[k];
+        for (int e = 0; e < 36; ++e) vm[36LL * o + e] = vb[36LL * k + e] * s;
+    }
+}
+
 // list[pos[i]] = i for every flagged i (pos = exclusive scan of flag)
 __global__ void k_compact(const int* flag, const int* pos, int n, int* list) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)

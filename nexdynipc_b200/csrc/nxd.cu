@@ -1128,13 +1128,16 @@ struct IpcState {
     GrowBuf e, grad12, lam, z, nterm, body, active, type, apos, alist;
     GrowBuf gkey, gval, gkey1, gval1, hkey, hval, hkey1, hval1;
     GrowBuf sflag, spos, sstart, gout, rowptr, colidx, vals, toi;
+    // full-IPC time step: rest-form and merged BSR, gradients, solve scratch
+    GrowBuf rrp, rci, rvv, rnz, mrp, mci, mvv, gr, gt, gneg, prod, xt, erow, items, iact, stat, val;
     std::vector<GrowBuf*> all() {
         return {&fbody, &fvert, &ebody, &evert, &x0, &x1, &pp0, &pq0, &pp1, &pq1, &wq0, &wq1, &qv, &qe,
                 &faces.k0, &faces.k1, &faces.i0, &faces.i1, &faces.leaf, &faces.nbox, &faces.child, &faces.parent,
                 &faces.flags, &faces.bounds, &edges.k0, &edges.k1, &edges.i0, &edges.i1, &edges.leaf, &edges.nbox,
                 &edges.child, &edges.parent, &edges.flags, &edges.bounds, &cnt, &off, &pt, &ee, &scal, &hist, &e,
                 &grad12, &lam, &z, &nterm, &body, &active, &type, &apos, &alist, &gkey, &gval, &gkey1, &gval1, &hkey,
-                &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi};
+                &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &rrp, &rci, &rvv,
+                &rnz, &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &val};
     }
     void release() { for (GrowBuf* b : all()) b->release(); }
 };
@@ -1168,13 +1171,14 @@ nxd_status ipc_prepare(nxd_ctx* c) {
 
 // World vertices at x (host 6N; NULL = the current poses) into wq0, and at
 // x + dx into wq1 when dx is given.
-nxd_status ipc_pose(nxd_ctx* c, const double* x, const double* dx) {
+nxd_status ipc_pose(nxd_ctx* c, const double* x, const double* dx, bool on_device = false) {
     IpcState* s = c->ipc;
     const int N = c->N;
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     IPC_ENSURE(s->pp0, 24 * (size_t)N); IPC_ENSURE(s->pq0, 32 * (size_t)N); IPC_ENSURE(s->wq0, 24 * (size_t)c->nv);
     IPC_ENSURE(s->x0, 48 * (size_t)N);
     if (x) {
-        NXD_CUDA(cudaMemcpyAsync(s->x0.p, x, 48 * (size_t)N, cudaMemcpyHostToDevice, c->stream));
+        NXD_CUDA(cudaMemcpyAsync(s->x0.p, x, 48 * (size_t)N, kind, c->stream));
         k_pose_at_x<<<grid_for(N, 128), 128, 0, c->stream>>>(N, s->x0.as<double>(), c->quat, s->pp0.as<double>(), s->pq0.as<double>());
     } else {
         NXD_CUDA(cudaMemcpyAsync(s->pp0.p, c->pos, 24 * (size_t)N, cudaMemcpyDeviceToDevice, c->stream));
@@ -1185,7 +1189,7 @@ nxd_status ipc_pose(nxd_ctx* c, const double* x, const double* dx) {
     if (dx) {
         IPC_ENSURE(s->x1, 48 * (size_t)N); IPC_ENSURE(s->pp1, 24 * (size_t)N); IPC_ENSURE(s->pq1, 32 * (size_t)N);
         IPC_ENSURE(s->wq1, 24 * (size_t)c->nv);
-        NXD_CUDA(cudaMemcpyAsync(s->x1.p, dx, 48 * (size_t)N, cudaMemcpyHostToDevice, c->stream));
+        NXD_CUDA(cudaMemcpyAsync(s->x1.p, dx, 48 * (size_t)N, kind, c->stream));
         k_axpy_vec<<<grid_for(6 * N, 256), 256, 0, c->stream>>>(s->x0.as<double>(), s->x1.as<double>(), 6 * N, s->x1.as<double>());
         k_pose_at_x<<<grid_for(N, 128), 128, 0, c->stream>>>(N, s->x1.as<double>(), c->quat, s->pp1.as<double>(), s->pq1.as<double>());
         k_world_vertices<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(c->geo, c->nv, c->vbody, s->pp1.as<double>(),
@@ -1325,17 +1329,16 @@ nxd_status nxd_ipc_candidates(nxd_ctx* c, const double* x, const double* dx, dou
     return (pt && s->n_pt > pt_cap) || (ee && s->n_ee > ee_cap) ? NXD_CAPACITY : NXD_OK;
 }
 
-nxd_status nxd_ipc_barrier(nxd_ctx* c, const double* x, double dhat, double kappa, double* energy, double* grad, int32_t* row_ptr,
-                           int32_t* col_idx, double* vals, int64_t cap_blocks, int64_t* nnzb, int64_t* n_pairs,
-                           int64_t* n_active) {
-    if (!c || !(dhat > 0.0) || !(kappa >= 0.0)) return NXD_INVALID_ARGUMENT;
-    nxd_status st = ipc_prepare(c);
-    if (st == NXD_OK) st = ipc_pose(c, x, nullptr);
-    if (st == NXD_OK) st = ipc_candidates(c, false, dhat);
-    if (st != NXD_OK) return st;
+}  // extern "C"
+
+namespace {
+
+// The barrier form over the candidates of the last ipc_candidates call:
+// energy (to the host), and with `full` the gradient in s->gout and the PSD
+// BSR Hessian in s->rowptr / s->colidx / s->vals (*nh blocks).
+nxd_status ipc_barrier_eval(nxd_ctx* c, double dhat, double kappa, bool full, double* energy, int* n_active, int* nh_out) {
     IpcState* s = c->ipc;
     const int N = c->N, n = s->n_pt + s->n_ee;
-    if (n_pairs) *n_pairs = n;
     const IpcPairs P{s->pt.as<int>(), s->n_pt, s->ee.as<int>(), s->n_ee};
     const IpcPose ps{s->wq0.as<double>(), s->pp0.as<double>()};
     const size_t nn = std::max(n, 1);
@@ -1357,6 +1360,7 @@ nxd_status nxd_ipc_barrier(nxd_ctx* c, const double* x, double dhat, double kapp
     NXD_CUDA(cudaStreamSynchronize(c->stream));
     if (energy) *energy = eh;
     if (n_active) *n_active = na;
+    if (!full) return NXD_OK;
     // contributions, stable-sorted by body / by (row body, col body)
     IPC_ENSURE(s->gkey, 16 * (size_t)std::max(na, 1)); IPC_ENSURE(s->gval, 8 * (size_t)std::max(na, 1));
     IPC_ENSURE(s->hkey, 32 * (size_t)std::max(na, 1)); IPC_ENSURE(s->hval, 16 * (size_t)std::max(na, 1));
@@ -1364,7 +1368,7 @@ nxd_status nxd_ipc_barrier(nxd_ctx* c, const double* x, double dhat, double kapp
         k_ipc_contrib<<<grid_for(na, 128), 128, 0, c->stream>>>(s->alist.as<int>(), na, s->body.as<int>(), N,
                                                                  s->gkey.as<unsigned long long>(), s->gval.as<int>(),
                                                                  s->hkey.as<unsigned long long>(), s->hval.as<int>());
-    st = radix_sort(c, s->gkey, s->gval, s->gkey1, s->gval1, 2 * na, 0, bits_for((unsigned long long)N));
+    nxd_status st = radix_sort(c, s->gkey, s->gval, s->gkey1, s->gval1, 2 * na, 0, bits_for((unsigned long long)N));
     if (st == NXD_OK)
         st = radix_sort(c, s->hkey, s->hval, s->hkey1, s->hval1, 4 * na, 0, bits_for((unsigned long long)N * (unsigned long long)N));
     if (st != NXD_OK) return st;
@@ -1380,17 +1384,11 @@ nxd_status nxd_ipc_barrier(nxd_ctx* c, const double* x, double dhat, double kapp
                                                                     s->sstart.as<int>(), s->scal.as<int>() + 2,
                                                                     s->grad12.as<double>(), s->gout.as<double>());
     }
-    if (grad) {
-        NXD_CUDA(cudaMemcpyAsync(grad, s->gout.p, 48 * (size_t)N, cudaMemcpyDeviceToHost, c->stream));
-        NXD_CUDA(cudaStreamSynchronize(c->stream));
-    }
     int nh = 0;
     if (na) {
         st = ipc_segments(c, s->hkey.as<unsigned long long>(), 4 * na, &nh);
         if (st != NXD_OK) return st;
     }
-    if (nnzb) *nnzb = nh;
-    if (nh > cap_blocks && (col_idx || vals)) return NXD_CAPACITY;
     IPC_ENSURE(s->rowptr, 4 * (size_t)(N + 1)); IPC_ENSURE(s->colidx, 4 * (size_t)std::max(nh, 1));
     IPC_ENSURE(s->vals, 288 * (size_t)std::max(nh, 1));
     if (nh)
@@ -1401,6 +1399,49 @@ nxd_status nxd_ipc_barrier(nxd_ctx* c, const double* x, double dhat, double kapp
     if (nh) k_ipc_rowptr<<<grid_for(N + 1, 128), 128, 0, c->stream>>>(s->hkey.as<unsigned long long>(), s->sstart.as<int>(),
                                                                         s->scal.as<int>() + 2, N, s->rowptr.as<int>());
     else NXD_CUDA(cudaMemsetAsync(s->rowptr.p, 0, 4 * (size_t)(N + 1), c->stream));
+    if (nh_out) *nh_out = nh;
+    NXD_CUDA(cudaGetLastError());
+    return NXD_OK;
+}
+
+// additive-CCD bound over the swept candidates of the last ipc_pose(x, dx)
+nxd_status ipc_accd(nxd_ctx* c, double eta, double* alpha) {
+    IpcState* s = c->ipc;
+    const int n = s->n_pt + s->n_ee;
+    IPC_ENSURE(s->toi, 8 * (size_t)std::max(n, 1));
+    const IpcPairs P{s->pt.as<int>(), s->n_pt, s->ee.as<int>(), s->n_ee};
+    double* d_a = reinterpret_cast<double*>(s->scal.as<char>() + 40);
+    if (n) k_ipc_accd<<<grid_for(n, 128), 128, 0, c->stream>>>(s->pg, P, s->wq0.as<double>(), s->wq1.as<double>(), eta, 1000,
+                                                                s->toi.as<double>());
+    k_min_reduce<<<1, 1024, 0, c->stream>>>(s->toi.as<double>(), n, 1.0, d_a);
+    NXD_CUDA(cudaMemcpyAsync(alpha, d_a, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    NXD_CUDA(cudaGetLastError());
+    return NXD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+nxd_status nxd_ipc_barrier(nxd_ctx* c, const double* x, double dhat, double kappa, double* energy, double* grad, int32_t* row_ptr,
+                           int32_t* col_idx, double* vals, int64_t cap_blocks, int64_t* nnzb, int64_t* n_pairs,
+                           int64_t* n_active) {
+    if (!c || !(dhat > 0.0) || !(kappa >= 0.0)) return NXD_INVALID_ARGUMENT;
+    nxd_status st = ipc_prepare(c);
+    if (st == NXD_OK) st = ipc_pose(c, x, nullptr);
+    if (st == NXD_OK) st = ipc_candidates(c, false, dhat);
+    if (st != NXD_OK) return st;
+    IpcState* s = c->ipc;
+    const int N = c->N;
+    if (n_pairs) *n_pairs = s->n_pt + s->n_ee;
+    int na = 0, nh = 0;
+    st = ipc_barrier_eval(c, dhat, kappa, true, energy, &na, &nh);
+    if (st != NXD_OK) return st;
+    if (n_active) *n_active = na;
+    if (grad) NXD_CUDA(cudaMemcpyAsync(grad, s->gout.p, 48 * (size_t)N, cudaMemcpyDeviceToHost, c->stream));
+    if (nnzb) *nnzb = nh;
+    if (nh > cap_blocks && (col_idx || vals)) { NXD_CUDA(cudaStreamSynchronize(c->stream)); return NXD_CAPACITY; }
     if (row_ptr) NXD_CUDA(cudaMemcpyAsync(row_ptr, s->rowptr.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, c->stream));
     if (col_idx && nh) NXD_CUDA(cudaMemcpyAsync(col_idx, s->colidx.p, 4 * (size_t)nh, cudaMemcpyDeviceToHost, c->stream));
     if (vals && nh) NXD_CUDA(cudaMemcpyAsync(vals, s->vals.p, 288 * (size_t)nh, cudaMemcpyDeviceToHost, c->stream));
@@ -1415,19 +1456,155 @@ nxd_status nxd_ipc_max_step(nxd_ctx* c, const double* x, const double* dx, doubl
     if (st == NXD_OK) st = ipc_pose(c, x, dx);
     if (st == NXD_OK) st = ipc_candidates(c, true, 0.0);
     if (st != NXD_OK) return st;
+    if (n_pairs) *n_pairs = c->ipc->n_pt + c->ipc->n_ee;
+    return ipc_accd(c, eta, alpha);
+}
+
+// Full-IPC time step: the x_tilde of implicit Euler (or Newmark) and the
+// reference's inertia, gravity, joint (fixed multipliers) and control forms,
+// with the primitive-pair barrier in place of the COM-distance contact forms.
+// Newton starts from the step-start configuration, which is free of
+// intersections, and follows NewtonSolver::minimize (|g|_inf test, Armijo
+// backtracking) with the CCD bound as the line search's first step, so no
+// iterate crosses a surface.  Every iterate rebuilds the LBVH candidates at
+// x (boxes inflated by dhat), and so does every trial point; the linear
+// solve is nxd_linear_solve's component LDL^T on the rest-form blocks
+// followed, row by row, by the barrier's blocks.
+nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_stats* out) {
+    if (!c || !p || !(dt > 0.0) || !(p->dhat > 0.0) || !(p->kappa >= 0.0) || !(p->eta > 0.0 && p->eta < 1.0) ||
+        p->newton_max_iters < 0 || p->ls_max_iters < 1)
+        return NXD_INVALID_ARGUMENT;
+    nxd_status st = ipc_prepare(c);
+    if (st != NXD_OK) return st;
     IpcState* s = c->ipc;
-    const int n = s->n_pt + s->n_ee;
-    if (n_pairs) *n_pairs = n;
-    IPC_ENSURE(s->toi, 8 * (size_t)std::max(n, 1));
-    const IpcPairs P{s->pt.as<int>(), s->n_pt, s->ee.as<int>(), s->n_ee};
-    double* d_a = reinterpret_cast<double*>(s->scal.as<char>() + 40);
-    if (n) k_ipc_accd<<<grid_for(n, 128), 128, 0, c->stream>>>(s->pg, P, s->wq0.as<double>(), s->wq1.as<double>(), eta, 1000,
-                                                                s->toi.as<double>());
-    k_min_reduce<<<1, 1024, 0, c->stream>>>(s->toi.as<double>(), n, 1.0, d_a);
-    NXD_CUDA(cudaMemcpyAsync(alpha, d_a, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    const int N = c->N, n6 = 6 * N;
+    cudaStream_t sm = c->stream;
+    StepCfg cfg = step_cfg(c);
+    cfg.enable_adaptive = 0;
+    cfg.enable_friction = 0;
+    k_step_setup<<<grid_for(std::max(N, c->D), 128), 128, 0, sm>>>(cfg, dt, c->pos, c->quat, c->vel, c->omega, c->lacc, c->aacc, c->x,
+        c->xhat, c->xprev, c->vprev, c->aprev, c->pos0, c->quat0, c->sc, c->dprm, c->dfilt, c->dfinit, c->dhas_prev);
+    NXD_CUDA(cudaMemsetAsync(&c->sc->n_contacts, 0, sizeof(int), sm));
+    NXD_CUDA(cudaMemcpyAsync(c->x, c->xprev, 8 * (size_t)n6, cudaMemcpyDeviceToDevice, sm));
+    const double scale = cfg.newmark ? (cfg.beta * dt) * dt : dt * dt;
+    const long long cap_r = N + 2LL * (c->J + c->D);
+    IPC_ENSURE(s->rrp, 4 * (size_t)(N + 1)); IPC_ENSURE(s->rci, 4 * (size_t)std::max(cap_r, 1LL));
+    IPC_ENSURE(s->rvv, 288 * (size_t)std::max(cap_r, 1LL));
+    IPC_ENSURE(s->rnz, 8); IPC_ENSURE(s->mrp, 4 * (size_t)(N + 1)); IPC_ENSURE(s->gr, 8 * (size_t)n6);
+    IPC_ENSURE(s->gt, 8 * (size_t)n6); IPC_ENSURE(s->gneg, 8 * (size_t)n6); IPC_ENSURE(s->prod, 8 * (size_t)n6);
+    IPC_ENSURE(s->xt, 8 * (size_t)n6); IPC_ENSURE(s->stat, 8); IPC_ENSURE(s->val, 16);
+    double* x = c->x;
+    double* val = s->val.as<double>();
+    std::vector<int> rpr(N + 1), rpb(N + 1), rpm(N + 1);
+    std::vector<double> gh(n6);
+    auto rest_value = [&](const double* xx, double* v) -> nxd_status {
+        k_form_eval<<<1, kSolverThreads, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 0, xx, val, nullptr, nullptr, nullptr, 0, nullptr);
+        NXD_CUDA(cudaMemcpyAsync(v, val, sizeof(double), cudaMemcpyDeviceToHost, sm));
+        NXD_CUDA(cudaStreamSynchronize(sm));
+        return NXD_OK;
+    };
+    auto barrier_value = [&](const double* xx, double* v) -> nxd_status {
+        nxd_status r = ipc_pose(c, xx, nullptr, true);
+        if (r == NXD_OK) r = ipc_candidates(c, false, p->dhat);
+        if (r == NXD_OK) r = ipc_barrier_eval(c, p->dhat, p->kappa, false, v, nullptr, nullptr);
+        return r;
+    };
+    int iters = 0, conv = 0, lsfail = 0, solvefail = 0, na = 0;
+    double amax = 1.0, fx = 0.0;
+    int64_t npairs = 0;
+    for (int it = 0; it < p->newton_max_iters; ++it) {
+        iters = it;
+        // gradient at x: rest forms, then the barrier over the candidates at x
+        k_form_eval<<<1, kSolverThreads, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 1, x, s->gr.as<double>(), nullptr, nullptr,
+                                                  nullptr, 0, nullptr);
+        double eb = 0.0;
+        int nh = 0;
+        st = ipc_pose(c, x, nullptr, true);
+        if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
+        if (st == NXD_OK) st = ipc_barrier_eval(c, p->dhat, p->kappa, true, &eb, &na, &nh);
+        if (st != NXD_OK) return st;
+        npairs = s->n_pt + s->n_ee;
+        k_grad_combine<<<grid_for(n6, 256), 256, 0, sm>>>(s->gr.as<double>(), s->gout.as<double>(), scale, n6,
+                                                          s->gt.as<double>(), s->gneg.as<double>());
+        NXD_CUDA(cudaMemcpyAsync(gh.data(), s->gt.p, 8 * (size_t)n6, cudaMemcpyDeviceToHost, sm));
+        NXD_CUDA(cudaStreamSynchronize(sm));
+        double ginf = 0.0;
+        for (double v : gh) ginf = std::max(ginf, std::fabs(v));
+        if (ginf < p->newton_tol) { conv = 1; break; }
+        // Hessian: rest-form blocks, then the barrier's, row by row
+        k_form_eval<<<1, kSolverThreads, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 2, x, nullptr, s->rrp.as<int>(), s->rci.as<int>(),
+                                                  s->rvv.as<double>(), cap_r, s->rnz.as<long long>());
+        long long nzr = 0;
+        NXD_CUDA(cudaMemcpyAsync(&nzr, s->rnz.p, sizeof(long long), cudaMemcpyDeviceToHost, sm));
+        NXD_CUDA(cudaMemcpyAsync(rpr.data(), s->rrp.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, sm));
+        NXD_CUDA(cudaMemcpyAsync(rpb.data(), s->rowptr.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, sm));
+        NXD_CUDA(cudaStreamSynchronize(sm));
+        if (nzr < 0 || nzr > cap_r) return NXD_CAPACITY;
+        rpm[0] = 0;
+        for (int i = 0; i < N; ++i) rpm[i + 1] = rpm[i] + (rpr[i + 1] - rpr[i]) + (nh ? rpb[i + 1] - rpb[i] : 0);
+        const long long nzm = rpm[N];
+        IPC_ENSURE(s->mci, 4 * (size_t)std::max<long long>(nzm, 1)); IPC_ENSURE(s->mvv, 288 * (size_t)std::max<long long>(nzm, 1));
+        IPC_ENSURE(s->erow, 4 * (size_t)std::max<long long>(nzm, 1)); IPC_ENSURE(s->items, 4 * (size_t)std::max<long long>(nzm, 1));
+        IPC_ENSURE(s->iact, 4 * (size_t)std::max<long long>(nzm, 1));
+        NXD_CUDA(cudaMemcpyAsync(s->mrp.p, rpm.data(), 4 * (size_t)(N + 1), cudaMemcpyHostToDevice, sm));
+        k_bsr_concat<<<grid_for(N, 128), 128, 0, sm>>>(N, s->rrp.as<int>(), s->rci.as<int>(), s->rvv.as<double>(),
+                                                       nh ? s->rowptr.as<int>() : nullptr, s->colidx.as<int>(),
+                                                       s->vals.as<double>(), scale, s->mrp.as<int>(), s->mci.as<int>(),
+                                                       s->mvv.as<double>());
+        // H dx = -g
+        Solver S = c->S;
+        S.ext_n = (int)nzm; S.ext_row = s->erow.as<int>(); S.ext_col = s->mci.as<int>(); S.ext_vals = s->mvv.as<double>();
+        S.items = s->items.as<int>(); S.iact = s->iact.as<int>(); S.status = s->stat.as<int>();
+        NXD_CUDA(cudaMemsetAsync(s->stat.p, 0, sizeof(int), sm));
+        k_bsr_prepare<<<grid_for(N, 128), 128, 0, sm>>>(S, s->mrp.as<int>(), s->gneg.as<double>(), s->erow.as<int>());
+        k_linear_solve<<<1, kNewtonThreads, kNewtonDynSmem, sm>>>(S);
+        int fail = 0, capst = 0;
+        NXD_CUDA(cudaMemcpyAsync(&fail, S.solve_fail, sizeof(int), cudaMemcpyDeviceToHost, sm));
+        NXD_CUDA(cudaMemcpyAsync(&capst, s->stat.p, sizeof(int), cudaMemcpyDeviceToHost, sm));
+        NXD_CUDA(cudaStreamSynchronize(sm));
+        if (capst) return NXD_CAPACITY;
+        if (fail) { solvefail = 1; break; }
+        double* dx = c->S.dx;
+        // the step bound: additive CCD over the swept candidates
+        st = ipc_pose(c, x, dx, true);
+        if (st == NXD_OK) st = ipc_candidates(c, true, 0.0);
+        if (st == NXD_OK) st = ipc_accd(c, p->eta, &amax);
+        if (st != NXD_OK) return st;
+        // line search from min(1, bound)
+        double er = 0.0;
+        if ((st = rest_value(x, &er)) != NXD_OK) return st;
+        fx = er + scale * eb;
+        k_mul_vec<<<grid_for(n6, 256), 256, 0, sm>>>(s->gt.as<double>(), dx, n6, s->prod.as<double>());
+        k_tree_sum<<<1, 1024, 0, sm>>>(s->prod.as<double>(), n6, val + 1);
+        double descent = 0.0;
+        NXD_CUDA(cudaMemcpyAsync(&descent, val + 1, sizeof(double), cudaMemcpyDeviceToHost, sm));
+        NXD_CUDA(cudaStreamSynchronize(sm));
+        if (descent > 0) { lsfail = 1; break; }
+        double alpha = std::min(1.0, amax);
+        bool done = false;
+        for (int ls = 0; ls < p->ls_max_iters; ++ls) {
+            k_axpy_alpha<<<grid_for(n6, 256), 256, 0, sm>>>(x, dx, alpha, n6, s->xt.as<double>());
+            double ert = 0.0, ebt = 0.0;
+            if ((st = rest_value(s->xt.as<double>(), &ert)) != NXD_OK) return st;
+            if ((st = barrier_value(s->xt.as<double>(), &ebt)) != NXD_OK) return st;
+            const double fn = ert + scale * ebt;
+            if (fn <= fx + c->s.ls_c1 * alpha * descent) { done = true; fx = fn; break; }
+            alpha *= c->s.ls_rho;
+        }
+        if (!done) { lsfail = 1; break; }
+        NXD_CUDA(cudaMemcpyAsync(x, s->xt.p, 8 * (size_t)n6, cudaMemcpyDeviceToDevice, sm));
+        if (it == p->newton_max_iters - 1) iters = p->newton_max_iters;
+    }
+    k_update_state<<<grid_for(N, 128), 128, 0, sm>>>(cfg, c->x, c->xprev, c->vprev, c->xhat, c->aprev, c->pos, c->quat, c->vel,
+                                                   c->omega, c->lacc, c->aacc, c->sc, c->da, c->db, c->dprm, c->dfilt);
+    NXD_CUDA(cudaStreamSynchronize(sm));
     NXD_CUDA(cudaGetLastError());
-    return NXD_OK;
+    if (out) {
+        out->newton_iterations = iters; out->converged = conv; out->line_search_failed = lsfail;
+        out->solve_failed = solvefail; out->last_alpha_max = amax; out->energy = fx; out->n_pairs = npairs;
+        out->n_active = na;
+    }
+    return solvefail ? NXD_FACTOR_FAILED : NXD_OK;
 }
 
 // ---------------------------------------------------------------------------

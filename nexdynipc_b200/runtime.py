@@ -57,6 +57,7 @@ def lib():
     L.nxd_normal_forces.argtypes = [vp, dp, dp, C.c_int32]
     L.nxd_eval_all.argtypes = [vp, dp, dp, dp, ip, ip, dp, C.c_int64, i64p]
     L.nxd_linear_solve.argtypes = [vp, C.POINTER(abi.NxdBsr), dp, dp, C.POINTER(abi.NxdSolveStats)]
+    L.nxd_ipc_step.argtypes = [vp, C.c_double, C.POINTER(abi.NxdIpcParams), C.POINTER(abi.NxdIpcStats)]
     L.nxd_batch_create.argtypes = [C.POINTER(abi.NxdSceneDesc), C.c_int32, C.POINTER(vp)]
     L.nxd_batch_destroy.argtypes = [vp]
     L.nxd_batch_step.argtypes = [vp, dp]
@@ -314,6 +315,14 @@ class Context:
                                                     C.byref(npairs), C.byref(nact)))
         m = nnzb.value
         return e.value, g, (rp, ci[:m], vv[:m]), npairs.value, nact.value
+
+    def ipc_step(self, params=None, dt=None) -> dict:
+        """One full-IPC time step (nxd_ipc_step); returns its statistics."""
+        p = params if params is not None else abi.ipc_params()
+        st = abi.NxdIpcStats()
+        _check("nxd_ipc_step", lib().nxd_ipc_step(self.h, float(self.scene.dt if dt is None else dt), C.byref(p),
+                                                  C.byref(st)))
+        return st.as_dict()
 
     def ipc_max_step(self, x, dx, eta: float = 0.1):
         """(alpha, n_pairs): additive-CCD bound of the step x -> x + dx."""

@@ -201,8 +201,25 @@ int nxo_ipc_candidates(nxo_world* w, const double* x, const double* dx, double i
 // Barrier over the candidates at x (boxes inflated by dhat): energy (fixed
 // tree over all pairs, PT then EE), gradient (6N, pair order) and, when H is
 // not NULL, the dense 6N x 6N PSD-projected Hessian (pair order per block).
+}  // extern "C"
+
+// nxo_ipc_barrier with, in `blocks` (when given), the body blocks the active
+// pairs touch: (a, a), (a, b), (b, a), (b, b) for each, sorted by (row, col),
+// the block structure of the device's BSR Hessian.
+int ipc_barrier_cpu(nxo_world* w, const double* x, double dhat, double kappa, double* energy, double* grad, double* H,
+                    std::vector<std::pair<int, int>>* blocks, int64_t* n_pairs, int64_t* n_active);
+
+extern "C" {
+
 int nxo_ipc_barrier(nxo_world* w, const double* x, double dhat, double kappa, double* energy, double* grad, double* H,
                     int64_t* n_pairs, int64_t* n_active) {
+    return ipc_barrier_cpu(w, x, dhat, kappa, energy, grad, H, nullptr, n_pairs, n_active);
+}
+
+}  // extern "C"
+
+int ipc_barrier_cpu(nxo_world* w, const double* x, double dhat, double kappa, double* energy, double* grad, double* H,
+                    std::vector<std::pair<int, int>>* blocks, int64_t* n_pairs, int64_t* n_active) {
     const Geo g = load(w, x, nullptr);
     std::vector<int32_t> P, E;
     candidates(g, dhat, P, E);
@@ -221,6 +238,10 @@ int nxo_ipc_barrier(nxo_world* w, const double* x, double dhat, double kappa, do
         e[p] = ev.e;
         if (!(ev.d2 < dhat * dhat)) continue;
         ++na;
+        if (blocks) {
+            blocks->push_back({bA, bA}); blocks->push_back({bA, bB});
+            blocks->push_back({bB, bA}); blocks->push_back({bB, bB});
+        }
         double g12[12];
         ipc::chain12(ev.grad, side, arm, g12);
         const int b[2] = {bA, bB};
@@ -242,8 +263,14 @@ int nxo_ipc_barrier(nxo_world* w, const double* x, double dhat, double kappa, do
     if (energy) *energy = tree_sum(e);
     if (n_pairs) *n_pairs = (int64_t)n;
     if (n_active) *n_active = na;
+    if (blocks) {
+        std::sort(blocks->begin(), blocks->end());
+        blocks->erase(std::unique(blocks->begin(), blocks->end()), blocks->end());
+    }
     return NXD_OK;
 }
+
+extern "C" {
 
 // Largest step fraction in [0, 1] along x -> x + dx that additive CCD allows
 // (eta: kept fraction of each pair's initial distance), over the pairs whose

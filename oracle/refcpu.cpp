@@ -42,6 +42,11 @@
 #include <omp.h>
 #endif
 
+
+// primitive-pair barrier of ipc_cpu.cpp with its block structure
+int ipc_barrier_cpu(nxo_world* w, const double* x, double dhat, double kappa, double* energy, double* grad, double* H,
+                    std::vector<std::pair<int, int>>* blocks, int64_t* n_pairs, int64_t* n_active);
+
 namespace {
 
 constexpr double kInf = std::numeric_limits<double>::infinity();
@@ -2385,6 +2390,132 @@ void nxo_set_options(nxo_world* w, int literal, int stride, int threads) {
     w->literal_min_distance = literal;
     w->md_stride = std::max(1, stride);
     w->num_threads = std::max(1, threads);
+}
+
+// Full-IPC time step, restating nxd_ipc_step on the oracle's forms and
+// solve: step()'s set-up with the contact forms off, Newton from the
+// step-start configuration with the |g|_inf test, the rest-form triplets
+// followed by the barrier's (the body blocks its active pairs touch, row by
+// row), the CCD bound as the first trial of the Armijo search, then step()'s
+// write-back.
+int nxo_ipc_step(nxo_world* w, double dt, const nxd_ipc_params* p, nxd_ipc_stats* out) {
+    const nxd_settings& s = w->s;
+    const int N = (int)w->bodies.size(), n = 6 * N;
+    std::vector<double> x(n, 0.0), v(n, 0.0), a(n, 0.0);
+    for (int i = 0; i < N; ++i) {
+        const Body& b = w->bodies[i];
+        for (int k = 0; k < 3; ++k) {
+            x[i * 6 + k] = b.position[k]; x[i * 6 + 3 + k] = 0.0;
+            v[i * 6 + k] = b.velocity[k]; v[i * 6 + 3 + k] = b.angular_velocity[k];
+            a[i * 6 + k] = b.linear_acceleration[k]; a[i * 6 + 3 + k] = b.angular_acceleration[k];
+        }
+    }
+    w->x_prev = x; w->v_prev = v; w->a_prev = a; w->dt = dt;
+    const bool newmark = s.integrator == NXD_INTEGRATOR_IMPLICIT_NEWMARK;
+    const double nm_s1 = (dt * dt) * (0.5 - s.newmark_beta);
+    std::vector<double> x_hat(n);
+    for (int i = 0; i < n; ++i) {
+        x_hat[i] = x[i] + dt * v[i];
+        if (newmark) x_hat[i] = x_hat[i] + nm_s1 * a[i];
+    }
+    w->x_hat = x_hat;
+    w->barrier_form = w->friction_form = w->barrier_in_forms = false;
+    w->barrier_contacts.clear();
+    w->friction_contacts.clear();
+    for (auto& d : w->drives) {
+        d.dt = dt;
+        if (d.delay_tau <= 0.0) { d.filtered = d.v_target; d.filter_init = false; }
+        else if (!d.filter_init) { d.filtered = d.v_target; d.filter_init = true; }
+        else if (d.dt > 0.0) { const double al = d.dt / (d.delay_tau + d.dt); d.filtered += al * (d.v_target - d.filtered); }
+        d.gA = d.bodyA >= 0 ? d.bodyA * 6 : -1;
+        d.gB = d.bodyB >= 0 ? d.bodyB * 6 : -1;
+        d.has_prev = false;
+    }
+    for (auto& J : w->joints) {
+        const int ia = body_index_of_id(w, J.bodyA_id);
+        if (J.type == NXD_JOINT_FIXED) {
+            J.gA = ia * 6; J.qA_ref = w->bodies[ia].orientation;
+        } else {
+            const int ib = body_index_of_id(w, J.bodyB_id);
+            J.gA = ia * 6; J.gB = ib * 6;
+            J.pA_ref = w->bodies[ia].position; J.qA_ref = w->bodies[ia].orientation;
+            J.pB_ref = w->bodies[ib].position; J.qB_ref = w->bodies[ib].orientation;
+        }
+    }
+    const double sc = scaling(w);
+    std::vector<double> xn = x, gr, gb(n), g(n), Hb((size_t)n * n), dx, xt(n), prod(n);
+    std::vector<Trip> trips;
+    std::vector<std::pair<int, int>> blocks;
+    int iters = 0, conv = 0, lsfail = 0, solvefail = 0;
+    int64_t npairs = 0, na = 0;
+    double amax = 1.0, fx = 0.0;
+    for (int it = 0; it < p->newton_max_iters; ++it) {
+        iters = it;
+        problem_gradient(w, xn, gr);
+        double eb = 0.0;
+        blocks.clear();
+        ipc_barrier_cpu(w, xn.data(), p->dhat, p->kappa, &eb, gb.data(), Hb.data(), &blocks, &npairs, &na);
+        for (int i = 0; i < n; ++i) g[i] = gr[i] + sc * gb[i];
+        double ginf = 0.0;
+        for (double vv : g) ginf = std::max(ginf, std::fabs(vv));
+        if (ginf < p->newton_tol) { conv = 1; break; }
+        problem_hessian(w, xn, trips);
+        for (const auto& bl : blocks)
+            for (int r = 0; r < 6; ++r)
+                for (int c = 0; c < 6; ++c) {
+                    const int gi = 6 * bl.first + r, gj = 6 * bl.second + c;
+                    trips.push_back({gi, gj, Hb[(size_t)gi * n + gj] * sc});
+                }
+        std::vector<double> rhs(n);
+        for (int i = 0; i < n; ++i) rhs[i] = -g[i];
+        if (!solve_system(n, trips, rhs, dx)) { solvefail = 1; break; }
+        int64_t np2 = 0;
+        amax = nxo_ipc_max_step(w, xn.data(), dx.data(), p->eta, &np2);
+        fx = problem_value(w, xn) + sc * eb;
+        for (int i = 0; i < n; ++i) prod[i] = g[i] * dx[i];
+        const double descent = tree_sum(prod);
+        if (descent > 0) { lsfail = 1; break; }
+        double alpha = std::min(1.0, amax);
+        bool done = false;
+        for (int ls = 0; ls < p->ls_max_iters; ++ls) {
+            for (int i = 0; i < n; ++i) xt[i] = xn[i] + alpha * dx[i];
+            const double ert = problem_value(w, xt);
+            double ebt = 0.0;
+            ipc_barrier_cpu(w, xt.data(), p->dhat, p->kappa, &ebt, nullptr, nullptr, nullptr, nullptr, nullptr);
+            const double fn = ert + sc * ebt;
+            if (fn <= fx + s.ls_c1 * alpha * descent) { done = true; fx = fn; break; }
+            alpha *= s.ls_rho;
+        }
+        if (!done) { lsfail = 1; break; }
+        xn = xt;
+        if (it == p->newton_max_iters - 1) iters = p->newton_max_iters;
+    }
+    std::vector<double> vn(n), an(n);
+    if (newmark) {
+        const double den = (s.newmark_beta * dt) * dt;
+        for (int i = 0; i < n; ++i) an[i] = (xn[i] - w->x_hat[i]) / den;
+        for (int i = 0; i < n; ++i)
+            vn[i] = w->v_prev[i] + dt * ((1.0 - s.newmark_gamma) * w->a_prev[i] + s.newmark_gamma * an[i]);
+    } else {
+        for (int i = 0; i < n; ++i) vn[i] = (xn[i] - w->x_prev[i]) / dt;
+        for (int i = 0; i < n; ++i) an[i] = (vn[i] - w->v_prev[i]) / dt;
+    }
+    for (int i = 0; i < N; ++i) {
+        Body& b = w->bodies[i];
+        const int idx = i * 6;
+        b.linear_acceleration = xseg(an, idx);
+        b.angular_acceleration = xseg(an, idx + 3);
+        b.velocity = xseg(vn, idx);
+        b.angular_velocity = xseg(vn, idx + 3);
+        b.position = xseg(xn, idx);
+        b.orientation = update_rotation_gt(b.orientation, xseg(xn, idx + 3));
+    }
+    if (out) {
+        out->newton_iterations = iters; out->converged = conv; out->line_search_failed = lsfail;
+        out->solve_failed = solvefail; out->last_alpha_max = amax; out->energy = fx; out->n_pairs = npairs;
+        out->n_active = na;
+    }
+    return solvefail ? NXD_FACTOR_FAILED : NXD_OK;
 }
 
 int nxo_step(nxo_world* w, double dt) {

@@ -61,6 +61,8 @@ int nxo_normal_forces(nxo_world* w, const double* x, double* out, int32_t n);
 /* LinearSolver on a caller's 6x6-block BSR matrix: blocks become triplets
  * in storage order, then the same per-component dense LDL^T as the Newton
  * solve.  Returns NXD_OK or NXD_FACTOR_FAILED. */
+/* Full-IPC time step (restates nxd_ipc_step). */
+int nxo_ipc_step(nxo_world* w, double dt, const nxd_ipc_params* p, nxd_ipc_stats* stats);
 int nxo_linear_solve(int32_t n_rows, int64_t nnzb, const int32_t* row_ptr, const int32_t* col_idx,
                      const double* vals, const double* b, double* x);
 /* LDL^T solve of H dx = b with the oracle's solver (dense H input). */

@@ -57,6 +57,7 @@ def lib():
     L.nxo_normal_forces.argtypes = [vp, dp, dp, C.c_int32]
     ip = C.POINTER(C.c_int32)
     L.nxo_linear_solve.argtypes = [C.c_int32, C.c_int64, ip, ip, dp, dp, dp]
+    L.nxo_ipc_step.argtypes = [vp, C.c_double, C.POINTER(abi.NxdIpcParams), C.POINTER(abi.NxdIpcStats)]
     L.nxo_ldlt_solve.argtypes = [dp, C.c_int32, dp, dp]
     L.nxo_select_top_k.argtypes = [dp, C.c_int32, C.c_int32, ip]
     L.nxo_libm.argtypes = [C.c_int32, dp, dp, dp, C.c_int32]
@@ -235,6 +236,15 @@ class OracleWorld:
         lib().nxo_ipc_barrier(self.h, _d(x), dhat, kappa, C.byref(e), abi.dptr(g), abi.dptr(H) if hessian else None,
                               C.byref(npairs), C.byref(nact))
         return e.value, g, H, npairs.value, nact.value
+
+    def ipc_step(self, params=None, dt=None) -> dict:
+        """One full-IPC time step (nxo_ipc_step): statistics plus "status"."""
+        p = params if params is not None else abi.ipc_params()
+        st = abi.NxdIpcStats()
+        rc = lib().nxo_ipc_step(self.h, float(self.scene.dt if dt is None else dt), C.byref(p), C.byref(st))
+        out = st.as_dict()
+        out["status"] = int(rc)
+        return out
 
     def ipc_max_step(self, x, dx, eta: float = 0.1):
         n = C.c_int64()
