@@ -253,6 +253,34 @@ def diff_leg(torch):
             "finite": bool(np.isfinite(J).all())}
 
 
+def ipc_step_leg(n_cubes: int = 8, settle: int = 30, steps: int = 20):
+    """Full-IPC time step (nxd_ipc_step) on a tower of tilted cubes falling
+    onto a ground box: after `settle` steps (the cubes in contact), wall
+    clock of `steps` steps, each a host-ordered Newton loop of device calls
+    (candidates, barrier, rest forms, block solve, CCD bound, line search)."""
+    import time
+    from nexdynipc_b200 import abi, runtime, scenes
+    sc = scenes.ipc_drop(n_cubes=n_cubes)
+    ctx = runtime.Context(sc)
+    p = abi.ipc_params(dhat=1e-3, kappa=1e11, eta=0.1, newton_tol=1e-5, newton_max_iters=50, ls_max_iters=30)
+    for _ in range(settle):
+        ctx.ipc_step(p)
+    its, act, pairs, conv, lsf = [], [], [], 0, 0
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        st = ctx.ipc_step(p)
+        its.append(st["newton_iterations"]); act.append(st["n_active"]); pairs.append(st["n_pairs"])
+        conv += st["converged"]
+        lsf += st["line_search_failed"]
+    wall = time.perf_counter() - t0
+    ctx.close()
+    return {"workload": f"{n_cubes} tilted 0.2 m cubes on a ground box, dhat 1e-3, kappa 1e11, dt {sc.dt}",
+            "steps": steps, "steps_per_s": steps / wall, "newton_iterations_mean": float(np.mean(its)),
+            "active_pairs_mean": float(np.mean(act)), "candidate_pairs_mean": float(np.mean(pairs)),
+            "converged_steps": conv, "line_search_failures": lsf,
+            "timing": "wall clock per nxd_ipc_step (it synchronises)"}
+
+
 def mode_i_leg(ctx, sc, reps: int = 5):
     """Primitive-level contact model on the workload's current state, through
     the C ABI (host arrays in and out, each call synchronising): LBVH
@@ -489,6 +517,8 @@ def main():
     per_family = {FAMILIES[i]: {"ms": round(float(prof_ms[i]), 3), "launches": int(prof_n[i])} for i in range(9)}
 
     mode_i = None if args.no_mode_i else mode_i_leg(ctx, sc)
+    if mode_i is not None:
+        mode_i["step"] = ipc_step_leg()
 
     batched = None
     if not args.no_batched:

@@ -409,8 +409,9 @@ nxd_status nxd_ipc_max_step(nxd_ctx* ctx, const double* x, const double* dx, dou
  * x_tilde and the inertia, gravity, joint and control forms are nxd_step's
  * (joints with their current multipliers, no ALM update); the
  * primitive-pair barrier replaces the COM-distance contact forms.  Newton
- * starts from the step-start configuration and uses the |g|_inf test and
- * Armijo backtracking (settings.ls_c1, ls_rho) from min(1, CCD bound);
+ * starts from the step-start configuration and stops at |g|_inf < tol or at
+ * a Newton step with |dx|_inf < tol * dt (IPC's velocity test); Armijo
+ * backtracking (settings.ls_c1, ls_rho) starts from min(1, CCD bound);
  * candidates are rebuilt at every iterate and trial point; each system is
  * solved by nxd_linear_solve; the state is written back as nxd_step does.
  * No friction term. */

@@ -1465,8 +1465,10 @@ nxd_status nxd_ipc_max_step(nxd_ctx* c, const double* x, const double* dx, doubl
 // with the primitive-pair barrier in place of the COM-distance contact forms.
 // Newton starts from the step-start configuration, which is free of
 // intersections, and follows NewtonSolver::minimize (|g|_inf test, Armijo
-// backtracking) with the CCD bound as the line search's first step, so no
-// iterate crosses a surface.  Every iterate rebuilds the LBVH candidates at
+// backtracking) with the CCD bound as the line search's first step, and
+// also stops when the Newton step is below tol * dt (IPC's velocity test:
+// against a stiff barrier the absolute gradient test is out of reach in
+// FP64).  Every iterate rebuilds the LBVH candidates at
 // x (boxes inflated by dhat), and so does every trial point; the linear
 // solve is nxd_linear_solve's component LDL^T on the rest-form blocks
 // followed, row by row, by the barrier's blocks.
@@ -1565,6 +1567,12 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
         if (capst) return NXD_CAPACITY;
         if (fail) { solvefail = 1; break; }
         double* dx = c->S.dx;
+        // the velocity criterion of IPC: a Newton step below tol * dt ends it
+        NXD_CUDA(cudaMemcpyAsync(gh.data(), dx, 8 * (size_t)n6, cudaMemcpyDeviceToHost, sm));
+        NXD_CUDA(cudaStreamSynchronize(sm));
+        double dxinf = 0.0;
+        for (double v : gh) dxinf = std::max(dxinf, std::fabs(v));
+        if (dxinf < p->newton_tol * dt) { conv = 1; break; }
         // the step bound: additive CCD over the swept candidates
         st = ipc_pose(c, x, dx, true);
         if (st == NXD_OK) st = ipc_candidates(c, true, 0.0);

@@ -2394,7 +2394,7 @@ void nxo_set_options(nxo_world* w, int literal, int stride, int threads) {
 
 // Full-IPC time step, restating nxd_ipc_step on the oracle's forms and
 // solve: step()'s set-up with the contact forms off, Newton from the
-// step-start configuration with the |g|_inf test, the rest-form triplets
+// step-start configuration with the |g|_inf and step (< tol * dt) tests, the rest-form triplets
 // followed by the barrier's (the body blocks its active pairs touch, row by
 // row), the CCD bound as the first trial of the Armijo search, then step()'s
 // write-back.
@@ -2469,6 +2469,9 @@ int nxo_ipc_step(nxo_world* w, double dt, const nxd_ipc_params* p, nxd_ipc_stats
         std::vector<double> rhs(n);
         for (int i = 0; i < n; ++i) rhs[i] = -g[i];
         if (!solve_system(n, trips, rhs, dx)) { solvefail = 1; break; }
+        double dxinf = 0.0;
+        for (double vv : dx) dxinf = std::max(dxinf, std::fabs(vv));
+        if (dxinf < p->newton_tol * dt) { conv = 1; break; }
         int64_t np2 = 0;
         amax = nxo_ipc_max_step(w, xn.data(), dx.data(), p->eta, &np2);
         fx = problem_value(w, xn) + sc * eb;
