@@ -212,7 +212,9 @@ def diff_leg(torch):
     initial velocities, 16 masses and the friction coefficient by central
     differences, i.e. 131 worlds stepped as one batch.  Reports the device
     time of the 50 batched steps (CUDA events) and the wall time of the whole
-    Jacobian call (scene copies, batch creation, read-back)."""
+    Jacobian call (scene copies, batch creation, read-back), and the ratio
+    of the Jacobian's device time to one forward rollout's (forward plus
+    gradient over forward)."""
     import time
     from nexdynipc_b200 import diff, runtime, scenes
     sc = scenes.diff_scene()
@@ -241,16 +243,64 @@ def diff_leg(torch):
         return out
 
     diff.rollout_jacobian(sc, spec, theta, 2, bodies, runner=runner)      # warm-up (module load, graphs)
+    runner([sc], steps)                                                   # the forward rollout alone
+    fwd_s = times["device_s"]
     t0 = time.perf_counter()
     y, J = diff.rollout_jacobian(sc, spec, theta, steps, bodies, runner=runner)
     wall = time.perf_counter() - t0
     worlds = 2 * theta.size + 1
     return {"workload": f"{sc.n_bodies - 1} icospheres (162 V) on a ground box, {steps} steps, dt {sc.dt}",
             "parameters": int(theta.size), "outputs": int(y.size), "worlds": worlds,
-            "device_s": times["device_s"], "wall_s": wall,
+            "device_s": times["device_s"], "wall_s": wall, "forward_device_s": fwd_s,
+            "fwd_plus_grad_over_fwd": times["device_s"] / fwd_s,
             "scene_steps_per_s": worlds * steps / times["device_s"],
             "jacobians_per_s_wall": 1.0 / wall, "status": int(times["status"]),
             "finite": bool(np.isfinite(J).all())}
+
+
+def pcg_leg(n_bodies: int = 200000, iters: int = 60):
+    """Block-Jacobi PCG (nxd_pcg_solve) on a synthetic SPD block system of
+    the size a large full-IPC Newton system reaches: n_bodies 6x6 block rows,
+    each coupled to its neighbours at offsets 1, 64 and 4096 (7 blocks per
+    row, 400 MB of blocks at 200k bodies, far above L2), tol 0 so that
+    exactly `iters` iterations run; CUDA-event time of the iteration kernel.
+    Algorithmic bytes per iteration: every block once (288 B + 4 B index),
+    the row pointers, the inverse diagonal blocks twice (preconditioner in
+    the reduction and in the update), thirteen 6N-vector passes."""
+    from nexdynipc_b200 import runtime, scenes
+    rng = np.random.default_rng(9000)
+    n = n_bodies
+    rows, cols, blks = [np.arange(n)], [np.arange(n)], []
+    M = rng.normal(size=(n, 6, 6)) * 0.05
+    blks.append(np.einsum("nij,nkj->nik", M, M) + (1.0 + 36 * 0.1) * np.eye(6))
+    for o in (1, 64, 4096):
+        i = np.arange(n - o)
+        B = rng.uniform(-0.1, 0.1, size=(n - o, 6, 6))
+        rows += [i, i + o]
+        cols += [i + o, i]
+        blks += [B, np.transpose(B, (0, 2, 1))]
+    r, c = np.concatenate(rows), np.concatenate(cols)
+    order = np.lexsort((c, r))
+    ci = np.ascontiguousarray(c[order], dtype=np.int32)
+    vals = np.ascontiguousarray(np.concatenate(blks)[order].reshape(-1, 36))
+    rp = np.zeros(n + 1, np.int64)
+    np.add.at(rp, r + 1, 1)
+    rp = np.cumsum(rp).astype(np.int32)
+    b = rng.normal(size=6 * n)
+    sb = scenes.SceneBuilder("host")
+    sb.add_body(np.zeros((0, 3)), np.zeros((0, 3), np.int32), (0.0, 0.0, 0.0), mass=1.0, inertia=np.eye(3))
+    from nexdynipc_b200 import abi
+    ctx = runtime.Context(sb.build(abi.default_settings(), 0.01, 1))
+    ctx.pcg_solve(rp, ci, vals, b, tol=0.0, max_iter=3, check=False)           # warm-up
+    x, st = ctx.pcg_solve(rp, ci, vals, b, tol=0.0, max_iter=iters, check=False)
+    ctx.close()
+    nnzb = len(ci)
+    per_iter = 292.0 * nnzb + 4.0 * (n + 1) + 2 * 288.0 * n + 13 * 48.0 * n
+    secs = st["kernel_ms"] / 1e3
+    return {"bodies": n, "blocks": nnzb, "iterations": st["iterations"], "kernel_ms": st["kernel_ms"],
+            "ms_per_iteration": st["kernel_ms"] / max(st["iterations"], 1), "relative_residual": st["relative_residual"],
+            "grid": st["grid"], "threads": st["threads"], "bytes_per_iteration": per_iter,
+            "achieved_gbs": per_iter * st["iterations"] / secs / 1e9 if secs > 0 else None}
 
 
 def ipc_step_leg(n_cubes: int = 8, settle: int = 30, steps: int = 20):
@@ -356,6 +406,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-mode-i", action="store_true")
     ap.add_argument("--no-diff", action="store_true")
+    ap.add_argument("--no-pcg", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.impl == "reference":
@@ -524,6 +575,7 @@ def main():
     if not args.no_batched:
         batched = batched_leg(torch, min(args.steps, 10), 2, flush)
     diffl = None if args.no_diff else diff_leg(torch)
+    pcg = None if args.no_pcg else pcg_leg()
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -549,9 +601,15 @@ def main():
                                                                "newton_iterations", "status")},
                    "batched": batched,
                    "diff": diffl,
+                   "pcg": pcg,
                    "mode_i": mode_i},
         "roofline": roof,
         "roofline_narrow_phase": roof_narrow,
+        "roofline_pcg": None if pcg is None else {
+            "kernel": "k_pcg", "bound": "hbm", "unit": "GB/s", "peak": peak, "peak_kind": peak_kind,
+            "achieved": pcg["achieved_gbs"], "frac": pcg["achieved_gbs"] / peak if pcg["achieved_gbs"] else None,
+            "traffic": ncu_traffic().get("k_pcg"), "bytes_per_iteration": pcg["bytes_per_iteration"],
+            "note": "block-Jacobi PCG, one cooperative kernel; the block product streams the 400 MB matrix each iteration"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": launches_total,

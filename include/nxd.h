@@ -322,6 +322,26 @@ typedef struct nxd_solve_stats {
  * arrays.  NXD_FACTOR_FAILED on a zero pivot; stats may be NULL. */
 nxd_status nxd_linear_solve(nxd_ctx* ctx, const nxd_bsr* H, const double* b, double* x, nxd_solve_stats* stats);
 
+/* Block-Jacobi preconditioned conjugate gradients on a 6x6-block BSR matrix
+ * (an iterative alternative to nxd_linear_solve for large systems, where a
+ * direct factorisation of one big component fills in): x0 = 0, stop at
+ * |r| <= tol |b| or after max_iter iterations (NXD_NOT_CONVERGED).  The
+ * matrix must be symmetric positive definite (NXD_FACTOR_FAILED when a
+ * diagonal block or p.Ap says otherwise).  H->n_rows may differ from the
+ * context's body count: only the context's device and stream are used.
+ * The whole iteration is one cooperative kernel; stats->kernel_ms is its
+ * device time. */
+typedef struct nxd_pcg_stats {
+    int32_t iterations;
+    int32_t status;
+    double relative_residual;   /* |r| / |b| at exit */
+    double kernel_ms;           /* device time of the iteration kernel */
+    int32_t grid;               /* CTAs of the cooperative launch */
+    int32_t threads;            /* threads per CTA */
+} nxd_pcg_stats;
+nxd_status nxd_pcg_solve(nxd_ctx* ctx, const nxd_bsr* H, const double* b, double* x, double tol, int32_t max_iter,
+                         nxd_pcg_stats* stats);
+
 /* DistanceBarrierForm::updateContacts + FrictionForm::updateContactPoints +
  * FrictionForm::updateNormalForces (normal_forces may be NULL: none) and
  * InertiaForm::setPredictiveState (x_hat may be NULL: keep). */

@@ -154,6 +154,17 @@ class NxdSolveStats(C.Structure):
     ]
 
 
+class NxdPcgStats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int32),
+        ("status", C.c_int32),
+        ("relative_residual", C.c_double),
+        ("kernel_ms", C.c_double),
+        ("grid", C.c_int32),
+        ("threads", C.c_int32),
+    ]
+
+
 class NxdIpcParams(C.Structure):
     _fields_ = [
         ("dhat", C.c_double),

@@ -14,6 +14,7 @@
 #include "step.cuh"
 #include "batch.cuh"
 #include "ipc.cuh"
+#include "pcg.cuh"
 
 using namespace nx;
 
@@ -1065,6 +1066,81 @@ nxd_status nxd_linear_solve(nxd_ctx* c, const nxd_bsr* H, const double* b, doubl
     tmp.release();
     if (capst) return NXD_CAPACITY;
     return fail ? NXD_FACTOR_FAILED : NXD_OK;
+}
+
+nxd_status nxd_pcg_solve(nxd_ctx* c, const nxd_bsr* H, const double* b, double* x, double tol, int32_t max_iter,
+                         nxd_pcg_stats* stats) {
+    if (!c || !H || !b || !x || H->n_rows <= 0 || H->nnzb < 0 || H->nnzb > INT32_MAX || max_iter < 0 || !(tol >= 0.0) ||
+        (H->nnzb > 0 && (!H->row_ptr || !H->col_idx || !H->vals)))
+        return NXD_INVALID_ARGUMENT;
+    const int N = H->n_rows;
+    const long long nb = H->nnzb, n6 = 6LL * N;
+    if (n6 > INT32_MAX) return NXD_INVALID_ARGUMENT;
+    for (int i = 0; i < N; ++i)
+        if (H->row_ptr[i] > H->row_ptr[i + 1] || H->row_ptr[i] < 0) return NXD_INVALID_ARGUMENT;
+    if (H->row_ptr[0] != 0 || H->row_ptr[N] != nb) return NXD_INVALID_ARGUMENT;
+    for (long long k = 0; k < nb; ++k)
+        if (H->col_idx[k] < 0 || H->col_idx[k] >= N) return NXD_INVALID_ARGUMENT;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, kPcgThreads, 0);
+    const long long need = (n6 + kPcgThreads - 1) / kPcgThreads;
+    // at most two CTAs per SM: every grid barrier of the iteration waits for
+    // all CTAs, so more of them cost more than their latency hiding gains
+    const int G = (int)std::max<long long>(1, std::min<long long>((long long)std::min(std::max(per_sm, 1), 2) * c->n_sm, need));
+    cudaStream_t st = c->stream;
+    DevArena tmp;
+    int* rp = tmp.alloc<int>(N + 1);
+    int* ci = tmp.alloc<int>(std::max<long long>(nb, 1));
+    double* vv = tmp.alloc<double>(36 * (size_t)std::max<long long>(nb, 1));
+    double* minv = tmp.alloc<double>(36 * (size_t)N);
+    double* vec = tmp.alloc<double>(7 * (size_t)n6);
+    double* part = tmp.alloc<double>(2 * kRedMaxQ * (size_t)G);
+    unsigned* bar = tmp.alloc<unsigned>(2);
+    int* ints = tmp.alloc<int>(3);
+    double* res = tmp.alloc<double>(1);
+    if (!tmp.ok) { tmp.release(); return NXD_CUDA_ERROR; }
+    NXD_CUDA(cudaMemcpyAsync(rp, H->row_ptr, sizeof(int) * (N + 1), cudaMemcpyHostToDevice, st));
+    if (nb > 0) {
+        NXD_CUDA(cudaMemcpyAsync(ci, H->col_idx, sizeof(int) * nb, cudaMemcpyHostToDevice, st));
+        NXD_CUDA(cudaMemcpyAsync(vv, H->vals, 36 * sizeof(double) * nb, cudaMemcpyHostToDevice, st));
+    }
+    double* bd = vec;
+    NXD_CUDA(cudaMemcpyAsync(bd, b, sizeof(double) * n6, cudaMemcpyHostToDevice, st));
+    NXD_CUDA(cudaMemsetAsync(ints, 0, 3 * sizeof(int), st));
+    NXD_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st));
+    k_pcg_prepare<<<grid_for(N, 128), 128, 0, st>>>(N, rp, ci, vv, minv, ints + 2);
+    PcgArgs A;
+    A.N = N; A.rp = rp; A.ci = ci; A.vals = vv; A.minv = minv; A.b = bd;
+    A.x = vec + n6; A.r[0] = vec + 2 * n6; A.r[1] = vec + 3 * n6; A.p[0] = vec + 4 * n6; A.p[1] = vec + 5 * n6;
+    A.q = vec + 6 * n6; A.tol = tol; A.max_iter = max_iter; A.part = part; A.stride = G;
+    A.bar_count = bar; A.bar_abort = (int*)(bar + 1); A.status = ints; A.iters_out = ints + 1; A.res_out = res;
+    int fail = 0;
+    NXD_CUDA(cudaMemcpyAsync(&fail, ints + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+    NXD_CUDA(cudaStreamSynchronize(st));
+    if (fail) { tmp.release(); return NXD_FACTOR_FAILED; }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    void* args[] = {(void*)&A};
+    cudaEventRecord(e0, st);
+    const cudaError_t le = cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(G), dim3(kPcgThreads), args, 0, st);
+    cudaEventRecord(e1, st);
+    NXD_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    if (le != cudaSuccess) { tmp.release(); return NXD_CUDA_ERROR; }
+    int h[2] = {0, 0};
+    double hr = 0.0;
+    cudaMemcpy(h, ints, 2 * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(&hr, res, sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(x, A.x, sizeof(double) * n6, cudaMemcpyDeviceToHost);
+    if (stats) {
+        stats->iterations = h[1]; stats->status = h[0]; stats->relative_residual = hr; stats->kernel_ms = ms;
+        stats->grid = G; stats->threads = kPcgThreads;
+    }
+    tmp.release();
+    if (h[0]) return (nxd_status)h[0];
+    return hr <= tol ? NXD_OK : NXD_NOT_CONVERGED;
 }
 
 nxd_status nxd_normal_forces(nxd_ctx* c, const double* x, double* out, int32_t n) {

@@ -1562,14 +1562,15 @@ struct GridCtx {
 struct GridRed {
     GridCtx* gc;
     double* sh;           // shared: kRedMaxQ * 32
-    double* part;         // global: 2 * kRedMaxQ * kMaxNewtonGrid
+    double* part;         // global: 2 * kRedMaxQ * stride
     int parity;
+    int stride;           // partials per reduction slot: >= G
     template <int Q, typename F>
     __device__ void sums(const int (&n)[Q], F f, double (&out)[Q]) {
         static_assert(Q <= kRedMaxQ, "too many simultaneous reductions");
         const int G = gc->G, b = gc->b, B = blockDim.x, nw = B >> 5;
         const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-        double* gp = part + parity * (kRedMaxQ * kMaxNewtonGrid);
+        double* gp = part + parity * (kRedMaxQ * stride);
         parity ^= 1;
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
@@ -1581,7 +1582,7 @@ struct GridRed {
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
                 const double t = warp_tree(l < nw ? sh[q * 32 + l] : 0.0);
-                if (l == 0) { if (G == 1) sh[q * 32] = t; else gp[q * kMaxNewtonGrid + b] = t; }
+                if (l == 0) { if (G == 1) sh[q * 32] = t; else gp[q * stride + b] = t; }
             }
         }
         gc->sync();
@@ -1593,12 +1594,12 @@ struct GridRed {
         }
 #pragma unroll
         for (int q = 0; q < Q; ++q)
-            out[q] = warp_tree(lane_fold(G, l, 32, [&](int e) { return __ldcg(gp + q * kMaxNewtonGrid + e); }));
+            out[q] = warp_tree(lane_fold(G, l, 32, [&](int e) { return __ldcg(gp + q * stride + e); }));
     }
     __device__ double max(double v) {
         const int G = gc->G, b = gc->b;
         for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-        double* gp = part + parity * (kRedMaxQ * kMaxNewtonGrid);
+        double* gp = part + parity * (kRedMaxQ * stride);
         parity ^= 1;
         if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
         __syncthreads();
@@ -1812,7 +1813,7 @@ __device__ __forceinline__ void newton_body(const Solver& S) {
     if (threadIdx.x == 0) sh_ok = 1;
     __syncthreads();
     GridRed R;
-    R.gc = &gc; R.sh = sh_red; R.part = S.gpart; R.parity = 0;
+    R.gc = &gc; R.sh = sh_red; R.part = S.gpart; R.parity = 0; R.stride = kMaxNewtonGrid;
     const int N = S.N;
     const int C = *S.ncontacts_ptr;
     const double s = *S.scale_ptr;   // ImplicitTimeIntegrator::acceleration_scaling
@@ -1995,7 +1996,7 @@ __global__ void __launch_bounds__(kNewtonThreads) k_linear_solve(const __grid_co
     gc.count = S.bar_count; gc.abort = S.bar_abort; gc.status = S.status; gc.target = 0; gc.sh_ok = &sh_ok;
     __syncthreads();
     GridRed R;
-    R.gc = &gc; R.sh = sh_red; R.part = S.gpart; R.parity = 0;
+    R.gc = &gc; R.sh = sh_red; R.part = S.gpart; R.parity = 0; R.stride = kMaxNewtonGrid;
     bool cached = false;
     grid_solve(S, 1.0, 0, gc, R, sh_scan, &sh_flag, sh_wcomp, cached);
 }

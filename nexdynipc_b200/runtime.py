@@ -58,6 +58,7 @@ def lib():
     L.nxd_eval_all.argtypes = [vp, dp, dp, dp, ip, ip, dp, C.c_int64, i64p]
     L.nxd_linear_solve.argtypes = [vp, C.POINTER(abi.NxdBsr), dp, dp, C.POINTER(abi.NxdSolveStats)]
     L.nxd_ipc_step.argtypes = [vp, C.c_double, C.POINTER(abi.NxdIpcParams), C.POINTER(abi.NxdIpcStats)]
+    L.nxd_pcg_solve.argtypes = [vp, C.POINTER(abi.NxdBsr), dp, dp, C.c_double, C.c_int32, C.POINTER(abi.NxdPcgStats)]
     L.nxd_batch_create.argtypes = [C.POINTER(abi.NxdSceneDesc), C.c_int32, C.POINTER(vp)]
     L.nxd_batch_destroy.argtypes = [vp]
     L.nxd_batch_step.argtypes = [vp, dp]
@@ -270,6 +271,24 @@ class Context:
         stt = abi.NxdSolveStats()
         _check("nxd_linear_solve", lib().nxd_linear_solve(self.h, C.byref(H), abi.dptr(bb), abi.dptr(x), C.byref(stt)))
         return x, {k: getattr(stt, k) for k, _ in abi.NxdSolveStats._fields_}
+
+    def pcg_solve(self, row_ptr, col_idx, vals, b, tol: float = 1e-12, max_iter: int = 1000, check: bool = True):
+        """x ~ H^-1 b by block-Jacobi PCG (nxd_pcg_solve); returns (x, stats
+        dict with the call's status).  H's block rows need not be this
+        context's bodies."""
+        rp = np.ascontiguousarray(row_ptr, np.int32)
+        ci = np.ascontiguousarray(col_idx, np.int32)
+        vv = np.ascontiguousarray(vals, np.float64)
+        bb = np.ascontiguousarray(b, np.float64)
+        H = abi.NxdBsr(len(rp) - 1, len(ci), abi.iptr(rp), abi.iptr(ci), abi.dptr(vv))
+        x = np.zeros(len(bb))
+        st = abi.NxdPcgStats()
+        rc = lib().nxd_pcg_solve(self.h, C.byref(H), abi.dptr(bb), abi.dptr(x), float(tol), int(max_iter), C.byref(st))
+        if check and rc not in (0, 1):
+            _check("nxd_pcg_solve", rc)
+        out = {k: getattr(st, k) for k, _ in abi.NxdPcgStats._fields_}
+        out["rc"] = int(rc)
+        return x, out
 
     def normal_forces(self, x, n: int) -> np.ndarray:
         out = np.zeros(max(n, 1))
