@@ -303,7 +303,7 @@ def pcg_leg(n_bodies: int = 200000, iters: int = 60):
             "achieved_gbs": per_iter * st["iterations"] / secs / 1e9 if secs > 0 else None}
 
 
-def ipc_step_leg(n_cubes: int = 8, settle: int = 30, steps: int = 20):
+def ipc_step_leg(n_cubes: int = 8, settle: int = 30, steps: int = 20, solver: int = 0):
     """Full-IPC time step (nxd_ipc_step) on a tower of tilted cubes falling
     onto a ground box: after `settle` steps (the cubes in contact), wall
     clock of `steps` steps, each a host-ordered Newton loop of device calls
@@ -312,7 +312,8 @@ def ipc_step_leg(n_cubes: int = 8, settle: int = 30, steps: int = 20):
     from nexdynipc_b200 import abi, runtime, scenes
     sc = scenes.ipc_drop(n_cubes=n_cubes)
     ctx = runtime.Context(sc)
-    p = abi.ipc_params(dhat=1e-3, kappa=1e11, eta=0.1, newton_tol=1e-5, newton_max_iters=50, ls_max_iters=30)
+    p = abi.ipc_params(dhat=1e-3, kappa=1e11, eta=0.1, newton_tol=1e-5, newton_max_iters=50, ls_max_iters=30,
+                       linear_solver=solver, pcg_max_iter=500, pcg_tol=1e-12)
     for _ in range(settle):
         ctx.ipc_step(p)
     its, act, pairs, conv, lsf = [], [], [], 0, 0
@@ -328,6 +329,7 @@ def ipc_step_leg(n_cubes: int = 8, settle: int = 30, steps: int = 20):
             "steps": steps, "steps_per_s": steps / wall, "newton_iterations_mean": float(np.mean(its)),
             "active_pairs_mean": float(np.mean(act)), "candidate_pairs_mean": float(np.mean(pairs)),
             "converged_steps": conv, "line_search_failures": lsf,
+            "linear_solver": "block-Jacobi PCG" if solver else "component LDL^T",
             "timing": "wall clock per nxd_ipc_step (it synchronises)"}
 
 
@@ -570,6 +572,7 @@ def main():
     mode_i = None if args.no_mode_i else mode_i_leg(ctx, sc)
     if mode_i is not None:
         mode_i["step"] = ipc_step_leg()
+        mode_i["step_pcg"] = ipc_step_leg(solver=1)
 
     batched = None
     if not args.no_batched:

@@ -433,7 +433,8 @@ nxd_status nxd_ipc_max_step(nxd_ctx* ctx, const double* x, const double* dx, dou
  * a Newton step with |dx|_inf < tol * dt (IPC's velocity test); Armijo
  * backtracking (settings.ls_c1, ls_rho) starts from min(1, CCD bound);
  * candidates are rebuilt at every iterate and trial point; each system is
- * solved by nxd_linear_solve; the state is written back as nxd_step does.
+ * solved by nxd_linear_solve's factorisation or by nxd_pcg_solve's PCG
+ * (linear_solver); the state is written back as nxd_step does.
  * No friction term. */
 typedef struct nxd_ipc_params {
     double dhat;                /* barrier activation distance               */
@@ -442,6 +443,10 @@ typedef struct nxd_ipc_params {
     double newton_tol;          /* |g|_inf                                   */
     int32_t newton_max_iters;
     int32_t ls_max_iters;
+    int32_t linear_solver;      /* 0: component LDL^T (nxd_linear_solve),
+                                   1: block-Jacobi PCG (nxd_pcg_solve)       */
+    int32_t pcg_max_iter;
+    double pcg_tol;             /* |r| / |b|                                 */
 } nxd_ipc_params;
 typedef struct nxd_ipc_stats {
     int32_t newton_iterations;
@@ -452,6 +457,7 @@ typedef struct nxd_ipc_stats {
     double energy;              /* total energy at the last accepted iterate */
     int64_t n_pairs;            /* candidate pairs at the last iterate       */
     int64_t n_active;           /* pairs within dhat                         */
+    int64_t pcg_iterations;     /* PCG iterations over the step              */
 } nxd_ipc_stats;
 nxd_status nxd_ipc_step(nxd_ctx* ctx, double dt, const nxd_ipc_params* p, nxd_ipc_stats* stats);
 

@@ -173,6 +173,9 @@ class NxdIpcParams(C.Structure):
         ("newton_tol", C.c_double),
         ("newton_max_iters", C.c_int32),
         ("ls_max_iters", C.c_int32),
+        ("linear_solver", C.c_int32),
+        ("pcg_max_iter", C.c_int32),
+        ("pcg_tol", C.c_double),
     ]
 
 
@@ -186,14 +189,20 @@ class NxdIpcStats(C.Structure):
         ("energy", C.c_double),
         ("n_pairs", C.c_int64),
         ("n_active", C.c_int64),
+        ("pcg_iterations", C.c_int64),
     ]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-def ipc_params(dhat=1e-3, kappa=1e8, eta=0.1, newton_tol=1e-6, newton_max_iters=50, ls_max_iters=30) -> "NxdIpcParams":
-    return NxdIpcParams(dhat, kappa, eta, newton_tol, newton_max_iters, ls_max_iters)
+IPC_SOLVER_DIRECT, IPC_SOLVER_PCG = 0, 1
+
+
+def ipc_params(dhat=1e-3, kappa=1e8, eta=0.1, newton_tol=1e-6, newton_max_iters=50, ls_max_iters=30,
+               linear_solver=IPC_SOLVER_DIRECT, pcg_max_iter=500, pcg_tol=1e-12) -> "NxdIpcParams":
+    return NxdIpcParams(dhat, kappa, eta, newton_tol, newton_max_iters, ls_max_iters, linear_solver, pcg_max_iter,
+                        pcg_tol)
 
 
 class NxdState(C.Structure):

@@ -1068,6 +1068,91 @@ nxd_status nxd_linear_solve(nxd_ctx* c, const nxd_bsr* H, const double* b, doubl
     return fail ? NXD_FACTOR_FAILED : NXD_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// A device buffer that grows on demand (cudaMalloc at the first use and
+// when a larger size is needed; kept until released).
+struct GrowBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    bool ensure(size_t bytes) {
+        bytes = std::max<size_t>(bytes, 256);
+        if (bytes <= cap) return true;
+        if (p) {
+            cudaDeviceSynchronize();   // queued kernels may still read the old buffer
+            cudaFree(p);
+        }
+        p = nullptr;
+        cap = 0;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) { p = nullptr; return false; }
+        cap = bytes;
+        return true;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+    void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+};
+
+// PCG on a device-resident BSR system; x (device) gets the solution.
+// Scratch comes from `buf` (grown as needed).  Returns the kernel's status
+// (NXD_OK, NXD_FACTOR_FAILED) or NXD_CUDA_ERROR; *iters / *res / *ms report.
+struct PcgScratch {
+    GrowBuf minv, vec, part, bar, ints, res;
+    void release() { minv.release(); vec.release(); part.release(); bar.release(); ints.release(); res.release(); }
+};
+nxd_status pcg_device(nxd_ctx* c, PcgScratch& w, int N, const int* rp, const int* ci, const double* vv, const double* bd,
+                      double* xd, double tol, int max_iter, int* iters, double* res, float* ms, int* grid) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, kPcgThreads, 0);
+    const long long n6 = 6LL * N;
+    const long long need = (n6 + kPcgThreads - 1) / kPcgThreads;
+    // at most two CTAs per SM: every grid barrier of the iteration waits for
+    // all CTAs, so more of them cost more than their latency hiding gains
+    const int G = (int)std::max<long long>(1, std::min<long long>((long long)std::min(std::max(per_sm, 1), 2) * c->n_sm, need));
+    cudaStream_t st = c->stream;
+    if (!w.minv.ensure(288 * (size_t)N) || !w.vec.ensure(48 * 6 * (size_t)N) || !w.part.ensure(8 * 2 * kPcgMaxQ * (size_t)G) ||
+        !w.bar.ensure(8) || !w.ints.ensure(12) || !w.res.ensure(8))
+        return NXD_CUDA_ERROR;
+    int* ints = w.ints.as<int>();
+    unsigned* bar = w.bar.as<unsigned>();
+    double* vec = w.vec.as<double>();
+    NXD_CUDA(cudaMemsetAsync(ints, 0, 3 * sizeof(int), st));
+    NXD_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st));
+    k_pcg_prepare<<<grid_for(N, 128), 128, 0, st>>>(N, rp, ci, vv, w.minv.as<double>(), ints + 2);
+    PcgArgs A;
+    A.N = N; A.rp = rp; A.ci = ci; A.vals = vv; A.minv = w.minv.as<double>(); A.b = bd;
+    A.x = xd; A.r[0] = vec; A.r[1] = vec + n6; A.p[0] = vec + 2 * n6; A.p[1] = vec + 3 * n6;
+    A.q = vec + 4 * n6; A.tol = tol; A.max_iter = max_iter; A.part = w.part.as<double>(); A.stride = G;
+    A.bar_count = bar; A.bar_abort = (int*)(bar + 1); A.status = ints; A.iters_out = ints + 1; A.res_out = w.res.as<double>();
+    int fail = 0;
+    NXD_CUDA(cudaMemcpyAsync(&fail, ints + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+    NXD_CUDA(cudaStreamSynchronize(st));
+    if (fail) return NXD_FACTOR_FAILED;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    void* args[] = {(void*)&A};
+    cudaEventRecord(e0, st);
+    const cudaError_t le = cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(G), dim3(kPcgThreads), args, 0, st);
+    cudaEventRecord(e1, st);
+    NXD_CUDA(cudaStreamSynchronize(st));
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    if (le != cudaSuccess) return NXD_CUDA_ERROR;
+    int h[2] = {0, 0};
+    NXD_CUDA(cudaMemcpy(h, ints, 2 * sizeof(int), cudaMemcpyDeviceToHost));
+    NXD_CUDA(cudaMemcpy(res, w.res.p, sizeof(double), cudaMemcpyDeviceToHost));
+    *iters = h[1];
+    if (ms) *ms = t;
+    if (grid) *grid = G;
+    return (nxd_status)h[0];
+}
+
+}  // namespace
+
+extern "C" {
+
 nxd_status nxd_pcg_solve(nxd_ctx* c, const nxd_bsr* H, const double* b, double* x, double tol, int32_t max_iter,
                          nxd_pcg_stats* stats) {
     if (!c || !H || !b || !x || H->n_rows <= 0 || H->nnzb < 0 || H->nnzb > INT32_MAX || max_iter < 0 || !(tol >= 0.0) ||
@@ -1081,65 +1166,33 @@ nxd_status nxd_pcg_solve(nxd_ctx* c, const nxd_bsr* H, const double* b, double* 
     if (H->row_ptr[0] != 0 || H->row_ptr[N] != nb) return NXD_INVALID_ARGUMENT;
     for (long long k = 0; k < nb; ++k)
         if (H->col_idx[k] < 0 || H->col_idx[k] >= N) return NXD_INVALID_ARGUMENT;
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, kPcgThreads, 0);
-    const long long need = (n6 + kPcgThreads - 1) / kPcgThreads;
-    // at most two CTAs per SM: every grid barrier of the iteration waits for
-    // all CTAs, so more of them cost more than their latency hiding gains
-    const int G = (int)std::max<long long>(1, std::min<long long>((long long)std::min(std::max(per_sm, 1), 2) * c->n_sm, need));
     cudaStream_t st = c->stream;
     DevArena tmp;
     int* rp = tmp.alloc<int>(N + 1);
     int* ci = tmp.alloc<int>(std::max<long long>(nb, 1));
     double* vv = tmp.alloc<double>(36 * (size_t)std::max<long long>(nb, 1));
-    double* minv = tmp.alloc<double>(36 * (size_t)N);
-    double* vec = tmp.alloc<double>(7 * (size_t)n6);
-    double* part = tmp.alloc<double>(2 * kRedMaxQ * (size_t)G);
-    unsigned* bar = tmp.alloc<unsigned>(2);
-    int* ints = tmp.alloc<int>(3);
-    double* res = tmp.alloc<double>(1);
+    double* bd = tmp.alloc<double>((size_t)n6);
+    double* xd = tmp.alloc<double>((size_t)n6);
     if (!tmp.ok) { tmp.release(); return NXD_CUDA_ERROR; }
     NXD_CUDA(cudaMemcpyAsync(rp, H->row_ptr, sizeof(int) * (N + 1), cudaMemcpyHostToDevice, st));
     if (nb > 0) {
         NXD_CUDA(cudaMemcpyAsync(ci, H->col_idx, sizeof(int) * nb, cudaMemcpyHostToDevice, st));
         NXD_CUDA(cudaMemcpyAsync(vv, H->vals, 36 * sizeof(double) * nb, cudaMemcpyHostToDevice, st));
     }
-    double* bd = vec;
     NXD_CUDA(cudaMemcpyAsync(bd, b, sizeof(double) * n6, cudaMemcpyHostToDevice, st));
-    NXD_CUDA(cudaMemsetAsync(ints, 0, 3 * sizeof(int), st));
-    NXD_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st));
-    k_pcg_prepare<<<grid_for(N, 128), 128, 0, st>>>(N, rp, ci, vv, minv, ints + 2);
-    PcgArgs A;
-    A.N = N; A.rp = rp; A.ci = ci; A.vals = vv; A.minv = minv; A.b = bd;
-    A.x = vec + n6; A.r[0] = vec + 2 * n6; A.r[1] = vec + 3 * n6; A.p[0] = vec + 4 * n6; A.p[1] = vec + 5 * n6;
-    A.q = vec + 6 * n6; A.tol = tol; A.max_iter = max_iter; A.part = part; A.stride = G;
-    A.bar_count = bar; A.bar_abort = (int*)(bar + 1); A.status = ints; A.iters_out = ints + 1; A.res_out = res;
-    int fail = 0;
-    NXD_CUDA(cudaMemcpyAsync(&fail, ints + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
-    NXD_CUDA(cudaStreamSynchronize(st));
-    if (fail) { tmp.release(); return NXD_FACTOR_FAILED; }
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0); cudaEventCreate(&e1);
-    void* args[] = {(void*)&A};
-    cudaEventRecord(e0, st);
-    const cudaError_t le = cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(G), dim3(kPcgThreads), args, 0, st);
-    cudaEventRecord(e1, st);
-    NXD_CUDA(cudaStreamSynchronize(st));
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0); cudaEventDestroy(e1);
-    if (le != cudaSuccess) { tmp.release(); return NXD_CUDA_ERROR; }
-    int h[2] = {0, 0};
+    PcgScratch w;
+    int iters = 0, G = 0;
     double hr = 0.0;
-    cudaMemcpy(h, ints, 2 * sizeof(int), cudaMemcpyDeviceToHost);
-    cudaMemcpy(&hr, res, sizeof(double), cudaMemcpyDeviceToHost);
-    cudaMemcpy(x, A.x, sizeof(double) * n6, cudaMemcpyDeviceToHost);
+    float ms = 0.f;
+    const nxd_status rc = pcg_device(c, w, N, rp, ci, vv, bd, xd, tol, max_iter, &iters, &hr, &ms, &G);
+    if (rc == NXD_OK) cudaMemcpy(x, xd, sizeof(double) * n6, cudaMemcpyDeviceToHost);
     if (stats) {
-        stats->iterations = h[1]; stats->status = h[0]; stats->relative_residual = hr; stats->kernel_ms = ms;
+        stats->iterations = iters; stats->status = rc; stats->relative_residual = hr; stats->kernel_ms = ms;
         stats->grid = G; stats->threads = kPcgThreads;
     }
+    w.release();
     tmp.release();
-    if (h[0]) return (nxd_status)h[0];
+    if (rc != NXD_OK) return rc;
     return hr <= tol ? NXD_OK : NXD_NOT_CONVERGED;
 }
 
@@ -1167,25 +1220,6 @@ nxd_status nxd_normal_forces(nxd_ctx* c, const double* x, double* out, int32_t n
 
 namespace {
 
-struct GrowBuf {
-    void* p = nullptr;
-    size_t cap = 0;
-    bool ensure(size_t bytes) {
-        bytes = std::max<size_t>(bytes, 256);
-        if (bytes <= cap) return true;
-        if (p) {
-            cudaDeviceSynchronize();   // queued kernels may still read the old buffer
-            cudaFree(p);
-        }
-        p = nullptr;
-        cap = 0;
-        if (cudaMalloc(&p, bytes) != cudaSuccess) { p = nullptr; return false; }
-        cap = bytes;
-        return true;
-    }
-    template <typename T> T* as() const { return static_cast<T*>(p); }
-    void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
-};
 
 struct Bvh {
     int n = 0;
@@ -1206,6 +1240,7 @@ struct IpcState {
     GrowBuf sflag, spos, sstart, gout, rowptr, colidx, vals, toi;
     // full-IPC time step: rest-form and merged BSR, gradients, solve scratch
     GrowBuf rrp, rci, rvv, rnz, mrp, mci, mvv, gr, gt, gneg, prod, xt, erow, items, iact, stat, val;
+    PcgScratch pcg;
     std::vector<GrowBuf*> all() {
         return {&fbody, &fvert, &ebody, &evert, &x0, &x1, &pp0, &pq0, &pp1, &pq1, &wq0, &wq1, &qv, &qe,
                 &faces.k0, &faces.k1, &faces.i0, &faces.i1, &faces.leaf, &faces.nbox, &faces.child, &faces.parent,
@@ -1215,7 +1250,7 @@ struct IpcState {
                 &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &rrp, &rci, &rvv,
                 &rnz, &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &val};
     }
-    void release() { for (GrowBuf* b : all()) b->release(); }
+    void release() { for (GrowBuf* b : all()) b->release(); pcg.release(); }
 };
 
 namespace {
@@ -1550,7 +1585,8 @@ nxd_status nxd_ipc_max_step(nxd_ctx* c, const double* x, const double* dx, doubl
 // followed, row by row, by the barrier's blocks.
 nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_stats* out) {
     if (!c || !p || !(dt > 0.0) || !(p->dhat > 0.0) || !(p->kappa >= 0.0) || !(p->eta > 0.0 && p->eta < 1.0) ||
-        p->newton_max_iters < 0 || p->ls_max_iters < 1)
+        p->newton_max_iters < 0 || p->ls_max_iters < 1 || p->linear_solver < 0 || p->linear_solver > 1 ||
+        (p->linear_solver == 1 && (p->pcg_max_iter < 1 || !(p->pcg_tol >= 0.0))))
         return NXD_INVALID_ARGUMENT;
     nxd_status st = ipc_prepare(c);
     if (st != NXD_OK) return st;
@@ -1587,7 +1623,7 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
         if (r == NXD_OK) r = ipc_barrier_eval(c, p->dhat, p->kappa, false, v, nullptr, nullptr);
         return r;
     };
-    int iters = 0, conv = 0, lsfail = 0, solvefail = 0, na = 0;
+    int iters = 0, conv = 0, lsfail = 0, solvefail = 0, na = 0, pcg_total = 0;
     double amax = 1.0, fx = 0.0;
     int64_t npairs = 0;
     for (int it = 0; it < p->newton_max_iters; ++it) {
@@ -1629,7 +1665,17 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
                                                        nh ? s->rowptr.as<int>() : nullptr, s->colidx.as<int>(),
                                                        s->vals.as<double>(), scale, s->mrp.as<int>(), s->mci.as<int>(),
                                                        s->mvv.as<double>());
-        // H dx = -g
+        // H dx = -g: block-Jacobi PCG, or the component LDL^T
+        if (p->linear_solver == 1) {
+            int pit = 0;
+            double pres = 0.0;
+            const nxd_status pr = pcg_device(c, s->pcg, N, s->mrp.as<int>(), s->mci.as<int>(), s->mvv.as<double>(),
+                                             s->gneg.as<double>(), c->S.dx, p->pcg_tol, p->pcg_max_iter, &pit, &pres,
+                                             nullptr, nullptr);
+            if (pr == NXD_CUDA_ERROR) return pr;
+            pcg_total += pit;
+            if (pr != NXD_OK) { solvefail = 1; break; }
+        } else {
         Solver S = c->S;
         S.ext_n = (int)nzm; S.ext_row = s->erow.as<int>(); S.ext_col = s->mci.as<int>(); S.ext_vals = s->mvv.as<double>();
         S.items = s->items.as<int>(); S.iact = s->iact.as<int>(); S.status = s->stat.as<int>();
@@ -1642,6 +1688,7 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
         NXD_CUDA(cudaStreamSynchronize(sm));
         if (capst) return NXD_CAPACITY;
         if (fail) { solvefail = 1; break; }
+        }
         double* dx = c->S.dx;
         // the velocity criterion of IPC: a Newton step below tol * dt ends it
         NXD_CUDA(cudaMemcpyAsync(gh.data(), dx, 8 * (size_t)n6, cudaMemcpyDeviceToHost, sm));
@@ -1686,7 +1733,7 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
     if (out) {
         out->newton_iterations = iters; out->converged = conv; out->line_search_failed = lsfail;
         out->solve_failed = solvefail; out->last_alpha_max = amax; out->energy = fx; out->n_pairs = npairs;
-        out->n_active = na;
+        out->n_active = na; out->pcg_iterations = pcg_total;
     }
     return solvefail ? NXD_FACTOR_FAILED : NXD_OK;
 }

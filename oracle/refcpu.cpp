@@ -2516,7 +2516,7 @@ int nxo_ipc_step(nxo_world* w, double dt, const nxd_ipc_params* p, nxd_ipc_stats
     if (out) {
         out->newton_iterations = iters; out->converged = conv; out->line_search_failed = lsfail;
         out->solve_failed = solvefail; out->last_alpha_max = amax; out->energy = fx; out->n_pairs = npairs;
-        out->n_active = na;
+        out->n_active = na; out->pcg_iterations = 0;
     }
     return solvefail ? NXD_FACTOR_FAILED : NXD_OK;
 }

@@ -74,3 +74,24 @@ def test_device_ipc_step_matches_oracle():
         worst = max(worst, float(np.abs(a["position"] - b["position"]).max()))
         assert worst <= 1e-6, (k, worst)
     assert ctx.diagnostics()["status"] == 0
+
+
+@pytest.mark.gpu
+def test_device_ipc_step_with_pcg_tracks_the_direct_solve():
+    # the same step with block-Jacobi PCG (tolerance 1e-13) for the Newton
+    # systems stays on the oracle's direct-solve trajectory
+    from nexdynipc_b200 import runtime
+    sc = scenes.ipc_drop(n_cubes=3)
+    ctx = runtime.Context(sc)
+    ow = refcpu.OracleWorld(sc)
+    pg = abi.ipc_params(**PARAMS, linear_solver=abi.IPC_SOLVER_PCG, pcg_max_iter=500, pcg_tol=1e-13)
+    po = abi.ipc_params(**PARAMS)
+    used = 0
+    for k in range(30):
+        sg = ctx.ipc_step(pg)
+        so = ow.ipc_step(po)
+        used += sg["pcg_iterations"]
+        assert sg["solve_failed"] == 0
+        d = float(np.abs(ctx.state()["position"] - ow.state()["position"]).max())
+        assert d <= 1e-6, (k, d)
+    assert used > 0
