@@ -1123,7 +1123,7 @@ nxd_status pcg_device(nxd_ctx* c, PcgScratch& w, int N, const int* rp, const int
     PcgArgs A;
     A.N = N; A.rp = rp; A.ci = ci; A.vals = vv; A.minv = w.minv.as<double>(); A.b = bd;
     A.x = xd; A.r[0] = vec; A.r[1] = vec + n6; A.p[0] = vec + 2 * n6; A.p[1] = vec + 3 * n6;
-    A.q = vec + 4 * n6; A.tol = tol; A.max_iter = max_iter; A.part = w.part.as<double>(); A.stride = G;
+    A.q = vec + 4 * n6; A.z = vec + 5 * n6; A.tol = tol; A.max_iter = max_iter; A.part = w.part.as<double>(); A.stride = G;
     A.bar_count = bar; A.bar_abort = (int*)(bar + 1); A.status = ints; A.iters_out = ints + 1; A.res_out = w.res.as<double>();
     int fail = 0;
     NXD_CUDA(cudaMemcpyAsync(&fail, ints + 2, sizeof(int), cudaMemcpyDeviceToHost, st));

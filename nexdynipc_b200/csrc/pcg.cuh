@@ -4,11 +4,11 @@
 // The iteration (x0 = 0, r = b, z = M^-1 r, p = z):
 //   q = A p;  alpha = (r.z) / (p.q);  r' = r - alpha q;  z' = M^-1 r';
 //   beta = (r'.z') / (r.z);  x += alpha p;  p' = z' + beta p
-// with M the block diagonal of A.  r' and z' are formed on the fly inside the
-// reduction that needs them and again, with the same arithmetic, in the
-// update, so an iteration crosses four grid barriers: after the product,
-// inside (p.q), inside the joint (r'.r', r'.z') reduction, after the update
-// (r, p double-buffered).  The product is the HBM-bound part: one thread per
+// with M the block diagonal of A.  r' and z' are formed inside the reduction
+// that needs them (z' stored there, r' formed again with the same arithmetic
+// in the update) and p.q is summed in the product's own pass, so an iteration
+// crosses three grid barriers: in the p.q sum, in the joint (r'.r', r'.z')
+// sum, after the update (r, p double-buffered).  The product is the HBM-bound part: one thread per
 // row component reads its row's 48-byte slices of every block in the row.
 // Sums use a fixed-order grid reduction over coalesced reads, so results do
 // not depend on timing.
@@ -22,7 +22,7 @@ struct PcgArgs {
     const double* minv;                                 // [36N] inverse diagonal blocks
     const double* b;
     double* x;
-    double* r[2]; double* p[2]; double* q;
+    double* r[2]; double* p[2]; double* q; double* z;
     double tol; int max_iter;
     double* part; int stride;                           // grid partial sums, 2 * kRedMaxQ * stride
     unsigned* bar_count; int* bar_abort; int* status;
@@ -54,7 +54,7 @@ __device__ __forceinline__ double pcg_row_product(const PcgArgs& A, const double
     const int i = e / 6, rr = e % 6;
     const int k0 = __ldg(A.rp + i), k1 = __ldg(A.rp + i + 1);
     double acc = 0.0;
-    for (int k = k0; k < k1; ++k) {
+    auto slice = [&](int k) {
         const double2* blk = reinterpret_cast<const double2*>(A.vals + 36LL * k + 6 * rr);
         const double2 a0 = __ldg(blk), a1 = __ldg(blk + 1), a2 = __ldg(blk + 2);
         const double2* pc = reinterpret_cast<const double2*>(p + 6LL * __ldg(A.ci + k));
@@ -62,8 +62,17 @@ __device__ __forceinline__ double pcg_row_product(const PcgArgs& A, const double
         double t = 0.0;
         t += a0.x * b0.x; t += a0.y * b0.y; t += a1.x * b1.x;
         t += a1.y * b1.y; t += a2.x * b2.x; t += a2.y * b2.y;
-        acc += t;
+        return t;
+    };
+    int k = k0;
+    // two blocks per trip: both blocks' loads are in flight together; the
+    // partial products still enter acc in block order
+    for (; k + 1 < k1; k += 2) {
+        const double t0 = slice(k), t1 = slice(k + 1);
+        acc += t0;
+        acc += t1;
     }
+    if (k < k1) acc += slice(k);
     return acc;
 }
 // component e of M^-1 (r - alpha q)
@@ -83,16 +92,26 @@ constexpr int kPcgMaxQ = 2;   // sums per reduction call
 // (T threads in the grid), then a shuffle-down tree per warp, a tree over
 // the CTA's warps, one partial per CTA, a grid barrier, and every thread
 // folds the G partials the same way.  Deterministic for a given grid.
+template <int Q>
+__device__ void pcg_grid_fold(GridCtx& gc, double* sh, double* part, int& parity, const double (&acc)[Q], double (&out)[Q]);
+
 template <int Q, typename F>
 __device__ void pcg_sums(GridCtx& gc, double* sh, double* part, int& parity, int n, F f, double (&out)[Q]) {
-    const unsigned full = 0xffffffffu;
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
     double acc[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) acc[q] = 0.0;
     for (int e = gc.gtid; e < n; e += gc.gthreads)
 #pragma unroll
         for (int q = 0; q < Q; ++q) acc[q] += f(q, e);
+    pcg_grid_fold<Q>(gc, sh, part, parity, acc, out);
+}
+
+// the grid part of pcg_sums, from each thread's running sums (includes one
+// grid barrier, so every write made before it is visible after it)
+template <int Q>
+__device__ void pcg_grid_fold(GridCtx& gc, double* sh, double* part, int& parity, const double (&acc)[Q], double (&out)[Q]) {
+    const unsigned full = 0xffffffffu;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
     // two alternating slots of a fixed size, so that a call's partials never
     // overwrite those of the previous call while a CTA may still fold them
     static_assert(Q <= kPcgMaxQ, "too many simultaneous sums");
@@ -152,17 +171,25 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const __grid_constant__ Pcg
     while (it < A.max_iter && res > A.tol) {
         const double* p = A.p[cur];
         const double* r = A.r[cur];
-        for (int e = gc.gtid; e < n; e += gc.gthreads) A.q[e] = pcg_row_product(A, p, e);
-        if (!gc.sync()) return;
-        double pqv[1];
-        pcg_sums<1>(gc, sh_red, A.part, parity, n, [&](int, int e) { return p[e] * A.q[e]; }, pqv);
+        // Ap and p.Ap in one pass (the fold's grid barrier publishes Ap)
+        double pqa[1] = {0.0}, pqv[1];
+        for (int e = gc.gtid; e < n; e += gc.gthreads) {
+            const double qe = pcg_row_product(A, p, e);
+            A.q[e] = qe;
+            pqa[0] += p[e] * qe;
+        }
+        pcg_grid_fold<1>(gc, sh_red, A.part, parity, pqa, pqv);
+        if (!*gc.sh_ok) return;
         const double pq = pqv[0];
         if (!(pq > 0.0)) { if (gc.gtid == 0) atomicExch(A.status, NXD_FACTOR_FAILED); break; }
         const double alpha = rz / pq;
         double s2[2];
         pcg_sums<2>(gc, sh_red, A.part, parity, n, [&](int qq, int e) {
             const double rn = r[e] - alpha * A.q[e];
-            return qq == 0 ? rn * rn : rn * pcg_precond(A, r, A.q, alpha, e);
+            if (qq == 0) return rn * rn;
+            const double zz = pcg_precond(A, r, A.q, alpha, e);
+            A.z[e] = zz;                    // kept for the update: one read of M^-1 per iteration
+            return rn * zz;
         }, s2);
         const double beta = s2[1] / rz;
         rz = s2[1];
@@ -171,7 +198,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const __grid_constant__ Pcg
         for (int e = gc.gtid; e < n; e += gc.gthreads) {
             A.x[e] += alpha * p[e];
             rn[e] = r[e] - alpha * A.q[e];
-            pn[e] = pcg_precond(A, r, A.q, alpha, e) + beta * p[e];
+            pn[e] = A.z[e] + beta * p[e];
         }
         if (!gc.sync()) return;
         cur ^= 1;
