@@ -128,19 +128,28 @@ __global__ void k_pairs(const __grid_constant__ Geo g, const __grid_constant__ P
 // n_dev (optional) caps n at a device-side count.  The scan runs only when
 // run_if is null or non-zero and skip_if is null or zero; when run_if is zero
 // the total is cleared, when skip_if is set nothing is written.
-__device__ __forceinline__ void scan_body(const int* in, int* out, int n, int* total, const int* run_if, const int* skip_if, const int* n_dev) {
-    if (skip_if && *skip_if != 0) return;
-    if (run_if && *run_if == 0) { if (threadIdx.x == 0 && total) *total = 0; return; }
-    if (n_dev) n = min(n, *n_dev);
+// Exclusive prefix sums of in[0..n) into out (in place allowed) by one CTA;
+// returns the total.  Each round, every thread takes kScanItems consecutive
+// elements, so a round covers blockDim.x * kScanItems of them with two block
+// barriers (the step's pair and hit counts, ~10^4 entries, take one round).
+constexpr int kScanItems = 16;
+__device__ int block_scan(const int* in, int* out, int n) {
     __shared__ int warp_sums[32];
     __shared__ int carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int base = 0; base < n; base += blockDim.x) {
-        const int i = base + threadIdx.x;
-        const int v = i < n ? in[i] : 0;
-        int x = v;
+    const int per_round = blockDim.x * kScanItems;
+    for (int base = 0; base < n; base += per_round) {
+        const int i0 = base + threadIdx.x * kScanItems;
+        int v[kScanItems];
+        int tsum = 0;
+#pragma unroll
+        for (int j = 0; j < kScanItems; ++j) {
+            v[j] = i0 + j < n ? in[i0 + j] : 0;
+            tsum += v[j];
+        }
+        int x = tsum;
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
@@ -148,21 +157,35 @@ __device__ __forceinline__ void scan_body(const int* in, int* out, int n, int* t
         if (lane == 31) warp_sums[wid] = x;
         __syncthreads();
         if (wid == 0) {
-            int s = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+            int sv = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
             for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, s, o);
-                if (lane >= o) s += y;
+                const int y = __shfl_up_sync(0xffffffffu, sv, o);
+                if (lane >= o) sv += y;
             }
-            warp_sums[lane] = s;
+            warp_sums[lane] = sv;
         }
         __syncthreads();
-        const int excl = carry + (wid > 0 ? warp_sums[wid - 1] : 0) + x - v;
-        if (i < n) out[i] = excl;
+        int run = carry + (wid > 0 ? warp_sums[wid - 1] : 0) + x - tsum;
+#pragma unroll
+        for (int j = 0; j < kScanItems; ++j) {
+            if (i0 + j < n) out[i0 + j] = run;
+            run += v[j];
+        }
         __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+        if (threadIdx.x == blockDim.x - 1) carry = run;
         __syncthreads();
     }
-    if (threadIdx.x == 0 && total) *total = carry;
+    const int total = carry;
+    __syncthreads();
+    return total;
+}
+
+__device__ __forceinline__ void scan_body(const int* in, int* out, int n, int* total, const int* run_if, const int* skip_if, const int* n_dev) {
+    if (skip_if && *skip_if != 0) return;
+    if (run_if && *run_if == 0) { if (threadIdx.x == 0 && total) *total = 0; return; }
+    if (n_dev) n = min(n, *n_dev);
+    const int t = block_scan(in, out, n);
+    if (threadIdx.x == 0 && total) *total = t;
 }
 constexpr int kLB_scan = 0;
 __global__ void k_scan(const int* in, int* out, int n, int* total, const int* run_if, const int* skip_if = nullptr, const int* n_dev = nullptr) { scan_body(in, out, n, total, run_if, skip_if, n_dev); }
@@ -654,42 +677,6 @@ constexpr int kLB_narrow_rows = 32 * kRowsWarps;
 __global__ void __launch_bounds__(32 * kRowsWarps) k_narrow_rows(const __grid_constant__ NarrowIn in, int mode, const __grid_constant__ NarrowScratch s, const int* skip_if) { narrow_rows_body(in, mode, s, skip_if); }
 
 // Exclusive scan of n ints by one block; returns the total (all threads).
-__device__ int block_scan(const int* in, int* out, int n) {
-    __shared__ int warp_sums[32];
-    __shared__ int carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int base = 0; base < n; base += blockDim.x) {
-        const int i = base + threadIdx.x;
-        const int v = i < n ? in[i] : 0;
-        int x = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) warp_sums[wid] = x;
-        __syncthreads();
-        if (wid == 0) {
-            int sv = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, sv, o);
-                if (lane >= o) sv += y;
-            }
-            warp_sums[lane] = sv;
-        }
-        __syncthreads();
-        const int excl = carry + (wid > 0 ? warp_sums[wid - 1] : 0) + x - v;
-        if (i < n) out[i] = excl;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
-        __syncthreads();
-    }
-    const int total = carry;
-    __syncthreads();
-    return total;
-}
-
 // Prefixes of the hit counts: nseg halves of cap entries each (FV, EE), the
 // first *npairs_ptr of each; totals -> tot[0..nseg).
 __device__ __forceinline__ void hit_scan_body(const int* cnt, int* off, int cap, const int* npairs_ptr, int nseg, int* tot0, int* tot1, const int* skip_if) {
