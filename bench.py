@@ -37,6 +37,19 @@ WORKLOAD = ("hopper_chains: 1024 convex hulls (64 seeded sphere points, 124 tris
 FAMILIES = ["assembly", "broad_phase", "topk", "narrow_phase", "min_distance", "newton", "alm_post", "scan", "other"]
 
 
+def max_over_ranks(x: float, device: str = "cuda") -> float:
+    """The largest x over the ranks of the process group (the timing rule for
+    several GPUs: the job takes as long as its slowest rank); x itself when
+    no group of more than one rank is running."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -484,10 +497,7 @@ def main():
     lib.nxd_profile(ctx_prof.h, 0, abi.dptr(prof_ms), prof_n.ctypes.data_as(C.POINTER(C.c_int64)))
     twin_equal = bool(np.array_equal(ctx.state()["position"], ctx_prof.state()["position"]))
     diag = ctx.diagnostics()
-    if ws > 1:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms)
     value = ws * args.steps / (total_ms / 1e3)
 
     # --- narrow-phase item counts of the current candidate set (roofline units)
@@ -521,10 +531,7 @@ def main():
         vin, vout = vout, vin
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    if ws > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s)
     e2e = ws * args.steps / e2e_s
 
     # --- roofline of the dominant kernel family (timed on the twin context
