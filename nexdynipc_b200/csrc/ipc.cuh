@@ -165,6 +165,20 @@ __global__ void k_bsr_concat(int N, const int* rpa, const int* cia, const double
     }
 }
 
+// pair (q, prim) <-> sort key (q << pbits) | prim
+__global__ void k_pair_keys(const int* pairs, int n, int pbits, unsigned long long* key, int* val) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        key[i] = ((unsigned long long)(unsigned)pairs[2 * i] << pbits) | (unsigned)pairs[2 * i + 1];
+        val[i] = i;
+    }
+}
+__global__ void k_pair_from_keys(const unsigned long long* key, int n, int pbits, int* pairs) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        pairs[2 * i] = (int)(key[i] >> pbits);
+        pairs[2 * i + 1] = (int)(key[i] & ((1ull << pbits) - 1ull));
+    }
+}
+
 // list[pos[i]] = i for every flagged i (pos = exclusive scan of flag)
 __global__ void k_compact(const int* flag, const int* pos, int n, int* list) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -292,7 +306,7 @@ __device__ __forceinline__ bool boxes_overlap(const double* a, const double* b) 
 }
 
 // Traversal of one query box against the tree; mode 0 counts, mode 1 writes
-// (prim ids ascending within the query: insertion into the query's slice).
+// the query's hits into its slice in traversal order (sorted afterwards).
 // kind 0: vertex queries vs faces (other body); 1: edge queries vs edges
 // (other body, query < prim).
 constexpr int kTravStack = 96;
@@ -316,14 +330,8 @@ __global__ void k_traverse(PrimGeo pg, int kind, const double* qbox, int nq, con
                 const int pbody = kind == 0 ? pg.fbody[prim] : pg.ebody[prim];
                 if (pbody == qbody || (kind == 1 && !(q < prim))) continue;
                 if (dst) {
-                    int k = c;
-                    while (k > 0 && dst[2 * (k - 1) + 1] > prim) {
-                        dst[2 * k] = dst[2 * (k - 1)];
-                        dst[2 * k + 1] = dst[2 * (k - 1) + 1];
-                        --k;
-                    }
-                    dst[2 * k] = q;
-                    dst[2 * k + 1] = prim;
+                    dst[2 * c] = q;
+                    dst[2 * c + 1] = prim;
                 }
                 ++c;
                 continue;

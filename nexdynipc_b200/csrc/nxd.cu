@@ -1238,6 +1238,7 @@ struct IpcState {
     GrowBuf e, grad12, lam, z, nterm, body, active, type, apos, alist;
     GrowBuf gkey, gval, gkey1, gval1, hkey, hval, hkey1, hval1;
     GrowBuf sflag, spos, sstart, gout, rowptr, colidx, vals, toi;
+    GrowBuf tkey, tval, tkey1, tval1;    // candidate pairs sorted by (query, primitive)
     // full-IPC time step: rest-form and merged BSR, gradients, solve scratch
     GrowBuf rrp, rci, rvv, rnz, mrp, mci, mvv, gr, gt, gneg, prod, xt, erow, items, iact, stat, val;
     PcgScratch pcg;
@@ -1248,7 +1249,8 @@ struct IpcState {
                 &edges.child, &edges.parent, &edges.flags, &edges.bounds, &cnt, &off, &pt, &ee, &scal, &hist, &e,
                 &grad12, &lam, &z, &nterm, &body, &active, &type, &apos, &alist, &gkey, &gval, &gkey1, &gval1, &hkey,
                 &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &rrp, &rci, &rvv,
-                &rnz, &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &val};
+                &rnz, &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &val, &tkey, &tval,
+                &tkey1, &tval1};
     }
     void release() { for (GrowBuf* b : all()) b->release(); pcg.release(); }
 };
@@ -1386,6 +1388,18 @@ nxd_status ipc_traverse(nxd_ctx* c, int kind, Bvh& B, const double* qbox, int nq
     IPC_ENSURE(out, 8 * (size_t)std::max(h[0], 1));
     k_traverse<<<grid, 128, 0, c->stream>>>(s->pg, kind, qbox, nq, B.nbox.as<double>(), B.child.as<int>(), B.i0.as<int>(), B.n,
                                             nullptr, s->off.as<int>(), out.as<int>(), d_status);
+    // (query, primitive) ascending: one stable radix sort of the packed pairs
+    const int m = h[0];
+    if (m > 1) {
+        const int pbits = bits_for((unsigned long long)std::max(B.n, 1));
+        const int qbits = bits_for((unsigned long long)std::max(nq, 1));
+        IPC_ENSURE(s->tkey, 8 * (size_t)m); IPC_ENSURE(s->tval, 4 * (size_t)m);
+        k_pair_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(out.as<int>(), m, pbits, s->tkey.as<unsigned long long>(),
+                                                             s->tval.as<int>());
+        const nxd_status st = radix_sort(c, s->tkey, s->tval, s->tkey1, s->tval1, m, 0, pbits + qbits);
+        if (st != NXD_OK) return st;
+        k_pair_from_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(s->tkey.as<unsigned long long>(), m, pbits, out.as<int>());
+    }
     NXD_CUDA(cudaGetLastError());
     return NXD_OK;
 }
