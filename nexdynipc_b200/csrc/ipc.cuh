@@ -305,6 +305,27 @@ __device__ __forceinline__ bool boxes_overlap(const double* a, const double* b) 
     return a[0] <= b[3] && b[0] <= a[3] && a[1] <= b[4] && b[1] <= a[4] && a[2] <= b[5] && b[2] <= a[5];
 }
 
+// Small scenes: every query against every primitive box, primitives in
+// ascending order, so each query's hits come out sorted; the same tests and
+// filters as k_traverse.  mode 0 counts into cnt, mode 1 writes at off.
+__global__ void k_sweep_all(PrimGeo pg, int kind, const double* qbox, int nq, const double* leaf, int nprim, int* cnt,
+                            const int* off, int* out) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        double qb[6];
+        for (int a = 0; a < 6; ++a) qb[a] = qbox[6 * q + a];
+        const int qbody = kind == 0 ? pg.vbody[q] : pg.ebody[q];
+        int c = 0;
+        int* dst = out ? out + 2 * (size_t)off[q] : nullptr;
+        for (int prim = kind == 1 ? q + 1 : 0; prim < nprim; ++prim) {
+            const int pbody = kind == 0 ? pg.fbody[prim] : pg.ebody[prim];
+            if (pbody == qbody || !boxes_overlap(qb, leaf + 6 * (size_t)prim)) continue;
+            if (dst) { dst[2 * c] = q; dst[2 * c + 1] = prim; }
+            ++c;
+        }
+        if (!out) cnt[q] = c;
+    }
+}
+
 // Traversal of one query box against the tree; mode 0 counts, mode 1 writes
 // the query's hits into its slice in traversal order (sorted afterwards).
 // kind 0: vertex queries vs faces (other body); 1: edge queries vs edges

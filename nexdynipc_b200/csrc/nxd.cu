@@ -1406,8 +1406,43 @@ nxd_status ipc_traverse(nxd_ctx* c, int kind, Bvh& B, const double* qbox, int nq
 
 // Candidate point-triangle and edge-edge pairs at the posed world vertices:
 // leaf boxes inflated by infl (swept over wq0 -> wq1 when swept).
+// Queries against every primitive (no tree): for scenes where that is at
+// most kSweepAllTests box tests.
+constexpr long long kSweepAllTests = 1LL << 22;
+nxd_status ipc_sweep_all(nxd_ctx* c, int kind, const double* leaf, int nprim, const double* qbox, int nq, GrowBuf& out,
+                         int* count) {
+    IpcState* s = c->ipc;
+    *count = 0;
+    if (nq == 0 || nprim == 0) return NXD_OK;
+    IPC_ENSURE(s->cnt, 4 * (size_t)nq); IPC_ENSURE(s->off, 4 * (size_t)nq);
+    int* d_tot = s->scal.as<int>();
+    const int grid = grid_for(nq, 128);
+    k_sweep_all<<<grid, 128, 0, c->stream>>>(s->pg, kind, qbox, nq, leaf, nprim, s->cnt.as<int>(), nullptr, nullptr);
+    k_scan<<<1, 1024, 0, c->stream>>>(s->cnt.as<int>(), s->off.as<int>(), nq, d_tot, nullptr, nullptr, nullptr);
+    int h = 0;
+    NXD_CUDA(cudaMemcpyAsync(&h, d_tot, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    *count = h;
+    IPC_ENSURE(out, 8 * (size_t)std::max(h, 1));
+    k_sweep_all<<<grid, 128, 0, c->stream>>>(s->pg, kind, qbox, nq, leaf, nprim, nullptr, s->off.as<int>(), out.as<int>());
+    NXD_CUDA(cudaGetLastError());
+    return NXD_OK;
+}
+
 nxd_status ipc_candidates(nxd_ctx* c, bool swept, double infl) {
     IpcState* s = c->ipc;
+    if ((long long)c->nv * c->nf + (long long)c->ne * c->ne <= kSweepAllTests) {
+        const double* w1 = swept ? s->wq1.as<double>() : nullptr;
+        IPC_ENSURE(s->faces.leaf, 48 * (size_t)std::max(c->nf, 1)); IPC_ENSURE(s->edges.leaf, 48 * (size_t)std::max(c->ne, 1));
+        IPC_ENSURE(s->qv, 48 * (size_t)std::max(c->nv, 1)); IPC_ENSURE(s->qe, 48 * (size_t)std::max(c->ne, 1));
+        if (c->nf) k_ipc_boxes<<<grid_for(c->nf, 256), 256, 0, c->stream>>>(s->pg, 0, s->wq0.as<double>(), w1, infl, s->faces.leaf.as<double>());
+        if (c->ne) k_ipc_boxes<<<grid_for(c->ne, 256), 256, 0, c->stream>>>(s->pg, 1, s->wq0.as<double>(), w1, infl, s->edges.leaf.as<double>());
+        if (c->nv) k_ipc_boxes<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(s->pg, 2, s->wq0.as<double>(), w1, 0.0, s->qv.as<double>());
+        if (c->ne) k_ipc_boxes<<<grid_for(c->ne, 256), 256, 0, c->stream>>>(s->pg, 3, s->wq0.as<double>(), w1, 0.0, s->qe.as<double>());
+        nxd_status st = ipc_sweep_all(c, 0, s->faces.leaf.as<double>(), c->nf, s->qv.as<double>(), c->nv, s->pt, &s->n_pt);
+        if (st == NXD_OK) st = ipc_sweep_all(c, 1, s->edges.leaf.as<double>(), c->ne, s->qe.as<double>(), c->ne, s->ee, &s->n_ee);
+        return st;
+    }
     nxd_status st = ipc_build_bvh(c, s->faces, 0, swept, infl);
     if (st == NXD_OK) st = ipc_build_bvh(c, s->edges, 1, swept, infl);
     if (st != NXD_OK) return st;
