@@ -305,24 +305,39 @@ __device__ __forceinline__ bool boxes_overlap(const double* a, const double* b) 
     return a[0] <= b[3] && b[0] <= a[3] && a[1] <= b[4] && b[1] <= a[4] && a[2] <= b[5] && b[2] <= a[5];
 }
 
-// Small scenes: every query against every primitive box, primitives in
-// ascending order, so each query's hits come out sorted; the same tests and
-// filters as k_traverse.  mode 0 counts into cnt, mode 1 writes at off.
+// Small scenes: every query against every primitive box, one warp per query
+// testing 32 consecutive primitives per trip; a ballot places each trip's
+// hits after the previous trip's in primitive order, so each query's hits
+// come out sorted.  The same tests and filters as k_traverse.  mode 0
+// counts into cnt, mode 1 writes at off.
 __global__ void k_sweep_all(PrimGeo pg, int kind, const double* qbox, int nq, const double* leaf, int nprim, int* cnt,
                             const int* off, int* out) {
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long qq = w0; qq < nq; qq += nw) {
+        const int q = (int)qq;
         double qb[6];
         for (int a = 0; a < 6; ++a) qb[a] = qbox[6 * q + a];
         const int qbody = kind == 0 ? pg.vbody[q] : pg.ebody[q];
         int c = 0;
         int* dst = out ? out + 2 * (size_t)off[q] : nullptr;
-        for (int prim = kind == 1 ? q + 1 : 0; prim < nprim; ++prim) {
-            const int pbody = kind == 0 ? pg.fbody[prim] : pg.ebody[prim];
-            if (pbody == qbody || !boxes_overlap(qb, leaf + 6 * (size_t)prim)) continue;
-            if (dst) { dst[2 * c] = q; dst[2 * c + 1] = prim; }
-            ++c;
+        for (int base = kind == 1 ? q + 1 : 0; base < nprim; base += 32) {
+            const int prim = base + lane;
+            bool hit = false;
+            if (prim < nprim) {
+                const int pbody = kind == 0 ? pg.fbody[prim] : pg.ebody[prim];
+                hit = pbody != qbody && boxes_overlap(qb, leaf + 6 * (size_t)prim);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (hit && dst) {
+                const int at = c + __popc(m & below);
+                dst[2 * at] = q; dst[2 * at + 1] = prim;
+            }
+            c += __popc(m);
         }
-        if (!out) cnt[q] = c;
+        if (!out && lane == 0) cnt[q] = c;
     }
 }
 
@@ -430,6 +445,20 @@ __global__ void k_ipc_pair_eval(PrimGeo pg, IpcPairs P, IpcPose ps, double dhat,
             o.lam[5 * (size_t)p + k] = ev.lam[k];
             ipc::chain12(ev.y[k], side, arm, o.z + 60 * (size_t)p + 12 * k);
         }
+    }
+}
+
+// Energy only (line-search trial points): the same classification and
+// barrier value as k_ipc_pair_eval's e, without the PSD projection.
+__global__ void k_ipc_pair_energy(PrimGeo pg, IpcPairs P, IpcPose ps, double dhat, double kappa, double* e) {
+    const int n = P.n_pt + P.n_ee;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        int kind, side[4], bA, bB;
+        V3 X[4], arm[4];
+        pair_points(pg, P, ps, p, kind, X, side, arm, bA, bB);
+        const ipc::DistForm f = ipc::classify(kind, X);
+        const V3 r = ipc::form_r(f, X);
+        e[p] = ipc::barrier_s(dot(r, r), dhat * dhat, kappa);
     }
 }
 
@@ -558,6 +587,22 @@ __global__ void k_min_reduce(const double* v, int n, double init, double* out) {
     if (threadIdx.x == 0) {
         double r = init;
         for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r = dmin(r, sm[k]);
+        *out = r;
+    }
+}
+
+// max |v_i| over n doubles, one block; a NaN entry makes the result NaN.
+__global__ void k_absmax(const double* v, int n, double* out) {
+    __shared__ double sm[32];
+    double m = 0.0;
+    auto fold = [](double a, double b) { return a != a ? a : ((b != b || b > a) ? b : a); };
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fold(m, fabs(v[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fold(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r = fold(r, sm[k]);
         *out = r;
     }
 }

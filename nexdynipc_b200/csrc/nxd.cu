@@ -1228,31 +1228,63 @@ struct Bvh {
 
 }  // namespace
 
+// Device scalars of the full-IPC path (in IpcState::scal), copied whole into
+// pinned host memory (IpcHost::sc) at each host wait, so that every value a
+// phase reads back arrives with one copy and one stream synchronisation.
+struct IpcScal {
+    int tot[2];         // candidate totals: point-triangle, edge-edge
+    int status;         // traversal status
+    int nseg;           // segment count of the last ipc_segments
+    int na;             // active barrier pairs
+    int pad;
+    long long rnz;      // rest-form Hessian blocks
+    double energy;      // barrier energy
+    double alpha;       // CCD step bound
+    double rest;        // rest-form value
+    double descent;     // g . dx
+    double ginf;        // |g|_inf
+    double dxinf;       // |dx|_inf
+};
+struct IpcHost {
+    IpcScal sc;
+    int fail, capst;    // linear-solve flags
+};
+
 struct IpcState {
     PrimGeo pg{};
     GrowBuf fbody, fvert, ebody, evert;
     GrowBuf x0, x1, pp0, pq0, pp1, pq1, wq0, wq1, qv, qe;
     Bvh faces, edges;
-    GrowBuf cnt, off, pt, ee, scal, hist;
+    GrowBuf cnt, off, cnt2, off2, pt, ee, scal, hist;
+    IpcHost* hp = nullptr;       // pinned
+    int* hrow = nullptr;         // pinned, 3 (N + 1) row pointers
+    IpcScal* ds() const { return scal.as<IpcScal>(); }
     int n_pt = 0, n_ee = 0;
     GrowBuf e, grad12, lam, z, nterm, body, active, type, apos, alist;
     GrowBuf gkey, gval, gkey1, gval1, hkey, hval, hkey1, hval1;
     GrowBuf sflag, spos, sstart, gout, rowptr, colidx, vals, toi;
     GrowBuf tkey, tval, tkey1, tval1;    // candidate pairs sorted by (query, primitive)
     // full-IPC time step: rest-form and merged BSR, gradients, solve scratch
-    GrowBuf rrp, rci, rvv, rnz, mrp, mci, mvv, gr, gt, gneg, prod, xt, erow, items, iact, stat, val;
+    GrowBuf rrp, rci, rvv, mrp, mci, mvv, gr, gt, gneg, prod, xt, erow, items, iact, stat;
     PcgScratch pcg;
     std::vector<GrowBuf*> all() {
         return {&fbody, &fvert, &ebody, &evert, &x0, &x1, &pp0, &pq0, &pp1, &pq1, &wq0, &wq1, &qv, &qe,
                 &faces.k0, &faces.k1, &faces.i0, &faces.i1, &faces.leaf, &faces.nbox, &faces.child, &faces.parent,
                 &faces.flags, &faces.bounds, &edges.k0, &edges.k1, &edges.i0, &edges.i1, &edges.leaf, &edges.nbox,
-                &edges.child, &edges.parent, &edges.flags, &edges.bounds, &cnt, &off, &pt, &ee, &scal, &hist, &e,
+                &edges.child, &edges.parent, &edges.flags, &edges.bounds, &cnt, &off, &cnt2, &off2, &pt, &ee, &scal, &hist, &e,
                 &grad12, &lam, &z, &nterm, &body, &active, &type, &apos, &alist, &gkey, &gval, &gkey1, &gval1, &hkey,
                 &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &rrp, &rci, &rvv,
-                &rnz, &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &val, &tkey, &tval,
+                &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &tkey, &tval,
                 &tkey1, &tval1};
     }
-    void release() { for (GrowBuf* b : all()) b->release(); pcg.release(); }
+    void release() {
+        for (GrowBuf* b : all()) b->release();
+        pcg.release();
+        if (hp) cudaFreeHost(hp);
+        if (hrow) cudaFreeHost(hrow);
+        hp = nullptr;
+        hrow = nullptr;
+    }
 };
 
 namespace {
@@ -1266,19 +1298,37 @@ void release_ipc(nxd_ctx* c) {
     c->ipc = nullptr;
 }
 
-nxd_status ipc_prepare(nxd_ctx* c) {
-    if (c->ipc) return NXD_OK;
-    IpcState* s = new (std::nothrow) IpcState();
-    if (!s) return NXD_CUDA_ERROR;
-    c->ipc = s;
+nxd_status ipc_init(nxd_ctx* c, IpcState* s) {
     IPC_ENSURE(s->fbody, 4 * (size_t)c->nf); IPC_ENSURE(s->fvert, 12 * (size_t)c->nf);
     IPC_ENSURE(s->ebody, 4 * (size_t)c->ne); IPC_ENSURE(s->evert, 8 * (size_t)c->ne);
     k_prim_topology<<<grid_for(c->N, 128), 128, 0, c->stream>>>(c->geo, s->fbody.as<int>(), s->fvert.as<int>(),
                                                               s->ebody.as<int>(), s->evert.as<int>());
     s->pg = PrimGeo{c->nv, c->nf, c->ne, c->vbody, s->fbody.as<int>(), s->ebody.as<int>(), s->fvert.as<int>(),
                     s->evert.as<int>()};
-    IPC_ENSURE(s->scal, 64);
+    IPC_ENSURE(s->scal, sizeof(IpcScal));
+    NXD_CUDA(cudaMemsetAsync(s->scal.p, 0, sizeof(IpcScal), c->stream));
+    NXD_CUDA(cudaMallocHost(&s->hp, sizeof(IpcHost)));
+    NXD_CUDA(cudaMallocHost(&s->hrow, 12 * (size_t)(c->N + 1)));
     NXD_CUDA(cudaGetLastError());
+    return NXD_OK;
+}
+
+nxd_status ipc_prepare(nxd_ctx* c) {
+    if (c->ipc) return NXD_OK;
+    IpcState* s = new (std::nothrow) IpcState();
+    if (!s) return NXD_CUDA_ERROR;
+    c->ipc = s;
+    const nxd_status st = ipc_init(c, s);
+    if (st != NXD_OK) release_ipc(c);   // a later call starts again from nothing
+    return st;
+}
+
+// One host wait: the device scalars into pinned memory (plus any copies
+// queued before this call), then a stream synchronisation.
+nxd_status ipc_fetch(nxd_ctx* c) {
+    IpcState* s = c->ipc;
+    NXD_CUDA(cudaMemcpyAsync(&s->hp->sc, s->scal.p, sizeof(IpcScal), cudaMemcpyDeviceToHost, c->stream));
+    NXD_CUDA(cudaStreamSynchronize(c->stream));
     return NXD_OK;
 }
 
@@ -1366,105 +1416,98 @@ nxd_status ipc_build_bvh(nxd_ctx* c, Bvh& B, int kind, bool swept, double infl) 
     return NXD_OK;
 }
 
-// Queries against a tree: counts, offsets, then the pairs (query-major,
-// prim ascending) into out; *count gets the number of pairs.
-nxd_status ipc_traverse(nxd_ctx* c, int kind, Bvh& B, const double* qbox, int nq, GrowBuf& out, int* count) {
-    IpcState* s = c->ipc;
-    *count = 0;
-    if (nq == 0 || B.n == 0) return NXD_OK;
-    IPC_ENSURE(s->cnt, 4 * (size_t)nq); IPC_ENSURE(s->off, 4 * (size_t)nq);
-    int* d_tot = s->scal.as<int>();
-    int* d_status = d_tot + 1;
-    NXD_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), c->stream));
-    const int grid = grid_for(nq, 128);
-    k_traverse<<<grid, 128, 0, c->stream>>>(s->pg, kind, qbox, nq, B.nbox.as<double>(), B.child.as<int>(), B.i0.as<int>(), B.n,
-                                            s->cnt.as<int>(), nullptr, nullptr, d_status);
-    k_scan<<<1, 1024, 0, c->stream>>>(s->cnt.as<int>(), s->off.as<int>(), nq, d_tot, nullptr, nullptr, nullptr);
-    int h[2];
-    NXD_CUDA(cudaMemcpyAsync(h, d_tot, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    NXD_CUDA(cudaStreamSynchronize(c->stream));
-    if (h[1] != 0) return (nxd_status)h[1];
-    *count = h[0];
-    IPC_ENSURE(out, 8 * (size_t)std::max(h[0], 1));
-    k_traverse<<<grid, 128, 0, c->stream>>>(s->pg, kind, qbox, nq, B.nbox.as<double>(), B.child.as<int>(), B.i0.as<int>(), B.n,
-                                            nullptr, s->off.as<int>(), out.as<int>(), d_status);
-    // (query, primitive) ascending: one stable radix sort of the packed pairs
-    const int m = h[0];
-    if (m > 1) {
-        const int pbits = bits_for((unsigned long long)std::max(B.n, 1));
-        const int qbits = bits_for((unsigned long long)std::max(nq, 1));
-        IPC_ENSURE(s->tkey, 8 * (size_t)m); IPC_ENSURE(s->tval, 4 * (size_t)m);
-        k_pair_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(out.as<int>(), m, pbits, s->tkey.as<unsigned long long>(),
-                                                             s->tval.as<int>());
-        const nxd_status st = radix_sort(c, s->tkey, s->tval, s->tkey1, s->tval1, m, 0, pbits + qbits);
-        if (st != NXD_OK) return st;
-        k_pair_from_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(s->tkey.as<unsigned long long>(), m, pbits, out.as<int>());
-    }
-    NXD_CUDA(cudaGetLastError());
-    return NXD_OK;
-}
-
-// Candidate point-triangle and edge-edge pairs at the posed world vertices:
-// leaf boxes inflated by infl (swept over wq0 -> wq1 when swept).
-// Queries against every primitive (no tree): for scenes where that is at
-// most kSweepAllTests box tests.
+// Candidate point-triangle (kind 0: vertex queries vs faces of another
+// body) and edge-edge pairs (kind 1: edge queries vs edges of another body,
+// query < primitive) at the posed world vertices: primitive boxes inflated
+// by infl (swept over wq0 -> wq1 when swept), query boxes not inflated.
+// Scenes of at most kSweepAllTests box tests take the all-pairs sweep, whose
+// hits come out sorted; larger ones build an LBVH per kind, traverse it and
+// sort each kind's pairs by (query, primitive) with one radix sort.  Both
+// kinds are counted before the one host wait that reads their totals.
 constexpr long long kSweepAllTests = 1LL << 22;
-nxd_status ipc_sweep_all(nxd_ctx* c, int kind, const double* leaf, int nprim, const double* qbox, int nq, GrowBuf& out,
-                         int* count) {
-    IpcState* s = c->ipc;
-    *count = 0;
-    if (nq == 0 || nprim == 0) return NXD_OK;
-    IPC_ENSURE(s->cnt, 4 * (size_t)nq); IPC_ENSURE(s->off, 4 * (size_t)nq);
-    int* d_tot = s->scal.as<int>();
-    const int grid = grid_for(nq, 128);
-    k_sweep_all<<<grid, 128, 0, c->stream>>>(s->pg, kind, qbox, nq, leaf, nprim, s->cnt.as<int>(), nullptr, nullptr);
-    k_scan<<<1, 1024, 0, c->stream>>>(s->cnt.as<int>(), s->off.as<int>(), nq, d_tot, nullptr, nullptr, nullptr);
-    int h = 0;
-    NXD_CUDA(cudaMemcpyAsync(&h, d_tot, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    NXD_CUDA(cudaStreamSynchronize(c->stream));
-    *count = h;
-    IPC_ENSURE(out, 8 * (size_t)std::max(h, 1));
-    k_sweep_all<<<grid, 128, 0, c->stream>>>(s->pg, kind, qbox, nq, leaf, nprim, nullptr, s->off.as<int>(), out.as<int>());
-    NXD_CUDA(cudaGetLastError());
-    return NXD_OK;
-}
-
 nxd_status ipc_candidates(nxd_ctx* c, bool swept, double infl) {
     IpcState* s = c->ipc;
-    if ((long long)c->nv * c->nf + (long long)c->ne * c->ne <= kSweepAllTests) {
-        const double* w1 = swept ? s->wq1.as<double>() : nullptr;
-        IPC_ENSURE(s->faces.leaf, 48 * (size_t)std::max(c->nf, 1)); IPC_ENSURE(s->edges.leaf, 48 * (size_t)std::max(c->ne, 1));
-        IPC_ENSURE(s->qv, 48 * (size_t)std::max(c->nv, 1)); IPC_ENSURE(s->qe, 48 * (size_t)std::max(c->ne, 1));
-        if (c->nf) k_ipc_boxes<<<grid_for(c->nf, 256), 256, 0, c->stream>>>(s->pg, 0, s->wq0.as<double>(), w1, infl, s->faces.leaf.as<double>());
-        if (c->ne) k_ipc_boxes<<<grid_for(c->ne, 256), 256, 0, c->stream>>>(s->pg, 1, s->wq0.as<double>(), w1, infl, s->edges.leaf.as<double>());
-        if (c->nv) k_ipc_boxes<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(s->pg, 2, s->wq0.as<double>(), w1, 0.0, s->qv.as<double>());
-        if (c->ne) k_ipc_boxes<<<grid_for(c->ne, 256), 256, 0, c->stream>>>(s->pg, 3, s->wq0.as<double>(), w1, 0.0, s->qe.as<double>());
-        nxd_status st = ipc_sweep_all(c, 0, s->faces.leaf.as<double>(), c->nf, s->qv.as<double>(), c->nv, s->pt, &s->n_pt);
-        if (st == NXD_OK) st = ipc_sweep_all(c, 1, s->edges.leaf.as<double>(), c->ne, s->qe.as<double>(), c->ne, s->ee, &s->n_ee);
-        return st;
-    }
-    nxd_status st = ipc_build_bvh(c, s->faces, 0, swept, infl);
-    if (st == NXD_OK) st = ipc_build_bvh(c, s->edges, 1, swept, infl);
-    if (st != NXD_OK) return st;
-    IPC_ENSURE(s->qv, 48 * (size_t)c->nv); IPC_ENSURE(s->qe, 48 * (size_t)c->ne);
+    IpcScal* ds = s->ds();
     const double* w1 = swept ? s->wq1.as<double>() : nullptr;
+    const bool sweep = (long long)c->nv * c->nf + (long long)c->ne * c->ne <= kSweepAllTests;
+    const int nq[2] = {c->nv, c->ne}, np[2] = {c->nf, c->ne};
+    GrowBuf* cnt[2] = {&s->cnt, &s->cnt2};
+    GrowBuf* off[2] = {&s->off, &s->off2};
+    GrowBuf* out[2] = {&s->pt, &s->ee};
+    Bvh* tree[2] = {&s->faces, &s->edges};
+    if (sweep) {
+        for (int k = 0; k < 2; ++k) {
+            tree[k]->n = np[k];
+            IPC_ENSURE(tree[k]->leaf, 48 * (size_t)std::max(np[k], 1));
+            if (np[k])
+                k_ipc_boxes<<<grid_for(np[k], 256), 256, 0, c->stream>>>(s->pg, k, s->wq0.as<double>(), w1, infl,
+                                                                         tree[k]->leaf.as<double>());
+        }
+    } else {
+        for (int k = 0; k < 2; ++k) {
+            const nxd_status st = ipc_build_bvh(c, *tree[k], k, swept, infl);
+            if (st != NXD_OK) return st;
+        }
+    }
+    IPC_ENSURE(s->qv, 48 * (size_t)std::max(c->nv, 1)); IPC_ENSURE(s->qe, 48 * (size_t)std::max(c->ne, 1));
     if (c->nv) k_ipc_boxes<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(s->pg, 2, s->wq0.as<double>(), w1, 0.0, s->qv.as<double>());
     if (c->ne) k_ipc_boxes<<<grid_for(c->ne, 256), 256, 0, c->stream>>>(s->pg, 3, s->wq0.as<double>(), w1, 0.0, s->qe.as<double>());
-    st = ipc_traverse(c, 0, s->faces, s->qv.as<double>(), c->nv, s->pt, &s->n_pt);
-    if (st == NXD_OK) st = ipc_traverse(c, 1, s->edges, s->qe.as<double>(), c->ne, s->ee, &s->n_ee);
-    return st;
+    const double* qbox[2] = {s->qv.as<double>(), s->qe.as<double>()};
+    NXD_CUDA(cudaMemsetAsync(ds, 0, 4 * sizeof(int), c->stream));   // totals, status, segment count
+    auto launch = [&](int k, bool count) {
+        Bvh& B = *tree[k];
+        int* cn = count ? cnt[k]->as<int>() : nullptr;
+        const int* of = count ? nullptr : off[k]->as<int>();
+        int* dst = count ? nullptr : out[k]->as<int>();
+        if (sweep)
+            k_sweep_all<<<grid_for(32LL * nq[k], 128), 128, 0, c->stream>>>(s->pg, k, qbox[k], nq[k], B.leaf.as<double>(), B.n,
+                                                                            cn, of, dst);
+        else
+            k_traverse<<<grid_for(nq[k], 128), 128, 0, c->stream>>>(s->pg, k, qbox[k], nq[k], B.nbox.as<double>(),
+                                                                    B.child.as<int>(), B.i0.as<int>(), B.n, cn, of, dst,
+                                                                    &ds->status);
+    };
+    for (int k = 0; k < 2; ++k) {
+        if (nq[k] == 0 || np[k] == 0) continue;
+        IPC_ENSURE(*cnt[k], 4 * (size_t)nq[k]); IPC_ENSURE(*off[k], 4 * (size_t)nq[k]);
+        launch(k, true);
+        k_scan<<<1, 1024, 0, c->stream>>>(cnt[k]->as<int>(), off[k]->as<int>(), nq[k], &ds->tot[k], nullptr, nullptr, nullptr);
+    }
+    nxd_status st = ipc_fetch(c);
+    if (st != NXD_OK) return st;
+    if (s->hp->sc.status != 0) return (nxd_status)s->hp->sc.status;
+    s->n_pt = s->hp->sc.tot[0];
+    s->n_ee = s->hp->sc.tot[1];
+    for (int k = 0; k < 2; ++k) {
+        const int m = s->hp->sc.tot[k];
+        IPC_ENSURE(*out[k], 8 * (size_t)std::max(m, 1));
+        if (m == 0) continue;
+        launch(k, false);
+        if (sweep || m < 2) continue;
+        // traversal order -> (query, primitive) ascending
+        const int pbits = bits_for((unsigned long long)std::max(np[k], 1));
+        const int qbits = bits_for((unsigned long long)std::max(nq[k], 1));
+        IPC_ENSURE(s->tkey, 8 * (size_t)m); IPC_ENSURE(s->tval, 4 * (size_t)m);
+        k_pair_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(out[k]->as<int>(), m, pbits, s->tkey.as<unsigned long long>(),
+                                                             s->tval.as<int>());
+        st = radix_sort(c, s->tkey, s->tval, s->tkey1, s->tval1, m, 0, pbits + qbits);
+        if (st != NXD_OK) return st;
+        k_pair_from_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(s->tkey.as<unsigned long long>(), m, pbits, out[k]->as<int>());
+    }
+    NXD_CUDA(cudaGetLastError());
+    return NXD_OK;
 }
 
-// Sorted segments of keys[0..m): starts in s->sstart (m_seg + 1 entries).
-nxd_status ipc_segments(nxd_ctx* c, const unsigned long long* keys, int m, int* nseg_host) {
+// Sorted segments of keys[0..m): starts in s->sstart (m_seg + 1 entries);
+// the segment count stays on the device (IpcScal::nseg).
+nxd_status ipc_segments(nxd_ctx* c, const unsigned long long* keys, int m) {
     IpcState* s = c->ipc;
     IPC_ENSURE(s->sflag, 4 * (size_t)m); IPC_ENSURE(s->spos, 4 * (size_t)m); IPC_ENSURE(s->sstart, 4 * (size_t)(m + 1));
-    int* d_n = s->scal.as<int>() + 2;
+    int* d_n = &s->ds()->nseg;
     k_seg_flags<<<grid_for(m, 256), 256, 0, c->stream>>>(keys, m, s->sflag.as<int>());
     k_scan<<<1, 1024, 0, c->stream>>>(s->sflag.as<int>(), s->spos.as<int>(), m, d_n, nullptr, nullptr, nullptr);
     k_seg_starts<<<grid_for(m, 256), 256, 0, c->stream>>>(s->sflag.as<int>(), s->spos.as<int>(), m, s->sstart.as<int>(), d_n);
-    NXD_CUDA(cudaMemcpyAsync(nseg_host, d_n, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    NXD_CUDA(cudaGetLastError());
     return NXD_OK;
 }
 
@@ -1493,89 +1536,91 @@ nxd_status nxd_ipc_candidates(nxd_ctx* c, const double* x, const double* dx, dou
 
 namespace {
 
-// The barrier form over the candidates of the last ipc_candidates call:
-// energy (to the host), and with `full` the gradient in s->gout and the PSD
-// BSR Hessian in s->rowptr / s->colidx / s->vals (*nh blocks).
-nxd_status ipc_barrier_eval(nxd_ctx* c, double dhat, double kappa, bool full, double* energy, int* n_active, int* nh_out) {
+// The barrier form over the candidates of the last ipc_candidates call.
+// The energy goes to IpcScal::energy on the device (read by the caller's
+// next ipc_fetch).  With `full`, also the active count (IpcScal::na, read
+// here with one host wait), the gradient in s->gout and the PSD BSR Hessian
+// in s->rowptr / s->colidx / s->vals, its block count s->rowptr[N] on the
+// device; *nh_out, when asked for, costs one more host wait.
+nxd_status ipc_barrier_eval(nxd_ctx* c, double dhat, double kappa, bool full, int* nh_out) {
     IpcState* s = c->ipc;
+    IpcScal* ds = s->ds();
     const int N = c->N, n = s->n_pt + s->n_ee;
     const IpcPairs P{s->pt.as<int>(), s->n_pt, s->ee.as<int>(), s->n_ee};
     const IpcPose ps{s->wq0.as<double>(), s->pp0.as<double>()};
     const size_t nn = std::max(n, 1);
-    IPC_ENSURE(s->e, 8 * nn); IPC_ENSURE(s->grad12, 96 * nn); IPC_ENSURE(s->lam, 40 * nn); IPC_ENSURE(s->z, 480 * nn);
+    IPC_ENSURE(s->e, 8 * nn);
+    if (!full) {
+        if (n) k_ipc_pair_energy<<<grid_for(n, 128), 128, 0, c->stream>>>(s->pg, P, ps, dhat, kappa, s->e.as<double>());
+        k_tree_sum<<<1, 1024, 0, c->stream>>>(s->e.as<double>(), n, &ds->energy);
+        NXD_CUDA(cudaGetLastError());
+        return NXD_OK;
+    }
+    IPC_ENSURE(s->grad12, 96 * nn); IPC_ENSURE(s->lam, 40 * nn); IPC_ENSURE(s->z, 480 * nn);
     IPC_ENSURE(s->nterm, 4 * nn); IPC_ENSURE(s->body, 8 * nn); IPC_ENSURE(s->active, 4 * nn); IPC_ENSURE(s->type, 4 * nn);
     IPC_ENSURE(s->apos, 4 * nn); IPC_ENSURE(s->alist, 4 * nn);
     const IpcEvalOut o{s->e.as<double>(), s->grad12.as<double>(), s->lam.as<double>(), s->z.as<double>(), s->nterm.as<int>(),
                        s->body.as<int>(), s->active.as<int>(), s->type.as<int>()};
-    double* d_energy = reinterpret_cast<double*>(s->scal.as<char>() + 32);
-    int* d_na = s->scal.as<int>() + 3;
     if (n) k_ipc_pair_eval<<<grid_for(n, 128), 128, 0, c->stream>>>(s->pg, P, ps, dhat, kappa, o);
-    k_tree_sum<<<1, 1024, 0, c->stream>>>(s->e.as<double>(), n, d_energy);
-    k_scan<<<1, 1024, 0, c->stream>>>(s->active.as<int>(), s->apos.as<int>(), n, d_na, nullptr, nullptr, nullptr);
+    k_tree_sum<<<1, 1024, 0, c->stream>>>(s->e.as<double>(), n, &ds->energy);
+    k_scan<<<1, 1024, 0, c->stream>>>(s->active.as<int>(), s->apos.as<int>(), n, &ds->na, nullptr, nullptr, nullptr);
     if (n) k_compact<<<grid_for(n, 256), 256, 0, c->stream>>>(s->active.as<int>(), s->apos.as<int>(), n, s->alist.as<int>());
-    int na = 0;
-    double eh = 0.0;
-    NXD_CUDA(cudaMemcpyAsync(&na, d_na, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    NXD_CUDA(cudaMemcpyAsync(&eh, d_energy, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    NXD_CUDA(cudaStreamSynchronize(c->stream));
-    if (energy) *energy = eh;
-    if (n_active) *n_active = na;
-    if (!full) return NXD_OK;
+    nxd_status st = ipc_fetch(c);
+    if (st != NXD_OK) return st;
+    const int na = s->hp->sc.na;
+    IPC_ENSURE(s->gout, 48 * (size_t)N);
+    IPC_ENSURE(s->rowptr, 4 * (size_t)(N + 1));
+    NXD_CUDA(cudaMemsetAsync(s->gout.p, 0, 48 * (size_t)N, c->stream));
+    if (na == 0) {
+        NXD_CUDA(cudaMemsetAsync(s->rowptr.p, 0, 4 * (size_t)(N + 1), c->stream));
+        if (nh_out) *nh_out = 0;
+        NXD_CUDA(cudaGetLastError());
+        return NXD_OK;
+    }
     // contributions, stable-sorted by body / by (row body, col body)
-    IPC_ENSURE(s->gkey, 16 * (size_t)std::max(na, 1)); IPC_ENSURE(s->gval, 8 * (size_t)std::max(na, 1));
-    IPC_ENSURE(s->hkey, 32 * (size_t)std::max(na, 1)); IPC_ENSURE(s->hval, 16 * (size_t)std::max(na, 1));
-    if (na)
-        k_ipc_contrib<<<grid_for(na, 128), 128, 0, c->stream>>>(s->alist.as<int>(), na, s->body.as<int>(), N,
-                                                                 s->gkey.as<unsigned long long>(), s->gval.as<int>(),
-                                                                 s->hkey.as<unsigned long long>(), s->hval.as<int>());
-    nxd_status st = radix_sort(c, s->gkey, s->gval, s->gkey1, s->gval1, 2 * na, 0, bits_for((unsigned long long)N));
+    IPC_ENSURE(s->gkey, 16 * (size_t)na); IPC_ENSURE(s->gval, 8 * (size_t)na);
+    IPC_ENSURE(s->hkey, 32 * (size_t)na); IPC_ENSURE(s->hval, 16 * (size_t)na);
+    k_ipc_contrib<<<grid_for(na, 128), 128, 0, c->stream>>>(s->alist.as<int>(), na, s->body.as<int>(), N,
+                                                             s->gkey.as<unsigned long long>(), s->gval.as<int>(),
+                                                             s->hkey.as<unsigned long long>(), s->hval.as<int>());
+    st = radix_sort(c, s->gkey, s->gval, s->gkey1, s->gval1, 2 * na, 0, bits_for((unsigned long long)N));
     if (st == NXD_OK)
         st = radix_sort(c, s->hkey, s->hval, s->hkey1, s->hval1, 4 * na, 0, bits_for((unsigned long long)N * (unsigned long long)N));
     if (st != NXD_OK) return st;
-    IPC_ENSURE(s->gout, 48 * (size_t)N);
-    NXD_CUDA(cudaMemsetAsync(s->gout.p, 0, 48 * (size_t)N, c->stream));
-    IPC_ENSURE(s->sflag, 16 * (size_t)std::max(na, 1)); IPC_ENSURE(s->spos, 16 * (size_t)std::max(na, 1));
-    IPC_ENSURE(s->sstart, 16 * (size_t)std::max(na, 1) + 4);
-    int ng = 0;
-    if (na) {
-        st = ipc_segments(c, s->gkey.as<unsigned long long>(), 2 * na, &ng);
-        if (st != NXD_OK) return st;
-        k_ipc_grad<<<grid_for(6LL * ng, 128), 128, 0, c->stream>>>(s->gkey.as<unsigned long long>(), s->gval.as<int>(),
-                                                                    s->sstart.as<int>(), s->scal.as<int>() + 2,
-                                                                    s->grad12.as<double>(), s->gout.as<double>());
-    }
-    int nh = 0;
-    if (na) {
-        st = ipc_segments(c, s->hkey.as<unsigned long long>(), 4 * na, &nh);
-        if (st != NXD_OK) return st;
-    }
-    IPC_ENSURE(s->rowptr, 4 * (size_t)(N + 1)); IPC_ENSURE(s->colidx, 4 * (size_t)std::max(nh, 1));
-    IPC_ENSURE(s->vals, 288 * (size_t)std::max(nh, 1));
-    if (nh)
-        k_ipc_hess<<<grid_for(36LL * nh, 128), 128, 0, c->stream>>>(s->hkey.as<unsigned long long>(), s->hval.as<int>(),
-                                                                     s->sstart.as<int>(), s->scal.as<int>() + 2, N,
-                                                                     s->lam.as<double>(), s->z.as<double>(), s->nterm.as<int>(),
-                                                                     s->colidx.as<int>(), s->vals.as<double>(), nh);
-    if (nh) k_ipc_rowptr<<<grid_for(N + 1, 128), 128, 0, c->stream>>>(s->hkey.as<unsigned long long>(), s->sstart.as<int>(),
-                                                                        s->scal.as<int>() + 2, N, s->rowptr.as<int>());
-    else NXD_CUDA(cudaMemsetAsync(s->rowptr.p, 0, 4 * (size_t)(N + 1), c->stream));
-    if (nh_out) *nh_out = nh;
+    // at most 2 na gradient segments and 4 na Hessian blocks: the kernels
+    // read the actual counts on the device, the grids cover the bounds
+    IPC_ENSURE(s->sflag, 16 * (size_t)na); IPC_ENSURE(s->spos, 16 * (size_t)na); IPC_ENSURE(s->sstart, 16 * (size_t)na + 4);
+    IPC_ENSURE(s->colidx, 16 * (size_t)na); IPC_ENSURE(s->vals, 1152 * (size_t)na);
+    int* d_nseg = &ds->nseg;
+    if ((st = ipc_segments(c, s->gkey.as<unsigned long long>(), 2 * na)) != NXD_OK) return st;
+    k_ipc_grad<<<grid_for(12LL * na, 128), 128, 0, c->stream>>>(s->gkey.as<unsigned long long>(), s->gval.as<int>(),
+                                                                 s->sstart.as<int>(), d_nseg, s->grad12.as<double>(),
+                                                                 s->gout.as<double>());
+    if ((st = ipc_segments(c, s->hkey.as<unsigned long long>(), 4 * na)) != NXD_OK) return st;
+    k_ipc_hess<<<grid_for(144LL * na, 128), 128, 0, c->stream>>>(s->hkey.as<unsigned long long>(), s->hval.as<int>(),
+                                                                  s->sstart.as<int>(), d_nseg, N, s->lam.as<double>(),
+                                                                  s->z.as<double>(), s->nterm.as<int>(), s->colidx.as<int>(),
+                                                                  s->vals.as<double>(), 4LL * na);
+    k_ipc_rowptr<<<grid_for(N + 1, 128), 128, 0, c->stream>>>(s->hkey.as<unsigned long long>(), s->sstart.as<int>(), d_nseg, N,
+                                                               s->rowptr.as<int>());
     NXD_CUDA(cudaGetLastError());
+    if (nh_out) {
+        if ((st = ipc_fetch(c)) != NXD_OK) return st;
+        *nh_out = s->hp->sc.nseg;
+    }
     return NXD_OK;
 }
 
-// additive-CCD bound over the swept candidates of the last ipc_pose(x, dx)
-nxd_status ipc_accd(nxd_ctx* c, double eta, double* alpha) {
+// additive-CCD bound over the swept candidates of the last ipc_pose(x, dx),
+// into IpcScal::alpha (read by the caller's next ipc_fetch)
+nxd_status ipc_accd(nxd_ctx* c, double eta) {
     IpcState* s = c->ipc;
     const int n = s->n_pt + s->n_ee;
     IPC_ENSURE(s->toi, 8 * (size_t)std::max(n, 1));
     const IpcPairs P{s->pt.as<int>(), s->n_pt, s->ee.as<int>(), s->n_ee};
-    double* d_a = reinterpret_cast<double*>(s->scal.as<char>() + 40);
     if (n) k_ipc_accd<<<grid_for(n, 128), 128, 0, c->stream>>>(s->pg, P, s->wq0.as<double>(), s->wq1.as<double>(), eta, 1000,
                                                                 s->toi.as<double>());
-    k_min_reduce<<<1, 1024, 0, c->stream>>>(s->toi.as<double>(), n, 1.0, d_a);
-    NXD_CUDA(cudaMemcpyAsync(alpha, d_a, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    NXD_CUDA(cudaStreamSynchronize(c->stream));
+    k_min_reduce<<<1, 1024, 0, c->stream>>>(s->toi.as<double>(), n, 1.0, &s->ds()->alpha);
     NXD_CUDA(cudaGetLastError());
     return NXD_OK;
 }
@@ -1595,10 +1640,11 @@ nxd_status nxd_ipc_barrier(nxd_ctx* c, const double* x, double dhat, double kapp
     IpcState* s = c->ipc;
     const int N = c->N;
     if (n_pairs) *n_pairs = s->n_pt + s->n_ee;
-    int na = 0, nh = 0;
-    st = ipc_barrier_eval(c, dhat, kappa, true, energy, &na, &nh);
+    int nh = 0;
+    st = ipc_barrier_eval(c, dhat, kappa, true, &nh);
     if (st != NXD_OK) return st;
-    if (n_active) *n_active = na;
+    if (energy) *energy = s->hp->sc.energy;
+    if (n_active) *n_active = s->hp->sc.na;
     if (grad) NXD_CUDA(cudaMemcpyAsync(grad, s->gout.p, 48 * (size_t)N, cudaMemcpyDeviceToHost, c->stream));
     if (nnzb) *nnzb = nh;
     if (nh > cap_blocks && (col_idx || vals)) { NXD_CUDA(cudaStreamSynchronize(c->stream)); return NXD_CAPACITY; }
@@ -1617,7 +1663,10 @@ nxd_status nxd_ipc_max_step(nxd_ctx* c, const double* x, const double* dx, doubl
     if (st == NXD_OK) st = ipc_candidates(c, true, 0.0);
     if (st != NXD_OK) return st;
     if (n_pairs) *n_pairs = c->ipc->n_pt + c->ipc->n_ee;
-    return ipc_accd(c, eta, alpha);
+    if (st == NXD_OK) st = ipc_accd(c, eta);
+    if (st == NXD_OK) st = ipc_fetch(c);
+    if (st == NXD_OK) *alpha = c->ipc->hp->sc.alpha;
+    return st;
 }
 
 // Full-IPC time step: the x_tilde of implicit Euler (or Newmark) and the
@@ -1640,6 +1689,8 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
     nxd_status st = ipc_prepare(c);
     if (st != NXD_OK) return st;
     IpcState* s = c->ipc;
+    IpcScal* ds = s->ds();
+    const IpcScal& hs = s->hp->sc;
     const int N = c->N, n6 = 6 * N;
     cudaStream_t sm = c->stream;
     StepCfg cfg = step_cfg(c);
@@ -1653,24 +1704,17 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
     const long long cap_r = N + 2LL * (c->J + c->D);
     IPC_ENSURE(s->rrp, 4 * (size_t)(N + 1)); IPC_ENSURE(s->rci, 4 * (size_t)std::max(cap_r, 1LL));
     IPC_ENSURE(s->rvv, 288 * (size_t)std::max(cap_r, 1LL));
-    IPC_ENSURE(s->rnz, 8); IPC_ENSURE(s->mrp, 4 * (size_t)(N + 1)); IPC_ENSURE(s->gr, 8 * (size_t)n6);
+    IPC_ENSURE(s->mrp, 4 * (size_t)(N + 1)); IPC_ENSURE(s->gr, 8 * (size_t)n6);
     IPC_ENSURE(s->gt, 8 * (size_t)n6); IPC_ENSURE(s->gneg, 8 * (size_t)n6); IPC_ENSURE(s->prod, 8 * (size_t)n6);
-    IPC_ENSURE(s->xt, 8 * (size_t)n6); IPC_ENSURE(s->stat, 8); IPC_ENSURE(s->val, 16);
+    IPC_ENSURE(s->xt, 8 * (size_t)n6); IPC_ENSURE(s->stat, 8);
     double* x = c->x;
-    double* val = s->val.as<double>();
-    std::vector<int> rpr(N + 1), rpb(N + 1), rpm(N + 1);
-    std::vector<double> gh(n6);
-    auto rest_value = [&](const double* xx, double* v) -> nxd_status {
-        k_form_eval<<<1, kSolverThreads, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 0, xx, val, nullptr, nullptr, nullptr, 0, nullptr);
-        NXD_CUDA(cudaMemcpyAsync(v, val, sizeof(double), cudaMemcpyDeviceToHost, sm));
-        NXD_CUDA(cudaStreamSynchronize(sm));
-        return NXD_OK;
-    };
-    auto barrier_value = [&](const double* xx, double* v) -> nxd_status {
-        nxd_status r = ipc_pose(c, xx, nullptr, true);
-        if (r == NXD_OK) r = ipc_candidates(c, false, p->dhat);
-        if (r == NXD_OK) r = ipc_barrier_eval(c, p->dhat, p->kappa, false, v, nullptr, nullptr);
-        return r;
+    int* rpr = s->hrow;                 // pinned: rest-form, barrier and merged row pointers
+    int* rpb = s->hrow + (N + 1);
+    int* rpm = s->hrow + 2 * (N + 1);
+    // rest-form value at xx into IpcScal::rest, read at the next fetch
+    auto rest_value = [&](const double* xx) {
+        k_form_eval<<<1, kSolverThreads, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 0, xx, &ds->rest, nullptr, nullptr, nullptr, 0,
+                                                  nullptr);
     };
     int iters = 0, conv = 0, lsfail = 0, solvefail = 0, na = 0, pcg_total = 0;
     double amax = 1.0, fx = 0.0;
@@ -1680,41 +1724,41 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
         // gradient at x: rest forms, then the barrier over the candidates at x
         k_form_eval<<<1, kSolverThreads, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 1, x, s->gr.as<double>(), nullptr, nullptr,
                                                   nullptr, 0, nullptr);
-        double eb = 0.0;
-        int nh = 0;
         st = ipc_pose(c, x, nullptr, true);
         if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
-        if (st == NXD_OK) st = ipc_barrier_eval(c, p->dhat, p->kappa, true, &eb, &na, &nh);
+        if (st == NXD_OK) st = ipc_barrier_eval(c, p->dhat, p->kappa, true, nullptr);
         if (st != NXD_OK) return st;
+        const double eb = hs.energy;
+        na = hs.na;
         npairs = s->n_pt + s->n_ee;
         k_grad_combine<<<grid_for(n6, 256), 256, 0, sm>>>(s->gr.as<double>(), s->gout.as<double>(), scale, n6,
                                                           s->gt.as<double>(), s->gneg.as<double>());
-        NXD_CUDA(cudaMemcpyAsync(gh.data(), s->gt.p, 8 * (size_t)n6, cudaMemcpyDeviceToHost, sm));
-        NXD_CUDA(cudaStreamSynchronize(sm));
-        double ginf = 0.0;
-        for (double v : gh) ginf = std::max(ginf, std::fabs(v));
-        if (ginf < p->newton_tol) { conv = 1; break; }
-        // Hessian: rest-form blocks, then the barrier's, row by row
+        k_absmax<<<1, 1024, 0, sm>>>(s->gt.as<double>(), n6, &ds->ginf);
+        // the rest forms' Hessian blocks and both row pointers come back with
+        // |g|_inf in one wait (unused when the gradient test ends the solve)
         k_form_eval<<<1, kSolverThreads, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 2, x, nullptr, s->rrp.as<int>(), s->rci.as<int>(),
-                                                  s->rvv.as<double>(), cap_r, s->rnz.as<long long>());
-        long long nzr = 0;
-        NXD_CUDA(cudaMemcpyAsync(&nzr, s->rnz.p, sizeof(long long), cudaMemcpyDeviceToHost, sm));
-        NXD_CUDA(cudaMemcpyAsync(rpr.data(), s->rrp.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, sm));
-        NXD_CUDA(cudaMemcpyAsync(rpb.data(), s->rowptr.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, sm));
-        NXD_CUDA(cudaStreamSynchronize(sm));
-        if (nzr < 0 || nzr > cap_r) return NXD_CAPACITY;
+                                                  s->rvv.as<double>(), cap_r, &ds->rnz);
+        NXD_CUDA(cudaMemcpyAsync(rpr, s->rrp.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, sm));
+        NXD_CUDA(cudaMemcpyAsync(rpb, s->rowptr.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, sm));
+        if ((st = ipc_fetch(c)) != NXD_OK) return st;
+        if (hs.ginf < p->newton_tol) { conv = 1; break; }
+        if (hs.rnz < 0 || hs.rnz > cap_r) return NXD_CAPACITY;
+        // Hessian: rest-form blocks, then the barrier's, row by row
         rpm[0] = 0;
-        for (int i = 0; i < N; ++i) rpm[i + 1] = rpm[i] + (rpr[i + 1] - rpr[i]) + (nh ? rpb[i + 1] - rpb[i] : 0);
+        for (int i = 0; i < N; ++i) rpm[i + 1] = rpm[i] + (rpr[i + 1] - rpr[i]) + (rpb[i + 1] - rpb[i]);
+        const int nh = rpb[N];
         const long long nzm = rpm[N];
         IPC_ENSURE(s->mci, 4 * (size_t)std::max<long long>(nzm, 1)); IPC_ENSURE(s->mvv, 288 * (size_t)std::max<long long>(nzm, 1));
         IPC_ENSURE(s->erow, 4 * (size_t)std::max<long long>(nzm, 1)); IPC_ENSURE(s->items, 4 * (size_t)std::max<long long>(nzm, 1));
         IPC_ENSURE(s->iact, 4 * (size_t)std::max<long long>(nzm, 1));
-        NXD_CUDA(cudaMemcpyAsync(s->mrp.p, rpm.data(), 4 * (size_t)(N + 1), cudaMemcpyHostToDevice, sm));
+        NXD_CUDA(cudaMemcpyAsync(s->mrp.p, rpm, 4 * (size_t)(N + 1), cudaMemcpyHostToDevice, sm));
         k_bsr_concat<<<grid_for(N, 128), 128, 0, sm>>>(N, s->rrp.as<int>(), s->rci.as<int>(), s->rvv.as<double>(),
                                                        nh ? s->rowptr.as<int>() : nullptr, s->colidx.as<int>(),
                                                        s->vals.as<double>(), scale, s->mrp.as<int>(), s->mci.as<int>(),
                                                        s->mvv.as<double>());
         // H dx = -g: block-Jacobi PCG, or the component LDL^T
+        s->hp->fail = 0;
+        s->hp->capst = 0;
         if (p->linear_solver == 1) {
             int pit = 0;
             double pres = 0.0;
@@ -1725,49 +1769,48 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
             pcg_total += pit;
             if (pr != NXD_OK) { solvefail = 1; break; }
         } else {
-        Solver S = c->S;
-        S.ext_n = (int)nzm; S.ext_row = s->erow.as<int>(); S.ext_col = s->mci.as<int>(); S.ext_vals = s->mvv.as<double>();
-        S.items = s->items.as<int>(); S.iact = s->iact.as<int>(); S.status = s->stat.as<int>();
-        NXD_CUDA(cudaMemsetAsync(s->stat.p, 0, sizeof(int), sm));
-        k_bsr_prepare<<<grid_for(N, 128), 128, 0, sm>>>(S, s->mrp.as<int>(), s->gneg.as<double>(), s->erow.as<int>());
-        k_linear_solve<<<1, kNewtonThreads, kNewtonDynSmem, sm>>>(S);
-        int fail = 0, capst = 0;
-        NXD_CUDA(cudaMemcpyAsync(&fail, S.solve_fail, sizeof(int), cudaMemcpyDeviceToHost, sm));
-        NXD_CUDA(cudaMemcpyAsync(&capst, s->stat.p, sizeof(int), cudaMemcpyDeviceToHost, sm));
-        NXD_CUDA(cudaStreamSynchronize(sm));
-        if (capst) return NXD_CAPACITY;
-        if (fail) { solvefail = 1; break; }
+            Solver S = c->S;
+            S.ext_n = (int)nzm; S.ext_row = s->erow.as<int>(); S.ext_col = s->mci.as<int>(); S.ext_vals = s->mvv.as<double>();
+            S.items = s->items.as<int>(); S.iact = s->iact.as<int>(); S.status = s->stat.as<int>();
+            NXD_CUDA(cudaMemsetAsync(s->stat.p, 0, sizeof(int), sm));
+            k_bsr_prepare<<<grid_for(N, 128), 128, 0, sm>>>(S, s->mrp.as<int>(), s->gneg.as<double>(), s->erow.as<int>());
+            k_linear_solve<<<1, kNewtonThreads, kNewtonDynSmem, sm>>>(S);
+            NXD_CUDA(cudaMemcpyAsync(&s->hp->fail, S.solve_fail, sizeof(int), cudaMemcpyDeviceToHost, sm));
+            NXD_CUDA(cudaMemcpyAsync(&s->hp->capst, s->stat.p, sizeof(int), cudaMemcpyDeviceToHost, sm));
         }
         double* dx = c->S.dx;
+        k_absmax<<<1, 1024, 0, sm>>>(dx, n6, &ds->dxinf);
+        if ((st = ipc_fetch(c)) != NXD_OK) return st;
+        if (s->hp->capst) return NXD_CAPACITY;
+        if (s->hp->fail) { solvefail = 1; break; }
         // the velocity criterion of IPC: a Newton step below tol * dt ends it
-        NXD_CUDA(cudaMemcpyAsync(gh.data(), dx, 8 * (size_t)n6, cudaMemcpyDeviceToHost, sm));
-        NXD_CUDA(cudaStreamSynchronize(sm));
-        double dxinf = 0.0;
-        for (double v : gh) dxinf = std::max(dxinf, std::fabs(v));
-        if (dxinf < p->newton_tol * dt) { conv = 1; break; }
-        // the step bound: additive CCD over the swept candidates
+        if (hs.dxinf < p->newton_tol * dt) { conv = 1; break; }
+        // the step bound (additive CCD over the swept candidates), the value
+        // at x and the descent g . dx, read back in one wait
         st = ipc_pose(c, x, dx, true);
         if (st == NXD_OK) st = ipc_candidates(c, true, 0.0);
-        if (st == NXD_OK) st = ipc_accd(c, p->eta, &amax);
+        if (st == NXD_OK) st = ipc_accd(c, p->eta);
         if (st != NXD_OK) return st;
-        // line search from min(1, bound)
-        double er = 0.0;
-        if ((st = rest_value(x, &er)) != NXD_OK) return st;
-        fx = er + scale * eb;
+        rest_value(x);
         k_mul_vec<<<grid_for(n6, 256), 256, 0, sm>>>(s->gt.as<double>(), dx, n6, s->prod.as<double>());
-        k_tree_sum<<<1, 1024, 0, sm>>>(s->prod.as<double>(), n6, val + 1);
-        double descent = 0.0;
-        NXD_CUDA(cudaMemcpyAsync(&descent, val + 1, sizeof(double), cudaMemcpyDeviceToHost, sm));
-        NXD_CUDA(cudaStreamSynchronize(sm));
+        k_tree_sum<<<1, 1024, 0, sm>>>(s->prod.as<double>(), n6, &ds->descent);
+        if ((st = ipc_fetch(c)) != NXD_OK) return st;
+        amax = hs.alpha;
+        fx = hs.rest + scale * eb;
+        const double descent = hs.descent;
         if (descent > 0) { lsfail = 1; break; }
+        // line search from min(1, bound)
         double alpha = std::min(1.0, amax);
         bool done = false;
         for (int ls = 0; ls < p->ls_max_iters; ++ls) {
             k_axpy_alpha<<<grid_for(n6, 256), 256, 0, sm>>>(x, dx, alpha, n6, s->xt.as<double>());
-            double ert = 0.0, ebt = 0.0;
-            if ((st = rest_value(s->xt.as<double>(), &ert)) != NXD_OK) return st;
-            if ((st = barrier_value(s->xt.as<double>(), &ebt)) != NXD_OK) return st;
-            const double fn = ert + scale * ebt;
+            rest_value(s->xt.as<double>());
+            st = ipc_pose(c, s->xt.as<double>(), nullptr, true);
+            if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
+            if (st == NXD_OK) st = ipc_barrier_eval(c, p->dhat, p->kappa, false, nullptr);
+            if (st == NXD_OK) st = ipc_fetch(c);
+            if (st != NXD_OK) return st;
+            const double fn = hs.rest + scale * hs.energy;
             if (fn <= fx + c->s.ls_c1 * alpha * descent) { done = true; fx = fn; break; }
             alpha *= c->s.ls_rho;
         }
