@@ -595,6 +595,28 @@ def diff_scene(seed: int = 5000) -> Scene:
     return sb.build(_settings(1e-3, 0.3), dt=1e-2, steps=50)
 
 
+def double_pendulum(dt: float = 1e-3, max_time: float = 1.5, inertia_zz=(1.0, 1.0)) -> Scene:
+    """The reference's double-pendulum regression case as its scene loader
+    builds it (nexdynipc/assets/double_pendulum/double_pendulum.json through
+    SceneLoader and Simulation::run): a meshless 1 kg anchor held by a
+    FixedJoint at the origin and two meshless 1 kg links with unit inertia at
+    (0.5, 0, 0) and (1.5, 0, 0), hinged about z at (0, 0, 0) and (1, 0, 0),
+    released at rest; ImplicitNewmark (beta 0.25, gamma 0.5), every joint at
+    the file's joint_stiffness 1e7, dt 1e-3, 1.5 s.  inertia_zz sets the
+    links' inertia about the hinge axis (the other diagonal entries stay 1)."""
+    from .sceneio import SimulationConfig, settings_from_config
+    sb = SceneBuilder("double_pendulum")
+    ev, ef = np.zeros((0, 3)), np.zeros((0, 3), np.int32)
+    sb.add_body(ev, ef, (0.0, 0.0, 0.0), mass=1.0, inertia=np.eye(3))
+    for k, x in enumerate((0.5, 1.5)):
+        sb.add_body(ev, ef, (x, 0.0, 0.0), mass=1.0, inertia=np.diag([1.0, 1.0, float(inertia_zz[k])]))
+    sb.fix(0, stiffness=1e7)
+    sb.hinge(0, 1, (0.0, 0.0, 0.0), (-0.5, 0.0, 0.0), (0.0, 0.0, 1.0), (0.0, 0.0, 1.0), stiffness=1e7)
+    sb.hinge(1, 2, (0.5, 0.0, 0.0), (-0.5, 0.0, 0.0), (0.0, 0.0, 1.0), (0.0, 0.0, 1.0), stiffness=1e7)
+    cfg = SimulationConfig(dt=dt, max_time=max_time, joint_stiffness=1e7)
+    return sb.build(settings_from_config(cfg), dt, int(math.ceil(max_time / dt - 1e-12)))
+
+
 CONFIGS = {
     "cube_stack": cube_stack,
     "sphere_bowl": sphere_bowl,
