@@ -316,17 +316,22 @@ def pcg_leg(n_bodies: int = 200000, iters: int = 60):
             "achieved_gbs": per_iter * st["iterations"] / secs / 1e9 if secs > 0 else None}
 
 
-def ipc_step_leg(n_cubes: int = 8, settle: int = 30, steps: int = 20, solver: int = 0):
-    """Full-IPC time step (nxd_ipc_step) on a tower of tilted cubes falling
+def ipc_step_params(solver: int = 0):
+    from nexdynipc_b200 import abi
+    return abi.ipc_params(dhat=1e-3, kappa=1e11, eta=0.1, newton_tol=1e-5, newton_max_iters=50, ls_max_iters=30,
+                          linear_solver=solver, pcg_max_iter=500, pcg_tol=1e-12)
+
+
+def ipc_step_leg(n_cubes: int = 8, columns: int = 1, settle: int = 30, steps: int = 20, solver: int = 0):
+    """Full-IPC time step (nxd_ipc_step) on stacks of tilted cubes falling
     onto a ground box: after `settle` steps (the cubes in contact), wall
     clock of `steps` steps, each a host-ordered Newton loop of device calls
     (candidates, barrier, rest forms, block solve, CCD bound, line search)."""
     import time
-    from nexdynipc_b200 import abi, runtime, scenes
-    sc = scenes.ipc_drop(n_cubes=n_cubes)
+    from nexdynipc_b200 import runtime, scenes
+    sc = scenes.ipc_drop(n_cubes=n_cubes, columns=columns)
     ctx = runtime.Context(sc)
-    p = abi.ipc_params(dhat=1e-3, kappa=1e11, eta=0.1, newton_tol=1e-5, newton_max_iters=50, ls_max_iters=30,
-                       linear_solver=solver, pcg_max_iter=500, pcg_tol=1e-12)
+    p = ipc_step_params(solver)
     for _ in range(settle):
         ctx.ipc_step(p)
     its, act, pairs, conv, lsf = [], [], [], 0, 0
@@ -338,12 +343,31 @@ def ipc_step_leg(n_cubes: int = 8, settle: int = 30, steps: int = 20, solver: in
         lsf += st["line_search_failed"]
     wall = time.perf_counter() - t0
     ctx.close()
-    return {"workload": f"{n_cubes} tilted 0.2 m cubes on a ground box, dhat 1e-3, kappa 1e11, dt {sc.dt}",
+    return {"workload": (f"{n_cubes} tilted 0.2 m cubes in {columns} stack(s) on a ground box, dhat 1e-3, "
+                         f"kappa 1e11, dt {sc.dt}; steps {settle + 1}-{settle + steps}"),
             "steps": steps, "steps_per_s": steps / wall, "newton_iterations_mean": float(np.mean(its)),
             "active_pairs_mean": float(np.mean(act)), "candidate_pairs_mean": float(np.mean(pairs)),
             "converged_steps": conv, "line_search_failures": lsf,
             "linear_solver": "block-Jacobi PCG" if solver else "component LDL^T",
             "timing": "wall clock per nxd_ipc_step (it synchronises)"}
+
+
+def ipc_step_cpu_baseline(n_cubes: int, columns: int, settle: int, steps: int):
+    """The CPU oracle's full-IPC step (serial) on the same trajectory segment
+    as ipc_step_leg: `settle` untimed steps, then wall clock of `steps`."""
+    from nexdynipc_b200 import scenes
+    from oracle.refcpu import OracleWorld
+    ow = OracleWorld(scenes.ipc_drop(n_cubes=n_cubes, columns=columns))
+    p = ipc_step_params(0)
+    for _ in range(settle):
+        ow.ipc_step(p)
+    t0 = time.perf_counter()
+    its = 0
+    for _ in range(steps):
+        its += ow.ipc_step(p)["newton_iterations"]
+    wall = time.perf_counter() - t0
+    return {"steps_per_s": steps / wall, "cores": 1, "kind": "port", "newton_iterations_mean": its / steps,
+            "sample": f"the same {steps} steps through the CPU oracle's nxo_ipc_step (serial), {wall:.2f} s wall"}
 
 
 def mode_i_leg(ctx, sc, reps: int = 5):
@@ -580,6 +604,7 @@ def main():
     if mode_i is not None:
         mode_i["step"] = ipc_step_leg()
         mode_i["step_pcg"] = ipc_step_leg(solver=1)
+        mode_i["step_64"] = ipc_step_leg(n_cubes=64, columns=16, settle=30, steps=10)
 
     batched = None
     if not args.no_batched:
@@ -595,6 +620,9 @@ def main():
                "sample": (f"first step of the same scene through the CPU oracle (serial, as the reference runs; "
                           f"the reference itself cannot be built here), literal computeSceneMinDistance over bodies "
                           f"i % {stride} == 0 scaled x{stride}; {wall:.1f} s wall")}
+        if mode_i is not None:
+            mode_i["step"]["cpu_baseline"] = ipc_step_cpu_baseline(8, 1, 30, 20)
+            mode_i["step_64"]["cpu_baseline"] = ipc_step_cpu_baseline(64, 16, 30, 10)
     launches_total = int(timed_n.sum())
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,

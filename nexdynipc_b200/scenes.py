@@ -559,22 +559,28 @@ def control_forms(seed: int = 6000, dhat: float = 1e-3, mu: float = 0.4) -> Scen
     return sb.build(_settings(dhat, mu), dt=1e-2, steps=60)
 
 
-def ipc_drop(seed: int = 7000, n_cubes: int = 2) -> Scene:
+def ipc_drop(seed: int = 7000, n_cubes: int = 2, columns: int = 1) -> Scene:
     """Full-IPC configuration: n 0.2 m cubes (8 kg) dropped, tilted and
-    jittered, onto a static 2 x 0.2 x 2 m ground box, their centres 0.2 m
-    apart from it and from each other plus 0.2 m per cube (clear of any
-    tilt); COM-distance contact forms off (enable_adaptive_barrier and
-    friction off), dt 1e-2, 80 steps.  Stepped with nxd_ipc_step."""
+    jittered, onto a static 2 x 0.2 x 2 m ground box in `columns` stacks on
+    a square grid of 0.4 m pitch centred on the origin (cube i in stack
+    i % columns, level i // columns), their centres 0.2 m above the ground
+    and 0.4 m apart per level (clear of any tilt); cubes above the first
+    level start at 1 m/s downward; COM-distance contact forms off
+    (enable_adaptive_barrier and friction off), dt 1e-2, 80 steps.  Stepped
+    with nxd_ipc_step."""
     rng = np.random.default_rng(seed)
     sb = SceneBuilder("ipc_drop")
     gv, gf = box_mesh(1.0, 0.1, 1.0)
     g = sb.add_body(gv, gf, (0.0, -0.1, 0.0))
     sb.fix(g)
     cv, cf = box_mesh(0.1, 0.1, 0.1)
+    side = int(math.ceil(math.sqrt(columns)))
     for i in range(n_cubes):
         jx, jz = rng.uniform(-0.05, 0.05, size=2)
         q = quat_from_axis_angle(rng.normal(size=3), rng.uniform(0.0, 0.4))
-        sb.add_body(cv, cf, (jx, 0.2 + 0.4 * i, jz), quat=q, vel=(0.0, -1.0 if i else 0.0, 0.0))
+        col, lvl = i % columns, i // columns
+        cx, cz = 0.4 * (col % side - 0.5 * (side - 1)), 0.4 * (col // side - 0.5 * (side - 1))
+        sb.add_body(cv, cf, (cx + jx, 0.2 + 0.4 * lvl, cz + jz), quat=q, vel=(0.0, -1.0 if lvl else 0.0, 0.0))
     s = _settings(1e-3, 0.0)
     s.enable_adaptive_barrier = 0
     s.enable_friction = 0

@@ -213,3 +213,17 @@ def test_device_identification_matches_the_oracle():
     theta, hist = diff.fit_trajectory(sc, spec, spec.get(sc), target, sc.steps, [1, 2], 10, iters=4)
     assert np.all(np.abs(theta - 1.0) < 0.01), theta
     assert hist[-1] < 1e-4 * hist[0]
+
+
+def test_oracle_double_pendulum_follows_the_reference_data():
+    # the reference's double-pendulum case with the scene file's parameters:
+    # the restated step stays within 1 mm (link 1) and 2 mm (link 2) RMS of
+    # the reference's trajectory data over the 1.5 s the file simulates
+    ref, t, target = pendulum_reference()
+    sc = scenes.double_pendulum()
+    y = diff.sampled_positions(oracle_sampler([sc], sc.steps, 10)[0], [1, 2]).reshape(-1, 2, 3)
+    e1 = diff.rmse_distance(y[:, 0], diff.reference_at(t, ref[0]))
+    e2 = diff.rmse_distance(y[:, 1], diff.reference_at(t, ref[1]))
+    assert e1 < 1e-3 and e2 < 2e-3, (e1, e2)
+    # the links swing through metres, so the match is not trivial
+    assert np.abs(target.reshape(-1, 2, 3)[:, 1] - np.array([1.5, 0.0, 0.0])).max() > 1.0
