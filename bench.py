@@ -446,8 +446,14 @@ def main():
     ap.add_argument("--no-mode-i", action="store_true")
     ap.add_argument("--no-diff", action="store_true")
     ap.add_argument("--no-pcg", action="store_true")
+    ap.add_argument("--ipc-step-only", type=int, nargs=4, metavar=("CUBES", "COLUMNS", "SETTLE", "STEPS"),
+                    help="run only the full-IPC step leg on that drop and print its JSON (for profiling)")
     args = ap.parse_args()
     ws, rank, local = dist_env()
+    if args.ipc_step_only:
+        n_cubes, columns, settle, steps = args.ipc_step_only
+        print(json.dumps(ipc_step_leg(n_cubes=n_cubes, columns=columns, settle=settle, steps=steps)), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args, ws, rank)
         return
@@ -461,15 +467,17 @@ def main():
     from nexdynipc_b200 import abi, runtime, scenes
 
     sc = scenes.hopper_chains()
-    # two contexts of the same scene: the step is deterministic, so both pass
+    # three contexts of the same scene: the step is deterministic, so all pass
     # through identical states; ctx is timed (graph replay), ctx_prof steps
-    # the same step indices with CUDA events around every launch
+    # the same step indices with CUDA events around every launch, ctx_e2e
+    # steps them again end to end through the C ABI with host buffers
     ctx = runtime.Context(sc)
     ctx_prof = runtime.Context(sc)
+    ctx_e2e = runtime.Context(sc)
     lib = runtime.lib()
     stream = torch.cuda.Stream()
-    lib.nxd_set_stream(ctx.h, C.c_void_p(stream.cuda_stream))
-    lib.nxd_set_stream(ctx_prof.h, C.c_void_p(stream.cuda_stream))
+    for c_ in (ctx, ctx_prof, ctx_e2e):
+        lib.nxd_set_stream(c_.h, C.c_void_p(stream.cuda_stream))
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")   # > 126 MB L2
     dt = sc.dt
 
@@ -482,6 +490,7 @@ def main():
         for _ in range(args.warmup):
             step()
             step(ctx_prof)
+            step(ctx_e2e)
     torch.cuda.synchronize()
     init_state = ctx.state()
 
@@ -541,22 +550,25 @@ def main():
     vin, vout = view(pinned), view(out_pinned)
     h2d = sum(v.numel() * 8 for v in pinned.values())
     d2h = sum(v.numel() * 8 for v in out_pinned.values())
-    # a host-driven loop continuing the timed trajectory: each step uploads
-    # the state the previous step read back
-    lib.nxd_get_state(ctx.h, C.byref(vin))
+    # a host-driven loop over the same step indices as the device-timed
+    # steps (ctx_e2e took the same warm-up steps): each step uploads the
+    # state the previous step read back
+    lib.nxd_get_state(ctx_e2e.h, C.byref(vin))
     if ws > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        lib.nxd_set_state(ctx.h, C.byref(vin))
-        step()
-        lib.nxd_get_state(ctx.h, C.byref(vout))
+        lib.nxd_set_state(ctx_e2e.h, C.byref(vin))
+        step(ctx_e2e)
+        lib.nxd_get_state(ctx_e2e.h, C.byref(vout))
         vin, vout = vout, vin
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s)
     e2e = ws * args.steps / e2e_s
+    e2e_equal = bool(np.array_equal(ctx.state()["position"], ctx_e2e.state()["position"]))
+    ctx_e2e.close()
 
     # --- roofline of the dominant kernel family (timed on the twin context
     # over the same step indices) and of the narrow phase
@@ -631,9 +643,11 @@ def main():
         "config": {"workload": WORKLOAD, "replicas": ws, "l2": "flushed between steps (256 MiB write, untimed)",
                    "timing": ("value: K steps, each the step's CUDA graph, CUDA events per step; per_family_ms and "
                               "roofline: the same K step indices on a twin context of the same scene with CUDA "
-                              "events around every launch; e2e: the next K steps of the trajectory, each "
-                              "nxd_set_state from pinned host memory, nxd_step, nxd_get_state back, wall clock"),
+                              "events around every launch; e2e: the same K step indices on a third context "
+                              "(same warm-up), each nxd_set_state from pinned host memory, nxd_step, "
+                              "nxd_get_state back, wall clock"),
                    "twin_state_equal": twin_equal,
+                   "e2e_state_equal": e2e_equal,
                    "per_family_ms": per_family, "last_step": {k: diag[k] for k in
                                                               ("n_body_pairs", "n_contacts", "alm_iterations",
                                                                "newton_iterations", "status")},

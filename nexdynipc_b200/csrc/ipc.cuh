@@ -552,11 +552,46 @@ __global__ void k_ipc_rowptr(const unsigned long long* hkey, const int* start, c
 
 // ---------------------------------------------------------------------------
 // Additive CCD over the candidate pairs (swept boxes): per pair the time of
-// impact along the chords of its points, then the minimum (one block).
+// impact along the chords of its points (ipc::accd_toi), one warp per pair
+// with a round's kAccdLookahead samples in its lanes, then the minimum (one
+// block).
 // ---------------------------------------------------------------------------
+static_assert(ipc::kAccdLookahead == 32, "one sample per lane");
+__device__ double accd_toi_warp(int kind, const V3* X0, const V3* P0, double t_max, double eta, int max_iter) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const double lp = ipc::accd_lipschitz(kind, P0);
+    const double d0 = sqrt(ipc::dist2(kind, X0));
+    if (!(lp > 0.0)) return t_max;
+    if (!(d0 > 0.0)) return 0.0;
+    const double g = eta * d0;
+    double t = 0.0, d = d0;
+    for (int it = 0; it < max_iter; ++it) {
+        const double dl = 0.9 * (d - g) / lp;
+        if (t + dl >= t_max) return t_max;
+        if (!(dl > 1e-12 * t_max)) return t;
+        const double thr = g + 0.9 * (d - g);
+        const double tj = t + (double)(lane + 1) * dl;
+        const bool past = tj >= t_max;
+        const double dj = past ? 0.0 : ipc::accd_distance(kind, X0, P0, tj);
+        // the round ends at the first sample past t_max or below thr
+        const unsigned stop = __ballot_sync(full, past || !(dj >= thr));
+        const int J = stop ? __ffs(stop) - 1 : 31;
+        if ((stop >> J) & 1u) {
+            if (__shfl_sync(full, past ? 1 : 0, J)) return t_max;
+        }
+        t = __shfl_sync(full, tj, J);
+        d = __shfl_sync(full, dj, J);
+    }
+    return t;
+}
+
 __global__ void k_ipc_accd(PrimGeo pg, IpcPairs P, const double* wq0, const double* wq1, double eta, int max_iter, double* toi) {
     const int n = P.n_pt + P.n_ee;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long pp = w0; pp < n; pp += nw) {
+        const int p = (int)pp;
         int vid[4], kind;
         if (p < P.n_pt) {
             kind = ipc::kPairPT;
@@ -573,7 +608,8 @@ __global__ void k_ipc_accd(PrimGeo pg, IpcPairs P, const double* wq0, const doub
             X[k] = ld3(wq0 + 3 * vid[k]);
             D[k] = ld3(wq1 + 3 * vid[k]) - X[k];
         }
-        toi[p] = ipc::accd_toi(kind, X, D, 1.0, eta, 1000, nullptr);
+        const double tp = accd_toi_warp(kind, X, D, 1.0, eta, max_iter);
+        if ((threadIdx.x & 31) == 0) toi[p] = tp;
     }
 }
 

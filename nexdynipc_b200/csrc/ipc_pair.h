@@ -350,17 +350,35 @@ NX_HD void chain12(const V12& z, const int* side, const V3* arm, double* out12) 
 
 // Additive CCD along linear point trajectories X + t P, t in [0, t_max]:
 // the relative motion of the pair (common translation removed) changes the
-// distance by at most lp per unit t, so from distance d at t the step
-// 0.9 (d - g) / lp keeps the distance above g = eta d(0).  Returns the
-// largest t reached (t_max when no approach below g happens); at most
-// max_iter advancements.  Every returned t keeps the distance >= g on [0, t].
-NX_HD double accd_toi(int kind, const V3* X0, const V3* P0, double t_max, double eta, int max_iter, int* iters) {
+// distance by at most lp per unit t, so from distance d at t every point of
+// [t, t + dl], dl = 0.9 (d - g) / lp, keeps the distance above g = eta d(0).
+// One round evaluates the distance d_j at the samples t_j = t + j dl,
+// j = 1..kAccdLookahead, and advances to the first sample with
+// d_j < g + 0.9 (d - g) (from a sample at or above that bound the next dl
+// keeps the distance above g), or to the last sample; a sample reached that
+// way at or past t_max returns t_max.  A contact that slides without
+// closing in advances kAccdLookahead steps per round instead of one.  At
+// most max_iter rounds; every returned t keeps the distance >= g on [0, t].
+// The sample loop below is sequential; the device evaluates a round's
+// samples in the lanes of one warp (accd_round_warp) with the same
+// arithmetic and the same choice.
+constexpr int kAccdLookahead = 32;
+
+NX_HD double accd_lipschitz(int kind, const V3* P0) {
     V3 P[4];
     const V3 mean = 0.25 * ((P0[0] + P0[1]) + (P0[2] + P0[3]));
     for (int k = 0; k < 4; ++k) P[k] = P0[k] - mean;
-    double lp;
-    if (kind == kPairPT) lp = norm(P[0]) + dmax(norm(P[1]), dmax(norm(P[2]), norm(P[3])));
-    else lp = dmax(norm(P[0]), norm(P[1])) + dmax(norm(P[2]), norm(P[3]));
+    if (kind == kPairPT) return norm(P[0]) + dmax(norm(P[1]), dmax(norm(P[2]), norm(P[3])));
+    return dmax(norm(P[0]), norm(P[1])) + dmax(norm(P[2]), norm(P[3]));
+}
+NX_HD double accd_distance(int kind, const V3* X0, const V3* P0, double t) {
+    V3 X[4];
+    for (int k = 0; k < 4; ++k) X[k] = X0[k] + t * P0[k];
+    return sqrt(dist2(kind, X));
+}
+
+NX_HD double accd_toi(int kind, const V3* X0, const V3* P0, double t_max, double eta, int max_iter, int* iters) {
+    const double lp = accd_lipschitz(kind, P0);
     if (iters) *iters = 0;
     const double d0 = sqrt(dist2(kind, X0));
     if (!(lp > 0.0)) return t_max;
@@ -369,13 +387,21 @@ NX_HD double accd_toi(int kind, const V3* X0, const V3* P0, double t_max, double
     double t = 0.0, d = d0;
     for (int it = 0; it < max_iter; ++it) {
         if (iters) *iters = it + 1;
-        const double tl = 0.9 * (d - g) / lp;
-        if (t + tl >= t_max) return t_max;
-        if (!(tl > 1e-12 * t_max)) return t;
-        t += tl;
-        V3 X[4];
-        for (int k = 0; k < 4; ++k) X[k] = X0[k] + t * P0[k];
-        d = sqrt(dist2(kind, X));
+        const double dl = 0.9 * (d - g) / lp;
+        if (t + dl >= t_max) return t_max;
+        if (!(dl > 1e-12 * t_max)) return t;
+        const double thr = g + 0.9 * (d - g);
+        double tn = t, dn = d;
+        for (int j = 1; j <= kAccdLookahead; ++j) {
+            const double tj = t + (double)j * dl;
+            if (tj >= t_max) return t_max;
+            const double dj = accd_distance(kind, X0, P0, tj);
+            tn = tj;
+            dn = dj;
+            if (!(dj >= thr)) break;
+        }
+        t = tn;
+        d = dn;
     }
     return t;
 }

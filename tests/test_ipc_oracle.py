@@ -164,6 +164,23 @@ def test_accd_head_on_and_separating():
     assert t == 1.0
 
 
+def test_accd_sliding_contact_advances_many_steps_per_round():
+    # a point 1e-4 above a triangle sliding 0.5 across it: the conservative
+    # step is ~1.6e-4 of the motion, about 6000 steps to t = 1; a round
+    # advances up to 32 of them, so t_max is reached within the cap, and a
+    # slow approach through the plane (at t = 0.5) stops short of g = 0.1 d0
+    X = np.array([0.25, 1e-4, 0.25, 0, 0, 0, 1, 0, 0, 0, 0, 1.0])
+    D = np.zeros(12)
+    D[0], D[2] = 0.5, 0.1
+    t, rounds = refcpu.ipc_accd(PT, X, D, 1.0, 0.1, 1000)
+    assert t == 1.0 and rounds < 200
+    D[1] = -2e-4
+    t, _ = refcpu.ipc_accd(PT, X, D, 1.0, 0.1, 1000)
+    assert 0.44 < t < 0.45
+    for tt in np.linspace(0.0, t, 201):
+        assert np.sqrt(refcpu.ipc_dist2(PT, X + tt * D)) >= 1e-5 * (1 - 1e-9)
+
+
 def brute_candidates(sc, x, inflation, ow):
     """Box tests of every (vertex, face) and (edge, edge) pair in numpy."""
     import ctypes as C
