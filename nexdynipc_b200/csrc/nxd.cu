@@ -1701,6 +1701,13 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
     NXD_CUDA(cudaMemsetAsync(&c->sc->n_contacts, 0, sizeof(int), sm));
     NXD_CUDA(cudaMemcpyAsync(c->x, c->xprev, 8 * (size_t)n6, cudaMemcpyDeviceToDevice, sm));
     const double scale = cfg.newmark ? (cfg.beta * dt) * dt : dt * dt;
+    // the rest-form kernel's CTA: a power of two from 64 to kSolverThreads
+    // covering its widest loop (6N DOFs, J joints, D drives; no contact
+    // forms here).  Its fixed-tree sums pad to powers of two with zeros, so
+    // the width changes no result, and a small scene no longer pays for
+    // 1024 threads on every call.
+    int ft = 64;
+    while (ft < kSolverThreads && ft < std::max({6 * N, c->J, c->D})) ft <<= 1;
     const long long cap_r = N + 2LL * (c->J + c->D);
     IPC_ENSURE(s->rrp, 4 * (size_t)(N + 1)); IPC_ENSURE(s->rci, 4 * (size_t)std::max(cap_r, 1LL));
     IPC_ENSURE(s->rvv, 288 * (size_t)std::max(cap_r, 1LL));
@@ -1713,7 +1720,7 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
     int* rpm = s->hrow + 2 * (N + 1);
     // rest-form value at xx into IpcScal::rest, read at the next fetch
     auto rest_value = [&](const double* xx) {
-        k_form_eval<<<1, kSolverThreads, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 0, xx, &ds->rest, nullptr, nullptr, nullptr, 0,
+        k_form_eval<<<1, ft, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 0, xx, &ds->rest, nullptr, nullptr, nullptr, 0,
                                                   nullptr);
     };
     int iters = 0, conv = 0, lsfail = 0, solvefail = 0, na = 0, pcg_total = 0;
@@ -1722,7 +1729,7 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
     for (int it = 0; it < p->newton_max_iters; ++it) {
         iters = it;
         // gradient at x: rest forms, then the barrier over the candidates at x
-        k_form_eval<<<1, kSolverThreads, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 1, x, s->gr.as<double>(), nullptr, nullptr,
+        k_form_eval<<<1, ft, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 1, x, s->gr.as<double>(), nullptr, nullptr,
                                                   nullptr, 0, nullptr);
         st = ipc_pose(c, x, nullptr, true);
         if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
@@ -1736,7 +1743,7 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
         k_absmax<<<1, 1024, 0, sm>>>(s->gt.as<double>(), n6, &ds->ginf);
         // the rest forms' Hessian blocks and both row pointers come back with
         // |g|_inf in one wait (unused when the gradient test ends the solve)
-        k_form_eval<<<1, kSolverThreads, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 2, x, nullptr, s->rrp.as<int>(), s->rci.as<int>(),
+        k_form_eval<<<1, ft, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 2, x, nullptr, s->rrp.as<int>(), s->rci.as<int>(),
                                                   s->rvv.as<double>(), cap_r, &ds->rnz);
         NXD_CUDA(cudaMemcpyAsync(rpr, s->rrp.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, sm));
         NXD_CUDA(cudaMemcpyAsync(rpb, s->rowptr.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, sm));
