@@ -180,37 +180,54 @@ NX_HD double barrier_s2(double s, double sh, double kappa) {
 
 // Cyclic Jacobi eigen-decomposition of a symmetric m x m matrix (m <= 5),
 // in place: on return A holds the eigenvalues on its diagonal and V the
-// eigenvectors (columns).  At most 16 sweeps.
+// eigenvectors (columns).  At most 16 sweeps.  Loops run to the fixed bound
+// M with m as a guard, so every index is a compile-time constant once
+// unrolled (the matrices can stay in registers); the operations and their
+// order are those of loops to m.
 template <int M>
 NX_HD void jacobi_eigen(double (&A)[M][M], double (&V)[M][M], int m) {
+NX_UNROLL
     for (int i = 0; i < M; ++i)
+NX_UNROLL
         for (int j = 0; j < M; ++j) V[i][j] = i == j ? 1.0 : 0.0;
     for (int sweep = 0; sweep < 16; ++sweep) {
         double off = 0.0, tot = 0.0;
-        for (int i = 0; i < m; ++i)
-            for (int j = 0; j < m; ++j) {
+NX_UNROLL
+        for (int i = 0; i < M; ++i)
+NX_UNROLL
+            for (int j = 0; j < M; ++j) {
+                if (i >= m || j >= m) continue;
                 tot += A[i][j] * A[i][j];
                 if (i != j) off += A[i][j] * A[i][j];
             }
         if (!(off > 1e-30 * tot)) break;
-        for (int p = 0; p < m - 1; ++p)
-            for (int q = p + 1; q < m; ++q) {
+NX_UNROLL
+        for (int p = 0; p < M - 1; ++p)
+NX_UNROLL
+            for (int q = p + 1; q < M; ++q) {
+                if (q >= m) continue;
                 const double apq = A[p][q];
                 if (apq == 0.0) continue;
                 const double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
                 const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
                 const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
-                for (int k = 0; k < m; ++k) {
+NX_UNROLL
+                for (int k = 0; k < M; ++k) {
+                    if (k >= m) continue;
                     const double akp = A[k][p], akq = A[k][q];
                     A[k][p] = c * akp - s * akq;
                     A[k][q] = s * akp + c * akq;
                 }
-                for (int k = 0; k < m; ++k) {
+NX_UNROLL
+                for (int k = 0; k < M; ++k) {
+                    if (k >= m) continue;
                     const double apk = A[p][k], aqk = A[q][k];
                     A[p][k] = c * apk - s * aqk;
                     A[q][k] = s * apk + c * aqk;
                 }
-                for (int k = 0; k < m; ++k) {
+NX_UNROLL
+                for (int k = 0; k < M; ++k) {
+                    if (k >= m) continue;
                     const double vkp = V[k][p], vkq = V[k][q];
                     V[k][p] = c * vkp - s * vkq;
                     V[k][q] = s * vkp + c * vkq;
@@ -282,50 +299,82 @@ NX_HD PairEval pair_barrier(const DistForm& f, const V3* X, double dhat, double 
     // orthonormal basis: w (x) e_a / |w| (a = x, y, z), then the c_j (x) r
     // directions orthogonalised against it (twice, modified Gram-Schmidt)
     const double wn = sqrt((f.w[0] * f.w[0] + f.w[1] * f.w[1]) + (f.w[2] * f.w[2] + f.w[3] * f.w[3]));
+    // (loops below run to fixed bounds with the runtime sizes as guards, so
+    // that every array index is a compile-time constant once unrolled; the
+    // operations and their order are those of loops to m and nu)
     V12 B[5];
-    int m = 0;
     const V3 ex = v3(1, 0, 0), ey = v3(0, 1, 0), ez = v3(0, 0, 1);
-    B[m++] = outer_wv(f.w, (1.0 / wn) * ex);
-    B[m++] = outer_wv(f.w, (1.0 / wn) * ey);
-    B[m++] = outer_wv(f.w, (1.0 / wn) * ez);
-    for (int j = 0; j < f.nu; ++j) {
+    B[0] = outer_wv(f.w, (1.0 / wn) * ex);
+    B[1] = outer_wv(f.w, (1.0 / wn) * ey);
+    B[2] = outer_wv(f.w, (1.0 / wn) * ez);
+    int m = 3;
+NX_UNROLL
+    for (int j = 0; j < 2; ++j) {
+        if (j >= f.nu) continue;
         const double cj[4] = {f.c[0][j], f.c[1][j], f.c[2][j], f.c[3][j]};
         V12 v = outer_wv(cj, r);
         const double n0 = sqrt(dot12(v, v));
+NX_UNROLL
         for (int pass = 0; pass < 2; ++pass)
-            for (int k = 0; k < m; ++k) axpy12(-dot12(B[k], v), B[k], v);
+NX_UNROLL
+            for (int k = 0; k < 4; ++k)
+                if (k < m) axpy12(-dot12(B[k], v), B[k], v);
         const double n1 = sqrt(dot12(v, v));
-        if (n1 > 1e-9 * n0 && n1 > 0.0) B[m++] = scale12(1.0 / n1, v);
+        if (n1 > 1e-9 * n0 && n1 > 0.0) {
+            const V12 u = scale12(1.0 / n1, v);
+            if (m == 3) B[3] = u;
+            else B[4] = u;
+            ++m;
+        }
     }
     // coordinates of grad d^2 and G_j in the basis; the basis image of
     // 2 (w w^T) (x) I3 is 2 |w|^2 on the first three coordinates
     double gam[5], Gam[2][5];
-    for (int k = 0; k < m; ++k) {
+NX_UNROLL
+    for (int k = 0; k < 5; ++k) {
+        if (k >= m) continue;
         gam[k] = dot12(B[k], gs);
-        for (int j = 0; j < f.nu; ++j) Gam[j][k] = dot12(B[k], G[j]);
+NX_UNROLL
+        for (int j = 0; j < 2; ++j)
+            if (j < f.nu) Gam[j][k] = dot12(B[k], G[j]);
     }
     double S[5][5], V[5][5];
+NX_UNROLL
     for (int i = 0; i < 5; ++i)
+NX_UNROLL
         for (int j = 0; j < 5; ++j) S[i][j] = 0.0;
-    for (int i = 0; i < m; ++i)
-        for (int j = 0; j < m; ++j) {
+NX_UNROLL
+    for (int i = 0; i < 5; ++i)
+NX_UNROLL
+        for (int j = 0; j < 5; ++j) {
+            if (i >= m || j >= m) continue;
             double hs = (i == j && i < 3) ? 2.0 * wn * wn : 0.0;
-            for (int p = 0; p < f.nu; ++p)
-                for (int q = 0; q < f.nu; ++q) hs -= Gam[p][i] * Minv[p][q] * Gam[q][j];
+NX_UNROLL
+            for (int p = 0; p < 2; ++p)
+NX_UNROLL
+                for (int q = 0; q < 2; ++q)
+                    if (p < f.nu && q < f.nu) hs -= Gam[p][i] * Minv[p][q] * Gam[q][j];
             S[i][j] = b2 * gam[i] * gam[j] + b1 * hs;
         }
-    for (int i = 0; i < m; ++i)
+NX_UNROLL
+    for (int i = 0; i < 5; ++i)
+NX_UNROLL
         for (int j = 0; j < i; ++j) {   // exact symmetry before the rotations
+            if (i >= m) continue;
             const double avg = 0.5 * (S[i][j] + S[j][i]);
             S[i][j] = avg; S[j][i] = avg;
         }
     jacobi_eigen<5>(S, V, m);
     int n = 0;
-    for (int k = 0; k < m; ++k) {
+NX_UNROLL
+    for (int k = 0; k < 5; ++k) {
+        if (k >= m) continue;
         const double lam = S[k][k];
         if (!(lam > 0.0)) continue;
         V12 y = scale12(V[0][k], B[0]);
-        for (int i = 1; i < m; ++i) axpy12(V[i][k], B[i], y);
+NX_UNROLL
+        for (int i = 1; i < 5; ++i)
+            if (i < m) axpy12(V[i][k], B[i], y);
         o.lam[n] = lam;
         o.y[n] = y;
         ++n;

@@ -19,8 +19,10 @@
 
 #ifdef __CUDACC__
 #define NX_HD __host__ __device__ __forceinline__
+#define NX_UNROLL _Pragma("unroll")
 #else
 #define NX_HD inline
+#define NX_UNROLL
 #endif
 
 namespace nx {
