@@ -1260,6 +1260,7 @@ struct IpcState {
     int* hrow = nullptr;         // pinned, 3 (N + 1) row pointers
     IpcScal* ds() const { return scal.as<IpcScal>(); }
     int n_pt = 0, n_ee = 0;
+    bool cand_swept = false;     // the last ipc_candidates_begin built swept boxes
     GrowBuf e, grad12, lam, z, nterm, body, active, type, apos, alist;
     GrowBuf gkey, gval, gkey1, gval1, hkey, hval, hkey1, hval1;
     GrowBuf sflag, spos, sstart, gout, rowptr, colidx, vals, toi;
@@ -1425,7 +1426,19 @@ nxd_status ipc_build_bvh(nxd_ctx* c, Bvh& B, int kind, bool swept, double infl) 
 // sort each kind's pairs by (query, primitive) with one radix sort.  Both
 // kinds are counted before the one host wait that reads their totals.
 constexpr long long kSweepAllTests = 1LL << 22;
+// ipc_candidates = ipc_candidates_begin (boxes, trees, counts and their
+// scans, all queued) + one ipc_fetch + ipc_candidates_end (the writes); a
+// caller may fold other read-backs into that fetch.
+nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase);
+nxd_status ipc_candidates_begin(nxd_ctx* c, bool swept, double infl) { return ipc_candidates_pass(c, swept, infl, 0); }
+nxd_status ipc_candidates_end(nxd_ctx* c) { return ipc_candidates_pass(c, c->ipc->cand_swept, 0.0, 1); }
 nxd_status ipc_candidates(nxd_ctx* c, bool swept, double infl) {
+    nxd_status st = ipc_candidates_begin(c, swept, infl);
+    if (st == NXD_OK) st = ipc_fetch(c);
+    if (st == NXD_OK) st = ipc_candidates_end(c);
+    return st;
+}
+nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
     IpcState* s = c->ipc;
     IpcScal* ds = s->ds();
     const double* w1 = swept ? s->wq1.as<double>() : nullptr;
@@ -1435,6 +1448,47 @@ nxd_status ipc_candidates(nxd_ctx* c, bool swept, double infl) {
     GrowBuf* off[2] = {&s->off, &s->off2};
     GrowBuf* out[2] = {&s->pt, &s->ee};
     Bvh* tree[2] = {&s->faces, &s->edges};
+    auto launch = [&](int k, bool count) {
+        Bvh& B = *tree[k];
+        const double* qbox[2] = {s->qv.as<double>(), s->qe.as<double>()};   // read at launch: the buffers may grow
+        int* cn = count ? cnt[k]->as<int>() : nullptr;
+        const int* of = count ? nullptr : off[k]->as<int>();
+        int* dst = count ? nullptr : out[k]->as<int>();
+        if (sweep)
+            k_sweep_all<<<grid_for(32LL * nq[k], 128), 128, 0, c->stream>>>(s->pg, k, qbox[k], nq[k], B.leaf.as<double>(), B.n,
+                                                                            cn, of, dst);
+        else
+            k_traverse<<<grid_for(nq[k], 128), 128, 0, c->stream>>>(s->pg, k, qbox[k], nq[k], B.nbox.as<double>(),
+                                                                    B.child.as<int>(), B.i0.as<int>(), B.n, cn, of, dst,
+                                                                    &ds->status);
+    };
+    if (phase == 1) {
+        // after the fetch: the totals in pinned memory, then the writes
+        nxd_status st = NXD_OK;
+        if (s->hp->sc.status != 0) return (nxd_status)s->hp->sc.status;
+        s->n_pt = s->hp->sc.tot[0];
+        s->n_ee = s->hp->sc.tot[1];
+        for (int k = 0; k < 2; ++k) {
+            const int m = s->hp->sc.tot[k];
+            IPC_ENSURE(*out[k], 8 * (size_t)std::max(m, 1));
+            if (m == 0) continue;
+            launch(k, false);
+            if (sweep || m < 2) continue;
+            // traversal order -> (query, primitive) ascending
+            const int pbits = bits_for((unsigned long long)std::max(np[k], 1));
+            const int qbits = bits_for((unsigned long long)std::max(nq[k], 1));
+            IPC_ENSURE(s->tkey, 8 * (size_t)m); IPC_ENSURE(s->tval, 4 * (size_t)m);
+            k_pair_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(out[k]->as<int>(), m, pbits, s->tkey.as<unsigned long long>(),
+                                                                 s->tval.as<int>());
+            st = radix_sort(c, s->tkey, s->tval, s->tkey1, s->tval1, m, 0, pbits + qbits);
+            if (st != NXD_OK) return st;
+            k_pair_from_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(s->tkey.as<unsigned long long>(), m, pbits,
+                                                                      out[k]->as<int>());
+        }
+        NXD_CUDA(cudaGetLastError());
+        return NXD_OK;
+    }
+    s->cand_swept = swept;
     if (sweep) {
         for (int k = 0; k < 2; ++k) {
             tree[k]->n = np[k];
@@ -1452,47 +1506,12 @@ nxd_status ipc_candidates(nxd_ctx* c, bool swept, double infl) {
     IPC_ENSURE(s->qv, 48 * (size_t)std::max(c->nv, 1)); IPC_ENSURE(s->qe, 48 * (size_t)std::max(c->ne, 1));
     if (c->nv) k_ipc_boxes<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(s->pg, 2, s->wq0.as<double>(), w1, 0.0, s->qv.as<double>());
     if (c->ne) k_ipc_boxes<<<grid_for(c->ne, 256), 256, 0, c->stream>>>(s->pg, 3, s->wq0.as<double>(), w1, 0.0, s->qe.as<double>());
-    const double* qbox[2] = {s->qv.as<double>(), s->qe.as<double>()};
     NXD_CUDA(cudaMemsetAsync(ds, 0, 4 * sizeof(int), c->stream));   // totals, status, segment count
-    auto launch = [&](int k, bool count) {
-        Bvh& B = *tree[k];
-        int* cn = count ? cnt[k]->as<int>() : nullptr;
-        const int* of = count ? nullptr : off[k]->as<int>();
-        int* dst = count ? nullptr : out[k]->as<int>();
-        if (sweep)
-            k_sweep_all<<<grid_for(32LL * nq[k], 128), 128, 0, c->stream>>>(s->pg, k, qbox[k], nq[k], B.leaf.as<double>(), B.n,
-                                                                            cn, of, dst);
-        else
-            k_traverse<<<grid_for(nq[k], 128), 128, 0, c->stream>>>(s->pg, k, qbox[k], nq[k], B.nbox.as<double>(),
-                                                                    B.child.as<int>(), B.i0.as<int>(), B.n, cn, of, dst,
-                                                                    &ds->status);
-    };
     for (int k = 0; k < 2; ++k) {
         if (nq[k] == 0 || np[k] == 0) continue;
         IPC_ENSURE(*cnt[k], 4 * (size_t)nq[k]); IPC_ENSURE(*off[k], 4 * (size_t)nq[k]);
         launch(k, true);
         k_scan<<<1, 1024, 0, c->stream>>>(cnt[k]->as<int>(), off[k]->as<int>(), nq[k], &ds->tot[k], nullptr, nullptr, nullptr);
-    }
-    nxd_status st = ipc_fetch(c);
-    if (st != NXD_OK) return st;
-    if (s->hp->sc.status != 0) return (nxd_status)s->hp->sc.status;
-    s->n_pt = s->hp->sc.tot[0];
-    s->n_ee = s->hp->sc.tot[1];
-    for (int k = 0; k < 2; ++k) {
-        const int m = s->hp->sc.tot[k];
-        IPC_ENSURE(*out[k], 8 * (size_t)std::max(m, 1));
-        if (m == 0) continue;
-        launch(k, false);
-        if (sweep || m < 2) continue;
-        // traversal order -> (query, primitive) ascending
-        const int pbits = bits_for((unsigned long long)std::max(np[k], 1));
-        const int qbits = bits_for((unsigned long long)std::max(nq[k], 1));
-        IPC_ENSURE(s->tkey, 8 * (size_t)m); IPC_ENSURE(s->tval, 4 * (size_t)m);
-        k_pair_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(out[k]->as<int>(), m, pbits, s->tkey.as<unsigned long long>(),
-                                                             s->tval.as<int>());
-        st = radix_sort(c, s->tkey, s->tval, s->tkey1, s->tval1, m, 0, pbits + qbits);
-        if (st != NXD_OK) return st;
-        k_pair_from_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(s->tkey.as<unsigned long long>(), m, pbits, out[k]->as<int>());
     }
     NXD_CUDA(cudaGetLastError());
     return NXD_OK;
@@ -1726,13 +1745,20 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
     int iters = 0, conv = 0, lsfail = 0, solvefail = 0, na = 0, pcg_total = 0;
     double amax = 1.0, fx = 0.0;
     int64_t npairs = 0;
+    bool cand_at_x = false;   // the last poses and dhat-inflated candidates were built at x
     for (int it = 0; it < p->newton_max_iters; ++it) {
         iters = it;
         // gradient at x: rest forms, then the barrier over the candidates at x
         k_form_eval<<<1, ft, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 1, x, s->gr.as<double>(), nullptr, nullptr,
                                                   nullptr, 0, nullptr);
-        st = ipc_pose(c, x, nullptr, true);
-        if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
+        // after an accepted trial the poses and candidates at x = xt (boxes
+        // inflated by dhat) are the trial's, still in place
+        st = NXD_OK;
+        if (!cand_at_x) {
+            st = ipc_pose(c, x, nullptr, true);
+            if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
+        }
+        cand_at_x = false;
         if (st == NXD_OK) st = ipc_barrier_eval(c, p->dhat, p->kappa, true, nullptr);
         if (st != NXD_OK) return st;
         const double eb = hs.energy;
@@ -1787,15 +1813,19 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
         }
         double* dx = c->S.dx;
         k_absmax<<<1, 1024, 0, sm>>>(dx, n6, &ds->dxinf);
-        if ((st = ipc_fetch(c)) != NXD_OK) return st;
+        // the swept candidates of the step bound are counted before the wait
+        // that reads the solve's flags (discarded when those end the loop)
+        st = ipc_pose(c, x, dx, true);
+        if (st == NXD_OK) st = ipc_candidates_begin(c, true, 0.0);
+        if (st == NXD_OK) st = ipc_fetch(c);
+        if (st != NXD_OK) return st;
         if (s->hp->capst) return NXD_CAPACITY;
         if (s->hp->fail) { solvefail = 1; break; }
         // the velocity criterion of IPC: a Newton step below tol * dt ends it
         if (hs.dxinf < p->newton_tol * dt) { conv = 1; break; }
         // the step bound (additive CCD over the swept candidates), the value
         // at x and the descent g . dx, read back in one wait
-        st = ipc_pose(c, x, dx, true);
-        if (st == NXD_OK) st = ipc_candidates(c, true, 0.0);
+        st = ipc_candidates_end(c);
         if (st == NXD_OK) st = ipc_accd(c, p->eta);
         if (st != NXD_OK) return st;
         rest_value(x);
@@ -1822,6 +1852,7 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
             alpha *= c->s.ls_rho;
         }
         if (!done) { lsfail = 1; break; }
+        cand_at_x = true;
         NXD_CUDA(cudaMemcpyAsync(x, s->xt.p, 8 * (size_t)n6, cudaMemcpyDeviceToDevice, sm));
         if (it == p->newton_max_iters - 1) iters = p->newton_max_iters;
     }
