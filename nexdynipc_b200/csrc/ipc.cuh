@@ -311,7 +311,7 @@ __device__ __forceinline__ bool boxes_overlap(const double* a, const double* b) 
 // come out sorted.  The same tests and filters as k_traverse.  mode 0
 // counts into cnt, mode 1 writes at off.
 __global__ void k_sweep_all(PrimGeo pg, int kind, const double* qbox, int nq, const double* leaf, int nprim, int* cnt,
-                            const int* off, int* out) {
+                            const int* off, int* out, long long cap = 0x7fffffffffffffffLL) {
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -333,7 +333,7 @@ __global__ void k_sweep_all(PrimGeo pg, int kind, const double* qbox, int nq, co
             const unsigned m = __ballot_sync(0xffffffffu, hit);
             if (hit && dst) {
                 const int at = c + __popc(m & below);
-                dst[2 * at] = q; dst[2 * at + 1] = prim;
+                if (off[q] + (long long)at < cap) { dst[2 * at] = q; dst[2 * at + 1] = prim; }   // writes stop at cap pairs
             }
             c += __popc(m);
         }
@@ -452,6 +452,25 @@ __global__ void k_ipc_pair_eval(PrimGeo pg, IpcPairs P, IpcPose ps, double dhat,
 // barrier value as k_ipc_pair_eval's e, without the PSD projection.
 __global__ void k_ipc_pair_energy(PrimGeo pg, IpcPairs P, IpcPose ps, double dhat, double kappa, double* e) {
     const int n = P.n_pt + P.n_ee;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        int kind, side[4], bA, bB;
+        V3 X[4], arm[4];
+        pair_points(pg, P, ps, p, kind, X, side, arm, bA, bB);
+        const ipc::DistForm f = ipc::classify(kind, X);
+        const V3 r = ipc::form_r(f, X);
+        e[p] = ipc::barrier_s(dot(r, r), dhat * dhat, kappa);
+    }
+}
+
+// k_ipc_pair_energy with the pair counts read on the device (tot[0] point-
+// triangle, tot[1] edge-edge); lists over their capacities (cap_pt, cap_ee
+// pairs) are left alone, the caller sees the totals and evaluates again.
+__global__ void k_ipc_pair_energy_dev(PrimGeo pg, const int* pt, const int* ee, const int* tot, int cap_pt, int cap_ee,
+                                      IpcPose ps, double dhat, double kappa, double* e) {
+    const int npt = tot[0], nee = tot[1];
+    if (npt > cap_pt || nee > cap_ee) return;
+    const IpcPairs P{pt, npt, ee, nee};
+    const int n = npt + nee;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         int kind, side[4], bA, bB;
         V3 X[4], arm[4];
@@ -641,6 +660,18 @@ __global__ void k_absmax(const double* v, int n, double* out) {
         for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r = fold(r, sm[k]);
         *out = r;
     }
+}
+
+// k_tree_sum of the n = tot[0] + tot[1] pair energies (nothing when the
+// lists overflowed their capacities, see k_ipc_pair_energy_dev).
+__global__ void __launch_bounds__(1024) k_tree_sum_pairs(const double* v, const int* tot, int cap_pt, int cap_ee, double* out) {
+    __shared__ double sh[2 * kRedMaxQ * 32];
+    if (tot[0] > cap_pt || tot[1] > cap_ee) return;
+    BlockRed R;
+    R.sh = sh;
+    R.parity = 0;
+    const double s = R.sum(tot[0] + tot[1], [&](int e) { return v[e]; });
+    if (threadIdx.x == 0) *out = s;
 }
 
 // Fixed-tree sum of n doubles (the padded pairwise tree), one block.

@@ -1488,6 +1488,19 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
         NXD_CUDA(cudaGetLastError());
         return NXD_OK;
     }
+    if (phase == 2) {
+        // all-pairs sweep only: the writes into the lists' current
+        // capacities, the totals still on the device (ipc_trial_energy)
+        for (int k = 0; k < 2; ++k) {
+            if (nq[k] == 0 || np[k] == 0) continue;
+            const double* qb = k == 0 ? s->qv.as<double>() : s->qe.as<double>();
+            k_sweep_all<<<grid_for(32LL * nq[k], 128), 128, 0, c->stream>>>(s->pg, k, qb, nq[k], tree[k]->leaf.as<double>(),
+                                                                            tree[k]->n, nullptr, off[k]->as<int>(),
+                                                                            out[k]->as<int>(), (long long)(out[k]->cap / 8));
+        }
+        NXD_CUDA(cudaGetLastError());
+        return NXD_OK;
+    }
     s->cand_swept = swept;
     if (sweep) {
         for (int k = 0; k < 2; ++k) {
@@ -1627,6 +1640,44 @@ nxd_status ipc_barrier_eval(nxd_ctx* c, double dhat, double kappa, bool full, in
         if ((st = ipc_fetch(c)) != NXD_OK) return st;
         *nh_out = s->hp->sc.nseg;
     }
+    return NXD_OK;
+}
+
+// One line-search trial's barrier energy at xt (device) with a single host
+// wait, for scenes on the all-pairs sweep: candidates counted and written
+// into the lists' current capacities (room for twice the last counts), the
+// energy summed over the device-side counts, then one fetch.  *ok is false
+// when the sweep does not apply or a list overflowed: the caller then runs
+// ipc_pose + ipc_candidates + ipc_barrier_eval.  The lists, their order and
+// the sums are that path's.
+nxd_status ipc_trial_energy(nxd_ctx* c, const double* xt, double dhat, double kappa, bool* ok) {
+    IpcState* s = c->ipc;
+    *ok = false;
+    if ((long long)c->nv * c->nf + (long long)c->ne * c->ne > kSweepAllTests) return NXD_OK;
+    // capacities grow geometrically, so that a count creeping upwards does
+    // not reallocate (and synchronise) on every trial
+    auto room = [](GrowBuf& b, size_t want) { return want <= b.cap || b.ensure(std::max(want, 2 * b.cap)); };
+    if (!room(s->pt, 16 * (size_t)std::max(s->n_pt, 16)) || !room(s->ee, 16 * (size_t)std::max(s->n_ee, 16)))
+        return NXD_CUDA_ERROR;
+    const int cap_pt = (int)std::min<size_t>(s->pt.cap / 8, (size_t)1 << 30);
+    const int cap_ee = (int)std::min<size_t>(s->ee.cap / 8, (size_t)1 << 30);
+    if (!room(s->e, 8 * ((size_t)cap_pt + (size_t)cap_ee))) return NXD_CUDA_ERROR;
+    nxd_status st = ipc_pose(c, xt, nullptr, true);
+    if (st == NXD_OK) st = ipc_candidates_begin(c, false, dhat);
+    if (st == NXD_OK) st = ipc_candidates_pass(c, false, dhat, 2);
+    if (st != NXD_OK) return st;
+    IpcScal* ds = s->ds();
+    const IpcPose ps{s->wq0.as<double>(), s->pp0.as<double>()};
+    k_ipc_pair_energy_dev<<<grid_for((long long)cap_pt + cap_ee, 128), 128, 0, c->stream>>>(
+        s->pg, s->pt.as<int>(), s->ee.as<int>(), ds->tot, cap_pt, cap_ee, ps, dhat, kappa, s->e.as<double>());
+    k_tree_sum_pairs<<<1, 1024, 0, c->stream>>>(s->e.as<double>(), ds->tot, cap_pt, cap_ee, &ds->energy);
+    if ((st = ipc_fetch(c)) != NXD_OK) return st;
+    const IpcScal& hs = s->hp->sc;
+    if (hs.status != 0) return (nxd_status)hs.status;
+    if (hs.tot[0] > cap_pt || hs.tot[1] > cap_ee) return NXD_OK;
+    s->n_pt = hs.tot[0];
+    s->n_ee = hs.tot[1];
+    *ok = true;
     return NXD_OK;
 }
 
@@ -1842,10 +1893,14 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
         for (int ls = 0; ls < p->ls_max_iters; ++ls) {
             k_axpy_alpha<<<grid_for(n6, 256), 256, 0, sm>>>(x, dx, alpha, n6, s->xt.as<double>());
             rest_value(s->xt.as<double>());
-            st = ipc_pose(c, s->xt.as<double>(), nullptr, true);
-            if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
-            if (st == NXD_OK) st = ipc_barrier_eval(c, p->dhat, p->kappa, false, nullptr);
-            if (st == NXD_OK) st = ipc_fetch(c);
+            bool one_wait = false;
+            st = ipc_trial_energy(c, s->xt.as<double>(), p->dhat, p->kappa, &one_wait);
+            if (st == NXD_OK && !one_wait) {
+                st = ipc_pose(c, s->xt.as<double>(), nullptr, true);
+                if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
+                if (st == NXD_OK) st = ipc_barrier_eval(c, p->dhat, p->kappa, false, nullptr);
+                if (st == NXD_OK) st = ipc_fetch(c);
+            }
             if (st != NXD_OK) return st;
             const double fn = hs.rest + scale * hs.energy;
             if (fn <= fx + c->s.ls_c1 * alpha * descent) { done = true; fx = fn; break; }
