@@ -107,7 +107,9 @@ def test_fit_recovers_initial_velocity():
 import os
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "double_pendulum")
-REF_SCENE = "/root/reference/assets/double_pendulum/double_pendulum.json"
+# the reference's scene file (assets/double_pendulum/double_pendulum.json),
+# copied by make_double_pendulum_reference.py
+REF_SCENE = os.path.join(GOLDEN, "double_pendulum.json")
 
 
 def oracle_sampler(worlds, steps, every):
@@ -131,7 +133,6 @@ def pendulum_reference(every=10):
     return ref, t, np.stack([diff.reference_at(t, r) for r in ref], axis=1).reshape(-1)
 
 
-@pytest.mark.skipif(not os.path.exists(REF_SCENE), reason="reference checkout not present")
 def test_double_pendulum_builder_is_the_reference_scene():
     import dataclasses
     from nexdynipc_b200 import sceneio
