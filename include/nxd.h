@@ -466,9 +466,13 @@ nxd_status nxd_ipc_step(nxd_ctx* ctx, double dt, const nxd_ipc_params* p, nxd_ip
  * themselves (a host engine's memory pool, a hard memory cap, a real-time
  * loop that forbids allocator calls) pass device buffers they own:
  * position [n*3], orientation [n*4] (w,x,y,z), local_box [n*6] (local AABB
- * min xyz, max xyz, i.e. MeshShape::computeAABB) and pairs [cap*2].  The
+ * min xyz, max xyz, i.e. MeshShape::computeAABB) and pairs [cap*2].  A body
+ * without a mesh (no vertices or no faces) takes part in no pair, as in
+ * nxd_body_pairs: pass its local box empty, min > max on some axis (e.g.
+ * min = (1,1,1), max = (-1,-1,-1)); a NaN bound counts as empty too.  The
  * result equals nxd_body_pairs on the same poses (reference order); *count
- * (host) gets the pair count, NXD_CAPACITY if it exceeds cap.
+ * (host) gets the pair count, NXD_CAPACITY if it exceeds cap (the first cap
+ * pairs are written, nothing past pairs[2*cap)).
  * The call allocates nothing: its scratch (world boxes, per-body counts and
  * offsets, about 0.9 MB) is a fixed array in the library that every GPU which
  * loads it holds until exit, so n is limited to NXD_NOALLOC_MAX_BODIES
@@ -476,7 +480,9 @@ nxd_status nxd_ipc_step(nxd_ctx* ctx, double dt, const nxd_ipc_params* p, nxd_ip
  * that array's device address; make it before any stream capture.  All calls
  * share the one array: calls that overlap on the GPU (different streams)
  * race.  The call synchronises `stream` (a cudaStream_t, may be NULL) before
- * returning the count. */
+ * returning the count.  The looked-up address is kept for the life of the
+ * process: a cudaDeviceReset (or any teardown of the device's primary
+ * context) after the first call is not supported. */
 #define NXD_NOALLOC_MAX_BODIES 16384
 nxd_status nxd_body_pairs_noalloc(const double* position, const double* orientation, const double* local_box,
                                   int32_t n, double inflation_radius, int32_t* pairs, int64_t cap,

@@ -8,7 +8,8 @@
 // loads the library keeps until the process exits.
 //
 // Result: the same pairs, in the same order, as nxd_body_pairs (the
-// reference's ContactAssembler::detectBodyPairs on the current poses).
+// reference's ContactAssembler::detectBodyPairs on the current poses), given
+// each body's local box -- an empty one (min > max) for a body without a mesh.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -71,10 +72,19 @@ nxd_status scratch_for_current_device(Scratch* out) {
     return NXD_OK;
 }
 
+// A local box with min > max on some axis (or a NaN) marks a body without a
+// mesh: nxd_body_pairs leaves such bodies out of every pair, so its world box
+// is stored as NaNs, which fail every overlap test at any inflation.
 __global__ void k_na_boxes(const double* pos, const double* quat, const double* lbox, int n, double* boxes) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const Box b = transform_local_box(ld3(lbox + 6 * i), ld3(lbox + 6 * i + 3), ld3(pos + 3 * i), ldq(quat + 4 * i));
+    const V3 lo = ld3(lbox + 6 * i), hi = ld3(lbox + 6 * i + 3);
+    if (!(lo.x <= hi.x && lo.y <= hi.y && lo.z <= hi.z)) {
+        const double q = __longlong_as_double(0x7ff8000000000000LL);
+        for (int k = 0; k < 6; ++k) boxes[6 * i + k] = q;
+        return;
+    }
+    const Box b = transform_local_box(lo, hi, ld3(pos + 3 * i), ldq(quat + 4 * i));
     st3(boxes + 6 * i, b.mn);
     st3(boxes + 6 * i + 3, b.mx);
 }
