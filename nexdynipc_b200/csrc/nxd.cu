@@ -105,6 +105,8 @@ struct nxd_ctx {
     ContactRec *contacts, *contacts_tmp;
     double* sort_key;
     int* sort_idx;
+    int *sort_g, *sort_l;       // G / L position lists of the contact sort's partitions
+    SortRange* sort_small;      // ranges the contact sort finishes one warp each
     double* nforce;
     Scalars* sc;
     int* i_scratch;   // small int scalars for scans
@@ -321,7 +323,8 @@ void launch_narrow_full(nxd_ctx* c, const double* wv, const double* pose_p, cons
                                                                       nullptr, skip_vv);
     NXD_K(c, NXD_PROF_NARROW, narrow_emit, (emit_blocks), (32 * kEmitWarps), (0), in, 1, ns, nullptr, c->contacts, skip_vv);
     NXD_K(c, NXD_PROF_OTHER, contact_totals, (1), (1), (0), c->sc, 1, skip_if, nullptr);
-    NXD_K(c, NXD_PROF_OTHER, sort_contacts, (1), (1024), (0), c->sc, c->contacts, c->contacts_tmp, c->sort_key, c->sort_idx, skip_if);
+    NXD_K(c, NXD_PROF_OTHER, sort_contacts, (1), (1024), (sort_smem_bytes(32)), c->sc, c->contacts, c->contacts_tmp, c->sort_key,
+          c->sort_idx, c->sort_g, c->sort_l, c->sort_small, skip_if);
 }
 
 }  // namespace
@@ -639,7 +642,9 @@ nxd_status nxd_create(const nxd_scene_desc* d, nxd_ctx** out) {
     c->hmask = m.alloc<unsigned>((size_t)c->pair_cap * kMaskWords);
     c->contacts = m.alloc<ContactRec>(kMaxRawContacts);
     c->contacts_tmp = m.alloc<ContactRec>(kMaxContacts);
-    c->sort_key = m.alloc<double>(65536); c->sort_idx = m.alloc<int>(65536);
+    c->sort_key = m.alloc<double>(kMaxRawContacts); c->sort_idx = m.alloc<int>(kMaxRawContacts);
+    c->sort_g = m.alloc<int>(kMaxRawContacts + 1); c->sort_l = m.alloc<int>(kMaxRawContacts + 1);
+    c->sort_small = m.alloc<SortRange>(kMaxContacts + kSortWarpRange + 64);
     c->nforce = m.alloc<double>(kMaxRawContacts);
     c->sc = m.alloc<Scalars>(1);
     c->i_scratch = m.alloc<int>(16);
@@ -652,6 +657,7 @@ nxd_status nxd_create(const nxd_scene_desc* d, nxd_ctx** out) {
     fill_solver(c);
     // top-k kernel needs opt-in shared memory above 48 KB
     cudaFuncSetAttribute(k_topk, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(k_sort_contacts, cudaFuncAttributeMaxDynamicSharedMemorySize, sort_smem_bytes(32));
     if (!m.ok || cudaDeviceSynchronize() != cudaSuccess) {
         m.release();
         delete c;

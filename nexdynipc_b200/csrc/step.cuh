@@ -188,40 +188,35 @@ __device__ __forceinline__ void contact_totals_body(Scalars* sc, int stage, cons
 constexpr int kLB_contact_totals = 0;
 __global__ void k_contact_totals(Scalars* sc, int stage, const int* skip_if, int* skip_vv) { contact_totals_body(sc, stage, skip_if, skip_vv); }
 
-// std::sort by distance + truncation to 2000 (IPCSolver.cpp:571-577): a
-// bitonic sort on (distance, original position); equal distances keep their
-// detection order.  One CTA; runs only when more than 2000 contacts exist.
-__device__ __forceinline__ void sort_contacts_body(Scalars* sc, ContactRec* c, ContactRec* tmp, double* key, int* idx, const int* skip_if) {
+// std::sort by distance + truncation to 2000 (IPCSolver.cpp:571-577).  The
+// sort is libstdc++'s introsort, which is not stable: equal distances (common:
+// hinged links overlap at their hinges, distance 0) come out in the order its
+// partitions leave them, which decides both the contact order the forms sum
+// in and which ties survive the cut.  sel_sort_prefix_block reproduces that
+// permutation over the first 2000 positions.  One CTA of 1024 threads with
+// sort_smem_bytes(32) of dynamic shared memory; runs only when more than 2000
+// contacts exist.
+__device__ __forceinline__ void sort_contacts_body(Scalars* sc, ContactRec* c, ContactRec* tmp, double* key, int* idx,
+                                                   int* gscr, int* lscr, SortRange* small, const int* skip_if) {
     if (skip_if && *skip_if != 0) return;
     const int raw = sc->n_contacts_raw;
     if (raw <= kMaxContacts) return;
-    const int P = pow2_ceil(raw);
-    for (int i = threadIdx.x; i < P; i += blockDim.x) {
-        key[i] = i < raw ? c[i].distance : INFINITY;
+    for (int i = threadIdx.x; i < raw; i += blockDim.x) {
+        key[i] = c[i].distance;
         idx[i] = i;
     }
     __syncthreads();
-    for (int k = 2; k <= P; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < P; i += blockDim.x) {
-                const int l = i ^ j;
-                if (l > i) {
-                    const bool up = (i & k) == 0;
-                    const double ki = key[i], kl = key[l];
-                    const int ii = idx[i], il = idx[l];
-                    const bool gt = (ki > kl) || (ki == kl && ii > il);
-                    if (gt == up) { key[i] = kl; key[l] = ki; idx[i] = il; idx[l] = ii; }
-                }
-            }
-            __syncthreads();
-        }
-    }
+    extern __shared__ __align__(16) unsigned char sort_slab[];
+    sel_sort_prefix_block(SelView{idx, key, gscr, lscr}, raw, kMaxContacts, small, sort_slab);
     for (int i = threadIdx.x; i < kMaxContacts; i += blockDim.x) tmp[i] = c[idx[i]];
     __syncthreads();
     for (int i = threadIdx.x; i < kMaxContacts; i += blockDim.x) c[i] = tmp[i];
 }
 constexpr int kLB_sort_contacts = 0;
-__global__ void k_sort_contacts(Scalars* sc, ContactRec* c, ContactRec* tmp, double* key, int* idx, const int* skip_if) { sort_contacts_body(sc, c, tmp, key, idx, skip_if); }
+__global__ void k_sort_contacts(Scalars* sc, ContactRec* c, ContactRec* tmp, double* key, int* idx, int* gscr, int* lscr,
+                                SortRange* small, const int* skip_if) {
+    sort_contacts_body(sc, c, tmp, key, idx, gscr, lscr, small, skip_if);
+}
 
 // After the Newton solve and the detection at x_new (IPCSolver.cpp:1112-1165):
 // normal forces, contact residual, ALM convergence.

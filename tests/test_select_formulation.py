@@ -192,3 +192,86 @@ def test_std_sort_stable_rank_finish():
         keys = rng.integers(0, 4, n).astype(float)
         got = refcpu.std_sort(keys).tolist()
         assert got == sorted(range(n), key=lambda i: (keys[i], i))
+
+
+# ---------------------------------------------------------------------------
+# The contact sort (sel_sort_prefix_block): std::sort of the raw contacts by
+# distance, exact in the first `keep` positions, formulated as CTA-partitioned
+# long ranges, warp-finished short ranges, leaves stably sorted, and ranges
+# that start at or beyond `keep` dropped.
+# ---------------------------------------------------------------------------
+def sort_heap(s, f, l):
+    while l - f > 1:
+        l -= 1
+        s.pop_heap(f, l, l)
+
+
+def finish_range(s, f, l, d, keep):
+    """One warp's range: introsort with leaves marked, then the stable sort
+    of each leaf."""
+    leaves = []
+    stack = [(f, l, d)]
+    while stack:
+        a, b, dd = stack.pop()
+        while True:
+            if a >= keep or b - a <= 16:
+                break
+            if dd == 0:
+                s.make_heap(a, b)
+                sort_heap(s, a, b)
+                break
+            dd -= 1
+            cut = s.partition_pivot(a, b)
+            stack.append((cut, b, dd))
+            b = cut
+        leaves.append(a)
+    starts = sorted(leaves) + [l]
+    for a, b in zip(starts[:-1], starts[1:]):
+        s.idx[a:b] = sorted(s.idx[a:b], key=lambda e, pos={e: p for p, e in enumerate(s.idx[a:b])}: (s.k[e], pos[e]))
+
+
+def sort_prefix(keys, keep, warp_range=256):
+    s = Sel(keys)
+    n = len(keys)
+    small = []
+    stack = [(0, n, 2 * lg(n))]
+    while stack:
+        f, l, d = stack.pop()
+        while True:
+            if f >= keep or l - f <= 1:
+                break
+            if l - f <= warp_range:
+                small.append((f, l, d))
+                break
+            if d == 0:
+                s.make_heap(f, l)
+                sort_heap(s, f, l)
+                break
+            d -= 1
+            cut = s.partition_pivot(f, l)
+            stack.append((cut, l, d))
+            l = cut
+    for f, l, d in small:
+        finish_range(s, f, l, d, keep)
+    return s.idx[:keep]
+
+
+def contact_like_cases():
+    rng = np.random.default_rng(11)
+    out = []
+    for n, keep in ((2001, 2000), (2600, 2000), (5000, 2000), (9000, 2000), (700, 300), (300, 40)):
+        z = rng.random(n) * 1e-3
+        z[rng.random(n) < 0.3] = 0.0                      # touching hinged links: distance 0
+        z[rng.random(n) < 0.1] = 2.1127e-4                 # a repeated value
+        out.append((z, keep))
+        out.append((np.round(rng.random(n) * 8) / 8, keep))   # few distinct values
+        out.append((np.zeros(n), keep))                      # all equal
+        out.append((np.arange(n, dtype=float)[::-1].copy(), keep))
+    return out
+
+
+@pytest.mark.parametrize("case", contact_like_cases(), ids=lambda c: f"n{len(c[0])}_keep{c[1]}")
+def test_contact_sort_prefix_matches_std_sort(case):
+    keys, keep = case
+    expect = refcpu.std_sort(keys).tolist()[:keep]
+    assert sort_prefix(keys, keep) == expect
