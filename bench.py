@@ -151,20 +151,29 @@ def newton_bytes(n_bodies: int, n_joints: int, n_contacts: float) -> float:
     return 2 * 288.0 * (n_bodies + n_joints + n_contacts) + 7 * 48.0 * n_bodies + 88.0 * n_contacts + 800.0 * n_joints
 
 
-def cpu_baseline_sample(scene_fn, threads: int, stride: int):
-    """One oracle step on the same scene with the reference's literal
-    computeSceneMinDistance restricted to bodies i % stride == 0; its time is
-    scaled by stride.  Returns estimated seconds per step."""
+def oracle_steps(scene_fn, threads: int, skip: int, steps: int, literal: bool):
+    """The CPU oracle (the reference's step restated) on the same scene and
+    step indices as the device: `skip` untimed steps with the pruned scene
+    minimum distance (exact below 1e-6, so its stiffness decisions and the
+    trajectory are the literal loop's), then `steps` steps timed one by one
+    (wall clock) with the literal O(N^2 V F) loop of
+    AdaptiveBarrier::computeSceneMinDistance (literal=True) or the pruned one.
+    Returns (seconds per timed step, untimed seconds)."""
     from oracle.refcpu import OracleWorld
     sc = scene_fn()
-    ow = OracleWorld(sc, literal_min_distance=True, threads=threads, md_stride=stride)
+    ow = OracleWorld(sc, literal_min_distance=False, threads=threads)
     t0 = time.perf_counter()
-    ow.step()
-    wall = time.perf_counter() - t0
-    t = ow.step_times()
-    est = t[5] + t[1] * (stride - 1)
+    for _ in range(skip):
+        ow.step()
+    ff = time.perf_counter() - t0
+    ow.set_options(literal_min_distance=literal, threads=threads)
+    walls = []
+    for _ in range(steps):
+        t1 = time.perf_counter()
+        ow.step()
+        walls.append(time.perf_counter() - t1)
     ow.close()
-    return est, wall
+    return walls, ff
 
 
 def batched_leg(torch, steps: int, warmup: int, flush):
@@ -174,7 +183,7 @@ def batched_leg(torch, steps: int, warmup: int, flush):
     each, stepped one after another on one stream).  Both device-timed with
     CUDA events per step, L2 flushed between steps."""
     from nexdynipc_b200 import runtime, scenes
-    scs = scenes.batched_scenes(256)
+    scs = scenes.batched_scenes(n_scenes=256)
     stream = torch.cuda.Stream()
     lib = runtime.lib()
     b = runtime.Batch(scs)
@@ -217,6 +226,35 @@ def batched_leg(torch, steps: int, warmup: int, flush):
         c.close()
     b.close()
     return out
+
+
+def full_run_leg(torch, lib, stream, flush):
+    """The workload's whole run: a fresh context of the same scene stepped
+    through all its steps (100), each step its CUDA graph, CUDA events per
+    step, L2 flushed between steps.  The bench's K-step window sits early in
+    the run; the pile forms later, so this is the configuration's full cost."""
+    from nexdynipc_b200 import runtime, scenes
+    sc = scenes.hopper_chains()
+    ctx = runtime.Context(sc)
+    lib.nxd_set_stream(ctx.h, C.c_void_p(stream.cuda_stream))
+    n = sc.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for k in range(n):
+            flush.fill_(k & 0xFF)
+            ev[k][0].record(stream)
+            st = lib.nxd_step(ctx.h, sc.dt)
+            if st != 0:
+                raise runtime.NxdError("nxd_step", st)
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    ms = np.array([a.elapsed_time(b) for a, b in ev])
+    d = ctx.diagnostics()
+    ctx.close()
+    return {"steps": n, "steps_per_s": n / (ms.sum() / 1e3), "ms_total": float(ms.sum()),
+            "steps_per_s_1_50": 50 / (ms[:50].sum() / 1e3), "steps_per_s_51_100": 50 / (ms[50:].sum() / 1e3),
+            "ms_max_step": float(ms.max()), "slowest_step": int(np.argmax(ms)) + 1, "status": int(d["status"])}
 
 
 def diff_leg(torch):
@@ -407,29 +445,54 @@ def mode_i_leg(ctx, sc, reps: int = 5):
             "primitives": {"vertices": int(sc.n_vertices), "faces": int(sc.n_faces)}}
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def run_reference(args, ws, rank):
+    """The reference arm: the reference's CPU step (the oracle's restatement:
+    the reference itself cannot be built here) on the host's cores, over the
+    step indices the device arm times.  The warm-up steps are fast-forwarded
+    untimed with the pruned scene minimum distance (same trajectory), then
+    each of the K timed steps runs the literal computeSceneMinDistance loop
+    of the reference on all host threads.  A second, labelled leg times the
+    first steps of the same window with the pruned loop (same trajectory,
+    the GPU's pruning on the CPU), separating the algorithm from the
+    hardware."""
     if rank != 0:
         return
     from nexdynipc_b200 import scenes
     threads = os.cpu_count() or 1
-    stride = 64
-    ests, walls = [], []
-    for i in range(args.warmup + args.steps):
-        est, wall = cpu_baseline_sample(scenes.hopper_chains, threads, stride)
-        if i >= args.warmup:
-            ests.append(est)
-            walls.append(wall)
-    value = len(ests) / sum(ests)
+    walls, ff = oracle_steps(scenes.hopper_chains, threads, args.warmup, args.steps, literal=True)
+    value = len(walls) / sum(walls)
+    n_pruned = min(args.steps, 5)
+    pwalls, pff = oracle_steps(scenes.hopper_chains, threads, args.warmup, n_pruned, literal=False)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(ests) / len(ests),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(walls) / len(walls),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD},
+        "config": {"workload": WORKLOAD,
+                   "timed_steps": f"{args.warmup + 1}-{args.warmup + args.steps} (the device arm's window)",
+                   "timed_s": sum(walls), "untimed_fast_forward_s": ff, "cpu": cpu_model(),
+                   "pruned_steps_per_s": n_pruned / sum(pwalls),
+                   "pruned_steps": f"{args.warmup + 1}-{args.warmup + n_pruned}"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": (f"each step: first step of the scene through the CPU oracle (the reference "
-                                    f"cannot be built here: Eigen/Boost absent) with {threads} OpenMP threads, "
-                                    f"literal O(N^2 V F) computeSceneMinDistance over bodies i % {stride} == 0 "
-                                    f"scaled x{stride}; measured wall {np.mean(walls):.1f} s per sample")},
+                         "sample": (f"steps {args.warmup + 1}-{args.warmup + args.steps} of the workload through the "
+                                    f"CPU oracle (the reference's step restated; the reference cannot be built here: "
+                                    f"Eigen/Boost absent) with {threads} OpenMP threads and the reference's literal "
+                                    f"O(N^2 V F) computeSceneMinDistance, every step timed whole "
+                                    f"({sum(walls):.1f} s); steps 1-{args.warmup} fast-forwarded untimed")},
+        "cpu_baseline_pruned": {"value": n_pruned / sum(pwalls), "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": (f"steps {args.warmup + 1}-{args.warmup + n_pruned}, the same oracle with "
+                                           f"the pruned scene minimum distance (identical trajectory), "
+                                           f"{sum(pwalls):.1f} s")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -607,10 +670,34 @@ def main():
                            note=("compute-bound: each pair's selected primitives are staged once and every "
                                  "candidate is tested from registers / shared memory (ncu: FP64 pipe ~40 % "
                                  "active); per_candidate_operand_gbs counts every candidate's operands"))
+    # FP64 roofline of the narrow phase against this device's measured DFMA
+    # throughput.  Algorithmic FP64 operations of the common path per item:
+    # a face-vertex item 8 (p - v0, the dot with the face normal; the
+    # barycentric test runs only inside dhat), an edge-edge item 12 (midpoint
+    # difference, its squared length, the sum of the radii and its square;
+    # the closest-point solve runs only inside the bounding spheres).  The
+    # kernels keep every multiply and add separately rounded (bit parity with
+    # the CPU path), so 0.5 of the FMA peak is their ceiling.
+    fp64_tflops, fp64_ms = runtime.fp64_peak(stream.cuda_stream)
+    roof_fp64 = None
+    if cand_counts:
+        fv, ee = cand_counts
+        passes = prof_n[FAMILIES.index("narrow_phase")] / 4.0
+        secs = prof_ms[FAMILIES.index("narrow_phase")] / 1e3
+        flops_pass = 8.0 * fv + 12.0 * ee
+        ach_tf = flops_pass * passes / secs / 1e12
+        roof_fp64 = {"kernel": "narrow_phase", "bound": "fp64", "unit": "TFLOP/s", "peak": fp64_tflops,
+                     "peak_kind": "measured (nxd_fp64_peak: DFMA chains on every SM, best of 5)",
+                     "achieved": ach_tf, "frac": ach_tf / fp64_tflops, "flops_per_pass": flops_pass,
+                     "fv_items": int(fv), "ee_items": int(ee),
+                     "note": ("common-path FP64 operations of every face-vertex (8) and edge-edge (12) item over the "
+                              "family's time (rows + emission launches); no FMA contraction, so 0.5 is the ceiling")}
     fam = int(np.argmax(prof_ms))
     roof = roof_newton if FAMILIES[fam] == "newton" else (roof_narrow if FAMILIES[fam] == "narrow_phase"
                                                           else dict(family_roof(fam), achieved=None, frac=None))
     per_family = {FAMILIES[i]: {"ms": round(float(prof_ms[i]), 3), "launches": int(prof_n[i])} for i in range(9)}
+
+    full = full_run_leg(torch, lib, stream, flush)
 
     mode_i = None if args.no_mode_i else mode_i_leg(ctx, sc)
     if mode_i is not None:
@@ -626,12 +713,13 @@ def main():
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        stride = 64
-        est, wall = cpu_baseline_sample(scenes.hopper_chains, 1, stride)
-        cpu = {"value": 1.0 / est, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": (f"first step of the same scene through the CPU oracle (serial, as the reference runs; "
-                          f"the reference itself cannot be built here), literal computeSceneMinDistance over bodies "
-                          f"i % {stride} == 0 scaled x{stride}; {wall:.1f} s wall")}
+        threads = os.cpu_count() or 1
+        walls, ff = oracle_steps(scenes.hopper_chains, threads, args.warmup, 1, literal=True)
+        cpu = {"value": 1.0 / walls[0], "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": (f"step {args.warmup + 1} (the first timed index) of the same scene through the CPU oracle "
+                          f"(the reference's step restated; the reference itself cannot be built here) on "
+                          f"{threads} threads with the reference's literal computeSceneMinDistance, timed whole: "
+                          f"{walls[0]:.1f} s; steps 1-{args.warmup} fast-forwarded untimed ({ff:.1f} s)")}
         if mode_i is not None:
             mode_i["step"]["cpu_baseline"] = ipc_step_cpu_baseline(8, 1, 30, 20)
             mode_i["step_64"]["cpu_baseline"] = ipc_step_cpu_baseline(64, 16, 30, 10)
@@ -648,6 +736,14 @@ def main():
                               "nxd_get_state back, wall clock"),
                    "twin_state_equal": twin_equal,
                    "e2e_state_equal": e2e_equal,
+                   "fp64_peak_tflops": fp64_tflops,
+                   "full_run_steps_per_s": full["steps_per_s"],
+                   "full_run_steps": full["steps"],
+                   "full_run_ms_max_step": full["ms_max_step"],
+                   "batched_scene_steps_per_s": None if batched is None else batched["value"],
+                   "batched_over_plain": None if batched is None else batched["batched_over_plain"],
+                   "batched_groups": None if batched is None else batched["groups"],
+                   "full_run": full,
                    "per_family_ms": per_family, "last_step": {k: diag[k] for k in
                                                               ("n_body_pairs", "n_contacts", "alm_iterations",
                                                                "newton_iterations", "status")},
@@ -657,6 +753,7 @@ def main():
                    "mode_i": mode_i},
         "roofline": roof,
         "roofline_narrow_phase": roof_narrow,
+        "roofline_fp64_narrow_phase": roof_fp64,
         "roofline_pcg": None if pcg is None else {
             "kernel": "k_pcg", "bound": "hbm", "unit": "GB/s", "peak": peak, "peak_kind": peak_kind,
             "achieved": pcg["achieved_gbs"], "frac": pcg["achieved_gbs"] / peak if pcg["achieved_gbs"] else None,

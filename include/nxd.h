@@ -488,6 +488,13 @@ nxd_status nxd_body_pairs_noalloc(const double* position, const double* orientat
                                   int32_t n, double inflation_radius, int32_t* pairs, int64_t cap,
                                   int64_t* count, void* stream);
 
+/* FP64 fused multiply-add throughput of the current device, in TFLOP/s
+ * (best of five timed launches of independent DFMA chains on every SM; *ms
+ * gets that launch's time, may be NULL).  A measurement helper for the FP64
+ * rooflines, with no counterpart in the reference; it allocates and frees a
+ * few KB and synchronises `stream`. */
+nxd_status nxd_fp64_peak(void* stream, double* tflops, double* ms);
+
 /* Library version string. */
 const char* nxd_version(void);
 

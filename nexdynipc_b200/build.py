@@ -12,7 +12,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libnxd_b200.so")
-SRCS = [os.path.join(HERE, "csrc", f) for f in ("nxd.cu", "noalloc.cu")]
+SRCS = [os.path.join(HERE, "csrc", f) for f in ("nxd.cu", "noalloc.cu", "peak.cu")]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17", "--fmad=false",

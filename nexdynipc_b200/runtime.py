@@ -76,6 +76,8 @@ def lib():
     L.nxd_batch_set_stream.restype = C.c_int
     L.nxd_body_pairs_noalloc.argtypes = [vp, vp, vp, C.c_int32, C.c_double, vp, C.c_int64, i64p, vp]
     L.nxd_body_pairs_noalloc.restype = C.c_int
+    L.nxd_fp64_peak.argtypes = [vp, dp, dp]
+    L.nxd_fp64_peak.restype = C.c_int
     L.nxd_profile.argtypes = [vp, C.c_int32, dp, i64p]
     L.nxd_profile.restype = C.c_int
     for name in ("nxd_set_form_state", "nxd_form_value", "nxd_form_gradient", "nxd_form_hessian_bsr",
@@ -411,6 +413,14 @@ def body_pairs_noalloc(position_ptr: int, orientation_ptr: int, local_box_ptr: i
         C.c_void_p(position_ptr), C.c_void_p(orientation_ptr), C.c_void_p(local_box_ptr), n, r,
         C.c_void_p(pairs_ptr), cap, C.byref(cnt), C.c_void_p(stream_ptr) if stream_ptr else None))
     return cnt.value
+
+
+def fp64_peak(stream_ptr: int = 0):
+    """nxd_fp64_peak: (TFLOP/s of FP64 FMA on the current device, ms)."""
+    tf, ms = C.c_double(0), C.c_double(0)
+    _check("nxd_fp64_peak", lib().nxd_fp64_peak(C.c_void_p(stream_ptr) if stream_ptr else None, C.byref(tf),
+                                                C.byref(ms)))
+    return tf.value, ms.value
 
 
 class World:
