@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -73,6 +74,7 @@ struct nxd_ctx {
     cudaStream_t stream = nullptr;
     int dev = 0, n_sm = 148;
     int newton_grid = 1;   // co-resident CTAs of k_newton (power of two)
+    bool newton_cluster = false;   // k_newton's CTAs launched as one thread-block cluster
     int N = 0, nv = 0, nf = 0, ne = 0, J = 0, D = 0;
     int max_prims = 0;
     int max_verts = 0;
@@ -179,6 +181,7 @@ void fill_solver(nxd_ctx* c) {
     S.contacts = c->contacts; S.ncontacts_ptr = &c->sc->n_contacts;
     S.nforce = c->nforce; S.nnf_ptr = &c->sc->nnf;
     S.cinc_off = m.alloc<int>(N + 1); S.cinc = m.alloc<int>(2 * C);
+    S.heavy = m.alloc<int>(N); S.heavy_list = m.alloc<int>(N); S.n_heavy = m.alloc<int>(1);
     S.dt_ptr = &c->sc->dt; S.scale_ptr = &c->sc->scale; S.bdhat_ptr = &c->sc->bdhat; S.bkappa_ptr = &c->sc->bkappa;
     S.barrier_in_forms_ptr = &c->sc->barrier_in_forms; S.friction_form_ptr = &c->sc->friction_form;
     S.friction_mu_ptr = &c->sc->friction_mu; S.friction_eps = 1e-8;
@@ -227,6 +230,24 @@ void fill_solver(nxd_ctx* c) {
     int g = 1;
     while (g < kMaxNewtonGrid && g * 2 <= coresident && (long long)g * kNewtonThreads < 6LL * N) g *= 2;
     c->newton_grid = g;
+    // up to 16 CTAs run as one thread-block cluster (hardware grid barrier)
+    // when the device can place such a cluster; NXD_NEWTON_BARRIER=global
+    // keeps the cooperative launch with the global-memory barrier
+    c->newton_cluster = false;
+    const char* nb = std::getenv("NXD_NEWTON_BARRIER");
+    if (g > 1 && g <= 16 && !(nb && std::strcmp(nb, "global") == 0)) {
+        cudaFuncSetAttribute(k_newton, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(g); cfg.blockDim = dim3(kNewtonThreads); cfg.dynamicSmemBytes = kNewtonDynSmem;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = g; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+        cfg.attrs = at; cfg.numAttrs = 1;
+        int ncl = 0;
+        if (cudaOccupancyMaxActiveClusters(&ncl, (const void*)k_newton, &cfg) == cudaSuccess && ncl >= 1)
+            c->newton_cluster = true;
+        cudaGetLastError();
+    }
 }
 
 StepCfg step_cfg(const nxd_ctx* c) {
@@ -253,6 +274,17 @@ void launch_newton(nxd_ctx* c) {
         return;
     }
     ProfScope ps_(c, NXD_PROF_NEWTON);
+    if (c->newton_cluster) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(c->newton_grid); cfg.blockDim = dim3(kNewtonThreads);
+        cfg.dynamicSmemBytes = kNewtonDynSmem; cfg.stream = c->stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = c->newton_grid; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+        cfg.attrs = at; cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k_newton, c->S);
+        return;
+    }
     cudaMemsetAsync(c->S.bar_count, 0, 2 * sizeof(unsigned), c->stream);
     void* args[] = {(void*)&c->S};
     cudaLaunchCooperativeKernel((const void*)k_newton, dim3(c->newton_grid), dim3(kNewtonThreads), args, kNewtonDynSmem, c->stream);
