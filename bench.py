@@ -176,14 +176,18 @@ def oracle_steps(scene_fn, threads: int, skip: int, steps: int, literal: bool):
     return walls, ff
 
 
-def batched_leg(torch, steps: int, warmup: int, flush):
+def batched_leg(torch, steps: int, warmup: int, flush, ws: int = 1, rank: int = 0):
     """256 independent scenes of 2-63 bodies (the batched configuration, seed
     4000): aggregate scene-steps/s of the batched form (one graph of batched
     launches per step) next to the plain path (the same scenes, one context
     each, stepped one after another on one stream).  Both device-timed with
-    CUDA events per step, L2 flushed between steps."""
-    from nexdynipc_b200 import runtime, scenes
-    scs = scenes.batched_scenes(n_scenes=256)
+    CUDA events per step, L2 flushed between steps.  Under several ranks the
+    scenes are sharded (nexdynipc_b200.shard: greedy by estimated cost, no
+    exchange while stepping): each rank steps its share, the time is the
+    slowest rank's, the value all 256 scenes' steps over it."""
+    from nexdynipc_b200 import runtime, scenes, shard
+    all_scs = scenes.batched_scenes(n_scenes=256)
+    idx, scs = shard.my_scenes(all_scs, rank, ws)
     stream = torch.cuda.Stream()
     lib = runtime.lib()
     b = runtime.Batch(scs)
@@ -213,15 +217,18 @@ def batched_leg(torch, steps: int, warmup: int, flush):
         torch.cuda.synchronize()
         return sum(a.elapsed_time(e) for a, e in ev) / 1e3
 
-    t_batched = timed(b.step)
-    t_plain = timed(plain_step)
+    if ws > 1:
+        torch.distributed.barrier()
+    t_batched = max_over_ranks(timed(b.step))
+    t_plain = max_over_ranks(timed(plain_step))
     status = max(b.diagnostics(i)["status"] for i in range(len(scs)))
     same = all(np.array_equal(b.state(i)["position"], singles[i].state()["position"]) for i in range(0, len(scs), 17))
-    n = len(scs)
-    out = {"scenes": n, "bodies": int(sum(s.n_bodies for s in scs)), "steps": steps,
+    n = len(all_scs)
+    out = {"scenes": n, "bodies": int(sum(s.n_bodies for s in all_scs)), "steps": steps,
            "value": n * steps / t_batched, "plain_value": n * steps / t_plain, "unit": "scene-steps/s",
            "batched_over_plain": t_plain / t_batched, "groups": b.groups(), "status": int(status),
-           "equal_to_plain_sample": bool(same)}
+           "equal_to_plain_sample": bool(same), "ranks": ws, "scenes_this_rank": len(scs),
+           "sharding": "greedy by estimated cost, no exchange while stepping" if ws > 1 else "one rank"}
     for c in singles:
         c.close()
     b.close()
@@ -707,7 +714,7 @@ def main():
 
     batched = None
     if not args.no_batched:
-        batched = batched_leg(torch, min(args.steps, 10), 2, flush)
+        batched = batched_leg(torch, min(args.steps, 10), 2, flush, ws, rank)
     diffl = None if args.no_diff else diff_leg(torch)
     pcg = None if args.no_pcg else pcg_leg()
 
