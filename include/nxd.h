@@ -488,6 +488,20 @@ nxd_status nxd_body_pairs_noalloc(const double* position, const double* orientat
                                   int32_t n, double inflation_radius, int32_t* pairs, int64_t cap,
                                   int64_t* count, void* stream);
 
+/* Failure-detection hook, no counterpart in the reference (its Newton solve
+ * has no waits and no failure report).  spin_limit > 0 bounds every grid-
+ * barrier wait of the Newton solve to that many polls (at most 2^20);
+ * hold_last_cta != 0 (needs spin_limit > 0) makes the solve's last CTA keep
+ * away from its first barrier until the others have given up (at most
+ * 64 x spin_limit polls), so their waits run out: the step then reports
+ * NXD_TIMEOUT in nxd_diagnostics.status and every CTA returns.  Both switch
+ * the solve to the global-memory barrier, whose waits are bounded (the
+ * cluster form waits in hardware).  nxd_debug_grid_wait(ctx, 0, 0) restores
+ * the normal solve and clears the sticky status; the context stays usable
+ * (set the state again before stepping on).  Synchronises the context's
+ * stream. */
+nxd_status nxd_debug_grid_wait(nxd_ctx* ctx, uint32_t spin_limit, int32_t hold_last_cta);
+
 /* FP64 fused multiply-add throughput of the current device, in TFLOP/s
  * (best of five timed launches of independent DFMA chains on every SM; *ms
  * gets that launch's time, may be NULL).  A measurement helper for the FP64

@@ -165,6 +165,8 @@ struct ProfScope {
         }                                                                                               \
     } while (0)
 
+void configure_newton_launch(nxd_ctx* c);
+
 void fill_solver(nxd_ctx* c) {
     Solver& S = c->S;
     const int N = c->N, J = c->J, D = c->D, C = kMaxRawContacts;
@@ -218,6 +220,7 @@ void fill_solver(nxd_ctx* c) {
     S.iact = m.alloc<int>(J + D + 2 * kMaxContacts);
     S.ext_n = -1; S.ext_row = nullptr; S.ext_col = nullptr; S.ext_vals = nullptr;
     S.bar_count = m.alloc<unsigned>(2); S.bar_abort = (int*)(S.bar_count + 1);
+    S.spin_limit = 0; S.dbg_hold = 0;
     S.gpart = m.alloc<double>(2 * kRedMaxQ * kMaxNewtonGrid);
     // one CTA of kNewtonThreads per 512 DOFs, a power of two no larger than
     // what the device keeps co-resident
@@ -230,9 +233,14 @@ void fill_solver(nxd_ctx* c) {
     int g = 1;
     while (g < kMaxNewtonGrid && g * 2 <= coresident && (long long)g * kNewtonThreads < 6LL * N) g *= 2;
     c->newton_grid = g;
-    // up to 16 CTAs run as one thread-block cluster (hardware grid barrier)
-    // when the device can place such a cluster; NXD_NEWTON_BARRIER=global
-    // keeps the cooperative launch with the global-memory barrier
+    configure_newton_launch(c);
+}
+
+// Up to 16 CTAs of k_newton run as one thread-block cluster (hardware grid
+// barrier) when the device can place such a cluster; NXD_NEWTON_BARRIER=global
+// keeps the cooperative launch with the global-memory barrier.
+void configure_newton_launch(nxd_ctx* c) {
+    const int g = c->newton_grid;
     c->newton_cluster = false;
     const char* nb = std::getenv("NXD_NEWTON_BARRIER");
     if (g > 1 && g <= 16 && !(nb && std::strcmp(nb, "global") == 0)) {
@@ -449,6 +457,7 @@ nxd_status enqueue_step(nxd_ctx* c, double dt) {
 // ===========================================================================
 namespace {
 void drop_step_graph(nxd_ctx* c);
+void configure_newton_launch(nxd_ctx* c);
 void release_ipc(nxd_ctx* c);
 }  // namespace
 
@@ -775,6 +784,24 @@ nxd_status nxd_step(nxd_ctx* c, double dt) {
     }
     for (int f = 0; f < NXD_PROF_FAMILIES; ++f) c->launches[f] += c->graph_launches[f];
     NXD_CUDA(cudaGraphLaunch(c->graph_exec, c->stream));
+    return NXD_OK;
+}
+
+nxd_status nxd_debug_grid_wait(nxd_ctx* c, uint32_t spin_limit, int32_t hold_last_cta) {
+    if (!c || spin_limit > (1u << 20) || (hold_last_cta && spin_limit == 0)) return NXD_INVALID_ARGUMENT;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return NXD_CUDA_ERROR;
+    drop_step_graph(c);                 // the captured step holds the old settings
+    c->S.spin_limit = spin_limit;
+    c->S.dbg_hold = hold_last_cta ? 1 : 0;
+    if (spin_limit || hold_last_cta) {
+        c->newton_cluster = false;      // the hardware barrier has no bounded form
+    } else {
+        configure_newton_launch(c);
+        // back to normal: the sticky status of the failed step is cleared
+        if (cudaMemsetAsync(&c->sc->status, 0, sizeof(int), c->stream) != cudaSuccess ||
+            cudaStreamSynchronize(c->stream) != cudaSuccess)
+            return NXD_CUDA_ERROR;
+    }
     return NXD_OK;
 }
 

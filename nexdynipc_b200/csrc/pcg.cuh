@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const __grid_constant__ Pcg
     gc.gtid = blockIdx.x * blockDim.x + threadIdx.x; gc.gthreads = gridDim.x * blockDim.x;
     gc.lin = gc.gtid;
     gc.count = A.bar_count; gc.abort = A.bar_abort; gc.status = A.status; gc.target = 0; gc.sh_ok = &sh_ok;
-    gc.cluster = false;
+    gc.cluster = false; gc.limit = kBarrierSpinLimit;
     __syncthreads();
     int parity = 0;
     const int n = 6 * A.N;

@@ -112,6 +112,8 @@ struct Solver {
     int ext_n; const int* ext_row; const int* ext_col; const double* ext_vals;
     // grid execution of k_newton
     unsigned* bar_count; int* bar_abort;          // barrier arrivals and give-up flag, zeroed per launch
+    unsigned spin_limit;                          // polls before a barrier wait gives up (0: kBarrierSpinLimit)
+    int dbg_hold;                                 // failure-detection hook: the last CTA stays away (bounded)
     double* gpart;                                // [2 * kRedMaxQ * kMaxNewtonGrid] per-CTA partial sums
     // outputs / state
     int* alm_done; int* status; int* newton_iters; int* converged; int* ls_fail;
@@ -1658,6 +1660,7 @@ struct GridCtx {
     int* abort;           // set by a CTA whose wait ran out
     int* status;
     unsigned target;
+    unsigned limit;       // polls before a wait gives up
     int* sh_ok;           // shared: 0 once this CTA has given up
     __device__ bool sync() {
         if (G == 1) { __syncthreads(); return true; }
@@ -1672,7 +1675,7 @@ struct GridCtx {
                 unsigned spins = 0;
                 while (ld_acquire_u32(count) < target) {
                     ++spins;
-                    if (spins > kBarrierSpinLimit || ((spins & 63u) == 0 && *(volatile int*)abort)) {
+                    if (spins > limit || ((spins & 63u) == 0 && *(volatile int*)abort)) {
                         ok = 0;
                         atomicExch(abort, 1);
                         atomicExch(status, NXD_TIMEOUT);
@@ -1944,8 +1947,17 @@ __device__ __forceinline__ void newton_body(const Solver& S) {
     gc.lin = threadIdx.x * gc.G + gc.b;
     gc.count = S.bar_count; gc.abort = S.bar_abort; gc.status = S.status; gc.target = 0; gc.sh_ok = &sh_ok;
     gc.cluster = gc.G > 1 && (int)cluster_ctas() == gc.G;
+    gc.limit = S.spin_limit ? S.spin_limit : kBarrierSpinLimit;
     if (threadIdx.x == 0) sh_ok = 1;
     __syncthreads();
+    if (S.dbg_hold && gc.G > 1 && !gc.cluster && gc.b == gc.G - 1) {
+        // failure-detection hook (nxd_debug_grid_wait): this CTA keeps away
+        // from the first barrier until the others have given up on it, or
+        // for at most 64 x limit polls
+        if (threadIdx.x == 0)
+            for (unsigned k = 0; k < 64u * gc.limit && !*(volatile int*)gc.abort; ++k) __nanosleep(64);
+        __syncthreads();
+    }
     GridRed R;
     R.gc = &gc; R.sh = sh_red; R.part = S.gpart; R.parity = 0; R.stride = kMaxNewtonGrid;
     const int N = S.N;
@@ -2159,7 +2171,7 @@ __global__ void __launch_bounds__(kNewtonThreads) k_linear_solve(const __grid_co
     GridCtx gc;
     gc.G = 1; gc.b = 0; gc.gtid = threadIdx.x; gc.gthreads = blockDim.x; gc.lin = threadIdx.x;
     gc.count = S.bar_count; gc.abort = S.bar_abort; gc.status = S.status; gc.target = 0; gc.sh_ok = &sh_ok;
-    gc.cluster = false;
+    gc.cluster = false; gc.limit = kBarrierSpinLimit;
     __syncthreads();
     GridRed R;
     R.gc = &gc; R.sh = sh_red; R.part = S.gpart; R.parity = 0; R.stride = kMaxNewtonGrid;

@@ -76,6 +76,8 @@ def lib():
     L.nxd_batch_set_stream.restype = C.c_int
     L.nxd_body_pairs_noalloc.argtypes = [vp, vp, vp, C.c_int32, C.c_double, vp, C.c_int64, i64p, vp]
     L.nxd_body_pairs_noalloc.restype = C.c_int
+    L.nxd_debug_grid_wait.argtypes = [vp, C.c_uint32, C.c_int32]
+    L.nxd_debug_grid_wait.restype = C.c_int
     L.nxd_fp64_peak.argtypes = [vp, dp, dp]
     L.nxd_fp64_peak.restype = C.c_int
     L.nxd_profile.argtypes = [vp, C.c_int32, dp, i64p]
@@ -146,6 +148,12 @@ class Context:
         mu = np.zeros(max(nj, 1))
         _check("nxd_get_joint_state", lib().nxd_get_joint_state(self.h, abi.dptr(lam), abi.dptr(mu)))
         return lam[:nj], mu[:nj]
+
+    def debug_grid_wait(self, spin_limit: int, hold_last_cta: bool):
+        """nxd_debug_grid_wait: bound the Newton solve's barrier waits and
+        optionally hold its last CTA back (failure-detection tests);
+        (0, False) restores the normal solve and clears the sticky status."""
+        _check("nxd_debug_grid_wait", lib().nxd_debug_grid_wait(self.h, int(spin_limit), int(hold_last_cta)))
 
     def body_pairs(self, r: float) -> np.ndarray:
         cnt = C.c_int64(0)
