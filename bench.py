@@ -316,6 +316,44 @@ def diff_leg(torch):
             "finite": bool(np.isfinite(J).all())}
 
 
+def adjoint_leg(torch, n_sets: int = 2):
+    """Differentiable configuration on the full-IPC step: 16 icospheres
+    (162 V) over a ground box, 50 steps, loss = squared error of the final
+    poses against a seeded target, gradients with respect to every initial
+    velocity, mass and the ground joint's stiffness by the adjoint
+    (nxd_ipc_adjoint per step, checkpoints every 10 steps, each segment
+    re-stepped in the backward pass), through torch.autograd.  Wall clock of
+    the forward rollout and of the backward pass, per parameter set (the
+    initial velocities perturbed per set)."""
+    from nexdynipc_b200 import abi, adjoint, runtime, scenes
+    params = abi.ipc_params(dhat=1e-3, kappa=1e9, eta=0.1, newton_tol=1e-9, newton_max_iters=100, ls_max_iters=40)
+    base = scenes.diff_ipc_scene()
+    fn = adjoint.make_rollout_function()
+    rng = np.random.default_rng(5100)
+    fwd, bwd, its, conv, gnorm = [], [], [], [], []
+    for k in range(n_sets):
+        v0 = torch.tensor(base.velocity + rng.normal(0, 0.05, base.velocity.shape), requires_grad=True)
+        m = torch.tensor(base.mass, requires_grad=True)
+        mu = torch.tensor(base.joint_stiffness, requires_grad=True)
+        tgt = torch.tensor(np.concatenate([base.position, base.orientation], 1) + rng.normal(0, 0.02, (base.n_bodies, 7)))
+        t0 = time.perf_counter()
+        out = fn.apply(v0, m, mu, base, params, base.steps, 10)
+        t1 = time.perf_counter()
+        loss = ((out - tgt) ** 2).sum()
+        loss.backward()
+        t2 = time.perf_counter()
+        fwd.append(t1 - t0)
+        bwd.append(t2 - t1)
+        gnorm.append(float(v0.grad.abs().max()))
+    return {"workload": (f"{base.n_bodies - 1} icospheres (162 V) on a ground box (fixed joint 1e5), {base.steps} "
+                         f"steps, dt {base.dt}, full-IPC step (kappa 1e9, dhat 1e-3, Newton |g| < 1e-9)"),
+            "parameter_sets": n_sets, "parameters_per_set": int(3 * base.n_bodies + base.n_bodies + 1),
+            "checkpoint_every": 10, "forward_s": float(np.mean(fwd)), "backward_s": float(np.mean(bwd)),
+            "fwd_plus_adj_over_fwd": float(np.mean([(a + b) / a for a, b in zip(fwd, bwd)])),
+            "max_abs_velocity_gradient": gnorm,
+            "timing": "wall clock; the backward pass re-steps each 10-step segment from its checkpoint"}
+
+
 def pcg_leg(n_bodies: int = 200000, iters: int = 60):
     """Block-Jacobi PCG (nxd_pcg_solve) on a synthetic SPD block system of
     the size a large full-IPC Newton system reaches: n_bodies 6x6 block rows,
@@ -516,6 +554,7 @@ def main():
     ap.add_argument("--no-mode-i", action="store_true")
     ap.add_argument("--no-diff", action="store_true")
     ap.add_argument("--no-pcg", action="store_true")
+    ap.add_argument("--adjoint-sets", type=int, default=2, help="parameter sets of the adjoint leg")
     ap.add_argument("--ipc-step-only", type=int, nargs=4, metavar=("CUBES", "COLUMNS", "SETTLE", "STEPS"),
                     help="run only the full-IPC step leg on that drop and print its JSON (for profiling)")
     args = ap.parse_args()
@@ -717,6 +756,7 @@ def main():
         batched = batched_leg(torch, min(args.steps, 10), 2, flush, ws, rank)
     diffl = None if args.no_diff else diff_leg(torch)
     pcg = None if args.no_pcg else pcg_leg()
+    adj = None if args.no_diff else adjoint_leg(torch, args.adjoint_sets)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -756,6 +796,8 @@ def main():
                                                                "newton_iterations", "status")},
                    "batched": batched,
                    "diff": diffl,
+                   "adjoint": adj,
+                   "adjoint_fwd_plus_adj_over_fwd": None if adj is None else adj["fwd_plus_adj_over_fwd"],
                    "pcg": pcg,
                    "mode_i": mode_i},
         "roofline": roof,

@@ -461,6 +461,37 @@ typedef struct nxd_ipc_stats {
 } nxd_ipc_stats;
 nxd_status nxd_ipc_step(nxd_ctx* ctx, double dt, const nxd_ipc_params* p, nxd_ipc_stats* stats);
 
+/* Adjoint of one full-IPC time step (nxd_ipc_step, implicit Euler) by the
+ * implicit function theorem.  No counterpart in the reference (its
+ * differentiable-physics plan, documents/2026.02.21/可微物理实现方案.md, is
+ * not implemented); it serves the parameter-identification workflow of
+ * tools/compare_with_reference.py:85-165.  The step solves G(x; z) = 0
+ * for x = (p, theta) per body; at its converged iterate x_star (6N: the new
+ * positions and angular_velocity * dt), for x_bar = dL/dx_star:
+ *   K^T lambda = x_bar,  K = dG/dx (exact, unprojected, symmetric),
+ * and the input adjoints -(dG/dz)^T lambda: phat_bar = m lambda_p (the
+ * predicted position p0 + dt v0), thetahat_bar = I^T lambda_theta (the
+ * predicted rotation dt w0), phi_bar (left rotations of the step-start
+ * orientations, tangent 3-vectors), mass_bar, inertia_bar (3x3 per body,
+ * row-major), joint_mu_bar (fixed joints' stiffness).  `start` is the step's
+ * input state (host arrays); the context is left at that state.  Supported:
+ * bodies, fixed joints (FixedJoint), no control forms, implicit Euler,
+ * N <= 128 bodies (dense K, one CTA); else NXD_INVALID_ARGUMENT.
+ * NXD_FACTOR_FAILED if K is singular.  Output pointers are host arrays and
+ * may be NULL. */
+typedef struct nxd_ipc_adjoint_out {
+    double* lambda;             /* [6N] */
+    double* phat_bar;           /* [3N] */
+    double* thetahat_bar;       /* [3N] */
+    double* phi_bar;            /* [3N] */
+    double* mass_bar;           /* [N]  */
+    double* inertia_bar;        /* [9N] */
+    double* joint_mu_bar;       /* [J]  */
+    int32_t* n_active;          /* active pairs at x_star (may be NULL) */
+} nxd_ipc_adjoint_out;
+nxd_status nxd_ipc_adjoint(nxd_ctx* ctx, double dt, const nxd_ipc_params* p, const nxd_state* start,
+                           const double* x_star, const double* x_bar, const nxd_ipc_adjoint_out* out);
+
 /* Body-pair broad phase for callers that cannot allocate device memory.
  * No counterpart in the reference.  Callers that manage every device byte
  * themselves (a host engine's memory pool, a hard memory cap, a real-time

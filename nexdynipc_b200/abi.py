@@ -205,6 +205,19 @@ def ipc_params(dhat=1e-3, kappa=1e8, eta=0.1, newton_tol=1e-6, newton_max_iters=
                         pcg_tol)
 
 
+class NxdIpcAdjointOut(C.Structure):
+    _fields_ = [
+        ("lam", _dp),
+        ("phat_bar", _dp),
+        ("thetahat_bar", _dp),
+        ("phi_bar", _dp),
+        ("mass_bar", _dp),
+        ("inertia_bar", _dp),
+        ("joint_mu_bar", _dp),
+        ("n_active", C.POINTER(C.c_int32)),
+    ]
+
+
 class NxdState(C.Structure):
     _fields_ = [
         ("position", _dp),

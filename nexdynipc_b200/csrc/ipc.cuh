@@ -391,7 +391,11 @@ struct IpcPairs {
 struct IpcPose {
     const double* wq;      // world vertices at x [nv*3]
     const double* pp;      // body positions at x [N*3]
+    const double* x;       // the iterate [6N] (rotation vectors theta), or null: theta = 0
 };
+__device__ __forceinline__ V3 pose_theta(const IpcPose& ps, int b) {
+    return ps.x ? ld3(ps.x + 6 * b + 3) : v3(0, 0, 0);
+}
 
 __device__ __forceinline__ void pair_points(const PrimGeo& pg, const IpcPairs& P, const IpcPose& ps, int p, int& kind,
                                             V3* X, int* side, V3* arm, int& bA, int& bB) {
@@ -439,11 +443,105 @@ __global__ void k_ipc_pair_eval(PrimGeo pg, IpcPairs P, IpcPose ps, double dhat,
         o.body[2 * p] = bA; o.body[2 * p + 1] = bB;
         o.type[p] = f.type;
         o.active[p] = ev.d2 < dhat * dhat ? 1 : 0;
-        ipc::chain12(ev.grad, side, arm, o.grad + 12 * (size_t)p);
+        const V3 thA = pose_theta(ps, bA), thB = pose_theta(ps, bB);
+        ipc::chain12_exact(ev.grad, side, arm, thA, thB, o.grad + 12 * (size_t)p);
         o.nterm[p] = ev.n_terms;
         for (int k = 0; k < ev.n_terms; ++k) {
             o.lam[5 * (size_t)p + k] = ev.lam[k];
-            ipc::chain12(ev.y[k], side, arm, o.z + 60 * (size_t)p + 12 * k);
+            ipc::chain12_exact(ev.y[k], side, arm, thA, thB, o.z + 60 * (size_t)p + 12 * k);
+        }
+    }
+}
+
+// Step adjoint, per candidate pair at the converged iterate: the exact
+// derivative of the pair's share of the step gradient G (point forces g_k,
+// torques J_r(theta) sum a_k x g_k) with respect to the two bodies' DOFs
+// (kp, 12 x 12: rows and columns A 0..5, B 6..11) and to left rotations phi
+// of their step-start orientations (kf, 12 x 6: columns phi_A, phi_B):
+//   kp = E^T H E + Q,  kf = E^T H F + Q_phi,
+// H the unprojected point Hessian (ipc::pair_barrier_exact), E_k = [I,
+// -[a_k]x J_l(theta)] and F_k = -[a_k]x Exp(theta) the points' derivatives,
+// Q = J_r (sum_k [g_k]x [a_k]x) J_l + d(J_r tau)/dtheta and Q_phi =
+// J_r (sum_k [g_k]x [a_k]x) Exp(theta) on each body's own rotation block.
+// Unscaled (the step scales the barrier by s); inactive pairs flagged 0.
+__global__ void k_ipc_pair_adjoint(PrimGeo pg, IpcPairs P, IpcPose ps, double dhat, double kappa, double* kp, double* kf,
+                                   int* body, int* active) {
+    const int n = P.n_pt + P.n_ee;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        int kind, side[4], bA, bB;
+        V3 X[4], arm[4];
+        pair_points(pg, P, ps, p, kind, X, side, arm, bA, bB);
+        const ipc::DistForm f = ipc::classify(kind, X);
+        double g12[12], H[144];
+        const double d2 = ipc::pair_barrier_exact(f, X, dhat, kappa, g12, H);
+        body[2 * p] = bA; body[2 * p + 1] = bB;
+        const bool act = d2 < dhat * dhat && d2 > 0.0;
+        active[p] = act ? 1 : 0;
+        if (!act) continue;
+        const V3 th[2] = {pose_theta(ps, bA), pose_theta(ps, bB)};
+        double R[2][9], Jl[2][9];
+        for (int sd = 0; sd < 2; ++sd) ipc::rot_exp_mats(th[sd], R[sd], Jl[sd]);
+        double E[144], F[72];
+        for (int e = 0; e < 144; ++e) E[e] = 0.0;
+        for (int e = 0; e < 72; ++e) F[e] = 0.0;
+        for (int k = 0; k < 4; ++k) {
+            const int sg = side[k];
+            double A[9], D[9], Fk[9];
+            ipc::m3_skew(arm[k], A);
+            ipc::m3_mul(A, Jl[sg], D);
+            ipc::m3_mul(A, R[sg], Fk);
+            for (int i = 0; i < 3; ++i) {
+                E[12 * (3 * k + i) + 6 * sg + i] = 1.0;
+                for (int j = 0; j < 3; ++j) {
+                    E[12 * (3 * k + i) + 6 * sg + 3 + j] = -D[3 * i + j];
+                    F[6 * (3 * k + i) + 3 * sg + j] = -Fk[3 * i + j];
+                }
+            }
+        }
+        double* KP = kp + 144 * (size_t)p;
+        double* KF = kf + 72 * (size_t)p;
+        for (int r = 0; r < 12; ++r) {
+            double he[12], hf[6];
+            for (int c = 0; c < 12; ++c) he[c] = 0.0;
+            for (int c = 0; c < 6; ++c) hf[c] = 0.0;
+            // rows of E^T H: sum_i E[i][r] H[i][.]
+            for (int i = 0; i < 12; ++i) {
+                const double eir = E[12 * i + r];
+                if (eir == 0.0) continue;
+                for (int j = 0; j < 12; ++j) {
+                    const double t = eir * H[12 * i + j];
+                    for (int c = 0; c < 12; ++c) he[c] += t * E[12 * j + c];
+                    for (int c = 0; c < 6; ++c) hf[c] += t * F[6 * j + c];
+                }
+            }
+            for (int c = 0; c < 12; ++c) KP[12 * r + c] = he[c];
+            for (int c = 0; c < 6; ++c) KF[6 * r + c] = hf[c];
+        }
+        for (int sg = 0; sg < 2; ++sg) {
+            double GA[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            V3 tau = v3(0, 0, 0);
+            for (int k = 0; k < 4; ++k) {
+                if (side[k] != sg) continue;
+                const V3 gk = v3(g12[3 * k], g12[3 * k + 1], g12[3 * k + 2]);
+                double SG[9], SA[9], P9[9];
+                ipc::m3_skew(gk, SG);
+                ipc::m3_skew(arm[k], SA);
+                ipc::m3_mul(SG, SA, P9);
+                for (int e = 0; e < 9; ++e) GA[e] += P9[e];
+                tau = tau + cross(arm[k], gk);
+            }
+            double Jr[9], T1[9], Q[9], QF[9], M[9];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) Jr[3 * i + j] = Jl[sg][3 * j + i];
+            ipc::m3_mul(Jr, GA, T1);
+            ipc::m3_mul(T1, Jl[sg], Q);
+            ipc::m3_mul(T1, R[sg], QF);
+            ipc::jr_torque_derivative(th[sg], tau, M);
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    KP[12 * (6 * sg + 3 + i) + 6 * sg + 3 + j] += Q[3 * i + j] + M[3 * i + j];
+                    KF[6 * (6 * sg + 3 + i) + 3 * sg + j] += QF[3 * i + j];
+                }
         }
     }
 }

@@ -383,6 +383,50 @@ NX_UNROLL
     return o;
 }
 
+// Exact (unprojected) barrier of one classified pair in point space, for the
+// step adjoint, which differentiates the gradient itself: g12 = b' grad d^2
+// and the 12 x 12 row-major Hessian H = b'' grad grad^T + b' hess d^2 with
+// hess d^2 = g_xx - sum_pq G_p (g_uu^-1)_pq G_q^T (the envelope formula of
+// the header comment).  Zero outside the barrier's support.  Returns d^2.
+NX_HD double pair_barrier_exact(const DistForm& f, const V3* X, double dhat, double kappa, double* g12, double* H) {
+    const V3 r = form_r(f, X);
+    const double s = dot(r, r), sh = dhat * dhat;
+    for (int i = 0; i < 12; ++i) g12[i] = 0.0;
+    for (int i = 0; i < 144; ++i) H[i] = 0.0;
+    if (!(s < sh) || !(s > 0.0)) return s;
+    const double b1 = barrier_s1(s, sh, kappa), b2 = barrier_s2(s, sh, kappa);
+    double gs[12];
+    for (int k = 0; k < 4; ++k) {
+        gs[3 * k] = f.w[k] * (2.0 * r.x); gs[3 * k + 1] = f.w[k] * (2.0 * r.y); gs[3 * k + 2] = f.w[k] * (2.0 * r.z);
+    }
+    for (int i = 0; i < 12; ++i) g12[i] = b1 * gs[i];
+    V3 a[2] = {v3(0, 0, 0), v3(0, 0, 0)};
+    for (int j = 0; j < f.nu; ++j)
+        a[j] = f.c[0][j] * X[0] + f.c[1][j] * X[1] + f.c[2][j] * X[2] + f.c[3][j] * X[3];
+    double Minv[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    if (f.nu == 1) {
+        Minv[0][0] = 1.0 / (2.0 * dot(a[0], a[0]));
+    } else if (f.nu == 2) {
+        const double m00 = 2.0 * dot(a[0], a[0]), m01 = 2.0 * dot(a[0], a[1]), m11 = 2.0 * dot(a[1], a[1]);
+        const double det = m00 * m11 - m01 * m01;
+        Minv[0][0] = m11 / det; Minv[0][1] = -m01 / det; Minv[1][0] = -m01 / det; Minv[1][1] = m00 / det;
+    }
+    double G[2][12];
+    for (int j = 0; j < 2; ++j)
+        for (int k = 0; k < 4; ++k) {
+            const V3 v = j < f.nu ? f.w[k] * (2.0 * a[j]) + f.c[k][j] * (2.0 * r) : v3(0, 0, 0);
+            G[j][3 * k] = v.x; G[j][3 * k + 1] = v.y; G[j][3 * k + 2] = v.z;
+        }
+    for (int i = 0; i < 12; ++i)
+        for (int j = 0; j < 12; ++j) {
+            double hs = (i % 3 == j % 3) ? 2.0 * (f.w[i / 3] * f.w[j / 3]) : 0.0;
+            for (int p = 0; p < f.nu; ++p)
+                for (int q = 0; q < f.nu; ++q) hs -= G[p][i] * Minv[p][q] * G[q][j];
+            H[12 * i + j] = b2 * gs[i] * gs[j] + b1 * hs;
+        }
+    return s;
+}
+
 // Rigid chain: point k of the pair belongs to body side[k] (0 = body A,
 // 1 = body B) at lever arm arm[k] = R r_k (world offset from the body's
 // position); its DOF Jacobian is [I3, -[arm]x].  The transposed Jacobian
@@ -395,6 +439,110 @@ NX_HD void chain12(const V12& z, const int* side, const V3* arm, double* out12) 
         o[0] += z.v[k].x; o[1] += z.v[k].y; o[2] += z.v[k].z;
         o[3] += t.x; o[4] += t.y; o[5] += t.z;
     }
+}
+
+// Rotations of the iterate are R = Exp(theta) R0 (rot_gt).  A point's world
+// offset a = Exp(theta) R0 r moves by da = -[a]x J_l(theta) dtheta, so the
+// exact gradient of an energy of world points with respect to theta is
+// J_l(theta)^T sum_k a_k x g_k = J_r(theta) (torque): the lever-arm torque
+// (chain12) times the right Jacobian of SO(3),
+//   J_r(theta) = I - c1 [theta]x + c2 [theta]x^2,
+//   c1 = (1 - cos phi) / phi^2,  c2 = (phi - sin phi) / phi^3,  phi = |theta|,
+// with the series below phi = 1e-2 (truncation far below rounding).
+NX_HD void jr_coeffs(double phi, double& c1, double& c2) {
+    const double p2 = phi * phi;
+    if (phi < 1e-2) {
+        c1 = 0.5 - p2 * (1.0 / 24.0) + (p2 * p2) * (1.0 / 720.0);
+        c2 = 1.0 / 6.0 - p2 * (1.0 / 120.0) + (p2 * p2) * (1.0 / 5040.0);
+        return;
+    }
+    double sn, cs;
+    nxm::sincos(phi, &sn, &cs);
+    c1 = (1.0 - cs) / p2;
+    c2 = (phi - sn) / (p2 * phi);
+}
+// J_r(theta) v
+NX_HD V3 jr_apply(V3 th, V3 v) {
+    double c1, c2;
+    jr_coeffs(sqrt(dot(th, th)), c1, c2);
+    const V3 tv = cross(th, v);
+    return v - c1 * tv + c2 * cross(th, tv);
+}
+// chain12 with the exact rotation derivative: the rotational parts of body
+// A (out12[3..5]) and B (out12[9..11]) multiplied by J_r(theta_A), J_r(theta_B)
+NX_HD void chain12_exact(const V12& z, const int* side, const V3* arm, V3 thA, V3 thB, double* out12) {
+    chain12(z, side, arm, out12);
+    const V3 ta = jr_apply(thA, v3(out12[3], out12[4], out12[5]));
+    const V3 tb = jr_apply(thB, v3(out12[9], out12[10], out12[11]));
+    out12[3] = ta.x; out12[4] = ta.y; out12[5] = ta.z;
+    out12[9] = tb.x; out12[10] = tb.y; out12[11] = tb.z;
+}
+
+// ---- step adjoint helpers -------------------------------------------------
+// c1, c2 of J_r and their derivatives over phi: d1 = c1'(phi) / phi,
+// d2 = c2'(phi) / phi (series below phi = 1e-2).
+NX_HD void jr_coeffs_d(double phi, double& c1, double& c2, double& d1, double& d2) {
+    const double p2 = phi * phi;
+    if (phi < 1e-2) {
+        const double p4 = p2 * p2;
+        c1 = 0.5 - p2 * (1.0 / 24.0) + p4 * (1.0 / 720.0);
+        c2 = 1.0 / 6.0 - p2 * (1.0 / 120.0) + p4 * (1.0 / 5040.0);
+        d1 = -2.0 / 24.0 + p2 * (4.0 / 720.0) - p4 * (6.0 / 40320.0);
+        d2 = -2.0 / 120.0 + p2 * (4.0 / 5040.0) - p4 * (6.0 / 362880.0);
+        return;
+    }
+    double sn, cs;
+    nxm::sincos(phi, &sn, &cs);
+    const double p3 = p2 * phi, p4 = p2 * p2;
+    c1 = (1.0 - cs) / p2;
+    c2 = (phi - sn) / p3;
+    d1 = sn / p3 - 2.0 * (1.0 - cs) / p4;
+    d2 = (1.0 - cs) / p4 - 3.0 * (phi - sn) / (p4 * phi);
+}
+// 3 x 3 row-major helpers
+NX_HD void m3_skew(V3 v, double* S) {
+    S[0] = 0.0; S[1] = -v.z; S[2] = v.y;
+    S[3] = v.z; S[4] = 0.0; S[5] = -v.x;
+    S[6] = -v.y; S[7] = v.x; S[8] = 0.0;
+}
+NX_HD void m3_mul(const double* A, const double* B, double* C) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
+}
+// Exp(theta) as a matrix: I + sinc [t]x + c1 [t]x^2, and J_l(theta) =
+// I + c1 [t]x + c2 [t]x^2 (J_r = J_l^T).
+NX_HD void rot_exp_mats(V3 th, double* R, double* Jl) {
+    const double phi = sqrt(dot(th, th));
+    double c1, c2, d1, d2;
+    jr_coeffs_d(phi, c1, c2, d1, d2);
+    double sinc;
+    if (phi < 1e-2) { const double p2 = phi * phi; sinc = 1.0 - p2 * (1.0 / 6.0) + (p2 * p2) * (1.0 / 120.0); }
+    else { double sn, cs; nxm::sincos(phi, &sn, &cs); sinc = sn / phi; }
+    double S[9], S2[9];
+    m3_skew(th, S);
+    m3_mul(S, S, S2);
+    for (int e = 0; e < 9; ++e) {
+        const double id = (e % 4 == 0) ? 1.0 : 0.0;
+        R[e] = id + sinc * S[e] + c1 * S2[e];
+        Jl[e] = id + c1 * S[e] + c2 * S2[e];
+    }
+}
+// M = d(J_r(theta) tau)/dtheta at fixed tau, row-major:
+//   -(t x tau) (d1 t)^T + c1 [tau]x + (t x (t x tau)) (d2 t)^T
+//   + c2 ((t . tau) I + t tau^T - 2 tau t^T)
+NX_HD void jr_torque_derivative(V3 th, V3 tau, double* M) {
+    double c1, c2, d1, d2;
+    jr_coeffs_d(sqrt(dot(th, th)), c1, c2, d1, d2);
+    const V3 tt = cross(th, tau), ttt = cross(th, tt);
+    const double td = dot(th, tau);
+    const double t[3] = {th.x, th.y, th.z}, u[3] = {tau.x, tau.y, tau.z};
+    const double a[3] = {tt.x, tt.y, tt.z}, b[3] = {ttt.x, ttt.y, ttt.z};
+    double S[9];
+    m3_skew(tau, S);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            M[3 * i + j] = -(a[i] * (d1 * t[j])) + c1 * S[3 * i + j] + b[i] * (d2 * t[j]) +
+                           c2 * ((i == j ? td : 0.0) + t[i] * u[j] - 2.0 * (u[i] * t[j]));
 }
 
 // Additive CCD along linear point trajectories X + t P, t in [0, t_max]:

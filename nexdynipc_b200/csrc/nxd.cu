@@ -15,6 +15,7 @@
 #include "step.cuh"
 #include "batch.cuh"
 #include "ipc.cuh"
+#include "adjoint.cuh"
 #include "pcg.cuh"
 
 using namespace nx;
@@ -81,6 +82,7 @@ struct nxd_ctx {
     int pair_cap = 0;
     nxd_settings s{};
     std::vector<int> h_body_ids;
+    std::vector<int> h_jtype;
     std::vector<int> h_voff, h_foff, h_eoff;
     // static device data
     Geo geo{};
@@ -649,6 +651,7 @@ nxd_status nxd_create(const nxd_scene_desc* d, nxd_ctx** out) {
     c->mass = m.upload(d->mass, N);
     c->inertia = m.upload(d->inertia_body, (size_t)9 * N);
     c->jtype = m.upload(jtype.data(), c->J); c->ja = m.upload(ja.data(), c->J); c->jb = m.upload(jb.data(), c->J);
+    c->h_jtype.assign(jtype.begin(), jtype.end());
     c->jparams = m.upload(jparams.data(), jparams.size()); c->jmu = m.upload(jmu.data(), c->J);
     c->jlam = m.upload(jlam.data(), jlam.size());
     c->jinc_off = m.upload(jinc_off.data(), N + 1); c->jinc = m.upload(jinc.data(), jinc.size());
@@ -1326,10 +1329,13 @@ struct IpcState {
     IpcScal* ds() const { return scal.as<IpcScal>(); }
     int n_pt = 0, n_ee = 0;
     bool cand_swept = false;     // the last ipc_candidates_begin built swept boxes
+    bool pose_x = false;         // the last ipc_pose was at an iterate (x0 holds it)
     GrowBuf e, grad12, lam, z, nterm, body, active, type, apos, alist;
     GrowBuf gkey, gval, gkey1, gval1, hkey, hval, hkey1, hval1;
     GrowBuf sflag, spos, sstart, gout, rowptr, colidx, vals, toi;
     GrowBuf tkey, tval, tkey1, tval1;    // candidate pairs sorted by (query, primitive)
+    // step adjoint: per-pair blocks, dense K^T and K_phi, vectors, outputs
+    GrowBuf akp, akf, abody, aact, aK, aKphi, ax, axb, alam, aout, afail;
     // full-IPC time step: rest-form and merged BSR, gradients, solve scratch
     GrowBuf rrp, rci, rvv, mrp, mci, mvv, gr, gt, gneg, prod, xt, erow, items, iact, stat;
     PcgScratch pcg;
@@ -1341,7 +1347,7 @@ struct IpcState {
                 &grad12, &lam, &z, &nterm, &body, &active, &type, &apos, &alist, &gkey, &gval, &gkey1, &gval1, &hkey,
                 &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &rrp, &rci, &rvv,
                 &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &tkey, &tval,
-                &tkey1, &tval1};
+                &tkey1, &tval1, &akp, &akf, &abody, &aact, &aK, &aKphi, &ax, &axb, &alam, &aout, &afail};
     }
     void release() {
         for (GrowBuf* b : all()) b->release();
@@ -1406,6 +1412,7 @@ nxd_status ipc_pose(nxd_ctx* c, const double* x, const double* dx, bool on_devic
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     IPC_ENSURE(s->pp0, 24 * (size_t)N); IPC_ENSURE(s->pq0, 32 * (size_t)N); IPC_ENSURE(s->wq0, 24 * (size_t)c->nv);
     IPC_ENSURE(s->x0, 48 * (size_t)N);
+    s->pose_x = x != nullptr;
     if (x) {
         NXD_CUDA(cudaMemcpyAsync(s->x0.p, x, 48 * (size_t)N, kind, c->stream));
         k_pose_at_x<<<grid_for(N, 128), 128, 0, c->stream>>>(N, s->x0.as<double>(), c->quat, s->pp0.as<double>(), s->pq0.as<double>());
@@ -1644,7 +1651,7 @@ nxd_status ipc_barrier_eval(nxd_ctx* c, double dhat, double kappa, bool full, in
     IpcScal* ds = s->ds();
     const int N = c->N, n = s->n_pt + s->n_ee;
     const IpcPairs P{s->pt.as<int>(), s->n_pt, s->ee.as<int>(), s->n_ee};
-    const IpcPose ps{s->wq0.as<double>(), s->pp0.as<double>()};
+    const IpcPose ps{s->wq0.as<double>(), s->pp0.as<double>(), s->pose_x ? s->x0.as<double>() : nullptr};
     const size_t nn = std::max(n, 1);
     IPC_ENSURE(s->e, 8 * nn);
     if (!full) {
@@ -1732,7 +1739,7 @@ nxd_status ipc_trial_energy(nxd_ctx* c, const double* xt, double dhat, double ka
     if (st == NXD_OK) st = ipc_candidates_pass(c, false, dhat, 2);
     if (st != NXD_OK) return st;
     IpcScal* ds = s->ds();
-    const IpcPose ps{s->wq0.as<double>(), s->pp0.as<double>()};
+    const IpcPose ps{s->wq0.as<double>(), s->pp0.as<double>(), s->pose_x ? s->x0.as<double>() : nullptr};
     k_ipc_pair_energy_dev<<<grid_for((long long)cap_pt + cap_ee, 128), 128, 0, c->stream>>>(
         s->pg, s->pt.as<int>(), s->ee.as<int>(), ds->tot, cap_pt, cap_ee, ps, dhat, kappa, s->e.as<double>());
     k_tree_sum_pairs<<<1, 1024, 0, c->stream>>>(s->e.as<double>(), ds->tot, cap_pt, cap_ee, &ds->energy);
@@ -1986,6 +1993,73 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
         out->n_active = na; out->pcg_iterations = pcg_total;
     }
     return solvefail ? NXD_FACTOR_FAILED : NXD_OK;
+}
+
+nxd_status nxd_ipc_adjoint(nxd_ctx* c, double dt, const nxd_ipc_params* p, const nxd_state* start, const double* x_star,
+                           const double* x_bar, const nxd_ipc_adjoint_out* out) {
+    if (!c || !p || !start || !x_star || !x_bar || !out || !(dt > 0.0) || !(p->dhat > 0.0) || !(p->kappa >= 0.0))
+        return NXD_INVALID_ARGUMENT;
+    const int N = c->N, J = c->J, n6 = 6 * N;
+    if (N > kAdjMaxBodies || c->D > 0 || c->s.integrator == NXD_INTEGRATOR_IMPLICIT_NEWMARK) return NXD_INVALID_ARGUMENT;
+    for (int j = 0; j < J; ++j)
+        if (c->h_jtype[j] != NXD_JOINT_FIXED) return NXD_INVALID_ARGUMENT;
+    nxd_status st = nxd_set_state(c, start);
+    if (st != NXD_OK) return st;
+    if ((st = ipc_prepare(c)) != NXD_OK) return st;
+    IpcState* s = c->ipc;
+    cudaStream_t sm = c->stream;
+    StepCfg cfg = step_cfg(c);
+    cfg.enable_adaptive = 0;
+    cfg.enable_friction = 0;
+    // the step's predicted pose and step-start orientations, as nxd_ipc_step sets them
+    k_step_setup<<<grid_for(std::max(N, 1), 128), 128, 0, sm>>>(cfg, dt, c->pos, c->quat, c->vel, c->omega, c->lacc, c->aacc,
+        c->x, c->xhat, c->xprev, c->vprev, c->aprev, c->pos0, c->quat0, c->sc, c->dprm, c->dfilt, c->dfinit, c->dhas_prev);
+    IPC_ENSURE(s->ax, 8 * (size_t)n6); IPC_ENSURE(s->axb, 8 * (size_t)n6); IPC_ENSURE(s->alam, 8 * (size_t)n6);
+    NXD_CUDA(cudaMemcpyAsync(s->ax.p, x_star, 8 * (size_t)n6, cudaMemcpyHostToDevice, sm));
+    NXD_CUDA(cudaMemcpyAsync(s->axb.p, x_bar, 8 * (size_t)n6, cudaMemcpyHostToDevice, sm));
+    // candidates at x* (boxes inflated by dhat), each pair's exact blocks
+    st = ipc_pose(c, s->ax.as<double>(), nullptr, true);
+    if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
+    if (st != NXD_OK) return st;
+    const int np = s->n_pt + s->n_ee;
+    const size_t nn = std::max(np, 1);
+    IPC_ENSURE(s->akp, 1152 * nn); IPC_ENSURE(s->akf, 576 * nn); IPC_ENSURE(s->abody, 8 * nn); IPC_ENSURE(s->aact, 4 * nn);
+    IPC_ENSURE(s->aK, 8 * (size_t)n6 * n6); IPC_ENSURE(s->aKphi, 8 * (size_t)n6 * 3 * N);
+    IPC_ENSURE(s->aout, 8 * (size_t)(3 * N * 3 + N + 9 * N + std::max(J, 1))); IPC_ENSURE(s->afail, 4);
+    const IpcPairs P{s->pt.as<int>(), s->n_pt, s->ee.as<int>(), s->n_ee};
+    const IpcPose ps{s->wq0.as<double>(), s->pp0.as<double>(), s->ax.as<double>()};
+    if (np) k_ipc_pair_adjoint<<<grid_for(np, 64), 64, 0, sm>>>(s->pg, P, ps, p->dhat, p->kappa, s->akp.as<double>(),
+                                                                s->akf.as<double>(), s->abody.as<int>(), s->aact.as<int>());
+    AdjIn ai{N, J, c->mass, c->inertia, c->jtype, c->ja, c->jparams, c->jmu, c->quat0, s->ax.as<double>(), c->xhat, dt * dt};
+    k_adj_assemble<<<1, kAdjThreads, 0, sm>>>(ai, s->abody.as<int>(), s->aact.as<int>(), s->akp.as<double>(),
+                                              s->akf.as<double>(), np, s->aK.as<double>(), s->aKphi.as<double>());
+    k_adj_solve<<<1, kAdjThreads, 0, sm>>>(s->aK.as<double>(), s->axb.as<double>(), n6, s->alam.as<double>(),
+                                           s->afail.as<int>());
+    double* o = s->aout.as<double>();
+    AdjOut ao{o, o + 3 * N, o + 6 * N, o + 9 * N, o + 10 * N, o + 19 * N};
+    k_adj_cross<<<grid_for(std::max(3 * N, J), 128), 128, 0, sm>>>(ai, s->alam.as<double>(), s->aKphi.as<double>(), ao);
+    int fail = 0;
+    NXD_CUDA(cudaMemcpyAsync(&fail, s->afail.p, sizeof(int), cudaMemcpyDeviceToHost, sm));
+    const size_t n3 = 8 * 3 * (size_t)N;
+    const cudaMemcpyKind d2h = cudaMemcpyDeviceToHost;
+    if (out->lambda) NXD_CUDA(cudaMemcpyAsync(out->lambda, s->alam.p, 8 * (size_t)n6, d2h, sm));
+    if (out->phat_bar) NXD_CUDA(cudaMemcpyAsync(out->phat_bar, ao.phat_bar, n3, d2h, sm));
+    if (out->thetahat_bar) NXD_CUDA(cudaMemcpyAsync(out->thetahat_bar, ao.thetahat_bar, n3, d2h, sm));
+    if (out->phi_bar) NXD_CUDA(cudaMemcpyAsync(out->phi_bar, ao.phi_bar, n3, d2h, sm));
+    if (out->mass_bar) NXD_CUDA(cudaMemcpyAsync(out->mass_bar, ao.mass_bar, 8 * (size_t)N, d2h, sm));
+    if (out->inertia_bar) NXD_CUDA(cudaMemcpyAsync(out->inertia_bar, ao.inertia_bar, 8 * 9 * (size_t)N, d2h, sm));
+    if (out->joint_mu_bar && J) NXD_CUDA(cudaMemcpyAsync(out->joint_mu_bar, ao.joint_mu_bar, 8 * (size_t)J, d2h, sm));
+    if (out->n_active) {
+        NXD_CUDA(cudaStreamSynchronize(sm));
+        std::vector<int> act(np);
+        if (np) NXD_CUDA(cudaMemcpy(act.data(), s->aact.p, 4 * (size_t)np, cudaMemcpyDeviceToHost));
+        int na = 0;
+        for (int a : act) na += a;
+        *out->n_active = na;
+    }
+    NXD_CUDA(cudaStreamSynchronize(sm));
+    NXD_CUDA(cudaGetLastError());
+    return fail ? NXD_FACTOR_FAILED : NXD_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -76,6 +76,9 @@ def lib():
     L.nxd_batch_set_stream.restype = C.c_int
     L.nxd_body_pairs_noalloc.argtypes = [vp, vp, vp, C.c_int32, C.c_double, vp, C.c_int64, i64p, vp]
     L.nxd_body_pairs_noalloc.restype = C.c_int
+    L.nxd_ipc_adjoint.argtypes = [vp, C.c_double, C.POINTER(abi.NxdIpcParams), C.POINTER(abi.NxdState), dp, dp,
+                                  C.POINTER(abi.NxdIpcAdjointOut)]
+    L.nxd_ipc_adjoint.restype = C.c_int
     L.nxd_debug_grid_wait.argtypes = [vp, C.c_uint32, C.c_int32]
     L.nxd_debug_grid_wait.restype = C.c_int
     L.nxd_fp64_peak.argtypes = [vp, dp, dp]
@@ -352,6 +355,29 @@ class Context:
         _check("nxd_ipc_step", lib().nxd_ipc_step(self.h, float(self.scene.dt if dt is None else dt), C.byref(p),
                                                   C.byref(st)))
         return st.as_dict()
+
+    def ipc_adjoint(self, start: dict, x_star, x_bar, params=None, dt=None) -> dict:
+        """nxd_ipc_adjoint: the adjoint of one full-IPC step from the state
+        `start` at its converged iterate x_star (6N) for x_bar = dL/dx_star.
+        Returns lam (6N), phat_bar / thetahat_bar / phi_bar (N, 3), mass_bar
+        (N), inertia_bar (N, 3, 3), joint_mu_bar (J), n_active."""
+        n, nj = self.scene.n_bodies, len(self.scene.joint_type)
+        p = params if params is not None else abi.ipc_params()
+        sb = abi.StateBuffers(n).load(start)
+        view = sb.view()
+        xs = np.ascontiguousarray(x_star, dtype=np.float64)
+        xb = np.ascontiguousarray(x_bar, dtype=np.float64)
+        out = {"lam": np.zeros(6 * n), "phat_bar": np.zeros((n, 3)), "thetahat_bar": np.zeros((n, 3)),
+               "phi_bar": np.zeros((n, 3)), "mass_bar": np.zeros(n), "inertia_bar": np.zeros((n, 3, 3)),
+               "joint_mu_bar": np.zeros(max(nj, 1))}
+        na = C.c_int32(0)
+        o = abi.NxdIpcAdjointOut(*[abi.dptr(out[k]) for k in ("lam", "phat_bar", "thetahat_bar", "phi_bar", "mass_bar",
+                                                                "inertia_bar", "joint_mu_bar")], C.pointer(na))
+        _check("nxd_ipc_adjoint", lib().nxd_ipc_adjoint(self.h, float(self.scene.dt if dt is None else dt), C.byref(p),
+                                                        C.byref(view), abi.dptr(xs), abi.dptr(xb), C.byref(o)))
+        out["joint_mu_bar"] = out["joint_mu_bar"][:nj]
+        out["n_active"] = na.value
+        return out
 
     def ipc_max_step(self, x, dx, eta: float = 0.1):
         """(alpha, n_pairs): additive-CCD bound of the step x -> x + dx."""

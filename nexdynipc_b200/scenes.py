@@ -601,6 +601,27 @@ def diff_scene(seed: int = 5000) -> Scene:
     return sb.build(_settings(1e-3, 0.3), dt=1e-2, steps=50)
 
 
+def diff_ipc_scene(seed: int = 5000, n_spheres: int = 16, subdiv: int = 2) -> Scene:
+    """The differentiable configuration for the full-IPC step and its
+    adjoint: diff_scene's 16 icospheres (162 V) over a ground box, the ground
+    held by a FixedJoint of stiffness 1e5 (its sag under the spheres stays
+    below 1e-5 m, and the joint does not amplify rounding the way 1e8 does),
+    COM-distance contact forms off (nxd_ipc_step), dt 1e-2, 50 steps."""
+    rng = np.random.default_rng(seed)
+    sb = SceneBuilder("diff_ipc_spheres")
+    gv, gf = box_mesh(2.0, 0.1, 2.0)
+    g = sb.add_body(gv, gf, (0.0, -0.1, 0.0))
+    sb.fix(g, stiffness=1e5)
+    iv, if_ = icosphere(subdiv)
+    for i in range(n_spheres):
+        sb.add_body(iv * 0.1, if_, (-0.6 + 0.4 * (i % 4), 0.12 + 0.05 * rng.random(), -0.6 + 0.4 * (i // 4)),
+                    quat=random_quaternion(rng), vel=rng.normal(0, 0.3, size=3))
+    s = _settings(1e-3, 0.0)
+    s.enable_adaptive_barrier = 0
+    s.enable_friction = 0
+    return sb.build(s, dt=1e-2, steps=50)
+
+
 def double_pendulum(dt: float = 1e-3, max_time: float = 1.5, inertia_zz=(1.0, 1.0)) -> Scene:
     """The reference's double-pendulum regression case as its scene loader
     builds it (nexdynipc/assets/double_pendulum/double_pendulum.json through

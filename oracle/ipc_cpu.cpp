@@ -30,6 +30,7 @@ struct Geo {
     int N = 0;
     std::vector<int32_t> vbody, fbody, fvert, ebody, evert;
     std::vector<double> wv, wv1, pos;
+    std::vector<double> theta;   // [3N] rotation vectors of the iterate (zeros without one)
 };
 
 Geo load(nxo_world* w, const double* x, const double* dx) {
@@ -40,6 +41,10 @@ Geo load(nxo_world* w, const double* x, const double* dx) {
     nxo_prim_topology(w, g.vbody.data(), g.fbody.data(), g.fvert.data(), g.ebody.data(), g.evert.data());
     g.wv.resize(3 * g.nv); g.pos.resize(3 * g.N);
     nxo_world_vertices_at(w, x, g.wv.data(), g.pos.data());
+    g.theta.assign(3 * (size_t)g.N, 0.0);
+    if (x)
+        for (int b = 0; b < g.N; ++b)
+            for (int k = 0; k < 3; ++k) g.theta[3 * b + k] = x[6 * b + 3 + k];
     if (dx) {
         std::vector<double> x1(6 * (size_t)g.N);
         for (size_t i = 0; i < x1.size(); ++i) x1[i] = x[i] + dx[i];
@@ -243,14 +248,15 @@ int ipc_barrier_cpu(nxo_world* w, const double* x, double dhat, double kappa, do
             blocks->push_back({bB, bA}); blocks->push_back({bB, bB});
         }
         double g12[12];
-        ipc::chain12(ev.grad, side, arm, g12);
+        const V3 thA = nx::ld3(&g.theta[3 * bA]), thB = nx::ld3(&g.theta[3 * bB]);
+        ipc::chain12_exact(ev.grad, side, arm, thA, thB, g12);
         const int b[2] = {bA, bB};
         if (grad)
             for (int s = 0; s < 2; ++s)
                 for (int d = 0; d < 6; ++d) grad[6 * b[s] + d] += g12[6 * s + d];
         if (!H) continue;
         double z[5][12];
-        for (int k = 0; k < ev.n_terms; ++k) ipc::chain12(ev.y[k], side, arm, z[k]);
+        for (int k = 0; k < ev.n_terms; ++k) ipc::chain12_exact(ev.y[k], side, arm, thA, thB, z[k]);
         for (int r = 0; r < 2; ++r)
             for (int c = 0; c < 2; ++c)
                 for (int i = 0; i < 6; ++i)

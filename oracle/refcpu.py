@@ -82,6 +82,11 @@ def lib():
     L.nxo_ipc_pair.argtypes = [C.c_int32, dp, C.c_double, C.c_double, dp, ip, dp, dp, dp, dp, dp]
     L.nxo_ipc_accd.restype = C.c_double
     L.nxo_ipc_accd.argtypes = [C.c_int32, dp, dp, C.c_double, C.c_double, C.c_int32, ip]
+    L.nxo_body_count.restype = C.c_int32
+    L.nxo_body_count.argtypes = [vp]
+    L.nxo_prim_counts.argtypes = [vp, i64p, i64p, i64p]
+    L.nxo_prim_topology.argtypes = [vp, ip, ip, ip, ip, ip]
+    L.nxo_world_vertices_at.argtypes = [vp, dp, dp, dp]
     L.nxo_ipc_dist2.restype = C.c_double
     L.nxo_ipc_dist2.argtypes = [C.c_int32, dp]
     _lib = L
@@ -245,6 +250,30 @@ class OracleWorld:
         out = st.as_dict()
         out["status"] = int(rc)
         return out
+
+    def prim_topology(self):
+        """(vbody, fbody, fvert [nf, 3], ebody, evert [ne, 2]): the global
+        primitive numbering of the full-IPC model (edges in first-seen order
+        per body), as the device numbers them."""
+        L = lib()
+        nv, nf, ne = C.c_int64(), C.c_int64(), C.c_int64()
+        L.nxo_prim_counts(self.h, C.byref(nv), C.byref(nf), C.byref(ne))
+        vb = np.zeros(max(nv.value, 1), np.int32); fb = np.zeros(max(nf.value, 1), np.int32)
+        fv = np.zeros((max(nf.value, 1), 3), np.int32); eb = np.zeros(max(ne.value, 1), np.int32)
+        ev = np.zeros((max(ne.value, 1), 2), np.int32)
+        L.nxo_prim_topology(self.h, abi.iptr(vb), abi.iptr(fb), abi.iptr(fv), abi.iptr(eb), abi.iptr(ev))
+        return vb[:nv.value], fb[:nf.value], fv[:nf.value], eb[:ne.value], ev[:ne.value]
+
+    def world_vertices_at(self, x):
+        """(world vertices [nv, 3], body positions [N, 3]) at the iterate x
+        (rotations exp(theta) applied to the world's current orientations)."""
+        L = lib()
+        nv, nf, ne = C.c_int64(), C.c_int64(), C.c_int64()
+        L.nxo_prim_counts(self.h, C.byref(nv), C.byref(nf), C.byref(ne))
+        wv = np.zeros((max(nv.value, 1), 3))
+        pos = np.zeros((self.n, 3))
+        L.nxo_world_vertices_at(self.h, _d(x), abi.dptr(wv), abi.dptr(pos))
+        return wv[:nv.value], pos
 
     def ipc_max_step(self, x, dx, eta: float = 0.1):
         n = C.c_int64()

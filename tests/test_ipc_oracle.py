@@ -250,3 +250,35 @@ def test_oracle_barrier_gradient_finite_differences():
         assert abs(fd - g[i]) <= 1e-4 * max(abs(g).max(), 1e-12), (i, fd, g[i])
     assert np.abs(H - H.T).max() <= 1e-12 * np.abs(H).max()
     assert np.linalg.eigvalsh(H).min() >= -1e-9 * np.abs(H).max()
+
+
+def test_oracle_barrier_gradient_exact_under_large_rotation_vectors():
+    # Each body's orientation is rewound by Exp(-theta0) and the iterate
+    # carries theta0 (|theta0| ~ 0.3 rad): the same world poses, so the
+    # contacts stay active, but the rotation derivative is now far from the
+    # lever arm; the chained gradient (torque times J_r(theta)) must still
+    # equal finite differences of the energy.
+    from oracle.ipc_adjoint import quat_mul
+    sc = scenes.cube_stack()
+    ow = refcpu.OracleWorld(sc)
+    rng = np.random.default_rng(4)
+    x = scene_x(sc, rng, 1e-4)
+    st = sc.initial_state()
+    for i in range(sc.n_bodies):
+        th0 = rng.normal(0, 0.2, 3)
+        a = np.linalg.norm(th0)
+        inv = np.concatenate([[np.cos(a / 2)], -np.sin(a / 2) * th0 / a])
+        st["orientation"][i] = quat_mul(inv, st["orientation"][i])
+        x[6 * i + 3:6 * i + 6] += th0
+    ow.set_state(st)
+    dhat, kappa = 1e-3, 1e4
+    e, g, H, npairs, nact = ow.ipc_barrier(x, dhat, kappa)
+    assert nact > 0 and e > 0
+    h = 1e-7
+    rot = [6 * i + 3 + k for i in range(1, sc.n_bodies) for k in range(3)]
+    for i in rng.choice(rot, 12, replace=False):
+        xp, xm = x.copy(), x.copy()
+        xp[i] += h
+        xm[i] -= h
+        fd = (ow.ipc_barrier(xp, dhat, kappa, hessian=False)[0] - ow.ipc_barrier(xm, dhat, kappa, hessian=False)[0]) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * max(abs(g).max(), 1e-12), (i, fd, g[i])
