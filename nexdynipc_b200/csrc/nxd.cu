@@ -1731,8 +1731,15 @@ nxd_status ipc_trial_energy(nxd_ctx* c, const double* xt, double dhat, double ka
     auto room = [](GrowBuf& b, size_t want) { return want <= b.cap || b.ensure(std::max(want, 2 * b.cap)); };
     if (!room(s->pt, 16 * (size_t)std::max(s->n_pt, 16)) || !room(s->ee, 16 * (size_t)std::max(s->n_ee, 16)))
         return NXD_CUDA_ERROR;
-    const int cap_pt = (int)std::min<size_t>(s->pt.cap / 8, (size_t)1 << 30);
-    const int cap_ee = (int)std::min<size_t>(s->ee.cap / 8, (size_t)1 << 30);
+    int cap_pt = (int)std::min<size_t>(s->pt.cap / 8, (size_t)1 << 30);
+    int cap_ee = (int)std::min<size_t>(s->ee.cap / 8, (size_t)1 << 30);
+    // test hook: NXD_IPC_TRIAL_CAP=<pairs> caps both lists, so that trials
+    // whose candidates exceed it take the overflow path (same results)
+    if (const char* tc = std::getenv("NXD_IPC_TRIAL_CAP")) {
+        const int lim = std::max(0, std::atoi(tc));
+        cap_pt = std::min(cap_pt, lim);
+        cap_ee = std::min(cap_ee, lim);
+    }
     if (!room(s->e, 8 * ((size_t)cap_pt + (size_t)cap_ee))) return NXD_CUDA_ERROR;
     nxd_status st = ipc_pose(c, xt, nullptr, true);
     if (st == NXD_OK) st = ipc_candidates_begin(c, false, dhat);

@@ -77,6 +77,31 @@ def test_device_ipc_step_matches_oracle():
 
 
 @pytest.mark.gpu
+def test_device_ipc_step_trial_overflow_path_matches_oracle(monkeypatch):
+    # every line-search trial's candidate lists forced over their capacity
+    # (NXD_IPC_TRIAL_CAP=0): each trial takes the two-wait fallback, and the
+    # step must still equal the oracle's bit for bit
+    from nexdynipc_b200 import runtime
+    monkeypatch.setenv("NXD_IPC_TRIAL_CAP", "0")
+    sc = scenes.ipc_drop(n_cubes=3)
+    ctx = runtime.Context(sc)
+    ow = refcpu.OracleWorld(sc)
+    p = abi.ipc_params(**PARAMS)
+    trials = 0
+    for k in range(30):
+        sg = ctx.ipc_step(p)
+        so = ow.ipc_step(p)
+        assert sg["newton_iterations"] == so["newton_iterations"], (k, sg, so)
+        assert sg["n_active"] == so["n_active"] and sg["converged"] == so["converged"]
+        a, b = ctx.state(), ow.state()
+        assert np.array_equal(a["position"], b["position"]), k
+        assert np.array_equal(a["orientation"], b["orientation"]), k
+        trials += sg["newton_iterations"]
+    assert trials > 0
+    assert ctx.diagnostics()["status"] == 0
+
+
+@pytest.mark.gpu
 def test_device_ipc_step_with_pcg_tracks_the_direct_solve():
     # the same step with block-Jacobi PCG (tolerance 1e-13) for the Newton
     # systems stays on the oracle's direct-solve trajectory
