@@ -698,8 +698,10 @@ def main():
     ach = nb * newton_iters / (prof_ms[FAMILIES.index("newton")] / 1e3) / 1e9
     roof_newton.update(achieved=ach, frac=ach / peak, algorithmic_bytes_per_newton_iteration=nb,
                        newton_iterations=newton_iters,
-                       note=("latency-bound: one Newton solve per ALM iteration on a cooperative grid of CTAs, "
-                             "about 25 grid barriers per Newton iteration; HBM is not the limiter"))
+                       note=("latency-bound: one Newton solve per ALM iteration on a 16-CTA thread-block cluster "
+                             "(hardware cluster barrier); phases wait on latency chains (joint Jacobians, trial "
+                             "energies, one-warp factorisation of the hopper's star component); under 1 MB of DRAM "
+                             "per launch, HBM is not the limiter"))
     roof_narrow = family_roof(FAMILIES.index("narrow_phase"))
     roof_narrow["traffic"] = traffic.get("k_narrow_rows")
     if cand_counts:
