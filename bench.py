@@ -400,57 +400,74 @@ def pcg_leg(n_bodies: int = 200000, iters: int = 60):
 
 
 def ipc_step_params(solver: int = 0):
-    from nexdynipc_b200 import abi
-    return abi.ipc_params(dhat=1e-3, kappa=1e11, eta=0.1, newton_tol=1e-5, newton_max_iters=50, ls_max_iters=30,
-                          linear_solver=solver, pcg_max_iter=500, pcg_tol=1e-12)
+    from nexdynipc_b200 import abi, scenes
+    return abi.ipc_params(**scenes.ipc_step_settings(solver))
 
 
-def ipc_step_leg(n_cubes: int = 8, columns: int = 1, settle: int = 30, steps: int = 20, solver: int = 0):
-    """Full-IPC time step (nxd_ipc_step) on stacks of tilted cubes falling
-    onto a ground box: after `settle` steps (the cubes in contact), wall
+def ipc_step_leg(n_cubes: int = 8, columns: int = 1, settle: int = 30, steps: int = 20, solver: int = 0,
+                 bowl: bool = False):
+    """Full-IPC time step (nxd_ipc_step): after `settle` untimed steps, wall
     clock of `steps` steps, each a host-ordered Newton loop of device calls
-    (candidates, barrier, rest forms, block solve, CCD bound, line search)."""
+    (candidates, barrier, rest forms, block solve, CCD bound, line search).
+    The scene is stacks of tilted cubes falling onto a ground box, or with
+    `bowl` the 64-sphere bowl configuration (642-vertex icospheres, 1280-face
+    bowl).  Per-step wall times are kept so that a CPU sample of the first
+    steps can be compared step for step."""
     import time
     from nexdynipc_b200 import runtime, scenes
-    sc = scenes.ipc_drop(n_cubes=n_cubes, columns=columns)
+    sc = scenes.sphere_bowl() if bowl else scenes.ipc_drop(n_cubes=n_cubes, columns=columns)
     ctx = runtime.Context(sc)
     p = ipc_step_params(solver)
     for _ in range(settle):
         ctx.ipc_step(p)
-    its, act, pairs, conv, lsf = [], [], [], 0, 0
+    its, act, pairs, conv, lsf, walls = [], [], [], 0, 0, []
     t0 = time.perf_counter()
     for _ in range(steps):
+        t1 = time.perf_counter()
         st = ctx.ipc_step(p)
+        walls.append(time.perf_counter() - t1)
         its.append(st["newton_iterations"]); act.append(st["n_active"]); pairs.append(st["n_pairs"])
         conv += st["converged"]
         lsf += st["line_search_failed"]
     wall = time.perf_counter() - t0
     ctx.close()
-    return {"workload": (f"{n_cubes} tilted 0.2 m cubes in {columns} stack(s) on a ground box, dhat 1e-3, "
-                         f"kappa 1e11, dt {sc.dt}; steps {settle + 1}-{settle + steps}"),
+    if bowl:
+        workload = (f"{sc.n_bodies - 1} icospheres (642 V) falling into a 1280-face bowl, full IPC, dhat 1e-3, "
+                    f"kappa 1e11, dt {sc.dt}; steps {settle + 1}-{settle + steps}")
+    else:
+        workload = (f"{n_cubes} tilted 0.2 m cubes in {columns} stack(s) on a ground box, dhat 1e-3, "
+                    f"kappa 1e11, dt {sc.dt}; steps {settle + 1}-{settle + steps}")
+    return {"workload": workload,
             "steps": steps, "steps_per_s": steps / wall, "newton_iterations_mean": float(np.mean(its)),
             "active_pairs_mean": float(np.mean(act)), "candidate_pairs_mean": float(np.mean(pairs)),
             "converged_steps": conv, "line_search_failures": lsf,
+            "step_ms": [round(1e3 * w, 3) for w in walls[:4]],
             "linear_solver": "block-Jacobi PCG" if solver else "component LDL^T",
             "timing": "wall clock per nxd_ipc_step (it synchronises)"}
 
 
-def ipc_step_cpu_baseline(n_cubes: int, columns: int, settle: int, steps: int):
-    """The CPU oracle's full-IPC step (serial) on the same trajectory segment
-    as ipc_step_leg: `settle` untimed steps, then wall clock of `steps`."""
+def ipc_step_cpu_baseline(n_cubes: int, columns: int, settle: int, steps: int, bowl: bool = False):
+    """The CPU oracle's full-IPC step on the same trajectory segment as
+    ipc_step_leg: `settle` untimed steps, then wall clock of `steps`.  The
+    oracle's candidate search runs on all host threads (OpenMP), the rest of
+    its step on one."""
     from nexdynipc_b200 import scenes
     from oracle.refcpu import OracleWorld
-    ow = OracleWorld(scenes.ipc_drop(n_cubes=n_cubes, columns=columns))
+    ow = OracleWorld(scenes.sphere_bowl() if bowl else scenes.ipc_drop(n_cubes=n_cubes, columns=columns))
     p = ipc_step_params(0)
     for _ in range(settle):
         ow.ipc_step(p)
     t0 = time.perf_counter()
-    its = 0
+    its, walls = 0, []
     for _ in range(steps):
+        t1 = time.perf_counter()
         its += ow.ipc_step(p)["newton_iterations"]
+        walls.append(time.perf_counter() - t1)
     wall = time.perf_counter() - t0
-    return {"steps_per_s": steps / wall, "cores": 1, "kind": "port", "newton_iterations_mean": its / steps,
-            "sample": f"the same {steps} steps through the CPU oracle's nxo_ipc_step (serial), {wall:.2f} s wall"}
+    return {"steps_per_s": steps / wall, "cores": os.cpu_count() or 1, "kind": "port", "newton_iterations_mean": its / steps,
+            "step_ms": [round(1e3 * w, 1) for w in walls],
+            "sample": (f"steps {settle + 1}-{settle + steps} through the CPU oracle's nxo_ipc_step (candidate search "
+                       f"on all host threads, the rest serial), {wall:.2f} s wall")}
 
 
 def mode_i_leg(ctx, sc, reps: int = 5):
@@ -752,6 +769,7 @@ def main():
         mode_i["step"] = ipc_step_leg()
         mode_i["step_pcg"] = ipc_step_leg(solver=1)
         mode_i["step_64"] = ipc_step_leg(n_cubes=64, columns=16, settle=30, steps=10)
+        mode_i["step_bowl"] = ipc_step_leg(settle=0, steps=40, bowl=True)
 
     batched = None
     if not args.no_batched:
@@ -772,6 +790,7 @@ def main():
         if mode_i is not None:
             mode_i["step"]["cpu_baseline"] = ipc_step_cpu_baseline(8, 1, 30, 20)
             mode_i["step_64"]["cpu_baseline"] = ipc_step_cpu_baseline(64, 16, 30, 10)
+            mode_i["step_bowl"]["cpu_baseline"] = ipc_step_cpu_baseline(0, 0, 0, 2, bowl=True)
     launches_total = int(timed_n.sum())
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,

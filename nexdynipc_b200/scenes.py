@@ -587,6 +587,16 @@ def ipc_drop(seed: int = 7000, n_cubes: int = 2, columns: int = 1) -> Scene:
     return sb.build(s, dt=1e-2, steps=80)
 
 
+def ipc_step_settings(solver: int = 0) -> dict:
+    """Keyword arguments of abi.ipc_params for the full-IPC steps run on
+    ipc_drop and on sphere_bowl: dhat 1e-3, kappa 1e11, eta 0.1 (the CCD
+    bound keeps 90 % of each pair's distance), Newton until |g|_inf < 1e-5
+    (or the step below 1e-5 dt) in at most 50 iterations, 30 Armijo trials;
+    solver 0 = component LDL^T, 1 = block-Jacobi PCG (500 iterations, 1e-12)."""
+    return dict(dhat=1e-3, kappa=1e11, eta=0.1, newton_tol=1e-5, newton_max_iters=50, ls_max_iters=30,
+                linear_solver=solver, pcg_max_iter=500, pcg_tol=1e-12)
+
+
 def diff_scene(seed: int = 5000) -> Scene:
     """16 icospheres (162 V) colliding on a ground box, dt 1e-2, 50 steps."""
     rng = np.random.default_rng(seed)

@@ -5,7 +5,7 @@
 // the published method (Li et al. 2020 IPC; Li et al. 2021 additive CCD)
 // with the per-pair arithmetic shared with the kernels (ipc_pair.h), and
 // checks everything around it independently:
-//   - candidate sets by an exact sweep over x-sorted boxes (no BVH);
+//   - candidate sets by an exact uniform-grid search over the boxes (no BVH);
 //   - the subspace PSD projection against a full 12x12 Jacobi projection
 //     of the raw pair Hessian (nxo_ipc_pair);
 //   - derivatives by finite differences (in tests/).
@@ -74,35 +74,83 @@ bool overlap(const Box& a, const Box& b) {
 }
 
 // All (query, leaf) pairs with overlapping boxes that `keep` accepts, query
-// ascending, leaf ascending: leaves sorted by min x; a query scans the
-// leaves whose min x lies in [q.min.x - widest, q.max.x]; leaves much wider
-// than the typical one are tested against every query.
+// ascending, leaf ascending, by a uniform grid over the leaves: cells of
+// twice the median leaf extent, each leaf listed in every cell its box
+// touches (CSR lists), each query gathering the leaves of the cells its box
+// touches; leaves much larger than the typical one are tested against every
+// query.  Every accepted pair is tested on the boxes themselves, so the set
+// is the exact all-pairs set whatever the cell size.
 template <typename Keep>
 std::vector<int32_t> sweep(const std::vector<Box>& q, const std::vector<Box>& leaf, Keep keep) {
-    std::vector<double> widths;
-    for (const Box& b : leaf) widths.push_back(b.mx[0] - b.mn[0]);
-    std::vector<double> ws = widths;
-    std::sort(ws.begin(), ws.end());
-    const double typical = ws.empty() ? 0.0 : ws[ws.size() / 2];
+    const int nl = (int)leaf.size();
+    std::vector<double> ext(nl);
+    for (int i = 0; i < nl; ++i)
+        ext[i] = std::max({leaf[i].mx[0] - leaf[i].mn[0], leaf[i].mx[1] - leaf[i].mn[1], leaf[i].mx[2] - leaf[i].mn[2]});
+    std::vector<double> es = ext;
+    std::sort(es.begin(), es.end());
+    const double typical = es.empty() ? 0.0 : es[es.size() / 2];
     std::vector<int> small, big;
-    for (int i = 0; i < (int)leaf.size(); ++i) (widths[i] > 8.0 * typical + 1e-12 ? big : small).push_back(i);
-    std::sort(small.begin(), small.end(), [&](int a, int b) { return leaf[a].mn[0] < leaf[b].mn[0] || (leaf[a].mn[0] == leaf[b].mn[0] && a < b); });
-    double widest = 0.0;
-    std::vector<double> smin;
-    for (int i : small) { widest = std::max(widest, widths[i]); smin.push_back(leaf[i].mn[0]); }
+    for (int i = 0; i < nl; ++i) (ext[i] > 8.0 * typical + 1e-12 ? big : small).push_back(i);
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    for (size_t k = 0; k < small.size(); ++k)
+        for (int d = 0; d < 3; ++d) {
+            const Box& b = leaf[small[k]];
+            lo[d] = k ? std::min(lo[d], b.mn[d]) : b.mn[d];
+            hi[d] = k ? std::max(hi[d], b.mx[d]) : b.mx[d];
+        }
+    double h = std::max(2.0 * typical, 1e-9);
+    int64_t dim[3];
+    for (;;) {
+        for (int d = 0; d < 3; ++d) dim[d] = std::max<int64_t>(1, (int64_t)std::floor((hi[d] - lo[d]) / h) + 1);
+        if (dim[0] * dim[1] * dim[2] <= (int64_t)1 << 22) break;
+        h *= 2.0;
+    }
+    auto cell = [&](double v, int d) {
+        const int64_t c = (int64_t)std::floor((v - lo[d]) / h);
+        return std::min<int64_t>(std::max<int64_t>(c, 0), dim[d] - 1);
+    };
+    const int64_t ncell = dim[0] * dim[1] * dim[2];
+    std::vector<int64_t> start(ncell + 1, 0);
+    std::vector<int32_t> items;
+    for (int pass = 0; pass < 2; ++pass) {
+        std::vector<int64_t> fill;
+        if (pass == 1) {
+            for (int64_t c = 0; c < ncell; ++c) start[c + 1] += start[c];
+            items.resize(start[ncell]);
+            fill.assign(start.begin(), start.end() - 1);
+        }
+        for (int i : small) {
+            const Box& b = leaf[i];
+            for (int64_t z = cell(b.mn[2], 2); z <= cell(b.mx[2], 2); ++z)
+                for (int64_t y = cell(b.mn[1], 1); y <= cell(b.mx[1], 1); ++y)
+                    for (int64_t x = cell(b.mn[0], 0); x <= cell(b.mx[0], 0); ++x) {
+                        const int64_t c = (z * dim[1] + y) * dim[0] + x;
+                        if (pass == 0) ++start[c + 1];
+                        else items[fill[c]++] = i;
+                    }
+        }
+    }
     std::vector<std::vector<int32_t>> hits(q.size());
 #pragma omp parallel for schedule(dynamic, 256)
     for (long long qi = 0; qi < (long long)q.size(); ++qi) {
         const Box& Q = q[qi];
-        std::vector<int32_t>& h = hits[qi];
-        const auto lo = std::lower_bound(smin.begin(), smin.end(), Q.mn[0] - widest) - smin.begin();
-        for (size_t k = lo; k < small.size() && smin[k] <= Q.mx[0]; ++k) {
-            const int L = small[k];
-            if (overlap(Q, leaf[L]) && keep((int)qi, L)) h.push_back(L);
-        }
+        std::vector<int32_t>& hv = hits[qi];
+        bool outside = small.empty();
+        for (int d = 0; d < 3; ++d) outside = outside || Q.mx[d] < lo[d] || Q.mn[d] > hi[d];
+        if (!outside)
+            for (int64_t z = cell(Q.mn[2], 2); z <= cell(Q.mx[2], 2); ++z)
+                for (int64_t y = cell(Q.mn[1], 1); y <= cell(Q.mx[1], 1); ++y)
+                    for (int64_t x = cell(Q.mn[0], 0); x <= cell(Q.mx[0], 0); ++x) {
+                        const int64_t c = (z * dim[1] + y) * dim[0] + x;
+                        for (int64_t k = start[c]; k < start[c + 1]; ++k) {
+                            const int L = items[k];
+                            if (overlap(Q, leaf[L]) && keep((int)qi, L)) hv.push_back(L);
+                        }
+                    }
         for (int L : big)
-            if (overlap(Q, leaf[L]) && keep((int)qi, L)) h.push_back(L);
-        std::sort(h.begin(), h.end());
+            if (overlap(Q, leaf[L]) && keep((int)qi, L)) hv.push_back(L);
+        std::sort(hv.begin(), hv.end());
+        hv.erase(std::unique(hv.begin(), hv.end()), hv.end());
     }
     std::vector<int32_t> out;
     for (size_t qi = 0; qi < q.size(); ++qi)

@@ -8,7 +8,10 @@ literal loop's) on all host threads:
 * ``traj_hopper_chains.npz`` -- 1024 hulls + 32 hinge chains (1313 bodies),
   100 steps of dt 5e-3;
 * ``traj_sphere_bowl.npz``   -- 64 icospheres (642 V) in the bowl, 200 steps;
-* ``traj_batched.npz``       -- the 256 uneven scenes, 100 steps each.
+* ``traj_batched.npz``       -- the 256 uneven scenes, 100 steps each;
+* ``traj_ipc_sphere_bowl.npz`` -- the same 64-sphere bowl stepped by the
+  full-IPC step (primitive-pair barrier, additive-CCD line search; the
+  oracle's nxo_ipc_step with scenes.ipc_step_settings()), its first 40 steps.
 
 Stored per fixture: positions and orientations at the checkpoint steps, and
 for every step the adaptive stiffness kappa, the contact count, the ALM and
@@ -17,7 +20,11 @@ bodies), so a device run can be compared with the oracle at every step
 without storing every state.  The batched fixture keeps the states of steps
 50 and 100 and the per-scene fingerprints every 10 steps.
 
-Usage: python tests/golden/make_trajectory_goldens.py [hopper|bowl|batched ...]
+The full-IPC fixture stores, for every step, the Newton iteration count, the
+convergence and line-search flags, the active and candidate pair counts and
+the full body state (positions, orientations).
+
+Usage: python tests/golden/make_trajectory_goldens.py [hopper|bowl|batched|ipc_bowl ...]
 (about 8 minutes for the hopper on 8 threads, a few minutes for the others).
 """
 from __future__ import annotations
@@ -115,6 +122,32 @@ def make_batched(path):
                         state_50=s50, state_100=s100)
 
 
+IPC_STAT_KEYS = ("newton_iterations", "converged", "line_search_failed", "n_active", "n_pairs")
+
+
+def run_ipc(sc, steps):
+    from nexdynipc_b200 import abi
+    from oracle import refcpu
+    ow = refcpu.OracleWorld(sc)
+    p = abi.ipc_params(**scenes.ipc_step_settings())
+    out = {k: np.zeros(steps, np.int64) for k in IPC_STAT_KEYS}
+    pos, quat = [], []
+    t0 = time.time()
+    for s in range(steps):
+        st = ow.ipc_step(p)
+        assert st["status"] == 0, (s, st)
+        for k in IPC_STAT_KEYS:
+            out[k][s] = st[k]
+        S = ow.state()
+        pos.append(S["position"])
+        quat.append(S["orientation"])
+        if (s + 1) % 10 == 0:
+            print(f"  {sc.name} (full IPC): step {s + 1}/{steps}, {time.time() - t0:.0f} s", flush=True)
+    out["position"] = np.stack(pos)
+    out["orientation"] = np.stack(quat)
+    return out
+
+
 def main(which):
     if "hopper" in which:
         t = time.time()
@@ -126,6 +159,11 @@ def main(which):
         out = run_single(scenes.sphere_bowl(), 20, os.cpu_count())
         np.savez_compressed(os.path.join(HERE, "traj_sphere_bowl.npz"), **out)
         print(f"bowl: {time.time() - t:.0f} s")
+    if "ipc_bowl" in which:
+        t = time.time()
+        out = run_ipc(scenes.sphere_bowl(), 40)
+        np.savez_compressed(os.path.join(HERE, "traj_ipc_sphere_bowl.npz"), **out)
+        print(f"ipc_bowl: {time.time() - t:.0f} s")
     if "batched" in which:
         t = time.time()
         make_batched(os.path.join(HERE, "traj_batched.npz"))

@@ -58,3 +58,16 @@ def test_batched_fixture_first_steps():
             d = ow.diagnostics()
             assert [d["n_contacts"], d["alm_iterations"], d["newton_iterations"]] == list(ref["diag"][i, s])
         assert fingerprint(ow.state()) == tuple(ref["fp"][i, 0])
+
+
+def test_ipc_sphere_bowl_fixture_first_step():
+    from nexdynipc_b200 import abi
+    ref = np.load(os.path.join(GOLDEN, "traj_ipc_sphere_bowl.npz"))
+    assert ref["position"].shape == (40, 65, 3)
+    ow = refcpu.OracleWorld(scenes.sphere_bowl())
+    st = ow.ipc_step(abi.ipc_params(**scenes.ipc_step_settings()))
+    for k in ("newton_iterations", "converged", "line_search_failed", "n_active", "n_pairs"):
+        assert st[k] == ref[k][0], k
+    s = ow.state()
+    assert np.array_equal(s["position"], ref["position"][0])
+    assert np.array_equal(s["orientation"], ref["orientation"][0])
