@@ -165,17 +165,37 @@ __global__ void k_bsr_concat(int N, const int* rpa, const int* cia, const double
     }
 }
 
-// pair (q, prim) <-> sort key (q << pbits) | prim
-__global__ void k_pair_keys(const int* pairs, int n, int pbits, unsigned long long* key, int* val) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        key[i] = ((unsigned long long)(unsigned)pairs[2 * i] << pbits) | (unsigned)pairs[2 * i + 1];
-        val[i] = i;
-    }
-}
-__global__ void k_pair_from_keys(const unsigned long long* key, int n, int pbits, int* pairs) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        pairs[2 * i] = (int)(key[i] >> pbits);
-        pairs[2 * i + 1] = (int)(key[i] & ((1ull << pbits) - 1ull));
+// Each query's slice of (query, primitive) pairs, [off[q], off[q] + cnt[q]),
+// sorted by primitive in place, one thread per query: insertion sort for
+// short slices, heapsort beyond (the primitives of a slice are distinct).
+__global__ void k_sort_query_slices(int* pairs, const int* off, const int* cnt, int nq) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const int m = cnt[q];
+        if (m < 2) continue;
+        int* p = pairs + 2 * (size_t)off[q] + 1;    // primitives at stride 2
+        if (m <= 48) {
+            for (int i = 1; i < m; ++i) {
+                const int v = p[2 * i];
+                int j = i - 1;
+                while (j >= 0 && p[2 * j] > v) { p[2 * (j + 1)] = p[2 * j]; --j; }
+                p[2 * (j + 1)] = v;
+            }
+            continue;
+        }
+        auto sift = [&](int root, int end) {
+            while (2 * root + 1 < end) {
+                int ch = 2 * root + 1;
+                if (ch + 1 < end && p[2 * ch] < p[2 * (ch + 1)]) ++ch;
+                if (!(p[2 * root] < p[2 * ch])) return;
+                const int t = p[2 * root]; p[2 * root] = p[2 * ch]; p[2 * ch] = t;
+                root = ch;
+            }
+        };
+        for (int r = m / 2 - 1; r >= 0; --r) sift(r, m);
+        for (int end = m - 1; end > 0; --end) {
+            const int t = p[0]; p[0] = p[2 * end]; p[2 * end] = t;
+            sift(0, end);
+        }
     }
 }
 
@@ -613,43 +633,102 @@ __global__ void k_seg_starts(const int* flag, const int* pos, int n, int* start,
     }
 }
 
-// Gradient: thread per (segment, dof) sums its contributions in pair order.
+// Segment sums of the barrier's gradient and Hessian blocks, in one fixed
+// order on the device and in the oracle: a segment of m <= kSegSerial
+// contributions (pair order) is summed left to right from 0; a longer one
+// as 32 partial sums, partial l taking the contributions i = l (mod 32) left
+// to right, then halved pairwise (a_l += a_{l+16}, ..., a_0 += a_1).  Light
+// segments take a thread each; heavy ones (a body touching many pairs, such
+// as a static container) a warp each, so their cost is m / 32 dependent
+// adds instead of m.
+constexpr int kSegSerial = 32;
+
+__device__ __forceinline__ double ipc_grad_term(const int* gval, const double* pgrad, int i, int dof) {
+    const int v = gval[i];
+    return pgrad[12 * (size_t)(v >> 1) + 6 * (v & 1) + dof];
+}
+__device__ __forceinline__ double ipc_hess_term(const int* hval, const double* lam, const double* z, const int* nterm, int s, int i,
+                                                int j) {
+    const int v = hval[s];
+    const int p = v >> 2, r = (v >> 1) & 1, c = v & 1;
+    double blk = 0.0;
+    for (int k = 0; k < nterm[p]; ++k) {
+        const double* zk = z + 60 * (size_t)p + 12 * k;
+        blk += (lam[5 * (size_t)p + k] * zk[6 * r + i]) * zk[6 * c + j];
+    }
+    return blk;
+}
+// lanes' partials halved pairwise into lane 0
+__device__ __forceinline__ double warp_halve_sum(double a) {
+    const int lane = threadIdx.x & 31;
+    for (int off = 16; off >= 1; off >>= 1) {
+        const double o = __shfl_down_sync(0xffffffffu, a, off);
+        if (lane < off) a += o;
+    }
+    return a;
+}
+
+// Gradient, light segments: thread per (segment, dof).
 __global__ void k_ipc_grad(const unsigned long long* gkey, const int* gval, const int* start, const int* nseg, const double* pgrad,
                            double* grad) {
     const int ns = *nseg;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 6 * ns; t += gridDim.x * blockDim.x) {
         const int sgm = t / 6, dof = t % 6;
+        if (start[sgm + 1] - start[sgm] > kSegSerial) continue;
         double acc = 0.0;
-        for (int i = start[sgm]; i < start[sgm + 1]; ++i) {
-            const int v = gval[i];
-            acc += pgrad[12 * (size_t)(v >> 1) + 6 * (v & 1) + dof];
-        }
+        for (int i = start[sgm]; i < start[sgm + 1]; ++i) acc += ipc_grad_term(gval, pgrad, i, dof);
         grad[6 * gkey[start[sgm]] + dof] = acc;
     }
 }
+// Gradient, heavy segments: warp per (segment, dof), warps striding over all.
+__global__ void k_ipc_grad_heavy(const unsigned long long* gkey, const int* gval, const int* start, const int* nseg,
+                                 const double* pgrad, double* grad) {
+    const int ns = *nseg, lane = threadIdx.x & 31;
+    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long t = w0; t < 6LL * ns; t += nw) {
+        const int sgm = (int)(t / 6), dof = (int)(t % 6);
+        const int a = start[sgm], b = start[sgm + 1];
+        if (b - a <= kSegSerial) continue;
+        double acc = 0.0;
+        for (int i = a + lane; i < b; i += 32) acc += ipc_grad_term(gval, pgrad, i, dof);
+        acc = warp_halve_sum(acc);
+        if (lane == 0) grad[6 * gkey[a] + dof] = acc;
+    }
+}
 
-// Hessian blocks: thread per (segment, entry); block (r, c) of pair p is
-// sum_k (lam_k z_k[r-side i]) z_k[c-side j], summed over the segment's pairs
-// in pair order.  Writes BSR col_idx / vals in sorted (row, col) order.
+// Hessian blocks: block (r, c) of pair p is sum_k (lam_k z_k[r-side i])
+// z_k[c-side j]; each block entry is its segment's sum in the order above.
+// Writes BSR col_idx / vals in sorted (row, col) order.  Light segments:
+// thread per (segment, entry).
 __global__ void k_ipc_hess(const unsigned long long* hkey, const int* hval, const int* start, const int* nseg, int N,
                            const double* lam, const double* z, const int* nterm, int* col_idx, double* vals, long long cap) {
     const int ns = *nseg;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 36 * ns; t += gridDim.x * blockDim.x) {
         const int sgm = t / 36, e = t % 36, i = e / 6, j = e % 6;
         if (sgm >= cap) continue;
-        double acc = 0.0;
-        for (int s = start[sgm]; s < start[sgm + 1]; ++s) {
-            const int v = hval[s];
-            const int p = v >> 2, r = (v >> 1) & 1, c = v & 1;
-            double blk = 0.0;
-            for (int k = 0; k < nterm[p]; ++k) {
-                const double* zk = z + 60 * (size_t)p + 12 * k;
-                blk += (lam[5 * (size_t)p + k] * zk[6 * r + i]) * zk[6 * c + j];
-            }
-            acc += blk;
-        }
-        vals[36 * (size_t)sgm + e] = acc;
         if (e == 0) col_idx[sgm] = (int)(hkey[start[sgm]] % (unsigned long long)N);
+        if (start[sgm + 1] - start[sgm] > kSegSerial) continue;
+        double acc = 0.0;
+        for (int s = start[sgm]; s < start[sgm + 1]; ++s) acc += ipc_hess_term(hval, lam, z, nterm, s, i, j);
+        vals[36 * (size_t)sgm + e] = acc;
+    }
+}
+// Hessian blocks, heavy segments: warp per (segment, entry).
+__global__ void k_ipc_hess_heavy(const int* hval, const int* start, const int* nseg, const double* lam, const double* z,
+                                 const int* nterm, double* vals, long long cap) {
+    const int ns = *nseg, lane = threadIdx.x & 31;
+    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long t = w0; t < 36LL * ns; t += nw) {
+        const int sgm = (int)(t / 36), e = (int)(t % 36), i = e / 6, j = e % 6;
+        if (sgm >= cap) continue;
+        const int a = start[sgm], b = start[sgm + 1];
+        if (b - a <= kSegSerial) continue;
+        double acc = 0.0;
+        for (int s = a + lane; s < b; s += 32) acc += ipc_hess_term(hval, lam, z, nterm, s, i, j);
+        acc = warp_halve_sum(acc);
+        if (lane == 0) vals[36 * (size_t)sgm + e] = acc;
     }
 }
 

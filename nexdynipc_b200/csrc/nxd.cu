@@ -1291,6 +1291,7 @@ namespace {
 
 struct Bvh {
     int n = 0;
+    int topo_n = -1;    // primitive count of the hierarchy in child / parent / i0 (-1: none built)
     GrowBuf k0, k1, i0, i1, leaf, nbox, child, parent, flags, bounds;
 };
 
@@ -1330,10 +1331,14 @@ struct IpcState {
     int n_pt = 0, n_ee = 0;
     bool cand_swept = false;     // the last ipc_candidates_begin built swept boxes
     bool pose_x = false;         // the last ipc_pose was at an iterate (x0 holds it)
+    // Inside one nxd_ipc_step the hierarchies built at the step's first
+    // iterate are refitted to every later iterate, swept pose and trial
+    // instead of rebuilt: the candidate lists are sorted by (query,
+    // primitive) whatever the hierarchy, so they are the same lists.
+    bool keep_trees = false;
     GrowBuf e, grad12, lam, z, nterm, body, active, type, apos, alist;
     GrowBuf gkey, gval, gkey1, gval1, hkey, hval, hkey1, hval1;
     GrowBuf sflag, spos, sstart, gout, rowptr, colidx, vals, toi;
-    GrowBuf tkey, tval, tkey1, tval1;    // candidate pairs sorted by (query, primitive)
     // step adjoint: per-pair blocks, dense K^T and K_phi, vectors, outputs
     GrowBuf akp, akf, abody, aact, aK, aKphi, ax, axb, alam, aout, afail;
     // full-IPC time step: rest-form and merged BSR, gradients, solve scratch
@@ -1346,8 +1351,8 @@ struct IpcState {
                 &edges.child, &edges.parent, &edges.flags, &edges.bounds, &cnt, &off, &cnt2, &off2, &pt, &ee, &scal, &hist, &e,
                 &grad12, &lam, &z, &nterm, &body, &active, &type, &apos, &alist, &gkey, &gval, &gkey1, &gval1, &hkey,
                 &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &rrp, &rci, &rvv,
-                &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &tkey, &tval,
-                &tkey1, &tval1, &akp, &akf, &abody, &aact, &aK, &aKphi, &ax, &axb, &alam, &aout, &afail};
+                &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &akp, &akf, &abody, &aact,
+                &aK, &aKphi, &ax, &axb, &alam, &aout, &afail};
     }
     void release() {
         for (GrowBuf* b : all()) b->release();
@@ -1471,6 +1476,15 @@ nxd_status ipc_build_bvh(nxd_ctx* c, Bvh& B, int kind, bool swept, double infl) 
     if (n == 0) return NXD_OK;
     const double* w1 = swept ? s->wq1.as<double>() : nullptr;
     k_ipc_boxes<<<grid_for(n, 256), 256, 0, c->stream>>>(s->pg, kind, s->wq0.as<double>(), w1, infl, B.leaf.as<double>());
+    if (s->keep_trees && B.topo_n == n) {
+        // the step's hierarchy, boxes refitted bottom-up
+        NXD_CUDA(cudaMemsetAsync(B.flags.p, 0, 4 * (size_t)n, c->stream));
+        k_refit<<<grid_for(n, 128), 128, 0, c->stream>>>(B.leaf.as<double>(), B.i0.as<int>(), n, B.child.as<int>(),
+                                                         B.parent.as<int>(), B.nbox.as<double>(), B.flags.as<int>());
+        NXD_CUDA(cudaGetLastError());
+        return NXD_OK;
+    }
+    B.topo_n = -1;
     IPC_ENSURE(B.bounds, 48);
     k_centroid_bounds<<<1, 1024, 0, c->stream>>>(B.leaf.as<double>(), n, B.bounds.as<double>());
     IPC_ENSURE(B.k0, 8 * (size_t)n); IPC_ENSURE(B.i0, 4 * (size_t)n);
@@ -1486,6 +1500,7 @@ nxd_status ipc_build_bvh(nxd_ctx* c, Bvh& B, int kind, bool swept, double infl) 
     k_refit<<<grid_for(n, 128), 128, 0, c->stream>>>(B.leaf.as<double>(), B.i0.as<int>(), n, B.child.as<int>(), B.parent.as<int>(),
                                                      B.nbox.as<double>(), B.flags.as<int>());
     NXD_CUDA(cudaGetLastError());
+    B.topo_n = n;
     return NXD_OK;
 }
 
@@ -1546,16 +1561,10 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
             if (m == 0) continue;
             launch(k, false);
             if (sweep || m < 2) continue;
-            // traversal order -> (query, primitive) ascending
-            const int pbits = bits_for((unsigned long long)std::max(np[k], 1));
-            const int qbits = bits_for((unsigned long long)std::max(nq[k], 1));
-            IPC_ENSURE(s->tkey, 8 * (size_t)m); IPC_ENSURE(s->tval, 4 * (size_t)m);
-            k_pair_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(out[k]->as<int>(), m, pbits, s->tkey.as<unsigned long long>(),
-                                                                 s->tval.as<int>());
-            st = radix_sort(c, s->tkey, s->tval, s->tkey1, s->tval1, m, 0, pbits + qbits);
-            if (st != NXD_OK) return st;
-            k_pair_from_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(s->tkey.as<unsigned long long>(), m, pbits,
-                                                                      out[k]->as<int>());
+            // traversal order -> (query, primitive) ascending: the queries'
+            // slices are already in query order, so each is sorted alone
+            k_sort_query_slices<<<grid_for(nq[k], 128), 128, 0, c->stream>>>(out[k]->as<int>(), off[k]->as<int>(),
+                                                                             cnt[k]->as<int>(), nq[k]);
         }
         NXD_CUDA(cudaGetLastError());
         return NXD_OK;
@@ -1700,11 +1709,19 @@ nxd_status ipc_barrier_eval(nxd_ctx* c, double dhat, double kappa, bool full, in
     k_ipc_grad<<<grid_for(12LL * na, 128), 128, 0, c->stream>>>(s->gkey.as<unsigned long long>(), s->gval.as<int>(),
                                                                  s->sstart.as<int>(), d_nseg, s->grad12.as<double>(),
                                                                  s->gout.as<double>());
+    const int heavy_grid = 4 * c->n_sm;   // 32 warps per SM striding over the segments
+    if (na > kSegSerial)
+        k_ipc_grad_heavy<<<heavy_grid, 256, 0, c->stream>>>(s->gkey.as<unsigned long long>(), s->gval.as<int>(),
+                                                             s->sstart.as<int>(), d_nseg, s->grad12.as<double>(),
+                                                             s->gout.as<double>());
     if ((st = ipc_segments(c, s->hkey.as<unsigned long long>(), 4 * na)) != NXD_OK) return st;
     k_ipc_hess<<<grid_for(144LL * na, 128), 128, 0, c->stream>>>(s->hkey.as<unsigned long long>(), s->hval.as<int>(),
                                                                   s->sstart.as<int>(), d_nseg, N, s->lam.as<double>(),
                                                                   s->z.as<double>(), s->nterm.as<int>(), s->colidx.as<int>(),
                                                                   s->vals.as<double>(), 4LL * na);
+    if (na > kSegSerial)
+        k_ipc_hess_heavy<<<heavy_grid, 256, 0, c->stream>>>(s->hval.as<int>(), s->sstart.as<int>(), d_nseg, s->lam.as<double>(),
+                                                             s->z.as<double>(), s->nterm.as<int>(), s->vals.as<double>(), 4LL * na);
     k_ipc_rowptr<<<grid_for(N + 1, 128), 128, 0, c->stream>>>(s->hkey.as<unsigned long long>(), s->sstart.as<int>(), d_nseg, N,
                                                                s->rowptr.as<int>());
     NXD_CUDA(cudaGetLastError());
@@ -1876,6 +1893,12 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
     double amax = 1.0, fx = 0.0;
     int64_t npairs = 0;
     bool cand_at_x = false;   // the last poses and dhat-inflated candidates were built at x
+    // the hierarchies built at the first iterate serve the whole step
+    struct TreeScope {
+        IpcState* s;
+        ~TreeScope() { s->keep_trees = false; }
+    } tree_scope{s};
+    s->keep_trees = false;
     for (int it = 0; it < p->newton_max_iters; ++it) {
         iters = it;
         // gradient at x: rest forms, then the barrier over the candidates at x
@@ -1887,6 +1910,7 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
         if (!cand_at_x) {
             st = ipc_pose(c, x, nullptr, true);
             if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
+            s->keep_trees = true;
         }
         cand_at_x = false;
         if (st == NXD_OK) st = ipc_barrier_eval(c, p->dhat, p->kappa, true, nullptr);

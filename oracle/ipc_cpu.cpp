@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <map>
 #include <vector>
 
 #include "refcpu.h"
@@ -203,6 +204,23 @@ double tree_sum(std::vector<double> v) {
     return v.empty() ? 0.0 : v[0];
 }
 
+// A gradient entry's or Hessian block entry's contributions (pair order),
+// summed as the device's segment kernels sum them: up to 32 left to right
+// from 0; more as 32 partials (partial l: contributions l, l + 32, ...,
+// left to right), halved pairwise, a_l += a_{l+16}, ..., a_0 += a_1.
+double seg_sum(const std::vector<double>& v) {
+    if (v.size() <= 32) {
+        double acc = 0.0;
+        for (double t : v) acc += t;
+        return acc;
+    }
+    double a[32] = {};
+    for (size_t i = 0; i < v.size(); ++i) a[i % 32] += v[i];
+    for (int off = 16; off >= 1; off /= 2)
+        for (int l = 0; l < off; ++l) a[l] += a[l + off];
+    return a[0];
+}
+
 // Raw 12x12 pair Hessian b'' grad grad^T + b' hess(d^2), written out densely.
 void raw_hessian(const ipc::DistForm& f, const V3* X, double dhat, double kappa, double* H) {
     for (int i = 0; i < 144; ++i) H[i] = 0.0;
@@ -281,7 +299,10 @@ int ipc_barrier_cpu(nxo_world* w, const double* x, double dhat, double kappa, do
     std::vector<double> e(n);
     if (grad) std::fill(grad, grad + N6, 0.0);
     if (H) std::fill(H, H + (size_t)N6 * N6, 0.0);
-    int64_t na = 0;
+    // per active pair (pair order): its bodies, chained gradient (12) and,
+    // with H, its four 6x6 blocks (r, c) = (0,0), (0,1), (1,0), (1,1)
+    std::vector<int> ab;
+    std::vector<double> ag, ah;
     for (size_t p = 0; p < n; ++p) {
         int kind, side[4], bA, bB;
         V3 X[4], arm[4];
@@ -290,18 +311,15 @@ int ipc_barrier_cpu(nxo_world* w, const double* x, double dhat, double kappa, do
         const ipc::PairEval ev = ipc::pair_barrier(f, X, dhat, kappa);
         e[p] = ev.e;
         if (!(ev.d2 < dhat * dhat)) continue;
-        ++na;
         if (blocks) {
             blocks->push_back({bA, bA}); blocks->push_back({bA, bB});
             blocks->push_back({bB, bA}); blocks->push_back({bB, bB});
         }
+        ab.push_back(bA); ab.push_back(bB);
         double g12[12];
         const V3 thA = nx::ld3(&g.theta[3 * bA]), thB = nx::ld3(&g.theta[3 * bB]);
         ipc::chain12_exact(ev.grad, side, arm, thA, thB, g12);
-        const int b[2] = {bA, bB};
-        if (grad)
-            for (int s = 0; s < 2; ++s)
-                for (int d = 0; d < 6; ++d) grad[6 * b[s] + d] += g12[6 * s + d];
+        ag.insert(ag.end(), g12, g12 + 12);
         if (!H) continue;
         double z[5][12];
         for (int k = 0; k < ev.n_terms; ++k) ipc::chain12_exact(ev.y[k], side, arm, thA, thB, z[k]);
@@ -311,12 +329,40 @@ int ipc_barrier_cpu(nxo_world* w, const double* x, double dhat, double kappa, do
                     for (int j = 0; j < 6; ++j) {
                         double blk = 0.0;
                         for (int k = 0; k < ev.n_terms; ++k) blk += (ev.lam[k] * z[k][6 * r + i]) * z[k][6 * c + j];
-                        H[(size_t)(6 * b[r] + i) * N6 + 6 * b[c] + j] += blk;
+                        ah.push_back(blk);
                     }
+    }
+    const size_t na = ab.size() / 2;
+    // each gradient entry / block entry: its contributions in pair order,
+    // summed as the device sums a segment (seg_sum)
+    std::vector<double> vals;
+    if (grad) {
+        std::vector<std::vector<std::pair<int, int>>> seg(g.N);   // (active pair, side)
+        for (size_t a = 0; a < na; ++a)
+            for (int sd = 0; sd < 2; ++sd) seg[ab[2 * a + sd]].push_back({(int)a, sd});
+        for (int b = 0; b < g.N; ++b)
+            for (int d = 0; seg[b].size() && d < 6; ++d) {
+                vals.clear();
+                for (const auto& t : seg[b]) vals.push_back(ag[12 * (size_t)t.first + 6 * t.second + d]);
+                grad[6 * b + d] = seg_sum(vals);
+            }
+    }
+    if (H) {
+        std::map<std::pair<int, int>, std::vector<std::pair<int, int>>> seg;   // (row, col body) -> (active pair, block)
+        for (size_t a = 0; a < na; ++a)
+            for (int r = 0; r < 2; ++r)
+                for (int c = 0; c < 2; ++c) seg[{ab[2 * a + r], ab[2 * a + c]}].push_back({(int)a, 2 * r + c});
+        for (const auto& kv : seg)
+            for (int i = 0; i < 6; ++i)
+                for (int j = 0; j < 6; ++j) {
+                    vals.clear();
+                    for (const auto& t : kv.second) vals.push_back(ah[144 * (size_t)t.first + 36 * t.second + 6 * i + j]);
+                    H[(size_t)(6 * kv.first.first + i) * N6 + 6 * kv.first.second + j] = seg_sum(vals);
+                }
     }
     if (energy) *energy = tree_sum(e);
     if (n_pairs) *n_pairs = (int64_t)n;
-    if (n_active) *n_active = na;
+    if (n_active) *n_active = (int64_t)na;
     if (blocks) {
         std::sort(blocks->begin(), blocks->end());
         blocks->erase(std::unique(blocks->begin(), blocks->end()), blocks->end());
