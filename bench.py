@@ -399,25 +399,29 @@ def pcg_leg(n_bodies: int = 200000, iters: int = 60):
             "achieved_gbs": per_iter * st["iterations"] / secs / 1e9 if secs > 0 else None}
 
 
-def ipc_step_params(solver: int = 0):
+def ipc_step_params(solver: int = 0, mu: float = 0.0):
     from nexdynipc_b200 import abi, scenes
-    return abi.ipc_params(**scenes.ipc_step_settings(solver))
+    return abi.ipc_params(**scenes.ipc_step_settings(solver, mu))
 
 
 def ipc_step_leg(n_cubes: int = 8, columns: int = 1, settle: int = 30, steps: int = 20, solver: int = 0,
-                 bowl: bool = False):
+                 bowl: bool = False, mu: float = 0.0):
     """Full-IPC time step (nxd_ipc_step): after `settle` untimed steps, wall
     clock of `steps` steps, each a host-ordered Newton loop of device calls
     (candidates, barrier, rest forms, block solve, CCD bound, line search).
     The scene is stacks of tilted cubes falling onto a ground box, or with
     `bowl` the 64-sphere bowl configuration (642-vertex icospheres, 1280-face
-    bowl).  Per-step wall times are kept so that a CPU sample of the first
-    steps can be compared step for step."""
+    bowl); mu > 0 adds lagged friction.  One untimed step on a throwaway
+    context of the same scene first loads the kernels; per-step wall times are
+    kept so that a CPU sample of the first steps can be compared step for step."""
     import time
     from nexdynipc_b200 import runtime, scenes
     sc = scenes.sphere_bowl() if bowl else scenes.ipc_drop(n_cubes=n_cubes, columns=columns)
+    p = ipc_step_params(solver, mu)
+    warm = runtime.Context(sc)
+    warm.ipc_step(p)
+    warm.close()
     ctx = runtime.Context(sc)
-    p = ipc_step_params(solver)
     for _ in range(settle):
         ctx.ipc_step(p)
     its, act, pairs, conv, lsf, walls = [], [], [], 0, 0, []
@@ -431,22 +435,23 @@ def ipc_step_leg(n_cubes: int = 8, columns: int = 1, settle: int = 30, steps: in
         lsf += st["line_search_failed"]
     wall = time.perf_counter() - t0
     ctx.close()
+    fric = f", lagged friction mu {mu} (eps 1e-5 m, 2 passes)" if mu > 0 else ""
     if bowl:
         workload = (f"{sc.n_bodies - 1} icospheres (642 V) falling into a 1280-face bowl, full IPC, dhat 1e-3, "
-                    f"kappa 1e11, dt {sc.dt}; steps {settle + 1}-{settle + steps}")
+                    f"kappa 1e11{fric}, dt {sc.dt}; steps {settle + 1}-{settle + steps}")
     else:
         workload = (f"{n_cubes} tilted 0.2 m cubes in {columns} stack(s) on a ground box, dhat 1e-3, "
                     f"kappa 1e11, dt {sc.dt}; steps {settle + 1}-{settle + steps}")
     return {"workload": workload,
             "steps": steps, "steps_per_s": steps / wall, "newton_iterations_mean": float(np.mean(its)),
             "active_pairs_mean": float(np.mean(act)), "candidate_pairs_mean": float(np.mean(pairs)),
-            "converged_steps": conv, "line_search_failures": lsf,
+            "converged_steps": conv, "line_search_failures": lsf, "friction_pairs_last": int(st["n_friction"]),
             "step_ms": [round(1e3 * w, 3) for w in walls[:4]],
             "linear_solver": "block-Jacobi PCG" if solver else "component LDL^T",
             "timing": "wall clock per nxd_ipc_step (it synchronises)"}
 
 
-def ipc_step_cpu_baseline(n_cubes: int, columns: int, settle: int, steps: int, bowl: bool = False):
+def ipc_step_cpu_baseline(n_cubes: int, columns: int, settle: int, steps: int, bowl: bool = False, mu: float = 0.0):
     """The CPU oracle's full-IPC step on the same trajectory segment as
     ipc_step_leg: `settle` untimed steps, then wall clock of `steps`.  The
     oracle's candidate search runs on all host threads (OpenMP), the rest of
@@ -454,7 +459,7 @@ def ipc_step_cpu_baseline(n_cubes: int, columns: int, settle: int, steps: int, b
     from nexdynipc_b200 import scenes
     from oracle.refcpu import OracleWorld
     ow = OracleWorld(scenes.sphere_bowl() if bowl else scenes.ipc_drop(n_cubes=n_cubes, columns=columns))
-    p = ipc_step_params(0)
+    p = ipc_step_params(0, mu)
     for _ in range(settle):
         ow.ipc_step(p)
     t0 = time.perf_counter()
@@ -770,6 +775,7 @@ def main():
         mode_i["step_pcg"] = ipc_step_leg(solver=1)
         mode_i["step_64"] = ipc_step_leg(n_cubes=64, columns=16, settle=30, steps=10)
         mode_i["step_bowl"] = ipc_step_leg(settle=0, steps=40, bowl=True)
+        mode_i["step_bowl_friction"] = ipc_step_leg(settle=0, steps=20, bowl=True, mu=0.3)
 
     batched = None
     if not args.no_batched:
@@ -791,6 +797,7 @@ def main():
             mode_i["step"]["cpu_baseline"] = ipc_step_cpu_baseline(8, 1, 30, 20)
             mode_i["step_64"]["cpu_baseline"] = ipc_step_cpu_baseline(64, 16, 30, 10)
             mode_i["step_bowl"]["cpu_baseline"] = ipc_step_cpu_baseline(0, 0, 0, 2, bowl=True)
+            mode_i["step_bowl_friction"]["cpu_baseline"] = ipc_step_cpu_baseline(0, 0, 0, 1, bowl=True, mu=0.3)
     launches_total = int(timed_n.sum())
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,

@@ -435,7 +435,14 @@ nxd_status nxd_ipc_max_step(nxd_ctx* ctx, const double* x, const double* dx, dou
  * candidates are rebuilt at every iterate and trial point; each system is
  * solved by nxd_linear_solve's factorisation or by nxd_pcg_solve's PCG
  * (linear_solver); the state is written back as nxd_step does.
- * No friction term. */
+ * Friction (mu > 0): the reference's smoothed friction potential
+ * (FrictionPotential, Friction.cpp:5-61; D = mu lam (sqrt(|u|^2 + eps^2) -
+ * eps)) on every pair active at a lag state, u the tangential displacement
+ * of the pair's closest points since the step start; the pairs, their
+ * normal forces lam = -db/dd, normals and closest-point weights frozen at
+ * the step start, then re-frozen at each pass's solution for
+ * friction_iters passes in all (the reference's lagged friction,
+ * IPCSolver.cpp:1112-1130). */
 typedef struct nxd_ipc_params {
     double dhat;                /* barrier activation distance               */
     double kappa;               /* barrier stiffness                         */
@@ -447,6 +454,10 @@ typedef struct nxd_ipc_params {
                                    1: block-Jacobi PCG (nxd_pcg_solve)       */
     int32_t pcg_max_iter;
     double pcg_tol;             /* |r| / |b|                                 */
+    double mu;                  /* friction coefficient (0: no friction)     */
+    double friction_eps;        /* eps of the smoothed norm (m)              */
+    int32_t friction_iters;     /* lagging passes (>= 1 when mu > 0)         */
+    int32_t pad;
 } nxd_ipc_params;
 typedef struct nxd_ipc_stats {
     int32_t newton_iterations;
@@ -458,6 +469,7 @@ typedef struct nxd_ipc_stats {
     int64_t n_pairs;            /* candidate pairs at the last iterate       */
     int64_t n_active;           /* pairs within dhat                         */
     int64_t pcg_iterations;     /* PCG iterations over the step              */
+    int64_t n_friction;         /* frozen friction pairs of the last pass    */
 } nxd_ipc_stats;
 nxd_status nxd_ipc_step(nxd_ctx* ctx, double dt, const nxd_ipc_params* p, nxd_ipc_stats* stats);
 

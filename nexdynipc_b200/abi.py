@@ -176,6 +176,10 @@ class NxdIpcParams(C.Structure):
         ("linear_solver", C.c_int32),
         ("pcg_max_iter", C.c_int32),
         ("pcg_tol", C.c_double),
+        ("mu", C.c_double),
+        ("friction_eps", C.c_double),
+        ("friction_iters", C.c_int32),
+        ("pad", C.c_int32),
     ]
 
 
@@ -190,6 +194,7 @@ class NxdIpcStats(C.Structure):
         ("n_pairs", C.c_int64),
         ("n_active", C.c_int64),
         ("pcg_iterations", C.c_int64),
+        ("n_friction", C.c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -200,9 +205,10 @@ IPC_SOLVER_DIRECT, IPC_SOLVER_PCG = 0, 1
 
 
 def ipc_params(dhat=1e-3, kappa=1e8, eta=0.1, newton_tol=1e-6, newton_max_iters=50, ls_max_iters=30,
-               linear_solver=IPC_SOLVER_DIRECT, pcg_max_iter=500, pcg_tol=1e-12) -> "NxdIpcParams":
+               linear_solver=IPC_SOLVER_DIRECT, pcg_max_iter=500, pcg_tol=1e-12, mu=0.0, friction_eps=1e-8,
+               friction_iters=1) -> "NxdIpcParams":
     return NxdIpcParams(dhat, kappa, eta, newton_tol, newton_max_iters, ls_max_iters, linear_solver, pcg_max_iter,
-                        pcg_tol)
+                        pcg_tol, mu, friction_eps, friction_iters, 0)
 
 
 class NxdIpcAdjointOut(C.Structure):

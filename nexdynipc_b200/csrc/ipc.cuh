@@ -473,6 +473,110 @@ __global__ void k_ipc_pair_eval(PrimGeo pg, IpcPairs P, IpcPose ps, double dhat,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Lagged friction (ipc::friction_pair) over a frozen set of pairs: built
+// from the active barrier pairs at the lag state (k_fric_lag), evaluated at
+// every iterate and trial point (k_fric_eval / k_fric_energy) against the
+// step-start world vertices x0.
+// ---------------------------------------------------------------------------
+struct IpcFric {
+    int n;
+    int* vid;          // [4n] the pair's four vertices
+    int* body;         // [2n] bodies A, B
+    int* kind;         // [n]  ipc::kPairPT / kPairEE (fixes the sides)
+    double* w;         // [4n] closest-point weights
+    double* nrm;       // [3n] unit normal
+    double* lam;       // [n]  normal force
+    const double* x0;  // step-start world vertices [nv*3]
+};
+
+__device__ __forceinline__ void pair_vids(const PrimGeo& pg, const IpcPairs& P, int p, int* vid, int& kind, int& bA, int& bB) {
+    if (p < P.n_pt) {
+        kind = ipc::kPairPT;
+        const int v = P.pt[2 * p], f = P.pt[2 * p + 1];
+        vid[0] = v; vid[1] = pg.fvert[3 * f]; vid[2] = pg.fvert[3 * f + 1]; vid[3] = pg.fvert[3 * f + 2];
+        bA = pg.vbody[v]; bB = pg.fbody[f];
+    } else {
+        kind = ipc::kPairEE;
+        const int q = p - P.n_pt;
+        const int e0 = P.ee[2 * q], e1 = P.ee[2 * q + 1];
+        vid[0] = pg.evert[2 * e0]; vid[1] = pg.evert[2 * e0 + 1]; vid[2] = pg.evert[2 * e1]; vid[3] = pg.evert[2 * e1 + 1];
+        bA = pg.ebody[e0]; bB = pg.ebody[e1];
+    }
+}
+__device__ __forceinline__ void fric_sides(int kind, int* side) {
+    side[0] = 0; side[1] = kind == ipc::kPairPT ? 1 : 0; side[2] = 1; side[3] = 1;
+}
+
+// The friction set from the active list (pair order) at the lag state.
+__global__ void k_fric_lag(PrimGeo pg, IpcPairs P, IpcPose ps, const int* alist, int na, double dhat, double kappa, IpcFric F) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
+        const int p = alist[a];
+        int vid[4], kind, bA, bB;
+        pair_vids(pg, P, p, vid, kind, bA, bB);
+        V3 X[4];
+        for (int k = 0; k < 4; ++k) X[k] = ld3(ps.wq + 3 * vid[k]);
+        const ipc::DistForm f = ipc::classify(kind, X);
+        ipc::FricLag L;
+        ipc::friction_lag(f, X, dhat, kappa, L);
+        for (int k = 0; k < 4; ++k) { F.vid[4 * a + k] = vid[k]; F.w[4 * a + k] = L.w[k]; }
+        F.body[2 * a] = bA; F.body[2 * a + 1] = bB;
+        F.kind[a] = kind;
+        F.nrm[3 * a] = L.n.x; F.nrm[3 * a + 1] = L.n.y; F.nrm[3 * a + 2] = L.n.z;
+        F.lam[a] = L.lam;
+    }
+}
+
+__device__ __forceinline__ ipc::FricEval fric_at(const IpcFric& F, const IpcPose& ps, int f, double mu, double eps, int* side,
+                                                 V3* arm, int& bA, int& bB) {
+    ipc::FricLag L;
+    V3 X[4], X0[4];
+    bA = F.body[2 * f]; bB = F.body[2 * f + 1];
+    fric_sides(F.kind[f], side);
+    for (int k = 0; k < 4; ++k) {
+        const int v = F.vid[4 * f + k];
+        X[k] = ld3(ps.wq + 3 * v);
+        X0[k] = ld3(F.x0 + 3 * v);
+        arm[k] = X[k] - ld3(ps.pp + 3 * (side[k] ? bB : bA));
+        L.w[k] = F.w[4 * f + k];
+    }
+    L.n = ld3(F.nrm + 3 * f);
+    L.lam = F.lam[f];
+    return ipc::friction_pair(L, X, X0, mu, eps);
+}
+
+// Friction pair f into slot base + f of the pair arrays (gradient, two
+// Hessian terms, bodies) and its energy into ef[f].
+__global__ void k_fric_eval(IpcFric F, IpcPose ps, double mu, double eps, int base, double* ef, IpcEvalOut o) {
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < F.n; f += gridDim.x * blockDim.x) {
+        int side[4], bA, bB;
+        V3 arm[4];
+        const ipc::FricEval ev = fric_at(F, ps, f, mu, eps, side, arm, bA, bB);
+        const size_t p = (size_t)base + f;
+        ef[f] = ev.e;
+        o.body[2 * p] = bA; o.body[2 * p + 1] = bB;
+        const V3 thA = pose_theta(ps, bA), thB = pose_theta(ps, bB);
+        ipc::chain12_exact(ev.grad, side, arm, thA, thB, o.grad + 12 * p);
+        o.nterm[p] = 2;
+        for (int k = 0; k < 2; ++k) {
+            o.lam[5 * p + k] = ev.lam[k];
+            ipc::chain12_exact(ev.y[k], side, arm, thA, thB, o.z + 60 * p + 12 * k);
+        }
+    }
+}
+__global__ void k_fric_energy(IpcFric F, IpcPose ps, double mu, double eps, double* ef) {
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < F.n; f += gridDim.x * blockDim.x) {
+        int side[4], bA, bB;
+        V3 arm[4];
+        ef[f] = fric_at(F, ps, f, mu, eps, side, arm, bA, bB).e;
+    }
+}
+// list[at + i] = base + i, i < n (the friction pairs after the active barrier pairs)
+__global__ void k_iota(int* list, const int* at, int base, int n) {
+    const int o = *at;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) list[o + i] = base + i;
+}
+
 // Step adjoint, per candidate pair at the converged iterate: the exact
 // derivative of the pair's share of the step gradient G (point forces g_k,
 // torques J_r(theta) sum a_k x g_k) with respect to the two bodies' DOFs

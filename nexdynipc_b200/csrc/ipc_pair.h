@@ -427,6 +427,86 @@ NX_HD double pair_barrier_exact(const DistForm& f, const V3* X, double dhat, dou
     return s;
 }
 
+// ---------------------------------------------------------------------------
+// Lagged friction on a primitive pair: the reference's smoothed friction
+// potential (FrictionPotential::value / gradient / hessian, Friction.cpp:5-61)
+//   D = mu lam (sqrt(|u|^2 + eps^2) - eps),
+// u the tangential displacement, here of the pair's closest points, with
+// the normal force, the normal and the closest-point weights frozen at a lag
+// state (the reference re-detects contacts and recomputes normal forces at
+// each outer iterate, IPCSolver.cpp:1112-1130):
+//   u = P sum_k w_k (X_k - X0_k),  P = I - n n^T,
+// X0 the points at the step start, w_k the DistForm weights (r = sum w_k X_k
+// runs from the closest point on B to the one on A), n = r / |r| and
+// lam = -db/dd = -2 d b'(d^2) at the lag state.  In the points the
+// Hessian mu lam / s (P - u u^T / s^2), s = sqrt(|u|^2 + eps^2), is PSD:
+// mu lam eps^2 / s^3 along u, mu lam / s across it in the tangent plane, 0
+// along n, i.e. two rank-one terms lam_m (w (x) t_m)(w (x) t_m)^T.  Below
+// |u| = 1e-12 the gradient is zero and the Hessian mu lam / eps P, as the
+// reference regularises it.  D is evaluated as mu lam |u|^2 / (s + eps),
+// the same number without the cancellation of s - eps.
+// ---------------------------------------------------------------------------
+struct FricLag {
+    double w[4];
+    V3 n;
+    double lam;
+};
+
+// The frozen quantities of a classified pair at the lag state; false when
+// the pair is not within dhat there.
+NX_HD bool friction_lag(const DistForm& f, const V3* X, double dhat, double kappa, FricLag& L) {
+    const V3 r = form_r(f, X);
+    const double s = dot(r, r), sh = dhat * dhat;
+    for (int k = 0; k < 4; ++k) L.w[k] = f.w[k];
+    L.n = v3(0.0, 0.0, 0.0);
+    L.lam = 0.0;
+    if (!(s < sh) || !(s > 0.0)) return false;
+    const double d = sqrt(s);
+    L.n = v3(r.x / d, r.y / d, r.z / d);
+    L.lam = -2.0 * d * barrier_s1(s, sh, kappa);
+    return true;
+}
+
+struct FricEval {
+    double e;
+    V12 grad;
+    double lam[2];
+    V12 y[2];
+};
+
+NX_HD FricEval friction_pair(const FricLag& L, const V3* X, const V3* X0, double mu, double eps) {
+    FricEval o;
+    V3 dsum = v3(0.0, 0.0, 0.0);
+    for (int k = 0; k < 4; ++k) dsum = dsum + L.w[k] * (X[k] - X0[k]);
+    const V3 u = dsum - dot(dsum, L.n) * L.n;
+    const double uu = dot(u, u), s = sqrt(uu + eps * eps), ml = mu * L.lam, un = sqrt(uu);
+    o.e = ml * (uu / (s + eps));
+    V3 g, t1, t2;
+    if (un < 1e-12) {
+        g = v3(0.0, 0.0, 0.0);
+        // a tangent basis: n x (the coordinate axis least aligned with n)
+        const double ax = fabs(L.n.x), ay = fabs(L.n.y), az = fabs(L.n.z);
+        const V3 e = (ax <= ay && ax <= az) ? v3(1.0, 0.0, 0.0) : (ay <= az ? v3(0.0, 1.0, 0.0) : v3(0.0, 0.0, 1.0));
+        const V3 c = cross(L.n, e);
+        const double cn = sqrt(dot(c, c));
+        t1 = v3(c.x / cn, c.y / cn, c.z / cn);
+        o.lam[0] = ml / eps;
+        o.lam[1] = ml / eps;
+    } else {
+        g = (ml / s) * u;
+        t1 = v3(u.x / un, u.y / un, u.z / un);
+        o.lam[0] = (ml / s) * ((eps * eps) / (s * s));
+        o.lam[1] = ml / s;
+    }
+    t2 = cross(L.n, t1);
+    for (int k = 0; k < 4; ++k) {
+        o.grad.v[k] = L.w[k] * g;
+        o.y[0].v[k] = L.w[k] * t1;
+        o.y[1].v[k] = L.w[k] * t2;
+    }
+    return o;
+}
+
 // Rigid chain: point k of the pair belongs to body side[k] (0 = body A,
 // 1 = body B) at lever arm arm[k] = R r_k (world offset from the body's
 // position); its DOF Jacobian is [I3, -[arm]x].  The transposed Jacobian

@@ -1313,6 +1313,7 @@ struct IpcScal {
     double descent;     // g . dx
     double ginf;        // |g|_inf
     double dxinf;       // |dx|_inf
+    double fenergy;     // friction energy (the frozen pairs' potential)
 };
 struct IpcHost {
     IpcScal sc;
@@ -1336,6 +1337,17 @@ struct IpcState {
     // instead of rebuilt: the candidate lists are sorted by (query,
     // primitive) whatever the hierarchy, so they are the same lists.
     bool keep_trees = false;
+    // lagged friction of the step: the frozen pairs (IpcFric), built from
+    // the active pairs of the barrier evaluation that follows fr_build, and
+    // the step-start world vertices they measure displacements from
+    GrowBuf fr_vid, fr_body, fr_kind, fr_w, fr_nrm, fr_lam, fr_x0, fr_e;
+    int fr_n = 0;
+    bool fr_build = false;
+    double fr_mu = 0.0, fr_eps = 1e-8;
+    IpcFric fric() {
+        return IpcFric{fr_n, fr_vid.as<int>(), fr_body.as<int>(), fr_kind.as<int>(), fr_w.as<double>(), fr_nrm.as<double>(),
+                       fr_lam.as<double>(), fr_x0.as<double>()};
+    }
     GrowBuf e, grad12, lam, z, nterm, body, active, type, apos, alist;
     GrowBuf gkey, gval, gkey1, gval1, hkey, hval, hkey1, hval1;
     GrowBuf sflag, spos, sstart, gout, rowptr, colidx, vals, toi;
@@ -1352,7 +1364,8 @@ struct IpcState {
                 &grad12, &lam, &z, &nterm, &body, &active, &type, &apos, &alist, &gkey, &gval, &gkey1, &gval1, &hkey,
                 &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &rrp, &rci, &rvv,
                 &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &akp, &akf, &abody, &aact,
-                &aK, &aKphi, &ax, &axb, &alam, &aout, &afail};
+                &aK, &aKphi, &ax, &axb, &alam, &aout, &afail, &fr_vid, &fr_body, &fr_kind, &fr_w, &fr_nrm, &fr_lam,
+                &fr_x0, &fr_e};
     }
     void release() {
         for (GrowBuf* b : all()) b->release();
@@ -1551,7 +1564,6 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
     };
     if (phase == 1) {
         // after the fetch: the totals in pinned memory, then the writes
-        nxd_status st = NXD_OK;
         if (s->hp->sc.status != 0) return (nxd_status)s->hp->sc.status;
         s->n_pt = s->hp->sc.tot[0];
         s->n_ee = s->hp->sc.tot[1];
@@ -1655,6 +1667,13 @@ namespace {
 // here with one host wait), the gradient in s->gout and the PSD BSR Hessian
 // in s->rowptr / s->colidx / s->vals, its block count s->rowptr[N] on the
 // device; *nh_out, when asked for, costs one more host wait.
+// Friction energy of the frozen pairs at the pose ps into IpcScal::fenergy.
+void ipc_friction_energy(nxd_ctx* c, const IpcPose& ps) {
+    IpcState* s = c->ipc;
+    k_fric_energy<<<grid_for(s->fr_n, 128), 128, 0, c->stream>>>(s->fric(), ps, s->fr_mu, s->fr_eps, s->fr_e.as<double>());
+    k_tree_sum<<<1, 1024, 0, c->stream>>>(s->fr_e.as<double>(), s->fr_n, &s->ds()->fenergy);
+}
+
 nxd_status ipc_barrier_eval(nxd_ctx* c, double dhat, double kappa, bool full, int* nh_out) {
     IpcState* s = c->ipc;
     IpcScal* ds = s->ds();
@@ -1666,12 +1685,17 @@ nxd_status ipc_barrier_eval(nxd_ctx* c, double dhat, double kappa, bool full, in
     if (!full) {
         if (n) k_ipc_pair_energy<<<grid_for(n, 128), 128, 0, c->stream>>>(s->pg, P, ps, dhat, kappa, s->e.as<double>());
         k_tree_sum<<<1, 1024, 0, c->stream>>>(s->e.as<double>(), n, &ds->energy);
+        if (s->fr_n) ipc_friction_energy(c, ps);
         NXD_CUDA(cudaGetLastError());
         return NXD_OK;
     }
-    IPC_ENSURE(s->grad12, 96 * nn); IPC_ENSURE(s->lam, 40 * nn); IPC_ENSURE(s->z, 480 * nn);
-    IPC_ENSURE(s->nterm, 4 * nn); IPC_ENSURE(s->body, 8 * nn); IPC_ENSURE(s->active, 4 * nn); IPC_ENSURE(s->type, 4 * nn);
-    IPC_ENSURE(s->apos, 4 * nn); IPC_ENSURE(s->alist, 4 * nn);
+    // per-pair slots: the candidates, then the friction pairs (at most the
+    // active candidates when the set is built at this evaluation)
+    const size_t nf = (size_t)(s->fr_build ? n : s->fr_n);
+    const size_t nt = std::max((size_t)n + nf, (size_t)1);
+    IPC_ENSURE(s->grad12, 96 * nt); IPC_ENSURE(s->lam, 40 * nt); IPC_ENSURE(s->z, 480 * nt);
+    IPC_ENSURE(s->nterm, 4 * nt); IPC_ENSURE(s->body, 8 * nt); IPC_ENSURE(s->active, 4 * nn); IPC_ENSURE(s->type, 4 * nn);
+    IPC_ENSURE(s->apos, 4 * nn); IPC_ENSURE(s->alist, 4 * nt);
     const IpcEvalOut o{s->e.as<double>(), s->grad12.as<double>(), s->lam.as<double>(), s->z.as<double>(), s->nterm.as<int>(),
                        s->body.as<int>(), s->active.as<int>(), s->type.as<int>()};
     if (n) k_ipc_pair_eval<<<grid_for(n, 128), 128, 0, c->stream>>>(s->pg, P, ps, dhat, kappa, o);
@@ -1680,7 +1704,23 @@ nxd_status ipc_barrier_eval(nxd_ctx* c, double dhat, double kappa, bool full, in
     if (n) k_compact<<<grid_for(n, 256), 256, 0, c->stream>>>(s->active.as<int>(), s->apos.as<int>(), n, s->alist.as<int>());
     nxd_status st = ipc_fetch(c);
     if (st != NXD_OK) return st;
-    const int na = s->hp->sc.na;
+    const int nb = s->hp->sc.na;
+    if (s->fr_build) {
+        // the friction set: the active pairs here, in pair order
+        s->fr_build = false;
+        s->fr_n = nb;
+        const size_t m = std::max(nb, 1);
+        IPC_ENSURE(s->fr_vid, 16 * m); IPC_ENSURE(s->fr_body, 8 * m); IPC_ENSURE(s->fr_kind, 4 * m);
+        IPC_ENSURE(s->fr_w, 32 * m); IPC_ENSURE(s->fr_nrm, 24 * m); IPC_ENSURE(s->fr_lam, 8 * m); IPC_ENSURE(s->fr_e, 8 * m);
+        if (nb) k_fric_lag<<<grid_for(nb, 128), 128, 0, c->stream>>>(s->pg, P, ps, s->alist.as<int>(), nb, dhat, kappa, s->fric());
+    }
+    if (s->fr_n) {
+        k_fric_eval<<<grid_for(s->fr_n, 128), 128, 0, c->stream>>>(s->fric(), ps, s->fr_mu, s->fr_eps, n, s->fr_e.as<double>(), o);
+        k_tree_sum<<<1, 1024, 0, c->stream>>>(s->fr_e.as<double>(), s->fr_n, &ds->fenergy);
+        k_iota<<<grid_for(s->fr_n, 256), 256, 0, c->stream>>>(s->alist.as<int>(), &ds->na, n, s->fr_n);
+    }
+    // contributions: the active barrier pairs (pair order), then the friction pairs
+    const int na = nb + s->fr_n;
     IPC_ENSURE(s->gout, 48 * (size_t)N);
     IPC_ENSURE(s->rowptr, 4 * (size_t)(N + 1));
     NXD_CUDA(cudaMemsetAsync(s->gout.p, 0, 48 * (size_t)N, c->stream));
@@ -1767,6 +1807,7 @@ nxd_status ipc_trial_energy(nxd_ctx* c, const double* xt, double dhat, double ka
     k_ipc_pair_energy_dev<<<grid_for((long long)cap_pt + cap_ee, 128), 128, 0, c->stream>>>(
         s->pg, s->pt.as<int>(), s->ee.as<int>(), ds->tot, cap_pt, cap_ee, ps, dhat, kappa, s->e.as<double>());
     k_tree_sum_pairs<<<1, 1024, 0, c->stream>>>(s->e.as<double>(), ds->tot, cap_pt, cap_ee, &ds->energy);
+    if (s->fr_n) ipc_friction_energy(c, ps);
     if ((st = ipc_fetch(c)) != NXD_OK) return st;
     const IpcScal& hs = s->hp->sc;
     if (hs.status != 0) return (nxd_status)hs.status;
@@ -1850,7 +1891,8 @@ nxd_status nxd_ipc_max_step(nxd_ctx* c, const double* x, const double* dx, doubl
 nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_stats* out) {
     if (!c || !p || !(dt > 0.0) || !(p->dhat > 0.0) || !(p->kappa >= 0.0) || !(p->eta > 0.0 && p->eta < 1.0) ||
         p->newton_max_iters < 0 || p->ls_max_iters < 1 || p->linear_solver < 0 || p->linear_solver > 1 ||
-        (p->linear_solver == 1 && (p->pcg_max_iter < 1 || !(p->pcg_tol >= 0.0))))
+        (p->linear_solver == 1 && (p->pcg_max_iter < 1 || !(p->pcg_tol >= 0.0))) || !(p->mu >= 0.0) ||
+        (p->mu > 0.0 && (!(p->friction_eps > 0.0) || p->friction_iters < 1)))
         return NXD_INVALID_ARGUMENT;
     nxd_status st = ipc_prepare(c);
     if (st != NXD_OK) return st;
@@ -1896,124 +1938,148 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
     // the hierarchies built at the first iterate serve the whole step
     struct TreeScope {
         IpcState* s;
-        ~TreeScope() { s->keep_trees = false; }
+        ~TreeScope() { s->keep_trees = false; s->fr_n = 0; s->fr_build = false; }
     } tree_scope{s};
     s->keep_trees = false;
-    for (int it = 0; it < p->newton_max_iters; ++it) {
-        iters = it;
-        // gradient at x: rest forms, then the barrier over the candidates at x
-        k_form_eval<<<1, ft, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 1, x, s->gr.as<double>(), nullptr, nullptr,
-                                                  nullptr, 0, nullptr);
-        // after an accepted trial the poses and candidates at x = xt (boxes
-        // inflated by dhat) are the trial's, still in place
-        st = NXD_OK;
-        if (!cand_at_x) {
-            st = ipc_pose(c, x, nullptr, true);
-            if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
-            s->keep_trees = true;
-        }
+    // lagged friction: pass 0 freezes the pairs active at the step start,
+    // each further pass those at the previous pass's solution and solves again
+    const bool friction = p->mu > 0.0;
+    const int passes = friction ? p->friction_iters : 1;
+    s->fr_n = 0;
+    s->fr_mu = p->mu;
+    s->fr_eps = friction ? p->friction_eps : 1e-8;
+    int iters_done = 0;
+    int64_t nfric = 0;
+    for (int pass = 0; pass < passes; ++pass) {
+        s->fr_build = friction;
         cand_at_x = false;
-        if (st == NXD_OK) st = ipc_barrier_eval(c, p->dhat, p->kappa, true, nullptr);
-        if (st != NXD_OK) return st;
-        const double eb = hs.energy;
-        na = hs.na;
-        npairs = s->n_pt + s->n_ee;
-        k_grad_combine<<<grid_for(n6, 256), 256, 0, sm>>>(s->gr.as<double>(), s->gout.as<double>(), scale, n6,
-                                                          s->gt.as<double>(), s->gneg.as<double>());
-        k_absmax<<<1, 1024, 0, sm>>>(s->gt.as<double>(), n6, &ds->ginf);
-        // the rest forms' Hessian blocks and both row pointers come back with
-        // |g|_inf in one wait (unused when the gradient test ends the solve)
-        k_form_eval<<<1, ft, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 2, x, nullptr, s->rrp.as<int>(), s->rci.as<int>(),
-                                                  s->rvv.as<double>(), cap_r, &ds->rnz);
-        NXD_CUDA(cudaMemcpyAsync(rpr, s->rrp.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, sm));
-        NXD_CUDA(cudaMemcpyAsync(rpb, s->rowptr.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, sm));
-        if ((st = ipc_fetch(c)) != NXD_OK) return st;
-        if (hs.ginf < p->newton_tol) { conv = 1; break; }
-        if (hs.rnz < 0 || hs.rnz > cap_r) return NXD_CAPACITY;
-        // Hessian: rest-form blocks, then the barrier's, row by row
-        rpm[0] = 0;
-        for (int i = 0; i < N; ++i) rpm[i + 1] = rpm[i] + (rpr[i + 1] - rpr[i]) + (rpb[i + 1] - rpb[i]);
-        const int nh = rpb[N];
-        const long long nzm = rpm[N];
-        IPC_ENSURE(s->mci, 4 * (size_t)std::max<long long>(nzm, 1)); IPC_ENSURE(s->mvv, 288 * (size_t)std::max<long long>(nzm, 1));
-        IPC_ENSURE(s->erow, 4 * (size_t)std::max<long long>(nzm, 1)); IPC_ENSURE(s->items, 4 * (size_t)std::max<long long>(nzm, 1));
-        IPC_ENSURE(s->iact, 4 * (size_t)std::max<long long>(nzm, 1));
-        NXD_CUDA(cudaMemcpyAsync(s->mrp.p, rpm, 4 * (size_t)(N + 1), cudaMemcpyHostToDevice, sm));
-        k_bsr_concat<<<grid_for(N, 128), 128, 0, sm>>>(N, s->rrp.as<int>(), s->rci.as<int>(), s->rvv.as<double>(),
-                                                       nh ? s->rowptr.as<int>() : nullptr, s->colidx.as<int>(),
-                                                       s->vals.as<double>(), scale, s->mrp.as<int>(), s->mci.as<int>(),
-                                                       s->mvv.as<double>());
-        // H dx = -g: block-Jacobi PCG, or the component LDL^T
-        s->hp->fail = 0;
-        s->hp->capst = 0;
-        if (p->linear_solver == 1) {
-            int pit = 0;
-            double pres = 0.0;
-            const nxd_status pr = pcg_device(c, s->pcg, N, s->mrp.as<int>(), s->mci.as<int>(), s->mvv.as<double>(),
-                                             s->gneg.as<double>(), c->S.dx, p->pcg_tol, p->pcg_max_iter, &pit, &pres,
-                                             nullptr, nullptr);
-            if (pr == NXD_CUDA_ERROR) return pr;
-            pcg_total += pit;
-            if (pr != NXD_OK) { solvefail = 1; break; }
-        } else {
-            Solver S = c->S;
-            S.ext_n = (int)nzm; S.ext_row = s->erow.as<int>(); S.ext_col = s->mci.as<int>(); S.ext_vals = s->mvv.as<double>();
-            S.items = s->items.as<int>(); S.iact = s->iact.as<int>(); S.status = s->stat.as<int>();
-            NXD_CUDA(cudaMemsetAsync(s->stat.p, 0, sizeof(int), sm));
-            k_bsr_prepare<<<grid_for(N, 128), 128, 0, sm>>>(S, s->mrp.as<int>(), s->gneg.as<double>(), s->erow.as<int>());
-            k_linear_solve<<<1, kNewtonThreads, kNewtonDynSmem, sm>>>(S);
-            NXD_CUDA(cudaMemcpyAsync(&s->hp->fail, S.solve_fail, sizeof(int), cudaMemcpyDeviceToHost, sm));
-            NXD_CUDA(cudaMemcpyAsync(&s->hp->capst, s->stat.p, sizeof(int), cudaMemcpyDeviceToHost, sm));
-        }
-        double* dx = c->S.dx;
-        k_absmax<<<1, 1024, 0, sm>>>(dx, n6, &ds->dxinf);
-        // the swept candidates of the step bound are counted before the wait
-        // that reads the solve's flags (discarded when those end the loop)
-        st = ipc_pose(c, x, dx, true);
-        if (st == NXD_OK) st = ipc_candidates_begin(c, true, 0.0);
-        if (st == NXD_OK) st = ipc_fetch(c);
-        if (st != NXD_OK) return st;
-        if (s->hp->capst) return NXD_CAPACITY;
-        if (s->hp->fail) { solvefail = 1; break; }
-        // the velocity criterion of IPC: a Newton step below tol * dt ends it
-        if (hs.dxinf < p->newton_tol * dt) { conv = 1; break; }
-        // the step bound (additive CCD over the swept candidates), the value
-        // at x and the descent g . dx, read back in one wait
-        st = ipc_candidates_end(c);
-        if (st == NXD_OK) st = ipc_accd(c, p->eta);
-        if (st != NXD_OK) return st;
-        rest_value(x);
-        k_mul_vec<<<grid_for(n6, 256), 256, 0, sm>>>(s->gt.as<double>(), dx, n6, s->prod.as<double>());
-        k_tree_sum<<<1, 1024, 0, sm>>>(s->prod.as<double>(), n6, &ds->descent);
-        if ((st = ipc_fetch(c)) != NXD_OK) return st;
-        amax = hs.alpha;
-        fx = hs.rest + scale * eb;
-        const double descent = hs.descent;
-        if (descent > 0) { lsfail = 1; break; }
-        // line search from min(1, bound)
-        double alpha = std::min(1.0, amax);
-        bool done = false;
-        for (int ls = 0; ls < p->ls_max_iters; ++ls) {
-            k_axpy_alpha<<<grid_for(n6, 256), 256, 0, sm>>>(x, dx, alpha, n6, s->xt.as<double>());
-            rest_value(s->xt.as<double>());
-            bool one_wait = false;
-            st = ipc_trial_energy(c, s->xt.as<double>(), p->dhat, p->kappa, &one_wait);
-            if (st == NXD_OK && !one_wait) {
-                st = ipc_pose(c, s->xt.as<double>(), nullptr, true);
+        conv = 0;
+        iters = 0;
+        for (int it = 0; it < p->newton_max_iters; ++it) {
+            iters = it;
+            // gradient at x: rest forms, then the barrier over the candidates at x
+            k_form_eval<<<1, ft, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 1, x, s->gr.as<double>(), nullptr, nullptr,
+                                                      nullptr, 0, nullptr);
+            // after an accepted trial the poses and candidates at x = xt (boxes
+            // inflated by dhat) are the trial's, still in place
+            st = NXD_OK;
+            if (!cand_at_x) {
+                st = ipc_pose(c, x, nullptr, true);
                 if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
-                if (st == NXD_OK) st = ipc_barrier_eval(c, p->dhat, p->kappa, false, nullptr);
-                if (st == NXD_OK) st = ipc_fetch(c);
+                s->keep_trees = true;
+                if (st == NXD_OK && friction && pass == 0 && it == 0) {
+                    // the step-start world vertices (x = the step-start configuration)
+                    IPC_ENSURE(s->fr_x0, 24 * (size_t)std::max(c->nv, 1));
+                    NXD_CUDA(cudaMemcpyAsync(s->fr_x0.p, s->wq0.p, 24 * (size_t)c->nv, cudaMemcpyDeviceToDevice, sm));
+                }
             }
+            cand_at_x = false;
+            if (st == NXD_OK) st = ipc_barrier_eval(c, p->dhat, p->kappa, true, nullptr);
             if (st != NXD_OK) return st;
-            const double fn = hs.rest + scale * hs.energy;
-            if (fn <= fx + c->s.ls_c1 * alpha * descent) { done = true; fx = fn; break; }
-            alpha *= c->s.ls_rho;
+            const double eb = hs.energy;   // the friction energy follows in the next fetch
+            na = hs.na;
+            nfric = s->fr_n;
+            npairs = s->n_pt + s->n_ee;
+            k_grad_combine<<<grid_for(n6, 256), 256, 0, sm>>>(s->gr.as<double>(), s->gout.as<double>(), scale, n6,
+                                                              s->gt.as<double>(), s->gneg.as<double>());
+            k_absmax<<<1, 1024, 0, sm>>>(s->gt.as<double>(), n6, &ds->ginf);
+            // the rest forms' Hessian blocks and both row pointers come back with
+            // |g|_inf in one wait (unused when the gradient test ends the solve)
+            k_form_eval<<<1, ft, 0, sm>>>(c->S, c->sc, NXD_FORM_TOTAL, 2, x, nullptr, s->rrp.as<int>(), s->rci.as<int>(),
+                                                      s->rvv.as<double>(), cap_r, &ds->rnz);
+            NXD_CUDA(cudaMemcpyAsync(rpr, s->rrp.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, sm));
+            NXD_CUDA(cudaMemcpyAsync(rpb, s->rowptr.p, 4 * (size_t)(N + 1), cudaMemcpyDeviceToHost, sm));
+            if ((st = ipc_fetch(c)) != NXD_OK) return st;
+            if (hs.ginf < p->newton_tol) { conv = 1; break; }
+            if (hs.rnz < 0 || hs.rnz > cap_r) return NXD_CAPACITY;
+            // Hessian: rest-form blocks, then the barrier's, row by row
+            rpm[0] = 0;
+            for (int i = 0; i < N; ++i) rpm[i + 1] = rpm[i] + (rpr[i + 1] - rpr[i]) + (rpb[i + 1] - rpb[i]);
+            const int nh = rpb[N];
+            const long long nzm = rpm[N];
+            IPC_ENSURE(s->mci, 4 * (size_t)std::max<long long>(nzm, 1)); IPC_ENSURE(s->mvv, 288 * (size_t)std::max<long long>(nzm, 1));
+            IPC_ENSURE(s->erow, 4 * (size_t)std::max<long long>(nzm, 1)); IPC_ENSURE(s->items, 4 * (size_t)std::max<long long>(nzm, 1));
+            IPC_ENSURE(s->iact, 4 * (size_t)std::max<long long>(nzm, 1));
+            NXD_CUDA(cudaMemcpyAsync(s->mrp.p, rpm, 4 * (size_t)(N + 1), cudaMemcpyHostToDevice, sm));
+            k_bsr_concat<<<grid_for(N, 128), 128, 0, sm>>>(N, s->rrp.as<int>(), s->rci.as<int>(), s->rvv.as<double>(),
+                                                           nh ? s->rowptr.as<int>() : nullptr, s->colidx.as<int>(),
+                                                           s->vals.as<double>(), scale, s->mrp.as<int>(), s->mci.as<int>(),
+                                                           s->mvv.as<double>());
+            // H dx = -g: block-Jacobi PCG, or the component LDL^T
+            s->hp->fail = 0;
+            s->hp->capst = 0;
+            if (p->linear_solver == 1) {
+                int pit = 0;
+                double pres = 0.0;
+                const nxd_status pr = pcg_device(c, s->pcg, N, s->mrp.as<int>(), s->mci.as<int>(), s->mvv.as<double>(),
+                                                 s->gneg.as<double>(), c->S.dx, p->pcg_tol, p->pcg_max_iter, &pit, &pres,
+                                                 nullptr, nullptr);
+                if (pr == NXD_CUDA_ERROR) return pr;
+                pcg_total += pit;
+                if (pr != NXD_OK) { solvefail = 1; break; }
+            } else {
+                Solver S = c->S;
+                S.ext_n = (int)nzm; S.ext_row = s->erow.as<int>(); S.ext_col = s->mci.as<int>(); S.ext_vals = s->mvv.as<double>();
+                S.items = s->items.as<int>(); S.iact = s->iact.as<int>(); S.status = s->stat.as<int>();
+                NXD_CUDA(cudaMemsetAsync(s->stat.p, 0, sizeof(int), sm));
+                k_bsr_prepare<<<grid_for(N, 128), 128, 0, sm>>>(S, s->mrp.as<int>(), s->gneg.as<double>(), s->erow.as<int>());
+                k_linear_solve<<<1, kNewtonThreads, kNewtonDynSmem, sm>>>(S);
+                NXD_CUDA(cudaMemcpyAsync(&s->hp->fail, S.solve_fail, sizeof(int), cudaMemcpyDeviceToHost, sm));
+                NXD_CUDA(cudaMemcpyAsync(&s->hp->capst, s->stat.p, sizeof(int), cudaMemcpyDeviceToHost, sm));
+            }
+            double* dx = c->S.dx;
+            k_absmax<<<1, 1024, 0, sm>>>(dx, n6, &ds->dxinf);
+            // the swept candidates of the step bound are counted before the wait
+            // that reads the solve's flags (discarded when those end the loop)
+            st = ipc_pose(c, x, dx, true);
+            if (st == NXD_OK) st = ipc_candidates_begin(c, true, 0.0);
+            if (st == NXD_OK) st = ipc_fetch(c);
+            if (st != NXD_OK) return st;
+            if (s->hp->capst) return NXD_CAPACITY;
+            if (s->hp->fail) { solvefail = 1; break; }
+            // the velocity criterion of IPC: a Newton step below tol * dt ends it
+            if (hs.dxinf < p->newton_tol * dt) { conv = 1; break; }
+            // the step bound (additive CCD over the swept candidates), the value
+            // at x and the descent g . dx, read back in one wait
+            st = ipc_candidates_end(c);
+            if (st == NXD_OK) st = ipc_accd(c, p->eta);
+            if (st != NXD_OK) return st;
+            rest_value(x);
+            k_mul_vec<<<grid_for(n6, 256), 256, 0, sm>>>(s->gt.as<double>(), dx, n6, s->prod.as<double>());
+            k_tree_sum<<<1, 1024, 0, sm>>>(s->prod.as<double>(), n6, &ds->descent);
+            if ((st = ipc_fetch(c)) != NXD_OK) return st;
+            amax = hs.alpha;
+            fx = hs.rest + scale * (s->fr_n ? eb + hs.fenergy : eb);
+            const double descent = hs.descent;
+            if (descent > 0) { lsfail = 1; break; }
+            // line search from min(1, bound)
+            double alpha = std::min(1.0, amax);
+            bool done = false;
+            for (int ls = 0; ls < p->ls_max_iters; ++ls) {
+                k_axpy_alpha<<<grid_for(n6, 256), 256, 0, sm>>>(x, dx, alpha, n6, s->xt.as<double>());
+                rest_value(s->xt.as<double>());
+                bool one_wait = false;
+                st = ipc_trial_energy(c, s->xt.as<double>(), p->dhat, p->kappa, &one_wait);
+                if (st == NXD_OK && !one_wait) {
+                    st = ipc_pose(c, s->xt.as<double>(), nullptr, true);
+                    if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
+                    if (st == NXD_OK) st = ipc_barrier_eval(c, p->dhat, p->kappa, false, nullptr);
+                    if (st == NXD_OK) st = ipc_fetch(c);
+                }
+                if (st != NXD_OK) return st;
+                const double fn = hs.rest + scale * (s->fr_n ? hs.energy + hs.fenergy : hs.energy);
+                if (fn <= fx + c->s.ls_c1 * alpha * descent) { done = true; fx = fn; break; }
+                alpha *= c->s.ls_rho;
+            }
+            if (!done) { lsfail = 1; break; }
+            cand_at_x = true;
+            NXD_CUDA(cudaMemcpyAsync(x, s->xt.p, 8 * (size_t)n6, cudaMemcpyDeviceToDevice, sm));
+            if (it == p->newton_max_iters - 1) iters = p->newton_max_iters;
         }
-        if (!done) { lsfail = 1; break; }
-        cand_at_x = true;
-        NXD_CUDA(cudaMemcpyAsync(x, s->xt.p, 8 * (size_t)n6, cudaMemcpyDeviceToDevice, sm));
-        if (it == p->newton_max_iters - 1) iters = p->newton_max_iters;
+        iters_done += iters;
+        if (!conv) break;   // a pass that did not converge ends the step
     }
+    iters = iters_done;
     k_update_state<<<grid_for(N, 128), 128, 0, sm>>>(cfg, c->x, c->xprev, c->vprev, c->xhat, c->aprev, c->pos, c->quat, c->vel,
                                                    c->omega, c->lacc, c->aacc, c->sc, c->da, c->db, c->dprm, c->dfilt);
     NXD_CUDA(cudaStreamSynchronize(sm));
@@ -2021,14 +2087,15 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
     if (out) {
         out->newton_iterations = iters; out->converged = conv; out->line_search_failed = lsfail;
         out->solve_failed = solvefail; out->last_alpha_max = amax; out->energy = fx; out->n_pairs = npairs;
-        out->n_active = na; out->pcg_iterations = pcg_total;
+        out->n_active = na; out->pcg_iterations = pcg_total; out->n_friction = nfric;
     }
     return solvefail ? NXD_FACTOR_FAILED : NXD_OK;
 }
 
 nxd_status nxd_ipc_adjoint(nxd_ctx* c, double dt, const nxd_ipc_params* p, const nxd_state* start, const double* x_star,
                            const double* x_bar, const nxd_ipc_adjoint_out* out) {
-    if (!c || !p || !start || !x_star || !x_bar || !out || !(dt > 0.0) || !(p->dhat > 0.0) || !(p->kappa >= 0.0))
+    if (!c || !p || !start || !x_star || !x_bar || !out || !(dt > 0.0) || !(p->dhat > 0.0) || !(p->kappa >= 0.0) ||
+        p->mu != 0.0)
         return NXD_INVALID_ARGUMENT;
     const int N = c->N, J = c->J, n6 = 6 * N;
     if (N > kAdjMaxBodies || c->D > 0 || c->s.integrator == NXD_INTEGRATOR_IMPLICIT_NEWMARK) return NXD_INVALID_ARGUMENT;

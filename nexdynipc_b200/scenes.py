@@ -587,14 +587,17 @@ def ipc_drop(seed: int = 7000, n_cubes: int = 2, columns: int = 1) -> Scene:
     return sb.build(s, dt=1e-2, steps=80)
 
 
-def ipc_step_settings(solver: int = 0) -> dict:
+def ipc_step_settings(solver: int = 0, mu: float = 0.0) -> dict:
     """Keyword arguments of abi.ipc_params for the full-IPC steps run on
     ipc_drop and on sphere_bowl: dhat 1e-3, kappa 1e11, eta 0.1 (the CCD
     bound keeps 90 % of each pair's distance), Newton until |g|_inf < 1e-5
     (or the step below 1e-5 dt) in at most 50 iterations, 30 Armijo trials;
-    solver 0 = component LDL^T, 1 = block-Jacobi PCG (500 iterations, 1e-12)."""
+    solver 0 = component LDL^T, 1 = block-Jacobi PCG (500 iterations, 1e-12).
+    mu > 0 adds lagged friction with eps 1e-5 m over 2 lagging passes (the
+    reference's default eps of 1e-8 m makes the sticking branch 1000x
+    stiffer, and Newton then stalls at its iteration limit on the bowl)."""
     return dict(dhat=1e-3, kappa=1e11, eta=0.1, newton_tol=1e-5, newton_max_iters=50, ls_max_iters=30,
-                linear_solver=solver, pcg_max_iter=500, pcg_tol=1e-12)
+                linear_solver=solver, pcg_max_iter=500, pcg_tol=1e-12, mu=mu, friction_eps=1e-5, friction_iters=2)
 
 
 def diff_scene(seed: int = 5000) -> Scene:

@@ -192,6 +192,18 @@ void pair_points(const Geo& g, const std::vector<int32_t>& pt, const std::vector
     }
 }
 
+void pair_vids(const Geo& g, const std::vector<int32_t>& pt, const std::vector<int32_t>& ee, size_t p, int* vid) {
+    const size_t npt = pt.size() / 2;
+    if (p < npt) {
+        const int v = pt[2 * p], f = pt[2 * p + 1];
+        vid[0] = v; vid[1] = g.fvert[3 * f]; vid[2] = g.fvert[3 * f + 1]; vid[3] = g.fvert[3 * f + 2];
+    } else {
+        const size_t q = p - npt;
+        vid[0] = g.evert[2 * ee[2 * q]]; vid[1] = g.evert[2 * ee[2 * q] + 1];
+        vid[2] = g.evert[2 * ee[2 * q + 1]]; vid[3] = g.evert[2 * ee[2 * q + 1] + 1];
+    }
+}
+
 // the device's fixed pairwise tree (pad to a power of two, halve)
 double tree_sum(std::vector<double> v) {
     size_t P = 1;
@@ -277,20 +289,60 @@ int nxo_ipc_candidates(nxo_world* w, const double* x, const double* dx, double i
 // nxo_ipc_barrier with, in `blocks` (when given), the body blocks the active
 // pairs touch: (a, a), (a, b), (b, a), (b, b) for each, sorted by (row, col),
 // the block structure of the device's BSR Hessian.
+// Lagged friction of a full-IPC step (ipc::friction_pair on frozen pairs):
+// `build` makes the next barrier evaluation freeze the pairs active there
+// (pair order); x0 holds the step-start world vertices, taken at the first
+// build.  The last evaluation's friction energy is in `energy`.
+struct IpcFricCtx {
+    double mu = 0.0, eps = 1e-8;
+    bool build = true;
+    bool only = false;   // gradient and Hessian of the friction alone
+    std::vector<double> x0;
+    struct Pair { int vid[4], body[2], kind; ipc::FricLag L; };
+    std::vector<Pair> set;
+    double energy = 0.0;
+};
+IpcFricCtx* ipc_fric_new(double mu, double eps) {
+    auto* f = new IpcFricCtx();
+    f->mu = mu; f->eps = eps;
+    return f;
+}
+void ipc_fric_free(IpcFricCtx* f) { delete f; }
+void ipc_fric_rebuild(IpcFricCtx* f) { f->build = true; }
+int64_t ipc_fric_count(const IpcFricCtx* f) { return (int64_t)f->set.size(); }
+double ipc_fric_energy(const IpcFricCtx* f) { return f->energy; }
+
 int ipc_barrier_cpu(nxo_world* w, const double* x, double dhat, double kappa, double* energy, double* grad, double* H,
-                    std::vector<std::pair<int, int>>* blocks, int64_t* n_pairs, int64_t* n_active);
+                    std::vector<std::pair<int, int>>* blocks, int64_t* n_pairs, int64_t* n_active, IpcFricCtx* fr);
 
 extern "C" {
 
 int nxo_ipc_barrier(nxo_world* w, const double* x, double dhat, double kappa, double* energy, double* grad, double* H,
                     int64_t* n_pairs, int64_t* n_active) {
-    return ipc_barrier_cpu(w, x, dhat, kappa, energy, grad, H, nullptr, n_pairs, n_active);
+    return ipc_barrier_cpu(w, x, dhat, kappa, energy, grad, H, nullptr, n_pairs, n_active, nullptr);
+}
+
+// Friction alone, for checking its derivatives: the pairs active at x_lag
+// frozen there (x0 = the world vertices at x_lag), the friction energy,
+// gradient (6N) and Gauss-Newton Hessian (dense 6N x 6N, or NULL) at x.
+int nxo_ipc_friction(nxo_world* w, const double* x_lag, const double* x, double dhat, double kappa, double mu, double eps,
+                     double* energy, double* grad, double* H, int64_t* n_friction) {
+    IpcFricCtx fr;
+    fr.mu = mu; fr.eps = eps; fr.only = true;
+    const int N6 = 6 * nxo_body_count(w);
+    std::vector<double> g(N6);
+    double e = 0.0;
+    ipc_barrier_cpu(w, x_lag, dhat, kappa, &e, g.data(), nullptr, nullptr, nullptr, nullptr, &fr);
+    ipc_barrier_cpu(w, x, dhat, kappa, &e, grad, H, nullptr, nullptr, nullptr, &fr);
+    *energy = fr.energy;
+    if (n_friction) *n_friction = (int64_t)fr.set.size();
+    return NXD_OK;
 }
 
 }  // extern "C"
 
 int ipc_barrier_cpu(nxo_world* w, const double* x, double dhat, double kappa, double* energy, double* grad, double* H,
-                    std::vector<std::pair<int, int>>* blocks, int64_t* n_pairs, int64_t* n_active) {
+                    std::vector<std::pair<int, int>>* blocks, int64_t* n_pairs, int64_t* n_active, IpcFricCtx* fr) {
     const Geo g = load(w, x, nullptr);
     std::vector<int32_t> P, E;
     candidates(g, dhat, P, E);
@@ -332,6 +384,65 @@ int ipc_barrier_cpu(nxo_world* w, const double* x, double dhat, double kappa, do
                         ah.push_back(blk);
                     }
     }
+    const size_t nbar = ab.size() / 2;
+    if (fr && fr->only) {
+        ab.clear(); ag.clear(); ah.clear();
+        if (blocks) blocks->clear();
+    }
+    if (fr && fr->build) {
+        // freeze the active pairs here (pair order)
+        fr->build = false;
+        if (fr->x0.empty()) fr->x0 = g.wv;
+        fr->set.clear();
+        for (size_t p = 0; p < n; ++p) {
+            int kind, side[4], bA, bB;
+            V3 X[4], arm[4];
+            pair_points(g, P, E, p, kind, X, side, arm, bA, bB);
+            const ipc::DistForm f = ipc::classify(kind, X);
+            IpcFricCtx::Pair fp;
+            if (!ipc::friction_lag(f, X, dhat, kappa, fp.L)) continue;
+            pair_vids(g, P, E, p, fp.vid);
+            fp.body[0] = bA; fp.body[1] = bB; fp.kind = kind;
+            fr->set.push_back(fp);
+        }
+    }
+    if (fr) {
+        // the frozen pairs after the active barrier pairs, energies in their own tree
+        std::vector<double> ef(fr->set.size());
+        for (size_t q = 0; q < fr->set.size(); ++q) {
+            const IpcFricCtx::Pair& fp = fr->set[q];
+            const int side[4] = {0, fp.kind == ipc::kPairPT ? 1 : 0, 1, 1};
+            V3 X[4], X0[4], arm[4];
+            for (int k = 0; k < 4; ++k) {
+                X[k] = nx::ld3(&g.wv[3 * fp.vid[k]]);
+                X0[k] = nx::ld3(&fr->x0[3 * fp.vid[k]]);
+                arm[k] = X[k] - nx::ld3(&g.pos[3 * fp.body[side[k]]]);
+            }
+            const ipc::FricEval ev = ipc::friction_pair(fp.L, X, X0, fr->mu, fr->eps);
+            ef[q] = ev.e;
+            ab.push_back(fp.body[0]); ab.push_back(fp.body[1]);
+            double g12[12];
+            const V3 thA = nx::ld3(&g.theta[3 * fp.body[0]]), thB = nx::ld3(&g.theta[3 * fp.body[1]]);
+            ipc::chain12_exact(ev.grad, side, arm, thA, thB, g12);
+            ag.insert(ag.end(), g12, g12 + 12);
+            if (!H) continue;
+            double z[2][12];
+            for (int k = 0; k < 2; ++k) ipc::chain12_exact(ev.y[k], side, arm, thA, thB, z[k]);
+            for (int r = 0; r < 2; ++r)
+                for (int c = 0; c < 2; ++c)
+                    for (int i = 0; i < 6; ++i)
+                        for (int j = 0; j < 6; ++j) {
+                            double blk = 0.0;
+                            for (int k = 0; k < 2; ++k) blk += (ev.lam[k] * z[k][6 * r + i]) * z[k][6 * c + j];
+                            ah.push_back(blk);
+                        }
+            if (blocks) {
+                blocks->push_back({fp.body[0], fp.body[0]}); blocks->push_back({fp.body[0], fp.body[1]});
+                blocks->push_back({fp.body[1], fp.body[0]}); blocks->push_back({fp.body[1], fp.body[1]});
+            }
+        }
+        fr->energy = tree_sum(ef);
+    }
     const size_t na = ab.size() / 2;
     // each gradient entry / block entry: its contributions in pair order,
     // summed as the device sums a segment (seg_sum)
@@ -362,7 +473,7 @@ int ipc_barrier_cpu(nxo_world* w, const double* x, double dhat, double kappa, do
     }
     if (energy) *energy = tree_sum(e);
     if (n_pairs) *n_pairs = (int64_t)n;
-    if (n_active) *n_active = (int64_t)na;
+    if (n_active) *n_active = (int64_t)nbar;
     if (blocks) {
         std::sort(blocks->begin(), blocks->end());
         blocks->erase(std::unique(blocks->begin(), blocks->end()), blocks->end());

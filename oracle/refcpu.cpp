@@ -43,9 +43,17 @@
 #endif
 
 
-// primitive-pair barrier of ipc_cpu.cpp with its block structure
+// primitive-pair barrier of ipc_cpu.cpp with its block structure, and its
+// lagged friction (IpcFricCtx: the frozen pairs, built at the evaluation
+// after ipc_fric_rebuild)
+struct IpcFricCtx;
+IpcFricCtx* ipc_fric_new(double mu, double eps);
+void ipc_fric_free(IpcFricCtx* f);
+void ipc_fric_rebuild(IpcFricCtx* f);
+int64_t ipc_fric_count(const IpcFricCtx* f);
+double ipc_fric_energy(const IpcFricCtx* f);
 int ipc_barrier_cpu(nxo_world* w, const double* x, double dhat, double kappa, double* energy, double* grad, double* H,
-                    std::vector<std::pair<int, int>>* blocks, int64_t* n_pairs, int64_t* n_active);
+                    std::vector<std::pair<int, int>>* blocks, int64_t* n_pairs, int64_t* n_active, IpcFricCtx* fr);
 
 namespace {
 
@@ -2446,53 +2454,69 @@ int nxo_ipc_step(nxo_world* w, double dt, const nxd_ipc_params* p, nxd_ipc_stats
     std::vector<double> xn = x, gr, gb(n), g(n), Hb((size_t)n * n), dx, xt(n), prod(n);
     std::vector<Trip> trips;
     std::vector<std::pair<int, int>> blocks;
-    int iters = 0, conv = 0, lsfail = 0, solvefail = 0;
-    int64_t npairs = 0, na = 0;
+    int iters = 0, conv = 0, lsfail = 0, solvefail = 0, iters_done = 0;
+    int64_t npairs = 0, na = 0, nfric = 0;
     double amax = 1.0, fx = 0.0;
-    for (int it = 0; it < p->newton_max_iters; ++it) {
-        iters = it;
-        problem_gradient(w, xn, gr);
-        double eb = 0.0;
-        blocks.clear();
-        ipc_barrier_cpu(w, xn.data(), p->dhat, p->kappa, &eb, gb.data(), Hb.data(), &blocks, &npairs, &na);
-        for (int i = 0; i < n; ++i) g[i] = gr[i] + sc * gb[i];
-        double ginf = 0.0;
-        for (double vv : g) ginf = std::max(ginf, std::fabs(vv));
-        if (ginf < p->newton_tol) { conv = 1; break; }
-        problem_hessian(w, xn, trips);
-        for (const auto& bl : blocks)
-            for (int r = 0; r < 6; ++r)
-                for (int c = 0; c < 6; ++c) {
-                    const int gi = 6 * bl.first + r, gj = 6 * bl.second + c;
-                    trips.push_back({gi, gj, Hb[(size_t)gi * n + gj] * sc});
-                }
-        std::vector<double> rhs(n);
-        for (int i = 0; i < n; ++i) rhs[i] = -g[i];
-        if (!solve_system(n, trips, rhs, dx)) { solvefail = 1; break; }
-        double dxinf = 0.0;
-        for (double vv : dx) dxinf = std::max(dxinf, std::fabs(vv));
-        if (dxinf < p->newton_tol * dt) { conv = 1; break; }
-        int64_t np2 = 0;
-        amax = nxo_ipc_max_step(w, xn.data(), dx.data(), p->eta, &np2);
-        fx = problem_value(w, xn) + sc * eb;
-        for (int i = 0; i < n; ++i) prod[i] = g[i] * dx[i];
-        const double descent = tree_sum(prod);
-        if (descent > 0) { lsfail = 1; break; }
-        double alpha = std::min(1.0, amax);
-        bool done = false;
-        for (int ls = 0; ls < p->ls_max_iters; ++ls) {
-            for (int i = 0; i < n; ++i) xt[i] = xn[i] + alpha * dx[i];
-            const double ert = problem_value(w, xt);
-            double ebt = 0.0;
-            ipc_barrier_cpu(w, xt.data(), p->dhat, p->kappa, &ebt, nullptr, nullptr, nullptr, nullptr, nullptr);
-            const double fn = ert + sc * ebt;
-            if (fn <= fx + s.ls_c1 * alpha * descent) { done = true; fx = fn; break; }
-            alpha *= s.ls_rho;
+    // lagged friction: pass 0 freezes the pairs active at the step start,
+    // each further pass those at the previous pass's solution
+    const bool friction = p->mu > 0.0;
+    const int passes = friction ? p->friction_iters : 1;
+    IpcFricCtx* fr = friction ? ipc_fric_new(p->mu, p->friction_eps) : nullptr;
+    for (int pass = 0; pass < passes; ++pass) {
+        if (fr) ipc_fric_rebuild(fr);
+        conv = 0;
+        iters = 0;
+        for (int it = 0; it < p->newton_max_iters; ++it) {
+            iters = it;
+            problem_gradient(w, xn, gr);
+            double eb = 0.0;
+            blocks.clear();
+            ipc_barrier_cpu(w, xn.data(), p->dhat, p->kappa, &eb, gb.data(), Hb.data(), &blocks, &npairs, &na, fr);
+            if (fr) { eb = eb + ipc_fric_energy(fr); nfric = ipc_fric_count(fr); }
+            for (int i = 0; i < n; ++i) g[i] = gr[i] + sc * gb[i];
+            double ginf = 0.0;
+            for (double vv : g) ginf = std::max(ginf, std::fabs(vv));
+            if (ginf < p->newton_tol) { conv = 1; break; }
+            problem_hessian(w, xn, trips);
+            for (const auto& bl : blocks)
+                for (int r = 0; r < 6; ++r)
+                    for (int c = 0; c < 6; ++c) {
+                        const int gi = 6 * bl.first + r, gj = 6 * bl.second + c;
+                        trips.push_back({gi, gj, Hb[(size_t)gi * n + gj] * sc});
+                    }
+            std::vector<double> rhs(n);
+            for (int i = 0; i < n; ++i) rhs[i] = -g[i];
+            if (!solve_system(n, trips, rhs, dx)) { solvefail = 1; break; }
+            double dxinf = 0.0;
+            for (double vv : dx) dxinf = std::max(dxinf, std::fabs(vv));
+            if (dxinf < p->newton_tol * dt) { conv = 1; break; }
+            int64_t np2 = 0;
+            amax = nxo_ipc_max_step(w, xn.data(), dx.data(), p->eta, &np2);
+            fx = problem_value(w, xn) + sc * eb;
+            for (int i = 0; i < n; ++i) prod[i] = g[i] * dx[i];
+            const double descent = tree_sum(prod);
+            if (descent > 0) { lsfail = 1; break; }
+            double alpha = std::min(1.0, amax);
+            bool done = false;
+            for (int ls = 0; ls < p->ls_max_iters; ++ls) {
+                for (int i = 0; i < n; ++i) xt[i] = xn[i] + alpha * dx[i];
+                const double ert = problem_value(w, xt);
+                double ebt = 0.0;
+                ipc_barrier_cpu(w, xt.data(), p->dhat, p->kappa, &ebt, nullptr, nullptr, nullptr, nullptr, nullptr, fr);
+                if (fr) ebt = ebt + ipc_fric_energy(fr);
+                const double fn = ert + sc * ebt;
+                if (fn <= fx + s.ls_c1 * alpha * descent) { done = true; fx = fn; break; }
+                alpha *= s.ls_rho;
+            }
+            if (!done) { lsfail = 1; break; }
+            xn = xt;
+            if (it == p->newton_max_iters - 1) iters = p->newton_max_iters;
         }
-        if (!done) { lsfail = 1; break; }
-        xn = xt;
-        if (it == p->newton_max_iters - 1) iters = p->newton_max_iters;
+        iters_done += iters;
+        if (!conv) break;   // a pass that did not converge ends the step
     }
+    iters = iters_done;
+    if (fr) ipc_fric_free(fr);
     std::vector<double> vn(n), an(n);
     if (newmark) {
         const double den = (s.newmark_beta * dt) * dt;
@@ -2516,7 +2540,7 @@ int nxo_ipc_step(nxo_world* w, double dt, const nxd_ipc_params* p, nxd_ipc_stats
     if (out) {
         out->newton_iterations = iters; out->converged = conv; out->line_search_failed = lsfail;
         out->solve_failed = solvefail; out->last_alpha_max = amax; out->energy = fx; out->n_pairs = npairs;
-        out->n_active = na; out->pcg_iterations = 0;
+        out->n_active = na; out->pcg_iterations = 0; out->n_friction = nfric;
     }
     return solvefail ? NXD_FACTOR_FAILED : NXD_OK;
 }

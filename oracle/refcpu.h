@@ -105,6 +105,8 @@ int nxo_ipc_candidates(nxo_world* w, const double* x, const double* dx, double i
 int nxo_ipc_barrier(nxo_world* w, const double* x, double dhat, double kappa, double* energy, double* grad, double* H,
                     int64_t* n_pairs, int64_t* n_active);
 double nxo_ipc_max_step(nxo_world* w, const double* x, const double* dx, double eta, int64_t* n_pairs);
+int nxo_ipc_friction(nxo_world* w, const double* x_lag, const double* x, double dhat, double kappa, double mu, double eps,
+                     double* energy, double* grad, double* H, int64_t* n_friction);
 int nxo_ipc_pair(int32_t kind, const double* X12, double dhat, double kappa, double* d2, int32_t* type, double* e,
                  double* g12, double* H_sub, double* H_raw, double* H_full);
 double nxo_ipc_accd(int32_t kind, const double* X12, const double* D12, double t_max, double eta, int32_t max_iter,

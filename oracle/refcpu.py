@@ -79,6 +79,7 @@ def lib():
     L.nxo_ipc_barrier.argtypes = [vp, dp, C.c_double, C.c_double, dp, dp, dp, i64p, i64p]
     L.nxo_ipc_max_step.restype = C.c_double
     L.nxo_ipc_max_step.argtypes = [vp, dp, dp, C.c_double, i64p]
+    L.nxo_ipc_friction.argtypes = [vp, dp, dp, C.c_double, C.c_double, C.c_double, C.c_double, dp, dp, dp, i64p]
     L.nxo_ipc_pair.argtypes = [C.c_int32, dp, C.c_double, C.c_double, dp, ip, dp, dp, dp, dp, dp]
     L.nxo_ipc_accd.restype = C.c_double
     L.nxo_ipc_accd.argtypes = [C.c_int32, dp, dp, C.c_double, C.c_double, C.c_int32, ip]
@@ -279,6 +280,18 @@ class OracleWorld:
         n = C.c_int64()
         a = lib().nxo_ipc_max_step(self.h, _d(x), _d(dx), eta, C.byref(n))
         return a, n.value
+
+    def ipc_friction(self, x_lag, x, dhat: float, kappa: float, mu: float, eps: float, hessian: bool = True):
+        """Lagged friction alone (nxo_ipc_friction): the pairs active at
+        x_lag frozen there, displacements measured from x_lag; (energy,
+        gradient[6N], Gauss-Newton Hessian[6N, 6N] or None, frozen pairs) at x."""
+        n6 = 6 * self.scene.n_bodies
+        g = np.zeros(n6)
+        H = np.zeros((n6, n6)) if hessian else None
+        e, nf = C.c_double(), C.c_int64()
+        lib().nxo_ipc_friction(self.h, _d(x_lag), _d(x), dhat, kappa, mu, eps, C.byref(e), abi.dptr(g),
+                               abi.dptr(H) if hessian else None, C.byref(nf))
+        return e.value, g, H, nf.value
 
 
 def ipc_pair(kind: int, X, dhat: float, kappa: float) -> dict:

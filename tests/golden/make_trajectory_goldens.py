@@ -11,7 +11,9 @@ literal loop's) on all host threads:
 * ``traj_batched.npz``       -- the 256 uneven scenes, 100 steps each;
 * ``traj_ipc_sphere_bowl.npz`` -- the same 64-sphere bowl stepped by the
   full-IPC step (primitive-pair barrier, additive-CCD line search; the
-  oracle's nxo_ipc_step with scenes.ipc_step_settings()), its first 40 steps.
+  oracle's nxo_ipc_step with scenes.ipc_step_settings()), its first 40 steps;
+* ``traj_ipc_sphere_bowl_friction.npz`` -- the same with the configuration's
+  mu 0.3 as lagged friction (scenes.ipc_step_settings(mu=0.3)), 20 steps.
 
 Stored per fixture: positions and orientations at the checkpoint steps, and
 for every step the adaptive stiffness kappa, the contact count, the ALM and
@@ -24,7 +26,7 @@ The full-IPC fixture stores, for every step, the Newton iteration count, the
 convergence and line-search flags, the active and candidate pair counts and
 the full body state (positions, orientations).
 
-Usage: python tests/golden/make_trajectory_goldens.py [hopper|bowl|batched|ipc_bowl ...]
+Usage: python tests/golden/make_trajectory_goldens.py [hopper|bowl|batched|ipc_bowl|ipc_bowl_friction ...]
 (about 8 minutes for the hopper on 8 threads, a few minutes for the others).
 """
 from __future__ import annotations
@@ -122,14 +124,14 @@ def make_batched(path):
                         state_50=s50, state_100=s100)
 
 
-IPC_STAT_KEYS = ("newton_iterations", "converged", "line_search_failed", "n_active", "n_pairs")
+IPC_STAT_KEYS = ("newton_iterations", "converged", "line_search_failed", "n_active", "n_pairs", "n_friction")
 
 
-def run_ipc(sc, steps):
+def run_ipc(sc, steps, mu=0.0):
     from nexdynipc_b200 import abi
     from oracle import refcpu
     ow = refcpu.OracleWorld(sc)
-    p = abi.ipc_params(**scenes.ipc_step_settings())
+    p = abi.ipc_params(**scenes.ipc_step_settings(mu=mu))
     out = {k: np.zeros(steps, np.int64) for k in IPC_STAT_KEYS}
     pos, quat = [], []
     t0 = time.time()
@@ -164,6 +166,11 @@ def main(which):
         out = run_ipc(scenes.sphere_bowl(), 40)
         np.savez_compressed(os.path.join(HERE, "traj_ipc_sphere_bowl.npz"), **out)
         print(f"ipc_bowl: {time.time() - t:.0f} s")
+    if "ipc_bowl_friction" in which:
+        t = time.time()
+        out = run_ipc(scenes.sphere_bowl(), 20, mu=0.3)
+        np.savez_compressed(os.path.join(HERE, "traj_ipc_sphere_bowl_friction.npz"), **out)
+        print(f"ipc_bowl_friction: {time.time() - t:.0f} s")
     if "batched" in which:
         t = time.time()
         make_batched(os.path.join(HERE, "traj_batched.npz"))
