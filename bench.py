@@ -176,7 +176,7 @@ def oracle_steps(scene_fn, threads: int, skip: int, steps: int, literal: bool):
     return walls, ff
 
 
-def batched_leg(torch, steps: int, warmup: int, flush, ws: int = 1, rank: int = 0):
+def batched_leg(torch, steps: int, warmup: int, flush, ws: int = 1, rank: int = 0, plain: bool = True):
     """256 independent scenes of 2-63 bodies (the batched configuration, seed
     4000): aggregate scene-steps/s of the batched form (one graph of batched
     launches per step) next to the plain path (the same scenes, one context
@@ -190,9 +190,18 @@ def batched_leg(torch, steps: int, warmup: int, flush, ws: int = 1, rank: int = 
     idx, scs = shard.my_scenes(all_scs, rank, ws)
     stream = torch.cuda.Stream()
     lib = runtime.lib()
+    # the queue grids of the narrow phase, tuned on a throwaway batch of the
+    # same scenes (the tuning steps it), then applied to the timed one
+    import tempfile
+    tb = runtime.Batch(scs)
+    with tempfile.TemporaryDirectory() as td:
+        tune = tb.autotune(cache_path=os.path.join(td, "autotune.json"), steps=2)
+    tb.close()
     b = runtime.Batch(scs)
+    for kname, v in tune["choice"].items():
+        b.set_queue_ctas(runtime.QUEUE_KERNELS[kname], v)
     b.set_stream(stream.cuda_stream)
-    singles = [runtime.Context(s) for s in scs]
+    singles = [runtime.Context(s) for s in scs] if plain else []
     for c in singles:
         lib.nxd_set_stream(c.h, C.c_void_p(stream.cuda_stream))
 
@@ -220,14 +229,16 @@ def batched_leg(torch, steps: int, warmup: int, flush, ws: int = 1, rank: int = 
     if ws > 1:
         torch.distributed.barrier()
     t_batched = max_over_ranks(timed(b.step))
-    t_plain = max_over_ranks(timed(plain_step))
+    t_plain = max_over_ranks(timed(plain_step)) if plain else None
     status = max(b.diagnostics(i)["status"] for i in range(len(scs)))
-    same = all(np.array_equal(b.state(i)["position"], singles[i].state()["position"]) for i in range(0, len(scs), 17))
+    same = plain and all(np.array_equal(b.state(i)["position"], singles[i].state()["position"])
+                         for i in range(0, len(scs), 17))
     n = len(all_scs)
     out = {"scenes": n, "bodies": int(sum(s.n_bodies for s in all_scs)), "steps": steps,
-           "value": n * steps / t_batched, "plain_value": n * steps / t_plain, "unit": "scene-steps/s",
-           "batched_over_plain": t_plain / t_batched, "groups": b.groups(), "status": int(status),
+           "value": n * steps / t_batched, "plain_value": n * steps / t_plain if plain else None, "unit": "scene-steps/s",
+           "batched_over_plain": t_plain / t_batched if plain else None, "groups": b.groups(), "status": int(status),
            "equal_to_plain_sample": bool(same), "ranks": ws, "scenes_this_rank": len(scs),
+           "queue_ctas_per_sm": tune["choice"], "autotune_ms": {k: round(v, 3) for k, v in tune["timings_ms"].items()},
            "sharding": "greedy by estimated cost, no exchange while stepping" if ws > 1 else "one rank"}
     for c in singles:
         c.close()
@@ -577,6 +588,8 @@ def main():
     ap.add_argument("--no-diff", action="store_true")
     ap.add_argument("--no-pcg", action="store_true")
     ap.add_argument("--adjoint-sets", type=int, default=2, help="parameter sets of the adjoint leg")
+    ap.add_argument("--batched-only", type=int, metavar="STEPS",
+                    help="only the batched form of the 256 scenes (1 warm-up step), one JSON line")
     ap.add_argument("--ipc-step-only", type=int, nargs=4, metavar=("CUBES", "COLUMNS", "SETTLE", "STEPS"),
                     help="run only the full-IPC step leg on that drop and print its JSON (for profiling)")
     args = ap.parse_args()
@@ -584,6 +597,11 @@ def main():
     if args.ipc_step_only:
         n_cubes, columns, settle, steps = args.ipc_step_only
         print(json.dumps(ipc_step_leg(n_cubes=n_cubes, columns=columns, settle=settle, steps=steps)), flush=True)
+        return
+    if args.batched_only:
+        import torch
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        print(json.dumps(batched_leg(torch, args.batched_only, 1, flush, plain=False)), flush=True)
         return
     if args.impl == "reference":
         run_reference(args, ws, rank)
@@ -803,7 +821,14 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "replicas": ws, "l2": "flushed between steps (256 MiB write, untimed)",
+        "config": {"workload": WORKLOAD,
+                   "batched_scene_steps_per_s": None if batched is None else batched["value"],
+                   "batched_over_plain": None if batched is None else batched["batched_over_plain"],
+                   "batched_groups": None if batched is None else batched["groups"],
+                   "adjoint_fwd_plus_adj_over_fwd": None if adj is None else adj["fwd_plus_adj_over_fwd"],
+                   "full_run_steps_per_s": full["steps_per_s"],
+                   "mode_i_bowl_steps_per_s": None if mode_i is None else mode_i["step_bowl"]["steps_per_s"],
+                   "replicas": ws, "l2": "flushed between steps (256 MiB write, untimed)",
                    "timing": ("value: K steps, each the step's CUDA graph, CUDA events per step; per_family_ms and "
                               "roofline: the same K step indices on a twin context of the same scene with CUDA "
                               "events around every launch; e2e: the same K step indices on a third context "
@@ -812,12 +837,8 @@ def main():
                    "twin_state_equal": twin_equal,
                    "e2e_state_equal": e2e_equal,
                    "fp64_peak_tflops": fp64_tflops,
-                   "full_run_steps_per_s": full["steps_per_s"],
                    "full_run_steps": full["steps"],
                    "full_run_ms_max_step": full["ms_max_step"],
-                   "batched_scene_steps_per_s": None if batched is None else batched["value"],
-                   "batched_over_plain": None if batched is None else batched["batched_over_plain"],
-                   "batched_groups": None if batched is None else batched["groups"],
                    "full_run": full,
                    "per_family_ms": per_family, "last_step": {k: diag[k] for k in
                                                               ("n_body_pairs", "n_contacts", "alm_iterations",
@@ -825,7 +846,6 @@ def main():
                    "batched": batched,
                    "diff": diffl,
                    "adjoint": adj,
-                   "adjoint_fwd_plus_adj_over_fwd": None if adj is None else adj["fwd_plus_adj_over_fwd"],
                    "pcg": pcg,
                    "mode_i": mode_i},
         "roofline": roof,

@@ -381,7 +381,14 @@ nxd_status nxd_profile(nxd_ctx* ctx, int32_t enable, double* ms, int64_t* launch
  * nxd_batch_step returns without synchronising; get_state synchronises.
  * nxd_batch_groups reports the number of groups; nxd_batch_set_stream makes
  * the batch issue its work on a caller's cudaStream_t (after synchronising
- * the previous one).  Neither has a reference counterpart. */
+ * the previous one).  Neither has a reference counterpart.
+ * The narrow-phase kernels (whose work per scene, the body-pair count, is
+ * known only on the device) run in a queue form: a persistent grid of
+ * ctas_per_sm CTAs per SM pulls (scene, chunk of body pairs) items from a
+ * device counter.  nxd_batch_set_queue_ctas sets that grid for one kernel
+ * (NXD_QUEUE_NARROW_ROWS / NXD_QUEUE_NARROW_EMIT; 1..64, default 4); the
+ * results do not depend on it, only the time; the groups are rebuilt at the
+ * next step. */
 typedef struct nxd_batch nxd_batch;
 nxd_status nxd_batch_create(const nxd_scene_desc* descs, int32_t n_scenes, nxd_batch** out);
 void nxd_batch_destroy(nxd_batch* b);
@@ -390,6 +397,13 @@ nxd_status nxd_batch_get_state(nxd_batch* b, int32_t scene, const nxd_state* out
 nxd_status nxd_batch_get_diagnostics(nxd_batch* b, int32_t scene, nxd_diagnostics* out);
 int32_t nxd_batch_groups(nxd_batch* b);
 nxd_status nxd_batch_set_stream(nxd_batch* b, void* stream);
+enum { NXD_QUEUE_NARROW_ROWS = 0, NXD_QUEUE_NARROW_EMIT = 1 };
+nxd_status nxd_batch_set_queue_ctas(nxd_batch* b, int32_t kernel, int32_t ctas_per_sm);
+/* n_steps nxd_batch_step calls timed on the batch's stream by CUDA events
+ * (synchronises); used by the autotuner of the queue grids. */
+nxd_status nxd_batch_timed_steps(nxd_batch* b, const double* dts, int32_t n_steps, double* ms);
+/* The current device's SM count and name (the autotuner's cache key). */
+nxd_status nxd_device_info(int32_t* sm_count, char* name, int32_t name_len);
 
 /* Primitive-level contact model (full IPC).  No counterpart in the
  * reference, which only has the body-COM barrier (its design notes plan

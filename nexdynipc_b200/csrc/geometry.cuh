@@ -571,7 +571,10 @@ __device__ __forceinline__ V3 ld_col(const double (&a)[3][kTopK], int c) { retur
 __device__ __forceinline__ void st_col(double (&a)[3][kTopK], int c, V3 v) { a[0][c] = v.x; a[1][c] = v.y; a[2][c] = v.z; }
 
 // Pass 1.  mode 0: FV and EE hit masks and counts; mode 1: the VV fallback.
-__device__ __forceinline__ void narrow_rows_body(const NarrowIn& in, int mode, const NarrowScratch& s, const int* skip_if) {
+// Block vb of a grid of vg blocks (blockIdx.x / gridDim.x of a plain launch;
+// a work item's chunk of the world's pairs in the batched queue form).
+__device__ __forceinline__ void narrow_rows_body(const NarrowIn& in, int mode, const NarrowScratch& s, const int* skip_if,
+                                                 int vb, int vg) {
     if (skip_if && *skip_if != 0) return;
     __shared__ WarpStage stage[kRowsWarps];
     const unsigned full = 0xffffffffu;
@@ -579,8 +582,8 @@ __device__ __forceinline__ void narrow_rows_body(const NarrowIn& in, int mode, c
     WarpStage& W = stage[threadIdx.x >> 5];
     const int np = min(*in.npairs_ptr, in.cap);
     const double dh = *in.dhat_ptr;
-    const int nwarps = gridDim.x * kRowsWarps;
-    for (int p = blockIdx.x * kRowsWarps + (threadIdx.x >> 5); p < np; p += nwarps) {
+    const int nwarps = vg * kRowsWarps;
+    for (int p = vb * kRowsWarps + (threadIdx.x >> 5); p < np; p += nwarps) {
         const int A = in.pairs[2 * p], B = in.pairs[2 * p + 1];
         if (in.n_allowed > 0 && allowed_index(in.allowed, in.n_allowed, A, B) < 0) {
             // detectContacts drops every contact of a pair that is not allowed
@@ -674,7 +677,12 @@ __device__ __forceinline__ void narrow_rows_body(const NarrowIn& in, int mode, c
     }
 }
 constexpr int kLB_narrow_rows = 32 * kRowsWarps;
-__global__ void __launch_bounds__(32 * kRowsWarps) k_narrow_rows(const __grid_constant__ NarrowIn in, int mode, const __grid_constant__ NarrowScratch s, const int* skip_if) { narrow_rows_body(in, mode, s, skip_if); }
+__global__ void __launch_bounds__(32 * kRowsWarps) k_narrow_rows(const __grid_constant__ NarrowIn in, int mode, const __grid_constant__ NarrowScratch s, const int* skip_if) { narrow_rows_body(in, mode, s, skip_if, blockIdx.x, gridDim.x); }
+// work items of one world in the queue form: chunks of kRowsWarps pairs
+__device__ __forceinline__ int narrow_rows_items(const NarrowIn& in, int, const NarrowScratch&, const int* skip_if) {
+    if (skip_if && *skip_if != 0) return 0;
+    return (min(*in.npairs_ptr, in.cap) + kRowsWarps - 1) / kRowsWarps;
+}
 
 // Exclusive scan of n ints by one block; returns the total (all threads).
 // Prefixes of the hit counts: nseg halves of cap entries each (FV, EE), the
@@ -722,11 +730,12 @@ __device__ __forceinline__ void emit_grid(const NarrowIn& in, int kind, int p, c
     pos += total;
 }
 
-__device__ __forceinline__ void narrow_emit_body(const NarrowIn& in, int mode, const NarrowScratch& s, const int* ee_base, ContactRec* out, const int* skip_if) {
+__device__ __forceinline__ void narrow_emit_body(const NarrowIn& in, int mode, const NarrowScratch& s, const int* ee_base, ContactRec* out, const int* skip_if,
+                                                 int vb, int vg) {
     if (skip_if && *skip_if != 0) return;
     const int np = min(*in.npairs_ptr, in.cap);
-    const int nwarps = gridDim.x * kEmitWarps;
-    for (int p = blockIdx.x * kEmitWarps + (threadIdx.x >> 5); p < np; p += nwarps) {
+    const int nwarps = vg * kEmitWarps;
+    for (int p = vb * kEmitWarps + (threadIdx.x >> 5); p < np; p += nwarps) {
         const int* n = in.topn + 6 * p;
         const unsigned* M = s.mask + (size_t)p * kMaskWords;
         if (mode == 1) {
@@ -749,7 +758,12 @@ __device__ __forceinline__ void narrow_emit_body(const NarrowIn& in, int mode, c
     }
 }
 constexpr int kLB_narrow_emit = 32 * kEmitWarps;
-__global__ void __launch_bounds__(32 * kEmitWarps) k_narrow_emit(const __grid_constant__ NarrowIn in, int mode, const __grid_constant__ NarrowScratch s, const int* ee_base, ContactRec* out, const int* skip_if) { narrow_emit_body(in, mode, s, ee_base, out, skip_if); }
+__global__ void __launch_bounds__(32 * kEmitWarps) k_narrow_emit(const __grid_constant__ NarrowIn in, int mode, const __grid_constant__ NarrowScratch s, const int* ee_base, ContactRec* out, const int* skip_if) { narrow_emit_body(in, mode, s, ee_base, out, skip_if, blockIdx.x, gridDim.x); }
+__device__ __forceinline__ int narrow_emit_items(const NarrowIn& in, int, const NarrowScratch&, const int*, ContactRec*,
+                                                 const int* skip_if) {
+    if (skip_if && *skip_if != 0) return 0;
+    return (min(*in.npairs_ptr, in.cap) + kEmitWarps - 1) / kEmitWarps;
+}
 
 // ---------------------------------------------------------------------------
 // Scene minimum distance, pruned (computeSceneMinDistance,

@@ -167,6 +167,22 @@ struct ProfScope {
         }                                                                                               \
     } while (0)
 
+// A launch of a narrow-phase kernel k_<name> (body <name>_body with a
+// trailing block index and count, item counter <name>_items): plain, or
+// recorded in the queue form for a batched replay (queue kind qk).
+#define NXD_KQ(ctx, fam, qk, name, grid, block, smem, ...)                                                      \
+    do {                                                                                                      \
+        if ((ctx)->rec) {                                                                                     \
+            record_queue_into<&name##_body, &name##_items, kLB_##name>(*(ctx)->rec, fam, qk, &name##_items,   \
+                                                                       dim3(grid), dim3(block), (size_t)(smem), \
+                                                                       __VA_ARGS__);                          \
+        } else {                                                                                              \
+            ProfScope ps_(ctx, fam);                                                                          \
+            k_##name<<<grid, block, smem, (ctx)->stream>>>(__VA_ARGS__);                                      \
+        }                                                                                                     \
+    } while (0)
+enum { kQueueNarrowRows = 0, kQueueNarrowEmit = 1, kQueueKinds = 2 };
+
 void configure_newton_launch(nxd_ctx* c);
 
 void fill_solver(nxd_ctx* c) {
@@ -354,16 +370,17 @@ void launch_narrow_full(nxd_ctx* c, const double* wv, const double* pose_p, cons
     const int emit_blocks = pair_grid(c, 1, 1, kEmitWarps, c->n_sm * 2);
     int* skip_vv = c->i_scratch;
     const int* np = &c->sc->n_pairs;
-    NXD_K(c, NXD_PROF_NARROW, narrow_rows, (rows_blocks), (32 * kRowsWarps), (0), in, 0, ns, skip_if);
+    NXD_KQ(c, NXD_PROF_NARROW, kQueueNarrowRows, narrow_rows, (rows_blocks), (32 * kRowsWarps), (0), in, 0, ns, skip_if);
     NXD_K(c, NXD_PROF_SCAN, hit_scan, (1), (1024), (0), c->hit_cnt, c->hit_off, c->pair_cap, np, 2, &c->sc->fv_hits,
                                                                       &c->sc->ee_hits, skip_if);
-    NXD_K(c, NXD_PROF_NARROW, narrow_emit, (emit_blocks), (32 * kEmitWarps), (0), in, 0, ns, &c->sc->fv_hits, c->contacts,
-                                                                                                skip_if);
+    NXD_KQ(c, NXD_PROF_NARROW, kQueueNarrowEmit, narrow_emit, (emit_blocks), (32 * kEmitWarps), (0), in, 0, ns,
+           &c->sc->fv_hits, c->contacts, skip_if);
     NXD_K(c, NXD_PROF_OTHER, contact_totals, (1), (1), (0), c->sc, 0, skip_if, skip_vv);
-    NXD_K(c, NXD_PROF_NARROW, narrow_rows, (rows_blocks), (32 * kRowsWarps), (0), in, 1, ns, skip_vv);
+    NXD_KQ(c, NXD_PROF_NARROW, kQueueNarrowRows, narrow_rows, (rows_blocks), (32 * kRowsWarps), (0), in, 1, ns, skip_vv);
     NXD_K(c, NXD_PROF_SCAN, hit_scan, (1), (1024), (0), c->hit_cnt, c->hit_off, c->pair_cap, np, 1, &c->sc->vv_hits,
                                                                       nullptr, skip_vv);
-    NXD_K(c, NXD_PROF_NARROW, narrow_emit, (emit_blocks), (32 * kEmitWarps), (0), in, 1, ns, nullptr, c->contacts, skip_vv);
+    NXD_KQ(c, NXD_PROF_NARROW, kQueueNarrowEmit, narrow_emit, (emit_blocks), (32 * kEmitWarps), (0), in, 1, ns, nullptr,
+           c->contacts, skip_vv);
     NXD_K(c, NXD_PROF_OTHER, contact_totals, (1), (1), (0), c->sc, 1, skip_if, nullptr);
     NXD_K(c, NXD_PROF_OTHER, sort_contacts, (1), (1024), (sort_smem_bytes(32)), c->sc, c->contacts, c->contacts_tmp, c->sort_key,
           c->sort_idx, c->sort_g, c->sort_l, c->sort_small, skip_if);
@@ -2172,10 +2189,11 @@ namespace {
 
 struct BatchGroup {
     std::vector<int> scenes;
-    std::vector<const void*> kern;
+    std::vector<const void*> kern, prep;
     std::vector<dim3> grid, block;
     std::vector<size_t> smem, table_off;
     void* table = nullptr;
+    int* queue = nullptr;     // per queue-form position: prefix (scenes + 1) and counter
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -2188,6 +2206,9 @@ struct nxd_batch {
     std::vector<double> dts;           // the dts the groups were recorded with
     std::vector<BatchGroup> groups;
     bool own_stream = true;
+    // persistent grid of each queue-form kernel: CTAs per SM (the result
+    // does not depend on it; nxd_batch_set_queue_ctas, the autotuner)
+    int queue_per_sm[kQueueKinds] = {4, 4};
 };
 
 namespace {
@@ -2197,6 +2218,7 @@ void release_groups(nxd_batch* b) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
         if (g.graph) cudaGraphDestroy(g.graph);
         if (g.table) cudaFree(g.table);
+        if (g.queue) cudaFree(g.queue);
     }
     b->groups.clear();
 }
@@ -2217,7 +2239,9 @@ nxd_status build_groups(nxd_batch* b, const double* dts) {
         if (recs[i].size() != recs[j].size()) return false;
         for (size_t k = 0; k < recs[i].size(); ++k) {
             const LaunchRec &x = recs[i][k], &y = recs[j][k];
-            if (x.kern != y.kern || x.block.x != y.block.x || x.block.y != y.block.y || x.block.z != y.block.z) return false;
+            if (x.kern != y.kern || x.prep != y.prep || x.block.x != y.block.x || x.block.y != y.block.y ||
+                x.block.z != y.block.z)
+                return false;
         }
         return true;
     };
@@ -2236,17 +2260,29 @@ nxd_status build_groups(nxd_batch* b, const double* dts) {
             bytes += (r0[k].args.size() * ns + 255) / 256 * 256;
         }
         std::vector<unsigned char> host(std::max<size_t>(bytes, 1));
+        int nq = 0;
+        const int n_sm = b->ctx[0]->n_sm;
         for (size_t k = 0; k < L; ++k) {
             unsigned gx = 1;
             size_t smem = 0;
+            long long gsum = 0;
             for (size_t q = 0; q < ns; ++q) {
                 const LaunchRec& r = recs[g.scenes[q]][k];
                 gx = std::max(gx, r.grid.x);
+                gsum += r.grid.x;
                 smem = std::max(smem, r.smem);
                 std::memcpy(host.data() + g.table_off[k] + q * r.args.size(), r.args.data(), r.args.size());
             }
             g.kern.push_back(r0[k].kern);
-            g.grid.push_back(dim3(gx, (unsigned)ns, 1));
+            g.prep.push_back(r0[k].prep);
+            if (r0[k].prep) {
+                // queue form: a persistent grid over all scenes' items
+                const long long ctas = std::min<long long>(gsum, (long long)b->queue_per_sm[r0[k].queue_kind] * n_sm);
+                g.grid.push_back(dim3((unsigned)std::max<long long>(ctas, 1), 1, 1));
+                ++nq;
+            } else {
+                g.grid.push_back(dim3(gx, (unsigned)ns, 1));
+            }
             g.block.push_back(r0[k].block);
             g.smem.push_back(smem);
             if (smem > 48 * 1024)
@@ -2254,9 +2290,21 @@ nxd_status build_groups(nxd_batch* b, const double* dts) {
         }
         NXD_CUDA(cudaMalloc(&g.table, host.size()));
         NXD_CUDA(cudaMemcpy(g.table, host.data(), host.size(), cudaMemcpyHostToDevice));
+        const size_t qstride = ns + 2;   // prefix[ns + 1], counter
+        if (nq) NXD_CUDA(cudaMalloc(&g.queue, sizeof(int) * qstride * nq));
         NXD_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        int qi = 0;
         for (size_t k = 0; k < L; ++k) {
             void* tab = (unsigned char*)g.table + g.table_off[k];
+            if (g.prep[k]) {
+                int nw = (int)ns;
+                int* prefix = g.queue + qstride * qi++;
+                int* counter = prefix + ns + 1;
+                void* pargs[] = {&tab, &nw, &prefix, &counter};
+                cudaLaunchKernel(g.prep[k], dim3(1), dim3(kQueuePrepThreads), pargs, 0, b->stream);
+                cudaLaunchKernel(g.kern[k], g.grid[k], g.block[k], pargs, g.smem[k], b->stream);
+                continue;
+            }
             void* args[] = {&tab};
             cudaLaunchKernel(g.kern[k], g.grid[k], g.block[k], args, g.smem[k], b->stream);
         }
@@ -2290,6 +2338,48 @@ nxd_status nxd_batch_create(const nxd_scene_desc* descs, int32_t n, nxd_batch** 
         b->ctx.push_back(c);
     }
     *out = b;
+    return NXD_OK;
+}
+
+nxd_status nxd_batch_timed_steps(nxd_batch* b, const double* dts, int32_t n_steps, double* ms) {
+    if (!b || !dts || n_steps < 1 || !ms) return NXD_INVALID_ARGUMENT;
+    cudaEvent_t e0, e1;
+    NXD_CUDA(cudaEventCreate(&e0));
+    NXD_CUDA(cudaEventCreate(&e1));
+    NXD_CUDA(cudaEventRecord(e0, b->stream));
+    nxd_status st = NXD_OK;
+    for (int k = 0; k < n_steps && st == NXD_OK; ++k) st = nxd_batch_step(b, dts);
+    NXD_CUDA(cudaEventRecord(e1, b->stream));
+    NXD_CUDA(cudaEventSynchronize(e1));
+    float f = 0.0f;
+    cudaEventElapsedTime(&f, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = f;
+    return st;
+}
+
+nxd_status nxd_device_info(int32_t* sm_count, char* name, int32_t name_len) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return NXD_NO_DEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return NXD_CUDA_ERROR;
+    if (sm_count) *sm_count = prop.multiProcessorCount;
+    if (name && name_len > 0) {
+        std::strncpy(name, prop.name, (size_t)name_len - 1);
+        name[name_len - 1] = 0;
+    }
+    return NXD_OK;
+}
+
+nxd_status nxd_batch_set_queue_ctas(nxd_batch* b, int32_t kernel, int32_t ctas_per_sm) {
+    if (!b || kernel < 0 || kernel >= kQueueKinds || ctas_per_sm < 1 || ctas_per_sm > 64) return NXD_INVALID_ARGUMENT;
+    if (b->queue_per_sm[kernel] != ctas_per_sm) {
+        NXD_CUDA(cudaStreamSynchronize(b->stream));
+        b->queue_per_sm[kernel] = ctas_per_sm;
+        release_groups(b);   // rebuilt at the next step
+        b->dts.clear();
+    }
     return NXD_OK;
 }
 

@@ -74,6 +74,12 @@ def lib():
     L.nxd_batch_groups.restype = C.c_int32
     L.nxd_batch_set_stream.argtypes = [vp, vp]
     L.nxd_batch_set_stream.restype = C.c_int
+    L.nxd_batch_set_queue_ctas.argtypes = [vp, C.c_int32, C.c_int32]
+    L.nxd_batch_set_queue_ctas.restype = C.c_int
+    L.nxd_batch_timed_steps.argtypes = [vp, dp, C.c_int32, dp]
+    L.nxd_batch_timed_steps.restype = C.c_int
+    L.nxd_device_info.argtypes = [C.POINTER(C.c_int32), C.c_char_p, C.c_int32]
+    L.nxd_device_info.restype = C.c_int
     L.nxd_body_pairs_noalloc.argtypes = [vp, vp, vp, C.c_int32, C.c_double, vp, C.c_int64, i64p, vp]
     L.nxd_body_pairs_noalloc.restype = C.c_int
     L.nxd_ipc_adjoint.argtypes = [vp, C.c_double, C.POINTER(abi.NxdIpcParams), C.POINTER(abi.NxdState), dp, dp,
@@ -390,6 +396,18 @@ class Context:
         return a.value, n.value
 
 
+QUEUE_KERNELS = {"narrow_rows": 0, "narrow_emit": 1}     # NXD_QUEUE_NARROW_ROWS / _EMIT
+AUTOTUNE_CTAS = (1, 2, 4, 8, 16)
+
+
+def device_info():
+    """(SM count, device name) of the current device (nxd_device_info)."""
+    sm = C.c_int32()
+    buf = C.create_string_buffer(256)
+    _check("nxd_device_info", lib().nxd_device_info(C.byref(sm), buf, 256))
+    return sm.value, buf.value.decode()
+
+
 class Batch:
     """Independent scenes stepped together (nxd_batch_*)."""
 
@@ -425,6 +443,66 @@ class Batch:
     def groups(self) -> int:
         """Number of launch groups (scenes with identical step sequences)."""
         return int(lib().nxd_batch_groups(self.h))
+
+    def set_queue_ctas(self, kernel: int, ctas_per_sm: int):
+        """Persistent grid (CTAs per SM) of a queue-form narrow-phase kernel
+        (QUEUE_NARROW_ROWS / QUEUE_NARROW_EMIT); results do not depend on it."""
+        _check("nxd_batch_set_queue_ctas", lib().nxd_batch_set_queue_ctas(self.h, int(kernel), int(ctas_per_sm)))
+
+    def timed_steps(self, n: int) -> float:
+        """n steps timed by CUDA events on the batch's stream; milliseconds."""
+        ms = C.c_double()
+        _check("nxd_batch_timed_steps", lib().nxd_batch_timed_steps(self.h, abi.dptr(self.dts), int(n), C.byref(ms)))
+        return ms.value
+
+    def size_bucket(self) -> str:
+        """The autotuner's scene-size bucket: scene count and largest body and
+        vertex counts, each rounded up to a power of two."""
+        p2 = lambda v: 1 << max(0, int(v) - 1).bit_length()
+        return (f"scenes{p2(len(self.scenes))}_bodies{p2(max(s.n_bodies for s in self.scenes))}"
+                f"_verts{p2(max(s.n_vertices for s in self.scenes))}")
+
+    def autotune(self, cache_path: str | None = None, steps: int = 2, candidates=AUTOTUNE_CTAS) -> dict:
+        """Picks each queue-form kernel's persistent grid (CTAs per SM) by
+        measurement and caches it in a JSON file keyed by device and size
+        bucket.  A cached entry is applied without timing.  Otherwise a
+        coordinate search: for each kernel in turn, each candidate is set,
+        stepped once untimed (the graphs are rebuilt) and then `steps` times
+        under CUDA events, and the fastest is kept.  The scenes advance while
+        tuning; their results do not depend on the grids.  Returns
+        {"key", "choice", "cached", "timings_ms"}."""
+        import json
+        sm, name = device_info()
+        key = f"{name}|sm{sm}|{self.size_bucket()}"
+        cache = {}
+        if cache_path and os.path.exists(cache_path):
+            with open(cache_path) as f:
+                cache = json.load(f)
+        if key in cache:
+            choice = {k: int(v) for k, v in cache[key].items()}
+            for kname, v in choice.items():
+                self.set_queue_ctas(QUEUE_KERNELS[kname], v)
+            return {"key": key, "choice": choice, "cached": True, "timings_ms": {}}
+        choice = {k: 4 for k in QUEUE_KERNELS}
+        timings = {}
+        for kname, kid in QUEUE_KERNELS.items():
+            best = None
+            for cand in candidates:
+                self.set_queue_ctas(kid, cand)
+                self.step()
+                ms = self.timed_steps(steps)
+                timings[f"{kname}={cand}"] = ms
+                if best is None or ms < best[1]:
+                    best = (cand, ms)
+            choice[kname] = best[0]
+            self.set_queue_ctas(kid, best[0])
+        if cache_path:
+            cache[key] = choice
+            tmp = cache_path + ".tmp"
+            with open(tmp, "w") as f:
+                json.dump(cache, f, indent=1, sort_keys=True)
+            os.replace(tmp, cache_path)
+        return {"key": key, "choice": choice, "cached": False, "timings_ms": timings}
 
     def state(self, i: int) -> dict:
         sb = abi.StateBuffers(self.scenes[i].n_bodies)

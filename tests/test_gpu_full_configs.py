@@ -8,7 +8,8 @@ same scene stored in tests/golden/traj_*.npz (make_trajectory_goldens.py):
 * 64 icospheres (642 V) falling into the bowl, 200 steps;
 * the 256 uneven batched scenes, 100 steps, as one batch;
 * the 64-sphere bowl stepped by the full-IPC step (nxd_ipc_step), 40 steps
-  against the oracle's nxo_ipc_step (traj_ipc_sphere_bowl.npz).
+  against the oracle's nxo_ipc_step (traj_ipc_sphere_bowl.npz), and 20 steps
+  with lagged friction mu 0.3 (traj_ipc_sphere_bowl_friction.npz).
 
 Every step: adaptive stiffness, contact count and ALM / Newton iteration
 counts equal, and the position / orientation fingerprints within the
@@ -118,23 +119,36 @@ def test_batched_256_scenes_full_run():
     assert worst_p <= TOL_P and worst_r <= TOL_R, (worst_p, worst_r)
 
 
-def test_sphere_bowl_full_ipc_steps():
-    # the primitive-pair model on the 64-sphere configuration: every step's
-    # Newton count, flags and active / candidate pair counts equal, every
-    # body within 1e-6 m and 1e-6 rad of the oracle's step at every step
+def run_ipc_against_fixture(name, mu):
     from nexdynipc_b200 import abi, runtime
-    ref = np.load(os.path.join(GOLDEN, "traj_ipc_sphere_bowl.npz"))
+    ref = np.load(os.path.join(GOLDEN, f"traj_{name}.npz"))
     sc = scenes.sphere_bowl()
     ctx = runtime.Context(sc)
-    p = abi.ipc_params(**scenes.ipc_step_settings())
+    p = abi.ipc_params(**scenes.ipc_step_settings(mu=mu))
     worst_p = worst_r = 0.0
+    keys = [k for k in ("newton_iterations", "converged", "line_search_failed", "n_active", "n_pairs", "n_friction")
+            if k in ref.files]
     for s in range(ref["position"].shape[0]):
         st = ctx.ipc_step(p)     # raises on a non-zero status
-        for k in ("newton_iterations", "converged", "line_search_failed", "n_active", "n_pairs"):
+        for k in keys:
             assert st[k] == ref[k][s], (s, k, st[k], ref[k][s])
         S = ctx.state()
         worst_p = max(worst_p, float(np.abs(S["position"] - ref["position"][s]).max()))
         worst_r = max(worst_r, float(quat_angle(S["orientation"], ref["orientation"][s]).max()))
         assert worst_p <= TOL_P and worst_r <= TOL_R, (s, worst_p, worst_r)
     ctx.close()
-    print(f"sphere_bowl full IPC 40 steps: max |dp| {worst_p:.3e} m, max rotation {worst_r:.3e} rad")
+    return ref["position"].shape[0], worst_p, worst_r
+
+
+def test_sphere_bowl_full_ipc_steps():
+    # the primitive-pair model on the 64-sphere configuration: every step's
+    # Newton count, flags and active / candidate pair counts equal, every
+    # body within 1e-6 m and 1e-6 rad of the oracle's step at every step
+    n, wp, wr = run_ipc_against_fixture("ipc_sphere_bowl", 0.0)
+    print(f"sphere_bowl full IPC {n} steps: max |dp| {wp:.3e} m, max rotation {wr:.3e} rad")
+
+
+def test_sphere_bowl_full_ipc_friction_steps():
+    # the same with the configuration's mu 0.3 as lagged friction (two passes)
+    n, wp, wr = run_ipc_against_fixture("ipc_sphere_bowl_friction", 0.3)
+    print(f"sphere_bowl full IPC + friction {n} steps: max |dp| {wp:.3e} m, max rotation {wr:.3e} rad")
