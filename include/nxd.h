@@ -327,8 +327,12 @@ nxd_status nxd_linear_solve(nxd_ctx* ctx, const nxd_bsr* H, const double* b, dou
  * direct factorisation of one big component fills in): x0 = 0, stop at
  * |r| <= tol |b| or after max_iter iterations (NXD_NOT_CONVERGED).  The
  * matrix must be symmetric positive definite (NXD_FACTOR_FAILED when a
- * diagonal block or p.Ap says otherwise).  H->n_rows may differ from the
- * context's body count: only the context's device and stream are used.
+ * diagonal block or p.Ap says otherwise); the iteration reads its upper
+ * block triangle only (the diagonal blocks' upper entries and the blocks
+ * with column > row; duplicates summed), as LAPACK's uplo = 'U' solvers do,
+ * so the block pattern must be symmetric (NXD_INVALID_ARGUMENT otherwise).
+ * H->n_rows may differ from the context's body count: only the context's
+ * device and stream are used.
  * The whole iteration is one cooperative kernel; stats->kernel_ms is its
  * device time. */
 typedef struct nxd_pcg_stats {

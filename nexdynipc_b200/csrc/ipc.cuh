@@ -166,36 +166,63 @@ __global__ void k_bsr_concat(int N, const int* rpa, const int* cia, const double
 }
 
 // Each query's slice of (query, primitive) pairs, [off[q], off[q] + cnt[q]),
-// sorted by primitive in place, one thread per query: insertion sort for
-// short slices, heapsort beyond (the primitives of a slice are distinct).
+// sorted by primitive in place by insertion, one thread per query (used
+// while no slice is longer than kSliceSortMax; the primitives of a slice are
+// distinct).
+constexpr int kSliceSortMax = 64;
+constexpr int kQueryBuf = 16;     // hits kept per query by k_traverse's count pass
 __global__ void k_sort_query_slices(int* pairs, const int* off, const int* cnt, int nq) {
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
         const int m = cnt[q];
-        if (m < 2) continue;
         int* p = pairs + 2 * (size_t)off[q] + 1;    // primitives at stride 2
-        if (m <= 48) {
-            for (int i = 1; i < m; ++i) {
-                const int v = p[2 * i];
-                int j = i - 1;
-                while (j >= 0 && p[2 * j] > v) { p[2 * (j + 1)] = p[2 * j]; --j; }
-                p[2 * (j + 1)] = v;
-            }
-            continue;
+        for (int i = 1; i < m; ++i) {
+            const int v = p[2 * i];
+            int j = i - 1;
+            while (j >= 0 && p[2 * j] > v) { p[2 * (j + 1)] = p[2 * j]; --j; }
+            p[2 * (j + 1)] = v;
         }
-        auto sift = [&](int root, int end) {
-            while (2 * root + 1 < end) {
-                int ch = 2 * root + 1;
-                if (ch + 1 < end && p[2 * ch] < p[2 * (ch + 1)]) ++ch;
-                if (!(p[2 * root] < p[2 * ch])) return;
-                const int t = p[2 * root]; p[2 * root] = p[2 * ch]; p[2 * ch] = t;
-                root = ch;
+    }
+}
+
+// Each query's hits from its qbuf row, sorted by primitive (insertion, in
+// registers), written as (query, primitive) pairs at off[q].  With `guard`
+// (the trial path) nothing is written while a query overflowed its row
+// (guard[0] or guard[1] set) or the list would pass `cap` pairs.
+__global__ void k_copy_slices(const int* qbuf, const int* cnt, const int* off, int* out, int nq, const int* guard,
+                              long long cap) {
+    if (guard && (guard[0] | guard[1])) return;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const int m = cnt[q];
+        if (m == 0 || off[q] + (long long)m > cap) continue;
+        int h[kQueryBuf];
+#pragma unroll
+        for (int i = 0; i < kQueryBuf; ++i) h[i] = i < m ? qbuf[(size_t)kQueryBuf * q + i] : 0x7fffffff;
+        // insertion sort over the fixed-size row (the padding sorts last)
+#pragma unroll
+        for (int i = 1; i < kQueryBuf; ++i) {
+#pragma unroll
+            for (int j = i; j > 0; --j) {
+                const int a = h[j - 1], b = h[j];
+                h[j - 1] = a < b ? a : b;
+                h[j] = a < b ? b : a;
             }
-        };
-        for (int r = m / 2 - 1; r >= 0; --r) sift(r, m);
-        for (int end = m - 1; end > 0; --end) {
-            const int t = p[0]; p[0] = p[2 * end]; p[2 * end] = t;
-            sift(0, end);
         }
+        int* dst = out + 2 * (size_t)off[q];
+        for (int i = 0; i < m; ++i) { dst[2 * i] = q; dst[2 * i + 1] = h[i]; }
+    }
+}
+
+// pair (q, prim) <-> sort key (q << pbits) | prim
+__global__ void k_pair_keys(const int* pairs, int n, int pbits, unsigned long long* key, int* val) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        key[i] = ((unsigned long long)(unsigned)pairs[2 * i] << pbits) | (unsigned)pairs[2 * i + 1];
+        val[i] = i;
+    }
+}
+__global__ void k_pair_from_keys(const unsigned long long* key, int n, int pbits, int* pairs) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        pairs[2 * i] = (int)(key[i] >> pbits);
+        pairs[2 * i + 1] = (int)(key[i] & ((1ull << pbits) - 1ull));
     }
 }
 
@@ -366,8 +393,12 @@ __global__ void k_sweep_all(PrimGeo pg, int kind, const double* qbox, int nq, co
 // kind 0: vertex queries vs faces (other body); 1: edge queries vs edges
 // (other body, query < prim).
 constexpr int kTravStack = 96;
+// In count mode each query's first kQueryBuf hits also go to its row of
+// qbuf (traversal order) and a query with more raises *maxq to its count,
+// so that a call whose queries all fit copies its lists from qbuf
+// (k_copy_slices) instead of traversing again.
 __global__ void k_traverse(PrimGeo pg, int kind, const double* qbox, int nq, const double* nbox, const int* child, const int* ids,
-                           int n, int* cnt, const int* off, int* out, int* status) {
+                           int n, int* cnt, const int* off, int* out, int* status, int* maxq, int* qbuf) {
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
         double qb[6];
         for (int a = 0; a < 6; ++a) qb[a] = qbox[6 * q + a];
@@ -388,6 +419,8 @@ __global__ void k_traverse(PrimGeo pg, int kind, const double* qbox, int nq, con
                 if (dst) {
                     dst[2 * c] = q;
                     dst[2 * c + 1] = prim;
+                } else if (qbuf && c < kQueryBuf) {
+                    qbuf[(size_t)kQueryBuf * q + c] = prim;
                 }
                 ++c;
                 continue;
@@ -396,7 +429,10 @@ __global__ void k_traverse(PrimGeo pg, int kind, const double* qbox, int nq, con
             stack[top++] = child[2 * node + 1];
             stack[top++] = child[2 * node];
         }
-        if (!out) cnt[q] = c;
+        if (!out) {
+            cnt[q] = c;
+            if (c > kQueryBuf) atomicMax(maxq, c);
+        }
     }
 }
 
@@ -688,9 +724,9 @@ __global__ void k_ipc_pair_energy(PrimGeo pg, IpcPairs P, IpcPose ps, double dha
 // triangle, tot[1] edge-edge); lists over their capacities (cap_pt, cap_ee
 // pairs) are left alone, the caller sees the totals and evaluates again.
 __global__ void k_ipc_pair_energy_dev(PrimGeo pg, const int* pt, const int* ee, const int* tot, int cap_pt, int cap_ee,
-                                      IpcPose ps, double dhat, double kappa, double* e) {
+                                      IpcPose ps, double dhat, double kappa, double* e, const int* guard = nullptr) {
     const int npt = tot[0], nee = tot[1];
-    if (npt > cap_pt || nee > cap_ee) return;
+    if (npt > cap_pt || nee > cap_ee || (guard && (guard[0] | guard[1]))) return;
     const IpcPairs P{pt, npt, ee, nee};
     const int n = npt + nee;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {

@@ -1184,7 +1184,11 @@ struct GrowBuf {
 // (NXD_OK, NXD_FACTOR_FAILED) or NXD_CUDA_ERROR; *iters / *res / *ms report.
 struct PcgScratch {
     GrowBuf minv, vec, part, bar, ints, res;
-    void release() { minv.release(); vec.release(); part.release(); bar.release(); ints.release(); res.release(); }
+    GrowBuf dsym, cnt, urp, uci, uvals, lrp, lidx, lrow;   // the upper block triangle (pcg.cuh)
+    void release() {
+        for (GrowBuf* g : {&minv, &vec, &part, &bar, &ints, &res, &dsym, &cnt, &urp, &uci, &uvals, &lrp, &lidx, &lrow})
+            g->release();
+    }
 };
 nxd_status pcg_device(nxd_ctx* c, PcgScratch& w, int N, const int* rp, const int* ci, const double* vv, const double* bd,
                       double* xd, double tol, int max_iter, int* iters, double* res, float* ms, int* grid) {
@@ -1196,24 +1200,46 @@ nxd_status pcg_device(nxd_ctx* c, PcgScratch& w, int N, const int* rp, const int
     // all CTAs, so more of them cost more than their latency hiding gains
     const int G = (int)std::max<long long>(1, std::min<long long>((long long)std::min(std::max(per_sm, 1), 2) * c->n_sm, need));
     cudaStream_t st = c->stream;
-    if (!w.minv.ensure(288 * (size_t)N) || !w.vec.ensure(48 * 6 * (size_t)N) || !w.part.ensure(8 * 2 * kPcgMaxQ * (size_t)G) ||
-        !w.bar.ensure(8) || !w.ints.ensure(12) || !w.res.ensure(8))
+    if (!w.minv.ensure(8 * kSym * (size_t)N) || !w.dsym.ensure(8 * kSym * (size_t)N) || !w.vec.ensure(48 * 6 * (size_t)N) ||
+        !w.part.ensure(8 * 2 * kPcgMaxQ * (size_t)G) || !w.bar.ensure(8) || !w.ints.ensure(16) || !w.res.ensure(8) ||
+        !w.cnt.ensure(8 * (size_t)N) || !w.urp.ensure(4 * (size_t)(N + 1)) || !w.lrp.ensure(4 * (size_t)(N + 1)))
         return NXD_CUDA_ERROR;
     int* ints = w.ints.as<int>();
     unsigned* bar = w.bar.as<unsigned>();
     double* vec = w.vec.as<double>();
-    NXD_CUDA(cudaMemsetAsync(ints, 0, 3 * sizeof(int), st));
+    int* urp = w.urp.as<int>();
+    int* lrp = w.lrp.as<int>();
+    NXD_CUDA(cudaMemsetAsync(ints, 0, 4 * sizeof(int), st));
     NXD_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st));
-    k_pcg_prepare<<<grid_for(N, 128), 128, 0, st>>>(N, rp, ci, vv, w.minv.as<double>(), ints + 2);
+    k_pcg_prepare<<<grid_for(N, 128), 128, 0, st>>>(N, rp, ci, vv, w.minv.as<double>(), w.dsym.as<double>(), ints + 2);
+    // the upper block triangle: distinct columns per row, their offsets
+    k_pcg_tri_count<<<grid_for(N, 128), 128, 0, st>>>(N, rp, ci, w.cnt.as<int>(), w.cnt.as<int>() + N);
+    k_scan<<<1, 1024, 0, st>>>(w.cnt.as<int>(), urp, N, urp + N, nullptr, nullptr, nullptr);
+    k_scan<<<1, 1024, 0, st>>>(w.cnt.as<int>() + N, lrp, N, lrp + N, nullptr, nullptr, nullptr);
+    int h4[3] = {0, 0, 0};   // fail, upper blocks, lower entries
+    NXD_CUDA(cudaMemcpyAsync(&h4[0], ints + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+    NXD_CUDA(cudaMemcpyAsync(&h4[1], urp + N, sizeof(int), cudaMemcpyDeviceToHost, st));
+    NXD_CUDA(cudaMemcpyAsync(&h4[2], lrp + N, sizeof(int), cudaMemcpyDeviceToHost, st));
+    NXD_CUDA(cudaStreamSynchronize(st));
+    if (h4[0]) return NXD_FACTOR_FAILED;
+    if (h4[1] != h4[2]) return NXD_INVALID_ARGUMENT;   // not structurally symmetric
+    const size_t nu = std::max(h4[1], 1);
+    if (!w.uci.ensure(4 * nu) || !w.uvals.ensure(288 * nu) || !w.lidx.ensure(4 * nu) || !w.lrow.ensure(4 * nu))
+        return NXD_CUDA_ERROR;
+    k_pcg_tri_upper<<<grid_for(N, 128), 128, 0, st>>>(N, rp, ci, vv, urp, w.uci.as<int>(), w.uvals.as<double>());
+    k_pcg_tri_lower<<<grid_for(N, 128), 128, 0, st>>>(N, rp, ci, urp, w.uci.as<int>(), lrp, w.lidx.as<int>(),
+                                                      w.lrow.as<int>(), ints + 3);
     PcgArgs A;
-    A.N = N; A.rp = rp; A.ci = ci; A.vals = vv; A.minv = w.minv.as<double>(); A.b = bd;
+    A.N = N; A.urp = urp; A.uci = w.uci.as<int>(); A.uvals = w.uvals.as<double>();
+    A.lrp = lrp; A.lidx = w.lidx.as<int>(); A.lrow = w.lrow.as<int>(); A.dsym = w.dsym.as<double>();
+    A.minv = w.minv.as<double>(); A.b = bd;
     A.x = xd; A.r[0] = vec; A.r[1] = vec + n6; A.p[0] = vec + 2 * n6; A.p[1] = vec + 3 * n6;
     A.q = vec + 4 * n6; A.z = vec + 5 * n6; A.tol = tol; A.max_iter = max_iter; A.part = w.part.as<double>(); A.stride = G;
     A.bar_count = bar; A.bar_abort = (int*)(bar + 1); A.status = ints; A.iters_out = ints + 1; A.res_out = w.res.as<double>();
     int fail = 0;
-    NXD_CUDA(cudaMemcpyAsync(&fail, ints + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+    NXD_CUDA(cudaMemcpyAsync(&fail, ints + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
     NXD_CUDA(cudaStreamSynchronize(st));
-    if (fail) return NXD_FACTOR_FAILED;
+    if (fail) return NXD_INVALID_ARGUMENT;            // a block without its transpose
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0); cudaEventCreate(&e1);
     void* args[] = {(void*)&A};
@@ -1321,6 +1347,7 @@ struct IpcScal {
     int tot[2];         // candidate totals: point-triangle, edge-edge
     int status;         // traversal status
     int nseg;           // segment count of the last ipc_segments
+    int maxq[2];        // the most candidates of one query, per kind
     int na;             // active barrier pairs
     int pad;
     long long rnz;      // rest-form Hessian blocks
@@ -1354,6 +1381,8 @@ struct IpcState {
     // instead of rebuilt: the candidate lists are sorted by (query,
     // primitive) whatever the hierarchy, so they are the same lists.
     bool keep_trees = false;
+    GrowBuf tkey, tval, tkey1, tval1;    // candidate pairs sorted by (query, primitive) keys
+    GrowBuf qbuf0, qbuf1;                // per query the first hits of the count traversal (k_traverse)
     // lagged friction of the step: the frozen pairs (IpcFric), built from
     // the active pairs of the barrier evaluation that follows fr_build, and
     // the step-start world vertices they measure displacements from
@@ -1381,7 +1410,7 @@ struct IpcState {
                 &grad12, &lam, &z, &nterm, &body, &active, &type, &apos, &alist, &gkey, &gval, &gkey1, &gval1, &hkey,
                 &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &rrp, &rci, &rvv,
                 &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &akp, &akf, &abody, &aact,
-                &aK, &aKphi, &ax, &axb, &alam, &aout, &afail, &fr_vid, &fr_body, &fr_kind, &fr_w, &fr_nrm, &fr_lam,
+                &aK, &aKphi, &ax, &axb, &alam, &aout, &afail, &tkey, &tval, &tkey1, &tval1, &qbuf0, &qbuf1, &fr_vid, &fr_body, &fr_kind, &fr_w, &fr_nrm, &fr_lam,
                 &fr_x0, &fr_e};
     }
     void release() {
@@ -1565,6 +1594,7 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
     GrowBuf* off[2] = {&s->off, &s->off2};
     GrowBuf* out[2] = {&s->pt, &s->ee};
     Bvh* tree[2] = {&s->faces, &s->edges};
+    GrowBuf* qbuf[2] = {&s->qbuf0, &s->qbuf1};
     auto launch = [&](int k, bool count) {
         Bvh& B = *tree[k];
         const double* qbox[2] = {s->qv.as<double>(), s->qe.as<double>()};   // read at launch: the buffers may grow
@@ -1577,7 +1607,8 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
         else
             k_traverse<<<grid_for(nq[k], 128), 128, 0, c->stream>>>(s->pg, k, qbox[k], nq[k], B.nbox.as<double>(),
                                                                     B.child.as<int>(), B.i0.as<int>(), B.n, cn, of, dst,
-                                                                    &ds->status);
+                                                                    &ds->status, &ds->maxq[k],
+                                                                    count ? qbuf[k]->as<int>() : nullptr);
     };
     if (phase == 1) {
         // after the fetch: the totals in pinned memory, then the writes
@@ -1588,25 +1619,54 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
             const int m = s->hp->sc.tot[k];
             IPC_ENSURE(*out[k], 8 * (size_t)std::max(m, 1));
             if (m == 0) continue;
+            if (!sweep && s->hp->sc.maxq[k] == 0) {
+                // every query's hits are in its qbuf row: copied and sorted there
+                k_copy_slices<<<grid_for(nq[k], 128), 128, 0, c->stream>>>(qbuf[k]->as<int>(), cnt[k]->as<int>(),
+                                                                           off[k]->as<int>(), out[k]->as<int>(), nq[k],
+                                                                           nullptr, (long long)m);
+                continue;
+            }
             launch(k, false);
             if (sweep || m < 2) continue;
             // traversal order -> (query, primitive) ascending: the queries'
             // slices are already in query order, so each is sorted alone
-            k_sort_query_slices<<<grid_for(nq[k], 128), 128, 0, c->stream>>>(out[k]->as<int>(), off[k]->as<int>(),
-                                                                             cnt[k]->as<int>(), nq[k]);
+            // (one thread each) while the longest is short; a query with
+            // many hits (a long edge against a fine mesh) would serialise a
+            // thread, so then one stable radix sort of (query, primitive) keys
+            if (s->hp->sc.maxq[k] <= kSliceSortMax) {
+                k_sort_query_slices<<<grid_for(nq[k], 128), 128, 0, c->stream>>>(out[k]->as<int>(), off[k]->as<int>(),
+                                                                                 cnt[k]->as<int>(), nq[k]);
+                continue;
+            }
+            const int pbits = bits_for((unsigned long long)std::max(np[k], 1));
+            const int qbits = bits_for((unsigned long long)std::max(nq[k], 1));
+            IPC_ENSURE(s->tkey, 8 * (size_t)m); IPC_ENSURE(s->tval, 4 * (size_t)m);
+            k_pair_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(out[k]->as<int>(), m, pbits, s->tkey.as<unsigned long long>(),
+                                                                 s->tval.as<int>());
+            const nxd_status st = radix_sort(c, s->tkey, s->tval, s->tkey1, s->tval1, m, 0, pbits + qbits);
+            if (st != NXD_OK) return st;
+            k_pair_from_keys<<<grid_for(m, 256), 256, 0, c->stream>>>(s->tkey.as<unsigned long long>(), m, pbits,
+                                                                      out[k]->as<int>());
         }
         NXD_CUDA(cudaGetLastError());
         return NXD_OK;
     }
     if (phase == 2) {
-        // all-pairs sweep only: the writes into the lists' current
-        // capacities, the totals still on the device (ipc_trial_energy)
+        // the writes into the lists' current capacities, the totals still on
+        // the device (ipc_trial_energy): the all-pairs sweep writes again;
+        // the tree copies the count pass's qbuf rows unless a query
+        // overflowed its row (IpcScal::maxq, then nothing is written)
         for (int k = 0; k < 2; ++k) {
             if (nq[k] == 0 || np[k] == 0) continue;
             const double* qb = k == 0 ? s->qv.as<double>() : s->qe.as<double>();
-            k_sweep_all<<<grid_for(32LL * nq[k], 128), 128, 0, c->stream>>>(s->pg, k, qb, nq[k], tree[k]->leaf.as<double>(),
-                                                                            tree[k]->n, nullptr, off[k]->as<int>(),
-                                                                            out[k]->as<int>(), (long long)(out[k]->cap / 8));
+            if (sweep)
+                k_sweep_all<<<grid_for(32LL * nq[k], 128), 128, 0, c->stream>>>(s->pg, k, qb, nq[k], tree[k]->leaf.as<double>(),
+                                                                                tree[k]->n, nullptr, off[k]->as<int>(),
+                                                                                out[k]->as<int>(), (long long)(out[k]->cap / 8));
+            else
+                k_copy_slices<<<grid_for(nq[k], 128), 128, 0, c->stream>>>(qbuf[k]->as<int>(), cnt[k]->as<int>(),
+                                                                           off[k]->as<int>(), out[k]->as<int>(), nq[k],
+                                                                           ds->maxq, (long long)(out[k]->cap / 8));
         }
         NXD_CUDA(cudaGetLastError());
         return NXD_OK;
@@ -1629,10 +1689,11 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
     IPC_ENSURE(s->qv, 48 * (size_t)std::max(c->nv, 1)); IPC_ENSURE(s->qe, 48 * (size_t)std::max(c->ne, 1));
     if (c->nv) k_ipc_boxes<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(s->pg, 2, s->wq0.as<double>(), w1, 0.0, s->qv.as<double>());
     if (c->ne) k_ipc_boxes<<<grid_for(c->ne, 256), 256, 0, c->stream>>>(s->pg, 3, s->wq0.as<double>(), w1, 0.0, s->qe.as<double>());
-    NXD_CUDA(cudaMemsetAsync(ds, 0, 4 * sizeof(int), c->stream));   // totals, status, segment count
+    NXD_CUDA(cudaMemsetAsync(ds, 0, 6 * sizeof(int), c->stream));   // totals, status, segment count, longest slices
     for (int k = 0; k < 2; ++k) {
         if (nq[k] == 0 || np[k] == 0) continue;
         IPC_ENSURE(*cnt[k], 4 * (size_t)nq[k]); IPC_ENSURE(*off[k], 4 * (size_t)nq[k]);
+        if (!sweep) IPC_ENSURE(*qbuf[k], 4 * (size_t)kQueryBuf * nq[k]);
         launch(k, true);
         k_scan<<<1, 1024, 0, c->stream>>>(cnt[k]->as<int>(), off[k]->as<int>(), nq[k], &ds->tot[k], nullptr, nullptr, nullptr);
     }
@@ -1790,16 +1851,20 @@ nxd_status ipc_barrier_eval(nxd_ctx* c, double dhat, double kappa, bool full, in
 }
 
 // One line-search trial's barrier energy at xt (device) with a single host
-// wait, for scenes on the all-pairs sweep: candidates counted and written
-// into the lists' current capacities (room for twice the last counts), the
-// energy summed over the device-side counts, then one fetch.  *ok is false
-// when the sweep does not apply or a list overflowed: the caller then runs
-// ipc_pose + ipc_candidates + ipc_barrier_eval.  The lists, their order and
-// the sums are that path's.
+// wait: candidates counted and written into the lists' current capacities
+// (room for twice the last counts) -- by the all-pairs sweep, or from the
+// refitted hierarchies' count pass (each query's hits kept in its qbuf row)
+// inside a step -- the energy summed over the device-side counts, then one
+// fetch.  *ok is false outside a step for a tree-sized scene, when a list
+// overflowed or a query had more hits than its row holds: the caller then
+// runs ipc_pose + ipc_candidates + ipc_barrier_eval.  The lists, their order
+// and the sums are that path's.
 nxd_status ipc_trial_energy(nxd_ctx* c, const double* xt, double dhat, double kappa, bool* ok) {
     IpcState* s = c->ipc;
     *ok = false;
-    if ((long long)c->nv * c->nf + (long long)c->ne * c->ne > kSweepAllTests) return NXD_OK;
+    const bool sweep = (long long)c->nv * c->nf + (long long)c->ne * c->ne <= kSweepAllTests;
+    // the hierarchies: only within a step, whose first iterate built them
+    if (!sweep && !s->keep_trees) return NXD_OK;
     // capacities grow geometrically, so that a count creeping upwards does
     // not reallocate (and synchronise) on every trial
     auto room = [](GrowBuf& b, size_t want) { return want <= b.cap || b.ensure(std::max(want, 2 * b.cap)); };
@@ -1822,13 +1887,15 @@ nxd_status ipc_trial_energy(nxd_ctx* c, const double* xt, double dhat, double ka
     IpcScal* ds = s->ds();
     const IpcPose ps{s->wq0.as<double>(), s->pp0.as<double>(), s->pose_x ? s->x0.as<double>() : nullptr};
     k_ipc_pair_energy_dev<<<grid_for((long long)cap_pt + cap_ee, 128), 128, 0, c->stream>>>(
-        s->pg, s->pt.as<int>(), s->ee.as<int>(), ds->tot, cap_pt, cap_ee, ps, dhat, kappa, s->e.as<double>());
+        s->pg, s->pt.as<int>(), s->ee.as<int>(), ds->tot, cap_pt, cap_ee, ps, dhat, kappa, s->e.as<double>(),
+        sweep ? nullptr : ds->maxq);
     k_tree_sum_pairs<<<1, 1024, 0, c->stream>>>(s->e.as<double>(), ds->tot, cap_pt, cap_ee, &ds->energy);
     if (s->fr_n) ipc_friction_energy(c, ps);
     if ((st = ipc_fetch(c)) != NXD_OK) return st;
     const IpcScal& hs = s->hp->sc;
     if (hs.status != 0) return (nxd_status)hs.status;
     if (hs.tot[0] > cap_pt || hs.tot[1] > cap_ee) return NXD_OK;
+    if (!sweep && (hs.maxq[0] | hs.maxq[1])) return NXD_OK;
     s->n_pt = hs.tot[0];
     s->n_ee = hs.tot[1];
     *ok = true;

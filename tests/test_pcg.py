@@ -87,3 +87,40 @@ def test_pcg_large_banded_system():
     r = bsr_matvec(rp, ci, vals, x) - b
     assert np.linalg.norm(r) <= 1e-11 * np.linalg.norm(b)
     assert st["grid"] > 1
+
+
+def test_pcg_reads_the_upper_block_triangle():
+    # the lower triangle is not read: zeroing it changes no bit of the
+    # solution; duplicate upper blocks are summed; a block without its
+    # transposed partner is rejected
+    ctx = small_context()
+    rp, ci, vals = banded_system(200, offsets=(1, 5, 33), seed=6)
+    b = np.random.default_rng(3).normal(size=6 * 200)
+    x, st = ctx.pcg_solve(rp, ci, vals, b, tol=1e-13, max_iter=500)
+    rows = np.repeat(np.arange(200), np.diff(rp))
+    low = vals.copy()
+    low[ci < rows] = 0.0
+    low[ci == rows] = np.triu(vals[ci == rows].reshape(-1, 6, 6)).reshape(-1, 36)
+    x2, _ = ctx.pcg_solve(rp, ci, low, b, tol=1e-13, max_iter=500)
+    assert np.array_equal(x, x2)
+    # split every upper block into two halves stored side by side
+    up = ci > rows
+    k_up = np.nonzero(up)[0]
+    rp3 = rp.copy()
+    for r in rows[k_up]:
+        rp3[r + 1:] += 1
+    order = np.argsort(np.concatenate([np.arange(len(ci)), k_up]), kind="stable")
+    ci3 = np.concatenate([ci, ci[k_up]])[order].astype(np.int32)
+    v3 = np.concatenate([np.where(up[:, None], 0.5 * vals, vals), 0.5 * vals[k_up]])[order]
+    x3, _ = ctx.pcg_solve(rp3, ci3, np.ascontiguousarray(v3), b, tol=1e-13, max_iter=500)
+    assert np.abs(x3 - x).max() <= 1e-12 * np.abs(x).max()
+    # drop one block below the diagonal: the pattern is no longer symmetric
+    from nexdynipc_b200 import runtime
+    k = int(np.nonzero(ci < rows)[0][5])
+    keep = np.ones(len(ci), bool)
+    keep[k] = False
+    rp4 = rp.copy()
+    rp4[rows[k] + 1:] -= 1
+    with pytest.raises(runtime.NxdError) as e:
+        ctx.pcg_solve(rp4, ci[keep], np.ascontiguousarray(vals[keep]), b)
+    assert e.value.status == 7                               # NXD_INVALID_ARGUMENT
