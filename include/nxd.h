@@ -438,8 +438,11 @@ nxd_status nxd_ipc_barrier(nxd_ctx* ctx, const double* x, double dhat, double ka
 /* nxd_ipc_max_step: the line-search bound OptimizationProblem::maxStep
  * (Math/NewtonSolver.h:42) for the step x -> x + dx: the smallest additive-CCD
  * time of impact in [0, 1] over the pairs whose swept boxes overlap, each
- * pair keeping eta of its initial distance (points move on the chords
- * between their positions at x and x + dx). */
+ * pair keeping eta of its initial distance.  The points move rigidly with
+ * their bodies along the iterates x + t dx (rotation vectors interpolated,
+ * so the pose at t is the one a line search evaluates at alpha = t); the
+ * swept boxes (here and in nxd_ipc_candidates with dx) are padded by each
+ * body's |dtheta| r_max / 2 so that they contain the rotation arcs. */
 nxd_status nxd_ipc_max_step(nxd_ctx* ctx, const double* x, const double* dx, double eta, double* alpha,
                             int64_t* n_pairs);
 

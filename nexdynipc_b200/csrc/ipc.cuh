@@ -104,14 +104,33 @@ __device__ __forceinline__ void box_of(const double* w0, const double* w1, const
     st3(out + 3, mx + e);
 }
 
-// kind 0: face leaves, 1: edge leaves, 2: vertex queries, 3: edge queries
-__global__ void k_ipc_boxes(PrimGeo pg, int kind, const double* w0, const double* w1, double infl, double* out) {
+// kind 0: face leaves, 1: edge leaves, 2: vertex queries, 3: edge queries.
+// pad (swept boxes of the rigid arcs, per body; may be null) widens each box
+// by its body's arc bound (ipc::arc_box_pad).
+__global__ void k_ipc_boxes(PrimGeo pg, int kind, const double* w0, const double* w1, double infl, double* out,
+                            const double* pad = nullptr) {
     const int n = kind == 0 ? pg.nf : (kind == 2 ? pg.nv : pg.ne);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        if (kind == 0) box_of(w0, w1, pg.fvert + 3 * i, 3, infl, out + 6 * i);
-        else if (kind == 2) box_of(w0, w1, &i, 1, infl, out + 6 * i);
-        else box_of(w0, w1, pg.evert + 2 * i, 2, infl, out + 6 * i);
+        const int b = kind == 0 ? pg.fbody[i] : (kind == 2 ? pg.vbody[i] : pg.ebody[i]);
+        const double e = pad ? infl + pad[b] : infl;
+        if (kind == 0) box_of(w0, w1, pg.fvert + 3 * i, 3, e, out + 6 * i);
+        else if (kind == 2) box_of(w0, w1, &i, 1, e, out + 6 * i);
+        else box_of(w0, w1, pg.evert + 2 * i, 2, e, out + 6 * i);
     }
+}
+
+// the largest |v| over each body's local vertices (0 for a meshless body)
+__global__ void k_body_rmax(Geo g, double* rmax) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < g.N; b += gridDim.x * blockDim.x) {
+        double r = 0.0;
+        for (int v = g.voff[b]; v < g.voff[b + 1]; ++v) r = dmax(r, norm(ld3(g.verts + 3 * v)));
+        rmax[b] = r;
+    }
+}
+// per body the arc pad of the swept boxes along dx
+__global__ void k_arc_pad(int N, const double* dx, const double* rmax, double* pad) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < N; b += gridDim.x * blockDim.x)
+        pad[b] = ipc::arc_box_pad(ld3(dx + 6 * b + 3), rmax[b]);
 }
 
 // Global primitive topology from the body-local meshes: one thread per body.
@@ -888,16 +907,17 @@ __global__ void k_ipc_rowptr(const unsigned long long* hkey, const int* start, c
 
 // ---------------------------------------------------------------------------
 // Additive CCD over the candidate pairs (swept boxes): per pair the time of
-// impact along the chords of its points (ipc::accd_toi), one warp per pair
-// with a round's kAccdLookahead samples in its lanes, then the minimum (one
-// block).
+// impact along its points' motion (ipc::accd_toi_motion; the step uses the
+// rigid arcs, ipc::ArcMotion), one warp per pair with a round's
+// kAccdLookahead samples in its lanes, then the minimum (one block).
 // ---------------------------------------------------------------------------
 static_assert(ipc::kAccdLookahead == 32, "one sample per lane");
-__device__ double accd_toi_warp(int kind, const V3* X0, const V3* P0, double t_max, double eta, int max_iter) {
+template <typename M>
+__device__ double accd_toi_warp(int kind, const M& m, double t_max, double eta, int max_iter) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const double lp = ipc::accd_lipschitz(kind, P0);
-    const double d0 = sqrt(ipc::dist2(kind, X0));
+    const double lp = m.lipschitz();
+    const double d0 = m.distance(0.0);
     if (!(lp > 0.0)) return t_max;
     if (!(d0 > 0.0)) return 0.0;
     const double g = eta * d0;
@@ -909,7 +929,7 @@ __device__ double accd_toi_warp(int kind, const V3* X0, const V3* P0, double t_m
         const double thr = g + 0.9 * (d - g);
         const double tj = t + (double)(lane + 1) * dl;
         const bool past = tj >= t_max;
-        const double dj = past ? 0.0 : ipc::accd_distance(kind, X0, P0, tj);
+        const double dj = past ? 0.0 : m.distance(tj);
         // the round ends at the first sample past t_max or below thr
         const unsigned stop = __ballot_sync(full, past || !(dj >= thr));
         const int J = stop ? __ffs(stop) - 1 : 31;
@@ -922,29 +942,30 @@ __device__ double accd_toi_warp(int kind, const V3* X0, const V3* P0, double t_m
     return t;
 }
 
-__global__ void k_ipc_accd(PrimGeo pg, IpcPairs P, const double* wq0, const double* wq1, double eta, int max_iter, double* toi) {
+// Time of impact of each candidate pair along the rigid arcs x + t dx
+// (ipc::ArcMotion: body-local vertices vloc, step-start orientations q0).
+__global__ void k_ipc_accd(PrimGeo pg, IpcPairs P, const double* vloc, const double* x, const double* dx, const double* q0,
+                           double eta, int max_iter, double* toi) {
     const int n = P.n_pt + P.n_ee;
     const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long pp = w0; pp < n; pp += nw) {
         const int p = (int)pp;
-        int vid[4], kind;
-        if (p < P.n_pt) {
-            kind = ipc::kPairPT;
-            const int v = P.pt[2 * p], f = P.pt[2 * p + 1];
-            vid[0] = v; vid[1] = pg.fvert[3 * f]; vid[2] = pg.fvert[3 * f + 1]; vid[3] = pg.fvert[3 * f + 2];
-        } else {
-            kind = ipc::kPairEE;
-            const int q = p - P.n_pt;
-            const int e0 = P.ee[2 * q], e1 = P.ee[2 * q + 1];
-            vid[0] = pg.evert[2 * e0]; vid[1] = pg.evert[2 * e0 + 1]; vid[2] = pg.evert[2 * e1]; vid[3] = pg.evert[2 * e1 + 1];
+        int vid[4], kind, bA, bB;
+        pair_vids(pg, P, p, vid, kind, bA, bB);
+        ipc::ArcMotion m;
+        m.kind = kind;
+        fric_sides(kind, m.side);
+        const int b[2] = {bA, bB};
+        for (int sd = 0; sd < 2; ++sd) {
+            m.b[sd].p = ld3(x + 6 * b[sd]);
+            m.b[sd].th = ld3(x + 6 * b[sd] + 3);
+            m.b[sd].dp = ld3(dx + 6 * b[sd]);
+            m.b[sd].dth = ld3(dx + 6 * b[sd] + 3);
+            m.b[sd].q0 = ldq(q0 + 4 * b[sd]);
         }
-        V3 X[4], D[4];
-        for (int k = 0; k < 4; ++k) {
-            X[k] = ld3(wq0 + 3 * vid[k]);
-            D[k] = ld3(wq1 + 3 * vid[k]) - X[k];
-        }
-        const double tp = accd_toi_warp(kind, X, D, 1.0, eta, max_iter);
+        for (int k = 0; k < 4; ++k) m.v[k] = ld3(vloc + 3 * vid[k]);
+        const double tp = accd_toi_warp(kind, m, 1.0, eta, max_iter);
         if ((threadIdx.x & 31) == 0) toi[p] = tp;
     }
 }

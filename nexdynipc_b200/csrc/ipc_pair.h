@@ -654,10 +654,62 @@ NX_HD double accd_distance(int kind, const V3* X0, const V3* P0, double t) {
     return sqrt(dist2(kind, X));
 }
 
-NX_HD double accd_toi(int kind, const V3* X0, const V3* P0, double t_max, double eta, int max_iter, int* iters) {
-    const double lp = accd_lipschitz(kind, P0);
+// The points moving on their chords: X_k(t) = X0_k + t P0_k.
+struct ChordMotion {
+    V3 X0[4], P0[4];
+    int kind;
+    NX_HD double lipschitz() const { return accd_lipschitz(kind, P0); }
+    NX_HD double distance(double t) const { return accd_distance(kind, X0, P0, t); }
+};
+
+// The points moving rigidly with their bodies along the iterates x + t dx:
+// point k (body-local v_k, body side[k]) at t is
+//   p + t dp + rot(Exp(theta + t dtheta) q0, v_k),
+// the world-vertex formula at the pose x + t dx, so the pose of a line-search
+// trial at alpha is this motion at t = alpha bit for bit.  Its speed is at
+// most |dp| + |dtheta| |v_k| (|J_l(theta)| <= 1); with the common velocity
+// dp_A removed, the distance changes at most at
+//   max_{k on A} |dtheta_A| |v_k| + max_{k on B} (|dp_B - dp_A| + |dtheta_B| |v_k|).
+struct ArcBody {
+    V3 p, dp, th, dth;
+    Q q0;
+};
+struct ArcMotion {
+    ArcBody b[2];
+    V3 v[4];
+    int side[4];
+    int kind;
+    NX_HD void points(double t, V3* X) const {
+        V3 pp[2];
+        Q q[2];
+        for (int s = 0; s < 2; ++s) {
+            pp[s] = b[s].p + t * b[s].dp;
+            q[s] = rot_gt(b[s].q0, b[s].th + t * b[s].dth);
+        }
+        for (int k = 0; k < 4; ++k) X[k] = pp[side[k]] + qrot(q[side[k]], v[k]);
+    }
+    NX_HD double lipschitz() const {
+        const double wa = norm(b[0].dth), wb = norm(b[1].dth), tb = norm(b[1].dp - b[0].dp);
+        double la = 0.0, lb = 0.0;
+        for (int k = 0; k < 4; ++k) {
+            if (side[k] == 0) la = dmax(la, wa * norm(v[k]));
+            else lb = dmax(lb, tb + wb * norm(v[k]));
+        }
+        return la + lb;
+    }
+    NX_HD double distance(double t) const {
+        V3 X[4];
+        points(t, X);
+        return sqrt(dist2(kind, X));
+    }
+};
+
+// Additive CCD along a motion M (ChordMotion or ArcMotion).
+template <typename M>
+NX_HD double accd_toi_motion(int kind, const M& m, double t_max, double eta, int max_iter, int* iters) {
+    const double lp = m.lipschitz();
     if (iters) *iters = 0;
-    const double d0 = sqrt(dist2(kind, X0));
+    const double d0 = m.distance(0.0);
     if (!(lp > 0.0)) return t_max;
     if (!(d0 > 0.0)) return 0.0;
     const double g = eta * d0;
@@ -672,7 +724,7 @@ NX_HD double accd_toi(int kind, const V3* X0, const V3* P0, double t_max, double
         for (int j = 1; j <= kAccdLookahead; ++j) {
             const double tj = t + (double)j * dl;
             if (tj >= t_max) return t_max;
-            const double dj = accd_distance(kind, X0, P0, tj);
+            const double dj = m.distance(tj);
             tn = tj;
             dn = dj;
             if (!(dj >= thr)) break;
@@ -682,6 +734,20 @@ NX_HD double accd_toi(int kind, const V3* X0, const V3* P0, double t_max, double
     }
     return t;
 }
+
+NX_HD double accd_toi(int kind, const V3* X0, const V3* P0, double t_max, double eta, int max_iter, int* iters) {
+    ChordMotion m;
+    for (int k = 0; k < 4; ++k) { m.X0[k] = X0[k]; m.P0[k] = P0[k]; }
+    m.kind = kind;
+    return accd_toi_motion(kind, m, t_max, eta, max_iter, iters);
+}
+
+// Swept boxes for the arc motion: a point's rotation part moves at most
+// |dtheta| |v| per unit t, so it stays within |dtheta| |v| / 2 of one of its
+// ends (the translation part is linear, exact on the chord); the box of a
+// body's endpoints padded by |dtheta_b| r_b / 2 (r_b its largest |v|)
+// contains its points' arcs.
+NX_HD double arc_box_pad(V3 dth, double r_body) { return 0.5 * (norm(dth) * r_body); }
 
 }  // namespace ipc
 }  // namespace nx

@@ -1383,6 +1383,7 @@ struct IpcState {
     bool keep_trees = false;
     GrowBuf tkey, tval, tkey1, tval1;    // candidate pairs sorted by (query, primitive) keys
     GrowBuf qbuf0, qbuf1;                // per query the first hits of the count traversal (k_traverse)
+    GrowBuf dxv, rmax, pad;              // the last ipc_pose's dx, per-body vertex radius and arc pad
     // lagged friction of the step: the frozen pairs (IpcFric), built from
     // the active pairs of the barrier evaluation that follows fr_build, and
     // the step-start world vertices they measure displacements from
@@ -1410,7 +1411,7 @@ struct IpcState {
                 &grad12, &lam, &z, &nterm, &body, &active, &type, &apos, &alist, &gkey, &gval, &gkey1, &gval1, &hkey,
                 &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &rrp, &rci, &rvv,
                 &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &akp, &akf, &abody, &aact,
-                &aK, &aKphi, &ax, &axb, &alam, &aout, &afail, &tkey, &tval, &tkey1, &tval1, &qbuf0, &qbuf1, &fr_vid, &fr_body, &fr_kind, &fr_w, &fr_nrm, &fr_lam,
+                &aK, &aKphi, &ax, &axb, &alam, &aout, &afail, &tkey, &tval, &tkey1, &tval1, &qbuf0, &qbuf1, &dxv, &rmax, &pad, &fr_vid, &fr_body, &fr_kind, &fr_w, &fr_nrm, &fr_lam,
                 &fr_x0, &fr_e};
     }
     void release() {
@@ -1443,6 +1444,8 @@ nxd_status ipc_init(nxd_ctx* c, IpcState* s) {
                     s->evert.as<int>()};
     IPC_ENSURE(s->scal, sizeof(IpcScal));
     NXD_CUDA(cudaMemsetAsync(s->scal.p, 0, sizeof(IpcScal), c->stream));
+    IPC_ENSURE(s->rmax, 8 * (size_t)c->N); IPC_ENSURE(s->pad, 8 * (size_t)c->N);
+    k_body_rmax<<<grid_for(c->N, 128), 128, 0, c->stream>>>(c->geo, s->rmax.as<double>());
     NXD_CUDA(cudaMallocHost(&s->hp, sizeof(IpcHost)));
     NXD_CUDA(cudaMallocHost(&s->hrow, 12 * (size_t)(c->N + 1)));
     NXD_CUDA(cudaGetLastError());
@@ -1488,7 +1491,9 @@ nxd_status ipc_pose(nxd_ctx* c, const double* x, const double* dx, bool on_devic
                                                                   s->wq0.as<double>());
     if (dx) {
         IPC_ENSURE(s->x1, 48 * (size_t)N); IPC_ENSURE(s->pp1, 24 * (size_t)N); IPC_ENSURE(s->pq1, 32 * (size_t)N);
-        IPC_ENSURE(s->wq1, 24 * (size_t)c->nv);
+        IPC_ENSURE(s->wq1, 24 * (size_t)c->nv); IPC_ENSURE(s->dxv, 48 * (size_t)N);
+        NXD_CUDA(cudaMemcpyAsync(s->dxv.p, dx, 48 * (size_t)N, kind, c->stream));
+        k_arc_pad<<<grid_for(N, 128), 128, 0, c->stream>>>(N, s->dxv.as<double>(), s->rmax.as<double>(), s->pad.as<double>());
         NXD_CUDA(cudaMemcpyAsync(s->x1.p, dx, 48 * (size_t)N, kind, c->stream));
         k_axpy_vec<<<grid_for(6 * N, 256), 256, 0, c->stream>>>(s->x0.as<double>(), s->x1.as<double>(), 6 * N, s->x1.as<double>());
         k_pose_at_x<<<grid_for(N, 128), 128, 0, c->stream>>>(N, s->x1.as<double>(), c->quat, s->pp1.as<double>(), s->pq1.as<double>());
@@ -1534,7 +1539,8 @@ nxd_status ipc_build_bvh(nxd_ctx* c, Bvh& B, int kind, bool swept, double infl) 
     IPC_ENSURE(B.leaf, 48 * (size_t)n);
     if (n == 0) return NXD_OK;
     const double* w1 = swept ? s->wq1.as<double>() : nullptr;
-    k_ipc_boxes<<<grid_for(n, 256), 256, 0, c->stream>>>(s->pg, kind, s->wq0.as<double>(), w1, infl, B.leaf.as<double>());
+    k_ipc_boxes<<<grid_for(n, 256), 256, 0, c->stream>>>(s->pg, kind, s->wq0.as<double>(), w1, infl, B.leaf.as<double>(),
+                                                         swept ? s->pad.as<double>() : nullptr);
     if (s->keep_trees && B.topo_n == n) {
         // the step's hierarchy, boxes refitted bottom-up
         NXD_CUDA(cudaMemsetAsync(B.flags.p, 0, 4 * (size_t)n, c->stream));
@@ -1672,13 +1678,14 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
         return NXD_OK;
     }
     s->cand_swept = swept;
+    const double* pad = swept ? s->pad.as<double>() : nullptr;
     if (sweep) {
         for (int k = 0; k < 2; ++k) {
             tree[k]->n = np[k];
             IPC_ENSURE(tree[k]->leaf, 48 * (size_t)std::max(np[k], 1));
             if (np[k])
                 k_ipc_boxes<<<grid_for(np[k], 256), 256, 0, c->stream>>>(s->pg, k, s->wq0.as<double>(), w1, infl,
-                                                                         tree[k]->leaf.as<double>());
+                                                                         tree[k]->leaf.as<double>(), pad);
         }
     } else {
         for (int k = 0; k < 2; ++k) {
@@ -1687,8 +1694,10 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
         }
     }
     IPC_ENSURE(s->qv, 48 * (size_t)std::max(c->nv, 1)); IPC_ENSURE(s->qe, 48 * (size_t)std::max(c->ne, 1));
-    if (c->nv) k_ipc_boxes<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(s->pg, 2, s->wq0.as<double>(), w1, 0.0, s->qv.as<double>());
-    if (c->ne) k_ipc_boxes<<<grid_for(c->ne, 256), 256, 0, c->stream>>>(s->pg, 3, s->wq0.as<double>(), w1, 0.0, s->qe.as<double>());
+    if (c->nv)
+        k_ipc_boxes<<<grid_for(c->nv, 256), 256, 0, c->stream>>>(s->pg, 2, s->wq0.as<double>(), w1, 0.0, s->qv.as<double>(), pad);
+    if (c->ne)
+        k_ipc_boxes<<<grid_for(c->ne, 256), 256, 0, c->stream>>>(s->pg, 3, s->wq0.as<double>(), w1, 0.0, s->qe.as<double>(), pad);
     NXD_CUDA(cudaMemsetAsync(ds, 0, 6 * sizeof(int), c->stream));   // totals, status, segment count, longest slices
     for (int k = 0; k < 2; ++k) {
         if (nq[k] == 0 || np[k] == 0) continue;
@@ -1909,8 +1918,9 @@ nxd_status ipc_accd(nxd_ctx* c, double eta) {
     const int n = s->n_pt + s->n_ee;
     IPC_ENSURE(s->toi, 8 * (size_t)std::max(n, 1));
     const IpcPairs P{s->pt.as<int>(), s->n_pt, s->ee.as<int>(), s->n_ee};
-    if (n) k_ipc_accd<<<grid_for(32LL * n, 128), 128, 0, c->stream>>>(s->pg, P, s->wq0.as<double>(), s->wq1.as<double>(), eta, 1000,
-                                                                s->toi.as<double>());
+    // along the rigid arcs from the last ipc_pose's x (x0) by its dx
+    if (n) k_ipc_accd<<<grid_for(32LL * n, 128), 128, 0, c->stream>>>(s->pg, P, c->geo.verts, s->x0.as<double>(),
+                                                                s->dxv.as<double>(), c->quat, eta, 1000, s->toi.as<double>());
     k_min_reduce<<<1, 1024, 0, c->stream>>>(s->toi.as<double>(), n, 1.0, &s->ds()->alpha);
     NXD_CUDA(cudaGetLastError());
     return NXD_OK;

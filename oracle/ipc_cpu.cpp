@@ -32,6 +32,9 @@ struct Geo {
     std::vector<int32_t> vbody, fbody, fvert, ebody, evert;
     std::vector<double> wv, wv1, pos;
     std::vector<double> theta;   // [3N] rotation vectors of the iterate (zeros without one)
+    // with dx: the arc motion (body-local vertices, orientations, x, dx) and
+    // each body's swept-box pad (ipc::arc_box_pad)
+    std::vector<double> vloc, quat, x, dx, pad;
 };
 
 Geo load(nxo_world* w, const double* x, const double* dx) {
@@ -51,13 +54,23 @@ Geo load(nxo_world* w, const double* x, const double* dx) {
         for (size_t i = 0; i < x1.size(); ++i) x1[i] = x[i] + dx[i];
         g.wv1.resize(3 * g.nv);
         nxo_world_vertices_at(w, x1.data(), g.wv1.data(), nullptr);
+        g.vloc.resize(3 * g.nv); g.quat.resize(4 * (size_t)g.N);
+        nxo_local_vertices(w, g.vloc.data(), g.quat.data());
+        g.x.assign(x, x + 6 * (size_t)g.N);
+        g.dx.assign(dx, dx + 6 * (size_t)g.N);
+        std::vector<double> rmax(g.N, 0.0);
+        for (int64_t v = 0; v < g.nv; ++v)
+            rmax[g.vbody[v]] = nx::dmax(rmax[g.vbody[v]], nx::norm(nx::ld3(&g.vloc[3 * v])));
+        g.pad.resize(g.N);
+        for (int b = 0; b < g.N; ++b) g.pad[b] = ipc::arc_box_pad(nx::ld3(&g.dx[6 * b + 3]), rmax[b]);
     }
     return g;
 }
 
 struct Box { double mn[3], mx[3]; };
 
-Box box_of(const Geo& g, const int32_t* vid, int nvid, double infl) {
+Box box_of(const Geo& g, const int32_t* vid, int nvid, double infl, int body) {
+    if (!g.pad.empty()) infl = infl + g.pad[body];
     V3 mn = nx::ld3(&g.wv[3 * vid[0]]), mx = mn;
     for (int k = 0; k < nvid; ++k) {
         const V3 a = nx::ld3(&g.wv[3 * vid[k]]);
@@ -161,9 +174,12 @@ std::vector<int32_t> sweep(const std::vector<Box>& q, const std::vector<Box>& le
 
 void candidates(const Geo& g, double infl, std::vector<int32_t>& pt, std::vector<int32_t>& ee) {
     std::vector<Box> fb(g.nf), eb(g.ne), qv(g.nv), qe(g.ne);
-    for (int64_t f = 0; f < g.nf; ++f) fb[f] = box_of(g, &g.fvert[3 * f], 3, infl);
-    for (int64_t e = 0; e < g.ne; ++e) { eb[e] = box_of(g, &g.evert[2 * e], 2, infl); qe[e] = box_of(g, &g.evert[2 * e], 2, 0.0); }
-    for (int64_t v = 0; v < g.nv; ++v) { const int32_t id = (int32_t)v; qv[v] = box_of(g, &id, 1, 0.0); }
+    for (int64_t f = 0; f < g.nf; ++f) fb[f] = box_of(g, &g.fvert[3 * f], 3, infl, g.fbody[f]);
+    for (int64_t e = 0; e < g.ne; ++e) {
+        eb[e] = box_of(g, &g.evert[2 * e], 2, infl, g.ebody[e]);
+        qe[e] = box_of(g, &g.evert[2 * e], 2, 0.0, g.ebody[e]);
+    }
+    for (int64_t v = 0; v < g.nv; ++v) { const int32_t id = (int32_t)v; qv[v] = box_of(g, &id, 1, 0.0, g.vbody[v]); }
     pt = sweep(qv, fb, [&](int v, int f) { return g.vbody[v] != g.fbody[f]; });
     ee = sweep(qe, eb, [&](int a, int b) { return a < b && g.ebody[a] != g.ebody[b]; });
 }
@@ -498,17 +514,20 @@ double nxo_ipc_max_step(nxo_world* w, const double* x, const double* dx, double 
         V3 X[4], arm[4];
         pair_points(g, P, E, p, kind, X, side, arm, bA, bB);
         int vid[4];
-        if (p < P.size() / 2) {
-            const int v = P[2 * p], f = P[2 * p + 1];
-            vid[0] = v; vid[1] = g.fvert[3 * f]; vid[2] = g.fvert[3 * f + 1]; vid[3] = g.fvert[3 * f + 2];
-        } else {
-            const size_t q = p - P.size() / 2;
-            vid[0] = g.evert[2 * E[2 * q]]; vid[1] = g.evert[2 * E[2 * q] + 1];
-            vid[2] = g.evert[2 * E[2 * q + 1]]; vid[3] = g.evert[2 * E[2 * q + 1] + 1];
+        pair_vids(g, P, E, p, vid);
+        // along the rigid arcs x + t dx (ipc::ArcMotion)
+        ipc::ArcMotion m;
+        m.kind = kind;
+        const int b[2] = {bA, bB};
+        for (int sd = 0; sd < 2; ++sd) {
+            m.b[sd].p = nx::ld3(&g.x[6 * b[sd]]);
+            m.b[sd].th = nx::ld3(&g.x[6 * b[sd] + 3]);
+            m.b[sd].dp = nx::ld3(&g.dx[6 * b[sd]]);
+            m.b[sd].dth = nx::ld3(&g.dx[6 * b[sd] + 3]);
+            m.b[sd].q0 = nx::ldq(&g.quat[4 * b[sd]]);
         }
-        V3 D[4];
-        for (int k = 0; k < 4; ++k) D[k] = nx::ld3(&g.wv1[3 * vid[k]]) - X[k];
-        t = nx::dmin(t, ipc::accd_toi(kind, X, D, 1.0, eta, 1000, nullptr));
+        for (int k = 0; k < 4; ++k) { m.side[k] = side[k]; m.v[k] = nx::ld3(&g.vloc[3 * vid[k]]); }
+        t = nx::dmin(t, ipc::accd_toi_motion(kind, m, 1.0, eta, 1000, nullptr));
     }
     return t;
 }

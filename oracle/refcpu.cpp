@@ -2908,6 +2908,22 @@ void nxo_prim_topology(nxo_world* w, int32_t* vbody, int32_t* fbody, int32_t* fv
 // World vertices and body positions at state x (6N; p = x[6i..], q =
 // exp(theta) q_body as in detectContactsAtState), or at the current poses
 // when x is NULL.
+// Body-local vertex coordinates in the global numbering (bodies in order)
+// and each body's orientation (w, x, y, z): the arc motion of the CCD.
+void nxo_local_vertices(nxo_world* w, double* vloc, double* quat) {
+    int vo = 0;
+    for (int i = 0; i < (int)w->bodies.size(); ++i) {
+        const Body& B = w->bodies[i];
+        if (quat) { quat[4 * i] = B.orientation.w; quat[4 * i + 1] = B.orientation.x; quat[4 * i + 2] = B.orientation.y; quat[4 * i + 3] = B.orientation.z; }
+        if (B.mesh < 0) continue;
+        const Mesh& M = w->meshes[B.mesh];
+        for (size_t v = 0; v < M.V.size(); ++v) {
+            if (vloc) { vloc[3 * (vo + v)] = M.V[v].x; vloc[3 * (vo + v) + 1] = M.V[v].y; vloc[3 * (vo + v) + 2] = M.V[v].z; }
+        }
+        vo += (int)M.V.size();
+    }
+}
+
 void nxo_world_vertices_at(nxo_world* w, const double* x, double* wv, double* pos) {
     int vo = 0;
     for (int i = 0; i < (int)w->bodies.size(); ++i) {

@@ -98,6 +98,7 @@ int32_t nxo_body_count(nxo_world* w);
 void nxo_prim_counts(nxo_world* w, int64_t* nv, int64_t* nf, int64_t* ne);
 void nxo_prim_topology(nxo_world* w, int32_t* vbody, int32_t* fbody, int32_t* fvert, int32_t* ebody, int32_t* evert);
 void nxo_world_vertices_at(nxo_world* w, const double* x, double* wv, double* pos);
+void nxo_local_vertices(nxo_world* w, double* vloc, double* quat);
 
 /* Primitive-level contact model (full IPC), ipc_cpu.cpp. */
 int nxo_ipc_candidates(nxo_world* w, const double* x, const double* dx, double inflation, int32_t* pt, int64_t pt_cap,

@@ -107,3 +107,26 @@ def test_ipc_max_step_matches_oracle(name):
     assert 0.0 <= ag <= 1.0
     assert ag <= ao + 1e-12
     assert ag == ao
+
+
+def test_ipc_max_step_follows_the_rotation_arc():
+    # the oracle's arc case (tests/test_ipc_oracle.py): a cube turned by 90
+    # degrees whose corners swing below the ground half-way; the device bound
+    # equals the oracle's bit for bit and stops before the arc's contact
+    sc = scenes.ipc_drop(n_cubes=1)
+    st = sc.initial_state()
+    st["orientation"][1] = [1.0, 0.0, 0.0, 0.0]
+    st["position"][1] = [0.0, 0.125, 0.0]
+    st["velocity"][1] = 0.0
+    st["angular_velocity"][1] = 0.0
+    ctx = runtime().Context(sc)
+    ctx.set_state(st)
+    ow = refcpu.OracleWorld(sc)
+    ow.set_state(st)
+    x = np.zeros(6 * sc.n_bodies)
+    x.reshape(-1, 6)[:, :3] = st["position"]
+    dx = np.zeros_like(x)
+    dx[6 + 5] = np.pi / 2
+    ag, ng = ctx.ipc_max_step(x, dx, 0.1)
+    ao, no = ow.ipc_max_step(x, dx, 0.1)
+    assert ng == no and ag == ao and 0.1 < ag < 0.19, (ag, ao)

@@ -282,3 +282,35 @@ def test_oracle_barrier_gradient_exact_under_large_rotation_vectors():
         xm[i] -= h
         fd = (ow.ipc_barrier(xp, dhat, kappa, hessian=False)[0] - ow.ipc_barrier(xm, dhat, kappa, hessian=False)[0]) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 * max(abs(g).max(), 1e-12), (i, fd, g[i])
+
+
+def test_accd_follows_the_rotation_arc():
+    # A 0.2 m cube 25 mm above the ground turned by 90 degrees about the
+    # horizontal z axis: both end poses are clear of the ground, and
+    # so are the chords between them, but half-way the bottom corners swing
+    # 16 mm below the ground's top face.  The step bound follows the rigid
+    # arc x + t dx, so it stops before the corners get there (first contact
+    # of the arc at t = 0.19), with every pose on [0, t] clear.
+    sc = scenes.ipc_drop(n_cubes=1)
+    ow = refcpu.OracleWorld(sc)
+    st = sc.initial_state()
+    st["orientation"][1] = [1.0, 0.0, 0.0, 0.0]
+    st["position"][1] = [0.0, 0.125, 0.0]
+    st["velocity"][1] = 0.0
+    st["angular_velocity"][1] = 0.0
+    ow.set_state(st)
+    n = 6 * sc.n_bodies
+    x = np.zeros(n)
+    x.reshape(-1, 6)[:, :3] = st["position"]
+    dx = np.zeros(n)
+    dx[6 + 5] = np.pi / 2
+    alpha, npairs = ow.ipc_max_step(x, dx, 0.1)
+    assert npairs > 0 and 0.1 < alpha < 0.19, alpha
+    lowest = []
+    for t in np.linspace(0.0, alpha, 200):
+        wv, _ = ow.world_vertices_at(x + t * dx)
+        lowest.append(wv[8:, 1].min())                      # the cube's vertices (the ground has 8)
+    assert min(lowest) > 0.0
+    # with the chord the end poses and every chord point would pass
+    wv1, _ = ow.world_vertices_at(x + dx)
+    assert wv1[8:, 1].min() > 0.02
