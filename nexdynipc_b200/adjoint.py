@@ -135,6 +135,7 @@ class IpcRollout:
         mass_bar = np.zeros(n)
         inertia_bar = np.zeros((n, 3, 3))
         mu_bar = np.zeros(nj)
+        friction_bar = 0.0
         for seg in range(len(self.checkpoints) - 1, -1, -1):
             t0 = seg * self.k
             t1 = min(self.steps, t0 + self.k)
@@ -152,15 +153,18 @@ class IpcRollout:
                 xbar[:, :3] = pb + vb / dt
                 xbar[:, 3:] = wb / dt + np.einsum("bji,bj->bi", np.array([left_jacobian(a) for a in th]), psib)
                 r = self.adjoint_fn(starts[t], xs, xbar.reshape(-1))
-                pb = -vb / dt + r["phat_bar"]
+                # the start positions enter through p^ = p0 + dt v0 and, with
+                # friction, through the pairs frozen at the step start
+                pb = -vb / dt + r["phat_bar"] + r.get("p0_bar", 0.0)
                 vb = dt * r["phat_bar"]
                 wb = dt * r["thetahat_bar"]
                 psib = np.einsum("bji,bj->bi", np.array([exp_mat(a) for a in th]), psib) + r["phi_bar"]
                 mass_bar += r["mass_bar"]
                 inertia_bar += r["inertia_bar"]
                 mu_bar += r["joint_mu_bar"]
+                friction_bar += r.get("friction_mu_bar", 0.0)
         return {"position": pb, "orientation_tangent": psib, "velocity": vb, "angular_velocity": wb,
-                "mass": mass_bar, "inertia": inertia_bar, "joint_stiffness": mu_bar}
+                "mass": mass_bar, "inertia": inertia_bar, "joint_stiffness": mu_bar, "friction": friction_bar}
 
 
 def with_parameters(scene, velocity=None, mass=None, joint_stiffness=None, angular_velocity=None):

@@ -125,16 +125,81 @@ def quat_tangent_adjoint(q, qbar):
     return 0.5 * (w * qbar[1:] + np.cross(v, qbar[1:]) - qbar[0] * v)
 
 
+def closest_weights(kind: int, typ: int, X):
+    """The DistForm weights w (r = sum_k w_k X_k) of a pair of distance type
+    `typ` (ipc_pair.h's codes) as a differentiable torch function of its
+    four points X (4, 3)."""
+    import torch
+    w = [X.new_zeros(()) for _ in range(4)]
+    one = X.new_ones(())
+    if kind == 0:
+        if typ == 6:
+            e1, e2, q = X[2] - X[1], X[3] - X[1], X[0] - X[1]
+            a, b, c, d, e = e1 @ e1, e1 @ e2, e2 @ e2, e1 @ q, e2 @ q
+            det = a * c - b * b
+            b1, b2 = (c * d - b * e) / det, (a * e - b * d) / det
+            w = [one, -(1.0 - b1 - b2), -b1, -b2]
+        elif typ in (3, 4, 5):
+            i, j = [(1, 2), (2, 3), (3, 1)][typ - 3]
+            ed = X[j] - X[i]
+            t = (X[0] - X[i]) @ ed / (ed @ ed)
+            w[0], w[i], w[j] = one, -(1.0 - t), -t
+        else:
+            w[0], w[typ + 1] = one, -one
+    else:
+        d1, d2, r = X[1] - X[0], X[3] - X[2], X[0] - X[2]
+        if typ == 8:
+            A, B, E, C, F = d1 @ d1, d1 @ d2, d2 @ d2, d1 @ r, d2 @ r
+            sp = (B * F - C * E) / (A * E - B * B)
+            tp = (B * sp + F) / E
+            w = [1.0 - sp, sp, -(1.0 - tp), -tp]
+        elif typ in (4, 5):
+            pb = typ - 2
+            sp = (X[pb] - X[0]) @ d1 / (d1 @ d1)
+            w[0], w[1], w[pb] = 1.0 - sp, sp, -one
+        elif typ in (6, 7):
+            pa = typ - 6
+            tp = (X[pa] - X[2]) @ d2 / (d2 @ d2)
+            w[pa], w[2], w[3] = one, -(1.0 - tp), -tp
+        else:
+            w[typ // 2], w[2 + typ % 2] = one, -one
+    return torch.stack([torch.as_tensor(v, dtype=X.dtype) for v in w])
+
+
+def friction_force(kind, typ, X, Xs, dhat, kappa, mu, eps):
+    """Point forces (12) of the lagged friction of one pair (ipc_pair.h's
+    friction_pair without the |u| < 1e-12 branch) as a torch function of the
+    points X at the iterate and Xs at the lag state (also the step start)."""
+    import torch
+    w = closest_weights(kind, typ, Xs)
+    r = (w[:, None] * Xs).sum(0)
+    s2 = r @ r
+    d = torch.sqrt(s2)
+    n = r / d
+    sh = dhat * dhat
+    b1 = -kappa * (2.0 * (s2 - sh) * torch.log(s2 / sh) + (s2 - sh) ** 2 / s2)
+    lam = -2.0 * d * b1
+    dsum = (w[:, None] * (X - Xs)).sum(0)
+    u = dsum - (dsum @ n) * n
+    s = torch.sqrt(u @ u + eps * eps)
+    h = mu * lam * u / s
+    return (w[:, None] * h[None, :]).reshape(12)
+
+
 class StepAdjoint:
     """Adjoint of one full-IPC step of `scene` (barrier dhat, kappa): fixed
-    joints and bodies only (no other joints, no control forms)."""
+    joints and bodies only (no other joints, no control forms).  With
+    friction mu > 0 (one lagging pass: the pairs frozen at the step start,
+    eps), the frozen quantities' dependence on the start state is included
+    (their derivatives by torch autograd of friction_force)."""
 
-    def __init__(self, scene, dhat: float, kappa: float):
+    def __init__(self, scene, dhat: float, kappa: float, mu: float = 0.0, eps: float = 1e-5):
         jt = np.asarray(scene.joint_type)
         if np.any(jt != abi.NXD_JOINT_FIXED) or len(scene.drive_body_b):
             raise ValueError("the step adjoint supports fixed joints and no control forms")
         self.sc = scene
         self.dhat, self.kappa = dhat, kappa
+        self.mu, self.eps = mu, eps
         self.ow = refcpu.OracleWorld(scene)
         self.vbody, self.fbody, self.fvert, self.ebody, self.evert = self.ow.prim_topology()
 
@@ -181,13 +246,10 @@ class StepAdjoint:
             tt = quat_log(dq)
             Kphi[6 * A + 3:6 * A + 6, 3 * A:3 * A + 3] += mus[j] * right_jacobian_inv(tt)
             Cj.append(np.concatenate([xs[6 * A:6 * A + 3] - jparams[j, :3], xs[6 * A + 3:6 * A + 6] - tt]))
-        for kind, vid, side, bodies in self.pairs(xs):
-            X = wv[vid]
-            ev = refcpu.ipc_pair(kind, X, self.dhat, self.kappa)
-            if not (ev["d2"] < self.dhat ** 2):
-                continue
-            g, H = ev["g"], ev["H_raw"]
-            # E: exact point velocities from body DOFs; F: from q0 rotations
+        def chain_pair(g, H, X, side, bodies):
+            """The pair's exact share of dG/dx (12 x 12) and of dG/dphi
+            (12 x 6) for point forces g and their point Jacobian H, and the
+            point-velocity map E."""
             E = np.zeros((12, 12))
             F = np.zeros((12, 6))
             arms = [X[k] - pos[bodies[side[k]]] for k in range(4)]
@@ -212,11 +274,64 @@ class StepAdjoint:
                     tau += np.cross(arms[k], gk)
                 Kp[6 * sg + 3:6 * sg + 6, 6 * sg + 3:6 * sg + 6] += Jr @ GA @ JL[b] + jr_torque_derivative(th[b], tau)
                 Kf[6 * sg + 3:6 * sg + 6, 3 * sg:3 * sg + 3] += Jr @ GA @ Rth[b]
+            return Kp, Kf, E
+
+        def scatter(Kp, Kf, bodies):
             for si in range(2):
                 for sj in range(2):
                     bi, bj = bodies[si], bodies[sj]
                     K[6 * bi:6 * bi + 6, 6 * bj:6 * bj + 6] += s * Kp[6 * si:6 * si + 6, 6 * sj:6 * sj + 6]
                     Kphi[6 * bi:6 * bi + 6, 3 * bj:3 * bj + 3] += s * Kf[6 * si:6 * si + 6, 3 * sj:3 * sj + 3]
+
+        for kind, vid, side, bodies in self.pairs(xs):
+            X = wv[vid]
+            ev = refcpu.ipc_pair(kind, X, self.dhat, self.kappa)
+            if not (ev["d2"] < self.dhat ** 2):
+                continue
+            Kp, Kf, _ = chain_pair(ev["g"], ev["H_raw"], X, side, bodies)
+            scatter(Kp, Kf, bodies)
+        # lagged friction (one pass): the pairs active at the step start, their
+        # point forces and point Jacobians (with respect to the iterate's
+        # points and to the step-start points, which are the lag state and the
+        # displacements' origin) by autograd; the step-start points move with
+        # the start positions and, on the left, with the orientations
+        Kps = np.zeros((6 * N, 3 * N))     # dG / d(step-start positions)
+        g_mu = np.zeros(6 * N)             # dG / d(mu)
+        if self.mu > 0.0:
+            import torch
+            x_start = np.zeros(6 * N)
+            x_start.reshape(N, 6)[:, :3] = np.asarray(state0["position"])
+            ws, pos_s = self.ow.world_vertices_at(x_start)
+            args = (self.dhat, self.kappa, self.mu, self.eps)
+            for kind, vid, side, bodies in self.pairs(x_start):
+                Xs = ws[vid]
+                ev = refcpu.ipc_pair(kind, Xs, self.dhat, self.kappa)
+                if not (ev["d2"] < self.dhat ** 2):
+                    continue
+                typ = int(ev["type"])
+                Xt = torch.tensor(wv[vid])
+                Xst = torch.tensor(Xs)
+                fn = lambda a, b_: friction_force(kind, typ, a, b_, *args)
+                g = fn(Xt, Xst).detach().numpy()
+                H, Hs = (j.reshape(12, 12).detach().numpy()
+                         for j in torch.autograd.functional.jacobian(fn, (Xt, Xst)))
+                Kp, Kf, E = chain_pair(g, H, wv[vid], side, bodies)
+                scatter(Kp, Kf, bodies)
+                S = np.zeros((12, 12))     # step-start points from (p_A, phi_A, p_B, phi_B)
+                for k in range(4):
+                    sg = side[k]
+                    a_s = Xs[k] - pos_s[bodies[sg]]
+                    S[3 * k:3 * k + 3, 6 * sg:6 * sg + 3] = np.eye(3)
+                    S[3 * k:3 * k + 3, 6 * sg + 3:6 * sg + 6] = -skew(a_s)
+                Ks = E.T @ Hs @ S
+                Gm = E.T @ g / self.mu
+                for si in range(2):
+                    bi = bodies[si]
+                    g_mu[6 * bi:6 * bi + 6] += s * Gm[6 * si:6 * si + 6]
+                    for sj in range(2):
+                        bj = bodies[sj]
+                        Kps[6 * bi:6 * bi + 6, 3 * bj:3 * bj + 3] += s * Ks[6 * si:6 * si + 6, 6 * sj:6 * sj + 3]
+                        Kphi[6 * bi:6 * bi + 6, 3 * bj:3 * bj + 3] += s * Ks[6 * si:6 * si + 6, 6 * sj + 3:6 * sj + 6]
         lam = np.linalg.solve(K.T, np.asarray(xbar, dtype=np.float64))
         L = lam.reshape(N, 6)
         p0, v0, w0 = (np.asarray(state0[k]) for k in ("position", "velocity", "angular_velocity"))
@@ -229,5 +344,7 @@ class StepAdjoint:
                "phi_bar": -(Kphi.T @ lam).reshape(N, 3),
                "mass_bar": -np.einsum("bi,bi->b", L[:, :3], (xp - phat) - s * GRAVITY[None, :] * 1.0),
                "inertia_bar": -np.einsum("bi,bj->bij", L[:, 3:], xt - that),
-               "joint_mu_bar": np.array([-L[int(sc.joint_body_a[j])] @ Cj[j] for j in range(len(sc.joint_type))])}
+               "joint_mu_bar": np.array([-L[int(sc.joint_body_a[j])] @ Cj[j] for j in range(len(sc.joint_type))]),
+               "p0_bar": -(Kps.T @ lam).reshape(N, 3), "Kps": Kps, "g_mu": g_mu,
+               "friction_mu_bar": float(-(lam @ g_mu))}
         return out

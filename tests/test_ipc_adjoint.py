@@ -153,3 +153,127 @@ def test_step_jacobian_matches_finite_differences_of_the_gradient():
         assert np.abs(K - Kfd).max() <= 1e-6 * np.abs(K).max(), np.abs(K - Kfd).max()
         done += 1
     assert done == 3
+
+
+# --- lagged friction (one pass: the pairs frozen at the step start) ---------
+
+MU, EPS = 0.4, 1e-5
+
+
+def params_f(mu=MU):
+    return abi.ipc_params(dhat=1e-3, kappa=1e9, eta=0.1, newton_tol=1e-12, newton_max_iters=100, ls_max_iters=40,
+                          mu=mu, friction_eps=EPS, friction_iters=1)
+
+
+def step_gradient_fric(sc, st0, x, mu=MU):
+    """step_gradient plus the oracle's friction gradient of the pairs frozen
+    at the start state's pose (nxo_ipc_friction with x_lag = that pose)."""
+    n = sc.n_bodies
+    ow = refcpu.OracleWorld(sc)
+    ow.set_state(st0)
+    xl = np.zeros(6 * n)
+    xl.reshape(n, 6)[:, :3] = st0["position"]
+    _, gf, _, nf = ow.ipc_friction(xl, x, PARAMS.dhat, PARAMS.kappa, mu, EPS, hessian=False)
+    return step_gradient(sc, st0, x) + sc.dt * sc.dt * gf, nf
+
+
+def left_rotated(q, phi):
+    a = np.linalg.norm(phi)
+    dq = np.concatenate([[np.cos(a / 2)], np.sin(a / 2) * phi / a])
+    return cpu_adj.quat_mul(dq, q)
+
+
+def test_friction_step_jacobian_and_start_state_terms():
+    # with friction the step Jacobian K is still the exact derivative of G
+    # (central differences at converged iterates), and the start state's
+    # position and orientation enter G through the frozen pairs as the
+    # adjoint's Kps / Kphi say: d G / d p0 = -m I + Kps, d G / d phi = Kphi
+    sc = scenes.diff_ipc_scene(n_spheres=4)
+    ow = refcpu.OracleWorld(sc)
+    adj = cpu_adj.StepAdjoint(sc, PARAMS.dhat, PARAMS.kappa, mu=MU, eps=EPS)
+    P = params_f()
+    done = 0
+    for t in range(12):
+        st0 = ow.state()
+        ow.ipc_step(P)
+        if t < 10:
+            continue
+        xs = adjoint.iterate_of(ow.state(), sc.dt)
+        r = adj(st0, xs, np.ones(6 * sc.n_bodies), sc.dt)
+        G, nf = step_gradient_fric(sc, st0, xs)
+        assert nf > 0 and np.abs(G).max() <= 1e-8
+        K = r["K"]
+        h = 1e-8
+        Kfd = np.zeros_like(K)
+        for j in range(len(xs)):
+            xp, xm = xs.copy(), xs.copy()
+            xp[j] += h
+            xm[j] -= h
+            Kfd[:, j] = (step_gradient_fric(sc, st0, xp)[0] - step_gradient_fric(sc, st0, xm)[0]) / (2 * h)
+        assert np.abs(K - Kfd).max() <= 1e-6 * np.abs(K).max(), np.abs(K - Kfd).max()
+        n = sc.n_bodies
+        for b in range(1, n):
+            for k in range(3):
+                sp, sm = {kk: np.array(v, copy=True) for kk, v in st0.items()}, {kk: np.array(v, copy=True) for kk, v in st0.items()}
+                sp["position"][b, k] += h
+                sm["position"][b, k] -= h
+                col = (step_gradient_fric(sc, sp, xs)[0] - step_gradient_fric(sc, sm, xs)[0]) / (2 * h)
+                want = r["Kps"][:, 3 * b + k].copy()
+                want[6 * b + k] -= sc.mass[b]
+                assert np.abs(col - want).max() <= 1e-6 * np.abs(K).max(), (b, k, np.abs(col - want).max())
+                e = np.zeros(3)
+                e[k] = 1.0
+                sp = {kk: np.array(v, copy=True) for kk, v in st0.items()}
+                sm = {kk: np.array(v, copy=True) for kk, v in st0.items()}
+                sp["orientation"][b] = left_rotated(st0["orientation"][b], h * e)
+                sm["orientation"][b] = left_rotated(st0["orientation"][b], -h * e)
+                col = (step_gradient_fric(sc, sp, xs)[0] - step_gradient_fric(sc, sm, xs)[0]) / (2 * h)
+                assert np.abs(col - r["Kphi"][:, 3 * b + k]).max() <= 1e-6 * np.abs(K).max(), (b, k)
+        # d G / d mu
+        gp = step_gradient_fric(sc, st0, xs, MU * (1 + 1e-6))[0]
+        gm = step_gradient_fric(sc, st0, xs, MU * (1 - 1e-6))[0]
+        assert np.abs((gp - gm) / (2e-6 * MU) - r["g_mu"]).max() <= 1e-6 * np.abs(r["g_mu"]).max()
+        done += 1
+    assert done == 2
+
+
+def test_friction_rollout_adjoint_matches_finite_differences():
+    # the rollout gradient with friction: initial velocities and the friction
+    # coefficient against central differences of the oracle's rollout
+    sc = small_scene()
+    steps = 8
+    P = params_f()
+    rng = np.random.default_rng(2)
+    ow = refcpu.OracleWorld(sc)
+    for _ in range(steps):
+        ow.ipc_step(P)
+    T = ow.state()
+    tgt_p = T["position"] + rng.normal(0, 0.01, T["position"].shape)
+    tgt_q = T["orientation"] + rng.normal(0, 0.01, T["orientation"].shape)
+
+    def rollout(scn, mu):
+        o = refcpu.OracleWorld(scn)
+        for _ in range(steps):
+            o.ipc_step(params_f(mu))
+        S = o.state()
+        return float(((S["position"] - tgt_p) ** 2).sum() + ((S["orientation"] - tgt_q) ** 2).sum())
+
+    adj = cpu_adj.StepAdjoint(sc, PARAMS.dhat, PARAMS.kappa, mu=MU, eps=EPS)
+    r = adjoint.IpcRollout(sc, P, checkpoint_every=3, ctx=refcpu.OracleWorld(sc),
+                           adjoint_fn=lambda st, xs, xb: adj(st, xs, xb, sc.dt))
+    T = r.forward(steps)
+    g = r.backward(2 * (T["position"] - tgt_p), 2 * (T["orientation"] - tgt_q))
+    h = 1e-4
+    checks = []
+    for b, k in ((1, 0), (2, 2), (3, 0)):
+        vp, vm = sc.velocity.copy(), sc.velocity.copy()
+        vp[b, k] += h
+        vm[b, k] -= h
+        fd = (rollout(adjoint.with_parameters(sc, velocity=vp), MU) - rollout(adjoint.with_parameters(sc, velocity=vm), MU)) / (2 * h)
+        checks.append((g["velocity"][b, k], fd))
+    hm = h * MU
+    fd_mu = (rollout(sc, MU + hm) - rollout(sc, MU - hm)) / (2 * hm)
+    checks.append((g["friction"], fd_mu))
+    a = np.array(checks)
+    scale = np.abs(a[:, 1]).max()
+    assert np.abs(a[:, 0] - a[:, 1]).max() <= 1e-4 * scale, a
