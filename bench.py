@@ -457,7 +457,8 @@ def ipc_step_leg(n_cubes: int = 8, columns: int = 1, settle: int = 30, steps: in
         workload = (f"{n_cubes} tilted 0.2 m cubes in {columns} stack(s) on a ground box, dhat 1e-3, "
                     f"kappa 1e11, dt {sc.dt}; steps {settle + 1}-{settle + steps}")
     return {"workload": workload,
-            "steps": steps, "steps_per_s": steps / wall, "newton_iterations_mean": float(np.mean(its)),
+            "steps": steps, "steps_per_s": steps / wall, "steps_per_s_median": 1.0 / float(np.median(walls)),
+            "newton_iterations_mean": float(np.mean(its)),
             "active_pairs_mean": float(np.mean(act)), "candidate_pairs_mean": float(np.mean(pairs)),
             "converged_steps": conv, "line_search_failures": lsf, "friction_pairs_last": int(st["n_friction"]),
             "step_ms": [round(1e3 * w, 3) for w in walls[:4]],

@@ -510,6 +510,12 @@ nxd_status nxd_ipc_step(nxd_ctx* ctx, double dt, const nxd_ipc_params* p, nxd_ip
  * input state (host arrays); the context is left at that state.  Supported:
  * bodies, fixed joints (FixedJoint), no control forms, implicit Euler,
  * N <= 128 bodies (dense K, one CTA); else NXD_INVALID_ARGUMENT.
+ * Friction (p->mu > 0) with one lagging pass (friction_iters = 1): the pairs
+ * frozen at the step start enter K, and, through their frozen normal
+ * forces, normals, closest-point weights and displacement origin, the
+ * step-start positions (p0_bar, added to what reaches p0 through the
+ * predicted position) and orientations (phi_bar); friction_mu_bar is the
+ * coefficient's adjoint.  More lagging passes: NXD_INVALID_ARGUMENT.
  * NXD_FACTOR_FAILED if K is singular.  Output pointers are host arrays and
  * may be NULL. */
 typedef struct nxd_ipc_adjoint_out {
@@ -521,6 +527,9 @@ typedef struct nxd_ipc_adjoint_out {
     double* inertia_bar;        /* [9N] */
     double* joint_mu_bar;       /* [J]  */
     int32_t* n_active;          /* active pairs at x_star (may be NULL) */
+    double* p0_bar;             /* [3N] step-start positions through the frozen
+                                   friction pairs (mu > 0; may be NULL)     */
+    double* friction_mu_bar;    /* [1]  the friction coefficient (may be NULL) */
 } nxd_ipc_adjoint_out;
 nxd_status nxd_ipc_adjoint(nxd_ctx* ctx, double dt, const nxd_ipc_params* p, const nxd_state* start,
                            const double* x_star, const double* x_bar, const nxd_ipc_adjoint_out* out);

@@ -221,6 +221,8 @@ class NxdIpcAdjointOut(C.Structure):
         ("inertia_bar", _dp),
         ("joint_mu_bar", _dp),
         ("n_active", C.POINTER(C.c_int32)),
+        ("p0_bar", _dp),
+        ("friction_mu_bar", _dp),
     ]
 
 

@@ -51,13 +51,28 @@ struct AdjIn {
     double s;                                           // barrier / gravity scale dt^2
 };
 
-// K^T (n x n) and K_phi (n x 3N), n = 6N; the pairs' blocks in pair order.
+// The frozen friction pairs' blocks (k_fric_pair_adjoint), when the step
+// has friction: kp / kf like the barrier's, ks on the step-start positions
+// and orientations, gm on mu.
+struct AdjFric {
+    int n;
+    const int* body; const double* kp; const double* kf; const double* ks; const double* gm;
+    double* Kps;    // [n6 x 3N] dG / d(step-start positions)
+    double* gmu;    // [n6]      dG / d(mu)
+};
+
+// K^T (n x n) and K_phi (n x 3N), n = 6N; the pairs' blocks in pair order,
+// then the friction pairs' in frozen order.
 __global__ void __launch_bounds__(kAdjThreads) k_adj_assemble(AdjIn a, const int* pair_body, const int* pair_active,
                                                               const double* kp, const double* kf, int n_pairs, double* Kt,
-                                                              double* Kphi) {
+                                                              double* Kphi, AdjFric fr) {
     const int n = 6 * a.N, m3 = 3 * a.N;
     for (long long e = threadIdx.x; e < (long long)n * n; e += blockDim.x) Kt[e] = 0.0;
     for (long long e = threadIdx.x; e < (long long)n * m3; e += blockDim.x) Kphi[e] = 0.0;
+    if (fr.n) {
+        for (long long e = threadIdx.x; e < (long long)n * m3; e += blockDim.x) fr.Kps[e] = 0.0;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) fr.gmu[e] = 0.0;
+    }
     __syncthreads();
     // inertia: K[p][p] = m I, K[theta][theta] = I_body (K^T holds its transpose)
     for (int b = threadIdx.x; b < a.N; b += blockDim.x) {
@@ -98,6 +113,32 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_assemble(AdjIn a, const int
             const int u = t - 144, r = u / 6, c = u % 6;
             const int gr = 6 * bd[r / 6] + r % 6, gc = 3 * bd[c / 3] + c % 3;
             Kphi[(size_t)gr * m3 + gc] += a.s * kf[72 * (size_t)p + u];
+        }
+        __syncthreads();
+    }
+    for (int f = 0; f < fr.n; ++f) {
+        const int bd[2] = {fr.body[2 * f], fr.body[2 * f + 1]};
+        const int t = threadIdx.x;
+        if (t < 144) {
+            const int r = t / 12, c = t % 12;
+            const int gr = 6 * bd[r / 6] + r % 6, gc = 6 * bd[c / 6] + c % 6;
+            Kt[(size_t)gc * n + gr] += a.s * fr.kp[144 * (size_t)f + t];
+        } else if (t < 216) {
+            const int u = t - 144, r = u / 6, c = u % 6;
+            const int gr = 6 * bd[r / 6] + r % 6, gc = 3 * bd[c / 3] + c % 3;
+            Kphi[(size_t)gr * m3 + gc] += a.s * fr.kf[72 * (size_t)f + u];
+        } else if (t < 228) {
+            const int r = t - 216;
+            fr.gmu[6 * bd[r / 6] + r % 6] += a.s * fr.gm[12 * (size_t)f + r];
+        }
+        __syncthreads();
+        // ks columns (p_A, phi_A, p_B, phi_B): positions to Kps, orientations
+        // to K_phi after kf's share of the same entries (no two threads on one)
+        if (t < 144) {
+            const int r = t / 12, c = t % 12;
+            const int gr = 6 * bd[r / 6] + r % 6, cb = 3 * bd[c / 6] + c % 3;
+            if (c % 6 < 3) fr.Kps[(size_t)gr * m3 + cb] += a.s * fr.ks[144 * (size_t)f + t];
+            else Kphi[(size_t)gr * m3 + cb] += a.s * fr.ks[144 * (size_t)f + t];
         }
         __syncthreads();
     }
@@ -186,15 +227,27 @@ struct AdjOut {
     double* mass_bar;       // [N]
     double* inertia_bar;    // [9N]  -lambda_theta (theta - theta^)^T
     double* joint_mu_bar;   // [J]   -lambda_A . C
+    double* p0_bar;         // [3N]  -(K_ps^T lambda) (friction)
+    double* friction_mu_bar;// [1]   -lambda . dG/dmu (friction)
 };
 
-__global__ void k_adj_cross(AdjIn a, const double* lam, const double* Kphi, AdjOut o) {
+__global__ void k_adj_cross(AdjIn a, const double* lam, const double* Kphi, AdjOut o, AdjFric fr) {
     const int n = 6 * a.N, m3 = 3 * a.N;
     const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
     for (int c = gt; c < m3; c += gs) {
         double acc = 0.0;
         for (int r = 0; r < n; ++r) acc += Kphi[(size_t)r * m3 + c] * lam[r];
         o.phi_bar[c] = -acc;
+        double ap = 0.0;
+        if (fr.n)
+            for (int r = 0; r < n; ++r) ap += fr.Kps[(size_t)r * m3 + c] * lam[r];
+        o.p0_bar[c] = -ap;
+    }
+    if (gt == 0) {
+        double acc = 0.0;
+        if (fr.n)
+            for (int r = 0; r < n; ++r) acc += fr.gmu[r] * lam[r];
+        *o.friction_mu_bar = -acc;
     }
     for (int b = gt; b < a.N; b += gs) {
         const double* L = lam + 6 * b;

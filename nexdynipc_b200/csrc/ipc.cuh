@@ -643,6 +643,76 @@ __global__ void k_iota(int* list, const int* at, int base, int n) {
 // Q = J_r (sum_k [g_k]x [a_k]x) J_l + d(J_r tau)/dtheta and Q_phi =
 // J_r (sum_k [g_k]x [a_k]x) Exp(theta) on each body's own rotation block.
 // Unscaled (the step scales the barrier by s); inactive pairs flagged 0.
+// The pair's share of dG/dx (KP, 12 x 12) and dG/dphi (KF, 12 x 6) for
+// point forces g12 with point Jacobian H (row 3k+i, column 3l+j), points of
+// bodies side[k] at arms arm[k], body rotations th; E (12 x 12) receives the
+// point-velocity map [I, -[a]x J_l(theta)].
+__device__ void pair_adjoint_blocks(const double* g12, const double* H, const int* side, const V3* arm, const V3* th,
+                                    double* KP, double* KF, double* E) {
+    double R[2][9], Jl[2][9];
+    for (int sd = 0; sd < 2; ++sd) ipc::rot_exp_mats(th[sd], R[sd], Jl[sd]);
+    double F[72];
+    for (int e = 0; e < 144; ++e) E[e] = 0.0;
+    for (int e = 0; e < 72; ++e) F[e] = 0.0;
+    for (int k = 0; k < 4; ++k) {
+        const int sg = side[k];
+        double A[9], D[9], Fk[9];
+        ipc::m3_skew(arm[k], A);
+        ipc::m3_mul(A, Jl[sg], D);
+        ipc::m3_mul(A, R[sg], Fk);
+        for (int i = 0; i < 3; ++i) {
+            E[12 * (3 * k + i) + 6 * sg + i] = 1.0;
+            for (int j = 0; j < 3; ++j) {
+                E[12 * (3 * k + i) + 6 * sg + 3 + j] = -D[3 * i + j];
+                F[6 * (3 * k + i) + 3 * sg + j] = -Fk[3 * i + j];
+            }
+        }
+    }
+    for (int r = 0; r < 12; ++r) {
+        double he[12], hf[6];
+        for (int c = 0; c < 12; ++c) he[c] = 0.0;
+        for (int c = 0; c < 6; ++c) hf[c] = 0.0;
+        // rows of E^T H: sum_i E[i][r] H[i][.]
+        for (int i = 0; i < 12; ++i) {
+            const double eir = E[12 * i + r];
+            if (eir == 0.0) continue;
+            for (int j = 0; j < 12; ++j) {
+                const double t = eir * H[12 * i + j];
+                for (int c = 0; c < 12; ++c) he[c] += t * E[12 * j + c];
+                for (int c = 0; c < 6; ++c) hf[c] += t * F[6 * j + c];
+            }
+        }
+        for (int c = 0; c < 12; ++c) KP[12 * r + c] = he[c];
+        for (int c = 0; c < 6; ++c) KF[6 * r + c] = hf[c];
+    }
+    for (int sg = 0; sg < 2; ++sg) {
+        double GA[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        V3 tau = v3(0, 0, 0);
+        for (int k = 0; k < 4; ++k) {
+            if (side[k] != sg) continue;
+            const V3 gk = v3(g12[3 * k], g12[3 * k + 1], g12[3 * k + 2]);
+            double SG[9], SA[9], P9[9];
+            ipc::m3_skew(gk, SG);
+            ipc::m3_skew(arm[k], SA);
+            ipc::m3_mul(SG, SA, P9);
+            for (int e = 0; e < 9; ++e) GA[e] += P9[e];
+            tau = tau + cross(arm[k], gk);
+        }
+        double Jr[9], T1[9], Q[9], QF[9], M[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) Jr[3 * i + j] = Jl[sg][3 * j + i];
+        ipc::m3_mul(Jr, GA, T1);
+        ipc::m3_mul(T1, Jl[sg], Q);
+        ipc::m3_mul(T1, R[sg], QF);
+        ipc::jr_torque_derivative(th[sg], tau, M);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                KP[12 * (6 * sg + 3 + i) + 6 * sg + 3 + j] += Q[3 * i + j] + M[3 * i + j];
+                KF[6 * (6 * sg + 3 + i) + 3 * sg + j] += QF[3 * i + j];
+            }
+    }
+}
+
 __global__ void k_ipc_pair_adjoint(PrimGeo pg, IpcPairs P, IpcPose ps, double dhat, double kappa, double* kp, double* kf,
                                    int* body, int* active) {
     const int n = P.n_pt + P.n_ee;
@@ -658,69 +728,69 @@ __global__ void k_ipc_pair_adjoint(PrimGeo pg, IpcPairs P, IpcPose ps, double dh
         active[p] = act ? 1 : 0;
         if (!act) continue;
         const V3 th[2] = {pose_theta(ps, bA), pose_theta(ps, bB)};
-        double R[2][9], Jl[2][9];
-        for (int sd = 0; sd < 2; ++sd) ipc::rot_exp_mats(th[sd], R[sd], Jl[sd]);
-        double E[144], F[72];
-        for (int e = 0; e < 144; ++e) E[e] = 0.0;
-        for (int e = 0; e < 72; ++e) F[e] = 0.0;
+        double E[144];
+        pair_adjoint_blocks(g12, H, side, arm, th, kp + 144 * (size_t)p, kf + 72 * (size_t)p, E);
+    }
+}
+
+// Step adjoint of the lagged friction, per frozen pair at the converged
+// iterate: kp / kf as for the barrier (ipc::friction_derivs' point forces
+// and H), ks (12 x 12, columns p_A, phi_A, p_B, phi_B) = E^T Hs S with S the
+// step-start points' derivatives ([I, -[a_s]x] per point, a_s the
+// step-start arm: the lag state moves with the start positions and, on the
+// left, orientations) and gm (12) = E^T F / mu, the derivative in mu.
+// Unscaled; the frozen set and its step-start points as the step built them.
+__global__ void k_fric_pair_adjoint(IpcFric Fz, IpcPose ps, const double* pos0, double dhat, double kappa, double mu,
+                                    double eps, double* kp, double* kf, double* ks, double* gm, int* body) {
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < Fz.n; f += gridDim.x * blockDim.x) {
+        int side[4];
+        const int bA = Fz.body[2 * f], bB = Fz.body[2 * f + 1];
+        const int kind = Fz.kind[f];
+        fric_sides(kind, side);
+        V3 X[4], Xs[4], arm[4], arm_s[4];
+        const int b[2] = {bA, bB};
+        for (int k = 0; k < 4; ++k) {
+            const int v = Fz.vid[4 * f + k];
+            X[k] = ld3(ps.wq + 3 * v);
+            Xs[k] = ld3(Fz.x0 + 3 * v);
+            arm[k] = X[k] - ld3(ps.pp + 3 * b[side[k]]);
+            arm_s[k] = Xs[k] - ld3(pos0 + 3 * b[side[k]]);
+        }
+        const ipc::DistForm fs = ipc::classify(kind, Xs);
+        double g12[12], H[144], Hs[144];
+        ipc::friction_derivs(fs, X, Xs, dhat, kappa, mu, eps, g12, H, Hs);
+        body[2 * f] = bA; body[2 * f + 1] = bB;
+        const V3 th[2] = {pose_theta(ps, bA), pose_theta(ps, bB)};
+        double E[144];
+        pair_adjoint_blocks(g12, H, side, arm, th, kp + 144 * (size_t)f, kf + 72 * (size_t)f, E);
+        // S: step-start points from (p_A, phi_A, p_B, phi_B)
+        double S[144];
+        for (int e = 0; e < 144; ++e) S[e] = 0.0;
         for (int k = 0; k < 4; ++k) {
             const int sg = side[k];
-            double A[9], D[9], Fk[9];
-            ipc::m3_skew(arm[k], A);
-            ipc::m3_mul(A, Jl[sg], D);
-            ipc::m3_mul(A, R[sg], Fk);
+            double A[9];
+            ipc::m3_skew(arm_s[k], A);
             for (int i = 0; i < 3; ++i) {
-                E[12 * (3 * k + i) + 6 * sg + i] = 1.0;
-                for (int j = 0; j < 3; ++j) {
-                    E[12 * (3 * k + i) + 6 * sg + 3 + j] = -D[3 * i + j];
-                    F[6 * (3 * k + i) + 3 * sg + j] = -Fk[3 * i + j];
-                }
+                S[12 * (3 * k + i) + 6 * sg + i] = 1.0;
+                for (int j = 0; j < 3; ++j) S[12 * (3 * k + i) + 6 * sg + 3 + j] = -A[3 * i + j];
             }
         }
-        double* KP = kp + 144 * (size_t)p;
-        double* KF = kf + 72 * (size_t)p;
+        double* KS = ks + 144 * (size_t)f;
         for (int r = 0; r < 12; ++r) {
-            double he[12], hf[6];
-            for (int c = 0; c < 12; ++c) he[c] = 0.0;
-            for (int c = 0; c < 6; ++c) hf[c] = 0.0;
-            // rows of E^T H: sum_i E[i][r] H[i][.]
+            double hs[12];
+            for (int c = 0; c < 12; ++c) hs[c] = 0.0;
             for (int i = 0; i < 12; ++i) {
                 const double eir = E[12 * i + r];
                 if (eir == 0.0) continue;
                 for (int j = 0; j < 12; ++j) {
-                    const double t = eir * H[12 * i + j];
-                    for (int c = 0; c < 12; ++c) he[c] += t * E[12 * j + c];
-                    for (int c = 0; c < 6; ++c) hf[c] += t * F[6 * j + c];
+                    const double t = eir * Hs[12 * i + j];
+                    for (int c = 0; c < 12; ++c) hs[c] += t * S[12 * j + c];
                 }
             }
-            for (int c = 0; c < 12; ++c) KP[12 * r + c] = he[c];
-            for (int c = 0; c < 6; ++c) KF[6 * r + c] = hf[c];
-        }
-        for (int sg = 0; sg < 2; ++sg) {
-            double GA[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-            V3 tau = v3(0, 0, 0);
-            for (int k = 0; k < 4; ++k) {
-                if (side[k] != sg) continue;
-                const V3 gk = v3(g12[3 * k], g12[3 * k + 1], g12[3 * k + 2]);
-                double SG[9], SA[9], P9[9];
-                ipc::m3_skew(gk, SG);
-                ipc::m3_skew(arm[k], SA);
-                ipc::m3_mul(SG, SA, P9);
-                for (int e = 0; e < 9; ++e) GA[e] += P9[e];
-                tau = tau + cross(arm[k], gk);
-            }
-            double Jr[9], T1[9], Q[9], QF[9], M[9];
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) Jr[3 * i + j] = Jl[sg][3 * j + i];
-            ipc::m3_mul(Jr, GA, T1);
-            ipc::m3_mul(T1, Jl[sg], Q);
-            ipc::m3_mul(T1, R[sg], QF);
-            ipc::jr_torque_derivative(th[sg], tau, M);
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) {
-                    KP[12 * (6 * sg + 3 + i) + 6 * sg + 3 + j] += Q[3 * i + j] + M[3 * i + j];
-                    KF[6 * (6 * sg + 3 + i) + 3 * sg + j] += QF[3 * i + j];
-                }
+            for (int c = 0; c < 12; ++c) KS[12 * r + c] = hs[c];
+            double gr = 0.0;
+            for (int i = 0; i < 12; ++i) gr += E[12 * i + r] * g12[i];
+            gm[12 * (size_t)f + r] = gr / mu;
         }
     }
 }

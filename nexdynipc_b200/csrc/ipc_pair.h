@@ -507,6 +507,90 @@ NX_HD FricEval friction_pair(const FricLag& L, const V3* X, const V3* X0, double
     return o;
 }
 
+// Derivatives of one frozen pair's friction point forces F_k = w_k h,
+// h = mu lam u / s (friction_pair; g12 keeps its |u| < 1e-12 branch) for the
+// step adjoint, lagged at the step-start points Xs (the lag state and the
+// displacements' origin; fs = classify(kind, Xs)):
+//   H  = dF/dX   (12 x 12, row 3k+i, column 3l+j): w_k w_l mu lam / s (P - u u^T / s^2),
+//   Hs = dF/dXs  (12 x 12): through the explicit -Xs in u and through the
+//        frozen weights, normal and normal force, whose derivatives follow
+//        from the DistForm (du* = -g_uu^-1 g_uX dXs, dw = c du*, dr = A du* +
+//        sum_k w_k dXs_k, dn = (I - n n^T) dr / d, dlam = (-2 b' - 4 d^2 b'') n.dr).
+NX_HD void friction_derivs(const DistForm& fs, const V3* X, const V3* Xs, double dhat, double kappa, double mu, double eps,
+                           double* g12, double* H, double* Hs) {
+    const V3 r = form_r(fs, Xs);
+    const double s2 = dot(r, r), sh = dhat * dhat, ds = sqrt(s2);
+    const V3 n = v3(r.x / ds, r.y / ds, r.z / ds);
+    const double b1 = barrier_s1(s2, sh, kappa), b2 = barrier_s2(s2, sh, kappa);
+    const double lam = -2.0 * ds * b1;
+    const double dlam_dd = -2.0 * b1 - 4.0 * s2 * b2;
+    V3 dX[4];
+    V3 dsum = v3(0.0, 0.0, 0.0);
+    for (int k = 0; k < 4; ++k) {
+        dX[k] = X[k] - Xs[k];
+        dsum = dsum + fs.w[k] * dX[k];
+    }
+    const V3 u = dsum - dot(dsum, n) * n;
+    const double uu = dot(u, u), s = sqrt(uu + eps * eps), ml = mu * lam;
+    const V3 h = (ml / s) * u;
+    const bool still = sqrt(uu) < 1e-12;
+    for (int k = 0; k < 4; ++k) {
+        const V3 f = still ? v3(0.0, 0.0, 0.0) : fs.w[k] * h;
+        g12[3 * k] = f.x; g12[3 * k + 1] = f.y; g12[3 * k + 2] = f.z;
+    }
+    // M = dh/du (3 x 3) and M P
+    double M[9], MP[9];
+    const double cu = ml / s, cs = 1.0 / (s * s);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            const double ui = get(u, i), uj = get(u, j), ni = get(n, i), nj = get(n, j);
+            M[3 * i + j] = cu * ((i == j ? 1.0 : 0.0) - ui * uj * cs);
+            MP[3 * i + j] = cu * ((i == j ? 1.0 : 0.0) - ni * nj - ui * uj * cs);
+        }
+    for (int k = 0; k < 4; ++k)
+        for (int l = 0; l < 4; ++l)
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) H[12 * (3 * k + i) + 3 * l + j] = (fs.w[k] * fs.w[l]) * MP[3 * i + j];
+    // the DistForm's parameter system at Xs
+    V3 a[2] = {v3(0, 0, 0), v3(0, 0, 0)};
+    for (int m = 0; m < fs.nu; ++m) a[m] = fs.c[0][m] * Xs[0] + fs.c[1][m] * Xs[1] + fs.c[2][m] * Xs[2] + fs.c[3][m] * Xs[3];
+    double G[2][2] = {{0, 0}, {0, 0}}, Gi[2][2] = {{0, 0}, {0, 0}};
+    for (int i = 0; i < fs.nu; ++i)
+        for (int j = 0; j < fs.nu; ++j) G[i][j] = 2.0 * dot(a[i], a[j]);
+    if (fs.nu == 1) Gi[0][0] = 1.0 / G[0][0];
+    if (fs.nu == 2) {
+        const double det = G[0][0] * G[1][1] - G[0][1] * G[1][0];
+        Gi[0][0] = G[1][1] / det; Gi[1][1] = G[0][0] / det; Gi[0][1] = -G[0][1] / det; Gi[1][0] = -G[1][0] / det;
+    }
+    for (int j = 0; j < 4; ++j)
+        for (int ax = 0; ax < 3; ++ax) {
+            V3 e = v3(0.0, 0.0, 0.0);
+            if (ax == 0) e.x = 1.0; else if (ax == 1) e.y = 1.0; else e.z = 1.0;
+            double du[2] = {0.0, 0.0};
+            for (int m = 0; m < fs.nu; ++m)
+                for (int q = 0; q < fs.nu; ++q)
+                    du[m] -= Gi[m][q] * (2.0 * (fs.w[j] * get(a[q], ax) + fs.c[j][q] * get(r, ax)));
+            double dw[4];
+            for (int k = 0; k < 4; ++k) dw[k] = fs.c[k][0] * du[0] + fs.c[k][1] * du[1];
+            const V3 dr = du[0] * a[0] + du[1] * a[1] + fs.w[j] * e;
+            const double dd = dot(n, dr);
+            const V3 dn = (1.0 / ds) * (dr - dd * n);
+            const double dlam = dlam_dd * dd;
+            V3 dds = (-fs.w[j]) * e;
+            for (int k = 0; k < 4; ++k) dds = dds + dw[k] * dX[k];
+            const V3 dU = dds - dot(dds, n) * n - dot(dsum, dn) * n - dot(dsum, n) * dn;
+            V3 dh = ((mu / s) * dlam) * u;
+            dh = dh + v3(M[0] * dU.x + M[1] * dU.y + M[2] * dU.z, M[3] * dU.x + M[4] * dU.y + M[5] * dU.z,
+                         M[6] * dU.x + M[7] * dU.y + M[8] * dU.z);
+            for (int k = 0; k < 4; ++k) {
+                const V3 dF = dw[k] * h + fs.w[k] * dh;
+                Hs[12 * (3 * k) + 3 * j + ax] = dF.x;
+                Hs[12 * (3 * k + 1) + 3 * j + ax] = dF.y;
+                Hs[12 * (3 * k + 2) + 3 * j + ax] = dF.z;
+            }
+        }
+}
+
 // Rigid chain: point k of the pair belongs to body side[k] (0 = body A,
 // 1 = body B) at lever arm arm[k] = R r_k (world offset from the body's
 // position); its DOF Jacobian is [I3, -[arm]x].  The transposed Jacobian

@@ -1400,6 +1400,7 @@ struct IpcState {
     GrowBuf sflag, spos, sstart, gout, rowptr, colidx, vals, toi;
     // step adjoint: per-pair blocks, dense K^T and K_phi, vectors, outputs
     GrowBuf akp, akf, abody, aact, aK, aKphi, ax, axb, alam, aout, afail;
+    GrowBuf afkp, afkf, afks, afgm, afbody, aKps, agmu;   // its friction pairs (lagged at the step start)
     // full-IPC time step: rest-form and merged BSR, gradients, solve scratch
     GrowBuf rrp, rci, rvv, mrp, mci, mvv, gr, gt, gneg, prod, xt, erow, items, iact, stat;
     PcgScratch pcg;
@@ -1411,7 +1412,8 @@ struct IpcState {
                 &grad12, &lam, &z, &nterm, &body, &active, &type, &apos, &alist, &gkey, &gval, &gkey1, &gval1, &hkey,
                 &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &rrp, &rci, &rvv,
                 &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &akp, &akf, &abody, &aact,
-                &aK, &aKphi, &ax, &axb, &alam, &aout, &afail, &tkey, &tval, &tkey1, &tval1, &qbuf0, &qbuf1, &dxv, &rmax, &pad, &fr_vid, &fr_body, &fr_kind, &fr_w, &fr_nrm, &fr_lam,
+                &aK, &aKphi, &ax, &axb, &alam, &aout, &afail, &tkey, &tval, &tkey1, &tval1, &qbuf0, &qbuf1, &dxv, &rmax, &pad, &afkp, &afkf, &afks, &afgm, &afbody,
+                &aKps, &agmu, &fr_vid, &fr_body, &fr_kind, &fr_w, &fr_nrm, &fr_lam,
                 &fr_x0, &fr_e};
     }
     void release() {
@@ -2189,7 +2191,7 @@ nxd_status nxd_ipc_step(nxd_ctx* c, double dt, const nxd_ipc_params* p, nxd_ipc_
 nxd_status nxd_ipc_adjoint(nxd_ctx* c, double dt, const nxd_ipc_params* p, const nxd_state* start, const double* x_star,
                            const double* x_bar, const nxd_ipc_adjoint_out* out) {
     if (!c || !p || !start || !x_star || !x_bar || !out || !(dt > 0.0) || !(p->dhat > 0.0) || !(p->kappa >= 0.0) ||
-        p->mu != 0.0)
+        !(p->mu >= 0.0) || (p->mu > 0.0 && (!(p->friction_eps > 0.0) || p->friction_iters != 1)))
         return NXD_INVALID_ARGUMENT;
     const int N = c->N, J = c->J, n6 = 6 * N;
     if (N > kAdjMaxBodies || c->D > 0 || c->s.integrator == NXD_INTEGRATOR_IMPLICIT_NEWMARK) return NXD_INVALID_ARGUMENT;
@@ -2209,6 +2211,26 @@ nxd_status nxd_ipc_adjoint(nxd_ctx* c, double dt, const nxd_ipc_params* p, const
     IPC_ENSURE(s->ax, 8 * (size_t)n6); IPC_ENSURE(s->axb, 8 * (size_t)n6); IPC_ENSURE(s->alam, 8 * (size_t)n6);
     NXD_CUDA(cudaMemcpyAsync(s->ax.p, x_star, 8 * (size_t)n6, cudaMemcpyHostToDevice, sm));
     NXD_CUDA(cudaMemcpyAsync(s->axb.p, x_bar, 8 * (size_t)n6, cudaMemcpyHostToDevice, sm));
+    // friction: the pairs frozen at the step start, as the step's single
+    // lagging pass froze them (pose x_prev = (p0, 0), dhat-inflated candidates)
+    struct FricScope {
+        IpcState* s;
+        ~FricScope() { s->fr_n = 0; s->fr_build = false; }
+    } fric_scope{s};
+    const bool friction = p->mu > 0.0;
+    s->fr_n = 0;
+    if (friction) {
+        st = ipc_pose(c, c->xprev, nullptr, true);
+        if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
+        if (st != NXD_OK) return st;
+        IPC_ENSURE(s->fr_x0, 24 * (size_t)std::max(c->nv, 1));
+        NXD_CUDA(cudaMemcpyAsync(s->fr_x0.p, s->wq0.p, 24 * (size_t)c->nv, cudaMemcpyDeviceToDevice, sm));
+        s->fr_build = true;
+        s->fr_mu = p->mu;
+        s->fr_eps = p->friction_eps;
+        if ((st = ipc_barrier_eval(c, p->dhat, p->kappa, true, nullptr)) != NXD_OK) return st;
+    }
+    const int nf = s->fr_n;
     // candidates at x* (boxes inflated by dhat), each pair's exact blocks
     st = ipc_pose(c, s->ax.as<double>(), nullptr, true);
     if (st == NXD_OK) st = ipc_candidates(c, false, p->dhat);
@@ -2217,19 +2239,30 @@ nxd_status nxd_ipc_adjoint(nxd_ctx* c, double dt, const nxd_ipc_params* p, const
     const size_t nn = std::max(np, 1);
     IPC_ENSURE(s->akp, 1152 * nn); IPC_ENSURE(s->akf, 576 * nn); IPC_ENSURE(s->abody, 8 * nn); IPC_ENSURE(s->aact, 4 * nn);
     IPC_ENSURE(s->aK, 8 * (size_t)n6 * n6); IPC_ENSURE(s->aKphi, 8 * (size_t)n6 * 3 * N);
-    IPC_ENSURE(s->aout, 8 * (size_t)(3 * N * 3 + N + 9 * N + std::max(J, 1))); IPC_ENSURE(s->afail, 4);
+    IPC_ENSURE(s->aout, 8 * (size_t)(3 * N * 3 + N + 9 * N + std::max(J, 1) + 3 * N + 1)); IPC_ENSURE(s->afail, 4);
+    const size_t nfn = std::max(nf, 1);
+    IPC_ENSURE(s->afkp, 1152 * nfn); IPC_ENSURE(s->afkf, 576 * nfn); IPC_ENSURE(s->afks, 1152 * nfn);
+    IPC_ENSURE(s->afgm, 96 * nfn); IPC_ENSURE(s->afbody, 8 * nfn);
+    IPC_ENSURE(s->aKps, 8 * (size_t)n6 * 3 * N); IPC_ENSURE(s->agmu, 8 * (size_t)n6);
     const IpcPairs P{s->pt.as<int>(), s->n_pt, s->ee.as<int>(), s->n_ee};
     const IpcPose ps{s->wq0.as<double>(), s->pp0.as<double>(), s->ax.as<double>()};
     if (np) k_ipc_pair_adjoint<<<grid_for(np, 64), 64, 0, sm>>>(s->pg, P, ps, p->dhat, p->kappa, s->akp.as<double>(),
                                                                 s->akf.as<double>(), s->abody.as<int>(), s->aact.as<int>());
+    if (nf)
+        k_fric_pair_adjoint<<<grid_for(nf, 64), 64, 0, sm>>>(s->fric(), ps, c->pos, p->dhat, p->kappa, p->mu,
+                                                             p->friction_eps, s->afkp.as<double>(), s->afkf.as<double>(),
+                                                             s->afks.as<double>(), s->afgm.as<double>(), s->afbody.as<int>());
+    const AdjFric afr{nf, s->afbody.as<int>(), s->afkp.as<double>(), s->afkf.as<double>(), s->afks.as<double>(),
+                      s->afgm.as<double>(), s->aKps.as<double>(), s->agmu.as<double>()};
     AdjIn ai{N, J, c->mass, c->inertia, c->jtype, c->ja, c->jparams, c->jmu, c->quat0, s->ax.as<double>(), c->xhat, dt * dt};
     k_adj_assemble<<<1, kAdjThreads, 0, sm>>>(ai, s->abody.as<int>(), s->aact.as<int>(), s->akp.as<double>(),
-                                              s->akf.as<double>(), np, s->aK.as<double>(), s->aKphi.as<double>());
+                                              s->akf.as<double>(), np, s->aK.as<double>(), s->aKphi.as<double>(), afr);
     k_adj_solve<<<1, kAdjThreads, 0, sm>>>(s->aK.as<double>(), s->axb.as<double>(), n6, s->alam.as<double>(),
                                            s->afail.as<int>());
     double* o = s->aout.as<double>();
-    AdjOut ao{o, o + 3 * N, o + 6 * N, o + 9 * N, o + 10 * N, o + 19 * N};
-    k_adj_cross<<<grid_for(std::max(3 * N, J), 128), 128, 0, sm>>>(ai, s->alam.as<double>(), s->aKphi.as<double>(), ao);
+    AdjOut ao{o, o + 3 * N, o + 6 * N, o + 9 * N, o + 10 * N, o + 19 * N, o + 19 * N + std::max(J, 1),
+              o + 22 * N + std::max(J, 1)};
+    k_adj_cross<<<grid_for(std::max(3 * N, J), 128), 128, 0, sm>>>(ai, s->alam.as<double>(), s->aKphi.as<double>(), ao, afr);
     int fail = 0;
     NXD_CUDA(cudaMemcpyAsync(&fail, s->afail.p, sizeof(int), cudaMemcpyDeviceToHost, sm));
     const size_t n3 = 8 * 3 * (size_t)N;
@@ -2241,6 +2274,8 @@ nxd_status nxd_ipc_adjoint(nxd_ctx* c, double dt, const nxd_ipc_params* p, const
     if (out->mass_bar) NXD_CUDA(cudaMemcpyAsync(out->mass_bar, ao.mass_bar, 8 * (size_t)N, d2h, sm));
     if (out->inertia_bar) NXD_CUDA(cudaMemcpyAsync(out->inertia_bar, ao.inertia_bar, 8 * 9 * (size_t)N, d2h, sm));
     if (out->joint_mu_bar && J) NXD_CUDA(cudaMemcpyAsync(out->joint_mu_bar, ao.joint_mu_bar, 8 * (size_t)J, d2h, sm));
+    if (out->p0_bar) NXD_CUDA(cudaMemcpyAsync(out->p0_bar, ao.p0_bar, n3, d2h, sm));
+    if (out->friction_mu_bar) NXD_CUDA(cudaMemcpyAsync(out->friction_mu_bar, ao.friction_mu_bar, 8, d2h, sm));
     if (out->n_active) {
         NXD_CUDA(cudaStreamSynchronize(sm));
         std::vector<int> act(np);

@@ -366,7 +366,9 @@ class Context:
         """nxd_ipc_adjoint: the adjoint of one full-IPC step from the state
         `start` at its converged iterate x_star (6N) for x_bar = dL/dx_star.
         Returns lam (6N), phat_bar / thetahat_bar / phi_bar (N, 3), mass_bar
-        (N), inertia_bar (N, 3, 3), joint_mu_bar (J), n_active."""
+        (N), inertia_bar (N, 3, 3), joint_mu_bar (J), n_active and, with
+        friction (params.mu > 0, one lagging pass), p0_bar (N, 3) and
+        friction_mu_bar."""
         n, nj = self.scene.n_bodies, len(self.scene.joint_type)
         p = params if params is not None else abi.ipc_params()
         sb = abi.StateBuffers(n).load(start)
@@ -375,13 +377,15 @@ class Context:
         xb = np.ascontiguousarray(x_bar, dtype=np.float64)
         out = {"lam": np.zeros(6 * n), "phat_bar": np.zeros((n, 3)), "thetahat_bar": np.zeros((n, 3)),
                "phi_bar": np.zeros((n, 3)), "mass_bar": np.zeros(n), "inertia_bar": np.zeros((n, 3, 3)),
-               "joint_mu_bar": np.zeros(max(nj, 1))}
+               "joint_mu_bar": np.zeros(max(nj, 1)), "p0_bar": np.zeros((n, 3)), "friction_mu_bar": np.zeros(1)}
         na = C.c_int32(0)
         o = abi.NxdIpcAdjointOut(*[abi.dptr(out[k]) for k in ("lam", "phat_bar", "thetahat_bar", "phi_bar", "mass_bar",
-                                                                "inertia_bar", "joint_mu_bar")], C.pointer(na))
+                                                                "inertia_bar", "joint_mu_bar")], C.pointer(na),
+                                 abi.dptr(out["p0_bar"]), abi.dptr(out["friction_mu_bar"]))
         _check("nxd_ipc_adjoint", lib().nxd_ipc_adjoint(self.h, float(self.scene.dt if dt is None else dt), C.byref(p),
                                                         C.byref(view), abi.dptr(xs), abi.dptr(xb), C.byref(o)))
         out["joint_mu_bar"] = out["joint_mu_bar"][:nj]
+        out["friction_mu_bar"] = float(out["friction_mu_bar"][0])
         out["n_active"] = na.value
         return out
 

@@ -582,6 +582,18 @@ double nxo_ipc_accd(int32_t kind, const double* X12, const double* D12, double t
     return t;
 }
 
+// One frozen pair's friction point forces and their derivatives with respect
+// to the points (H) and to the lag points (Hs), ipc::friction_derivs; the
+// distance type of the lag points in *type.
+void nxo_ipc_friction_derivs(int32_t kind, const double* X12, const double* Xs12, double dhat, double kappa, double mu,
+                             double eps, double* g12, double* H, double* Hs, int32_t* type) {
+    V3 X[4], Xs[4];
+    for (int k = 0; k < 4; ++k) { X[k] = nx::ld3(X12 + 3 * k); Xs[k] = nx::ld3(Xs12 + 3 * k); }
+    const ipc::DistForm fs = ipc::classify(kind, Xs);
+    if (type) *type = fs.type;
+    ipc::friction_derivs(fs, X, Xs, dhat, kappa, mu, eps, g12, H, Hs);
+}
+
 double nxo_ipc_dist2(int32_t kind, const double* X12) {
     V3 X[4];
     for (int k = 0; k < 4; ++k) X[k] = nx::ld3(X12 + 3 * k);

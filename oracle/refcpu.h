@@ -113,6 +113,8 @@ int nxo_ipc_pair(int32_t kind, const double* X12, double dhat, double kappa, dou
 double nxo_ipc_accd(int32_t kind, const double* X12, const double* D12, double t_max, double eta, int32_t max_iter,
                     int32_t* iters);
 double nxo_ipc_dist2(int32_t kind, const double* X12);
+void nxo_ipc_friction_derivs(int32_t kind, const double* X12, const double* Xs12, double dhat, double kappa, double mu,
+                             double eps, double* g12, double* H, double* Hs, int32_t* type);
 
 #ifdef __cplusplus
 }

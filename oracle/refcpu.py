@@ -80,6 +80,8 @@ def lib():
     L.nxo_ipc_max_step.restype = C.c_double
     L.nxo_ipc_max_step.argtypes = [vp, dp, dp, C.c_double, i64p]
     L.nxo_ipc_friction.argtypes = [vp, dp, dp, C.c_double, C.c_double, C.c_double, C.c_double, dp, dp, dp, i64p]
+    L.nxo_ipc_friction_derivs.argtypes = [C.c_int32, dp, dp, C.c_double, C.c_double, C.c_double, C.c_double, dp, dp,
+                                          dp, C.POINTER(C.c_int32)]
     L.nxo_ipc_pair.argtypes = [C.c_int32, dp, C.c_double, C.c_double, dp, ip, dp, dp, dp, dp, dp]
     L.nxo_ipc_accd.restype = C.c_double
     L.nxo_ipc_accd.argtypes = [C.c_int32, dp, dp, C.c_double, C.c_double, C.c_int32, ip]
@@ -292,6 +294,19 @@ class OracleWorld:
         lib().nxo_ipc_friction(self.h, _d(x_lag), _d(x), dhat, kappa, mu, eps, C.byref(e), abi.dptr(g),
                                abi.dptr(H) if hessian else None, C.byref(nf))
         return e.value, g, H, nf.value
+
+
+def ipc_friction_derivs(kind: int, X, Xs, dhat: float, kappa: float, mu: float, eps: float) -> dict:
+    """One frozen pair's friction point forces (12) and their derivatives
+    with respect to its points (H) and its lag points (Hs), 12 x 12 each
+    (ipc::friction_derivs), and the lag points' distance type."""
+    X = np.ascontiguousarray(X, dtype=np.float64).reshape(12)
+    Xs = np.ascontiguousarray(Xs, dtype=np.float64).reshape(12)
+    g, H, Hs = np.zeros(12), np.zeros(144), np.zeros(144)
+    t = C.c_int32()
+    lib().nxo_ipc_friction_derivs(kind, _d(X), _d(Xs), dhat, kappa, mu, eps, abi.dptr(g), abi.dptr(H), abi.dptr(Hs),
+                                  C.byref(t))
+    return {"g": g, "H": H.reshape(12, 12), "Hs": Hs.reshape(12, 12), "type": t.value}
 
 
 def ipc_pair(kind: int, X, dhat: float, kappa: float) -> dict:

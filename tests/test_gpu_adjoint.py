@@ -108,3 +108,40 @@ def test_device_rollout_gradients_match_finite_differences():
         worst = max(worst, err)
     assert compared >= 0.6 * total, (compared, total)
     assert worst <= 5e-3, worst
+
+
+def test_device_friction_adjoint_matches_cpu_restatement():
+    # with lagged friction (one pass, mu 0.4): the device's analytic
+    # derivatives of the frozen pairs (ipc::friction_derivs) against the
+    # restatement's autograd, through every output, including the step-start
+    # positions' and the friction coefficient's adjoints.  Tolerance 1e-6 of
+    # each output's largest entry: the sticking stiffness mu lam / eps
+    # (~1e6 N/m at eps 1e-5 m) enters K and K_phi, and the outputs are sums of
+    # terms that large which cancel to O(1), so two different operation
+    # orders differ by more than the frictionless test's 1e-8 (a lost update
+    # in the assembly showed as 1e-3).
+    from nexdynipc_b200 import runtime
+    from oracle import ipc_adjoint as cpu_adj
+    mu, eps = 0.4, 1e-5
+    P = abi.ipc_params(dhat=1e-3, kappa=1e9, eta=0.1, newton_tol=1e-9, newton_max_iters=100, ls_max_iters=40,
+                       mu=mu, friction_eps=eps, friction_iters=1)
+    sc = scenes.diff_ipc_scene(n_spheres=6)
+    ctx = runtime.Context(sc)
+    cpu = cpu_adj.StepAdjoint(sc, P.dhat, P.kappa, mu=mu, eps=eps)
+    rng = np.random.default_rng(4)
+    checked = 0
+    for t in range(14):
+        st0 = ctx.state()
+        stats = ctx.ipc_step(P)
+        st1 = ctx.state()
+        xs = adjoint.iterate_of(st1, sc.dt)
+        xb = rng.normal(size=6 * sc.n_bodies)
+        d = ctx.ipc_adjoint(st0, xs, xb, P)
+        c = cpu(st0, xs, xb, sc.dt)
+        for k in ("lam", "phat_bar", "thetahat_bar", "phi_bar", "mass_bar", "inertia_bar", "joint_mu_bar", "p0_bar",
+                  "friction_mu_bar"):
+            ref = np.asarray(c[k])
+            assert np.abs(np.asarray(d[k]) - ref).max() <= 1e-6 * max(np.abs(ref).max(), 1e-30), (t, k)
+        checked += stats["n_friction"] > 0
+        ctx.set_state(st1)
+    assert checked >= 4

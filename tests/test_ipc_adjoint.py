@@ -277,3 +277,44 @@ def test_friction_rollout_adjoint_matches_finite_differences():
     a = np.array(checks)
     scale = np.abs(a[:, 1]).max()
     assert np.abs(a[:, 0] - a[:, 1]).max() <= 1e-4 * scale, a
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_friction_pair_derivatives_match_autograd(kind):
+    # the analytic derivatives the device adjoint uses (ipc::friction_derivs)
+    # against autograd of the torch restatement, over random pairs of every
+    # distance type near contact, their points displaced from the lag state
+    import torch
+    from test_ipc_oracle import random_pair
+    rng = np.random.default_rng(11 + kind)
+    dhat, kappa, mu, eps = 1e-1, 1e3, 0.4, 1e-3
+    types = set()
+    for it in range(90):
+        Xs = random_pair(rng, kind, rng.uniform(0.01, 0.09))
+        if kind == 1 and it % 3:
+            # slide edge b (or a) along itself just past an end: the closest
+            # points move to that end vertex (edge-vertex, vertex-vertex types)
+            Y = Xs.reshape(4, 3)
+            lo = 2 if it % 3 == 1 else 0
+            dv = Y[lo + 1] - Y[lo]
+            frac = (0.55 + rng.uniform(0.0, 0.05)) * (1.0 if it % 2 else -1.0)
+            Y[lo:lo + 2] += frac * dv
+            if it % 9 == 5:
+                Y[2:] += 0.56 * (Y[3] - Y[2])
+            Xs = Y.reshape(12)
+        X = Xs + rng.normal(0, 2e-3, 12)
+        ev = refcpu.ipc_pair(kind, Xs, dhat, kappa)
+        if not (ev["d2"] < dhat * dhat):
+            continue
+        r = refcpu.ipc_friction_derivs(kind, X, Xs, dhat, kappa, mu, eps)
+        typ = r["type"]
+        types.add(typ)
+        fn = lambda a, b_: cpu_adj.friction_force(kind, typ, a, b_, dhat, kappa, mu, eps)
+        Xt, Xst = torch.tensor(X.reshape(4, 3)), torch.tensor(Xs.reshape(4, 3))
+        g = fn(Xt, Xst).detach().numpy()
+        H, Hs = (j.reshape(12, 12).detach().numpy() for j in torch.autograd.functional.jacobian(fn, (Xt, Xst)))
+        sc = max(np.abs(H).max(), np.abs(Hs).max())
+        assert np.abs(r["g"] - g).max() <= 1e-10 * np.abs(g).max()
+        assert np.abs(r["H"] - H).max() <= 1e-10 * sc
+        assert np.abs(r["Hs"] - Hs).max() <= 1e-9 * sc, (typ, np.abs(r["Hs"] - Hs).max() / sc)
+    assert len(types) >= 3, types
