@@ -335,20 +335,24 @@ def adjoint_leg(torch, n_sets: int = 2):
     (nxd_ipc_adjoint per step, checkpoints every 10 steps, each segment
     re-stepped in the backward pass), through torch.autograd.  Wall clock of
     the forward rollout and of the backward pass, per parameter set (the
-    initial velocities perturbed per set)."""
+    initial velocities perturbed per set).  The step has lagged friction
+    (mu 0.4, eps 1e-5 m, one lagging pass), and the friction coefficient is
+    one of the differentiated parameters."""
     from nexdynipc_b200 import abi, adjoint, runtime, scenes
-    params = abi.ipc_params(dhat=1e-3, kappa=1e9, eta=0.1, newton_tol=1e-9, newton_max_iters=100, ls_max_iters=40)
+    params = abi.ipc_params(dhat=1e-3, kappa=1e9, eta=0.1, newton_tol=1e-9, newton_max_iters=100, ls_max_iters=40,
+                            mu=0.4, friction_eps=1e-5, friction_iters=1)
     base = scenes.diff_ipc_scene()
     fn = adjoint.make_rollout_function()
     rng = np.random.default_rng(5100)
-    fwd, bwd, its, conv, gnorm = [], [], [], [], []
+    fwd, bwd, its, conv, gnorm, gfric = [], [], [], [], [], []
     for k in range(n_sets):
         v0 = torch.tensor(base.velocity + rng.normal(0, 0.05, base.velocity.shape), requires_grad=True)
         m = torch.tensor(base.mass, requires_grad=True)
         mu = torch.tensor(base.joint_stiffness, requires_grad=True)
+        fr = torch.tensor(0.4, dtype=torch.float64, requires_grad=True)
         tgt = torch.tensor(np.concatenate([base.position, base.orientation], 1) + rng.normal(0, 0.02, (base.n_bodies, 7)))
         t0 = time.perf_counter()
-        out = fn.apply(v0, m, mu, base, params, base.steps, 10)
+        out = fn.apply(v0, m, mu, base, params, base.steps, 10, fr)
         t1 = time.perf_counter()
         loss = ((out - tgt) ** 2).sum()
         loss.backward()
@@ -356,9 +360,12 @@ def adjoint_leg(torch, n_sets: int = 2):
         fwd.append(t1 - t0)
         bwd.append(t2 - t1)
         gnorm.append(float(v0.grad.abs().max()))
+        gfric.append(float(fr.grad))
     return {"workload": (f"{base.n_bodies - 1} icospheres (162 V) on a ground box (fixed joint 1e5), {base.steps} "
-                         f"steps, dt {base.dt}, full-IPC step (kappa 1e9, dhat 1e-3, Newton |g| < 1e-9)"),
-            "parameter_sets": n_sets, "parameters_per_set": int(3 * base.n_bodies + base.n_bodies + 1),
+                         f"steps, dt {base.dt}, full-IPC step (kappa 1e9, dhat 1e-3, Newton |g| < 1e-9), lagged "
+                         f"friction mu 0.4"),
+            "parameter_sets": n_sets, "parameters_per_set": int(3 * base.n_bodies + base.n_bodies + 1 + 1),
+            "friction_coefficient_gradient": gfric,
             "checkpoint_every": 10, "forward_s": float(np.mean(fwd)), "backward_s": float(np.mean(bwd)),
             "fwd_plus_adj_over_fwd": float(np.mean([(a + b) / a for a, b in zip(fwd, bwd)])),
             "max_abs_velocity_gradient": gnorm,

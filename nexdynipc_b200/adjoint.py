@@ -187,16 +187,22 @@ def with_parameters(scene, velocity=None, mass=None, joint_stiffness=None, angul
 
 def make_rollout_function():
     """torch.autograd.Function: (velocity (N,3), mass (N), joint_stiffness
-    (J)) -> final poses (N, 7: position, orientation w x y z) of a full-IPC
-    rollout, with the adjoint backward.  Built lazily so that importing this
-    module does not import torch."""
+    (J), friction coefficient (scalar, or None: params.mu)) -> final poses
+    (N, 7: position, orientation w x y z) of a full-IPC rollout, with the
+    adjoint backward (the coefficient's gradient needs params with one
+    lagging pass).  Built lazily so that importing this module does not
+    import torch."""
     import torch
 
     class IpcRolloutFunction(torch.autograd.Function):
         @staticmethod
-        def forward(fctx, velocity, mass, joint_stiffness, scene, params, steps, checkpoint_every):
+        def forward(fctx, velocity, mass, joint_stiffness, scene, params, steps, checkpoint_every, friction=None):
             sc = with_parameters(scene, velocity=velocity.detach().cpu().numpy(), mass=mass.detach().cpu().numpy(),
                                  joint_stiffness=joint_stiffness.detach().cpu().numpy())
+            if friction is not None:
+                params = abi.NxdIpcParams.from_buffer_copy(params)
+                params.mu = float(friction.detach().cpu())
+            fctx.has_friction = friction is not None
             r = IpcRollout(sc, params, checkpoint_every)
             st = r.forward(int(steps))
             fctx.rollout = r
@@ -210,6 +216,7 @@ def make_rollout_function():
             b = r.backward(g[:, :3], g[:, 3:])
             dev = grad.device
             to = lambda a: torch.as_tensor(np.asarray(a), dtype=torch.float64, device=dev)
-            return to(b["velocity"]), to(b["mass"]), to(b["joint_stiffness"]), None, None, None, None
+            gf = to(b["friction"]) if fctx.has_friction else None
+            return to(b["velocity"]), to(b["mass"]), to(b["joint_stiffness"]), None, None, None, None, gf
 
     return IpcRolloutFunction

@@ -145,3 +145,77 @@ def test_device_friction_adjoint_matches_cpu_restatement():
         checked += stats["n_friction"] > 0
         ctx.set_state(st1)
     assert checked >= 4
+
+
+def test_device_friction_rollout_gradient_matches_finite_differences():
+    # the friction coefficient's and initial velocities' gradients of a
+    # device rollout with lagged friction (three spheres landing and sliding
+    # on a ground box from the first steps, so friction acts on most steps)
+    # against central differences of device rollouts on the same branch of
+    # active-pair counts; Newton to |g| < 1e-12 as in the CPU test
+    from nexdynipc_b200 import runtime
+    from test_ipc_adjoint import small_scene
+    mu, eps, steps = 0.4, 1e-5, 8
+
+    def params(m):
+        return abi.ipc_params(dhat=1e-3, kappa=1e9, eta=0.1, newton_tol=1e-12, newton_max_iters=100, ls_max_iters=40,
+                              mu=m, friction_eps=eps, friction_iters=1)
+
+    sc = small_scene()
+    ctx = runtime.Context(sc)
+    r = adjoint.IpcRollout(sc, params(mu), checkpoint_every=3, ctx=ctx)
+    T = r.forward(steps)
+    assert sum(s["n_friction"] for s in r.stats) > 0
+    branch = [s["n_active"] for s in r.stats]
+    rng = np.random.default_rng(2)
+    tgt_p = T["position"] + rng.normal(0, 0.01, T["position"].shape)
+    tgt_q = T["orientation"] + rng.normal(0, 0.01, T["orientation"].shape)
+    g = r.backward(2 * (T["position"] - tgt_p), 2 * (T["orientation"] - tgt_q))
+    fd_ctx = runtime.Context(sc)
+
+    def loss(scn, m):
+        fd_ctx.set_state(scn.initial_state())
+        act = [fd_ctx.ipc_step(params(m))["n_active"] for _ in range(steps)]
+        S = fd_ctx.state()
+        return float(((S["position"] - tgt_p) ** 2).sum() + ((S["orientation"] - tgt_q) ** 2).sum()), act
+
+    checks = []
+    h = 1e-4 * mu
+    (lp, ap), (lm, am) = loss(sc, mu + h), loss(sc, mu - h)
+    assert ap == branch and am == branch
+    checks.append((g["friction"], (lp - lm) / (2 * h)))
+    for b, k in ((1, 0), (2, 2), (3, 0)):
+        vp, vm = sc.velocity.copy(), sc.velocity.copy()
+        vp[b, k] += 1e-4
+        vm[b, k] -= 1e-4
+        (lp, ap), (lm, am) = (loss(adjoint.with_parameters(sc, velocity=vp), mu),
+                              loss(adjoint.with_parameters(sc, velocity=vm), mu))
+        if ap == branch and am == branch:
+            checks.append((g["velocity"][b, k], (lp - lm) / 2e-4))
+    a = np.array(checks)
+    assert np.abs(a[:, 0] - a[:, 1]).max() <= 1e-3 * np.abs(a[:, 1]).max(), a
+
+
+def test_autograd_function_passes_the_adjoint_through():
+    # torch.autograd over the rollout function: the gradients of velocity,
+    # mass, joint stiffness and friction coefficient equal IpcRollout's
+    import torch
+    sc = scenes.diff_ipc_scene(n_spheres=4)
+    P = abi.ipc_params(dhat=1e-3, kappa=1e9, eta=0.1, newton_tol=1e-9, newton_max_iters=100, ls_max_iters=40,
+                       mu=0.4, friction_eps=1e-5, friction_iters=1)
+    fn = adjoint.make_rollout_function()
+    v0 = torch.tensor(sc.velocity, requires_grad=True)
+    m = torch.tensor(sc.mass, requires_grad=True)
+    mu = torch.tensor(sc.joint_stiffness, requires_grad=True)
+    fr = torch.tensor(0.4, dtype=torch.float64, requires_grad=True)
+    out = fn.apply(v0, m, mu, sc, P, 8, 3, fr)
+    tgt = out.detach() + 0.01
+    ((out - tgt) ** 2).sum().backward()
+    r = adjoint.IpcRollout(sc, P, checkpoint_every=3)
+    T = r.forward(8)
+    o = np.concatenate([T["position"], T["orientation"]], 1)
+    g = r.backward(2 * (o[:, :3] - tgt.numpy()[:, :3]), 2 * (o[:, 3:] - tgt.numpy()[:, 3:]))
+    assert np.allclose(v0.grad.numpy(), g["velocity"], rtol=1e-12, atol=0)
+    assert np.allclose(m.grad.numpy(), g["mass"], rtol=1e-12, atol=0)
+    assert np.allclose(mu.grad.numpy(), g["joint_stiffness"], rtol=1e-12, atol=0)
+    assert float(fr.grad) == pytest.approx(g["friction"], rel=1e-12)
