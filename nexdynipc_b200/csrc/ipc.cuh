@@ -184,6 +184,39 @@ __global__ void k_bsr_concat(int N, const int* rpa, const int* cia, const double
     }
 }
 
+// Exclusive scan of n ints over many CTAs (the candidate counts, active
+// flags and segment flags of the full-IPC path reach 10^5 entries, where
+// one CTA's rounds cost ~50 us): per tile of kScanTile entries its sum,
+// one CTA scans the tile sums (the total with them), then each tile is
+// scanned by block_scan and offset.  Integer sums: the same result as k_scan.
+constexpr int kScanTileThreads = 256;
+constexpr int kScanTile = kScanTileThreads * kScanItems;
+__global__ void __launch_bounds__(kScanTileThreads) k_scan_tile_sums(const int* in, int n, int* sums) {
+    __shared__ int ws[kScanTileThreads / 32];
+    const int base = blockIdx.x * kScanTile, end = min(n, base + kScanTile);
+    int v = 0;
+    for (int i = base + threadIdx.x; i < end; i += kScanTileThreads) v += in[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < kScanTileThreads / 32; ++w) t += ws[w];
+        sums[blockIdx.x] = t;
+    }
+}
+__global__ void k_scan_sums(int* sums, int nt, int* total) {
+    const int t = block_scan(sums, sums, nt);
+    if (threadIdx.x == 0 && total) *total = t;
+}
+__global__ void __launch_bounds__(kScanTileThreads) k_scan_tiles(const int* in, int* out, int n, const int* offs) {
+    const int base = blockIdx.x * kScanTile, m = min(kScanTile, n - base);
+    block_scan(in + base, out + base, m);
+    __syncthreads();
+    const int o = offs[blockIdx.x];
+    for (int i = threadIdx.x; i < m; i += kScanTileThreads) out[base + i] += o;
+}
+
 // Each query's slice of (query, primitive) pairs, [off[q], off[q] + cnt[q]),
 // sorted by primitive in place by insertion, one thread per query (used
 // while no slice is longer than kSliceSortMax; the primitives of a slice are

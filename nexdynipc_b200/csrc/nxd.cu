@@ -1384,6 +1384,7 @@ struct IpcState {
     GrowBuf tkey, tval, tkey1, tval1;    // candidate pairs sorted by (query, primitive) keys
     GrowBuf qbuf0, qbuf1;                // per query the first hits of the count traversal (k_traverse)
     GrowBuf dxv, rmax, pad;              // the last ipc_pose's dx, per-body vertex radius and arc pad
+    GrowBuf scan_sums;                   // tile sums of scan_ints
     // lagged friction of the step: the frozen pairs (IpcFric), built from
     // the active pairs of the barrier evaluation that follows fr_build, and
     // the step-start world vertices they measure displacements from
@@ -1412,7 +1413,7 @@ struct IpcState {
                 &grad12, &lam, &z, &nterm, &body, &active, &type, &apos, &alist, &gkey, &gval, &gkey1, &gval1, &hkey,
                 &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &rrp, &rci, &rvv,
                 &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &akp, &akf, &abody, &aact,
-                &aK, &aKphi, &ax, &axb, &alam, &aout, &afail, &tkey, &tval, &tkey1, &tval1, &qbuf0, &qbuf1, &dxv, &rmax, &pad, &afkp, &afkf, &afks, &afgm, &afbody,
+                &aK, &aKphi, &ax, &axb, &alam, &aout, &afail, &tkey, &tval, &tkey1, &tval1, &qbuf0, &qbuf1, &dxv, &rmax, &pad, &scan_sums, &afkp, &afkf, &afks, &afgm, &afbody,
                 &aKps, &agmu, &fr_vid, &fr_body, &fr_kind, &fr_w, &fr_nrm, &fr_lam,
                 &fr_x0, &fr_e};
     }
@@ -1503,6 +1504,21 @@ nxd_status ipc_pose(nxd_ctx* c, const double* x, const double* dx, bool on_devic
                                                                       s->pq1.as<double>(), s->wq1.as<double>());
     }
     NXD_CUDA(cudaGetLastError());
+    return NXD_OK;
+}
+
+// Exclusive scan of n ints into out, the total into *total (device): one
+// CTA below 8192 entries, the tiled multi-CTA scan above (sums: scratch).
+nxd_status scan_ints(cudaStream_t st, GrowBuf& sums, const int* in, int* out, int n, int* total) {
+    if (n <= 8192) {
+        k_scan<<<1, 1024, 0, st>>>(in, out, n, total, nullptr, nullptr, nullptr);
+        return NXD_OK;
+    }
+    const int nt = (n + kScanTile - 1) / kScanTile;
+    if (!sums.ensure(4 * (size_t)nt)) return NXD_CUDA_ERROR;
+    k_scan_tile_sums<<<nt, kScanTileThreads, 0, st>>>(in, n, sums.as<int>());
+    k_scan_sums<<<1, 1024, 0, st>>>(sums.as<int>(), nt, total);
+    k_scan_tiles<<<nt, kScanTileThreads, 0, st>>>(in, out, n, sums.as<int>());
     return NXD_OK;
 }
 
@@ -1706,7 +1722,8 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
         IPC_ENSURE(*cnt[k], 4 * (size_t)nq[k]); IPC_ENSURE(*off[k], 4 * (size_t)nq[k]);
         if (!sweep) IPC_ENSURE(*qbuf[k], 4 * (size_t)kQueryBuf * nq[k]);
         launch(k, true);
-        k_scan<<<1, 1024, 0, c->stream>>>(cnt[k]->as<int>(), off[k]->as<int>(), nq[k], &ds->tot[k], nullptr, nullptr, nullptr);
+        if (scan_ints(c->stream, s->scan_sums, cnt[k]->as<int>(), off[k]->as<int>(), nq[k], &ds->tot[k]) != NXD_OK)
+            return NXD_CUDA_ERROR;
     }
     NXD_CUDA(cudaGetLastError());
     return NXD_OK;
@@ -1719,7 +1736,7 @@ nxd_status ipc_segments(nxd_ctx* c, const unsigned long long* keys, int m) {
     IPC_ENSURE(s->sflag, 4 * (size_t)m); IPC_ENSURE(s->spos, 4 * (size_t)m); IPC_ENSURE(s->sstart, 4 * (size_t)(m + 1));
     int* d_n = &s->ds()->nseg;
     k_seg_flags<<<grid_for(m, 256), 256, 0, c->stream>>>(keys, m, s->sflag.as<int>());
-    k_scan<<<1, 1024, 0, c->stream>>>(s->sflag.as<int>(), s->spos.as<int>(), m, d_n, nullptr, nullptr, nullptr);
+    if (scan_ints(c->stream, s->scan_sums, s->sflag.as<int>(), s->spos.as<int>(), m, d_n) != NXD_OK) return NXD_CUDA_ERROR;
     k_seg_starts<<<grid_for(m, 256), 256, 0, c->stream>>>(s->sflag.as<int>(), s->spos.as<int>(), m, s->sstart.as<int>(), d_n);
     NXD_CUDA(cudaGetLastError());
     return NXD_OK;
@@ -1789,7 +1806,8 @@ nxd_status ipc_barrier_eval(nxd_ctx* c, double dhat, double kappa, bool full, in
                        s->body.as<int>(), s->active.as<int>(), s->type.as<int>()};
     if (n) k_ipc_pair_eval<<<grid_for(n, 128), 128, 0, c->stream>>>(s->pg, P, ps, dhat, kappa, o);
     k_tree_sum<<<1, 1024, 0, c->stream>>>(s->e.as<double>(), n, &ds->energy);
-    k_scan<<<1, 1024, 0, c->stream>>>(s->active.as<int>(), s->apos.as<int>(), n, &ds->na, nullptr, nullptr, nullptr);
+    if (scan_ints(c->stream, s->scan_sums, s->active.as<int>(), s->apos.as<int>(), n, &ds->na) != NXD_OK)
+        return NXD_CUDA_ERROR;
     if (n) k_compact<<<grid_for(n, 256), 256, 0, c->stream>>>(s->active.as<int>(), s->apos.as<int>(), n, s->alist.as<int>());
     nxd_status st = ipc_fetch(c);
     if (st != NXD_OK) return st;
