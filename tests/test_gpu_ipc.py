@@ -3,11 +3,11 @@ oracle, through the C ABI (nxd_ipc_candidates / nxd_ipc_barrier /
 nxd_ipc_max_step).
 
 Candidate sets must be identical (sorted pair lists).  Energies, gradients
-and Hessian blocks are compared with the north-star tolerance (1e-10
-relative); both sides run the same per-pair arithmetic without FMA
-contraction and sum in the same fixed orders, so they agree bit for bit,
-which the tests report.  The CCD bound must not exceed the oracle's by more
-than 1e-12, and the pairs keep their gap along the chords up to it.
+and Hessian blocks are compared within 1e-10 relative; both sides run the
+same per-pair arithmetic without FMA contraction and sum in the same fixed
+orders, so they agree bit for bit, which the tests report.  The CCD bound
+must not exceed the oracle's by more than 1e-12 (it equals it), and it
+follows the rigid rotation arcs of the iterates.
 """
 import numpy as np
 import pytest

@@ -3,7 +3,7 @@ seeded inputs, through the C ABI.
 
 Integer / index outputs (body pairs, candidate lists, contact primitive ids)
 must be identical, in the reference's order.  Floating-point outputs are
-compared with the north-star tolerances: form energies and gradients within
+compared within the parity tolerances: form energies and gradients within
 1e-10 relative, trajectories within 1e-6 m / 1e-6 rad; both sides round the
 same way (no FMA contraction, same reduction trees), so most of them agree
 bit for bit, which the tests report.
