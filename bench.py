@@ -331,20 +331,19 @@ def adjoint_leg(torch, n_sets: int = 2):
     """Differentiable configuration on the full-IPC step: 16 icospheres
     (162 V) over a ground box, 50 steps, loss = squared error of the final
     poses against a seeded target, gradients with respect to every initial
-    velocity, mass and the ground joint's stiffness by the adjoint
-    (nxd_ipc_adjoint per step, checkpoints every 10 steps, each segment
-    re-stepped in the backward pass), through torch.autograd.  Wall clock of
-    the forward rollout and of the backward pass, per parameter set (the
-    initial velocities perturbed per set).  The step has lagged friction
-    (mu 0.4, eps 1e-5 m, one lagging pass), and the friction coefficient is
-    one of the differentiated parameters."""
+    velocity, mass, the ground joint's stiffness and the friction coefficient
+    by the adjoint (nxd_ipc_adjoint per step, checkpoints every 10 steps, each
+    segment re-stepped in the backward pass), through torch.autograd.  The
+    step has lagged friction (mu 0.4, eps 1e-5 m, one lagging pass).  Wall
+    clock of the forward rollout and of the backward pass, per parameter set
+    (the initial velocities perturbed per set), the sets one after another."""
     from nexdynipc_b200 import abi, adjoint, runtime, scenes
     params = abi.ipc_params(dhat=1e-3, kappa=1e9, eta=0.1, newton_tol=1e-9, newton_max_iters=100, ls_max_iters=40,
                             mu=0.4, friction_eps=1e-5, friction_iters=1)
     base = scenes.diff_ipc_scene()
     fn = adjoint.make_rollout_function()
     rng = np.random.default_rng(5100)
-    fwd, bwd, its, conv, gnorm, gfric = [], [], [], [], [], []
+    fwd, bwd, gnorm, gfric = [], [], [], []
     for k in range(n_sets):
         v0 = torch.tensor(base.velocity + rng.normal(0, 0.05, base.velocity.shape), requires_grad=True)
         m = torch.tensor(base.mass, requires_grad=True)
@@ -365,10 +364,9 @@ def adjoint_leg(torch, n_sets: int = 2):
                          f"steps, dt {base.dt}, full-IPC step (kappa 1e9, dhat 1e-3, Newton |g| < 1e-9), lagged "
                          f"friction mu 0.4"),
             "parameter_sets": n_sets, "parameters_per_set": int(3 * base.n_bodies + base.n_bodies + 1 + 1),
-            "friction_coefficient_gradient": gfric,
             "checkpoint_every": 10, "forward_s": float(np.mean(fwd)), "backward_s": float(np.mean(bwd)),
             "fwd_plus_adj_over_fwd": float(np.mean([(a + b) / a for a, b in zip(fwd, bwd)])),
-            "max_abs_velocity_gradient": gnorm,
+            "max_abs_velocity_gradient": gnorm, "friction_coefficient_gradient": gfric,
             "timing": "wall clock; the backward pass re-steps each 10-step segment from its checkpoint"}
 
 

@@ -91,12 +91,17 @@ class IpcRollout:
     device (runtime.Context.ipc_step / ipc_adjoint)."""
 
     def __init__(self, scene, params=None, checkpoint_every: int = 10, ctx=None,
-                 adjoint_fn: Optional[Callable] = None):
+                 adjoint_fn: Optional[Callable] = None, stream: Optional[int] = None):
         from . import runtime
         self.scene = scene
         self.params = params if params is not None else abi.ipc_params()
         self.k = max(1, int(checkpoint_every))
         self.ctx = ctx if ctx is not None else runtime.Context(scene)
+        if stream:
+            # its own CUDA stream (raw cudaStream_t), so that rollouts on other
+            # host threads overlap on the device
+            import ctypes
+            runtime.lib().nxd_set_stream(self.ctx.h, ctypes.c_void_p(stream))
         self.adjoint_fn = adjoint_fn or (lambda start, xs, xb: self.ctx.ipc_adjoint(start, xs, xb, self.params))
         self.checkpoints = []
         self.steps = 0
@@ -185,12 +190,14 @@ def with_parameters(scene, velocity=None, mass=None, joint_stiffness=None, angul
     return new
 
 
-def make_rollout_function():
+def make_rollout_function(stream: Optional[int] = None):
     """torch.autograd.Function: (velocity (N,3), mass (N), joint_stiffness
     (J), friction coefficient (scalar, or None: params.mu)) -> final poses
     (N, 7: position, orientation w x y z) of a full-IPC rollout, with the
     adjoint backward (the coefficient's gradient needs params with one
-    lagging pass).  Built lazily so that importing this module does not
+    lagging pass).  With `stream` (a raw cudaStream_t) the rollout's context
+    issues its work there, so that several parameter sets run concurrently
+    from host threads.  Built lazily so that importing this module does not
     import torch."""
     import torch
 
@@ -203,7 +210,7 @@ def make_rollout_function():
                 params = abi.NxdIpcParams.from_buffer_copy(params)
                 params.mu = float(friction.detach().cpu())
             fctx.has_friction = friction is not None
-            r = IpcRollout(sc, params, checkpoint_every)
+            r = IpcRollout(sc, params, checkpoint_every, stream=stream)
             st = r.forward(int(steps))
             fctx.rollout = r
             out = np.concatenate([st["position"], st["orientation"]], axis=1)
