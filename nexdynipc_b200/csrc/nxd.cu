@@ -2339,6 +2339,12 @@ struct nxd_batch {
     // persistent grid of each queue-form kernel: CTAs per SM (the result
     // does not depend on it; nxd_batch_set_queue_ctas, the autotuner)
     int queue_per_sm[kQueueKinds] = {4, 4};
+    // with several groups, each group's graph runs on a stream of its own,
+    // forked from and joined back into `stream` (the groups share nothing,
+    // so one group's Newton CTAs fill the SMs another's leave early)
+    std::vector<cudaStream_t> gstream;
+    std::vector<cudaEvent_t> gdone;
+    cudaEvent_t fork = nullptr;
 };
 
 namespace {
@@ -2517,6 +2523,9 @@ void nxd_batch_destroy(nxd_batch* b) {
     if (!b) return;
     cudaStreamSynchronize(b->stream);
     release_groups(b);
+    for (cudaStream_t st : b->gstream) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : b->gdone) cudaEventDestroy(ev);
+    if (b->fork) cudaEventDestroy(b->fork);
     for (nxd_ctx* c : b->ctx) { c->stream = nullptr; nxd_destroy(c); }
     if (b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -2533,7 +2542,26 @@ nxd_status nxd_batch_step(nxd_batch* b, const double* dts) {
         const nxd_status st = build_groups(b, dts);
         if (st != NXD_OK) return st;
     }
-    for (BatchGroup& g : b->groups) NXD_CUDA(cudaGraphLaunch(g.exec, b->stream));
+    if (b->groups.size() == 1) {
+        NXD_CUDA(cudaGraphLaunch(b->groups[0].exec, b->stream));
+        return NXD_OK;
+    }
+    if (!b->fork) NXD_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    while (b->gstream.size() < b->groups.size()) {
+        cudaStream_t st;
+        cudaEvent_t ev;
+        NXD_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        NXD_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        b->gstream.push_back(st);
+        b->gdone.push_back(ev);
+    }
+    NXD_CUDA(cudaEventRecord(b->fork, b->stream));
+    for (size_t i = 0; i < b->groups.size(); ++i) {
+        NXD_CUDA(cudaStreamWaitEvent(b->gstream[i], b->fork, 0));
+        NXD_CUDA(cudaGraphLaunch(b->groups[i].exec, b->gstream[i]));
+        NXD_CUDA(cudaEventRecord(b->gdone[i], b->gstream[i]));
+        NXD_CUDA(cudaStreamWaitEvent(b->stream, b->gdone[i], 0));
+    }
     return NXD_OK;
 }
 
