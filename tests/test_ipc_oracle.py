@@ -314,3 +314,41 @@ def test_accd_follows_the_rotation_arc():
     # with the chord the end poses and every chord point would pass
     wv1, _ = ow.world_vertices_at(x + dx)
     assert wv1[8:, 1].min() > 0.02
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_step_bound_keeps_every_pair_apart_along_the_arc(seed):
+    # the step bound's guarantee on the rigid arcs: two settled cubes and the
+    # ground moved by a random step with rotations up to ~0.6 rad; at every
+    # sampled pose x + t dx, t <= the bound, every swept candidate pair keeps
+    # at least eta of its distance at x (distances by brute force over the
+    # pair's closest points, evaluated on the posed world vertices)
+    sc = scenes.ipc_drop(n_cubes=2)
+    ow = refcpu.OracleWorld(sc)
+    from nexdynipc_b200 import abi
+    p = abi.ipc_params(**scenes.ipc_step_settings())
+    for _ in range(25):
+        ow.ipc_step(p)
+    st = ow.state()
+    n = 6 * sc.n_bodies
+    x = np.zeros(n)
+    x.reshape(-1, 6)[:, :3] = st["position"]
+    rng = np.random.default_rng(100 + seed)
+    dx = np.zeros(n)
+    for b in range(1, sc.n_bodies):
+        dx[6 * b:6 * b + 3] = rng.normal(0, 0.03, 3) + np.array([0.0, -0.05, 0.0])
+        dx[6 * b + 3:6 * b + 6] = rng.normal(0, 0.35, 3)
+    eta = 0.1
+    alpha, npairs = ow.ipc_max_step(x, dx, eta)
+    assert npairs > 0 and 0.0 < alpha <= 1.0
+    pt, ee = ow.ipc_candidates(x, dx, 0.0)
+    vb, fb, fv, eb, ev = ow.prim_topology()
+    pairs = [(0, [v, *fv[f]]) for v, f in pt] + [(1, [*ev[a], *ev[b]]) for a, b in ee]
+    w0, _ = ow.world_vertices_at(x)
+    d0 = [np.sqrt(refcpu.ipc_dist2(k, w0[vid])) for k, vid in pairs]
+    worst = np.inf
+    for t in np.linspace(0.0, alpha, 41):
+        wt, _ = ow.world_vertices_at(x + t * dx)
+        for (k, vid), dd in zip(pairs, d0):
+            worst = min(worst, np.sqrt(refcpu.ipc_dist2(k, wt[vid])) / (eta * dd))
+    assert worst >= 1.0 - 1e-9, worst
