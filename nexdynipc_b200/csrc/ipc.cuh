@@ -443,43 +443,78 @@ __global__ void k_sweep_all(PrimGeo pg, int kind, const double* qbox, int nq, co
 // Traversal of one query box against the tree; mode 0 counts, mode 1 writes
 // the query's hits into its slice in traversal order (sorted afterwards).
 // kind 0: vertex queries vs faces (other body); 1: edge queries vs edges
-// (other body, query < prim).
+// (other body, query < prim).  Both children's boxes are loaded and tested
+// at their parent (independent loads); an overlapping leaf is taken there,
+// one overlapping inner child is entered directly and only the second of
+// two is pushed.  A leaf is a hit iff its box and every ancestor's box
+// overlap the query box, so the hit set does not depend on the order.
+// With qorder (edge queries against the edge tree) thread t takes query
+// qorder[t], the tree's t-th leaf, so a warp's queries are neighbours in
+// space and walk the same nodes.
 constexpr int kTravStack = 96;
 // In count mode each query's first kQueryBuf hits also go to its row of
 // qbuf (traversal order) and a query with more raises *maxq to its count,
 // so that a call whose queries all fit copies its lists from qbuf
 // (k_copy_slices) instead of traversing again.
+__device__ __forceinline__ void load_node_box(const double* p, double b[6]) {
+    const double2* p2 = reinterpret_cast<const double2*>(p);   // 48-byte records, 16-byte aligned
+    const double2 u = __ldg(p2), v = __ldg(p2 + 1), w = __ldg(p2 + 2);
+    b[0] = u.x; b[1] = u.y; b[2] = v.x; b[3] = v.y; b[4] = w.x; b[5] = w.y;
+}
 __global__ void k_traverse(PrimGeo pg, int kind, const double* qbox, int nq, const double* nbox, const int* child, const int* ids,
-                           int n, int* cnt, const int* off, int* out, int* status, int* maxq, int* qbuf) {
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+                           int n, int* cnt, const int* off, int* out, int* status, int* maxq, int* qbuf, const int* qorder) {
+    const int2* ch2 = reinterpret_cast<const int2*>(child);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += gridDim.x * blockDim.x) {
+        const int q = qorder ? qorder[t] : t;
         double qb[6];
         for (int a = 0; a < 6; ++a) qb[a] = qbox[6 * q + a];
         const int qbody = kind == 0 ? pg.vbody[q] : pg.ebody[q];
         int c = 0;
         int* dst = out ? out + 2 * (size_t)off[q] : nullptr;
-        int stack[kTravStack];
-        int top = 0;
-        stack[top++] = n == 1 ? ~0 : 0;
-        while (top > 0) {
-            const int node = stack[--top];
-            const int slot = node >= 0 ? node : (n - 1) + ~node;
-            if (!boxes_overlap(qb, nbox + 6 * slot)) continue;
-            if (node < 0) {
-                const int prim = ids[~node];
-                const int pbody = kind == 0 ? pg.fbody[prim] : pg.ebody[prim];
-                if (pbody == qbody || (kind == 1 && !(q < prim))) continue;
-                if (dst) {
-                    dst[2 * c] = q;
-                    dst[2 * c + 1] = prim;
-                } else if (qbuf && c < kQueryBuf) {
-                    qbuf[(size_t)kQueryBuf * q + c] = prim;
-                }
-                ++c;
-                continue;
+        auto leaf_hit = [&](int leaf) {
+            const int prim = ids[leaf];
+            const int pbody = kind == 0 ? pg.fbody[prim] : pg.ebody[prim];
+            if (pbody == qbody || (kind == 1 && !(q < prim))) return;
+            if (dst) {
+                dst[2 * c] = q;
+                dst[2 * c + 1] = prim;
+            } else if (qbuf && c < kQueryBuf) {
+                qbuf[(size_t)kQueryBuf * q + c] = prim;
             }
-            if (top + 2 > kTravStack) { atomicExch(status, NXD_CAPACITY); continue; }
-            stack[top++] = child[2 * node + 1];
-            stack[top++] = child[2 * node];
+            ++c;
+        };
+        double rb[6];
+        load_node_box(nbox, rb);   // slot 0: the root (inner node 0, or the single leaf)
+        if (boxes_overlap(qb, rb)) {
+            if (n == 1) {
+                leaf_hit(0);
+            } else {
+                int stack[kTravStack];
+                int top = 0, node = 0;
+                for (;;) {
+                    const int2 cc = __ldg(ch2 + node);
+                    double bl[6], br[6];
+                    load_node_box(nbox + 6 * (size_t)(cc.x >= 0 ? cc.x : (n - 1) + ~cc.x), bl);
+                    load_node_box(nbox + 6 * (size_t)(cc.y >= 0 ? cc.y : (n - 1) + ~cc.y), br);
+                    const bool ol = boxes_overlap(qb, bl), orr = boxes_overlap(qb, br);
+                    if (ol && cc.x < 0) leaf_hit(~cc.x);
+                    if (orr && cc.y < 0) leaf_hit(~cc.y);
+                    const bool dl = ol && cc.x >= 0, dr = orr && cc.y >= 0;
+                    if (dl && dr) {
+                        if (top < kTravStack) stack[top++] = cc.y;
+                        else atomicExch(status, NXD_CAPACITY);
+                        node = cc.x;
+                    } else if (dl) {
+                        node = cc.x;
+                    } else if (dr) {
+                        node = cc.y;
+                    } else if (top > 0) {
+                        node = stack[--top];
+                    } else {
+                        break;
+                    }
+                }
+            }
         }
         if (!out) {
             cnt[q] = c;

@@ -1632,7 +1632,8 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
             k_traverse<<<grid_for(nq[k], 128), 128, 0, c->stream>>>(s->pg, k, qbox[k], nq[k], B.nbox.as<double>(),
                                                                     B.child.as<int>(), B.i0.as<int>(), B.n, cn, of, dst,
                                                                     &ds->status, &ds->maxq[k],
-                                                                    count ? qbuf[k]->as<int>() : nullptr);
+                                                                    count ? qbuf[k]->as<int>() : nullptr,
+                                                                    k == 1 && B.n == nq[1] ? B.i0.as<int>() : nullptr);
     };
     if (phase == 1) {
         // after the fetch: the totals in pinned memory, then the writes
