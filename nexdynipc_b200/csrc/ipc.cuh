@@ -344,7 +344,7 @@ __device__ __forceinline__ int kdelta(const unsigned long long* k, int n, int i,
     return __clzll(k[i] ^ k[j]);
 }
 
-__global__ void k_karras(const unsigned long long* k, int n, int* child, int* parent) {
+__global__ void k_karras(const unsigned long long* k, int n, int* child, int* parent, int2* rng) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x) {
         const int d = (kdelta(k, n, i, i + 1) - kdelta(k, n, i, i - 1)) >= 0 ? 1 : -1;
         const int dmin_ = kdelta(k, n, i, i - d);
@@ -366,6 +366,7 @@ __global__ void k_karras(const unsigned long long* k, int n, int* child, int* pa
         const int right = hi == gamma + 1 ? ~(gamma + 1) : gamma + 1;
         child[2 * i] = left;
         child[2 * i + 1] = right;
+        rng[i] = make_int2(lo, hi);
         parent[left >= 0 ? left : (n - 1) + ~left] = i;
         parent[right >= 0 ? right : (n - 1) + ~right] = i;
     }
@@ -374,29 +375,62 @@ __global__ void k_karras(const unsigned long long* k, int n, int* child, int* pa
 
 // Bottom-up boxes: node slots 0..n-2 internal, n-1+s leaf s (sorted order).
 // The second child to arrive at a node (atomic counter) merges its two boxes.
-__global__ void k_refit(const double* leaf_box, const int* ids, int n, const int* child, const int* parent, double* nbox,
-                        int* flags) {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
-        double* lb = nbox + 6 * ((n - 1) + s);
-        const double* src = leaf_box + 6 * ids[s];
-        for (int a = 0; a < 6; ++a) lb[a] = src[a];
-        if (n == 1) continue;
-        __threadfence();
-        int node = parent[(n - 1) + s];
-        for (int guard = 0; node >= 0 && guard < 64 + n; ++guard) {
-            if (atomicAdd(&flags[node], 1) == 0) break;   // first arrival: the sibling finishes
-            __threadfence();
-            const int c0 = child[2 * node], c1 = child[2 * node + 1];
-            const double* b0 = nbox + 6 * (c0 >= 0 ? c0 : (n - 1) + ~c0);
-            const double* b1 = nbox + 6 * (c1 >= 0 ? c1 : (n - 1) + ~c1);
-            double* bn = nbox + 6 * node;
-            for (int a = 0; a < 3; ++a) {
-                bn[a] = dmin(__ldcg(b0 + a), __ldcg(b1 + a));
-                bn[3 + a] = dmax(__ldcg(b0 + 3 + a), __ldcg(b1 + 3 + a));
-            }
-            __threadfence();
-            node = parent[node];
+// Block b takes the kRefitChunk leaves from s0 = b * kRefitChunk; an inner
+// node whose leaf range (rng, from k_karras) lies inside that chunk has
+// its index there too (a Karras node's index is an end of its range), so
+// its counter and box live in the block's shared memory: the lower levels
+// of the climb hand over at shared-memory latency, and only the nodes that
+// straddle chunks take the device-wide counter and fences.  The boxes are
+// minima and maxima, so the merge order changes no bit of them.
+constexpr int kRefitChunk = 256;
+__global__ void __launch_bounds__(kRefitChunk) k_refit(const double* leaf_box, const int* ids, int n, const int* child,
+                                                       const int* parent, const int2* rng, double* nbox, int* flags) {
+    __shared__ double sbox[2 * kRefitChunk][6];   // [0, C): inner nodes s0.., [C, 2C): leaves s0..
+    __shared__ int sflag[kRefitChunk];
+    const int s0 = blockIdx.x * kRefitChunk, s = s0 + threadIdx.x;
+    sflag[threadIdx.x] = 0;
+    __syncthreads();
+    if (s >= n) return;
+    const int last = min(s0 + kRefitChunk, n) - 1;
+    double b[6];
+    const double* src = leaf_box + 6 * (size_t)ids[s];
+    double* lb = nbox + 6 * ((size_t)(n - 1) + s);
+    for (int a = 0; a < 6; ++a) { b[a] = src[a]; lb[a] = b[a]; sbox[kRefitChunk + threadIdx.x][a] = b[a]; }
+    if (n == 1) return;
+    auto slot = [&](int ch) { return ch >= 0 ? ch - s0 : kRefitChunk + (~ch - s0); };
+    bool local = true;
+    int node = parent[(n - 1) + s];
+    for (int guard = 0; node >= 0 && guard < 64 + n; ++guard) {
+        const int c0 = child[2 * node], c1 = child[2 * node + 1];
+        if (local) {
+            const int2 r = rng[node];
+            local = r.x >= s0 && r.y <= last;
         }
+        if (local) {
+            __threadfence_block();
+            if (atomicAdd_block(&sflag[node - s0], 1) == 0) return;   // first arrival: the sibling finishes
+            __threadfence_block();
+            const double* b0 = sbox[slot(c0)];
+            const double* b1 = sbox[slot(c1)];
+            for (int a = 0; a < 3; ++a) {
+                b[a] = dmin(b0[a], b1[a]);
+                b[3 + a] = dmax(b0[3 + a], b1[3 + a]);
+            }
+            for (int a = 0; a < 6; ++a) sbox[node - s0][a] = b[a];
+        } else {
+            __threadfence();
+            if (atomicAdd(&flags[node], 1) == 0) return;
+            __threadfence();
+            const double* b0 = nbox + 6 * (size_t)(c0 >= 0 ? c0 : (n - 1) + ~c0);
+            const double* b1 = nbox + 6 * (size_t)(c1 >= 0 ? c1 : (n - 1) + ~c1);
+            for (int a = 0; a < 3; ++a) {
+                b[a] = dmin(__ldcg(b0 + a), __ldcg(b1 + a));
+                b[3 + a] = dmax(__ldcg(b0 + 3 + a), __ldcg(b1 + 3 + a));
+            }
+        }
+        double* bn = nbox + 6 * (size_t)node;
+        for (int a = 0; a < 6; ++a) bn[a] = b[a];
+        node = parent[node];
     }
 }
 

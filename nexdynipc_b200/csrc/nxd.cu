@@ -1335,7 +1335,7 @@ namespace {
 struct Bvh {
     int n = 0;
     int topo_n = -1;    // primitive count of the hierarchy in child / parent / i0 (-1: none built)
-    GrowBuf k0, k1, i0, i1, leaf, nbox, child, parent, flags, bounds;
+    GrowBuf k0, k1, i0, i1, leaf, nbox, child, parent, rng, flags, bounds;
 };
 
 }  // namespace
@@ -1407,8 +1407,8 @@ struct IpcState {
     PcgScratch pcg;
     std::vector<GrowBuf*> all() {
         return {&fbody, &fvert, &ebody, &evert, &x0, &x1, &pp0, &pq0, &pp1, &pq1, &wq0, &wq1, &qv, &qe,
-                &faces.k0, &faces.k1, &faces.i0, &faces.i1, &faces.leaf, &faces.nbox, &faces.child, &faces.parent,
-                &faces.flags, &faces.bounds, &edges.k0, &edges.k1, &edges.i0, &edges.i1, &edges.leaf, &edges.nbox,
+                &faces.k0, &faces.k1, &faces.i0, &faces.i1, &faces.leaf, &faces.nbox, &faces.child, &faces.parent, &faces.rng,
+                &faces.flags, &faces.bounds, &edges.k0, &edges.k1, &edges.i0, &edges.i1, &edges.leaf, &edges.nbox, &edges.rng,
                 &edges.child, &edges.parent, &edges.flags, &edges.bounds, &cnt, &off, &cnt2, &off2, &pt, &ee, &scal, &hist, &e,
                 &grad12, &lam, &z, &nterm, &body, &active, &type, &apos, &alist, &gkey, &gval, &gkey1, &gval1, &hkey,
                 &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &rrp, &rci, &rvv,
@@ -1562,8 +1562,9 @@ nxd_status ipc_build_bvh(nxd_ctx* c, Bvh& B, int kind, bool swept, double infl) 
     if (s->keep_trees && B.topo_n == n) {
         // the step's hierarchy, boxes refitted bottom-up
         NXD_CUDA(cudaMemsetAsync(B.flags.p, 0, 4 * (size_t)n, c->stream));
-        k_refit<<<grid_for(n, 128), 128, 0, c->stream>>>(B.leaf.as<double>(), B.i0.as<int>(), n, B.child.as<int>(),
-                                                         B.parent.as<int>(), B.nbox.as<double>(), B.flags.as<int>());
+        k_refit<<<(n + kRefitChunk - 1) / kRefitChunk, kRefitChunk, 0, c->stream>>>(
+            B.leaf.as<double>(), B.i0.as<int>(), n, B.child.as<int>(), B.parent.as<int>(), B.rng.as<int2>(), B.nbox.as<double>(),
+            B.flags.as<int>());
         NXD_CUDA(cudaGetLastError());
         return NXD_OK;
     }
@@ -1576,12 +1577,14 @@ nxd_status ipc_build_bvh(nxd_ctx* c, Bvh& B, int kind, bool swept, double infl) 
     nxd_status st = radix_sort(c, B.k0, B.i0, B.k1, B.i1, n, 32, 64);
     if (st != NXD_OK) return st;
     IPC_ENSURE(B.nbox, 48 * (size_t)(2 * n - 1)); IPC_ENSURE(B.child, 8 * (size_t)n);
-    IPC_ENSURE(B.parent, 4 * (size_t)(2 * n)); IPC_ENSURE(B.flags, 4 * (size_t)n);
+    IPC_ENSURE(B.parent, 4 * (size_t)(2 * n)); IPC_ENSURE(B.flags, 4 * (size_t)n); IPC_ENSURE(B.rng, 8 * (size_t)n);
     NXD_CUDA(cudaMemsetAsync(B.flags.p, 0, 4 * (size_t)n, c->stream));
     k_karras<<<grid_for(std::max(n - 1, 1), 128), 128, 0, c->stream>>>(B.k0.as<unsigned long long>(), n, B.child.as<int>(),
-                                                                        B.parent.as<int>());
-    k_refit<<<grid_for(n, 128), 128, 0, c->stream>>>(B.leaf.as<double>(), B.i0.as<int>(), n, B.child.as<int>(), B.parent.as<int>(),
-                                                     B.nbox.as<double>(), B.flags.as<int>());
+                                                                        B.parent.as<int>(), B.rng.as<int2>());
+    k_refit<<<(n + kRefitChunk - 1) / kRefitChunk, kRefitChunk, 0, c->stream>>>(B.leaf.as<double>(), B.i0.as<int>(), n,
+                                                                                  B.child.as<int>(), B.parent.as<int>(),
+                                                                                  B.rng.as<int2>(), B.nbox.as<double>(),
+                                                                                  B.flags.as<int>());
     NXD_CUDA(cudaGetLastError());
     B.topo_n = n;
     return NXD_OK;
