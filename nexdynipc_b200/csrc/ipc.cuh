@@ -383,6 +383,14 @@ __global__ void k_karras(const unsigned long long* k, int n, int* child, int* pa
 // straddle chunks take the device-wide counter and fences.  The boxes are
 // minima and maxima, so the merge order changes no bit of them.
 constexpr int kRefitChunk = 256;
+// fetch-and-add with release (this thread's earlier writes are visible
+// before the add) and acquire (writes released by earlier adds are visible
+// after it) at device scope
+__device__ __forceinline__ int atomic_add_acq_rel(int* p, int v) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
 __global__ void __launch_bounds__(kRefitChunk) k_refit(const double* leaf_box, const int* ids, int n, const int* child,
                                                        const int* parent, const int2* rng, double* nbox, int* flags) {
     __shared__ double sbox[2 * kRefitChunk][6];   // [0, C): inner nodes s0.., [C, 2C): leaves s0..
@@ -399,37 +407,35 @@ __global__ void __launch_bounds__(kRefitChunk) k_refit(const double* leaf_box, c
     if (n == 1) return;
     auto slot = [&](int ch) { return ch >= 0 ? ch - s0 : kRefitChunk + (~ch - s0); };
     bool local = true;
+    int from = ~s;   // the child this thread arrives from; its box is b
     int node = parent[(n - 1) + s];
     for (int guard = 0; node >= 0 && guard < 64 + n; ++guard) {
         const int c0 = child[2 * node], c1 = child[2 * node + 1];
+        const int sib = c0 == from ? c1 : c0;
         if (local) {
             const int2 r = rng[node];
             local = r.x >= s0 && r.y <= last;
         }
+        double o[6];
         if (local) {
             __threadfence_block();
             if (atomicAdd_block(&sflag[node - s0], 1) == 0) return;   // first arrival: the sibling finishes
             __threadfence_block();
-            const double* b0 = sbox[slot(c0)];
-            const double* b1 = sbox[slot(c1)];
-            for (int a = 0; a < 3; ++a) {
-                b[a] = dmin(b0[a], b1[a]);
-                b[3 + a] = dmax(b0[3 + a], b1[3 + a]);
-            }
-            for (int a = 0; a < 6; ++a) sbox[node - s0][a] = b[a];
+            for (int a = 0; a < 6; ++a) o[a] = sbox[slot(sib)][a];
         } else {
-            __threadfence();
-            if (atomicAdd(&flags[node], 1) == 0) return;
-            __threadfence();
-            const double* b0 = nbox + 6 * (size_t)(c0 >= 0 ? c0 : (n - 1) + ~c0);
-            const double* b1 = nbox + 6 * (size_t)(c1 >= 0 ? c1 : (n - 1) + ~c1);
-            for (int a = 0; a < 3; ++a) {
-                b[a] = dmin(__ldcg(b0 + a), __ldcg(b1 + a));
-                b[3 + a] = dmax(__ldcg(b0 + 3 + a), __ldcg(b1 + 3 + a));
-            }
+            if (atomic_add_acq_rel(&flags[node], 1) == 0) return;
+            const double* sb = nbox + 6 * (size_t)(sib >= 0 ? sib : (n - 1) + ~sib);
+            for (int a = 0; a < 6; ++a) o[a] = __ldcg(sb + a);
         }
+        for (int a = 0; a < 3; ++a) {
+            b[a] = dmin(b[a], o[a]);
+            b[3 + a] = dmax(b[3 + a], o[3 + a]);
+        }
+        if (local)
+            for (int a = 0; a < 6; ++a) sbox[node - s0][a] = b[a];
         double* bn = nbox + 6 * (size_t)node;
         for (int a = 0; a < 6; ++a) bn[a] = b[a];
+        from = node;
         node = parent[node];
     }
 }
