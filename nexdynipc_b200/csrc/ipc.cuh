@@ -501,10 +501,27 @@ __device__ __forceinline__ void load_node_box(const double* p, double b[6]) {
     const double2 u = __ldg(p2), v = __ldg(p2 + 1), w = __ldg(p2 + 2);
     b[0] = u.x; b[1] = u.y; b[2] = v.x; b[3] = v.y; b[4] = w.x; b[5] = w.y;
 }
-__global__ void k_traverse(PrimGeo pg, int kind, const double* qbox, int nq, const double* nbox, const int* child, const int* ids,
-                           int n, int* cnt, const int* off, int* out, int* status, int* maxq, int* qbuf, const int* qorder) {
-    const int2* ch2 = reinterpret_cast<const int2*>(child);
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += gridDim.x * blockDim.x) {
+// One traversal job: a query kind against its tree.  k_traverse runs two
+// jobs in one launch (blocks [0, nb0) the first, the rest the second), so
+// the 41 k vertex queries of a mesh scene do not run alone on a mostly idle
+// device beside the edge queries.
+struct TravJob {
+    int kind;
+    const double* qbox; int nq;
+    const double* nbox; const int* child; const int* ids; int n;
+    int* cnt; const int* off; int* out; int* maxq; int* qbuf; const int* qorder;
+};
+__device__ __forceinline__ void traverse_job(const PrimGeo& pg, const TravJob& j, int t0, int stride, int* status) {
+    const int kind = j.kind, nq = j.nq, n = j.n;
+    const double* qbox = j.qbox;
+    const double* nbox = j.nbox;
+    const int* ids = j.ids;
+    const int* off = j.off;
+    int* out = j.out;
+    int* qbuf = j.qbuf;
+    const int* qorder = j.qorder;
+    const int2* ch2 = reinterpret_cast<const int2*>(j.child);
+    for (int t = t0; t < nq; t += stride) {
         const int q = qorder ? qorder[t] : t;
         double qb[6];
         for (int a = 0; a < 6; ++a) qb[a] = qbox[6 * q + a];
@@ -557,10 +574,14 @@ __global__ void k_traverse(PrimGeo pg, int kind, const double* qbox, int nq, con
             }
         }
         if (!out) {
-            cnt[q] = c;
-            if (c > kQueryBuf) atomicMax(maxq, c);
+            j.cnt[q] = c;
+            if (c > kQueryBuf) atomicMax(j.maxq, c);
         }
     }
+}
+__global__ void k_traverse(PrimGeo pg, TravJob j0, TravJob j1, int nb0, int* status) {
+    if ((int)blockIdx.x < nb0) traverse_job(pg, j0, blockIdx.x * blockDim.x + threadIdx.x, nb0 * blockDim.x, status);
+    else traverse_job(pg, j1, (blockIdx.x - nb0) * blockDim.x + threadIdx.x, (gridDim.x - nb0) * blockDim.x, status);
 }
 
 // ---------------------------------------------------------------------------

@@ -1622,21 +1622,33 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
     GrowBuf* out[2] = {&s->pt, &s->ee};
     Bvh* tree[2] = {&s->faces, &s->edges};
     GrowBuf* qbuf[2] = {&s->qbuf0, &s->qbuf1};
-    auto launch = [&](int k, bool count) {
+    // one kind's traversal job (buffers read at launch: they may grow)
+    auto job = [&](int k, bool count) {
         Bvh& B = *tree[k];
-        const double* qbox[2] = {s->qv.as<double>(), s->qe.as<double>()};   // read at launch: the buffers may grow
-        int* cn = count ? cnt[k]->as<int>() : nullptr;
-        const int* of = count ? nullptr : off[k]->as<int>();
-        int* dst = count ? nullptr : out[k]->as<int>();
+        TravJob j{};
+        j.kind = k;
+        j.qbox = k == 0 ? s->qv.as<double>() : s->qe.as<double>();
+        j.nq = nq[k];
+        j.nbox = B.nbox.as<double>(); j.child = B.child.as<int>(); j.ids = B.i0.as<int>(); j.n = B.n;
+        j.cnt = count ? cnt[k]->as<int>() : nullptr;
+        j.off = count ? nullptr : off[k]->as<int>();
+        j.out = count ? nullptr : out[k]->as<int>();
+        j.maxq = &ds->maxq[k];
+        j.qbuf = count ? qbuf[k]->as<int>() : nullptr;
+        j.qorder = k == 1 && B.n == nq[1] ? B.i0.as<int>() : nullptr;   // edge queries in the edge tree's leaf order
+        return j;
+    };
+    auto traverse = [&](const TravJob& a, const TravJob* b) {
+        const int nb0 = grid_for(a.nq, 128), nb1 = b ? grid_for(b->nq, 128) : 0;
+        k_traverse<<<nb0 + nb1, 128, 0, c->stream>>>(s->pg, a, b ? *b : a, nb0, &ds->status);
+    };
+    auto launch = [&](int k, bool count) {
         if (sweep)
-            k_sweep_all<<<grid_for(32LL * nq[k], 128), 128, 0, c->stream>>>(s->pg, k, qbox[k], nq[k], B.leaf.as<double>(), B.n,
-                                                                            cn, of, dst);
+            k_sweep_all<<<grid_for(32LL * nq[k], 128), 128, 0, c->stream>>>(
+                s->pg, k, k == 0 ? s->qv.as<double>() : s->qe.as<double>(), nq[k], tree[k]->leaf.as<double>(), tree[k]->n,
+                count ? cnt[k]->as<int>() : nullptr, count ? nullptr : off[k]->as<int>(), count ? nullptr : out[k]->as<int>());
         else
-            k_traverse<<<grid_for(nq[k], 128), 128, 0, c->stream>>>(s->pg, k, qbox[k], nq[k], B.nbox.as<double>(),
-                                                                    B.child.as<int>(), B.i0.as<int>(), B.n, cn, of, dst,
-                                                                    &ds->status, &ds->maxq[k],
-                                                                    count ? qbuf[k]->as<int>() : nullptr,
-                                                                    k == 1 && B.n == nq[1] ? B.i0.as<int>() : nullptr);
+            traverse(job(k, count), nullptr);
     };
     if (phase == 1) {
         // after the fetch: the totals in pinned memory, then the writes
@@ -1721,14 +1733,23 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
     if (c->ne)
         k_ipc_boxes<<<grid_for(c->ne, 256), 256, 0, c->stream>>>(s->pg, 3, s->wq0.as<double>(), w1, 0.0, s->qe.as<double>(), pad);
     NXD_CUDA(cudaMemsetAsync(ds, 0, 6 * sizeof(int), c->stream));   // totals, status, segment count, longest slices
+    bool on[2];
     for (int k = 0; k < 2; ++k) {
-        if (nq[k] == 0 || np[k] == 0) continue;
+        on[k] = nq[k] > 0 && np[k] > 0;
+        if (!on[k]) continue;
         IPC_ENSURE(*cnt[k], 4 * (size_t)nq[k]); IPC_ENSURE(*off[k], 4 * (size_t)nq[k]);
         if (!sweep) IPC_ENSURE(*qbuf[k], 4 * (size_t)kQueryBuf * nq[k]);
-        launch(k, true);
-        if (scan_ints(c->stream, s->scan_sums, cnt[k]->as<int>(), off[k]->as<int>(), nq[k], &ds->tot[k]) != NXD_OK)
-            return NXD_CUDA_ERROR;
     }
+    if (sweep) {
+        for (int k = 0; k < 2; ++k)
+            if (on[k]) launch(k, true);
+    } else if (on[0] || on[1]) {
+        const TravJob a = job(on[0] ? 0 : 1, true), b = job(1, true);   // both kinds counted in one launch
+        traverse(a, on[0] && on[1] ? &b : nullptr);
+    }
+    for (int k = 0; k < 2; ++k)
+        if (on[k] && scan_ints(c->stream, s->scan_sums, cnt[k]->as<int>(), off[k]->as<int>(), nq[k], &ds->tot[k]) != NXD_OK)
+            return NXD_CUDA_ERROR;
     NXD_CUDA(cudaGetLastError());
     return NXD_OK;
 }
