@@ -218,20 +218,57 @@ __global__ void __launch_bounds__(kScanTileThreads) k_scan_tiles(const int* in, 
 }
 
 // Each query's slice of (query, primitive) pairs, [off[q], off[q] + cnt[q]),
-// sorted by primitive in place by insertion, one thread per query (used
-// while no slice is longer than kSliceSortMax; the primitives of a slice are
-// distinct).
+// sorted by primitive in place (the primitives of a slice are distinct).
+// Each warp takes 32 consecutive queries: a slice of at most kSliceSortMax
+// is sorted by its lane (insertion), and the warp then sorts its longer
+// slices one after another together (bitonic network over the slice
+// padded to a power of two in the warp's shared row).  Used while no slice
+// is longer than kLongSliceMax.
 constexpr int kSliceSortMax = 64;
+constexpr int kLongSliceMax = 2048;
 constexpr int kQueryBuf = 16;     // hits kept per query by k_traverse's count pass
-__global__ void k_sort_query_slices(int* pairs, const int* off, const int* cnt, int nq) {
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
-        const int m = cnt[q];
-        int* p = pairs + 2 * (size_t)off[q] + 1;    // primitives at stride 2
-        for (int i = 1; i < m; ++i) {
-            const int v = p[2 * i];
-            int j = i - 1;
-            while (j >= 0 && p[2 * j] > v) { p[2 * (j + 1)] = p[2 * j]; --j; }
-            p[2 * (j + 1)] = v;
+constexpr int kSliceSortThreads = 128;
+__global__ void __launch_bounds__(kSliceSortThreads) k_sort_query_slices(int* pairs, const int* off, const int* cnt, int nq) {
+    __shared__ int row[kSliceSortThreads / 32][kLongSliceMax];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int* sh = row[threadIdx.x >> 5];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; base < nq; base += stride) {
+        const int q = (int)base + lane;
+        const int m = q < nq ? cnt[q] : 0;
+        if (m <= kSliceSortMax) {
+            int* p = pairs + 2 * (size_t)(q < nq ? off[q] : 0) + 1;    // primitives at stride 2
+            for (int i = 1; i < m; ++i) {
+                const int v = p[2 * i];
+                int j = i - 1;
+                while (j >= 0 && p[2 * j] > v) { p[2 * (j + 1)] = p[2 * j]; --j; }
+                p[2 * (j + 1)] = v;
+            }
+        }
+        unsigned longer = __ballot_sync(full, m > kSliceSortMax);
+        while (longer) {
+            const int src = __ffs(longer) - 1;
+            longer &= longer - 1;
+            const int mm = __shfl_sync(full, m, src);
+            int* p = pairs + 2 * (size_t)off[(int)base + src] + 1;
+            int P = 2 * kSliceSortMax;
+            while (P < mm) P <<= 1;
+            for (int i = lane; i < P; i += 32) sh[i] = i < mm ? p[2 * i] : 0x7fffffff;
+            __syncwarp();
+            for (int k = 2; k <= P; k <<= 1)
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    for (int i = lane; i < P; i += 32) {
+                        const int l = i ^ j;
+                        if (l > i) {
+                            const int x = sh[i], y = sh[l];
+                            if ((i & k) == 0 ? x > y : x < y) { sh[i] = y; sh[l] = x; }
+                        }
+                    }
+                    __syncwarp();
+                }
+            for (int i = lane; i < mm; i += 32) p[2 * i] = sh[i];
+            __syncwarp();
         }
     }
 }

@@ -1670,12 +1670,13 @@ nxd_status ipc_candidates_pass(nxd_ctx* c, bool swept, double infl, int phase) {
             if (sweep || m < 2) continue;
             // traversal order -> (query, primitive) ascending: the queries'
             // slices are already in query order, so each is sorted alone
-            // (one thread each) while the longest is short; a query with
-            // many hits (a long edge against a fine mesh) would serialise a
-            // thread, so then one stable radix sort of (query, primitive) keys
-            if (s->hp->sc.maxq[k] <= kSliceSortMax) {
-                k_sort_query_slices<<<grid_for(nq[k], 128), 128, 0, c->stream>>>(out[k]->as<int>(), off[k]->as<int>(),
-                                                                                 cnt[k]->as<int>(), nq[k]);
+            // (by its lane, or by its warp when longer than kSliceSortMax)
+            // while the longest fits a warp's shared row; past that (a long
+            // edge against thousands of a fine mesh's edges) one stable
+            // radix sort of (query, primitive) keys
+            if (s->hp->sc.maxq[k] <= kLongSliceMax) {
+                k_sort_query_slices<<<grid_for(nq[k], kSliceSortThreads), kSliceSortThreads, 0, c->stream>>>(
+                    out[k]->as<int>(), off[k]->as<int>(), cnt[k]->as<int>(), nq[k]);
                 continue;
             }
             const int pbits = bits_for((unsigned long long)std::max(np[k], 1));

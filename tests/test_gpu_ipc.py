@@ -67,6 +67,35 @@ def test_ipc_candidates_identical(name):
         assert np.array_equal(a, b)
 
 
+def long_slice_scene():
+    """A 2562-vertex icosphere (7680 edges) resting on a 12-triangle box: the
+    box's edges are queries whose hits cover the sphere's edges."""
+    sb = scenes.SceneBuilder("long_slices")
+    gv, gf = scenes.box_mesh(0.3, 0.05, 0.3)
+    g = sb.add_body(gv, gf, (0.0, -0.05, 0.0))
+    sb.fix(g)
+    iv, if_ = scenes.icosphere(4)
+    sb.add_body(iv * 0.1, if_, (0.0, 0.1005, 0.0))
+    return sb.build(scenes._settings(1e-3, 0.0), dt=1e-2, steps=1)
+
+
+def test_ipc_candidates_long_slices():
+    """Candidate lists whose longest per-query slice takes each sort: at
+    inflation 0.02 the longest edge slice has 800 pairs (past the per-lane
+    insertion sort, inside a warp's shared row); at 0.5 the slices reach
+    5120 and 7680 pairs (the radix sort of packed keys)."""
+    sc = long_slice_scene()
+    ctx = runtime().Context(sc)
+    ow = refcpu.OracleWorld(sc)
+    x = scene_x(sc, 1, 1e-5)
+    for infl, longest in ((0.02, 800), (0.5, 7680)):
+        gpt, gee = ctx.ipc_candidates(x, None, infl)
+        opt, oee = ow.ipc_candidates(x, None, infl)
+        assert max(np.bincount(a[:, 0]).max() for a in (opt, oee)) == longest
+        assert np.array_equal(gpt, opt), (infl, len(gpt), len(opt))
+        assert np.array_equal(gee, oee), (infl, len(gee), len(oee))
+
+
 @pytest.mark.parametrize("name", list(SCENES))
 def test_ipc_barrier_matches_oracle(name):
     make, jitter = SCENES[name]
