@@ -1144,18 +1144,18 @@ __global__ void k_ipc_rowptr(const unsigned long long* hkey, const int* start, c
 // ---------------------------------------------------------------------------
 // Additive CCD over the candidate pairs (swept boxes): per pair the time of
 // impact along its points' motion (ipc::accd_toi_motion; the step uses the
-// rigid arcs, ipc::ArcMotion), one warp per pair with a round's
-// kAccdLookahead samples in its lanes, then the minimum (one block).
+// rigid arcs, ipc::ArcMotion), then the minimum (one block).  Each warp
+// takes 32 pairs: every lane evaluates its pair's Lipschitz bound and
+// start distance and settles the pairs whose first safe advance already
+// reaches t_max (most candidates of a step); the warp then runs the pairs
+// left one after another, a round's kAccdLookahead samples in its lanes.
+// The arithmetic per pair is accd_toi_motion's, so the bound is the same.
 // ---------------------------------------------------------------------------
 static_assert(ipc::kAccdLookahead == 32, "one sample per lane");
 template <typename M>
-__device__ double accd_toi_warp(int kind, const M& m, double t_max, double eta, int max_iter) {
+__device__ double accd_toi_warp(const M& m, double lp, double d0, double t_max, double eta, int max_iter) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const double lp = m.lipschitz();
-    const double d0 = m.distance(0.0);
-    if (!(lp > 0.0)) return t_max;
-    if (!(d0 > 0.0)) return 0.0;
     const double g = eta * d0;
     double t = 0.0, d = d0;
     for (int it = 0; it < max_iter; ++it) {
@@ -1180,29 +1180,59 @@ __device__ double accd_toi_warp(int kind, const M& m, double t_max, double eta, 
 
 // Time of impact of each candidate pair along the rigid arcs x + t dx
 // (ipc::ArcMotion: body-local vertices vloc, step-start orientations q0).
+__device__ __forceinline__ void arc_motion_of(const PrimGeo& pg, const IpcPairs& P, int p, const double* vloc,
+                                              const double* x, const double* dx, const double* q0, ipc::ArcMotion& m) {
+    int vid[4], kind, bA, bB;
+    pair_vids(pg, P, p, vid, kind, bA, bB);
+    m.kind = kind;
+    fric_sides(kind, m.side);
+    const int b[2] = {bA, bB};
+    for (int sd = 0; sd < 2; ++sd) {
+        m.b[sd].p = ld3(x + 6 * b[sd]);
+        m.b[sd].th = ld3(x + 6 * b[sd] + 3);
+        m.b[sd].dp = ld3(dx + 6 * b[sd]);
+        m.b[sd].dth = ld3(dx + 6 * b[sd] + 3);
+        m.b[sd].q0 = ldq(q0 + 4 * b[sd]);
+    }
+    for (int k = 0; k < 4; ++k) m.v[k] = ld3(vloc + 3 * vid[k]);
+}
 __global__ void k_ipc_accd(PrimGeo pg, IpcPairs P, const double* vloc, const double* x, const double* dx, const double* q0,
                            double eta, int max_iter, double* toi) {
+    const unsigned full = 0xffffffffu;
+    const double t_max = 1.0;
     const int n = P.n_pt + P.n_ee;
-    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long pp = w0; pp < n; pp += nw) {
-        const int p = (int)pp;
-        int vid[4], kind, bA, bB;
-        pair_vids(pg, P, p, vid, kind, bA, bB);
-        ipc::ArcMotion m;
-        m.kind = kind;
-        fric_sides(kind, m.side);
-        const int b[2] = {bA, bB};
-        for (int sd = 0; sd < 2; ++sd) {
-            m.b[sd].p = ld3(x + 6 * b[sd]);
-            m.b[sd].th = ld3(x + 6 * b[sd] + 3);
-            m.b[sd].dp = ld3(dx + 6 * b[sd]);
-            m.b[sd].dth = ld3(dx + 6 * b[sd] + 3);
-            m.b[sd].q0 = ldq(q0 + 4 * b[sd]);
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; base < n; base += stride) {
+        const int p = (int)base + lane;
+        double lp = 0.0, d0 = 0.0;
+        bool need = false;
+        if (p < n) {
+            ipc::ArcMotion m;
+            arc_motion_of(pg, P, p, vloc, x, dx, q0, m);
+            lp = m.lipschitz();
+            d0 = m.distance(0.0);
+            // accd_toi_motion's exits before its first round of samples
+            double res = 0.0;
+            if (!(lp > 0.0)) {
+                res = t_max;
+            } else if (d0 > 0.0 && max_iter > 0) {
+                const double dl = 0.9 * (d0 - eta * d0) / lp;
+                if (0.0 + dl >= t_max) res = t_max;
+                else need = dl > 1e-12 * t_max;
+            }
+            if (!need) toi[p] = res;
         }
-        for (int k = 0; k < 4; ++k) m.v[k] = ld3(vloc + 3 * vid[k]);
-        const double tp = accd_toi_warp(kind, m, 1.0, eta, max_iter);
-        if ((threadIdx.x & 31) == 0) toi[p] = tp;
+        unsigned todo = __ballot_sync(full, need);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const double lps = __shfl_sync(full, lp, src), d0s = __shfl_sync(full, d0, src);
+            ipc::ArcMotion m;
+            arc_motion_of(pg, P, (int)base + src, vloc, x, dx, q0, m);
+            const double tp = accd_toi_warp(m, lps, d0s, t_max, eta, max_iter);
+            if (lane == 0) toi[(int)base + src] = tp;
+        }
     }
 }
 

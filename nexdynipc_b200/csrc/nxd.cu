@@ -1965,7 +1965,7 @@ nxd_status ipc_accd(nxd_ctx* c, double eta) {
     IPC_ENSURE(s->toi, 8 * (size_t)std::max(n, 1));
     const IpcPairs P{s->pt.as<int>(), s->n_pt, s->ee.as<int>(), s->n_ee};
     // along the rigid arcs from the last ipc_pose's x (x0) by its dx
-    if (n) k_ipc_accd<<<grid_for(32LL * n, 128), 128, 0, c->stream>>>(s->pg, P, c->geo.verts, s->x0.as<double>(),
+    if (n) k_ipc_accd<<<grid_for(n, 128), 128, 0, c->stream>>>(s->pg, P, c->geo.verts, s->x0.as<double>(),
                                                                 s->dxv.as<double>(), c->quat, eta, 1000, s->toi.as<double>());
     k_min_reduce<<<1, 1024, 0, c->stream>>>(s->toi.as<double>(), n, 1.0, &s->ds()->alpha);
     NXD_CUDA(cudaGetLastError());
