@@ -1144,12 +1144,13 @@ __global__ void k_ipc_rowptr(const unsigned long long* hkey, const int* start, c
 // ---------------------------------------------------------------------------
 // Additive CCD over the candidate pairs (swept boxes): per pair the time of
 // impact along its points' motion (ipc::accd_toi_motion; the step uses the
-// rigid arcs, ipc::ArcMotion), then the minimum (one block).  Each warp
-// takes 32 pairs: every lane evaluates its pair's Lipschitz bound and
-// start distance and settles the pairs whose first safe advance already
-// reaches t_max (most candidates of a step); the warp then runs the pairs
-// left one after another, a round's kAccdLookahead samples in its lanes.
-// The arithmetic per pair is accd_toi_motion's, so the bound is the same.
+// rigid arcs, ipc::ArcMotion), then the minimum (one block).  A thread per
+// pair evaluates its Lipschitz bound and start distance and settles the
+// pairs whose first safe advance already reaches t_max (most candidates of
+// a step); the pairs left are appended to a list (k_ipc_accd), and a warp
+// per listed pair then samples kAccdLookahead points a round in its lanes
+// (k_ipc_accd_rounds).  The arithmetic per pair is accd_toi_motion's, so
+// the bound is the same, whichever warp takes which pair.
 // ---------------------------------------------------------------------------
 static_assert(ipc::kAccdLookahead == 32, "one sample per lane");
 template <typename M>
@@ -1197,7 +1198,7 @@ __device__ __forceinline__ void arc_motion_of(const PrimGeo& pg, const IpcPairs&
     for (int k = 0; k < 4; ++k) m.v[k] = ld3(vloc + 3 * vid[k]);
 }
 __global__ void k_ipc_accd(PrimGeo pg, IpcPairs P, const double* vloc, const double* x, const double* dx, const double* q0,
-                           double eta, int max_iter, double* toi) {
+                           double eta, int max_iter, double* toi, int* list, double2* lpd0, int* nlist) {
     const unsigned full = 0xffffffffu;
     const double t_max = 1.0;
     const int n = P.n_pt + P.n_ee;
@@ -1223,16 +1224,31 @@ __global__ void k_ipc_accd(PrimGeo pg, IpcPairs P, const double* vloc, const dou
             }
             if (!need) toi[p] = res;
         }
-        unsigned todo = __ballot_sync(full, need);
-        while (todo) {
-            const int src = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const double lps = __shfl_sync(full, lp, src), d0s = __shfl_sync(full, d0, src);
-            ipc::ArcMotion m;
-            arc_motion_of(pg, P, (int)base + src, vloc, x, dx, q0, m);
-            const double tp = accd_toi_warp(m, lps, d0s, t_max, eta, max_iter);
-            if (lane == 0) toi[(int)base + src] = tp;
+        const unsigned todo = __ballot_sync(full, need);
+        if (!todo) continue;
+        int at = 0;
+        if (lane == 0) at = atomicAdd(nlist, __popc(todo));
+        at = __shfl_sync(full, at, 0) + __popc(todo & ((1u << lane) - 1u));
+        if (need) {
+            list[at] = p;
+            lpd0[at] = make_double2(lp, d0);
         }
+    }
+}
+// One warp per listed pair: accd_toi_motion's rounds from its start.
+__global__ void k_ipc_accd_rounds(PrimGeo pg, IpcPairs P, const double* vloc, const double* x, const double* dx,
+                                  const double* q0, double eta, int max_iter, const int* list, const double2* lpd0,
+                                  const int* nlist, double* toi) {
+    const int m_ = *nlist;
+    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long k = w0; k < m_; k += nw) {
+        const int p = list[k];
+        const double2 ld = lpd0[k];
+        ipc::ArcMotion m;
+        arc_motion_of(pg, P, p, vloc, x, dx, q0, m);
+        const double tp = accd_toi_warp(m, ld.x, ld.y, 1.0, eta, max_iter);
+        if ((threadIdx.x & 31) == 0) toi[p] = tp;
     }
 }
 

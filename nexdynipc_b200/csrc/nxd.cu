@@ -1349,7 +1349,7 @@ struct IpcScal {
     int nseg;           // segment count of the last ipc_segments
     int maxq[2];        // the most candidates of one query, per kind
     int na;             // active barrier pairs
-    int pad;
+    int naccd;          // CCD pairs left for the sampling rounds
     long long rnz;      // rest-form Hessian blocks
     double energy;      // barrier energy
     double alpha;       // CCD step bound
@@ -1398,7 +1398,7 @@ struct IpcState {
     }
     GrowBuf e, grad12, lam, z, nterm, body, active, type, apos, alist;
     GrowBuf gkey, gval, gkey1, gval1, hkey, hval, hkey1, hval1;
-    GrowBuf sflag, spos, sstart, gout, rowptr, colidx, vals, toi;
+    GrowBuf sflag, spos, sstart, gout, rowptr, colidx, vals, toi, accd_list, accd_lpd0;
     // step adjoint: per-pair blocks, dense K^T and K_phi, vectors, outputs
     GrowBuf akp, akf, abody, aact, aK, aKphi, ax, axb, alam, aout, afail;
     GrowBuf afkp, afkf, afks, afgm, afbody, aKps, agmu;   // its friction pairs (lagged at the step start)
@@ -1411,7 +1411,7 @@ struct IpcState {
                 &faces.flags, &faces.bounds, &edges.k0, &edges.k1, &edges.i0, &edges.i1, &edges.leaf, &edges.nbox, &edges.rng,
                 &edges.child, &edges.parent, &edges.flags, &edges.bounds, &cnt, &off, &cnt2, &off2, &pt, &ee, &scal, &hist, &e,
                 &grad12, &lam, &z, &nterm, &body, &active, &type, &apos, &alist, &gkey, &gval, &gkey1, &gval1, &hkey,
-                &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &rrp, &rci, &rvv,
+                &hval, &hkey1, &hval1, &sflag, &spos, &sstart, &gout, &rowptr, &colidx, &vals, &toi, &accd_list, &accd_lpd0, &rrp, &rci, &rvv,
                 &mrp, &mci, &mvv, &gr, &gt, &gneg, &prod, &xt, &erow, &items, &iact, &stat, &akp, &akf, &abody, &aact,
                 &aK, &aKphi, &ax, &axb, &alam, &aout, &afail, &tkey, &tval, &tkey1, &tval1, &qbuf0, &qbuf1, &dxv, &rmax, &pad, &scan_sums, &afkp, &afkf, &afks, &afgm, &afbody,
                 &aKps, &agmu, &fr_vid, &fr_body, &fr_kind, &fr_w, &fr_nrm, &fr_lam,
@@ -1963,10 +1963,21 @@ nxd_status ipc_accd(nxd_ctx* c, double eta) {
     IpcState* s = c->ipc;
     const int n = s->n_pt + s->n_ee;
     IPC_ENSURE(s->toi, 8 * (size_t)std::max(n, 1));
+    IPC_ENSURE(s->accd_list, 4 * (size_t)std::max(n, 1));
+    IPC_ENSURE(s->accd_lpd0, 16 * (size_t)std::max(n, 1));
     const IpcPairs P{s->pt.as<int>(), s->n_pt, s->ee.as<int>(), s->n_ee};
     // along the rigid arcs from the last ipc_pose's x (x0) by its dx
-    if (n) k_ipc_accd<<<grid_for(n, 128), 128, 0, c->stream>>>(s->pg, P, c->geo.verts, s->x0.as<double>(),
-                                                                s->dxv.as<double>(), c->quat, eta, 1000, s->toi.as<double>());
+    if (n) {
+        int* nl = &s->ds()->naccd;
+        NXD_CUDA(cudaMemsetAsync(nl, 0, sizeof(int), c->stream));
+        k_ipc_accd<<<grid_for(n, 128), 128, 0, c->stream>>>(s->pg, P, c->geo.verts, s->x0.as<double>(), s->dxv.as<double>(),
+                                                            c->quat, eta, 1000, s->toi.as<double>(), s->accd_list.as<int>(),
+                                                            s->accd_lpd0.as<double2>(), nl);
+        // a warp per listed pair: at most 16 warps per SM, striding over the list
+        k_ipc_accd_rounds<<<grid_for(32LL * n, 128, 148 * 4), 128, 0, c->stream>>>(
+            s->pg, P, c->geo.verts, s->x0.as<double>(), s->dxv.as<double>(), c->quat, eta, 1000, s->accd_list.as<int>(),
+            s->accd_lpd0.as<double2>(), nl, s->toi.as<double>());
+    }
     k_min_reduce<<<1, 1024, 0, c->stream>>>(s->toi.as<double>(), n, 1.0, &s->ds()->alpha);
     NXD_CUDA(cudaGetLastError());
     return NXD_OK;
