@@ -1595,9 +1595,12 @@ nxd_status ipc_build_bvh(nxd_ctx* c, Bvh& B, int kind, bool swept, double infl) 
 // query < primitive) at the posed world vertices: primitive boxes inflated
 // by infl (swept over wq0 -> wq1 when swept), query boxes not inflated.
 // Scenes of at most kSweepAllTests box tests take the all-pairs sweep, whose
-// hits come out sorted; larger ones build an LBVH per kind, traverse it and
-// sort each kind's pairs by (query, primitive) with one radix sort.  Both
-// kinds are counted before the one host wait that reads their totals.
+// hits come out sorted; larger ones build (or refit) an LBVH per kind,
+// count both kinds' hits in one traversal launch and put each query's hits
+// in primitive order (copied from the count pass's per-query rows, or
+// written by a second traversal and sorted per query, or past 2048 hits in
+// one query by a radix sort of all pairs).  Both kinds are counted before
+// the one host wait that reads their totals.
 constexpr long long kSweepAllTests = 1LL << 22;
 // ipc_candidates = ipc_candidates_begin (boxes, trees, counts and their
 // scans, all queued) + one ipc_fetch + ipc_candidates_end (the writes); a
