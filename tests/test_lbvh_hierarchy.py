@@ -11,6 +11,9 @@ k_karras builds it over sorted unique 64-bit keys (Morton << 32 | index)).
 - A walk that tests both children at their parent (k_traverse) finds
   exactly the leaves whose boxes overlap the query box.
 - The depth stays far below the traversal's stack of 96 entries.
+- The bitonic network that sorts a query's candidate slice longer than 64
+  in its warp's shared row (k_sort_query_slices) sorts every length up to
+  2048.
 """
 import numpy as np
 
@@ -218,3 +221,34 @@ def test_depth_is_within_the_traversal_stack():
     for bits in (30, 8):
         child, _ = karras(sample_keys(r, 4000, bits))
         assert depth(child) < 96
+
+
+def bitonic_slice_sort(vals):
+    """k_sort_query_slices' network for a slice longer than 64: padded with
+    INT_MAX to a power of two P >= 128, compare-exchange over (k, j), the
+    element pairs (i, i ^ j) ascending where i & k == 0."""
+    m = len(vals)
+    P = 128
+    while P < m:
+        P <<= 1
+    sh = list(vals) + [0x7fffffff] * (P - m)
+    k = 2
+    while k <= P:
+        j = k >> 1
+        while j > 0:
+            for i in range(P):
+                l = i ^ j
+                if l > i:
+                    x, y = sh[i], sh[l]
+                    if (x > y) if (i & k) == 0 else (x < y):
+                        sh[i], sh[l] = y, x
+            j >>= 1
+        k <<= 1
+    return sh[:m]
+
+
+def test_slice_bitonic_network_sorts_every_length():
+    r = np.random.default_rng(15)
+    for m in list(range(65, 140)) + [255, 256, 257, 511, 1000, 1023, 1024, 1025, 2047, 2048]:
+        vals = r.choice(200000, size=m, replace=False).tolist()   # a slice's primitives are distinct
+        assert bitonic_slice_sort(vals) == sorted(vals)
